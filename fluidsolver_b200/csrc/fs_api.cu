@@ -1,0 +1,1016 @@
+// C-ABI of the B200 hot path (declared in include/fluidsolver_b200.h):
+// context management, host transfers, the neighborhood-search pipeline and
+// the per-solver step sequences.
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "fs_context.cuh"
+#include "fs_search.cuh"
+#include "fs_solvers.cuh"
+
+using namespace fsb;
+
+namespace {
+
+thread_local std::string g_error;
+
+fs_status fail(fs_status s, const std::string& msg) {
+    g_error = msg;
+    return s;
+}
+
+#define FS_CUDA(call)                                                                              \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(FS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));          \
+    } while (0)
+
+#define FS_TRY(call)                       \
+    do {                                   \
+        fs_status s_ = (call);             \
+        if (s_ != FS_OK) return s_;        \
+    } while (0)
+
+constexpr int kBlock = 128;
+
+inline unsigned grid_for(int64_t n, int block = kBlock) {
+    int64_t g = (n + block - 1) / block;
+    return (unsigned)std::max<int64_t>(g, 1);
+}
+
+template <typename T> fs_status dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    FS_CUDA(cudaMalloc((void**)p, count * sizeof(T)));
+    return FS_OK;
+}
+
+// host-side replicas of the reference's float constants
+float kernel_alpha(int dim, float h) {
+    const float pi = 3.14159265358979323846f;
+    if (dim == 2) return 5.0f / (14.0f * pi * (h * h));
+    return 1.0f / (4.0f * pi * ((h * h) * h));
+}
+
+bool contract_is_2d(int search) {
+    return search == FS_SEARCH_QUADRATIC_2D || search == FS_SEARCH_HASHED_2D || search == FS_SEARCH_COMPACT_2D;
+}
+
+// owners of the contract's lists, as a bit mask over particle types
+uint32_t contract_owner_mask(int search) {
+    const uint32_t normal = 1u << FS_TYPE_NORMAL, bnd = 1u << FS_TYPE_BOUNDARY, ina = 1u << FS_TYPE_INACTIVE;
+    switch (search) {
+        case FS_SEARCH_QUADRATIC_2D: return normal | bnd | ina;
+        case FS_SEARCH_HASHED_2D: return normal;
+        default: return normal | bnd;
+    }
+}
+
+int contract_capacity(int search) {
+    if (search == FS_SEARCH_COMPRESSED_3D) return 97;   // CompressedNeighbors.hpp:29-33 (first + 96 deltas)
+    if (search == FS_SEARCH_COMPACT_2D) return 40;      // CompactHashingNeighborhoodSearch.cpp:5
+    return 0;
+}
+
+template <typename R> State<R> state_of(fs_ctx* c) {
+    State<R> s;
+    s.pos = (V4<R>*)c->pos[c->cur];
+    s.vel = (V4<R>*)c->vel[c->cur];
+    s.acc = (V4<R>*)c->acc[c->cur];
+    s.ext = (V4<R>*)c->ext[c->cur];
+    s.rho = (R*)c->rho[c->cur];
+    s.rho_prev = (R*)c->rho_prev;
+    s.p = (R*)c->p[c->cur];
+    s.vstar = (V4<R>*)c->vstar;
+    s.anp = (V4<R>*)c->anp;
+    s.err = (R*)c->err;
+    s.type = c->type[c->cur];
+    s.hidx = c->hidx[c->cur];
+    return s;
+}
+
+template <typename R> SolverConsts<R> consts_of(fs_ctx* c) {
+    const fs_params& p = c->prm;
+    SolverConsts<R> k;
+    k.kern.h = (R)c->kernel_h;
+    k.kern.alpha = (R)c->kernel_alpha;
+    k.rest_density = (R)p.rest_density;
+    k.rho0_sq = (R)(p.rest_density * p.rest_density);
+    k.gravity = (R)p.gravity;
+    k.visc_eps = (R)((0.01f * p.particle_size) * p.particle_size);
+    k.two_nu = (R)(2.0f * p.viscosity);
+    k.omega = (R)p.omega;
+    k.gamma = (R)p.gamma;
+    k.two_gamma = (R)(2.0f * p.gamma);
+    k.gamma1 = (R)p.single_layer_gamma_1;
+    k.gamma2 = (R)p.single_layer_gamma_2;
+    k.stiffness = (R)p.stiffness;
+    k.single_layer = c->dim == 3 && p.single_layer_boundary != 0;
+    k.dim = c->dim;
+    k.max_density_error = (R)p.max_density_error;
+    k.min_iterations = p.min_iterations;
+    k.max_iterations = p.max_iterations;
+    if (std::is_same<R, double>::value) {
+        // the FP64 build evaluates the same formulas in double
+        const double h = (double)p.particle_size * 2.0 / 2.0;
+        const double pi = 3.14159265358979323846;
+        k.kern.h = (R)h;
+        k.kern.alpha = (R)(c->dim == 2 ? 5.0 / (14.0 * pi * h * h) : 1.0 / (4.0 * pi * h * h * h));
+        k.rho0_sq = (R)((double)p.rest_density * p.rest_density);
+        k.visc_eps = (R)(0.01 * p.particle_size * p.particle_size);
+        k.two_nu = (R)(2.0 * p.viscosity);
+        k.two_gamma = (R)(2.0 * p.gamma);
+    }
+    return k;
+}
+
+Lists lists_of(fs_ctx* c) {
+    Lists L;
+    L.nbr = c->nbr;
+    L.count = c->nbr_count;
+    L.stride = c->nbr_stride;
+    L.K = c->nbr_capacity;
+    return L;
+}
+
+WalkParams walk_of(fs_ctx* c, bool for_solver) {
+    WalkParams w;
+    w.r = c->search_radius;
+    w.r2 = c->radius2;
+    w.dim = c->dim;
+    w.regions = c->reference_order ? 1 : (c->include_inactive && !for_solver ? 3 : 2);
+    w.candidates_inactive = c->include_inactive && !for_solver;
+    w.d0 = c->dims[0];
+    w.d1 = c->dims[1];
+    w.d2 = c->dims[2];
+    w.cell_cap = c->cell_capacity;
+    return w;
+}
+
+fs_status check_params(const fs_params* p) {
+    if (!p) return fail(FS_ERR_INVALID, "params is null");
+    if (p->dim != 2 && p->dim != 3) return fail(FS_ERR_INVALID, "dim must be 2 or 3");
+    if (p->search < FS_SEARCH_QUADRATIC_2D || p->search > FS_SEARCH_COMPRESSED_3D)
+        return fail(FS_ERR_INVALID, "unknown search kind");
+    if (contract_is_2d(p->search) != (p->dim == 2))
+        return fail(FS_ERR_INVALID, "search kind does not match the dimension");
+    if (p->solver == FS_SOLVER_SESPH_2D || p->solver == FS_SOLVER_IISPH_2D) {
+        if (p->dim != 2) return fail(FS_ERR_INVALID, "2D solver needs dim 2");
+    } else if (p->solver == FS_SOLVER_SESPH_3D || p->solver == FS_SOLVER_IISPH_3D) {
+        if (p->dim != 3) return fail(FS_ERR_INVALID, "3D solver needs dim 3");
+    } else if (p->solver != FS_SOLVER_NONE) {
+        return fail(FS_ERR_INVALID, "unknown solver kind");
+    }
+    if (p->precision < 0 || p->precision > 2) return fail(FS_ERR_INVALID, "unknown precision");
+    if (!(p->particle_size > 0.0f)) return fail(FS_ERR_INVALID, "Search radius is smaller or equal to zero.");
+    if (p->solver == FS_SOLVER_IISPH_2D || p->solver == FS_SOLVER_IISPH_3D) {
+        if (p->max_iterations < p->min_iterations)
+            return fail(FS_ERR_INVALID, "Max iterations are less than min number of iterations.");
+        if (!(p->max_density_error > 0.0f))
+            return fail(FS_ERR_INVALID, "MaxDensityErrorAllowed is smaller or equal to zero.");
+        if (p->min_iterations < 0) return fail(FS_ERR_INVALID, "min iterations must be >= 0");
+    }
+    if (p->solver != FS_SOLVER_NONE && !(p->timestep > 0.0f))
+        return fail(FS_ERR_INVALID, "Timestep is smaller or equal to zero.");
+    if (p->max_particles <= 0 || p->max_particles > (int64_t)0x7fffffff)
+        return fail(FS_ERR_INVALID, "max_particles must be in [1, 2^31)");
+    return FS_OK;
+}
+
+void derive(fs_ctx* c) {
+    const fs_params& p = c->prm;
+    c->dim = p.dim;
+    c->precision = p.precision;
+    c->real_size = p.precision == FS_PRECISION_FP64 ? 8 : 4;
+    c->search_radius = p.particle_size * 2.0f;                 // kernel_support_factor (LibFluidMath.hpp:11)
+    c->radius2 = c->search_radius * c->search_radius;         // HashedNeighborhoodSearch3D.cpp:305
+    c->kernel_h = (p.particle_size * 2.0f) / 2.0f;             // CubicSplineKernel3D.cpp:69
+    c->kernel_alpha = kernel_alpha(p.dim, c->kernel_h);
+    c->reference_order = (p.flags & FS_FLAG_REFERENCE_ORDER) != 0;
+    c->include_inactive = p.search == FS_SEARCH_QUADRATIC_2D || p.search == FS_SEARCH_HASHED_2D;
+}
+
+fs_status free_all(fs_ctx* c) {
+    void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc[0], c->acc[1], c->ext[0], c->ext[1],
+                    c->rho[0], c->rho[1], c->p[0], c->p[1], c->type[0], c->type[1], c->hidx[0], c->hidx[1],
+                    c->rho_prev, c->vstar, c->anp, c->err, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
+                    c->perm[0], c->perm[1], c->cub_temp, c->cell_range, c->bbox, c->origin, c->nbr, c->nbr_count,
+                    c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->scalars};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->scalars_host) cudaFreeHost(c->scalars_host);
+    if (c->loop_exec) cudaGraphExecDestroy(c->loop_exec);
+    if (c->loop_graph) cudaGraphDestroy(c->loop_graph);
+    if (c->step_exec) cudaGraphExecDestroy(c->step_exec);
+    if (c->step_graph) cudaGraphDestroy(c->step_graph);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    return FS_OK;
+}
+
+fs_status ensure_staging(fs_ctx* c, size_t bytes) {
+    if (c->staging_bytes >= bytes) return FS_OK;
+    if (c->staging) cudaFree(c->staging);
+    c->staging = nullptr;
+    c->staging_bytes = 0;
+    FS_CUDA(cudaMalloc(&c->staging, bytes));
+    c->staging_bytes = bytes;
+    return FS_OK;
+}
+
+fs_status ensure_lists(fs_ctx* c, int K) {
+    const int64_t stride = ((c->cap + 31) / 32) * 32;
+    if (c->nbr && c->nbr_capacity >= K && c->nbr_stride == stride) return FS_OK;
+    if (c->nbr) cudaFree(c->nbr);
+    c->nbr = nullptr;
+    FS_TRY(dalloc(&c->nbr, (size_t)K * stride));
+    c->nbr_capacity = K;
+    c->nbr_stride = stride;
+    return FS_OK;
+}
+
+// cell-grid dims from the host positions: bounding box + margin, clamped to
+// 1024 per axis and to a total table size
+void choose_dims(fs_ctx* c, const float* pos, const uint8_t* type, int64_t n) {
+    int lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+    const int dim = c->dim;
+    for (int64_t i = 0; i < n; i++) {
+        if (!c->include_inactive && type && type[i] == FS_TYPE_INACTIVE) continue;
+        for (int a = 0; a < dim; a++) {
+            float x = pos[i * dim + a];
+            if (!(std::fabs(x) < 1e30f)) continue;
+            float q = std::floor(x / c->search_radius);
+            int cc = (int)std::max(-1.0e9f, std::min(1.0e9f, q));
+            lo[a] = std::min(lo[a], cc);
+            hi[a] = std::max(hi[a], cc);
+        }
+    }
+    int64_t ext[3] = {1, 1, 1};
+    for (int a = 0; a < dim; a++) {
+        if (lo[a] > hi[a]) { lo[a] = hi[a] = 0; }
+        int64_t e = (int64_t)hi[a] - lo[a] + 1;
+        int64_t margin = std::max<int64_t>(4, e / 4);
+        ext[a] = std::min<int64_t>(kMaxDimCells, e + 2 * margin);
+    }
+    const int64_t max_cells = std::max<int64_t>(int64_t(1) << 22, 8 * std::max<int64_t>(c->cap, 1));
+    while (ext[0] * ext[1] * ext[2] > max_cells) {
+        int a = (ext[0] >= ext[1] && ext[0] >= ext[2]) ? 0 : (ext[1] >= ext[2] ? 1 : 2);
+        ext[a] = std::max<int64_t>(1, (ext[a] * 3) / 4);
+    }
+    for (int a = 0; a < 3; a++) c->dims[a] = (int)ext[a];
+}
+
+fs_status ensure_cells(fs_ctx* c) {
+    const int64_t cells = (int64_t)c->dims[0] * c->dims[1] * c->dims[2];
+    if (c->cell_range && c->cell_capacity >= cells) return FS_OK;
+    if (c->cell_range) cudaFree(c->cell_range);
+    c->cell_range = nullptr;
+    c->cell_capacity = cells;
+    FS_TRY(dalloc(&c->cell_range, (size_t)3 * cells));
+    return FS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// upload / download
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void k_pack(int64_t n, int dim, const float* __restrict__ pos, const float* __restrict__ vel,
+                       const float* __restrict__ acc, const float* __restrict__ ext, const float* __restrict__ mass,
+                       const float* __restrict__ rho, const float* __restrict__ p, const uint8_t* __restrict__ type,
+                       float rest_density, State<R> s, uint8_t* __restrict__ type_out, uint32_t* __restrict__ hidx_out) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    auto ld = [&](const float* a) -> V3<R> {
+        if (!a) return v3<R>(R(0), R(0), R(0));
+        return dim == 2 ? v3<R>((R)a[2 * i], (R)a[2 * i + 1], R(0)) : v3<R>((R)a[3 * i], (R)a[3 * i + 1], (R)a[3 * i + 2]);
+    };
+    s.pos[i] = v4<R>(ld(pos), mass ? (R)mass[i] : R(1));
+    s.vel[i] = v4<R>(ld(vel), R(0));
+    s.acc[i] = v4<R>(ld(acc), R(0));
+    s.ext[i] = v4<R>(ld(ext), R(0));
+    s.rho[i] = rho ? (R)rho[i] : (R)rest_density;
+    s.p[i] = p ? (R)p[i] : R(0);
+    type_out[i] = type ? type[i] : (uint8_t)FS_TYPE_NORMAL;
+    hidx_out[i] = (uint32_t)i;
+}
+
+// field f of the sorted state, scattered to host order
+template <typename R>
+__global__ void k_unpack(int64_t n, int dim, int field, State<R> s, float* __restrict__ out, uint8_t* __restrict__ out_u8,
+                         uint32_t* __restrict__ out_u32) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t h = s.hidx[k];
+    auto st = [&](V3<R> v) {
+        out[(int64_t)h * dim] = (float)v.x;
+        out[(int64_t)h * dim + 1] = (float)v.y;
+        if (dim == 3) out[(int64_t)h * dim + 2] = (float)v.z;
+    };
+    switch (field) {
+        case 0: st(xyz<R>(s.pos[k])); break;
+        case 1: st(xyz<R>(s.vel[k])); break;
+        case 2: st(xyz<R>(s.acc[k])); break;
+        case 3: st(xyz<R>(s.ext[k])); break;
+        case 4: out[h] = (float)s.pos[k].w; break;
+        case 5: out[h] = (float)s.rho[k]; break;
+        case 6: out[h] = (float)s.p[k]; break;
+        case 7: out_u8[h] = s.type[k]; break;
+        case 8: out_u32[h] = h; break;
+        case 9: st(xyz<R>(s.vstar[k])); break;
+        case 10: st(xyz<R>(s.anp[k])); break;
+        case 11: out[h] = (float)s.vstar[k].w; break;
+        case 12: out[h] = (float)s.anp[k].w; break;
+    }
+}
+
+template <typename R> fs_status upload_impl(fs_ctx* c, const fs_particles* in) {
+    const int64_t n = in->n;
+    const int dim = c->dim;
+    const size_t vec = (size_t)n * dim * sizeof(float), sc = (size_t)n * sizeof(float);
+    FS_TRY(ensure_staging(c, 4 * vec + 3 * sc + (size_t)n + 64));
+    char* st = (char*)c->staging;
+    auto put = [&](const void* src, size_t bytes, size_t& off) -> const float* {
+        if (!src) return nullptr;
+        char* dst = st + off;
+        off += (bytes + 15) & ~size_t(15);
+        if (cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess) return nullptr;
+        return (const float*)dst;
+    };
+    size_t off = 0;
+    const float* d_pos = put(in->position, vec, off);
+    if (!d_pos) return fail(FS_ERR_INVALID, "position is required for upload");
+    const float* d_vel = put(in->velocity, vec, off);
+    const float* d_acc = put(in->acceleration, vec, off);
+    const float* d_ext = put(in->external, vec, off);
+    const float* d_mass = put(in->mass, sc, off);
+    const float* d_rho = put(in->density, sc, off);
+    const float* d_p = put(in->pressure, sc, off);
+    const uint8_t* d_type = (const uint8_t*)put(in->type, (size_t)n, off);
+    FS_CUDA(cudaGetLastError());
+    c->cur = 0;
+    State<R> s = state_of<R>(c);
+    k_pack<R><<<grid_for(n), kBlock, 0, c->stream>>>(n, dim, d_pos, d_vel, d_acc, d_ext, d_mass, d_rho, d_p, d_type,
+                                                     c->prm.rest_density, s, c->type[0], c->hidx[0]);
+    FS_CUDA(cudaGetLastError());
+    FS_CUDA(cudaStreamSynchronize(c->stream));
+    return FS_OK;
+}
+
+template <typename R> fs_status download_impl(fs_ctx* c, fs_particles* out) {
+    const int64_t n = c->n;
+    const int dim = c->dim;
+    const size_t vec = (size_t)n * dim * sizeof(float);
+    FS_TRY(ensure_staging(c, std::max<size_t>(vec, (size_t)n * 4) + 64));
+    State<R> s = state_of<R>(c);
+    struct F {
+        int field;
+        void* dst;
+        size_t bytes;
+    } fields[] = {
+        {0, out->position, vec}, {1, out->velocity, vec}, {2, out->acceleration, vec}, {3, out->external, vec},
+        {4, out->mass, (size_t)n * 4}, {5, out->density, (size_t)n * 4}, {6, out->pressure, (size_t)n * 4},
+        {7, out->type, (size_t)n}, {8, out->tag, (size_t)n * 4}, {9, out->predicted_velocity, vec},
+        {10, out->non_pressure_acceleration, vec}, {11, out->source_term, (size_t)n * 4},
+        {12, out->diagonal_element, (size_t)n * 4},
+    };
+    for (auto& f : fields) {
+        if (!f.dst) continue;
+        k_unpack<R><<<grid_for(n), kBlock, 0, c->stream>>>(n, dim, f.field, s, (float*)c->staging,
+                                                           (uint8_t*)c->staging, (uint32_t*)c->staging);
+        FS_CUDA(cudaGetLastError());
+        FS_CUDA(cudaMemcpyAsync(f.dst, c->staging, f.bytes, cudaMemcpyDeviceToHost, c->stream));
+    }
+    FS_CUDA(cudaStreamSynchronize(c->stream));
+    return FS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// neighborhood search
+// ---------------------------------------------------------------------------
+template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
+    const int64_t n = c->n;
+    cudaStream_t st = c->stream;
+    const bool single = c->reference_order;
+    State<R> s = state_of<R>(c);
+    // bbox of the structure's cells -> grid origin
+    FS_CUDA(cudaMemsetAsync(c->bbox, 0x7f, 3 * sizeof(int), st));
+    FS_CUDA(cudaMemsetAsync(c->bbox + 3, 0x80, 3 * sizeof(int), st));
+    const unsigned gb = std::min<unsigned>(grid_for(n, 256), 148u * 8u);
+    k_bbox<R><<<gb, 256, 0, st>>>(n, s.pos, s.type, c->include_inactive, c->search_radius, c->bbox, c->status);
+    k_origin<<<1, 32, 0, st>>>(c->bbox, c->origin, c->dims[0], c->dims[1], c->dims[2]);
+    // keys + sort
+    unsigned long long* k64 = single ? c->keys64[0] : nullptr;
+    k_keys<R><<<grid_for(n), kBlock, 0, st>>>(n, s.pos, s.type, s.hidx, c->include_inactive, single, c->search_radius,
+                                              c->origin, c->dims[0], c->dims[1], c->dims[2], c->keys[0], k64, c->perm[0]);
+    FS_CUDA(cudaGetLastError());
+    size_t temp = c->cub_temp_bytes;
+    if (single) {
+        FS_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_temp, temp, c->keys64[0], c->keys64[1], c->perm[0], c->perm[1],
+                                                (int)n, 0, 64, st));
+    } else {
+        FS_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_temp, temp, c->keys[0], c->keys[1], c->perm[0], c->perm[1],
+                                                (int)n, 0, 32, st));
+    }
+    // gather every persistent field into the other buffer
+    const int nx = c->cur ^ 1;
+    k_reorder<R><<<grid_for(n), kBlock, 0, st>>>(
+        n, c->perm[1], (const V4<R>*)c->pos[c->cur], (V4<R>*)c->pos[nx], (const V4<R>*)c->vel[c->cur],
+        (V4<R>*)c->vel[nx], (const V4<R>*)c->acc[c->cur], (V4<R>*)c->acc[nx], (const V4<R>*)c->ext[c->cur],
+        (V4<R>*)c->ext[nx], (const R*)c->rho[c->cur], (R*)c->rho[nx], (const R*)c->p[c->cur], (R*)c->p[nx],
+        c->type[c->cur], c->type[nx], c->hidx[c->cur], c->hidx[nx]);
+    FS_CUDA(cudaGetLastError());
+    c->cur = nx;
+    s = state_of<R>(c);
+    // cell ranges
+    FS_CUDA(cudaMemsetAsync(c->cell_range, 0, sizeof(uint2) * 3 * c->cell_capacity, st));
+    k_cell_ranges<<<grid_for(c->n_struct), kBlock, 0, st>>>(c->n_struct, single ? nullptr : c->keys[1],
+                                                            single ? c->keys64[1] : nullptr, c->dims[0], c->dims[1],
+                                                            c->cell_capacity, c->cell_range);
+    FS_CUDA(cudaGetLastError());
+    if (solver_lists) {
+        WalkParams w = walk_of(c, true);
+        const uint32_t owners = 1u << FS_TYPE_NORMAL;
+        k_build_lists<R><<<grid_for(c->n_owners), kBlock, 0, st>>>(c->n_owners, s.pos, s.type, c->cell_range, c->origin,
+                                                                    w, owners, true, c->nbr, c->nbr_stride,
+                                                                    c->nbr_capacity, c->nbr_count, c->status, c->scalars);
+        FS_CUDA(cudaGetLastError());
+        c->have_lists = true;
+    }
+    return FS_OK;
+}
+
+// layout bookkeeping after an upload: counts per type and owner range
+fs_status layout_from_types(fs_ctx* c, const uint8_t* type, int64_t n) {
+    int64_t nf = 0, nb = 0, ni = 0;
+    for (int64_t i = 0; i < n; i++) {
+        uint8_t t = type ? type[i] : (uint8_t)FS_TYPE_NORMAL;
+        if (t == FS_TYPE_NORMAL) nf++;
+        else if (t == FS_TYPE_BOUNDARY) nb++;
+        else if (t == FS_TYPE_INACTIVE) ni++;
+        else return fail(FS_ERR_INVALID, "particle type must be 0, 1 or 2");
+    }
+    c->n = n;
+    c->n_fluid = nf;
+    c->n_boundary = nb;
+    c->n_inactive = ni;
+    c->n_struct = c->include_inactive ? n : nf + nb;
+    c->n_owners = c->reference_order ? c->n_struct : nf;
+    return FS_OK;
+}
+
+fs_status read_scalars(fs_ctx* c) {
+    FS_CUDA(cudaMemcpyAsync(c->scalars_host, c->scalars, sizeof(StepScalars), cudaMemcpyDeviceToHost, c->stream));
+    FS_CUDA(cudaStreamSynchronize(c->stream));
+    return FS_OK;
+}
+
+fs_status read_status(fs_ctx* c, int* st) {
+    FS_CUDA(cudaMemcpyAsync(st, c->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    FS_CUDA(cudaStreamSynchronize(c->stream));
+    return FS_OK;
+}
+
+__global__ void k_step_begin(StepScalars* sc, float desired_dt) {
+    StepScalars z{};
+    z.desired_dt = desired_dt;
+    z.dt = desired_dt;
+    *sc = z;
+}
+
+// ---------------------------------------------------------------------------
+// solver steps
+// ---------------------------------------------------------------------------
+template <typename R, bool KAHAN> fs_status step_iisph3d(fs_ctx* c) {
+    cudaStream_t st = c->stream;
+    const int64_t n = c->n, no = c->n_owners;
+    const SolverConsts<R> k = consts_of<R>(c);
+    const Lists L = lists_of(c);
+    const bool split = c->reference_order;
+    const bool fp32 = c->precision == FS_PRECISION_FP32;
+    // density double buffer: the current density becomes rho_prev
+    std::swap(c->rho[c->cur], c->rho_prev);
+    State<R> s = state_of<R>(c);
+    cudaEventRecord(c->ev[1], st);
+    if (split) {
+        k_iisph3d_density<R, KAHAN><<<grid_for(n), kBlock, 0, st>>>(n, s, L, k, c->status);
+        k_iisph3d_l1<R, KAHAN, true><<<grid_for(n), kBlock, 0, st>>>(n, s, L, k, c->scalars, c->status);
+    } else {
+        k_iisph3d_l1<R, KAHAN, false><<<grid_for(n), kBlock, 0, st>>>(n, s, L, k, c->scalars, c->status);
+    }
+    FS_CUDA(cudaGetLastError());
+    cudaEventRecord(c->ev[2], st);
+    if (fp32) k_iisph3d_l2<R, KAHAN, true><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
+    else k_iisph3d_l2<R, KAHAN, false><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
+    FS_CUDA(cudaGetLastError());
+    cudaEventRecord(c->ev[3], st);
+    const int max_it = c->prm.max_iterations;
+    const bool fp64_test = !fp32;
+    for (int it = 0; it < max_it; it++) {
+        k_iisph3d_pressure_acc<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
+        k_iisph3d_pressure_update<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
+        k_iisph_check<<<1, 1, 0, st>>>(c->scalars, c->prm.min_iterations, max_it, c->prm.max_density_error, fp64_test,
+                                       false, c->status);
+        FS_CUDA(cudaGetLastError());
+        FS_TRY(read_scalars(c));
+        if (c->scalars_host->done) break;
+    }
+    cudaEventRecord(c->ev[4], st);
+    k_cfl<<<1, 1, 0, st>>>(c->scalars, c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
+                           c->status);
+    k_iisph3d_integrate<R><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
+    FS_CUDA(cudaGetLastError());
+    cudaEventRecord(c->ev[5], st);
+    return FS_OK;
+}
+
+template <typename R, bool KAHAN> fs_status step_sesph(fs_ctx* c) {
+    cudaStream_t st = c->stream;
+    const int64_t n = c->n, no = c->n_owners;
+    const SolverConsts<R> k = consts_of<R>(c);
+    const Lists L = lists_of(c);
+    State<R> s = state_of<R>(c);
+    cudaEventRecord(c->ev[1], st);
+    k_sesph_density<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->status);
+    cudaEventRecord(c->ev[2], st);
+    k_sesph_accel<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->status);
+    cudaEventRecord(c->ev[3], st);
+    if (c->dim == 3) {
+        k_sesph_maxima<R><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
+        k_sesph_maxima_final<<<1, 1, 0, st>>>(c->scalars);
+        k_cfl<<<1, 1, 0, st>>>(c->scalars, c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
+                               c->status);
+    }
+    cudaEventRecord(c->ev[4], st);
+    k_sesph_integrate<R><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
+    FS_CUDA(cudaGetLastError());
+    cudaEventRecord(c->ev[5], st);
+    return FS_OK;
+}
+
+template <typename R, bool KAHAN> fs_status step_iisph2d(fs_ctx* c) {
+    cudaStream_t st = c->stream;
+    const int64_t n = c->n, no = c->n_owners;
+    const SolverConsts<R> k = consts_of<R>(c);
+    const Lists L = lists_of(c);
+    const bool split = c->reference_order;
+    std::swap(c->rho[c->cur], c->rho_prev);
+    State<R> s = state_of<R>(c);
+    cudaEventRecord(c->ev[1], st);
+    if (split) {
+        k_iisph2d_density<R, KAHAN><<<grid_for(n), kBlock, 0, st>>>(n, s, L, k, c->status);
+        k_iisph2d_l1<R, KAHAN, true><<<grid_for(n), kBlock, 0, st>>>(n, s, L, k, c->scalars, c->status);
+    } else {
+        k_iisph2d_l1<R, KAHAN, false><<<grid_for(n), kBlock, 0, st>>>(n, s, L, k, c->scalars, c->status);
+    }
+    cudaEventRecord(c->ev[2], st);
+    k_iisph2d_l2<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
+    FS_CUDA(cudaGetLastError());
+    cudaEventRecord(c->ev[3], st);
+    const int max_it = c->prm.max_iterations;
+    const bool fp64_test = c->precision != FS_PRECISION_FP32;
+    for (int it = 0; it < max_it; it++) {
+        k_iisph2d_pressure_acc<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
+        k_iisph2d_pressure_update<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
+        k_iisph_check<<<1, 1, 0, st>>>(c->scalars, c->prm.min_iterations, max_it, c->prm.max_density_error, fp64_test,
+                                       true, c->status);
+        FS_CUDA(cudaGetLastError());
+        FS_TRY(read_scalars(c));
+        if (c->scalars_host->done) break;
+    }
+    cudaEventRecord(c->ev[4], st);
+    k_iisph2d_integrate<R><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
+    FS_CUDA(cudaGetLastError());
+    cudaEventRecord(c->ev[5], st);
+    return FS_OK;
+}
+
+template <typename R, bool KAHAN> fs_status step_dispatch(fs_ctx* c) {
+    switch (c->prm.solver) {
+        case FS_SOLVER_IISPH_3D: return step_iisph3d<R, KAHAN>(c);
+        case FS_SOLVER_SESPH_2D:
+        case FS_SOLVER_SESPH_3D: return step_sesph<R, KAHAN>(c);
+        case FS_SOLVER_IISPH_2D: return step_iisph2d<R, KAHAN>(c);
+        default: return fail(FS_ERR_INVALID, "context has no solver");
+    }
+}
+
+fs_status search_dispatch(fs_ctx* c, bool solver_lists) {
+    if (c->precision == FS_PRECISION_FP64) return search_impl<double>(c, solver_lists);
+    return search_impl<float>(c, solver_lists);
+}
+
+fs_status fill_stats(fs_ctx* c, fs_step_stats* stats, int st) {
+    const StepScalars& h = *c->scalars_host;
+    if (stats) {
+        stats->desired_dt = h.desired_dt;
+        stats->actual_dt = h.dt;
+        stats->iterations = h.iteration;
+        stats->avg_density_error = h.avg_err;
+        stats->avg_density_error_fp64 = h.avg_err64;
+        stats->max_density_error = h.max_err;
+        stats->max_velocity = std::sqrt(h.final_max_v2);
+        stats->max_acceleration = std::sqrt(h.final_max_a2);
+        stats->status = st;
+        stats->max_neighbors = h.max_neighbors;
+    }
+    return FS_OK;
+}
+
+// neighborhood search of a step (with solver lists). A list overflow stops
+// every later kernel (they check the status word); with an automatic
+// capacity the lists are grown and the search is repeated once.
+fs_status search_for_step(fs_ctx* c, float dt) {
+    for (int attempt = 0; attempt < 2; attempt++) {
+        k_step_begin<<<1, 1, 0, c->stream>>>(c->scalars, dt);
+        FS_CUDA(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
+        cudaEventRecord(c->ev[0], c->stream);
+        FS_TRY(search_dispatch(c, c->prm.solver != FS_SOLVER_NONE));
+        int st = 0;
+        FS_TRY(read_status(c, &st));
+        if (st == FS_ERR_CAPACITY && attempt == 0 && c->prm.neighbor_capacity == 0 &&
+            c->prm.solver != FS_SOLVER_NONE) {
+            FS_TRY(read_scalars(c));
+            int K = 32;
+            while (K < c->scalars_host->max_neighbors) K *= 2;
+            FS_TRY(ensure_lists(c, K));
+            continue;
+        }
+        if (st != FS_OK) return fail((fs_status)st, "neighbor list capacity exceeded");
+        c->searched_dt = dt;
+        return FS_OK;
+    }
+    return fail(FS_ERR_CAPACITY, "neighbor list capacity exceeded");
+}
+
+// solver phases of a step on the lists of the last search
+fs_status solve_after_search(fs_ctx* c, float dt, fs_step_stats* stats) {
+    if (!c->have_lists) return fail(FS_ERR_STATE, "execute the neighborhood search first");
+    k_step_begin<<<1, 1, 0, c->stream>>>(c->scalars, dt);
+    fs_status r;
+    if (c->precision == FS_PRECISION_FP64) r = step_dispatch<double, false>(c);
+    else if (c->precision == FS_PRECISION_FP32) r = step_dispatch<float, false>(c);
+    else r = step_dispatch<float, true>(c);
+    if (r != FS_OK) return r;
+    c->have_lists = false;  // positions moved: the lists belong to the old positions
+    FS_TRY(read_scalars(c));
+    int st = 0;
+    FS_TRY(read_status(c, &st));
+    for (int i = 0; i < 5; i++) cudaEventElapsedTime(&c->phase_ms[i], c->ev[i], c->ev[i + 1]);
+    fill_stats(c, stats, st);
+    if (st != FS_OK) return fail((fs_status)st, "device reported an error during the step");
+    return FS_OK;
+}
+
+fs_status one_step(fs_ctx* c, float desired_dt, fs_step_stats* stats) {
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    if (c->prm.solver == FS_SOLVER_NONE) return fail(FS_ERR_INVALID, "context has no solver");
+    const float dt = desired_dt > 0.0f ? desired_dt : c->prm.timestep;
+    FS_TRY(search_for_step(c, dt));
+    return solve_after_search(c, dt, stats);
+}
+
+}  // namespace
+
+// ===========================================================================
+// extern "C"
+// ===========================================================================
+extern "C" {
+
+int32_t fs_abi_version(void) { return FS_ABI_VERSION; }
+
+const char* fs_last_error(void) { return g_error.c_str(); }
+
+void fs_params_default(fs_params* p, int32_t dim, int32_t solver, int32_t search) {
+    std::memset(p, 0, sizeof(*p));
+    p->dim = dim;
+    p->solver = solver;
+    p->search = search;
+    p->precision = FS_PRECISION_FP32_KAHAN;
+    p->rest_density = 1000.0f;   // IFluidSolver.hpp:19-21
+    p->gravity = 9.81f;
+    p->particle_size = 0.1f;
+    p->stiffness = 100000.0f;    // SESPHSettings*.hpp
+    p->viscosity = 5.0f;
+    p->single_layer_boundary = 0;
+    p->single_layer_gamma_1 = 1.1f;
+    p->single_layer_gamma_2 = 1.1f;
+    p->max_density_error = 0.001f;  // IISPHSettings*.hpp
+    p->min_iterations = 2;
+    p->max_iterations = 100;
+    p->omega = 0.5f;
+    p->gamma = 0.7f;
+    p->timestep = 0.001f;        // ConstantTimestepGenerator.hpp:8-13
+    p->lambda_v = 0.4f;
+    p->lambda_a = 0.25f;
+    p->max_particles = 0;
+    p->neighbor_capacity = 0;
+    p->device = 0;
+}
+
+fs_status fs_create(const fs_params* p, fs_ctx** out) {
+    if (!out) return fail(FS_ERR_INVALID, "out is null");
+    *out = nullptr;
+    FS_TRY(check_params(p));
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FS_ERR_NO_DEVICE, "no CUDA device");
+    if (p->device < 0 || p->device >= ndev) return fail(FS_ERR_INVALID, "device ordinal out of range");
+    FS_CUDA(cudaSetDevice(p->device));
+    cudaDeviceProp prop;
+    FS_CUDA(cudaGetDeviceProperties(&prop, p->device));
+    if (prop.major < 10) return fail(FS_ERR_NO_DEVICE, "device is not sm_100 class");
+    fs_ctx* c = new (std::nothrow) fs_ctx();
+    if (!c) return fail(FS_ERR_INVALID, "out of host memory");
+    c->prm = *p;
+    c->device = p->device;
+    derive(c);
+    c->cap = p->max_particles;
+    auto bail = [&](fs_status s) {
+        free_all(c);
+        delete c;
+        return s;
+    };
+#define FS_ALLOC(ptr, count)                      \
+    do {                                          \
+        fs_status s_ = dalloc(&(ptr), (count));   \
+        if (s_ != FS_OK) return bail(s_);         \
+    } while (0)
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(FS_ERR_CUDA, "cudaStreamCreate failed"));
+    const size_t cap = (size_t)c->cap;
+    const size_t v4 = c->real_size * 4, r1 = c->real_size;
+    for (int b = 0; b < 2; b++) {
+        char** fields[] = {(char**)&c->pos[b], (char**)&c->vel[b], (char**)&c->acc[b], (char**)&c->ext[b]};
+        for (char** f : fields) FS_ALLOC(*f, cap * v4);
+        FS_ALLOC(*(char**)&c->rho[b], cap * r1);
+        FS_ALLOC(*(char**)&c->p[b], cap * r1);
+        FS_ALLOC(c->type[b], cap);
+        FS_ALLOC(c->hidx[b], cap);
+        FS_ALLOC(c->keys[b], cap);
+        FS_ALLOC(c->perm[b], cap);
+        if (c->reference_order) FS_ALLOC(c->keys64[b], cap);
+    }
+    FS_ALLOC(*(char**)&c->rho_prev, cap * r1);
+    FS_ALLOC(*(char**)&c->vstar, cap * v4);
+    FS_ALLOC(*(char**)&c->anp, cap * v4);
+    FS_ALLOC(*(char**)&c->err, cap * r1);
+    FS_ALLOC(c->bbox, 6);
+    FS_ALLOC(c->origin, 4);
+    FS_ALLOC(c->status, 1);
+    FS_ALLOC(c->scalars, 1);
+    FS_ALLOC(c->nbr_count, cap);
+    if (cudaMallocHost((void**)&c->scalars_host, sizeof(StepScalars)) != cudaSuccess)
+        return bail(fail(FS_ERR_CUDA, "cudaMallocHost failed"));
+    // CUB temp storage for the largest sort
+    size_t temp = 0;
+    if (c->reference_order)
+        cub::DeviceRadixSort::SortPairs(nullptr, temp, c->keys64[0], c->keys64[1], c->perm[0], c->perm[1], (int)cap, 0,
+                                        64, c->stream);
+    else
+        cub::DeviceRadixSort::SortPairs(nullptr, temp, c->keys[0], c->keys[1], c->perm[0], c->perm[1], (int)cap, 0, 32,
+                                        c->stream);
+    size_t scan_temp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_temp, (uint32_t*)nullptr, (int64_t*)nullptr, (int)cap + 1, c->stream);
+    c->cub_temp_bytes = std::max(temp, scan_temp);
+    FS_ALLOC(*(char**)&c->cub_temp, c->cub_temp_bytes);
+    int K = p->neighbor_capacity > 0 ? p->neighbor_capacity : (p->dim == 2 ? 32 : 64);
+    if (contract_capacity(p->search) > 0) K = std::min(K, contract_capacity(p->search) + 1);
+    {
+        fs_status s_ = ensure_lists(c, K);
+        if (s_ != FS_OK) return bail(s_);
+    }
+    for (auto& e : c->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) return bail(fail(FS_ERR_CUDA, "cudaEventCreate failed"));
+    if (cudaMemsetAsync(c->status, 0, sizeof(int), c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return bail(fail(FS_ERR_CUDA, "initialisation failed"));
+#undef FS_ALLOC
+    *out = c;
+    return FS_OK;
+}
+
+fs_status fs_destroy(fs_ctx* c) {
+    if (!c) return FS_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_all(c);
+    delete c;
+    return FS_OK;
+}
+
+fs_status fs_set_params(fs_ctx* c, const fs_params* p) {
+    if (!c) return fail(FS_ERR_INVALID, "ctx is null");
+    FS_TRY(check_params(p));
+    if (p->dim != c->prm.dim || p->solver != c->prm.solver || p->search != c->prm.search ||
+        p->precision != c->prm.precision || p->flags != c->prm.flags || p->max_particles != c->prm.max_particles)
+        return fail(FS_ERR_INVALID, "layout-defining parameters cannot change; create a new context");
+    c->prm = *p;
+    derive(c);
+    return FS_OK;
+}
+
+fs_status fs_upload(fs_ctx* c, const fs_particles* in) {
+    if (!c || !in) return fail(FS_ERR_INVALID, "null argument");
+    if (in->n < 0 || in->n > c->cap) return fail(FS_ERR_INVALID, "particle count exceeds the context capacity");
+    FS_CUDA(cudaSetDevice(c->device));
+    FS_TRY(layout_from_types(c, in->type, in->n));
+    choose_dims(c, in->position, in->type, in->n);
+    FS_TRY(ensure_cells(c));
+    fs_status r = c->precision == FS_PRECISION_FP64 ? upload_impl<double>(c, in) : upload_impl<float>(c, in);
+    if (r != FS_OK) return r;
+    c->have_state = true;
+    c->have_lists = false;
+    return FS_OK;
+}
+
+fs_status fs_download(fs_ctx* c, fs_particles* out) {
+    if (!c || !out) return fail(FS_ERR_INVALID, "null argument");
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    FS_CUDA(cudaSetDevice(c->device));
+    if (c->precision == FS_PRECISION_FP64) return download_impl<double>(c, out);
+    return download_impl<float>(c, out);
+}
+
+fs_status fs_find_neighbors(fs_ctx* c) {
+    if (!c) return fail(FS_ERR_INVALID, "ctx is null");
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    FS_CUDA(cudaSetDevice(c->device));
+    FS_TRY(search_for_step(c, c->prm.timestep));
+    cudaEventRecord(c->ev[1], c->stream);
+    FS_CUDA(cudaStreamSynchronize(c->stream));
+    cudaEventElapsedTime(&c->phase_ms[0], c->ev[0], c->ev[1]);
+    return FS_OK;
+}
+
+fs_status fs_solve_step(fs_ctx* c, float desired_dt, fs_step_stats* stats) {
+    if (!c) return fail(FS_ERR_INVALID, "ctx is null");
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    if (c->prm.solver == FS_SOLVER_NONE) return fail(FS_ERR_INVALID, "context has no solver");
+    FS_CUDA(cudaSetDevice(c->device));
+    const float dt = desired_dt > 0.0f ? desired_dt : c->prm.timestep;
+    return solve_after_search(c, dt, stats);
+}
+
+fs_status fs_get_neighbors_csr(fs_ctx* c, int64_t* offsets, int64_t* indices, int64_t* total) {
+    if (!c || !offsets) return fail(FS_ERR_INVALID, "null argument");
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    FS_CUDA(cudaSetDevice(c->device));
+    const int64_t n = c->n;
+    const int64_t ns = c->n_struct;
+    cudaStream_t st = c->stream;
+    if (c->csr_capacity < n + 1) {
+        if (c->csr_offsets) cudaFree(c->csr_offsets);
+        if (c->csr_counts) cudaFree(c->csr_counts);
+        c->csr_offsets = nullptr;
+        c->csr_counts = nullptr;
+        FS_TRY(dalloc(&c->csr_offsets, (size_t)n + 1));
+        FS_TRY(dalloc(&c->csr_counts, (size_t)n + 1));
+        c->csr_capacity = n + 1;
+    }
+    WalkParams w = walk_of(c, false);
+    const uint32_t mask = contract_owner_mask(c->prm.search);
+    FS_CUDA(cudaMemsetAsync(c->csr_counts, 0, sizeof(uint32_t) * (n + 1), st));
+    if (c->precision == FS_PRECISION_FP64) {
+        State<double> s = state_of<double>(c);
+        k_csr_count<double><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_range, c->origin, w, mask,
+                                                             c->csr_counts);
+    } else {
+        State<float> s = state_of<float>(c);
+        k_csr_count<float><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_range, c->origin, w, mask,
+                                                            c->csr_counts);
+    }
+    FS_CUDA(cudaGetLastError());
+    size_t temp = c->cub_temp_bytes;
+    FS_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_temp, temp, c->csr_counts, c->csr_offsets, (int)(n + 1), st));
+    int64_t tot = 0;
+    FS_CUDA(cudaMemcpyAsync(&tot, c->csr_offsets + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    FS_CUDA(cudaStreamSynchronize(st));
+    if (total) *total = tot;
+    // per-list capacity of the contract (the reference throws beyond it)
+    const int cap = contract_capacity(c->prm.search);
+    std::vector<uint32_t> counts((size_t)n);
+    FS_CUDA(cudaMemcpy(counts.data(), c->csr_counts, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> hidx((size_t)n);
+    FS_CUDA(cudaMemcpy(hidx.data(), c->hidx[c->cur], sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+    bool over = false;
+    std::vector<int64_t> cnt_host((size_t)n, 0);
+    for (int64_t k = 0; k < n; k++) {
+        cnt_host[hidx[k]] = counts[k];
+        if (cap > 0 && (int64_t)counts[k] > cap) over = true;
+    }
+    offsets[0] = 0;
+    for (int64_t h = 0; h < n; h++) offsets[h + 1] = offsets[h] + cnt_host[h];
+    if (over) {
+        g_error = "a neighbor list exceeds the contract's capacity";
+        if (!indices) return FS_ERR_CAPACITY;
+    }
+    if (!indices) return over ? FS_ERR_CAPACITY : FS_OK;
+    uint32_t* d_idx = nullptr;
+    FS_TRY(dalloc(&d_idx, (size_t)std::max<int64_t>(tot, 1)));
+    if (c->precision == FS_PRECISION_FP64) {
+        State<double> s = state_of<double>(c);
+        k_csr_fill<double><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_range, c->origin, w, mask,
+                                                            c->csr_offsets, d_idx);
+    } else {
+        State<float> s = state_of<float>(c);
+        k_csr_fill<float><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_range, c->origin, w, mask,
+                                                           c->csr_offsets, d_idx);
+    }
+    std::vector<uint32_t> idx((size_t)tot);
+    std::vector<int64_t> off_sorted((size_t)n + 1);
+    cudaError_t e1 = cudaGetLastError();
+    cudaError_t e2 = cudaMemcpyAsync(idx.data(), d_idx, sizeof(uint32_t) * tot, cudaMemcpyDeviceToHost, st);
+    cudaError_t e3 = cudaMemcpyAsync(off_sorted.data(), c->csr_offsets, sizeof(int64_t) * (n + 1),
+                                     cudaMemcpyDeviceToHost, st);
+    cudaError_t e4 = cudaStreamSynchronize(st);
+    cudaFree(d_idx);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess)
+        return fail(FS_ERR_CUDA, "CSR export failed");
+    for (int64_t k = 0; k < n; k++) {
+        const int64_t h = hidx[k];
+        int64_t o = offsets[h];
+        for (int64_t q = off_sorted[k]; q < off_sorted[k + 1]; q++) indices[o++] = hidx[idx[q]];
+        std::sort(indices + offsets[h], indices + offsets[h + 1]);
+    }
+    return over ? FS_ERR_CAPACITY : FS_OK;
+}
+
+fs_status fs_query_position(fs_ctx* c, const float* position, int64_t* out, int64_t cap, int64_t* count) {
+    if (!c || !position) return fail(FS_ERR_INVALID, "null argument");
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    FS_CUDA(cudaSetDevice(c->device));
+    WalkParams w = walk_of(c, false);
+    uint32_t* d_out = nullptr;
+    unsigned long long* d_cnt = nullptr;
+    const int64_t room = std::max<int64_t>(cap, 0);
+    FS_TRY(dalloc(&d_out, (size_t)std::max<int64_t>(room, 1)));
+    if (dalloc(&d_cnt, 1) != FS_OK) {
+        cudaFree(d_out);
+        return FS_ERR_CUDA;
+    }
+    const float z = c->dim == 3 ? position[2] : 0.0f;
+    if (c->precision == FS_PRECISION_FP64) {
+        State<double> s = state_of<double>(c);
+        k_query_position<double><<<1, 32, 0, c->stream>>>(v3<double>(position[0], position[1], z), s.pos, s.type,
+                                                          c->cell_range, c->origin, w, d_out, room, d_cnt);
+    } else {
+        State<float> s = state_of<float>(c);
+        k_query_position<float><<<1, 32, 0, c->stream>>>(v3<float>(position[0], position[1], z), s.pos, s.type,
+                                                         c->cell_range, c->origin, w, d_out, room, d_cnt);
+    }
+    unsigned long long cnt = 0;
+    std::vector<uint32_t> tmp((size_t)room);
+    cudaMemcpyAsync(&cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream);
+    if (room) cudaMemcpyAsync(tmp.data(), d_out, sizeof(uint32_t) * room, cudaMemcpyDeviceToHost, c->stream);
+    std::vector<uint32_t> hidx((size_t)c->n);
+    cudaMemcpyAsync(hidx.data(), c->hidx[c->cur], sizeof(uint32_t) * c->n, cudaMemcpyDeviceToHost, c->stream);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_out);
+    cudaFree(d_cnt);
+    if (e != cudaSuccess) return fail(FS_ERR_CUDA, cudaGetErrorString(e));
+    const int64_t m = std::min<int64_t>((int64_t)cnt, room);
+    for (int64_t q = 0; q < m; q++) out[q] = hidx[tmp[q]];
+    std::sort(out, out + m);
+    if (count) *count = (int64_t)cnt;
+    return FS_OK;
+}
+
+fs_status fs_step(fs_ctx* c, float desired_dt, fs_step_stats* stats) {
+    if (!c) return fail(FS_ERR_INVALID, "ctx is null");
+    FS_CUDA(cudaSetDevice(c->device));
+    return one_step(c, desired_dt, stats);
+}
+
+fs_status fs_run(fs_ctx* c, int32_t steps, float desired_dt, fs_step_stats* stats) {
+    if (!c) return fail(FS_ERR_INVALID, "ctx is null");
+    FS_CUDA(cudaSetDevice(c->device));
+    for (int32_t i = 0; i < steps; i++) FS_TRY(one_step(c, desired_dt, stats));
+    return FS_OK;
+}
+
+fs_status fs_last_phase_times(fs_ctx* c, float* ms5) {
+    if (!c || !ms5) return fail(FS_ERR_INVALID, "null argument");
+    for (int i = 0; i < 5; i++) ms5[i] = c->phase_ms[i];
+    return FS_OK;
+}
+
+fs_status fs_batch_create(const fs_params*, int32_t, const int64_t*, fs_ctx** out) {
+    if (out) *out = nullptr;
+    return fail(FS_ERR_INVALID, "batched scenes are not available in this build");
+}
+
+fs_status fs_batch_run(fs_ctx*, int32_t, float, fs_step_stats*) {
+    return fail(FS_ERR_INVALID, "batched scenes are not available in this build");
+}
+
+}  // extern "C"

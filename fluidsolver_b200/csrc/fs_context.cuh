@@ -1,0 +1,114 @@
+// Host-side context of one simulation (or one batch of scenes) on one GPU:
+// device buffers, the stream, and the layout bookkeeping shared by the search
+// and the solver phases.
+//
+// HBM layout (structure of arrays, all in the device's sorted order):
+//   pos   V4: x, y, z, mass          vel  V4: x, y, z, -
+//   acc   V4: MovementData acceleration (IISPH: pressure acceleration)
+//   ext   V4: ExternalForces accumulator
+//   rho, rho_prev, p   scalars (rho_prev: the density read by the viscosity term)
+//   vstar V4: predicted velocity, w = source term
+//   anp   V4: original non-pressure acceleration, w = diagonal element
+//   err   scalar: predicted density error
+//   type  uint8, hidx uint32 (host index of the particle at this position)
+// Sorted order puts fluid particles first, then boundary particles, then the
+// inactive particles a contract still lists, then excluded inactive ones,
+// each block in Z-order of its cells (a single Z-ordered block in the
+// reference-order mode). Fluid-only phases run over [0, n_fluid).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "fs_common.cuh"
+
+struct fs_ctx {
+    fs_params prm{};
+    int dim = 3;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int64_t cap = 0;          // particle capacity
+    int64_t n = 0;            // particles uploaded
+    int64_t n_fluid = 0, n_boundary = 0, n_inactive = 0;
+    int64_t n_struct = 0;     // particles that take part in the cell structure
+    bool have_state = false;
+    bool have_lists = false;
+    float searched_dt = 0.f;
+    bool reference_order = false;
+    bool include_inactive = false;  // contract lists inactive particles (2D quadratic / hashed)
+    int ns_owner_mode = 0;          // 0 all in structure, 1 fluid only, 2 active only
+    int precision = FS_PRECISION_FP32_KAHAN;
+    size_t real_size = 4;
+
+    // derived constants (float, computed exactly as the reference does)
+    float search_radius = 0.f;   // particle_size * 2
+    float radius2 = 0.f;         // search_radius * search_radius
+    float kernel_h = 0.f;        // kernel_support / 2
+    float kernel_alpha = 0.f;
+
+    // state, double-buffered for the reorder gather
+    void* pos[2] = {};
+    void* vel[2] = {};
+    void* acc[2] = {};
+    void* ext[2] = {};
+    void* rho[2] = {};
+    void* p[2] = {};
+    uint8_t* type[2] = {};
+    uint32_t* hidx[2] = {};
+    int cur = 0;
+    void* rho_prev = nullptr;
+    void* vstar = nullptr;
+    void* anp = nullptr;
+    void* err = nullptr;
+
+    // search
+    uint32_t* keys[2] = {};
+    unsigned long long* keys64[2] = {};
+    uint32_t* perm[2] = {};
+    void* cub_temp = nullptr;
+    size_t cub_temp_bytes = 0;
+    uint2* cell_range = nullptr;   // [3][cell_capacity] (start, end) per region
+    int64_t cell_capacity = 0;
+    int dims[3] = {1, 1, 1};
+    int* bbox = nullptr;           // device: min xyz, max xyz (cell coordinates)
+    int* origin = nullptr;         // device: cell-grid origin used this step
+    uint32_t* nbr = nullptr;       // solver lists, slot-major: nbr[s * nbr_stride + k]
+    uint32_t* nbr_count = nullptr;
+    int nbr_capacity = 0;          // K
+    int64_t nbr_stride = 0;
+    int64_t n_owners = 0;          // owners of the solver lists: [0, n_owners)
+
+    // CSR export of the last search (sorted space)
+    int64_t* csr_offsets = nullptr;
+    uint32_t* csr_indices = nullptr;
+    int64_t csr_capacity = 0;
+    uint32_t* csr_counts = nullptr;
+
+    // staging for host transfers
+    void* staging = nullptr;
+    size_t staging_bytes = 0;
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+
+    int* status = nullptr;                  // device status word
+    fsb::StepScalars* scalars = nullptr;    // device
+    fsb::StepScalars* scalars_host = nullptr;  // pinned mirror
+
+    // CUDA graph of the IISPH pressure loop (conditional while node)
+    cudaGraphExec_t loop_exec = nullptr;
+    cudaGraph_t loop_graph = nullptr;
+    cudaGraphConditionalHandle loop_handle = 0;
+    bool loop_graph_ready = false;
+    cudaGraphExec_t step_exec = nullptr;
+    cudaGraph_t step_graph = nullptr;
+    float step_graph_dt = -1.f;
+
+    cudaEvent_t ev[6] = {};
+    float phase_ms[5] = {};
+
+    // batched scenes
+    int32_t scenes = 0;
+    std::vector<int64_t> scene_offsets;
+};

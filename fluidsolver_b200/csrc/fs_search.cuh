@@ -1,0 +1,304 @@
+// Neighborhood search: cell keys -> radix sort -> Z-order reordering of the
+// particle SoA -> per-region cell ranges -> neighbor lists.
+//
+// One device search serves every reference contract. What the contract fixes
+// (and the reference line it follows):
+//   predicate   2D: sqrt(dot(d,d)) <= r   (HashedNeighborhoodSearch.cpp:56,
+//                    QuadraticNeighborhoodSearchDynamicAllocated.cpp:32,
+//                    CompactHashingNeighborhoodSearch.cpp:235)
+//               3D: dot(d,d) <= r*r       (HashedNeighborhoodSearch3D.cpp:334,
+//                    QuadraticNeighborhoodSearch3D.cpp:60, CompressedNeighbors.cpp:576)
+//   owners / candidates: see fs_search_kind in the public header.
+// The cell grid (cell edge = search radius, cell = floor(x / r) as in
+// HashedNeighborhoodSearch3D.cpp:224-228) is ours; because every candidate is
+// tested with the contract's exact float predicate, the neighbor SETS do not
+// depend on it.
+//
+// Cells are indexed relative to the particles' bounding box; a grid that
+// would exceed the allocated table is clamped, and candidates found through a
+// clamped cell are accepted only if their own cell is the visited one.
+#pragma once
+
+#include "fs_common.cuh"
+
+namespace fsb {
+
+constexpr uint32_t kInactiveKey = 0xffffffffu;
+constexpr int kMaxDimCells = 1024;  // 10 Morton bits per axis
+
+__device__ __forceinline__ uint32_t morton_spread10(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+__device__ __forceinline__ uint32_t morton_compact10(uint32_t v) {
+    v &= 0x09249249u;
+    v = (v | (v >> 2)) & 0x030c30c3u;
+    v = (v | (v >> 4)) & 0x0300f00fu;
+    v = (v | (v >> 8)) & 0x030000ffu;
+    v = (v | (v >> 16)) & 0x000003ffu;
+    return v;
+}
+
+struct GridInfo {
+    int dims[3];
+    float inv_unused;
+    float radius;  // cell edge
+};
+
+// cell coordinate of a position: (int)floor(x / r)
+template <typename R> __device__ __forceinline__ int cell_coord(R x, float r) {
+    return (int)floor((float)x / r);
+}
+
+// ---------------------------------------------------------------------------
+// bounding box of the cells of all particles in the structure
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void k_bbox(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type, bool include_inactive,
+                       float r, int* __restrict__ bbox, const int* __restrict__ status) {
+    int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        if (!include_inactive && type[k] == FS_TYPE_INACTIVE) continue;
+        V4<R> p = pos[k];
+        int c0 = cell_coord<R>(p.x, r), c1 = cell_coord<R>(p.y, r), c2 = cell_coord<R>(p.z, r);
+        mn[0] = min(mn[0], c0); mn[1] = min(mn[1], c1); mn[2] = min(mn[2], c2);
+        mx[0] = max(mx[0], c0); mx[1] = max(mx[1], c1); mx[2] = max(mx[2], c2);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[a] = min(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+            mx[a] = max(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            if (mn[a] != INT_MAX) atomicMin(&bbox[a], mn[a]);
+            if (mx[a] != INT_MIN) atomicMax(&bbox[3 + a], mx[a]);
+        }
+    }
+}
+
+// Grid origin for this step: the bbox minimum, shifted so that the box is
+// centred in the allocated dims when it is smaller.
+__global__ void k_origin(const int* __restrict__ bbox, int* __restrict__ origin, int d0, int d1, int d2) {
+    if (threadIdx.x != 0) return;
+    int d[3] = {d0, d1, d2};
+    for (int a = 0; a < 3; a++) {
+        int lo = bbox[a], hi = bbox[3 + a];
+        if (lo > hi) { lo = 0; hi = 0; }
+        long long ext = (long long)hi - lo + 1;
+        long long slack = (long long)d[a] - ext;
+        origin[a] = (int)(slack > 0 ? (long long)lo - slack / 2 : (long long)lo);
+    }
+}
+
+// clamped local cell of a cell coordinate; *clamped set when outside the grid
+__device__ __forceinline__ int local_cell(int c, int origin, int dim, bool& clamped) {
+    long long l = (long long)c - origin;
+    if (l < 0) { clamped = true; return 0; }
+    if (l >= dim) { clamped = true; return dim - 1; }
+    return (int)l;
+}
+
+// region of a particle in the sorted layout (0 fluid, 1 boundary, 2 listed inactive)
+__device__ __forceinline__ uint32_t region_of(uint8_t t, bool single_region) {
+    if (single_region) return 0;
+    return t == FS_TYPE_NORMAL ? 0u : (t == FS_TYPE_BOUNDARY ? 1u : 2u);
+}
+
+template <typename R>
+__global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
+                       const uint32_t* __restrict__ hidx, bool include_inactive, bool single_region, float r,
+                       const int* __restrict__ origin, int d0, int d1, int d2, uint32_t* __restrict__ keys,
+                       unsigned long long* __restrict__ keys64, uint32_t* __restrict__ perm) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    uint8_t t = type[k];
+    uint32_t key;
+    if (!include_inactive && t == FS_TYPE_INACTIVE) {
+        key = kInactiveKey;
+    } else {
+        V4<R> p = pos[k];
+        bool cl = false;
+        int lx = local_cell(cell_coord<R>(p.x, r), origin[0], d0, cl);
+        int ly = local_cell(cell_coord<R>(p.y, r), origin[1], d1, cl);
+        int lz = local_cell(cell_coord<R>(p.z, r), origin[2], d2, cl);
+        uint32_t m = morton_spread10(lx) | (morton_spread10(ly) << 1) | (morton_spread10(lz) << 2);
+        key = (region_of(t, single_region) << 30) | m;
+    }
+    if (keys64) keys64[k] = ((unsigned long long)key << 32) | hidx[k];
+    else keys[k] = key;
+    perm[k] = (uint32_t)k;
+}
+
+// new[k] = old[perm[k]] for every persistent field
+template <typename R>
+__global__ void k_reorder(int64_t n, const uint32_t* __restrict__ perm, const V4<R>* __restrict__ pos0, V4<R>* __restrict__ pos1,
+                          const V4<R>* __restrict__ vel0, V4<R>* __restrict__ vel1, const V4<R>* __restrict__ acc0,
+                          V4<R>* __restrict__ acc1, const V4<R>* __restrict__ ext0, V4<R>* __restrict__ ext1,
+                          const R* __restrict__ rho0, R* __restrict__ rho1, const R* __restrict__ p0, R* __restrict__ p1,
+                          const uint8_t* __restrict__ t0, uint8_t* __restrict__ t1, const uint32_t* __restrict__ h0,
+                          uint32_t* __restrict__ h1) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    uint32_t s = perm[k];
+    pos1[k] = pos0[s];
+    vel1[k] = vel0[s];
+    acc1[k] = acc0[s];
+    ext1[k] = ext0[s];
+    rho1[k] = rho0[s];
+    p1[k] = p0[s];
+    t1[k] = t0[s];
+    h1[k] = h0[s];
+}
+
+__device__ __forceinline__ int64_t lin_cell(uint32_t m, int d0, int d1) {
+    uint32_t lx = morton_compact10(m), ly = morton_compact10(m >> 1), lz = morton_compact10(m >> 2);
+    return ((int64_t)lz * d1 + ly) * d0 + lx;
+}
+
+// cell ranges: for region g and linear cell c, cell_range[g * cap + c] = [start, end)
+__global__ void k_cell_ranges(int64_t n_struct, const uint32_t* __restrict__ keys, const unsigned long long* __restrict__ keys64,
+                              int d0, int d1, int64_t cell_cap, uint2* __restrict__ cell_range) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n_struct) return;
+    uint32_t key = keys64 ? (uint32_t)(keys64[k] >> 32) : keys[k];
+    uint32_t prev = k > 0 ? (keys64 ? (uint32_t)(keys64[k - 1] >> 32) : keys[k - 1]) : 0xffffffffu;
+    uint32_t next = k + 1 < n_struct ? (keys64 ? (uint32_t)(keys64[k + 1] >> 32) : keys[k + 1]) : 0xffffffffu;
+    int64_t c = (int64_t)(key >> 30) * cell_cap + lin_cell(key & 0x3fffffffu, d0, d1);
+    if (k == 0 || prev != key) cell_range[c].x = (uint32_t)k;
+    if (k + 1 == n_struct || next != key) cell_range[c].y = (uint32_t)(k + 1);
+}
+
+// ---------------------------------------------------------------------------
+// the per-particle candidate walk shared by list building and position queries
+// ---------------------------------------------------------------------------
+struct WalkParams {
+    float r;        // search radius
+    float r2;       // r * r
+    int dim;        // 2 or 3
+    int regions;    // number of regions to visit (1 in single-region mode)
+    bool candidates_inactive;  // contract lists inactive neighbors
+    int d0, d1, d2;
+    int64_t cell_cap;
+};
+
+// predicate of the contract; d = x_i - x_j
+template <typename R> __device__ __forceinline__ bool within(V3<R> d, const WalkParams& w) {
+    if (w.dim == 2) {
+        float q = (float)d.x * (float)d.x + (float)d.y * (float)d.y;
+        return __fsqrt_rn(q) <= w.r;
+    }
+    float q = ((float)d.x * (float)d.x + (float)d.y * (float)d.y) + (float)d.z * (float)d.z;
+    return q <= w.r2;
+}
+
+// Visits the neighbors of position xi in HashedNeighborhoodSearch3D's order
+// (cells dx, dy, dz ascending with dx outermost; within a cell, sorted order).
+// f(j, entry) is called for every neighbor j; entry carries the boundary bit.
+template <typename R, typename F>
+__device__ __forceinline__ void walk_neighbors(V3<R> xi, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
+                                               const uint2* __restrict__ cell_range, const int* __restrict__ origin,
+                                               const WalkParams& w, F&& f) {
+    const int ci[3] = {cell_coord<R>(xi.x, w.r), cell_coord<R>(xi.y, w.r), cell_coord<R>(xi.z, w.r)};
+    const int zr = w.dim == 2 ? 0 : 1;
+    const int o0 = origin[0], o1 = origin[1], o2 = origin[2];
+    for (int dx = -1; dx <= 1; dx++) {
+        for (int dy = -1; dy <= 1; dy++) {
+            for (int dz = -zr; dz <= zr; dz++) {
+                const int c0 = ci[0] + dx, c1 = ci[1] + dy, c2 = ci[2] + dz;
+                bool cl = false;
+                const int l0 = local_cell(c0, o0, w.d0, cl);
+                const int l1 = local_cell(c1, o1, w.d1, cl);
+                const int l2 = local_cell(c2, o2, w.d2, cl);
+                const int64_t lc = ((int64_t)l2 * w.d1 + l1) * w.d0 + l0;
+                for (int g = 0; g < w.regions; g++) {
+                    const uint2 rg = cell_range[g * w.cell_cap + lc];
+                    for (uint32_t j = rg.x; j < rg.y; j++) {
+                        const V4<R> pj = pos[j];
+                        if (cl) {
+                            if (cell_coord<R>(pj.x, w.r) != c0 || cell_coord<R>(pj.y, w.r) != c1 ||
+                                cell_coord<R>(pj.z, w.r) != c2)
+                                continue;
+                        }
+                        const uint8_t tj = type[j];
+                        if (!w.candidates_inactive && tj == FS_TYPE_INACTIVE) continue;
+                        const V3<R> d = xi - xyz<R>(pj);
+                        if (within<R>(d, w)) f(j, tj);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Solver lists: for owner k in [0, n_owners) with an owner type accepted by
+// owner_mask (bit per particle type), write up to K entries slot-major.
+template <typename R>
+__global__ void k_build_lists(int64_t n_owners, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
+                              const uint2* __restrict__ cell_range, const int* __restrict__ origin, WalkParams w,
+                              uint32_t owner_mask, bool solver_lists, uint32_t* __restrict__ nbr, int64_t stride, int K,
+                              uint32_t* __restrict__ count, int* __restrict__ status, StepScalars* __restrict__ sc) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n_owners) return;
+    const uint8_t tk = type[k];
+    uint32_t c = 0;
+    if ((owner_mask >> tk) & 1u) {
+        const V3<R> xi = xyz<R>(pos[k]);
+        walk_neighbors<R>(xi, pos, type, cell_range, origin, w, [&](uint32_t j, uint8_t tj) {
+            // solver lists never carry inactive particles (the solvers skip them)
+            if (solver_lists && tj == FS_TYPE_INACTIVE) return;
+            if ((int)c < K) nbr[(int64_t)c * stride + k] = j | (tj == FS_TYPE_BOUNDARY ? kBoundaryBit : 0u);
+            c++;
+        });
+    }
+    count[k] = c;
+    if ((int)c > K) raise_status(status, FS_ERR_CAPACITY);
+    atomicMax(&sc->max_neighbors, (int)c);
+}
+
+// CSR export: counts (pass 1) and fill (pass 2) in sorted index space
+template <typename R>
+__global__ void k_csr_count(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
+                            const uint2* __restrict__ cell_range, const int* __restrict__ origin, WalkParams w,
+                            uint32_t owner_mask, uint32_t* __restrict__ count) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    uint32_t c = 0;
+    if ((owner_mask >> type[k]) & 1u)
+        walk_neighbors<R>(xyz<R>(pos[k]), pos, type, cell_range, origin, w, [&](uint32_t, uint8_t) { c++; });
+    count[k] = c;
+}
+
+template <typename R>
+__global__ void k_csr_fill(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
+                           const uint2* __restrict__ cell_range, const int* __restrict__ origin, WalkParams w,
+                           uint32_t owner_mask, const int64_t* __restrict__ offsets, uint32_t* __restrict__ out) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (!((owner_mask >> type[k]) & 1u)) return;
+    int64_t o = offsets[k];
+    walk_neighbors<R>(xyz<R>(pos[k]), pos, type, cell_range, origin, w, [&](uint32_t j, uint8_t) { out[o++] = j; });
+}
+
+// neighbors of one arbitrary position (get_neighbors(vec)), sorted space
+template <typename R>
+__global__ void k_query_position(V3<R> x, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
+                                 const uint2* __restrict__ cell_range, const int* __restrict__ origin, WalkParams w,
+                                 uint32_t* __restrict__ out, int64_t cap, unsigned long long* __restrict__ count) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long c = 0;
+    walk_neighbors<R>(x, pos, type, cell_range, origin, w, [&](uint32_t j, uint8_t) {
+        if ((int64_t)c < cap) out[c] = j;
+        c++;
+    });
+    *count = c;
+}
+
+}  // namespace fsb

@@ -1,0 +1,764 @@
+// SESPH and IISPH timestep phases as gather kernels over the neighbor lists.
+//
+// Each kernel restates one parallel loop of the reference solver; the
+// comments give the loop and the float expression order it follows.
+// Neighbor sums are accumulated with Acc<R, KAHAN>: plain sums in the
+// reference's operation order (FP32 / FP64 modes), or Kahan-compensated sums.
+#pragma once
+
+#include "fs_common.cuh"
+
+namespace fsb {
+
+template <typename R> struct SolverConsts {
+    SplineKernel<R> kern;
+    R rest_density;
+    R rho0_sq;        // Math::pow2(rest_density)
+    R gravity;
+    R visc_eps;       // (0.01f * particle_size) * particle_size
+    R two_nu;         // 2.0f * viscosity
+    R omega, gamma;
+    R two_gamma;      // 2.0f * gamma
+    R gamma1, gamma2;
+    R stiffness;
+    bool single_layer;
+    int dim;
+    R max_density_error;
+    int min_iterations, max_iterations;
+};
+
+struct Lists {
+    const uint32_t* __restrict__ nbr;
+    const uint32_t* __restrict__ count;
+    int64_t stride;
+    int K;
+    __device__ __forceinline__ uint32_t size(int64_t k) const { return min(count[k], (uint32_t)K); }
+    __device__ __forceinline__ uint32_t at(int64_t k, uint32_t s) const { return nbr[(int64_t)s * stride + k]; }
+};
+
+template <typename R> struct State {
+    V4<R>* __restrict__ pos;
+    V4<R>* __restrict__ vel;
+    V4<R>* __restrict__ acc;
+    V4<R>* __restrict__ ext;
+    R* __restrict__ rho;       // density of this step (written by the density phase)
+    R* __restrict__ rho_prev;  // density read by the viscosity term
+    R* __restrict__ p;
+    V4<R>* __restrict__ vstar; // w: source term
+    V4<R>* __restrict__ anp;   // w: diagonal element
+    R* __restrict__ err;
+    const uint8_t* __restrict__ type;
+    const uint32_t* __restrict__ hidx;
+};
+
+__device__ __forceinline__ float fmax_(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double fmax_(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float fmin_(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double fmin_(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float abs_(float a) { return fabsf(a); }
+__device__ __forceinline__ double abs_(double a) { return fabs(a); }
+
+// float maxima of non-negative values, kept as ordered bit patterns; NaN is
+// ignored like std::fmax ignores it
+__device__ __forceinline__ void atomic_max_nonneg(unsigned int* a, float v) {
+    if (v >= 0.0f) atomicMax(a, __float_as_uint(v));
+}
+
+template <typename T> __device__ __forceinline__ T warp_sum(T v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// ===========================================================================
+// viscosity term (IISPHFluidSolver3D.hpp:43-76, SESPHFluidSolver3D.hpp:293-324,
+// IISPHFluidSolver.hpp:240-277, SESPHFluidSolver.hpp:254-285):
+//   tmp += (m_j / rho_j) * (dot(v_ij, x_ij) / (dot(x_ij, x_ij) + eps)) * gradW
+//   return (2 nu) * tmp
+// rho_of(j, entry) supplies the neighbor density the reference reads.
+// ===========================================================================
+template <typename R, bool KAHAN, typename RhoOf>
+__device__ __forceinline__ V3<R> viscosity(int64_t k, const State<R>& s, const Lists& L, const SolverConsts<R>& c,
+                                           V3<R> xi, V3<R> vi, RhoOf&& rho_of) {
+    Acc3<R, KAHAN> tmp;
+    const uint32_t n = L.size(k);
+    for (uint32_t q = 0; q < n; q++) {
+        const uint32_t e = L.at(k, q);
+        const uint32_t j = e & kIndexMask;
+        const R rj = rho_of(j, e);
+        if (rj == R(0)) continue;
+        const V4<R> pj = s.pos[j];
+        const V4<R> vj = s.vel[j];
+        const V3<R> vij = vi - xyz<R>(vj);
+        const V3<R> xij = xi - xyz<R>(pj);
+        const R f = (pj.w / rj) * (dot(vij, xij) / (dot(xij, xij) + c.visc_eps));
+        tmp.add(f * c.kern.gradW(xij));
+    }
+    return c.two_nu * tmp.get();
+}
+
+// ===========================================================================
+// IISPH 3D, first loop (IISPHFluidSolver3D.hpp:141-212): p = 0; non-pressure
+// acceleration (gravity + viscosity) for non-boundary particles; v*; store
+// a_np; reset ExternalForces; density for fluid particles.
+// SPLIT = false: one pass, viscosity reads the previous density for every j.
+// SPLIT = true : density in k_iisph3d_density first, then this kernel reads the
+//                new density of fluid neighbors with a smaller host index and
+//                the previous one otherwise -- the order the reference's serial
+//                loop produces (it overwrites densities while reading them).
+// ===========================================================================
+template <typename R, bool KAHAN, bool SPLIT>
+__global__ void k_iisph3d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* __restrict__ sc,
+                             const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    const uint8_t t = s.type[k];
+    if (t == FS_TYPE_INACTIVE) {
+        if (!SPLIT) s.rho[k] = s.rho_prev[k];  // carry the density through the double buffer
+        return;
+    }
+    const R dt = (R)sc->dt;
+    const V4<R> pk = s.pos[k];
+    const V4<R> vk = s.vel[k];
+    s.p[k] = R(0);
+    V3<R> npa = xyz<R>(s.ext[k]);
+    if (t != FS_TYPE_BOUNDARY) {
+        npa = npa + v3<R>(R(0), -c.gravity, R(0));
+        V3<R> visc;
+        if (SPLIT) {
+            const uint32_t hk = s.hidx[k];
+            visc = viscosity<R, KAHAN>(k, s, L, c, xyz<R>(pk), xyz<R>(vk), [&](uint32_t j, uint32_t e) -> R {
+                if (!(e & kBoundaryBit) && s.hidx[j] < hk) return s.rho[j];
+                return s.rho_prev[j];
+            });
+        } else {
+            visc = viscosity<R, KAHAN>(k, s, L, c, xyz<R>(pk), xyz<R>(vk),
+                                       [&](uint32_t j, uint32_t) -> R { return s.rho_prev[j]; });
+        }
+        npa = npa + visc;
+    }
+    const V3<R> vstar = xyz<R>(vk) + dt * npa;
+    s.vstar[k] = v4<R>(vstar, R(0));
+    s.anp[k] = v4<R>(npa, R(0));
+    s.ext[k] = v4<R>(v3<R>(R(0), R(0), R(0)), R(0));
+    if (t == FS_TYPE_BOUNDARY) {
+        if (!SPLIT) s.rho[k] = s.rho_prev[k];
+        return;
+    }
+    if (!SPLIT) {
+        Acc<R, KAHAN> rho;
+        const uint32_t nn = L.size(k);
+        for (uint32_t q = 0; q < nn; q++) {
+            const uint32_t e = L.at(k, q);
+            const V4<R> pj = s.pos[e & kIndexMask];
+            R m = pj.w;
+            if (c.single_layer && (e & kBoundaryBit)) m = m * c.gamma1;
+            rho.add(m * c.kern.W(xyz<R>(pk) - xyz<R>(pj)));
+        }
+        s.rho[k] = rho.get();
+    }
+}
+
+// density only (IISPHFluidSolver3D.hpp:184-210), for the split first loop
+template <typename R, bool KAHAN>
+__global__ void k_iisph3d_density(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    const uint8_t t = s.type[k];
+    if (t != FS_TYPE_NORMAL) {
+        s.rho[k] = s.rho_prev[k];
+        return;
+    }
+    const V3<R> xk = xyz<R>(s.pos[k]);
+    Acc<R, KAHAN> rho;
+    const uint32_t nn = L.size(k);
+    for (uint32_t q = 0; q < nn; q++) {
+        const uint32_t e = L.at(k, q);
+        const V4<R> pj = s.pos[e & kIndexMask];
+        R m = pj.w;
+        if (c.single_layer && (e & kBoundaryBit)) m = m * c.gamma1;
+        rho.add(m * c.kern.W(xk - xyz<R>(pj)));
+    }
+    s.rho[k] = rho.get();
+}
+
+// ===========================================================================
+// IISPH 3D, second loop (IISPHFluidSolver3D.hpp:216-339): source term and
+// diagonal element for fluid particles.
+//   s_i   = (rho0 - rho_i) - dt * sum_j m_j dot(v*_i - v*_j, gradW)   (boundary: v*_j dropped)
+//   d_i   = - sum_j w_j m_j / rho0^2 gradW          (w_j = 2 gamma / 2 for boundary)
+//   a_ii  = dt^2 [ sum_j m_j dot(d_i, gradW) + sum_fluid m_j dot(-(m_i/rho0^2) gradW, gradW) ]
+// TWO_PASS = true walks the list a second time for a_ii exactly as the
+// reference does; otherwise a_ii is assembled from the same single pass as
+// dot(d_i, sum_j m_j gradW) - (m_i/rho0^2) sum_fluid m_j |gradW|^2 (the same sum
+// regrouped, used with the compensated sums).
+// ===========================================================================
+template <typename R, bool KAHAN, bool TWO_PASS>
+__global__ void k_iisph3d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* __restrict__ sc,
+                             const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    if (s.type[k] != FS_TYPE_NORMAL) return;
+    const R dt = (R)sc->dt;
+    const V4<R> pk = s.pos[k];
+    const V3<R> xk = xyz<R>(pk);
+    const V4<R> vsk4 = s.vstar[k];
+    const V3<R> vsk = xyz<R>(vsk4);
+    const uint32_t nn = L.size(k);
+    Acc<R, KAHAN> contrib;
+    Acc3<R, KAHAN> inner;
+    Acc3<R, KAHAN> mg;    // sum_j m_j gradW      (single-pass a_ii)
+    Acc<R, KAHAN> mg2;    // sum_fluid m_j |gradW|^2
+    for (uint32_t q = 0; q < nn; q++) {
+        const uint32_t e = L.at(k, q);
+        const uint32_t j = e & kIndexMask;
+        const V4<R> pj = s.pos[j];
+        const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+        if (!(e & kBoundaryBit)) {
+            const V3<R> vsj = xyz<R>(s.vstar[j]);
+            contrib.add(pj.w * dot(vsk - vsj, g));
+            inner.sub((pj.w / c.rho0_sq) * g);
+            if (!TWO_PASS) mg2.add(pj.w * dot(g, g));
+        } else {
+            contrib.add(pj.w * dot(vsk, g));
+            if (c.single_layer) inner.sub(((c.two_gamma * pj.w) / c.rho0_sq) * g);
+            else inner.sub(((R(2) * pj.w) / c.rho0_sq) * g);
+        }
+        if (!TWO_PASS) mg.add(pj.w * g);
+    }
+    const R source = (c.rest_density - s.rho[k]) - dt * contrib.get();
+    const V3<R> in = inner.get();
+    R diag;
+    if (TWO_PASS) {
+        Acc<R, KAHAN> d;
+        const R mi = pk.w / c.rho0_sq;
+        for (uint32_t q = 0; q < nn; q++) {
+            const uint32_t e = L.at(k, q);
+            const uint32_t j = e & kIndexMask;
+            const V4<R> pj = s.pos[j];
+            const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+            d.add(pj.w * dot(in, g));
+            // gradW(x_j - x_i) == -gradW(x_i - x_j) bit for bit
+            if (!(e & kBoundaryBit)) d.add(pj.w * dot(mi * (-g), g));
+        }
+        diag = d.get() * (dt * dt);
+    } else {
+        diag = (dot(in, mg.get()) - (pk.w / c.rho0_sq) * mg2.get()) * (dt * dt);
+    }
+    s.vstar[k] = v4<R>(vsk, source);
+    s.anp[k].w = diag;
+}
+
+// ===========================================================================
+// IISPH 3D iteration (a): pressure acceleration (IISPHFluidSolver3D.hpp:348-397)
+//   a_i = - sum_fluid m_j (p_i/rho0^2 + p_j/rho0^2) gradW
+//         - sum_bdy (gamma m_j 2 p_i / rho0^2) gradW       (single layer; no gamma otherwise)
+// ===========================================================================
+template <typename R, bool KAHAN>
+__global__ void k_iisph3d_pressure_acc(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
+                                       const StepScalars* __restrict__ sc, const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status || sc->done) return;
+    if (s.type[k] != FS_TYPE_NORMAL) return;
+    const V3<R> xk = xyz<R>(s.pos[k]);
+    const R pk = s.p[k];
+    const uint32_t nn = L.size(k);
+    Acc3<R, KAHAN> pa;
+    for (uint32_t q = 0; q < nn; q++) {
+        const uint32_t e = L.at(k, q);
+        const uint32_t j = e & kIndexMask;
+        const V4<R> pj = s.pos[j];
+        const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+        if (!(e & kBoundaryBit)) {
+            pa.sub((pj.w * (pk / c.rho0_sq + s.p[j] / c.rho0_sq)) * g);
+        } else if (c.single_layer) {
+            pa.sub(((((c.gamma * pj.w) * R(2)) * pk) / c.rho0_sq) * g);
+        } else {
+            pa.sub((((pj.w * R(2)) * pk) / c.rho0_sq) * g);
+        }
+    }
+    s.acc[k] = v4<R>(pa.get(), R(0));
+}
+
+// ===========================================================================
+// IISPH 3D iteration (b): A p, relaxed Jacobi update and the per-particle
+// density error (IISPHFluidSolver3D.hpp:402-461), fused with the convergence
+// scan of :467-512 (block partial sums into StepScalars, FP64 residual).
+// ===========================================================================
+template <typename R, bool KAHAN>
+__global__ void k_iisph3d_pressure_update(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
+                                          StepScalars* __restrict__ sc, const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (*status || sc->done) return;
+    double e_sum = 0.0;
+    unsigned int e_cnt = 0;
+    float e_max = 0.f, a2 = 0.f, v2 = 0.f;
+    if (k < n && s.type[k] == FS_TYPE_NORMAL) {
+        const R dt = (R)sc->dt;
+        const V3<R> xk = xyz<R>(s.pos[k]);
+        const V3<R> ak = xyz<R>(s.acc[k]);
+        const uint32_t nn = L.size(k);
+        Acc<R, KAHAN> ap;
+        for (uint32_t q = 0; q < nn; q++) {
+            const uint32_t e = L.at(k, q);
+            const uint32_t j = e & kIndexMask;
+            const V4<R> pj = s.pos[j];
+            const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+            if (!(e & kBoundaryBit)) ap.add(pj.w * dot(ak - xyz<R>(s.acc[j]), g));
+            else ap.add(pj.w * dot(ak, g));
+        }
+        const R Ap = ap.get() * (dt * dt);
+        const V4<R> vs = s.vstar[k];   // w: source term
+        const R aii = s.anp[k].w;
+        R p = s.p[k];
+        const bool has_diag = abs_(aii) > R(kFltEps);
+        if (has_diag) p = fmax_(R(0), p + c.omega * ((vs.w - Ap) / aii));
+        else p = R(0);
+        s.p[k] = p;
+        R perr = abs_(vs.w - Ap);
+        if (has_diag) {
+            if (abs_(p) <= R(kFltEps)) perr = R(0);
+            s.err[k] = perr;
+            e_sum = (double)perr;
+            e_cnt = 1;
+            e_max = (float)perr;
+        }
+        // max |a|^2 and |v* + dt a|^2 of the fluid particles (CFL input)
+        a2 = (float)dot(ak, ak);
+        const V3<R> vf = xyz<R>(vs) + dt * ak;
+        v2 = (float)dot(vf, vf);
+        if (!(a2 >= 0.f)) a2 = 0.f;
+        if (!(v2 >= 0.f)) v2 = 0.f;
+        if (!(e_max >= 0.f)) e_max = 0.f;
+    }
+    e_sum = warp_sum(e_sum);
+    e_cnt = warp_sum(e_cnt);
+    e_max = warp_max(e_max);
+    a2 = warp_max(a2);
+    v2 = warp_max(v2);
+    __shared__ double s_sum[32];
+    __shared__ unsigned int s_cnt[32];
+    __shared__ float s_max[3][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_sum[wid] = e_sum; s_cnt[wid] = e_cnt;
+        s_max[0][wid] = e_max; s_max[1][wid] = a2; s_max[2][wid] = v2;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+        e_sum = lane < nw ? s_sum[lane] : 0.0;
+        e_cnt = lane < nw ? s_cnt[lane] : 0u;
+        e_max = lane < nw ? s_max[0][lane] : 0.f;
+        a2 = lane < nw ? s_max[1][lane] : 0.f;
+        v2 = lane < nw ? s_max[2][lane] : 0.f;
+        e_sum = warp_sum(e_sum);
+        e_cnt = warp_sum(e_cnt);
+        e_max = warp_max(e_max);
+        a2 = warp_max(a2);
+        v2 = warp_max(v2);
+        if (lane == 0) {
+            if (e_cnt) {
+                atomicAdd(&sc->err_sum, e_sum);
+                atomicAdd(&sc->err_count, (unsigned long long)e_cnt);
+            }
+            atomic_max_nonneg(&sc->max_err_bits, e_max);
+            atomic_max_nonneg(&sc->max_a2_bits, a2);
+            atomic_max_nonneg(&sc->max_v2_bits, v2);
+        }
+    }
+}
+
+// Convergence test after each iteration (IISPHFluidSolver3D.hpp:463-522) and
+// the 2D variant (IISPHFluidSolver.hpp:400-402, 513-523). One thread.
+//   FP32 mode : avg = (float)sum / (float)count, compared in float
+//   otherwise : avg compared in FP64
+__global__ void k_iisph_check(StepScalars* __restrict__ sc, int min_it, int max_it, float max_err, bool fp64_test,
+                              bool two_d, const int* __restrict__ status) {
+    if (*status || sc->done) return;
+    const int it = sc->iteration;  // iterations completed before this one
+    const unsigned long long cnt = sc->err_count;
+    const double sum = sc->err_sum;
+    float avg = 0.f;
+    double avg64 = 0.0;
+    if (cnt > 0) {
+        avg64 = sum / (double)cnt;
+        avg = fp64_test ? (float)avg64 : (float)sum / (float)cnt;
+    }
+    sc->avg_err = avg;
+    sc->avg_err64 = avg64;
+    sc->max_err = __uint_as_float(sc->max_err_bits);
+    sc->final_max_a2 = __uint_as_float(sc->max_a2_bits);
+    sc->final_max_v2 = __uint_as_float(sc->max_v2_bits);
+    const int done_it = it + 1;
+    sc->iteration = done_it;
+    bool done = false;
+    const bool below = fp64_test ? (avg64 <= (double)max_err) : (avg <= max_err);
+    if (two_d) {
+        // while ((it < min || err > max) && it < max): stop when it >= min and err <= max
+        done = (done_it >= min_it && below) || done_it >= max_it;
+    } else {
+        // if (iteration >= min - 1 && avg <= max) break;  (size_t: min == 0 never breaks early)
+        done = (min_it >= 1 && it >= min_it - 1 && below) || done_it >= max_it;
+    }
+    sc->done = done ? 1 : 0;
+    sc->err_sum = 0.0;
+    sc->err_count = 0ull;
+    sc->max_err_bits = 0u;
+    sc->max_a2_bits = 0u;
+    sc->max_v2_bits = 0u;
+}
+
+// CFL clamp (IISPHFluidSolver3D.hpp:525-535, SESPHFluidSolver3D.hpp:109-116) with
+// ConstantTimestepGenerator::get_non_cfl_validating_timestep
+// (ConstantTimestepGenerator.cpp:17-41). The reference evaluates
+// sqrt(size / a) * lambda_a in double (its unqualified sqrt is the C double
+// function) and rounds the product to float; the rest is float.
+__global__ void k_cfl(StepScalars* __restrict__ sc, float particle_size, float timestep, float lambda_v, float lambda_a,
+                      const int* __restrict__ status) {
+    if (*status) return;
+    const float max_v = sqrtf(sc->final_max_v2);
+    const float max_a = sqrtf(sc->final_max_a2);
+    float dta = timestep, dtv = timestep;
+    if (max_a > 0.0f) dta = (float)(sqrt((double)(particle_size / max_a)) * (double)lambda_a);
+    if (max_v > 0.0f) dtv = particle_size / max_v * lambda_v;
+    float nt = fmaxf(fminf(dta, dtv), 0.000001f);
+    nt = fminf(nt, sc->desired_dt);
+    sc->dt = nt;
+}
+
+// ===========================================================================
+// IISPH 3D integration (IISPHFluidSolver3D.hpp:539-561), all active particles:
+//   if dt changed: v* = (v* - old_dt a_np) + dt a_np
+//   v = v* + dt a ;  x = x + dt v
+// ===========================================================================
+template <typename R>
+__global__ void k_iisph3d_integrate(int64_t n, State<R> s, const StepScalars* __restrict__ sc,
+                                    const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    if (s.type[k] == FS_TYPE_INACTIVE) return;
+    const R dt = (R)sc->dt, old = (R)sc->desired_dt;
+    V3<R> vs = xyz<R>(s.vstar[k]);
+    if (sc->dt != sc->desired_dt) {
+        const V3<R> a = xyz<R>(s.anp[k]);
+        vs = (vs - old * a) + dt * a;
+    }
+    const V3<R> v = vs + dt * xyz<R>(s.acc[k]);
+    const V4<R> p = s.pos[k];
+    const V3<R> x = xyz<R>(p) + dt * v;
+    s.vel[k] = v4<R>(v, s.vel[k].w);
+    s.pos[k] = v4<R>(x, p.w);
+}
+
+// ===========================================================================
+// SESPH (SESPHFluidSolver3D.hpp:49-130, SESPHFluidSolver.hpp:49-111)
+// ===========================================================================
+// density and pressure of fluid particles
+//   3D: boundary j contributes (gamma_1 m_j) W if single layer (:216-225)
+//   p = max(k (rho / rho0 - 1), 0)  (std::max: NaN propagates)
+template <typename R, bool KAHAN>
+__global__ void k_sesph_density(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    if (s.type[k] != FS_TYPE_NORMAL) return;
+    const V3<R> xk = xyz<R>(s.pos[k]);
+    Acc<R, KAHAN> rho;
+    const uint32_t nn = L.size(k);
+    for (uint32_t q = 0; q < nn; q++) {
+        const uint32_t e = L.at(k, q);
+        const V4<R> pj = s.pos[e & kIndexMask];
+        const R w = c.kern.W(xk - xyz<R>(pj));
+        if ((e & kBoundaryBit) && c.single_layer) rho.add((c.gamma1 * pj.w) * w);
+        else rho.add(pj.w * w);
+    }
+    const R r = rho.get();
+    s.rho[k] = r;
+    const R pr = c.stiffness * (r / c.rest_density - R(1));
+    s.p[k] = (pr < R(0)) ? R(0) : pr;
+}
+
+// accelerations of fluid particles: a = pressure acc + (gravity + viscosity)
+//   pressure acc (:245-290): pdd = (rho == 0) ? 0 : p / rho^2
+//     fluid j   : += (-m_j (pdd_i + pdd_j)) gradW
+//     boundary j: += (-m_i (pdd_i + pdd_i)) gradW [* gamma_2 if single layer, 3D]
+template <typename R, bool KAHAN>
+__global__ void k_sesph_accel(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    if (s.type[k] != FS_TYPE_NORMAL) return;
+    const V4<R> pk = s.pos[k];
+    const V3<R> xk = xyz<R>(pk);
+    const R rk = s.rho[k];
+    const R pdd = rk == R(0) ? R(0) : s.p[k] / (rk * rk);
+    V3<R> npa = v3<R>(R(0), R(0), R(0)) + v3<R>(R(0), -c.gravity, R(0));
+    npa = npa + viscosity<R, KAHAN>(k, s, L, c, xk, xyz<R>(s.vel[k]),
+                                    [&](uint32_t j, uint32_t) -> R { return s.rho[j]; });
+    Acc3<R, KAHAN> pa;
+    const uint32_t nn = L.size(k);
+    for (uint32_t q = 0; q < nn; q++) {
+        const uint32_t e = L.at(k, q);
+        const uint32_t j = e & kIndexMask;
+        const V4<R> pj = s.pos[j];
+        const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+        if (e & kBoundaryBit) {
+            const R f = -pk.w * (pdd + pdd);
+            if (c.single_layer) pa.add((f * g) * c.gamma2);
+            else pa.add(f * g);
+        } else {
+            const R rj = s.rho[j];
+            const R pddj = rj == R(0) ? R(0) : s.p[j] / (rj * rj);
+            pa.add((-pj.w * (pdd + pddj)) * g);
+        }
+    }
+    s.acc[k] = v4<R>(pa.get() + npa, R(0));
+}
+
+// max |a|^2, |v + dt a|^2 over ALL particles (SESPHFluidSolver3D.hpp:93-107)
+template <typename R>
+__global__ void k_sesph_maxima(int64_t n, State<R> s, StepScalars* __restrict__ sc, const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (*status) return;
+    float a2 = 0.f, v2 = 0.f;
+    if (k < n) {
+        const R dt = (R)sc->desired_dt;
+        const V3<R> a = xyz<R>(s.acc[k]);
+        a2 = (float)dot(a, a);
+        const V3<R> v = xyz<R>(s.vel[k]) + dt * a;
+        v2 = (float)dot(v, v);
+        if (!(a2 >= 0.f)) a2 = 0.f;
+        if (!(v2 >= 0.f)) v2 = 0.f;
+    }
+    a2 = warp_max(a2);
+    v2 = warp_max(v2);
+    if ((threadIdx.x & 31) == 0) {
+        atomic_max_nonneg(&sc->max_a2_bits, a2);
+        atomic_max_nonneg(&sc->max_v2_bits, v2);
+    }
+}
+
+__global__ void k_sesph_maxima_final(StepScalars* __restrict__ sc) {
+    sc->final_max_a2 = __uint_as_float(sc->max_a2_bits);
+    sc->final_max_v2 = __uint_as_float(sc->max_v2_bits);
+    sc->max_a2_bits = 0u;
+    sc->max_v2_bits = 0u;
+}
+
+// Euler-Cromer for every active particle: v += dt a; x += dt v
+template <typename R>
+__global__ void k_sesph_integrate(int64_t n, State<R> s, const StepScalars* __restrict__ sc,
+                                  const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    if (s.type[k] == FS_TYPE_INACTIVE) return;
+    const R dt = (R)sc->dt;
+    const V4<R> vv = s.vel[k];
+    const V3<R> v = xyz<R>(vv) + dt * xyz<R>(s.acc[k]);
+    const V4<R> p = s.pos[k];
+    s.vel[k] = v4<R>(v, vv.w);
+    s.pos[k] = v4<R>(xyz<R>(p) + dt * v, p.w);
+}
+
+// ===========================================================================
+// IISPH 2D (IISPHFluidSolver.hpp:139-525)
+// ===========================================================================
+// first loop (:160-167, 196-237): density (fluid), then non-pressure
+// acceleration + v* (all active); viscosity reads neighbor densities as in the
+// 3D first loop (SPLIT selects the serial-order emulation).
+template <typename R, bool KAHAN, bool SPLIT>
+__global__ void k_iisph2d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* __restrict__ sc,
+                             const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    const uint8_t t = s.type[k];
+    if (t == FS_TYPE_INACTIVE) {
+        if (!SPLIT) s.rho[k] = s.rho_prev[k];  // carry the density through the double buffer
+        return;
+    }
+    const R dt = (R)sc->dt;
+    const V4<R> pk = s.pos[k];
+    const V4<R> vk = s.vel[k];
+    R rho_k = s.rho_prev[k];
+    if (t == FS_TYPE_NORMAL && !SPLIT) {
+        Acc<R, KAHAN> rho;
+        const uint32_t nn = L.size(k);
+        for (uint32_t q = 0; q < nn; q++) {
+            const V4<R> pj = s.pos[L.at(k, q) & kIndexMask];
+            rho.add(pj.w * c.kern.W(xyz<R>(pk) - xyz<R>(pj)));
+        }
+        rho_k = rho.get();
+    }
+    if (SPLIT) rho_k = s.rho[k];
+    V3<R> npa = xyz<R>(s.ext[k]);
+    if (t != FS_TYPE_BOUNDARY) {
+        npa = npa + v3<R>(R(0), -c.gravity, R(0));
+        V3<R> visc;
+        if (SPLIT) {
+            const uint32_t hk = s.hidx[k];
+            visc = viscosity<R, KAHAN>(k, s, L, c, xyz<R>(pk), xyz<R>(vk), [&](uint32_t j, uint32_t e) -> R {
+                if (j == (uint32_t)k) return rho_k;
+                if (!(e & kBoundaryBit) && s.hidx[j] < hk) return s.rho[j];
+                return s.rho_prev[j];
+            });
+        } else {
+            visc = viscosity<R, KAHAN>(k, s, L, c, xyz<R>(pk), xyz<R>(vk), [&](uint32_t j, uint32_t) -> R {
+                return j == (uint32_t)k ? rho_k : s.rho_prev[j];
+            });
+        }
+        npa = npa + visc;
+    }
+    s.vstar[k] = v4<R>(xyz<R>(vk) + dt * npa, R(0));
+    s.ext[k] = v4<R>(v3<R>(R(0), R(0), R(0)), R(0));
+    if (!SPLIT) s.rho[k] = rho_k;
+}
+
+// density for the split 2D first loop
+template <typename R, bool KAHAN>
+__global__ void k_iisph2d_density(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    if (s.type[k] != FS_TYPE_NORMAL) {
+        s.rho[k] = s.rho_prev[k];
+        return;
+    }
+    const V3<R> xk = xyz<R>(s.pos[k]);
+    Acc<R, KAHAN> rho;
+    const uint32_t nn = L.size(k);
+    for (uint32_t q = 0; q < nn; q++) {
+        const V4<R> pj = s.pos[L.at(k, q) & kIndexMask];
+        rho.add(pj.w * c.kern.W(xk - xyz<R>(pj)));
+    }
+    s.rho[k] = rho.get();
+}
+
+// second loop (:170-180, 280-376): source term, diagonal element, p = 0.
+// The reference's O(n^2) diagonal recomputes the same inner sum for every
+// outer neighbor; it is computed once here (the value is identical).
+template <typename R, bool KAHAN>
+__global__ void k_iisph2d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* __restrict__ sc,
+                             const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    if (s.type[k] != FS_TYPE_NORMAL) return;
+    const R dt = (R)sc->dt;
+    const V4<R> pk = s.pos[k];
+    const V3<R> xk = xyz<R>(pk);
+    const V3<R> vsk = xyz<R>(s.vstar[k]);
+    const uint32_t nn = L.size(k);
+    Acc<R, KAHAN> sum;
+    Acc3<R, KAHAN> internal;
+    for (uint32_t q = 0; q < nn; q++) {
+        const uint32_t e = L.at(k, q);
+        const uint32_t j = e & kIndexMask;
+        const V4<R> pj = s.pos[j];
+        const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+        sum.add(pj.w * dot(vsk - xyz<R>(s.vstar[j]), g));
+        if (!(e & kBoundaryBit)) internal.add(((pj.w / c.rest_density) / c.rest_density) * g);
+        else internal.add((((c.two_gamma * pj.w) / c.rest_density) / c.rest_density) * g);
+    }
+    const R source = (c.rest_density - s.rho[k]) - dt * sum.get();
+    const V3<R> neg_in = -internal.get();
+    const R mi = (pk.w / c.rest_density) / c.rest_density;
+    Acc<R, KAHAN> d;
+    for (uint32_t q = 0; q < nn; q++) {
+        const V4<R> pj = s.pos[L.at(k, q) & kIndexMask];
+        d.add(pj.w * dot(neg_in, c.kern.gradW(xk - xyz<R>(pj))));
+    }
+    for (uint32_t q = 0; q < nn; q++) {
+        const uint32_t e = L.at(k, q);
+        if (e & kBoundaryBit) continue;
+        const V4<R> pj = s.pos[e & kIndexMask];
+        const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+        d.add(pj.w * dot(mi * (-g), g));
+    }
+    s.vstar[k] = v4<R>(vsk, source);
+    s.anp[k] = v4<R>(v3<R>(R(0), R(0), R(0)), (dt * dt) * d.get());
+    s.p[k] = R(0);
+}
+
+// 2D iteration (a) (:408-444): a_i = -sum
+template <typename R, bool KAHAN>
+__global__ void k_iisph2d_pressure_acc(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
+                                       const StepScalars* __restrict__ sc, const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status || sc->done) return;
+    if (s.type[k] != FS_TYPE_NORMAL) return;
+    const V3<R> xk = xyz<R>(s.pos[k]);
+    const R pk = s.p[k];
+    const R pr = (pk / c.rest_density) / c.rest_density;
+    const uint32_t nn = L.size(k);
+    Acc3<R, KAHAN> sum;
+    for (uint32_t q = 0; q < nn; q++) {
+        const uint32_t e = L.at(k, q);
+        const uint32_t j = e & kIndexMask;
+        const V4<R> pj = s.pos[j];
+        const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+        if (!(e & kBoundaryBit)) sum.add((pj.w * (pr + (s.p[j] / c.rest_density) / c.rest_density)) * g);
+        else sum.add((((c.gamma * pj.w) * R(2)) * pr) * g);
+    }
+    s.acc[k] = v4<R>(-sum.get(), R(0));
+}
+
+// 2D iteration (b) (:447-511): Ap = dt^2 sum, update, density error
+template <typename R, bool KAHAN>
+__global__ void k_iisph2d_pressure_update(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
+                                          StepScalars* __restrict__ sc, const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (*status || sc->done) return;
+    double e_sum = 0.0;
+    unsigned int e_cnt = 0;
+    if (k < n && s.type[k] == FS_TYPE_NORMAL) {
+        const R dt = (R)sc->dt;
+        const V3<R> xk = xyz<R>(s.pos[k]);
+        const V3<R> ak = xyz<R>(s.acc[k]);
+        const uint32_t nn = L.size(k);
+        Acc<R, KAHAN> sum;
+        for (uint32_t q = 0; q < nn; q++) {
+            const uint32_t e = L.at(k, q);
+            const uint32_t j = e & kIndexMask;
+            const V4<R> pj = s.pos[j];
+            const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+            if (!(e & kBoundaryBit)) sum.add(pj.w * dot(ak - xyz<R>(s.acc[j]), g));
+            else sum.add(pj.w * dot(ak, g));
+        }
+        const R Ap = (dt * dt) * sum.get();
+        const R aii = s.anp[k].w;
+        const R src = s.vstar[k].w;
+        R p = s.p[k];
+        const bool has_diag = abs_(aii) > R(kFltEps);
+        if (has_diag) p = fmax_(R(0), p + c.omega * ((src - Ap) / aii));
+        else p = R(0);
+        s.p[k] = p;
+        R perr = abs_(src - Ap);
+        if (has_diag) {
+            if (abs_(p) <= R(kFltEps)) perr = R(0);
+            e_sum = (double)perr;
+            e_cnt = 1;
+        }
+    }
+    e_sum = warp_sum(e_sum);
+    e_cnt = warp_sum(e_cnt);
+    if ((threadIdx.x & 31) == 0 && e_cnt) {
+        atomicAdd(&sc->err_sum, e_sum);
+        atomicAdd(&sc->err_count, (unsigned long long)e_cnt);
+    }
+}
+
+// 2D integration (:379-392): v = v* + dt a; x += dt v (no CFL clamp)
+template <typename R>
+__global__ void k_iisph2d_integrate(int64_t n, State<R> s, const StepScalars* __restrict__ sc,
+                                    const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    if (s.type[k] == FS_TYPE_INACTIVE) return;
+    const R dt = (R)sc->dt;
+    const V3<R> v = xyz<R>(s.vstar[k]) + dt * xyz<R>(s.acc[k]);
+    const V4<R> p = s.pos[k];
+    s.vel[k] = v4<R>(v, s.vel[k].w);
+    s.pos[k] = v4<R>(xyz<R>(p) + dt * v, p.w);
+}
+
+}  // namespace fsb

@@ -1,0 +1,438 @@
+"""Host-side mirror of libFluid's solver and neighborhood-search interfaces
+over the C-ABI, so that parity tests and benchmarks drive the device path the
+way libFluid's own code drives its solvers:
+
+    solver = IISPHFluidSolver3D(search="hashed-3d")
+    solver.parameters.particle_size = 0.01 ...        (IFluidSolver.hpp:18-23)
+    solver.settings.omega = 0.5 ...                   (IISPHSettings3D.hpp:6-20)
+    solver.timestep_generator.settings.timestep = ... (ConstantTimestepGenerator.hpp:8-13)
+    solver.data.collection = ParticleCollection(...)
+    solver.execute_neighborhood_search()              (IFluidSolver.hpp:31)
+    solver.execute_simulation_step(timepoint)         (IFluidSolver.hpp:30)
+
+The collection is device resident between calls; `solver.collection()` copies
+it back (the reference's host ParticleCollection is authoritative only when an
+entity or sensor reads it).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as F
+
+SEARCH_KINDS = {
+    "quadratic-2d": F.FS_SEARCH_QUADRATIC_2D,
+    "hashed-2d": F.FS_SEARCH_HASHED_2D,
+    "compact-hashing-2d": F.FS_SEARCH_COMPACT_2D,
+    "quadratic-3d": F.FS_SEARCH_QUADRATIC_3D,
+    "hashed-3d": F.FS_SEARCH_HASHED_3D,
+    "compressed-3d": F.FS_SEARCH_COMPRESSED_3D,
+}
+PRECISIONS = {"fp32": F.FS_PRECISION_FP32, "fp32-kahan": F.FS_PRECISION_FP32_KAHAN, "fp64": F.FS_PRECISION_FP64}
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data
+
+
+@dataclass
+class ParticleCollection:
+    """Dense SoA particle arrays in host order (the components of
+    fluidSolver/Particle.hpp:15-50 that the hot path reads and writes)."""
+
+    position: np.ndarray
+    velocity: np.ndarray | None = None
+    acceleration: np.ndarray | None = None
+    external: np.ndarray | None = None
+    mass: np.ndarray | None = None
+    density: np.ndarray | None = None
+    pressure: np.ndarray | None = None
+    type: np.ndarray | None = None
+    tag: np.ndarray | None = None
+    # IISPH data (download only)
+    predicted_velocity: np.ndarray | None = None
+    non_pressure_acceleration: np.ndarray | None = None
+    source_term: np.ndarray | None = None
+    diagonal_element: np.ndarray | None = None
+
+    @property
+    def dim(self) -> int:
+        return self.position.shape[1]
+
+    def __len__(self) -> int:
+        return self.position.shape[0]
+
+    def size(self) -> int:
+        return len(self)
+
+    def normalized(self) -> "ParticleCollection":
+        n, d = self.position.shape
+        f32 = lambda a, shape: np.ascontiguousarray(a, dtype=np.float32).reshape(shape) if a is not None else None
+        return ParticleCollection(
+            position=f32(self.position, (n, d)), velocity=f32(self.velocity, (n, d)),
+            acceleration=f32(self.acceleration, (n, d)), external=f32(self.external, (n, d)),
+            mass=f32(self.mass, (n,)), density=f32(self.density, (n,)), pressure=f32(self.pressure, (n,)),
+            type=np.ascontiguousarray(self.type, dtype=np.uint8) if self.type is not None else None,
+            tag=np.ascontiguousarray(self.tag, dtype=np.uint32) if self.tag is not None else None)
+
+    def as_fs(self) -> F.FsParticles:
+        p = F.FsParticles()
+        p.n = len(self)
+        for name in ("position", "velocity", "acceleration", "external", "mass", "density", "pressure", "type", "tag",
+                     "predicted_velocity", "non_pressure_acceleration", "source_term", "diagonal_element"):
+            setattr(p, name, _ptr(getattr(self, name)))
+        return p
+
+
+@dataclass
+class Timepoint:
+    """time/Timepoint.hpp:7-14"""
+    timestep_number: int = 0
+    simulation_time: float = 0.0
+    desired_time_step: float = 0.0
+    actual_time_step: float = 0.0
+
+
+@dataclass
+class SimulationParameters:
+    rest_density: float = 1000.0
+    gravity: float = 9.81
+    particle_size: float = 0.1
+
+
+@dataclass
+class ConstantTimestepGeneratorSettings:
+    timestep: float = 0.001
+    lambda_v: float = 0.4
+    lambda_a: float = 0.25
+
+
+@dataclass
+class ConstantTimestepGenerator:
+    """time/ConstantTimestepGenerator.hpp: generate_next_timestep() returns settings.timestep."""
+    settings: ConstantTimestepGeneratorSettings = field(default_factory=ConstantTimestepGeneratorSettings)
+
+    def generate_next_timestep(self) -> None:
+        pass
+
+    def get_generated_timestep(self) -> float:
+        return self.settings.timestep
+
+
+@dataclass
+class IISPHSettings3D:
+    max_density_error_allowed: float = 0.001
+    min_number_of_iterations: int = 2
+    max_number_of_iterations: int = 100
+    omega: float = 0.5
+    gamma: float = 0.7
+    viscosity: float = 5.0
+    single_layer_boundary: bool = False
+    single_layer_boundary_gamma_1: float = 1.1
+
+
+@dataclass
+class IISPHSettings:
+    MaxDensityErrorAllowed: float = 0.001
+    MinNumberOfIterations: int = 2
+    MaxNumberOfIterations: int = 100
+    Omega: float = 0.5
+    Gamma: float = 0.7
+    Viscosity: float = 5.0
+
+
+@dataclass
+class SESPHSettings3D:
+    StiffnessK: float = 100000.0
+    Viscosity: float = 5.0
+    single_layer_boundary: bool = False
+    single_layer_boundary_gamma_1: float = 1.1
+    single_layer_boundary_gamma_2: float = 1.1
+
+
+@dataclass
+class SESPHSettings:
+    StiffnessK: float = 100000.0
+    Viscosity: float = 5.0
+
+
+class _Data:
+    def __init__(self):
+        self.collection: ParticleCollection | None = None
+        self.changed = True
+
+    def notify_that_data_changed(self):
+        self.changed = True
+
+
+class _DeviceContext:
+    """Owns one fs_ctx."""
+
+    def __init__(self, params: F.FsParams):
+        self.L = F.lib()
+        self.params = params
+        self.ctx = ctypes.c_void_p()
+        F.check(self.L.fs_create(ctypes.byref(params), ctypes.byref(self.ctx)))
+
+    def close(self):
+        if self.ctx:
+            self.L.fs_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FluidSolverBase:
+    """IFluidSolverBase (IFluidSolver.hpp:16-34) over the device path."""
+
+    DIM = 3
+    SOLVER = F.FS_SOLVER_NONE
+    DEFAULT_SEARCH = "hashed-3d"
+
+    def __init__(self, search: str | None = None, precision: str = "fp32-kahan", reference_order: bool = False,
+                 device: int = 0, neighbor_capacity: int = 0):
+        self.search = search or self.DEFAULT_SEARCH
+        if self.search not in SEARCH_KINDS:
+            raise ValueError(f"unknown neighborhood search {self.search!r}")
+        self.precision = precision
+        self.reference_order = reference_order
+        self.device = device
+        self.neighbor_capacity = neighbor_capacity
+        self.parameters = SimulationParameters()
+        self.timestep_generator = ConstantTimestepGenerator()
+        self.data = _Data()
+        self._dev: _DeviceContext | None = None
+        self._key = None
+        self.last_stats = F.FsStepStats()
+
+    # ---- configuration -------------------------------------------------
+    def _fill_settings(self, p: F.FsParams) -> None:
+        raise NotImplementedError
+
+    def _params(self, n: int) -> F.FsParams:
+        p = F.FsParams()
+        F.lib().fs_params_default(ctypes.byref(p), self.DIM, self.SOLVER, SEARCH_KINDS[self.search])
+        p.precision = PRECISIONS[self.precision]
+        p.flags = F.FS_FLAG_REFERENCE_ORDER if self.reference_order else 0
+        p.device = self.device
+        p.rest_density = self.parameters.rest_density
+        p.gravity = self.parameters.gravity
+        p.particle_size = self.parameters.particle_size
+        g = self.timestep_generator.settings
+        p.timestep, p.lambda_v, p.lambda_a = g.timestep, g.lambda_v, g.lambda_a
+        p.max_particles = max(n, 1)
+        p.neighbor_capacity = self.neighbor_capacity
+        self._fill_settings(p)
+        return p
+
+    def initialize(self) -> None:
+        """Creates / reconfigures the device context and uploads the
+        collection when data changed (IISPHFluidSolver3D.hpp:79-103)."""
+        col = self.data.collection
+        if col is None:
+            raise F.FluidSolverError(F.FS_ERR_INVALID, "Particle collection is null.")
+        p = self._params(len(col))
+        key = (p.max_particles, p.precision, p.flags, p.search, p.solver)
+        if self._dev is None or key != self._key:
+            if self._dev is not None:
+                self._dev.close()
+            self._dev = _DeviceContext(p)
+            self._key = key
+            self.data.changed = True
+        else:
+            F.check(F.lib().fs_set_params(self._dev.ctx, ctypes.byref(p)))
+        if self.data.changed:
+            self._uploaded = col.normalized()
+            F.check(F.lib().fs_upload(self._dev.ctx, ctypes.byref(self._uploaded.as_fs())))
+            self.data.changed = False
+
+    @property
+    def ctx(self):
+        if self._dev is None:
+            self.initialize()
+        return self._dev.ctx
+
+    # ---- IFluidSolverBase ---------------------------------------------
+    def execute_neighborhood_search(self) -> None:
+        self.initialize()
+        F.check(F.lib().fs_find_neighbors(self._dev.ctx))
+
+    def execute_simulation_step(self, timepoint: Timepoint) -> None:
+        self.initialize()
+        F.check(F.lib().fs_solve_step(self._dev.ctx, float(timepoint.desired_time_step), ctypes.byref(self.last_stats)))
+        timepoint.actual_time_step = float(self.last_stats.actual_dt)
+
+    def step(self, desired_dt: float | None = None) -> F.FsStepStats:
+        """Neighborhood search + step in one call (fs_step)."""
+        self.initialize()
+        dt = self.timestep_generator.settings.timestep if desired_dt is None else desired_dt
+        F.check(F.lib().fs_step(self._dev.ctx, float(dt), ctypes.byref(self.last_stats)))
+        return self.last_stats
+
+    def phase_times(self) -> list[float]:
+        out = np.zeros(5, np.float32)
+        F.check(F.lib().fs_last_phase_times(self.ctx, out.ctypes.data))
+        return out.tolist()
+
+    # ---- neighborhood interface ---------------------------------------
+    def neighbor_lists(self) -> tuple[np.ndarray, np.ndarray]:
+        """CSR (offsets, indices) of the contract's lists in host index space, each list ascending."""
+        n = len(self.data.collection)
+        off = np.zeros(n + 1, np.int64)
+        tot = ctypes.c_int64()
+        st = F.lib().fs_get_neighbors_csr(self.ctx, off.ctypes.data, None, ctypes.byref(tot))
+        if st not in (F.FS_OK, F.FS_ERR_CAPACITY):
+            F.check(st)
+        idx = np.zeros(max(tot.value, 1), np.int64)
+        F.check(F.lib().fs_get_neighbors_csr(self.ctx, off.ctypes.data, idx.ctypes.data, ctypes.byref(tot)))
+        return off, idx[:tot.value]
+
+    def get_neighbors(self, index: int) -> np.ndarray:
+        off, idx = self.neighbor_lists()
+        return idx[off[index]:off[index + 1]]
+
+    def get_neighbors_of_position(self, position, cap: int = 4096) -> np.ndarray:
+        pos = np.zeros(3, np.float32)
+        pos[:self.DIM] = np.asarray(position, np.float32)[:self.DIM]
+        out = np.zeros(cap, np.int64)
+        cnt = ctypes.c_int64()
+        F.check(F.lib().fs_query_position(self.ctx, pos.ctypes.data, out.ctypes.data, cap, ctypes.byref(cnt)))
+        return out[:min(cnt.value, cap)]
+
+    # ---- state ---------------------------------------------------------
+    def collection(self, iisph: bool = False) -> ParticleCollection:
+        """Downloads the device state in host order."""
+        n = len(self.data.collection)
+        d = self.DIM
+        out = ParticleCollection(
+            position=np.zeros((n, d), np.float32), velocity=np.zeros((n, d), np.float32),
+            acceleration=np.zeros((n, d), np.float32), external=np.zeros((n, d), np.float32),
+            mass=np.zeros(n, np.float32), density=np.zeros(n, np.float32), pressure=np.zeros(n, np.float32),
+            type=np.zeros(n, np.uint8), tag=np.zeros(n, np.uint32))
+        if iisph:
+            out.predicted_velocity = np.zeros((n, d), np.float32)
+            out.non_pressure_acceleration = np.zeros((n, d), np.float32)
+            out.source_term = np.zeros(n, np.float32)
+            out.diagonal_element = np.zeros(n, np.float32)
+        F.check(F.lib().fs_download(self.ctx, ctypes.byref(out.as_fs())))
+        return out
+
+    def close(self):
+        if self._dev is not None:
+            self._dev.close()
+            self._dev = None
+
+
+class IISPHFluidSolver3D(FluidSolverBase):
+    """IISPHFluidSolver3D (fluidSolver/solver/IISPHFluidSolver3D.hpp:22-610)."""
+    DIM = 3
+    SOLVER = F.FS_SOLVER_IISPH_3D
+    DEFAULT_SEARCH = "hashed-3d"
+
+    def __init__(self, *a, **k):
+        super().__init__(*a, **k)
+        self.settings = IISPHSettings3D()
+
+    @property
+    def stat_last_iteration_count(self) -> int:
+        return int(self.last_stats.iterations)
+
+    @property
+    def stat_last_average_predicted_density_error(self) -> float:
+        return float(self.last_stats.avg_density_error)
+
+    def _fill_settings(self, p):
+        s = self.settings
+        p.max_density_error = s.max_density_error_allowed
+        p.min_iterations = s.min_number_of_iterations
+        p.max_iterations = s.max_number_of_iterations
+        p.omega, p.gamma, p.viscosity = s.omega, s.gamma, s.viscosity
+        p.single_layer_boundary = 1 if s.single_layer_boundary else 0
+        p.single_layer_gamma_1 = s.single_layer_boundary_gamma_1
+
+
+class IISPHFluidSolver(FluidSolverBase):
+    """IISPHFluidSolver, 2D (fluidSolver/solver/IISPHFluidSolver.hpp:21-548)."""
+    DIM = 2
+    SOLVER = F.FS_SOLVER_IISPH_2D
+    DEFAULT_SEARCH = "quadratic-2d"
+
+    def __init__(self, *a, **k):
+        super().__init__(*a, **k)
+        self.settings = IISPHSettings()
+
+    def _fill_settings(self, p):
+        s = self.settings
+        p.max_density_error = s.MaxDensityErrorAllowed
+        p.min_iterations = s.MinNumberOfIterations
+        p.max_iterations = s.MaxNumberOfIterations
+        p.omega, p.gamma, p.viscosity = s.Omega, s.Gamma, s.Viscosity
+
+
+class SESPHFluidSolver3D(FluidSolverBase):
+    """SESPHFluidSolver3D (fluidSolver/solver/SESPHFluidSolver3D.hpp:12-339)."""
+    DIM = 3
+    SOLVER = F.FS_SOLVER_SESPH_3D
+    DEFAULT_SEARCH = "hashed-3d"
+
+    def __init__(self, *a, **k):
+        super().__init__(*a, **k)
+        self.settings = SESPHSettings3D()
+
+    def _fill_settings(self, p):
+        s = self.settings
+        p.stiffness, p.viscosity = s.StiffnessK, s.Viscosity
+        p.single_layer_boundary = 1 if s.single_layer_boundary else 0
+        p.single_layer_gamma_1 = s.single_layer_boundary_gamma_1
+        p.single_layer_gamma_2 = s.single_layer_boundary_gamma_2
+
+
+class SESPHFluidSolver(FluidSolverBase):
+    """SESPHFluidSolver, 2D (fluidSolver/solver/SESPHFluidSolver.hpp:12-299)."""
+    DIM = 2
+    SOLVER = F.FS_SOLVER_SESPH_2D
+    DEFAULT_SEARCH = "quadratic-2d"
+
+    def __init__(self, *a, **k):
+        super().__init__(*a, **k)
+        self.settings = SESPHSettings()
+
+    def _fill_settings(self, p):
+        s = self.settings
+        p.stiffness, p.viscosity = s.StiffnessK, s.Viscosity
+
+
+class NeighborhoodSearch(FluidSolverBase):
+    """A neighborhood search on its own (the NS concept, IFluidSolver.hpp:36-73):
+    collection, search_radius, find_neighbors(), get_neighbors(index | position).
+    The search radius is 2 * particle_size as the solvers set it
+    (IISPHFluidSolver3D.hpp:94)."""
+
+    SOLVER = F.FS_SOLVER_NONE
+
+    def __init__(self, search: str, search_radius: float, **k):
+        super().__init__(search=search, **k)
+        self.DIM = 2 if search.endswith("2d") else 3
+        self.parameters.particle_size = search_radius / 2.0
+        self.settings = None
+
+    @property
+    def search_radius(self) -> float:
+        return self.parameters.particle_size * 2.0
+
+    def _fill_settings(self, p):
+        pass
+
+    def find_neighbors(self) -> None:
+        self.execute_neighborhood_search()
+
+    def set_positions(self, position: np.ndarray) -> None:
+        self.data.collection.position = np.ascontiguousarray(position, np.float32)
+        self.data.changed = True

@@ -1,0 +1,231 @@
+/*
+ * fluidsolver_b200 -- C-ABI of the B200 implementation of libFluid's
+ * per-timestep hot path: the neighborhood search and the SESPH / IISPH steps
+ * in 2D and 3D.
+ *
+ * The boundary replaces these reference interfaces (paths relative to the
+ * FluidSolver repository):
+ *   - IFluidSolverBase::execute_neighborhood_search / execute_simulation_step
+ *     (src/libFluid/fluidSolver/IFluidSolver.hpp:16-34), as implemented by
+ *     SESPHFluidSolver (solver/SESPHFluidSolver.hpp:49-111),
+ *     SESPHFluidSolver3D (solver/SESPHFluidSolver3D.hpp:49-130),
+ *     IISPHFluidSolver (solver/IISPHFluidSolver.hpp:139-188) and
+ *     IISPHFluidSolver3D (solver/IISPHFluidSolver3D.hpp:120-562);
+ *   - the neighborhood-search concept (IFluidSolver.hpp:36-73): find_neighbors,
+ *     get_neighbors(index), get_neighbors(position) of
+ *     QuadraticNeighborhoodSearchDynamicAllocated, HashedNeighborhoodSearch,
+ *     QuadraticNeighborhoodSearch3D, HashedNeighborhoodSearch3D,
+ *     CompressedNeighborhoodSearch and CompactHashingNeighborhoodSearch;
+ *   - the particle-collection components the path reads and writes
+ *     (fluidSolver/Particle.hpp:15-50, ParticleCollection.hpp:11-177).
+ *
+ * Conventions
+ *   - Every function returns an fs_status; FS_OK is 0. fs_last_error() gives a
+ *     one-line message for the last failure on the calling thread.
+ *   - A context owns one CUDA stream on one device; all work is ordered on it
+ *     and every call that returns data to the host synchronises that stream.
+ *   - Particle arrays passed in or out are dense, in the caller's index order
+ *     ("host order"): vectors hold `dim` floats per particle. The device keeps
+ *     its own spatially sorted order internally; indices that cross the
+ *     boundary are always host indices.
+ *   - No call waits on the device without a bound: device-side failures
+ *     (neighbor overflow, non-finite state, an exhausted iteration cap) are
+ *     reported through the status word read back by the call.
+ */
+#ifndef FLUIDSOLVER_B200_H
+#define FLUIDSOLVER_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FS_ABI_VERSION 1
+
+typedef enum fs_status {
+    FS_OK = 0,
+    FS_ERR_INVALID = 1,   /* bad argument or configuration (CompatibilityReport issue in the reference) */
+    FS_ERR_CAPACITY = 2,  /* a neighbor list exceeded its capacity (the reference throws, CompressedNeighbors.cpp:276-321) */
+    FS_ERR_NAN = 3,       /* non-finite particle state detected */
+    FS_ERR_TIMEOUT = 4,   /* a bounded device-side wait gave up */
+    FS_ERR_CUDA = 5,      /* a CUDA runtime call failed */
+    FS_ERR_NO_DEVICE = 6, /* no usable sm_100 device */
+    FS_ERR_STATE = 7      /* call out of order (e.g. lists requested before a search) */
+} fs_status;
+
+/* Solver selected by SolverSerializer's "type" string (SolverSerializer.cpp:137-219). */
+typedef enum fs_solver_kind {
+    FS_SOLVER_NONE = 0,     /* neighborhood search only */
+    FS_SOLVER_SESPH_2D = 1, /* "sesph"    */
+    FS_SOLVER_SESPH_3D = 2, /* "sesph-3d" */
+    FS_SOLVER_IISPH_2D = 3, /* "iisph"    */
+    FS_SOLVER_IISPH_3D = 4  /* "iisph-3d" */
+} fs_solver_kind;
+
+/*
+ * Neighbor-set contract of the reference search being replaced. One device
+ * search (cell-key radix sort + Z-order reordering + cell table) serves all of
+ * them; the contract fixes the predicate, which particles own a list, which
+ * particles may appear in one, and the capacity limit.
+ */
+typedef enum fs_search_kind {
+    FS_SEARCH_QUADRATIC_2D = 0,  /* QuadraticNeighborhoodSearchDynamicAllocated.cpp:11-38: every particle, every j, length(d) <= r */
+    FS_SEARCH_HASHED_2D = 1,     /* HashedNeighborhoodSearch.cpp:9-73: fluid owners only, every j, length(d) <= r */
+    FS_SEARCH_COMPACT_2D = 2,    /* CompactHashingNeighborhoodSearch.cpp:14-84,210-247: active owners, active j, length(d) <= r, <= 40 */
+    FS_SEARCH_QUADRATIC_3D = 3,  /* QuadraticNeighborhoodSearch3D.cpp:32-69: active owners, active j, dot(d,d) <= r*r */
+    FS_SEARCH_HASHED_3D = 4,     /* HashedNeighborhoodSearch3D.cpp:134-185: as quadratic-3d */
+    FS_SEARCH_COMPRESSED_3D = 5  /* CompressedNeighbors.cpp:536-595: as quadratic-3d, <= 97 neighbors */
+} fs_search_kind;
+
+typedef enum fs_precision {
+    FS_PRECISION_FP32 = 0,       /* plain float sums in the reference's operation order */
+    FS_PRECISION_FP32_KAHAN = 1, /* float state, Kahan-compensated neighbor sums, FP64 residual (default) */
+    FS_PRECISION_FP64 = 2        /* double state and arithmetic (error reference) */
+} fs_precision;
+
+/* fs_params.flags */
+#define FS_FLAG_REFERENCE_ORDER 0x1u  /* sum neighbors in HashedNeighborhoodSearch3D's list order and
+                                         reproduce the serial L1 density read order of the reference
+                                         (IISPHFluidSolver3D.hpp:60-64 vs :210); for bit-level parity runs */
+#define FS_FLAG_SYNC_EACH_ITERATION 0x2u /* host-driven IISPH loop (one readback per iteration) instead of the
+                                            device-side early exit inside a CUDA graph */
+
+/* Particle types (Particle.hpp:7-12). */
+#define FS_TYPE_NORMAL 0
+#define FS_TYPE_BOUNDARY 1
+#define FS_TYPE_INACTIVE 2
+
+typedef struct fs_params {
+    int32_t dim;        /* 2 or 3 */
+    int32_t solver;     /* fs_solver_kind */
+    int32_t search;     /* fs_search_kind */
+    int32_t precision;  /* fs_precision */
+    uint32_t flags;     /* FS_FLAG_* */
+    int32_t device;     /* CUDA device ordinal */
+
+    /* IFluidSolverBase::SimulationParameters (IFluidSolver.hpp:18-23) */
+    float rest_density;
+    float gravity;
+    float particle_size; /* h; the kernel support and search radius are 2*h (LibFluidMath.hpp:11) */
+
+    /* SESPHSettings / SESPHSettings3D (settings/SESPHSettings*.hpp) */
+    float stiffness;
+    /* viscosity of whichever solver is selected */
+    float viscosity;
+    int32_t single_layer_boundary;
+    float single_layer_gamma_1;
+    float single_layer_gamma_2; /* SESPH-3D only */
+
+    /* IISPHSettings / IISPHSettings3D (settings/IISPHSettings*.hpp) */
+    float max_density_error;
+    int32_t min_iterations;
+    int32_t max_iterations;
+    float omega;
+    float gamma;
+
+    /* ConstantTimestepGenerator settings (ConstantTimestepGenerator.hpp:8-13) */
+    float timestep;
+    float lambda_v;
+    float lambda_a;
+
+    /* capacities */
+    int64_t max_particles;      /* device arrays are sized for this many particles */
+    int32_t neighbor_capacity;  /* per-particle list slots for the solver (0: chosen from the scene) */
+    int32_t reserved;
+} fs_params;
+
+/* Fills *p with libFluid's defaults for the given solver and dimension
+ * (IISPHSettings3D.hpp:6-20 etc.; rest density 1000, gravity 9.81, size 0.1). */
+void fs_params_default(fs_params* p, int32_t dim, int32_t solver, int32_t search);
+
+/* Dense host arrays in host order. Pointers not needed by a call may be NULL
+ * (on upload: NULL means "zero" for velocity/acceleration/external, "rest
+ * density" for density, 0 for pressure, tag = index). */
+typedef struct fs_particles {
+    int64_t n;
+    float* position;     /* dim per particle  (MovementData{,3D}.position)      */
+    float* velocity;     /* dim per particle  (MovementData{,3D}.velocity)      */
+    float* acceleration; /* dim per particle  (MovementData{,3D}.acceleration)  */
+    float* external;     /* dim per particle  (ExternalForces{,3D})             */
+    float* mass;         /* ParticleData.mass     */
+    float* density;      /* ParticleData.density  */
+    float* pressure;     /* ParticleData.pressure */
+    uint8_t* type;       /* ParticleInfo.type     */
+    uint32_t* tag;       /* ParticleInfo.tag      */
+    /* IISPH per-particle data (IISPHParticleData3D, IISPHFluidSolver3D.hpp:13-19); download only */
+    float* predicted_velocity;       /* dim per particle */
+    float* non_pressure_acceleration;/* dim per particle (3D only) */
+    float* source_term;
+    float* diagonal_element;
+} fs_particles;
+
+/* IISPHFluidSolver3D's statistics (IISPHFluidSolver3D.hpp:32-33) plus the step's time step. */
+typedef struct fs_step_stats {
+    float desired_dt;
+    float actual_dt;             /* Timepoint::actual_time_step after the CFL clamp */
+    int32_t iterations;          /* stat_last_iteration_count */
+    float avg_density_error;     /* stat_last_average_predicted_density_error (absolute, density units) */
+    double avg_density_error_fp64;
+    float max_density_error;
+    float max_velocity;
+    float max_acceleration;
+    int32_t status;              /* fs_status of the device status word */
+    int32_t max_neighbors;       /* largest list seen by the last search */
+} fs_step_stats;
+
+typedef struct fs_ctx fs_ctx;
+
+int32_t fs_abi_version(void);
+const char* fs_last_error(void);
+
+/* Creates a context (device buffers for p->max_particles particles, a stream). */
+fs_status fs_create(const fs_params* p, fs_ctx** out);
+fs_status fs_destroy(fs_ctx* ctx);
+/* Replaces the settings (data-change propagation of IFluidSolverBase::initialize). */
+fs_status fs_set_params(fs_ctx* ctx, const fs_params* p);
+
+/* Copies a whole particle collection to the device (host order). */
+fs_status fs_upload(fs_ctx* ctx, const fs_particles* in);
+/* Copies the device state back in host order into the non-NULL arrays of *out. */
+fs_status fs_download(fs_ctx* ctx, fs_particles* out);
+
+/* Neighborhood search on the current positions (find_neighbors). */
+fs_status fs_find_neighbors(fs_ctx* ctx);
+/* Neighbor lists of the last search in host-index space, each list ascending:
+ * offsets has n+1 entries; indices may be NULL to query *total first. */
+fs_status fs_get_neighbors_csr(fs_ctx* ctx, int64_t* offsets, int64_t* indices, int64_t* total);
+/* Neighbors of an arbitrary position (get_neighbors(vec)); ascending host indices.
+ * Writes min(count, cap) indices and the full count to *count. */
+fs_status fs_query_position(fs_ctx* ctx, const float* position, int64_t* out, int64_t cap, int64_t* count);
+
+/* The solver's timestep on the lists of the preceding fs_find_neighbors
+ * (IFluidSolverBase::execute_simulation_step, IFluidSolver.hpp:30); the
+ * CFL-clamped time step is returned in stats->actual_dt. desired_dt <= 0 uses
+ * p->timestep. */
+fs_status fs_solve_step(fs_ctx* ctx, float desired_dt, fs_step_stats* stats);
+/* One solver step: neighborhood search + the solver's timestep, like
+ * Simulator::execute_simulation_step (Simulator.cpp:7-57) without entities
+ * and sensors. desired_dt <= 0 uses p->timestep. */
+fs_status fs_step(fs_ctx* ctx, float desired_dt, fs_step_stats* stats);
+/* `steps` steps back to back without host synchronisation in between
+ * (captured once in a CUDA graph); stats of the last step. */
+fs_status fs_run(fs_ctx* ctx, int32_t steps, float desired_dt, fs_step_stats* stats);
+
+/* Device time of the phases of the last fs_step (ms): [0] search, [1] L1,
+ * [2] L2, [3] pressure iterations, [4] integration. */
+fs_status fs_last_phase_times(fs_ctx* ctx, float* ms5);
+
+/* ---- batched scenes -------------------------------------------------------
+ * Many independent scenes of uneven size advance together: one launch per
+ * sub-phase covers every scene, each scene keeps its own convergence test and
+ * time step. Scene s owns host particles [offsets[s], offsets[s+1]). */
+fs_status fs_batch_create(const fs_params* p, int32_t scenes, const int64_t* offsets, fs_ctx** out);
+/* stats has one entry per scene. */
+fs_status fs_batch_run(fs_ctx* ctx, int32_t steps, float desired_dt, fs_step_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLUIDSOLVER_B200_H */
