@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Benchmark of the 3D IISPH timestep (neighborhood search + IISPH step) on
+one or more B200s; prints one JSON line.
+
+Workload (default): the 1M-fluid breaking dam -- a 100 x 100 x 100 block with
++-1 % seeded jitter in a single-layer tank (256,624 boundary particles), cubic
+spline kernel with support 2 x spacing, relaxed Jacobi omega 0.5, gamma 0.7,
+<= 0.1 % average density error, 2..100 iterations, viscosity 0.01, single-layer
+gamma_1 1.1. The scene is in the reference's own units (particle size 1, rest
+density 1, dt 0.005; see fluidsolver_b200/scenes.py). A "step" is one
+Simulator step: search + IISPH step over the whole scene. The metric counts
+fluid particles: fluid particle-steps per second.
+
+  python bench.py [--gpus N --steps K --warmup W]     # this implementation
+  python bench.py --impl reference ...                # the reference's CPU code
+
+Under torchrun with N ranks every rank advances its own replica of the scene
+on its own GPU (independent scenes, no exchange): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "3D IISPH fluid particle-steps/s (1M breaking dam), <= 0.1% avg density error"
+UNIT = "fluid particle-steps/s"
+
+# algorithmic bytes (compulsory SoA traffic per phase; neighbor gathers are
+# on-chip reuse and neighbor lists are not counted)
+BYTES_SEARCH = 144   # per active particle: keys, 2 radix passes, permute pos/vel/rho/tag, cell ranges
+BYTES_L1 = 76        # per fluid particle: read pos4 vel4 rho, write rho v*4 a_np4 p
+BYTES_L2 = 44        # per fluid particle: read pos4 v*4 rho, write s a_ii
+BYTES_ITER = 84      # per fluid particle and iteration: pressure acceleration 36 + update 48
+BYTES_INTEGRATE = 96  # per active particle: read pos4 v*4 a_np4 a4, write pos4 vel4
+PHASES = ["search", "iisph_l1", "iisph_l2", "pressure_iterations", "integration"]
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device: int):
+        try:
+            import torch
+            self.index = "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
+        except Exception:
+            self.index = str(device)
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None:
+            return None
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 8:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_solver(scene, device, precision="fp32-kahan"):
+    from fluidsolver_b200 import IISPHFluidSolver3D
+    from fluidsolver_b200.scenes import REFERENCE_UNITS_DT
+    s = IISPHFluidSolver3D(search="hashed-3d", precision=precision, device=device)
+    s.parameters.rest_density = scene.rest_density
+    s.parameters.gravity = 9.81
+    s.parameters.particle_size = scene.particle_size
+    s.settings.viscosity = 0.01
+    s.settings.single_layer_boundary = True
+    s.settings.single_layer_boundary_gamma_1 = 1.1
+    s.settings.max_density_error_allowed = 0.001
+    s.settings.min_number_of_iterations = 2
+    s.settings.max_number_of_iterations = 100
+    s.settings.omega = 0.5
+    s.settings.gamma = 0.7
+    s.timestep_generator.settings.timestep = REFERENCE_UNITS_DT
+    s.data.collection = scene.collection
+    return s
+
+
+def reference_settings():
+    from oracle import ref_oracle as R
+    from fluidsolver_b200.scenes import REFERENCE_UNITS_DT
+    return ((1.0, 9.81, 1.0), R.iisph3d_settings(max_err=0.001, min_it=2, max_it=100, omega=0.5, gamma=0.7,
+                                                   viscosity=0.01, single_layer=True, gamma1=1.1),
+            (REFERENCE_UNITS_DT, 0.4, 0.25))
+
+
+def cpu_baseline_from_state(state, n_fluid, seconds_budget=25.0):
+    """The reference's own CPU code (oracle/_ref, all host cores) continuing
+    from the GPU's state: bounded to ~one or two steps of the same scene."""
+    from oracle import ref_oracle as R
+    variant = "omp" if R.available("omp") else ("serial" if R.available("serial") else None)
+    if variant is None:
+        return None
+    params, settings, gen = reference_settings()
+    ref = R.RefSolver("iisph-3d", "hashed-3d", state, params, settings, gen, variant=variant)
+    steps, t0 = 0, time.perf_counter()
+    iters = []
+    while True:
+        iters.append(ref.step()["iterations"])
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > seconds_budget / 2 or steps >= 3:
+            break
+    ref.close()
+    cores = os.cpu_count() if variant == "omp" else 1
+    return {"value": n_fluid * steps / el, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{steps} step(s) of the same 1M-fluid scene continuing from the GPU state, "
+                      f"reference libFluid IISPHFluidSolver3D<CubicSplineKernel3D, HashedNeighborhoodSearch3D> "
+                      f"({'OpenMP over its 16-particle chunks' if variant == 'omp' else 'as built, serial'}), "
+                      f"iterations {iters}, {el:.1f} s"}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from fluidsolver_b200 import _lib as F
+    from fluidsolver_b200 import scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    scene = scenes.dam_1m(seed=5 + rank)
+    n_active = scene.n_fluid + scene.n_boundary
+    solver = make_solver(scene, local, args.precision)
+    L = F.lib()
+    for _ in range(args.warmup):
+        solver.step()
+    ctx = solver.ctx
+    stream = torch.cuda.ExternalStream(L.fs_stream(ctx), device=torch.device("cuda", local))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = L.fs_launch_count(ctx)
+    phase = np.zeros(5)
+    iters, errs = [], []
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            st = solver.step()
+            phase += np.array(solver.phase_times())
+            iters.append(int(st.iterations))
+            errs.append(float(st.avg_density_error_fp64))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    launches = L.fs_launch_count(ctx) - launches0
+    value = scene.n_fluid * args.steps * world / (ms / 1e3)
+
+    # roofline of the dominant phase (algorithmic bytes / its event-timed duration)
+    F_, N_ = scene.n_fluid, n_active
+    it_total = float(sum(iters))
+    phase_bytes = [BYTES_SEARCH * N_ * args.steps, BYTES_L1 * F_ * args.steps, BYTES_L2 * F_ * args.steps,
+                   BYTES_ITER * F_ * it_total, BYTES_INTEGRATE * N_ * args.steps]
+    dom = int(np.argmax(phase))
+    peak, peak_kind = measured_peak()
+    achieved = phase_bytes[dom] / (phase[dom] / 1e3) / 1e9
+    step_bytes = sum(phase_bytes) / args.steps
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(PHASES[dom])
+
+    # end to end through the public API: pinned host state in, step, state out
+    e2e = run_e2e(solver, scene, min(args.steps, 5), local, max_over_ranks)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        state = solver.collection()
+        cpu = cpu_baseline_from_state(state, scene.n_fluid)
+
+    clocks = clk.summary()
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (Kahan-compensated sums, FP64 residual)" if args.precision ==
+            "fp32-kahan" else args.precision, "data": "synthetic (seeded breaking-dam scenes)",
+            "config": {"workload": "3D IISPH breaking dam, 1,000,000 fluid + 256,624 boundary particles, "
+                       "hashed-3d neighbor contract, dt 0.005 (reference units), single-layer boundary",
+                       "fluid_particles_per_gpu": scene.n_fluid, "boundary_particles_per_gpu": scene.n_boundary,
+                       "parallelism": f"replicas x{world} (independent scenes)",
+                       "l2": "inputs larger than L2 (~0.5 GB of particle state and lists per step)",
+                       "iterations_mean": it_total / args.steps, "avg_density_error_max": max(errs),
+                       "phase_ms_per_step": dict(zip(PHASES, (phase / args.steps).round(4).tolist())),
+                       "algorithmic_bytes_per_step": step_bytes,
+                       "step_fraction_of_hbm_roofline": step_bytes / (ms / args.steps / 1e3) / 1e9 / peak},
+            "roofline": {"bound": "hbm", "kernel": PHASES[dom], "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+        }
+        print(json.dumps(out))
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_e2e(solver, scene, steps, device, max_over_ranks):
+    """Per step: upload the state from pinned host memory, search + step,
+    download the state to pinned host memory (the host collection stays
+    authoritative, as when entities or sensors touch it every step)."""
+    import torch
+    from fluidsolver_b200 import _lib as F
+    L = F.lib()
+    n = len(scene.collection)
+
+    def pinned(shape, dtype):
+        return torch.empty(shape, dtype=dtype, pin_memory=True).numpy()
+
+    src = scene.collection
+    inp = {"position": pinned((n, 3), torch.float32), "velocity": pinned((n, 3), torch.float32),
+           "mass": pinned((n,), torch.float32), "density": pinned((n,), torch.float32),
+           "type": pinned((n,), torch.uint8)}
+    for k, a in inp.items():
+        a[...] = getattr(src, k)
+    out = {"position": pinned((n, 3), torch.float32), "velocity": pinned((n, 3), torch.float32),
+           "density": pinned((n,), torch.float32), "pressure": pinned((n,), torch.float32)}
+    fin = F.FsParticles()
+    fin.n = n
+    for k, a in inp.items():
+        setattr(fin, k, a.ctypes.data)
+    fout = F.FsParticles()
+    fout.n = n
+    for k, a in out.items():
+        setattr(fout, k, a.ctypes.data)
+    h2d = sum(a.nbytes for a in inp.values())
+    d2h = sum(a.nbytes for a in out.values())
+    ctx = solver.ctx
+    stats = F.FsStepStats()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        F.check(L.fs_upload(ctx, ctypes.byref(fin)))
+        F.check(L.fs_step(ctx, ctypes.c_float(0.0), ctypes.byref(stats)))
+        F.check(L.fs_download(ctx, ctypes.byref(fout)))
+        inp["position"][...] = out["position"]
+        inp["velocity"][...] = out["velocity"]
+        inp["density"][...] = out["density"]
+    el = max_over_ranks(time.perf_counter() - t0)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"value": scene.n_fluid * steps * world / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "steps": steps,
+            "path": "fs_upload (pinned host) -> fs_step -> fs_download (pinned host), wall clock"}
+
+
+def run_reference(args):
+    """The reference's own CPU implementation (libFluid sources compiled
+    unmodified in oracle/_ref) on all host cores, on a bounded sample of the
+    workload: the 100k-fluid breaking dam of the same scene family."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import ref_oracle as R
+    from fluidsolver_b200 import scenes
+    variant = "omp" if R.available("omp") else ("serial" if R.available("serial") else None)
+    if variant is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (needs the reference "
+                          "checkout at build time)"}))
+        return
+    scene = scenes.dam_100k()
+    params, settings, gen = reference_settings()
+    ref = R.RefSolver("iisph-3d", "hashed-3d", scene.collection, params, settings, gen, variant=variant)
+    for _ in range(args.warmup):
+        ref.step()
+    iters = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        iters.append(ref.step()["iterations"])
+    el = time.perf_counter() - t0
+    ref.close()
+    value = scene.n_fluid * args.steps / el
+    cores = os.cpu_count() if variant == "omp" else 1
+    sample = (f"100,000-fluid breaking dam (40x50x50 column, 59,684 boundary) of the same scene family, "
+              f"{args.steps} steps after {args.warmup} warm-up steps, mean iterations {np.mean(iters):.2f}")
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded breaking-dam scenes)",
+        "impl": "reference",
+        "config": {"workload": "3D IISPH breaking dam (bounded sample: 100k fluid), hashed-3d, dt 0.005",
+                   "implementation": "libFluid IISPHFluidSolver3D<CubicSplineKernel3D, HashedNeighborhoodSearch3D>, "
+                                     + ("OpenMP over its 16-particle chunks" if variant == "omp" else "as built")},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32-kahan", choices=["fp32", "fp32-kahan", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

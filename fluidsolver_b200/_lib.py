@@ -50,7 +50,7 @@ FS_TYPE_INACTIVE = 2
 EXPORTED_SYMBOLS = (
     "fs_abi_version", "fs_last_error", "fs_params_default", "fs_create", "fs_destroy", "fs_set_params",
     "fs_upload", "fs_download", "fs_find_neighbors", "fs_get_neighbors_csr", "fs_query_position", "fs_solve_step", "fs_step",
-    "fs_run", "fs_last_phase_times", "fs_batch_create", "fs_batch_run",
+    "fs_run", "fs_last_phase_times", "fs_stream", "fs_launch_count", "fs_batch_create", "fs_batch_run",
 )
 
 
@@ -123,6 +123,10 @@ def lib() -> ctypes.CDLL:
     L.fs_solve_step.argtypes = [ctx_p, c_float, POINTER(FsStepStats)]
     L.fs_run.argtypes = [ctx_p, c_int32, c_float, POINTER(FsStepStats)]
     L.fs_last_phase_times.argtypes = [ctx_p, c_void_p]
+    L.fs_stream.argtypes = [ctx_p]
+    L.fs_stream.restype = c_void_p
+    L.fs_launch_count.argtypes = [ctx_p]
+    L.fs_launch_count.restype = c_int64
     L.fs_batch_create.argtypes = [POINTER(FsParams), c_int32, c_void_p, POINTER(ctx_p)]
     L.fs_batch_run.argtypes = [ctx_p, c_int32, c_float, c_void_p]
     for name in ("fs_create", "fs_destroy", "fs_set_params", "fs_upload", "fs_download", "fs_find_neighbors",

@@ -130,6 +130,9 @@ template <typename R> SolverConsts<R> consts_of(fs_ctx* c) {
         k.two_nu = (R)(2.0 * p.viscosity);
         k.two_gamma = (R)(2.0 * p.gamma);
     }
+    k.inv_rho0_sq = R(1) / k.rho0_sq;
+    k.kern.inv_h = R(1) / k.kern.h;
+    k.kern.alpha_h = k.kern.alpha * k.kern.h;
     return k;
 }
 
@@ -149,6 +152,7 @@ WalkParams walk_of(fs_ctx* c, bool for_solver) {
     w.dim = c->dim;
     w.regions = c->reference_order ? 1 : (c->include_inactive && !for_solver ? 3 : 2);
     w.candidates_inactive = c->include_inactive && !for_solver;
+    w.trunc = c->truncate_cells;
     w.d0 = c->dims[0];
     w.d1 = c->dims[1];
     w.d2 = c->dims[2];
@@ -197,6 +201,17 @@ void derive(fs_ctx* c) {
     c->kernel_alpha = kernel_alpha(p.dim, c->kernel_h);
     c->reference_order = (p.flags & FS_FLAG_REFERENCE_ORDER) != 0;
     c->include_inactive = p.search == FS_SEARCH_QUADRATIC_2D || p.search == FS_SEARCH_HASHED_2D;
+    c->truncate_cells = c->reference_order && p.search == FS_SEARCH_HASHED_2D;
+    c->sort_lists_by_host = c->reference_order && (p.search == FS_SEARCH_QUADRATIC_2D || p.search == FS_SEARCH_QUADRATIC_3D);
+}
+
+// graphs bake in buffer pointers, sizes and settings: dropped whenever one changes
+void clear_graphs(fs_ctx* c) {
+    for (auto& g : c->solve_graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
+    c->solve_graphs.clear();
 }
 
 fs_status free_all(fs_ctx* c) {
@@ -209,10 +224,8 @@ fs_status free_all(fs_ctx* c) {
         if (q) cudaFree(q);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->scalars_host) cudaFreeHost(c->scalars_host);
-    if (c->loop_exec) cudaGraphExecDestroy(c->loop_exec);
-    if (c->loop_graph) cudaGraphDestroy(c->loop_graph);
-    if (c->step_exec) cudaGraphExecDestroy(c->step_exec);
-    if (c->step_graph) cudaGraphDestroy(c->step_graph);
+    clear_graphs(c);
+    if (c->body_stream) cudaStreamDestroy(c->body_stream);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -232,6 +245,7 @@ fs_status ensure_staging(fs_ctx* c, size_t bytes) {
 fs_status ensure_lists(fs_ctx* c, int K) {
     const int64_t stride = ((c->cap + 31) / 32) * 32;
     if (c->nbr && c->nbr_capacity >= K && c->nbr_stride == stride) return FS_OK;
+    clear_graphs(c);
     if (c->nbr) cudaFree(c->nbr);
     c->nbr = nullptr;
     FS_TRY(dalloc(&c->nbr, (size_t)K * stride));
@@ -360,6 +374,7 @@ template <typename R> fs_status upload_impl(fs_ctx* c, const fs_particles* in) {
     FS_CUDA(cudaGetLastError());
     c->cur = 0;
     State<R> s = state_of<R>(c);
+    c->launches++;
     k_pack<R><<<grid_for(n), kBlock, 0, c->stream>>>(n, dim, d_pos, d_vel, d_acc, d_ext, d_mass, d_rho, d_p, d_type,
                                                      c->prm.rest_density, s, c->type[0], c->hidx[0]);
     FS_CUDA(cudaGetLastError());
@@ -386,6 +401,7 @@ template <typename R> fs_status download_impl(fs_ctx* c, fs_particles* out) {
     };
     for (auto& f : fields) {
         if (!f.dst) continue;
+    c->launches++;
         k_unpack<R><<<grid_for(n), kBlock, 0, c->stream>>>(n, dim, f.field, s, (float*)c->staging,
                                                            (uint8_t*)c->staging, (uint32_t*)c->staging);
         FS_CUDA(cudaGetLastError());
@@ -402,17 +418,25 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     const int64_t n = c->n;
     cudaStream_t st = c->stream;
     const bool single = c->reference_order;
+    if (n == 0) {
+        c->have_lists = solver_lists;
+        return FS_OK;
+    }
     State<R> s = state_of<R>(c);
     // bbox of the structure's cells -> grid origin
     FS_CUDA(cudaMemsetAsync(c->bbox, 0x7f, 3 * sizeof(int), st));
     FS_CUDA(cudaMemsetAsync(c->bbox + 3, 0x80, 3 * sizeof(int), st));
     const unsigned gb = std::min<unsigned>(grid_for(n, 256), 148u * 8u);
-    k_bbox<R><<<gb, 256, 0, st>>>(n, s.pos, s.type, c->include_inactive, c->search_radius, c->bbox, c->status);
+    c->launches++;
+    k_bbox<R><<<gb, 256, 0, st>>>(n, s.pos, s.type, c->include_inactive, c->search_radius, c->truncate_cells, c->bbox,
+                                  c->status);
+    c->launches++;
     k_origin<<<1, 32, 0, st>>>(c->bbox, c->origin, c->dims[0], c->dims[1], c->dims[2]);
     // keys + sort
     unsigned long long* k64 = single ? c->keys64[0] : nullptr;
+    c->launches++;
     k_keys<R><<<grid_for(n), kBlock, 0, st>>>(n, s.pos, s.type, s.hidx, c->include_inactive, single, c->search_radius,
-                                              c->origin, c->dims[0], c->dims[1], c->dims[2], c->keys[0], k64, c->perm[0]);
+                                              c->truncate_cells, c->origin, c->dims[0], c->dims[1], c->dims[2], c->keys[0], k64, c->perm[0]);
     FS_CUDA(cudaGetLastError());
     size_t temp = c->cub_temp_bytes;
     if (single) {
@@ -424,6 +448,7 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     }
     // gather every persistent field into the other buffer
     const int nx = c->cur ^ 1;
+    c->launches++;
     k_reorder<R><<<grid_for(n), kBlock, 0, st>>>(
         n, c->perm[1], (const V4<R>*)c->pos[c->cur], (V4<R>*)c->pos[nx], (const V4<R>*)c->vel[c->cur],
         (V4<R>*)c->vel[nx], (const V4<R>*)c->acc[c->cur], (V4<R>*)c->acc[nx], (const V4<R>*)c->ext[c->cur],
@@ -434,6 +459,7 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     s = state_of<R>(c);
     // cell ranges
     FS_CUDA(cudaMemsetAsync(c->cell_range, 0, sizeof(uint2) * 3 * c->cell_capacity, st));
+    c->launches++;
     k_cell_ranges<<<grid_for(c->n_struct), kBlock, 0, st>>>(c->n_struct, single ? nullptr : c->keys[1],
                                                             single ? c->keys64[1] : nullptr, c->dims[0], c->dims[1],
                                                             c->cell_capacity, c->cell_range);
@@ -441,10 +467,17 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     if (solver_lists) {
         WalkParams w = walk_of(c, true);
         const uint32_t owners = 1u << FS_TYPE_NORMAL;
+    c->launches++;
         k_build_lists<R><<<grid_for(c->n_owners), kBlock, 0, st>>>(c->n_owners, s.pos, s.type, c->cell_range, c->origin,
                                                                     w, owners, true, c->nbr, c->nbr_stride,
                                                                     c->nbr_capacity, c->nbr_count, c->status, c->scalars);
         FS_CUDA(cudaGetLastError());
+        if (c->sort_lists_by_host) {
+    c->launches++;
+            k_sort_lists_by_host<<<grid_for(c->n_owners), kBlock, 0, st>>>(c->n_owners, c->nbr, c->nbr_stride,
+                                                                           c->nbr_capacity, c->nbr_count, s.hidx);
+            FS_CUDA(cudaGetLastError());
+        }
         c->have_lists = true;
     }
     return FS_OK;
@@ -481,17 +514,81 @@ fs_status read_status(fs_ctx* c, int* st) {
     return FS_OK;
 }
 
-__global__ void k_step_begin(StepScalars* sc, float desired_dt) {
+// Phase timestamp i on stream st. While the stream is being captured the
+// event becomes an event-record node of the graph (recorded when the graph
+// runs), so the phase times stay measurable in graph mode.
+fs_status mark(fs_ctx* c, int i, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    FS_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs == cudaStreamCaptureStatusActive) FS_CUDA(cudaEventRecordWithFlags(c->ev[i], st, cudaEventRecordExternal));
+    else FS_CUDA(cudaEventRecord(c->ev[i], st));
+    return FS_OK;
+}
+
+// resets the per-step scalars; keep_search keeps the statistics of the
+// search that precedes the solver phases
+__global__ void k_step_begin(StepScalars* sc, float desired_dt, bool keep_search) {
     StepScalars z{};
     z.desired_dt = desired_dt;
     z.dt = desired_dt;
+    if (keep_search) z.max_neighbors = sc->max_neighbors;
     *sc = z;
 }
 
 // ---------------------------------------------------------------------------
 // solver steps
 // ---------------------------------------------------------------------------
-template <typename R, bool KAHAN> fs_status step_iisph3d(fs_ctx* c) {
+// The IISPH pressure iterations. Eagerly, the host reads the exit flag after
+// every iteration. While the stream is being captured, the loop becomes a
+// conditional WHILE node: its body is the iteration followed by the
+// convergence test, which ends the loop on the device (and always within
+// max_iterations executions, see k_iisph_check).
+template <typename Body>
+fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_test, Body&& body) {
+    const int max_it = c->prm.max_iterations;
+    if (max_it <= 0) return FS_OK;
+    cudaStream_t st = c->stream;
+    if (!capture) {
+        for (int it = 0; it < max_it; it++) {
+            body(st);
+            c->launches++;
+            k_iisph_check<<<1, 1, 0, st>>>(c->scalars, c->prm.min_iterations, max_it, c->prm.max_density_error,
+                                           fp64_test, two_d, c->status, 0, false);
+            FS_CUDA(cudaGetLastError());
+            FS_TRY(read_scalars(c));
+            if (c->scalars_host->done) break;
+        }
+        return FS_OK;
+    }
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraph_t graph;
+    FS_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps));
+    cudaGraphConditionalHandle handle;
+    FS_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    FS_CUDA(cudaGraphAddNode(&node, graph, deps, ndeps, &cp));
+    cudaGraph_t body_graph = cp.conditional.phGraph_out[0];
+    FS_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    FS_CUDA(cudaStreamBeginCaptureToGraph(c->body_stream, body_graph, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed));
+    body(c->body_stream);
+    c->launches++;
+    k_iisph_check<<<1, 1, 0, c->body_stream>>>(c->scalars, c->prm.min_iterations, max_it, c->prm.max_density_error,
+                                                fp64_test, two_d, c->status, handle, true);
+    cudaError_t e = cudaGetLastError();
+    cudaError_t e2 = cudaStreamEndCapture(c->body_stream, nullptr);
+    if (e != cudaSuccess || e2 != cudaSuccess) return fail(FS_ERR_CUDA, "capture of the pressure loop failed");
+    return FS_OK;
+}
+
+template <typename R, bool KAHAN> fs_status step_iisph3d(fs_ctx* c, bool capture) {
     cudaStream_t st = c->stream;
     const int64_t n = c->n, no = c->n_owners;
     const SolverConsts<R> k = consts_of<R>(c);
@@ -501,36 +598,40 @@ template <typename R, bool KAHAN> fs_status step_iisph3d(fs_ctx* c) {
     // density double buffer: the current density becomes rho_prev
     std::swap(c->rho[c->cur], c->rho_prev);
     State<R> s = state_of<R>(c);
-    cudaEventRecord(c->ev[1], st);
+    FS_TRY(mark(c, 1, st));
     if (split) {
+    c->launches++;
         k_iisph3d_density<R, KAHAN><<<grid_for(n), kBlock, 0, st>>>(n, s, L, k, c->status);
+    c->launches++;
         k_iisph3d_l1<R, KAHAN, true><<<grid_for(n), kBlock, 0, st>>>(n, s, L, k, c->scalars, c->status);
     } else {
+    c->launches++;
         k_iisph3d_l1<R, KAHAN, false><<<grid_for(n), kBlock, 0, st>>>(n, s, L, k, c->scalars, c->status);
     }
     FS_CUDA(cudaGetLastError());
-    cudaEventRecord(c->ev[2], st);
-    if (fp32) k_iisph3d_l2<R, KAHAN, true><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
-    else k_iisph3d_l2<R, KAHAN, false><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
-    FS_CUDA(cudaGetLastError());
-    cudaEventRecord(c->ev[3], st);
-    const int max_it = c->prm.max_iterations;
-    const bool fp64_test = !fp32;
-    for (int it = 0; it < max_it; it++) {
-        k_iisph3d_pressure_acc<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
-        k_iisph3d_pressure_update<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
-        k_iisph_check<<<1, 1, 0, st>>>(c->scalars, c->prm.min_iterations, max_it, c->prm.max_density_error, fp64_test,
-                                       false, c->status);
-        FS_CUDA(cudaGetLastError());
-        FS_TRY(read_scalars(c));
-        if (c->scalars_host->done) break;
+    FS_TRY(mark(c, 2, st));
+    if (fp32) {
+    c->launches++;
+        k_iisph3d_l2<R, KAHAN, true><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
+    } else {
+    c->launches++;
+        k_iisph3d_l2<R, KAHAN, false><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
     }
-    cudaEventRecord(c->ev[4], st);
+    FS_CUDA(cudaGetLastError());
+    FS_TRY(mark(c, 3, st));
+    FS_TRY(enqueue_pressure_loop(c, capture, false, !fp32, [&](cudaStream_t bs) {
+        c->launches += 2;
+        k_iisph3d_pressure_acc<R, KAHAN><<<grid_for(no), kBlock, 0, bs>>>(no, s, L, k, c->scalars, c->status);
+        k_iisph3d_pressure_update<R, KAHAN><<<grid_for(no), kBlock, 0, bs>>>(no, s, L, k, c->scalars, c->status);
+    }));
+    FS_TRY(mark(c, 4, st));
+    c->launches++;
     k_cfl<<<1, 1, 0, st>>>(c->scalars, c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
                            c->status);
+    c->launches++;
     k_iisph3d_integrate<R><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
     FS_CUDA(cudaGetLastError());
-    cudaEventRecord(c->ev[5], st);
+    FS_TRY(mark(c, 5, st));
     return FS_OK;
 }
 
@@ -540,25 +641,31 @@ template <typename R, bool KAHAN> fs_status step_sesph(fs_ctx* c) {
     const SolverConsts<R> k = consts_of<R>(c);
     const Lists L = lists_of(c);
     State<R> s = state_of<R>(c);
-    cudaEventRecord(c->ev[1], st);
+    FS_TRY(mark(c, 1, st));
+    c->launches++;
     k_sesph_density<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->status);
-    cudaEventRecord(c->ev[2], st);
+    FS_TRY(mark(c, 2, st));
+    c->launches++;
     k_sesph_accel<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->status);
-    cudaEventRecord(c->ev[3], st);
+    FS_TRY(mark(c, 3, st));
     if (c->dim == 3) {
+    c->launches++;
         k_sesph_maxima<R><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
+    c->launches++;
         k_sesph_maxima_final<<<1, 1, 0, st>>>(c->scalars);
+    c->launches++;
         k_cfl<<<1, 1, 0, st>>>(c->scalars, c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
                                c->status);
     }
-    cudaEventRecord(c->ev[4], st);
+    FS_TRY(mark(c, 4, st));
+    c->launches++;
     k_sesph_integrate<R><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
     FS_CUDA(cudaGetLastError());
-    cudaEventRecord(c->ev[5], st);
+    FS_TRY(mark(c, 5, st));
     return FS_OK;
 }
 
-template <typename R, bool KAHAN> fs_status step_iisph2d(fs_ctx* c) {
+template <typename R, bool KAHAN> fs_status step_iisph2d(fs_ctx* c, bool capture) {
     cudaStream_t st = c->stream;
     const int64_t n = c->n, no = c->n_owners;
     const SolverConsts<R> k = consts_of<R>(c);
@@ -566,43 +673,48 @@ template <typename R, bool KAHAN> fs_status step_iisph2d(fs_ctx* c) {
     const bool split = c->reference_order;
     std::swap(c->rho[c->cur], c->rho_prev);
     State<R> s = state_of<R>(c);
-    cudaEventRecord(c->ev[1], st);
+    FS_TRY(mark(c, 1, st));
     if (split) {
+    c->launches++;
         k_iisph2d_density<R, KAHAN><<<grid_for(n), kBlock, 0, st>>>(n, s, L, k, c->status);
+    c->launches++;
         k_iisph2d_l1<R, KAHAN, true><<<grid_for(n), kBlock, 0, st>>>(n, s, L, k, c->scalars, c->status);
     } else {
+    c->launches++;
         k_iisph2d_l1<R, KAHAN, false><<<grid_for(n), kBlock, 0, st>>>(n, s, L, k, c->scalars, c->status);
     }
-    cudaEventRecord(c->ev[2], st);
+    FS_TRY(mark(c, 2, st));
+    c->launches++;
     k_iisph2d_l2<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
     FS_CUDA(cudaGetLastError());
-    cudaEventRecord(c->ev[3], st);
-    const int max_it = c->prm.max_iterations;
-    const bool fp64_test = c->precision != FS_PRECISION_FP32;
-    for (int it = 0; it < max_it; it++) {
-        k_iisph2d_pressure_acc<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
-        k_iisph2d_pressure_update<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
-        k_iisph_check<<<1, 1, 0, st>>>(c->scalars, c->prm.min_iterations, max_it, c->prm.max_density_error, fp64_test,
-                                       true, c->status);
-        FS_CUDA(cudaGetLastError());
-        FS_TRY(read_scalars(c));
-        if (c->scalars_host->done) break;
-    }
-    cudaEventRecord(c->ev[4], st);
+    FS_TRY(mark(c, 3, st));
+    FS_TRY(enqueue_pressure_loop(c, capture, true, c->precision != FS_PRECISION_FP32, [&](cudaStream_t bs) {
+        c->launches += 2;
+        k_iisph2d_pressure_acc<R, KAHAN><<<grid_for(no), kBlock, 0, bs>>>(no, s, L, k, c->scalars, c->status);
+        k_iisph2d_pressure_update<R, KAHAN><<<grid_for(no), kBlock, 0, bs>>>(no, s, L, k, c->scalars, c->status);
+    }));
+    FS_TRY(mark(c, 4, st));
+    c->launches++;
     k_iisph2d_integrate<R><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
     FS_CUDA(cudaGetLastError());
-    cudaEventRecord(c->ev[5], st);
+    FS_TRY(mark(c, 5, st));
     return FS_OK;
 }
 
-template <typename R, bool KAHAN> fs_status step_dispatch(fs_ctx* c) {
+template <typename R, bool KAHAN> fs_status step_dispatch(fs_ctx* c, bool capture) {
     switch (c->prm.solver) {
-        case FS_SOLVER_IISPH_3D: return step_iisph3d<R, KAHAN>(c);
+        case FS_SOLVER_IISPH_3D: return step_iisph3d<R, KAHAN>(c, capture);
         case FS_SOLVER_SESPH_2D:
         case FS_SOLVER_SESPH_3D: return step_sesph<R, KAHAN>(c);
-        case FS_SOLVER_IISPH_2D: return step_iisph2d<R, KAHAN>(c);
+        case FS_SOLVER_IISPH_2D: return step_iisph2d<R, KAHAN>(c, capture);
         default: return fail(FS_ERR_INVALID, "context has no solver");
     }
+}
+
+fs_status step_dispatch_any(fs_ctx* c, bool capture) {
+    if (c->precision == FS_PRECISION_FP64) return step_dispatch<double, false>(c, capture);
+    if (c->precision == FS_PRECISION_FP32) return step_dispatch<float, false>(c, capture);
+    return step_dispatch<float, true>(c, capture);
 }
 
 fs_status search_dispatch(fs_ctx* c, bool solver_lists) {
@@ -632,7 +744,8 @@ fs_status fill_stats(fs_ctx* c, fs_step_stats* stats, int st) {
 // capacity the lists are grown and the search is repeated once.
 fs_status search_for_step(fs_ctx* c, float dt) {
     for (int attempt = 0; attempt < 2; attempt++) {
-        k_step_begin<<<1, 1, 0, c->stream>>>(c->scalars, dt);
+        c->launches++;
+        k_step_begin<<<1, 1, 0, c->stream>>>(c->scalars, dt, false);
         FS_CUDA(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
         cudaEventRecord(c->ev[0], c->stream);
         FS_TRY(search_dispatch(c, c->prm.solver != FS_SOLVER_NONE));
@@ -653,15 +766,75 @@ fs_status search_for_step(fs_ctx* c, float dt) {
     return fail(FS_ERR_CAPACITY, "neighbor list capacity exceeded");
 }
 
+// Solver phases as one CUDA graph (the IISPH loop a conditional node in it),
+// captured once per buffer assignment and reused. Capturing runs the same
+// host code as the eager path, which also rotates the host-side buffer
+// pointers; a replay applies the rotation recorded at capture time.
+fs_status solve_graph(fs_ctx* c, float dt) {
+    fs_ctx::SolveGraph key;
+    key.cur = c->cur;
+    key.rho0 = c->rho[0];
+    key.rho1 = c->rho[1];
+    key.rho_prev = c->rho_prev;
+    key.K = c->nbr_capacity;
+    key.n = c->n;
+    key.n_owners = c->n_owners;
+    key.dt = dt;
+    for (auto& g : c->solve_graphs) {
+        if (g.same_key(key)) {
+            const int64_t per_launch = g.launches;
+            FS_CUDA(cudaGraphLaunch(g.exec, c->stream));
+            c->launches += per_launch;
+            c->cur = g.post_cur;
+            c->rho[0] = g.post_rho0;
+            c->rho[1] = g.post_rho1;
+            c->rho_prev = g.post_rho_prev;
+            return FS_OK;
+        }
+    }
+    const int64_t launches0 = c->launches;
+    FS_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    c->launches++;
+    k_step_begin<<<1, 1, 0, c->stream>>>(c->scalars, dt, true);
+    fs_status r = step_dispatch_any(c, true);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (r != FS_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        c->cur = key.cur;
+        c->rho[0] = key.rho0;
+        c->rho[1] = key.rho1;
+        c->rho_prev = key.rho_prev;
+        return r != FS_OK ? r : fail(FS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    }
+    fs_ctx::SolveGraph g = key;
+    g.graph = graph;
+    e = cudaGraphInstantiate(&g.exec, graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return fail(FS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    g.launches = c->launches - launches0;
+    g.post_cur = c->cur;
+    g.post_rho0 = c->rho[0];
+    g.post_rho1 = c->rho[1];
+    g.post_rho_prev = c->rho_prev;
+    c->solve_graphs.push_back(g);
+    FS_CUDA(cudaGraphLaunch(g.exec, c->stream));
+    return FS_OK;
+}
+
 // solver phases of a step on the lists of the last search
 fs_status solve_after_search(fs_ctx* c, float dt, fs_step_stats* stats) {
     if (!c->have_lists) return fail(FS_ERR_STATE, "execute the neighborhood search first");
-    k_step_begin<<<1, 1, 0, c->stream>>>(c->scalars, dt);
-    fs_status r;
-    if (c->precision == FS_PRECISION_FP64) r = step_dispatch<double, false>(c);
-    else if (c->precision == FS_PRECISION_FP32) r = step_dispatch<float, false>(c);
-    else r = step_dispatch<float, true>(c);
-    if (r != FS_OK) return r;
+    const bool graphs = !(c->prm.flags & FS_FLAG_SYNC_EACH_ITERATION);
+    if (graphs) {
+        FS_TRY(solve_graph(c, dt));
+    } else {
+        c->launches++;
+        k_step_begin<<<1, 1, 0, c->stream>>>(c->scalars, dt, true);
+        FS_TRY(step_dispatch_any(c, false));
+    }
     c->have_lists = false;  // positions moved: the lists belong to the old positions
     FS_TRY(read_scalars(c));
     int st = 0;
@@ -745,7 +918,8 @@ fs_status fs_create(const fs_params* p, fs_ctx** out) {
         fs_status s_ = dalloc(&(ptr), (count));   \
         if (s_ != FS_OK) return bail(s_);         \
     } while (0)
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(FS_ERR_CUDA, "cudaStreamCreate failed"));
     const size_t cap = (size_t)c->cap;
     const size_t v4 = c->real_size * 4, r1 = c->real_size;
@@ -814,6 +988,10 @@ fs_status fs_set_params(fs_ctx* c, const fs_params* p) {
     if (p->dim != c->prm.dim || p->solver != c->prm.solver || p->search != c->prm.search ||
         p->precision != c->prm.precision || p->flags != c->prm.flags || p->max_particles != c->prm.max_particles)
         return fail(FS_ERR_INVALID, "layout-defining parameters cannot change; create a new context");
+    if (std::memcmp(&c->prm, p, sizeof(fs_params)) == 0) return FS_OK;
+    FS_CUDA(cudaSetDevice(c->device));
+    FS_CUDA(cudaStreamSynchronize(c->stream));
+    clear_graphs(c);
     c->prm = *p;
     derive(c);
     return FS_OK;
@@ -823,7 +1001,9 @@ fs_status fs_upload(fs_ctx* c, const fs_particles* in) {
     if (!c || !in) return fail(FS_ERR_INVALID, "null argument");
     if (in->n < 0 || in->n > c->cap) return fail(FS_ERR_INVALID, "particle count exceeds the context capacity");
     FS_CUDA(cudaSetDevice(c->device));
+    const int64_t n_before = c->n, owners_before = c->n_owners;
     FS_TRY(layout_from_types(c, in->type, in->n));
+    if (c->n != n_before || c->n_owners != owners_before) clear_graphs(c);
     choose_dims(c, in->position, in->type, in->n);
     FS_TRY(ensure_cells(c));
     fs_status r = c->precision == FS_PRECISION_FP64 ? upload_impl<double>(c, in) : upload_impl<float>(c, in);
@@ -868,6 +1048,11 @@ fs_status fs_get_neighbors_csr(fs_ctx* c, int64_t* offsets, int64_t* indices, in
     const int64_t n = c->n;
     const int64_t ns = c->n_struct;
     cudaStream_t st = c->stream;
+    if (n == 0) {
+        offsets[0] = 0;
+        if (total) *total = 0;
+        return FS_OK;
+    }
     if (c->csr_capacity < n + 1) {
         if (c->csr_offsets) cudaFree(c->csr_offsets);
         if (c->csr_counts) cudaFree(c->csr_counts);
@@ -882,10 +1067,12 @@ fs_status fs_get_neighbors_csr(fs_ctx* c, int64_t* offsets, int64_t* indices, in
     FS_CUDA(cudaMemsetAsync(c->csr_counts, 0, sizeof(uint32_t) * (n + 1), st));
     if (c->precision == FS_PRECISION_FP64) {
         State<double> s = state_of<double>(c);
+    c->launches++;
         k_csr_count<double><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_range, c->origin, w, mask,
                                                              c->csr_counts);
     } else {
         State<float> s = state_of<float>(c);
+    c->launches++;
         k_csr_count<float><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_range, c->origin, w, mask,
                                                             c->csr_counts);
     }
@@ -919,10 +1106,12 @@ fs_status fs_get_neighbors_csr(fs_ctx* c, int64_t* offsets, int64_t* indices, in
     FS_TRY(dalloc(&d_idx, (size_t)std::max<int64_t>(tot, 1)));
     if (c->precision == FS_PRECISION_FP64) {
         State<double> s = state_of<double>(c);
+    c->launches++;
         k_csr_fill<double><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_range, c->origin, w, mask,
                                                             c->csr_offsets, d_idx);
     } else {
         State<float> s = state_of<float>(c);
+    c->launches++;
         k_csr_fill<float><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_range, c->origin, w, mask,
                                                            c->csr_offsets, d_idx);
     }
@@ -961,10 +1150,12 @@ fs_status fs_query_position(fs_ctx* c, const float* position, int64_t* out, int6
     const float z = c->dim == 3 ? position[2] : 0.0f;
     if (c->precision == FS_PRECISION_FP64) {
         State<double> s = state_of<double>(c);
+    c->launches++;
         k_query_position<double><<<1, 32, 0, c->stream>>>(v3<double>(position[0], position[1], z), s.pos, s.type,
                                                           c->cell_range, c->origin, w, d_out, room, d_cnt);
     } else {
         State<float> s = state_of<float>(c);
+    c->launches++;
         k_query_position<float><<<1, 32, 0, c->stream>>>(v3<float>(position[0], position[1], z), s.pos, s.type,
                                                          c->cell_range, c->origin, w, d_out, room, d_cnt);
     }
@@ -1003,6 +1194,10 @@ fs_status fs_last_phase_times(fs_ctx* c, float* ms5) {
     for (int i = 0; i < 5; i++) ms5[i] = c->phase_ms[i];
     return FS_OK;
 }
+
+void* fs_stream(fs_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int64_t fs_launch_count(fs_ctx* c) { return c ? c->launches : 0; }
 
 fs_status fs_batch_create(const fs_params*, int32_t, const int64_t*, fs_ctx** out) {
     if (out) *out = nullptr;

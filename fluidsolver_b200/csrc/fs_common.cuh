@@ -88,7 +88,51 @@ template <typename R> struct SplineKernel {
     }
 
     static __device__ __forceinline__ R sqrt_(R x);
+
+    // ---- fast evaluation (compensated-sum mode): one rsqrt, no divisions,
+    // fused multiply-adds. The same piecewise cubic; rounding differs from the
+    // reference's by a few ulp per pair.
+    R inv_h;     // 1 / h
+    R alpha_h;   // alpha * h
+
+    __device__ __forceinline__ R Wf(V3<R> d) const {
+        const R r2 = fma_(d.z, d.z, fma_(d.y, d.y, d.x * d.x));
+        const R q = sqrt_fast(r2) * inv_h;
+        const R a = R(2) - q, b = R(1) - q;
+        if (q < R(1)) return alpha * fma_(R(-4) * b * b, b, a * a * a);
+        if (q < R(2)) return alpha * (a * a * a);
+        return R(0);
+    }
+    __device__ __forceinline__ V3<R> gradWf(V3<R> d) const {
+        const R r2 = fma_(d.z, d.z, fma_(d.y, d.y, d.x * d.x));
+        if (!(r2 > R(kFltEps) * R(kFltEps))) return v3<R>(0, 0, 0);
+        const R inv = rsqrt_fast(r2);
+        const R q = r2 * inv * inv_h;
+        const R a = R(2) - q, b = R(1) - q;
+        R poly;
+        if (q < R(1)) poly = fma_(R(12) * b, b, R(-3) * a * a);
+        else if (q < R(2)) poly = R(-3) * a * a;
+        else return v3<R>(0, 0, 0);
+        const R f = alpha_h * poly * inv;
+        return v3<R>(f * d.x, f * d.y, f * d.z);
+    }
+    template <bool FAST> __device__ __forceinline__ R w(V3<R> d) const { return FAST ? Wf(d) : W(d); }
+    template <bool FAST> __device__ __forceinline__ V3<R> grad(V3<R> d) const { return FAST ? gradWf(d) : gradW(d); }
+
+    static __device__ __forceinline__ R fma_(R a, R b, R c);
+    static __device__ __forceinline__ R rsqrt_fast(R x);
+    static __device__ __forceinline__ R sqrt_fast(R x);
 };
+template <> __device__ __forceinline__ float SplineKernel<float>::fma_(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+template <> __device__ __forceinline__ double SplineKernel<double>::fma_(double a, double b, double c) { return __fma_rn(a, b, c); }
+template <> __device__ __forceinline__ float SplineKernel<float>::rsqrt_fast(float x) { return rsqrtf(x); }
+template <> __device__ __forceinline__ double SplineKernel<double>::rsqrt_fast(double x) { return rsqrt(x); }
+template <> __device__ __forceinline__ float SplineKernel<float>::sqrt_fast(float x) { return x > 0.f ? x * rsqrtf(x) : 0.f; }
+template <> __device__ __forceinline__ double SplineKernel<double>::sqrt_fast(double x) { return sqrt(x); }
+
+// division: exact (reference order) or reciprocal-based (fast mode)
+template <bool FAST> __device__ __forceinline__ float fdiv(float a, float b) { return FAST ? __fdividef(a, b) : a / b; }
+template <bool FAST> __device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
 template <> __device__ __forceinline__ float SplineKernel<float>::sqrt_(float x) { return __fsqrt_rn(x); }
 template <> __device__ __forceinline__ double SplineKernel<double>::sqrt_(double x) { return __dsqrt_rn(x); }
 
@@ -147,7 +191,7 @@ struct StepScalars {
     float final_max_a2;      // of the last iteration (CFL input)
     float final_max_v2;
     int max_neighbors;
-    int pad_;
+    int loop_guard;          // executions of the pressure-loop body this step
 };
 
 }  // namespace fsb

@@ -38,6 +38,8 @@ struct fs_ctx {
     float searched_dt = 0.f;
     bool reference_order = false;
     bool include_inactive = false;  // contract lists inactive particles (2D quadratic / hashed)
+    bool truncate_cells = false;    // hashed-2D cells (reference-order mode)
+    bool sort_lists_by_host = false;  // quadratic list order (reference-order mode)
     int ns_owner_mode = 0;          // 0 all in structure, 1 fluid only, 2 active only
     int precision = FS_PRECISION_FP32_KAHAN;
     size_t real_size = 4;
@@ -79,6 +81,7 @@ struct fs_ctx {
     int nbr_capacity = 0;          // K
     int64_t nbr_stride = 0;
     int64_t n_owners = 0;          // owners of the solver lists: [0, n_owners)
+    int64_t launches = 0;          // this library's kernel launches
 
     // CSR export of the last search (sorted space)
     int64_t* csr_offsets = nullptr;
@@ -96,14 +99,26 @@ struct fs_ctx {
     fsb::StepScalars* scalars = nullptr;    // device
     fsb::StepScalars* scalars_host = nullptr;  // pinned mirror
 
-    // CUDA graph of the IISPH pressure loop (conditional while node)
-    cudaGraphExec_t loop_exec = nullptr;
-    cudaGraph_t loop_graph = nullptr;
-    cudaGraphConditionalHandle loop_handle = 0;
-    bool loop_graph_ready = false;
-    cudaGraphExec_t step_exec = nullptr;
-    cudaGraph_t step_graph = nullptr;
-    float step_graph_dt = -1.f;
+    // CUDA graphs of the solver phases (the IISPH loop is a conditional WHILE
+    // node inside), one per buffer assignment they were captured with
+    struct SolveGraph {
+        int cur = 0;
+        void *rho0 = nullptr, *rho1 = nullptr, *rho_prev = nullptr;
+        int K = 0;
+        int64_t n = 0, n_owners = 0;
+        float dt = 0.f;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        int64_t launches = 0;
+        int post_cur = 0;
+        void *post_rho0 = nullptr, *post_rho1 = nullptr, *post_rho_prev = nullptr;
+        bool same_key(const SolveGraph& o) const {
+            return cur == o.cur && rho0 == o.rho0 && rho1 == o.rho1 && rho_prev == o.rho_prev && K == o.K &&
+                   n == o.n && n_owners == o.n_owners && dt == o.dt;
+        }
+    };
+    std::vector<SolveGraph> solve_graphs;
+    cudaStream_t body_stream = nullptr;  // captures conditional-node bodies
 
     cudaEvent_t ev[6] = {};
     float phase_ms[5] = {};

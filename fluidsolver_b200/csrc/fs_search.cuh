@@ -49,9 +49,11 @@ struct GridInfo {
     float radius;  // cell edge
 };
 
-// cell coordinate of a position: (int)floor(x / r)
-template <typename R> __device__ __forceinline__ int cell_coord(R x, float r) {
-    return (int)floor((float)x / r);
+// cell coordinate of a position: (int)floor(x / r), or the truncation toward
+// zero of HashedNeighborhoodSearch (2D) (HashedNeighborhoodSearch.cpp:108-115)
+// when its list order is reproduced
+template <typename R> __device__ __forceinline__ int cell_coord(R x, float r, bool trunc) {
+    return trunc ? (int)((float)x / r) : (int)floor((float)x / r);
 }
 
 // ---------------------------------------------------------------------------
@@ -59,12 +61,12 @@ template <typename R> __device__ __forceinline__ int cell_coord(R x, float r) {
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void k_bbox(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type, bool include_inactive,
-                       float r, int* __restrict__ bbox, const int* __restrict__ status) {
+                       float r, bool trunc, int* __restrict__ bbox, const int* __restrict__ status) {
     int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         if (!include_inactive && type[k] == FS_TYPE_INACTIVE) continue;
         V4<R> p = pos[k];
-        int c0 = cell_coord<R>(p.x, r), c1 = cell_coord<R>(p.y, r), c2 = cell_coord<R>(p.z, r);
+        int c0 = cell_coord<R>(p.x, r, trunc), c1 = cell_coord<R>(p.y, r, trunc), c2 = cell_coord<R>(p.z, r, trunc);
         mn[0] = min(mn[0], c0); mn[1] = min(mn[1], c1); mn[2] = min(mn[2], c2);
         mx[0] = max(mx[0], c0); mx[1] = max(mx[1], c1); mx[2] = max(mx[2], c2);
     }
@@ -115,7 +117,7 @@ __device__ __forceinline__ uint32_t region_of(uint8_t t, bool single_region) {
 template <typename R>
 __global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
                        const uint32_t* __restrict__ hidx, bool include_inactive, bool single_region, float r,
-                       const int* __restrict__ origin, int d0, int d1, int d2, uint32_t* __restrict__ keys,
+                       bool trunc, const int* __restrict__ origin, int d0, int d1, int d2, uint32_t* __restrict__ keys,
                        unsigned long long* __restrict__ keys64, uint32_t* __restrict__ perm) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -126,9 +128,9 @@ __global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* 
     } else {
         V4<R> p = pos[k];
         bool cl = false;
-        int lx = local_cell(cell_coord<R>(p.x, r), origin[0], d0, cl);
-        int ly = local_cell(cell_coord<R>(p.y, r), origin[1], d1, cl);
-        int lz = local_cell(cell_coord<R>(p.z, r), origin[2], d2, cl);
+        int lx = local_cell(cell_coord<R>(p.x, r, trunc), origin[0], d0, cl);
+        int ly = local_cell(cell_coord<R>(p.y, r, trunc), origin[1], d1, cl);
+        int lz = local_cell(cell_coord<R>(p.z, r, trunc), origin[2], d2, cl);
         uint32_t m = morton_spread10(lx) | (morton_spread10(ly) << 1) | (morton_spread10(lz) << 2);
         key = (region_of(t, single_region) << 30) | m;
     }
@@ -185,6 +187,7 @@ struct WalkParams {
     int dim;        // 2 or 3
     int regions;    // number of regions to visit (1 in single-region mode)
     bool candidates_inactive;  // contract lists inactive neighbors
+    bool trunc;                // cells by truncation toward zero (hashed 2D order)
     int d0, d1, d2;
     int64_t cell_cap;
 };
@@ -206,7 +209,7 @@ template <typename R, typename F>
 __device__ __forceinline__ void walk_neighbors(V3<R> xi, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
                                                const uint2* __restrict__ cell_range, const int* __restrict__ origin,
                                                const WalkParams& w, F&& f) {
-    const int ci[3] = {cell_coord<R>(xi.x, w.r), cell_coord<R>(xi.y, w.r), cell_coord<R>(xi.z, w.r)};
+    const int ci[3] = {cell_coord<R>(xi.x, w.r, w.trunc), cell_coord<R>(xi.y, w.r, w.trunc), cell_coord<R>(xi.z, w.r, w.trunc)};
     const int zr = w.dim == 2 ? 0 : 1;
     const int o0 = origin[0], o1 = origin[1], o2 = origin[2];
     for (int dx = -1; dx <= 1; dx++) {
@@ -223,8 +226,8 @@ __device__ __forceinline__ void walk_neighbors(V3<R> xi, const V4<R>* __restrict
                     for (uint32_t j = rg.x; j < rg.y; j++) {
                         const V4<R> pj = pos[j];
                         if (cl) {
-                            if (cell_coord<R>(pj.x, w.r) != c0 || cell_coord<R>(pj.y, w.r) != c1 ||
-                                cell_coord<R>(pj.z, w.r) != c2)
+                            if (cell_coord<R>(pj.x, w.r, w.trunc) != c0 || cell_coord<R>(pj.y, w.r, w.trunc) != c1 ||
+                                cell_coord<R>(pj.z, w.r, w.trunc) != c2)
                                 continue;
                         }
                         const uint8_t tj = type[j];
@@ -261,6 +264,28 @@ __global__ void k_build_lists(int64_t n_owners, const V4<R>* __restrict__ pos, c
     count[k] = c;
     if ((int)c > K) raise_status(status, FS_ERR_CAPACITY);
     atomicMax(&sc->max_neighbors, (int)c);
+}
+
+// Quadratic searches list neighbors by ascending index
+// (QuadraticNeighborhoodSearch3D.cpp:52-66); with the reference's summation
+// order requested, each solver list is sorted by host index.
+__global__ void k_sort_lists_by_host(int64_t n_owners, uint32_t* __restrict__ nbr, int64_t stride, int K,
+                                     const uint32_t* __restrict__ count, const uint32_t* __restrict__ hidx) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n_owners) return;
+    const int c = min((int)count[k], K);
+    for (int a = 1; a < c; a++) {
+        const uint32_t e = nbr[(int64_t)a * stride + k];
+        const uint32_t h = hidx[e & kIndexMask];
+        int b = a - 1;
+        while (b >= 0) {
+            const uint32_t f = nbr[(int64_t)b * stride + k];
+            if (hidx[f & kIndexMask] <= h) break;
+            nbr[(int64_t)(b + 1) * stride + k] = f;
+            b--;
+        }
+        nbr[(int64_t)(b + 1) * stride + k] = e;
+    }
 }
 
 // CSR export: counts (pass 1) and fill (pass 2) in sorted index space

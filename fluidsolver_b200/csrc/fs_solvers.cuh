@@ -14,6 +14,7 @@ template <typename R> struct SolverConsts {
     SplineKernel<R> kern;
     R rest_density;
     R rho0_sq;        // Math::pow2(rest_density)
+    R inv_rho0_sq;    // 1 / rho0^2 (fast mode)
     R gravity;
     R visc_eps;       // (0.01f * particle_size) * particle_size
     R two_nu;         // 2.0f * viscosity
@@ -94,8 +95,9 @@ __device__ __forceinline__ V3<R> viscosity(int64_t k, const State<R>& s, const L
         const V4<R> vj = s.vel[j];
         const V3<R> vij = vi - xyz<R>(vj);
         const V3<R> xij = xi - xyz<R>(pj);
-        const R f = (pj.w / rj) * (dot(vij, xij) / (dot(xij, xij) + c.visc_eps));
-        tmp.add(f * c.kern.gradW(xij));
+        const R f = KAHAN ? fdiv<true>(pj.w * dot(vij, xij), rj * (dot(xij, xij) + c.visc_eps))
+                          : (pj.w / rj) * (dot(vij, xij) / (dot(xij, xij) + c.visc_eps));
+        tmp.add(f * c.kern.template grad<KAHAN>(xij));
     }
     return c.two_nu * tmp.get();
 }
@@ -156,7 +158,7 @@ __global__ void k_iisph3d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
             const V4<R> pj = s.pos[e & kIndexMask];
             R m = pj.w;
             if (c.single_layer && (e & kBoundaryBit)) m = m * c.gamma1;
-            rho.add(m * c.kern.W(xyz<R>(pk) - xyz<R>(pj)));
+            rho.add(m * c.kern.template w<KAHAN>(xyz<R>(pk) - xyz<R>(pj)));
         }
         s.rho[k] = rho.get();
     }
@@ -180,7 +182,7 @@ __global__ void k_iisph3d_density(int64_t n, State<R> s, Lists L, SolverConsts<R
         const V4<R> pj = s.pos[e & kIndexMask];
         R m = pj.w;
         if (c.single_layer && (e & kBoundaryBit)) m = m * c.gamma1;
-        rho.add(m * c.kern.W(xk - xyz<R>(pj)));
+        rho.add(m * c.kern.template w<KAHAN>(xk - xyz<R>(pj)));
     }
     s.rho[k] = rho.get();
 }
@@ -216,16 +218,16 @@ __global__ void k_iisph3d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
         const uint32_t e = L.at(k, q);
         const uint32_t j = e & kIndexMask;
         const V4<R> pj = s.pos[j];
-        const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+        const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
         if (!(e & kBoundaryBit)) {
             const V3<R> vsj = xyz<R>(s.vstar[j]);
             contrib.add(pj.w * dot(vsk - vsj, g));
-            inner.sub((pj.w / c.rho0_sq) * g);
+            inner.sub((KAHAN ? pj.w * c.inv_rho0_sq : pj.w / c.rho0_sq) * g);
             if (!TWO_PASS) mg2.add(pj.w * dot(g, g));
         } else {
             contrib.add(pj.w * dot(vsk, g));
-            if (c.single_layer) inner.sub(((c.two_gamma * pj.w) / c.rho0_sq) * g);
-            else inner.sub(((R(2) * pj.w) / c.rho0_sq) * g);
+            const R w = c.single_layer ? c.two_gamma * pj.w : R(2) * pj.w;
+            inner.sub((KAHAN ? w * c.inv_rho0_sq : w / c.rho0_sq) * g);
         }
         if (!TWO_PASS) mg.add(pj.w * g);
     }
@@ -239,7 +241,7 @@ __global__ void k_iisph3d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
             const uint32_t e = L.at(k, q);
             const uint32_t j = e & kIndexMask;
             const V4<R> pj = s.pos[j];
-            const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+            const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
             d.add(pj.w * dot(in, g));
             // gradW(x_j - x_i) == -gradW(x_i - x_j) bit for bit
             if (!(e & kBoundaryBit)) d.add(pj.w * dot(mi * (-g), g));
@@ -271,8 +273,12 @@ __global__ void k_iisph3d_pressure_acc(int64_t n, State<R> s, Lists L, SolverCon
         const uint32_t e = L.at(k, q);
         const uint32_t j = e & kIndexMask;
         const V4<R> pj = s.pos[j];
-        const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
-        if (!(e & kBoundaryBit)) {
+        const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
+        if (KAHAN) {
+            const R f = !(e & kBoundaryBit) ? pj.w * (pk + s.p[j])
+                                            : (c.single_layer ? c.two_gamma : R(2)) * pj.w * pk;
+            pa.sub((f * c.inv_rho0_sq) * g);
+        } else if (!(e & kBoundaryBit)) {
             pa.sub((pj.w * (pk / c.rho0_sq + s.p[j] / c.rho0_sq)) * g);
         } else if (c.single_layer) {
             pa.sub(((((c.gamma * pj.w) * R(2)) * pk) / c.rho0_sq) * g);
@@ -306,7 +312,7 @@ __global__ void k_iisph3d_pressure_update(int64_t n, State<R> s, Lists L, Solver
             const uint32_t e = L.at(k, q);
             const uint32_t j = e & kIndexMask;
             const V4<R> pj = s.pos[j];
-            const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+            const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
             if (!(e & kBoundaryBit)) ap.add(pj.w * dot(ak - xyz<R>(s.acc[j]), g));
             else ap.add(pj.w * dot(ak, g));
         }
@@ -376,9 +382,20 @@ __global__ void k_iisph3d_pressure_update(int64_t n, State<R> s, Lists L, Solver
 // the 2D variant (IISPHFluidSolver.hpp:400-402, 513-523). One thread.
 //   FP32 mode : avg = (float)sum / (float)count, compared in float
 //   otherwise : avg compared in FP64
+//
+// Inside a CUDA graph the kernel ends the conditional WHILE loop through
+// `handle`. The loop is bounded independently of the state: loop_guard counts
+// executions of the body and stops it after max_it, whatever the status word
+// or the residual say.
 __global__ void k_iisph_check(StepScalars* __restrict__ sc, int min_it, int max_it, float max_err, bool fp64_test,
-                              bool two_d, const int* __restrict__ status) {
-    if (*status || sc->done) return;
+                              bool two_d, const int* __restrict__ status, cudaGraphConditionalHandle handle,
+                              bool set_condition) {
+    const int guard = ++sc->loop_guard;
+    bool stop = guard >= max_it;
+    if (*status || sc->done) {
+        if (set_condition) cudaGraphSetConditional(handle, 0u);
+        return;
+    }
     const int it = sc->iteration;  // iterations completed before this one
     const unsigned long long cnt = sc->err_count;
     const double sum = sc->err_sum;
@@ -398,8 +415,12 @@ __global__ void k_iisph_check(StepScalars* __restrict__ sc, int min_it, int max_
     bool done = false;
     const bool below = fp64_test ? (avg64 <= (double)max_err) : (avg <= max_err);
     if (two_d) {
-        // while ((it < min || err > max) && it < max): stop when it >= min and err <= max
-        done = (done_it >= min_it && below) || done_it >= max_it;
+        // while ((it < min || abs(err) > max) && it < max). The reference's
+        // unqualified abs there is the C int abs: the float error is
+        // truncated to an integer before the comparison.
+        const float e = fp64_test ? (float)avg64 : avg;
+        const float trunc_abs = (e >= 2147483647.0f || e <= -2147483647.0f) ? fabsf(e) : (float)abs((int)e);
+        done = (done_it >= min_it && trunc_abs <= max_err) || done_it >= max_it;
     } else {
         // if (iteration >= min - 1 && avg <= max) break;  (size_t: min == 0 never breaks early)
         done = (min_it >= 1 && it >= min_it - 1 && below) || done_it >= max_it;
@@ -410,6 +431,8 @@ __global__ void k_iisph_check(StepScalars* __restrict__ sc, int min_it, int max_
     sc->max_err_bits = 0u;
     sc->max_a2_bits = 0u;
     sc->max_v2_bits = 0u;
+    stop = stop || done;
+    if (set_condition) cudaGraphSetConditional(handle, stop ? 0u : 1u);
 }
 
 // CFL clamp (IISPHFluidSolver3D.hpp:525-535, SESPHFluidSolver3D.hpp:109-116) with
@@ -471,7 +494,7 @@ __global__ void k_sesph_density(int64_t n, State<R> s, Lists L, SolverConsts<R> 
     for (uint32_t q = 0; q < nn; q++) {
         const uint32_t e = L.at(k, q);
         const V4<R> pj = s.pos[e & kIndexMask];
-        const R w = c.kern.W(xk - xyz<R>(pj));
+        const R w = c.kern.template w<KAHAN>(xk - xyz<R>(pj));
         if ((e & kBoundaryBit) && c.single_layer) rho.add((c.gamma1 * pj.w) * w);
         else rho.add(pj.w * w);
     }
@@ -503,14 +526,14 @@ __global__ void k_sesph_accel(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
         const uint32_t e = L.at(k, q);
         const uint32_t j = e & kIndexMask;
         const V4<R> pj = s.pos[j];
-        const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+        const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
         if (e & kBoundaryBit) {
             const R f = -pk.w * (pdd + pdd);
             if (c.single_layer) pa.add((f * g) * c.gamma2);
             else pa.add(f * g);
         } else {
             const R rj = s.rho[j];
-            const R pddj = rj == R(0) ? R(0) : s.p[j] / (rj * rj);
+            const R pddj = rj == R(0) ? R(0) : fdiv<KAHAN>(s.p[j], rj * rj);
             pa.add((-pj.w * (pdd + pddj)) * g);
         }
     }
@@ -587,7 +610,7 @@ __global__ void k_iisph2d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
         const uint32_t nn = L.size(k);
         for (uint32_t q = 0; q < nn; q++) {
             const V4<R> pj = s.pos[L.at(k, q) & kIndexMask];
-            rho.add(pj.w * c.kern.W(xyz<R>(pk) - xyz<R>(pj)));
+            rho.add(pj.w * c.kern.template w<KAHAN>(xyz<R>(pk) - xyz<R>(pj)));
         }
         rho_k = rho.get();
     }
@@ -629,7 +652,7 @@ __global__ void k_iisph2d_density(int64_t n, State<R> s, Lists L, SolverConsts<R
     const uint32_t nn = L.size(k);
     for (uint32_t q = 0; q < nn; q++) {
         const V4<R> pj = s.pos[L.at(k, q) & kIndexMask];
-        rho.add(pj.w * c.kern.W(xk - xyz<R>(pj)));
+        rho.add(pj.w * c.kern.template w<KAHAN>(xk - xyz<R>(pj)));
     }
     s.rho[k] = rho.get();
 }
@@ -654,7 +677,7 @@ __global__ void k_iisph2d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
         const uint32_t e = L.at(k, q);
         const uint32_t j = e & kIndexMask;
         const V4<R> pj = s.pos[j];
-        const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+        const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
         sum.add(pj.w * dot(vsk - xyz<R>(s.vstar[j]), g));
         if (!(e & kBoundaryBit)) internal.add(((pj.w / c.rest_density) / c.rest_density) * g);
         else internal.add((((c.two_gamma * pj.w) / c.rest_density) / c.rest_density) * g);
@@ -665,13 +688,13 @@ __global__ void k_iisph2d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
     Acc<R, KAHAN> d;
     for (uint32_t q = 0; q < nn; q++) {
         const V4<R> pj = s.pos[L.at(k, q) & kIndexMask];
-        d.add(pj.w * dot(neg_in, c.kern.gradW(xk - xyz<R>(pj))));
+        d.add(pj.w * dot(neg_in, c.kern.template grad<KAHAN>(xk - xyz<R>(pj))));
     }
     for (uint32_t q = 0; q < nn; q++) {
         const uint32_t e = L.at(k, q);
         if (e & kBoundaryBit) continue;
         const V4<R> pj = s.pos[e & kIndexMask];
-        const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+        const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
         d.add(pj.w * dot(mi * (-g), g));
     }
     s.vstar[k] = v4<R>(vsk, source);
@@ -695,7 +718,7 @@ __global__ void k_iisph2d_pressure_acc(int64_t n, State<R> s, Lists L, SolverCon
         const uint32_t e = L.at(k, q);
         const uint32_t j = e & kIndexMask;
         const V4<R> pj = s.pos[j];
-        const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+        const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
         if (!(e & kBoundaryBit)) sum.add((pj.w * (pr + (s.p[j] / c.rest_density) / c.rest_density)) * g);
         else sum.add((((c.gamma * pj.w) * R(2)) * pr) * g);
     }
@@ -720,7 +743,7 @@ __global__ void k_iisph2d_pressure_update(int64_t n, State<R> s, Lists L, Solver
             const uint32_t e = L.at(k, q);
             const uint32_t j = e & kIndexMask;
             const V4<R> pj = s.pos[j];
-            const V3<R> g = c.kern.gradW(xk - xyz<R>(pj));
+            const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
             if (!(e & kBoundaryBit)) sum.add(pj.w * dot(ak - xyz<R>(s.acc[j]), g));
             else sum.add(pj.w * dot(ak, g));
         }

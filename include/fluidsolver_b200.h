@@ -215,6 +215,12 @@ fs_status fs_run(fs_ctx* ctx, int32_t steps, float desired_dt, fs_step_stats* st
 /* Device time of the phases of the last fs_step (ms): [0] search, [1] L1,
  * [2] L2, [3] pressure iterations, [4] integration. */
 fs_status fs_last_phase_times(fs_ctx* ctx, float* ms5);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order
+ * their own work against the library's. */
+void* fs_stream(fs_ctx* ctx);
+/* Number of this library's own kernel launches since the context was created
+ * (library kernels such as the radix sort's are not counted). */
+int64_t fs_launch_count(fs_ctx* ctx);
 
 /* ---- batched scenes -------------------------------------------------------
  * Many independent scenes of uneven size advance together: one launch per

@@ -1,0 +1,116 @@
+"""TEST INFRASTRUCTURE -- ctypes access to the plain-C restatement of the
+reference hot path (oracle/fs_oracle.c, built into oracle/_build by
+`make -C oracle`). Used by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg only, as the checker; the product never calls it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from ctypes import c_float, c_int, c_int64, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libfs_oracle.so")
+
+NS_KINDS = {"quadratic-2d": 0, "hashed-2d": 1, "compact-hashing-2d": 2, "quadratic-3d": 3, "hashed-3d": 4,
+            "compressed-3d": 5}
+SOLVERS = {"sesph-2d": 0, "sesph-3d": 1, "iisph-2d": 2, "iisph-3d": 3}
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = ctypes.CDLL(LIB)
+        L.oracle_kernel_eval.argtypes = [c_int, c_float, c_int64, c_void_p, c_void_p, c_void_p]
+        L.oracle_cfl.argtypes = [c_float] * 6
+        L.oracle_cfl.restype = c_float
+        L.oracle_ns.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_float, c_void_p, c_void_p]
+        L.oracle_ns.restype = c_int64
+        L.oracle_run.argtypes = [c_void_p, c_int64, c_int] + [c_void_p] * 13 + [c_int, c_void_p, c_int]
+        L.oracle_run.restype = c_int
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def kernel_eval(dim, support, x):
+    x = np.ascontiguousarray(x, np.float32)
+    W = np.zeros(len(x), np.float32)
+    dW = np.zeros((len(x), dim), np.float32)
+    lib().oracle_kernel_eval(dim, support, len(x), _p(x), _p(W), _p(dW))
+    return W, dW
+
+
+def cfl(timestep, lambda_v, lambda_a, particle_size, max_acc, max_vel) -> float:
+    return lib().oracle_cfl(timestep, lambda_v, lambda_a, particle_size, max_acc, max_vel)
+
+
+def search(kind: str, position, radius: float, type_=None):
+    """(offsets, indices, ok): lists in the contract's order; ok is False when a
+    list exceeds the contract's capacity (the reference throws there)."""
+    pos = np.ascontiguousarray(position, np.float32)
+    n = len(pos)
+    t = None if type_ is None else np.ascontiguousarray(type_, np.uint8)
+    off = np.zeros(n + 1, np.int64)
+    tot = lib().oracle_ns(NS_KINDS[kind], n, _p(pos), _p(t), radius, _p(off), None)
+    ok = tot >= 0
+    total = int(off[n])
+    idx = np.zeros(max(total, 1), np.int64)
+    lib().oracle_ns(NS_KINDS[kind], n, _p(pos), _p(t), radius, _p(off), _p(idx))
+    return off, idx[:total], ok
+
+
+def config(solver: str, search: str, rest_density=1.0, gravity=9.81, particle_size=1.0, stiffness=1000.0,
+           viscosity=0.01, single_layer=True, gamma1=1.1, gamma2=1.1, max_err=0.001, min_it=2, max_it=100, omega=0.5,
+           gamma=0.7, timestep=0.005, lambda_v=0.4, lambda_a=0.25) -> np.ndarray:
+    return np.array([SOLVERS[solver], NS_KINDS[search], rest_density, gravity, particle_size, stiffness, viscosity,
+                     1.0 if single_layer else 0.0, gamma1, gamma2, max_err, min_it, max_it, omega, gamma, timestep,
+                     lambda_v, lambda_a], np.float32)
+
+
+class State:
+    """A copy of a particle collection the oracle advances in place."""
+
+    def __init__(self, col):
+        n, d = col.position.shape
+        f = lambda a, shape: np.array(np.zeros(shape) if a is None else a, np.float32).reshape(shape)
+        self.n, self.dim = n, d
+        self.position = f(col.position, (n, d))
+        self.velocity = f(col.velocity, (n, d))
+        self.acceleration = f(col.acceleration, (n, d))
+        self.external = f(col.external, (n, d))
+        self.mass = f(col.mass, (n,))
+        self.density = f(col.density, (n,))
+        self.pressure = f(col.pressure, (n,))
+        self.type = np.array(col.type, np.uint8)
+        self.predicted_velocity = np.zeros((n, d), np.float32)
+        self.non_pressure_acceleration = np.zeros((n, d), np.float32)
+        self.source_term = np.zeros(n, np.float32)
+        self.diagonal_element = np.zeros(n, np.float32)
+        self.density_error = np.zeros(n, np.float32)
+
+    def run(self, cfg: np.ndarray, steps: int = 1, abs_int: bool = False) -> np.ndarray:
+        """Advances `steps` steps; returns per-step {desired, actual dt, iterations, avg error}."""
+        stats = np.zeros((steps, 4), np.float32)
+        r = lib().oracle_run(_p(cfg), self.n, self.dim, _p(self.position), _p(self.velocity), _p(self.acceleration),
+                             _p(self.external), _p(self.mass), _p(self.density), _p(self.pressure), _p(self.type),
+                             _p(self.predicted_velocity), _p(self.non_pressure_acceleration), _p(self.source_term),
+                             _p(self.diagonal_element), _p(self.density_error), steps, _p(stats), 1 if abs_int else 0)
+        if r != 0:
+            raise RuntimeError("oracle_run failed")
+        return stats

@@ -1,0 +1,183 @@
+"""Generates the golden fixtures in tests/golden/ from the reference's own
+libFluid sources compiled in oracle/_ref (make -C oracle/ref, which needs the
+reference checkout). Run from the repository root:
+
+    python tests/golden/make_golden.py
+
+Every fixture records the inputs (seeded) and the reference's outputs, so the
+CPU tests can pin the C restatement (oracle/fs_oracle.c) and the GPU tests can
+check the device path where the reference checkout is absent.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from fluidsolver_b200 import scenes  # noqa: E402
+from oracle import ref_oracle as R  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def sample_grid(start, step, stop):
+    """GetSampleGrid of tests/NeighborhoodSearchTests.cpp:51-62 (float loop
+    counters, row-major with x fastest)."""
+    pts = []
+    y = np.float32(start)
+    while y <= np.float32(stop):
+        x = np.float32(start)
+        while x <= np.float32(stop):
+            pts.append((x, y))
+            x = np.float32(x + np.float32(step))
+        y = np.float32(y + np.float32(step))
+    return np.array(pts, np.float32)
+
+
+def kernel_fixture():
+    rng = np.random.default_rng(11)
+    out = {}
+    for dim in (2, 3):
+        for support in (1.0, 2.0, 0.02, 8.5):
+            h = support / 2
+            x = (rng.uniform(-2.2, 2.2, (2000, dim)) * h).astype(np.float32)
+            x[:5] = 0.0  # |x| <= FLT_EPSILON branch
+            W, dW = R.kernel_eval(dim, support, x)
+            key = f"d{dim}_s{support}"
+            out[key + "_x"] = x
+            out[key + "_W"] = W
+            out[key + "_dW"] = dW
+    np.savez_compressed(os.path.join(OUT, "kernel.npz"), **out)
+
+
+def cfl_fixture():
+    rng = np.random.default_rng(12)
+    a = (10 ** rng.uniform(-3, 4, 4000)).astype(np.float32)
+    v = (10 ** rng.uniform(-3, 2, 4000)).astype(np.float32)
+    a[:10] = 0.0
+    v[10:20] = 0.0
+    out = {}
+    for la in (0.25, 0.3):
+        out[f"dt_la{la}"] = R.cfl_timestep(0.005, 0.4, la, 1.0, a, v)
+    np.savez_compressed(os.path.join(OUT, "cfl.npz"), max_acc=a, max_vel=v, **out)
+
+
+def _lists(kind, pos, radius, typ, calls=1, moves=None):
+    s = R.RefSearch(kind, pos, radius, typ)
+    ok = s.find()
+    off, idx = s.lists() if ok else (np.zeros(len(pos) + 1, np.int64), np.zeros(0, np.int64))
+    return ok, off, idx
+
+
+def search_fixture():
+    out = {}
+    # the reference's googletest grids (NeighborhoodSearchTests.cpp:131-299)
+    grids = {"grid11": (sample_grid(-5, 1, 5), 2.0), "grid3": (sample_grid(-1, 1, 1), 2.0),
+             "grid11x2": (sample_grid(-10, 2, 10), 4.0)}
+    for name, (pos, r) in grids.items():
+        for kind in ("quadratic-2d", "hashed-2d"):
+            ok, off, idx = _lists(kind, pos, r, None)
+            out[f"{name}_{kind}_pos"] = pos
+            out[f"{name}_{kind}_off"] = off.astype(np.int32)
+            out[f"{name}_{kind}_idx"] = idx.astype(np.int32)
+            out[f"{name}_{kind}_r"] = np.float32(r)
+    # 3D sets with every particle type, including inactive ones
+    sc = scenes.breaking_dam_3d(8, 9, 7, 1.0, tank=(14, 12, 11), seed=21)
+    typ = sc.collection.type.copy()
+    typ[::23] = 2
+    for kind in ("hashed-3d", "quadratic-3d", "compressed-3d"):
+        ok, off, idx = _lists(kind, sc.collection.position, 2.0, typ)
+        out[f"dam3d_{kind}_ok"] = np.int32(ok)
+        out[f"dam3d_{kind}_off"] = off.astype(np.int32)
+        out[f"dam3d_{kind}_idx"] = idx.astype(np.int32)
+    out["dam3d_pos"] = sc.collection.position
+    out["dam3d_type"] = typ
+    # 2D with inactive particles
+    sc2 = scenes.breaking_dam_2d(12, 10, width=20, height=16)
+    t2 = sc2.collection.type.copy()
+    t2[::11] = 2
+    for kind in ("quadratic-2d", "hashed-2d"):
+        ok, off, idx = _lists(kind, sc2.collection.position, 2.0, t2)
+        out[f"dam2d_{kind}_off"] = off.astype(np.int32)
+        out[f"dam2d_{kind}_idx"] = idx.astype(np.int32)
+    out["dam2d_pos"] = sc2.collection.position
+    out["dam2d_type"] = t2
+    # uniform random 3D points (the microbenchmark's distribution, 4096 points)
+    rng = np.random.default_rng(2)
+    pts = rng.random((4096, 3)).astype(np.float32)
+    for kind in ("hashed-3d", "compressed-3d"):
+        ok, off, idx = _lists(kind, pts, 0.1, None)
+        out[f"rand_{kind}_ok"] = np.int32(ok)
+        out[f"rand_{kind}_off"] = off.astype(np.int32)
+        out[f"rand_{kind}_idx"] = idx.astype(np.int32)
+    out["rand_pos"] = pts
+    # a dense cluster: more than 97 neighbors. The compressed search's
+    # std::bitset::set throws inside std::for_each(std::execution::par, ...),
+    # which ends the process through std::terminate; run it in a child process
+    # and record how it ended.
+    blob = (rng.normal(0.5, 0.02, (600, 3))).astype(np.float32)
+    np.save(os.path.join(OUT, "_blob_tmp.npy"), blob)
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); from oracle import ref_oracle as R; "
+            "p = np.load(%r); s = R.RefSearch('compressed-3d', p, 0.1); sys.exit(0 if s.find() else 3)"
+            % (ROOT, os.path.join(OUT, "_blob_tmp.npy")))
+    rc = subprocess.run([sys.executable, "-c", code], capture_output=True).returncode
+    os.remove(os.path.join(OUT, "_blob_tmp.npy"))
+    out["blob_pos"] = blob
+    out["blob_compressed_exit"] = np.int32(rc)
+    np.savez_compressed(os.path.join(OUT, "search.npz"), **out)
+
+
+SOLVER_CASES = {
+    # name: (solver, search, scene builder, generator, settings, steps)
+    "iisph3d_hashed": ("iisph-3d", "hashed-3d", lambda: scenes.breaking_dam_3d(6, 8, 5, 1.0, tank=(12, 12, 10), seed=31),
+                       (0.005, 0.4, 0.25), R.iisph3d_settings(), 4),
+    "iisph3d_multilayer": ("iisph-3d", "quadratic-3d",
+                           lambda: scenes.breaking_dam_3d(5, 6, 5, 1.0, tank=(10, 10, 8), seed=32, layers=2),
+                           (0.005, 0.4, 0.25), R.iisph3d_settings(single_layer=False, viscosity=5.0), 3),
+    "sesph3d_hashed": ("sesph-3d", "hashed-3d", lambda: scenes.breaking_dam_3d(6, 8, 5, 1.0, tank=(12, 12, 10), seed=33),
+                       (0.001, 0.4, 0.25), R.sesph3d_settings(k=1000.0), 4),
+    "sesph2d_quadratic": ("sesph-2d", "quadratic-2d", lambda: scenes.breaking_dam_2d(12, 10, width=20, height=16, seed=1),
+                          (0.001, 0.4, 0.25), R.sesph2d_settings(k=1000.0), 4),
+    "sesph2d_hashed": ("sesph-2d", "hashed-2d", lambda: scenes.breaking_dam_2d(12, 10, width=20, height=16, seed=2),
+                       (0.001, 0.4, 0.25), R.sesph2d_settings(k=1000.0), 4),
+    "iisph2d_quadratic": ("iisph-2d", "quadratic-2d", lambda: scenes.breaking_dam_2d(12, 10, width=20, height=16, seed=3),
+                          (0.005, 0.4, 0.25), R.iisph2d_settings(), 4),
+}
+
+
+def solver_fixture():
+    out = {}
+    for name, (solver, search, build, gen, settings, steps) in SOLVER_CASES.items():
+        sc = build()
+        col = sc.collection
+        ref = R.RefSolver(solver, search, col, (1.0, 9.81, 1.0), settings, gen)
+        out[f"{name}_in_position"] = col.position
+        out[f"{name}_in_type"] = col.type
+        stats = []
+        for k in range(steps):
+            st = ref.step()
+            stats.append([st["desired_dt"], st["actual_dt"], st["iterations"], st["avg_density_error"]])
+            s = ref.state()
+            for f in ("position", "velocity", "density", "pressure"):
+                out[f"{name}_step{k}_{f}"] = s[f]
+        out[f"{name}_stats"] = np.array(stats, np.float32)
+        out[f"{name}_settings"] = np.array(settings, np.float32)
+        out[f"{name}_generator"] = np.array(gen, np.float32)
+    np.savez_compressed(os.path.join(OUT, "solvers.npz"), **out)
+
+
+if __name__ == "__main__":
+    if not R.available():
+        sys.exit("oracle/_ref is not built; run `make -C oracle/ref` where the reference checkout is available")
+    kernel_fixture()
+    cfl_fixture()
+    search_fixture()
+    solver_fixture()
+    for f in sorted(os.listdir(OUT)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")

@@ -1,0 +1,88 @@
+"""CPU tests of the C-ABI boundary: the library builds and loads, exports every
+function include/fluidsolver_b200.h declares, fills libFluid's defaults, and
+rejects bad configurations before touching a device."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT, gpu_available
+from fluidsolver_b200 import _lib as F
+from fluidsolver_b200 import build
+
+
+@pytest.fixture(scope="module")
+def L():
+    build.build()
+    return F.lib()
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "fluidsolver_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(fs_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_header_declares_the_boundary():
+    names = declared_functions()
+    for must in ("fs_create", "fs_upload", "fs_find_neighbors", "fs_solve_step", "fs_step", "fs_download",
+                 "fs_get_neighbors_csr", "fs_query_position", "fs_destroy"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(L):
+    for name in declared_functions():
+        assert hasattr(L, name), name
+    assert set(F.EXPORTED_SYMBOLS) <= set(declared_functions())
+
+
+def test_abi_version(L):
+    assert L.fs_abi_version() == 1
+
+
+def test_params_default_are_libfluid_defaults(L):
+    p = F.FsParams()
+    L.fs_params_default(ctypes.byref(p), 3, F.FS_SOLVER_IISPH_3D, F.FS_SEARCH_HASHED_3D)
+    # IFluidSolver.hpp:18-23, IISPHSettings3D.hpp:6-20, ConstantTimestepGenerator.hpp:8-13
+    assert (p.rest_density, round(p.gravity, 5), round(p.particle_size, 5)) == (1000.0, 9.81, 0.1)
+    assert (round(p.max_density_error, 6), p.min_iterations, p.max_iterations) == (0.001, 2, 100)
+    assert (p.omega, round(p.gamma, 5), p.viscosity) == (0.5, 0.7, 5.0)
+    assert (p.single_layer_boundary, round(p.single_layer_gamma_1, 5)) == (0, 1.1)
+    assert (round(p.timestep, 6), round(p.lambda_v, 5), p.lambda_a) == (0.001, 0.4, 0.25)
+    assert p.precision == F.FS_PRECISION_FP32_KAHAN
+
+
+def _params(L, **kw):
+    p = F.FsParams()
+    L.fs_params_default(ctypes.byref(p), 3, F.FS_SOLVER_IISPH_3D, F.FS_SEARCH_HASHED_3D)
+    p.max_particles = 100
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+@pytest.mark.parametrize("bad", [
+    dict(dim=4), dict(search=17), dict(solver=9), dict(search=F.FS_SEARCH_HASHED_2D),
+    dict(max_iterations=1, min_iterations=2), dict(max_density_error=0.0), dict(particle_size=0.0),
+    dict(timestep=-1.0), dict(max_particles=0), dict(precision=7),
+])
+def test_invalid_configurations_are_rejected(L, bad):
+    ctx = ctypes.c_void_p()
+    assert L.fs_create(ctypes.byref(_params(L, **bad)), ctypes.byref(ctx)) == F.FS_ERR_INVALID
+    assert not ctx.value
+    assert L.fs_last_error()
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-device path")
+def test_no_device_fails_loudly(L):
+    ctx = ctypes.c_void_p()
+    st = L.fs_create(ctypes.byref(_params(L)), ctypes.byref(ctx))
+    assert st == F.FS_ERR_NO_DEVICE
+    assert not ctx.value
+
+
+def test_null_arguments(L):
+    assert L.fs_destroy(None) == F.FS_OK
+    assert L.fs_upload(None, None) == F.FS_ERR_INVALID
+    assert L.fs_step(None, ctypes.c_float(0.0), None) == F.FS_ERR_INVALID
