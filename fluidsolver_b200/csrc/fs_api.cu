@@ -156,7 +156,7 @@ WalkParams walk_of(fs_ctx* c, bool for_solver) {
     w.d0 = c->dims[0];
     w.d1 = c->dims[1];
     w.d2 = c->dims[2];
-    w.cell_cap = c->cell_capacity;
+    w.cells = c->cells;
     return w;
 }
 
@@ -218,7 +218,7 @@ fs_status free_all(fs_ctx* c) {
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc[0], c->acc[1], c->ext[0], c->ext[1],
                     c->rho[0], c->rho[1], c->p[0], c->p[1], c->type[0], c->type[1], c->hidx[0], c->hidx[1],
                     c->rho_prev, c->vstar, c->anp, c->err, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
-                    c->perm[0], c->perm[1], c->cub_temp, c->cell_range, c->bbox, c->origin, c->nbr, c->nbr_count,
+                    c->perm[0], c->perm[1], c->cub_temp, c->cell_start, c->cell_counts, c->bbox, c->origin, c->nbr, c->nbr_count,
                     c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->scalars};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -275,7 +275,7 @@ void choose_dims(fs_ctx* c, const float* pos, const uint8_t* type, int64_t n) {
         if (lo[a] > hi[a]) { lo[a] = hi[a] = 0; }
         int64_t e = (int64_t)hi[a] - lo[a] + 1;
         int64_t margin = std::max<int64_t>(4, e / 4);
-        ext[a] = std::min<int64_t>(kMaxDimCells, e + 2 * margin);
+        ext[a] = std::min<int64_t>(int64_t(1) << 20, e + 2 * margin);
     }
     const int64_t max_cells = std::max<int64_t>(int64_t(1) << 22, 8 * std::max<int64_t>(c->cap, 1));
     while (ext[0] * ext[1] * ext[2] > max_cells) {
@@ -285,13 +285,29 @@ void choose_dims(fs_ctx* c, const float* pos, const uint8_t* type, int64_t n) {
     for (int a = 0; a < 3; a++) c->dims[a] = (int)ext[a];
 }
 
+// cell tables for the current dims (and the scan's temporary storage)
 fs_status ensure_cells(fs_ctx* c) {
-    const int64_t cells = (int64_t)c->dims[0] * c->dims[1] * c->dims[2];
-    if (c->cell_range && c->cell_capacity >= cells) return FS_OK;
-    if (c->cell_range) cudaFree(c->cell_range);
-    c->cell_range = nullptr;
-    c->cell_capacity = cells;
-    FS_TRY(dalloc(&c->cell_range, (size_t)3 * cells));
+    c->cells = (int64_t)c->dims[0] * c->dims[1] * c->dims[2];
+    c->regions = c->reference_order ? 1 : (c->include_inactive ? 3 : 2);
+    const int64_t need = c->cells + 1;
+    if (!c->cell_start || c->cell_alloc < need) {
+        clear_graphs(c);
+        if (c->cell_start) cudaFree(c->cell_start);
+        if (c->cell_counts) cudaFree(c->cell_counts);
+        c->cell_start = c->cell_counts = nullptr;
+        FS_TRY(dalloc(&c->cell_start, (size_t)3 * need));
+        FS_TRY(dalloc(&c->cell_counts, (size_t)3 * need));
+        c->cell_alloc = need;
+    }
+    size_t temp = 0;
+    FS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, c->cell_counts, c->cell_start, (int)(3 * need), c->stream));
+    if (temp > c->cub_temp_bytes) {
+        clear_graphs(c);
+        if (c->cub_temp) cudaFree(c->cub_temp);
+        c->cub_temp = nullptr;
+        FS_CUDA(cudaMalloc(&c->cub_temp, temp));
+        c->cub_temp_bytes = temp;
+    }
     return FS_OK;
 }
 
@@ -457,19 +473,24 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     FS_CUDA(cudaGetLastError());
     c->cur = nx;
     s = state_of<R>(c);
-    // cell ranges
-    FS_CUDA(cudaMemsetAsync(c->cell_range, 0, sizeof(uint2) * 3 * c->cell_capacity, st));
+    // cell-start table: per-cell counts of every region, then one exclusive
+    // scan over the concatenated tables (regions are consecutive blocks of the
+    // sorted order, so region g's entries come out offset by its first index)
+    const int64_t table = (int64_t)c->regions * (c->cells + 1);
+    FS_CUDA(cudaMemsetAsync(c->cell_counts, 0, sizeof(uint32_t) * table, st));
     c->launches++;
-    k_cell_ranges<<<grid_for(c->n_struct), kBlock, 0, st>>>(c->n_struct, single ? nullptr : c->keys[1],
-                                                            single ? c->keys64[1] : nullptr, c->dims[0], c->dims[1],
-                                                            c->cell_capacity, c->cell_range);
+    k_cell_counts<<<grid_for(c->n_struct), kBlock, 0, st>>>(c->n_struct, single ? nullptr : c->keys[1],
+                                                            single ? c->keys64[1] : nullptr, c->cells, c->cell_counts);
     FS_CUDA(cudaGetLastError());
+    temp = c->cub_temp_bytes;
+    FS_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_temp, temp, c->cell_counts, c->cell_start, (int)table, st));
     if (solver_lists) {
         WalkParams w = walk_of(c, true);
         const uint32_t owners = 1u << FS_TYPE_NORMAL;
-    c->launches++;
-        k_build_lists<R><<<grid_for(c->n_owners), kBlock, 0, st>>>(c->n_owners, s.pos, s.type, c->cell_range, c->origin,
-                                                                    w, owners, true, c->nbr, c->nbr_stride,
+        const bool rows = !c->reference_order && c->dim == 3;
+        c->launches++;
+        k_build_lists<R><<<grid_for(c->n_owners), kBlock, 0, st>>>(c->n_owners, s.pos, s.type, c->cell_start, c->origin,
+                                                                    w, owners, rows, c->nbr, c->nbr_stride,
                                                                     c->nbr_capacity, c->nbr_count, c->status, c->scalars);
         FS_CUDA(cudaGetLastError());
         if (c->sort_lists_by_host) {
@@ -770,7 +791,10 @@ fs_status search_for_step(fs_ctx* c, float dt) {
 // captured once per buffer assignment and reused. Capturing runs the same
 // host code as the eager path, which also rotates the host-side buffer
 // pointers; a replay applies the rotation recorded at capture time.
-fs_status solve_graph(fs_ctx* c, float dt) {
+// with_search: the graph also holds the neighborhood search of the step (no
+// host synchronisation inside the step; a list overflow is found afterwards
+// in the status word, which the search sets and every solver kernel honours).
+fs_status solve_graph(fs_ctx* c, float dt, bool with_search = false) {
     fs_ctx::SolveGraph key;
     key.cur = c->cur;
     key.rho0 = c->rho[0];
@@ -780,6 +804,10 @@ fs_status solve_graph(fs_ctx* c, float dt) {
     key.n = c->n;
     key.n_owners = c->n_owners;
     key.dt = dt;
+    key.with_search = with_search;
+    key.cells = c->cells;
+    key.dims0 = c->dims[0];
+    key.dims1 = c->dims[1];
     for (auto& g : c->solve_graphs) {
         if (g.same_key(key)) {
             const int64_t per_launch = g.launches;
@@ -794,9 +822,16 @@ fs_status solve_graph(fs_ctx* c, float dt) {
     }
     const int64_t launches0 = c->launches;
     FS_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    fs_status r = FS_OK;
+    if (with_search) {
+        c->launches++;
+        k_step_begin<<<1, 1, 0, c->stream>>>(c->scalars, dt, false);
+        r = mark(c, 0, c->stream);
+        if (r == FS_OK) r = search_dispatch(c, true);
+    }
     c->launches++;
     k_step_begin<<<1, 1, 0, c->stream>>>(c->scalars, dt, true);
-    fs_status r = step_dispatch_any(c, true);
+    if (r == FS_OK) r = step_dispatch_any(c, true);
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
     if (r != FS_OK || e != cudaSuccess) {
@@ -845,10 +880,41 @@ fs_status solve_after_search(fs_ctx* c, float dt, fs_step_stats* stats) {
     return FS_OK;
 }
 
+// Enqueues `steps` whole steps (search + solver) as CUDA-graph launches with
+// no host synchronisation in between. The status word is cleared once: after
+// a failure every later step skips its solver phases, leaving the state as
+// the last successful step left it (up to the search's reordering).
+fs_status enqueue_steps(fs_ctx* c, int32_t steps, float dt) {
+    FS_CUDA(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
+    for (int32_t i = 0; i < steps; i++) FS_TRY(solve_graph(c, dt, true));
+    c->have_lists = false;
+    return FS_OK;
+}
+
+fs_status finish_steps(fs_ctx* c, fs_step_stats* stats, int* st) {
+    FS_TRY(read_scalars(c));
+    FS_TRY(read_status(c, st));
+    for (int i = 0; i < 5; i++) cudaEventElapsedTime(&c->phase_ms[i], c->ev[i], c->ev[i + 1]);
+    fill_stats(c, stats, *st);
+    return FS_OK;
+}
+
 fs_status one_step(fs_ctx* c, float desired_dt, fs_step_stats* stats) {
     if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
     if (c->prm.solver == FS_SOLVER_NONE) return fail(FS_ERR_INVALID, "context has no solver");
     const float dt = desired_dt > 0.0f ? desired_dt : c->prm.timestep;
+    if (!(c->prm.flags & FS_FLAG_SYNC_EACH_ITERATION)) {
+        FS_TRY(enqueue_steps(c, 1, dt));
+        int st = 0;
+        FS_TRY(finish_steps(c, stats, &st));
+        if (st == FS_OK) return FS_OK;
+        if (st != FS_ERR_CAPACITY || c->prm.neighbor_capacity != 0)
+            return fail((fs_status)st, "device reported an error during the step");
+        // the lists overflowed: the solver phases did not run; grow and redo
+        int K = 32;
+        while (K < c->scalars_host->max_neighbors) K *= 2;
+        FS_TRY(ensure_lists(c, K));
+    }
     FS_TRY(search_for_step(c, dt));
     return solve_after_search(c, dt, stats);
 }
@@ -1068,12 +1134,12 @@ fs_status fs_get_neighbors_csr(fs_ctx* c, int64_t* offsets, int64_t* indices, in
     if (c->precision == FS_PRECISION_FP64) {
         State<double> s = state_of<double>(c);
     c->launches++;
-        k_csr_count<double><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_range, c->origin, w, mask,
+        k_csr_count<double><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_start, c->origin, w, mask,
                                                              c->csr_counts);
     } else {
         State<float> s = state_of<float>(c);
     c->launches++;
-        k_csr_count<float><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_range, c->origin, w, mask,
+        k_csr_count<float><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_start, c->origin, w, mask,
                                                             c->csr_counts);
     }
     FS_CUDA(cudaGetLastError());
@@ -1107,12 +1173,12 @@ fs_status fs_get_neighbors_csr(fs_ctx* c, int64_t* offsets, int64_t* indices, in
     if (c->precision == FS_PRECISION_FP64) {
         State<double> s = state_of<double>(c);
     c->launches++;
-        k_csr_fill<double><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_range, c->origin, w, mask,
+        k_csr_fill<double><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_start, c->origin, w, mask,
                                                             c->csr_offsets, d_idx);
     } else {
         State<float> s = state_of<float>(c);
     c->launches++;
-        k_csr_fill<float><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_range, c->origin, w, mask,
+        k_csr_fill<float><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_start, c->origin, w, mask,
                                                            c->csr_offsets, d_idx);
     }
     std::vector<uint32_t> idx((size_t)tot);
@@ -1152,12 +1218,12 @@ fs_status fs_query_position(fs_ctx* c, const float* position, int64_t* out, int6
         State<double> s = state_of<double>(c);
     c->launches++;
         k_query_position<double><<<1, 32, 0, c->stream>>>(v3<double>(position[0], position[1], z), s.pos, s.type,
-                                                          c->cell_range, c->origin, w, d_out, room, d_cnt);
+                                                          c->cell_start, c->origin, w, d_out, room, d_cnt);
     } else {
         State<float> s = state_of<float>(c);
     c->launches++;
         k_query_position<float><<<1, 32, 0, c->stream>>>(v3<float>(position[0], position[1], z), s.pos, s.type,
-                                                         c->cell_range, c->origin, w, d_out, room, d_cnt);
+                                                         c->cell_start, c->origin, w, d_out, room, d_cnt);
     }
     unsigned long long cnt = 0;
     std::vector<uint32_t> tmp((size_t)room);
@@ -1184,8 +1250,22 @@ fs_status fs_step(fs_ctx* c, float desired_dt, fs_step_stats* stats) {
 
 fs_status fs_run(fs_ctx* c, int32_t steps, float desired_dt, fs_step_stats* stats) {
     if (!c) return fail(FS_ERR_INVALID, "ctx is null");
+    if (steps < 0) return fail(FS_ERR_INVALID, "steps must be >= 0");
     FS_CUDA(cudaSetDevice(c->device));
-    for (int32_t i = 0; i < steps; i++) FS_TRY(one_step(c, desired_dt, stats));
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    if (c->prm.solver == FS_SOLVER_NONE) return fail(FS_ERR_INVALID, "context has no solver");
+    if (steps == 0) return FS_OK;
+    if (c->prm.flags & FS_FLAG_SYNC_EACH_ITERATION) {
+        for (int32_t i = 0; i < steps; i++) FS_TRY(one_step(c, desired_dt, stats));
+        return FS_OK;
+    }
+    // one step first: it settles the list capacity (and captures the graph)
+    FS_TRY(one_step(c, desired_dt, stats));
+    const float dt = desired_dt > 0.0f ? desired_dt : c->prm.timestep;
+    FS_TRY(enqueue_steps(c, steps - 1, dt));
+    int st = 0;
+    FS_TRY(finish_steps(c, stats, &st));
+    if (st != FS_OK) return fail((fs_status)st, "device reported an error during fs_run");
     return FS_OK;
 }
 

@@ -71,8 +71,11 @@ struct fs_ctx {
     uint32_t* perm[2] = {};
     void* cub_temp = nullptr;
     size_t cub_temp_bytes = 0;
-    uint2* cell_range = nullptr;   // [3][cell_capacity] (start, end) per region
-    int64_t cell_capacity = 0;
+    uint32_t* cell_start = nullptr;   // [regions][cells + 1] first sorted index of cell >= c
+    uint32_t* cell_counts = nullptr;  // [regions][cells + 1] scratch for the scan
+    int64_t cells = 0;                // dims[0] * dims[1] * dims[2]
+    int64_t cell_alloc = 0;           // entries allocated per table
+    int regions = 2;                  // regions in the sorted layout
     int dims[3] = {1, 1, 1};
     int* bbox = nullptr;           // device: min xyz, max xyz (cell coordinates)
     int* origin = nullptr;         // device: cell-grid origin used this step
@@ -107,6 +110,9 @@ struct fs_ctx {
         int K = 0;
         int64_t n = 0, n_owners = 0;
         float dt = 0.f;
+        bool with_search = false;
+        int64_t cells = 0;
+        int dims0 = 0, dims1 = 0;
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         int64_t launches = 0;
@@ -114,7 +120,8 @@ struct fs_ctx {
         void *post_rho0 = nullptr, *post_rho1 = nullptr, *post_rho_prev = nullptr;
         bool same_key(const SolveGraph& o) const {
             return cur == o.cur && rho0 == o.rho0 && rho1 == o.rho1 && rho_prev == o.rho_prev && K == o.K &&
-                   n == o.n && n_owners == o.n_owners && dt == o.dt;
+                   n == o.n && n_owners == o.n_owners && dt == o.dt && with_search == o.with_search &&
+                   cells == o.cells && dims0 == o.dims0 && dims1 == o.dims1;
         }
     };
     std::vector<SolveGraph> solve_graphs;

@@ -1,5 +1,5 @@
-// Neighborhood search: cell keys -> radix sort -> Z-order reordering of the
-// particle SoA -> per-region cell ranges -> neighbor lists.
+// Neighborhood search: cell keys -> radix sort -> reordering of the particle
+// SoA -> per-region cell-start table -> neighbor lists.
 //
 // One device search serves every reference contract. What the contract fixes
 // (and the reference line it follows):
@@ -10,13 +10,22 @@
 //                    QuadraticNeighborhoodSearch3D.cpp:60, CompressedNeighbors.cpp:576)
 //   owners / candidates: see fs_search_kind in the public header.
 // The cell grid (cell edge = search radius, cell = floor(x / r) as in
-// HashedNeighborhoodSearch3D.cpp:224-228) is ours; because every candidate is
-// tested with the contract's exact float predicate, the neighbor SETS do not
+// HashedNeighborhoodSearch3D.cpp:224-228) is ours; every candidate is tested
+// with the contract's exact float predicate, so the neighbor SETS do not
 // depend on it.
 //
-// Cells are indexed relative to the particles' bounding box; a grid that
-// would exceed the allocated table is clamped, and candidates found through a
-// clamped cell are accepted only if their own cell is the visited one.
+// Layout. Cells are numbered linearly, x fastest, relative to a grid origin
+// that follows the particles' bounding box. Sorting by (region, cell) makes
+// the three cells x-1, x, x+1 of every (y, z) row one contiguous particle
+// range, so a particle's 27 neighbor cells are 9 ranges. Regions keep fluid,
+// boundary and listed-inactive particles in separate blocks (one block in the
+// reference-order mode). cell_start[g][c] is the first sorted index of region
+// g whose cell is >= c (an exclusive scan of the per-cell counts).
+//
+// A grid smaller than the bounding box is clamped: such particles go to border
+// cells. Particles in or next to border cells take a slow path that checks
+// every candidate's own cell; for all others no check is needed, because a
+// clamped particle lies at least two cells away from them (farther than r).
 #pragma once
 
 #include "fs_common.cuh"
@@ -24,30 +33,7 @@
 namespace fsb {
 
 constexpr uint32_t kInactiveKey = 0xffffffffu;
-constexpr int kMaxDimCells = 1024;  // 10 Morton bits per axis
-
-__device__ __forceinline__ uint32_t morton_spread10(uint32_t v) {
-    v &= 0x3ffu;
-    v = (v | (v << 16)) & 0x030000ffu;
-    v = (v | (v << 8)) & 0x0300f00fu;
-    v = (v | (v << 4)) & 0x030c30c3u;
-    v = (v | (v << 2)) & 0x09249249u;
-    return v;
-}
-__device__ __forceinline__ uint32_t morton_compact10(uint32_t v) {
-    v &= 0x09249249u;
-    v = (v | (v >> 2)) & 0x030c30c3u;
-    v = (v | (v >> 4)) & 0x0300f00fu;
-    v = (v | (v >> 8)) & 0x030000ffu;
-    v = (v | (v >> 16)) & 0x000003ffu;
-    return v;
-}
-
-struct GridInfo {
-    int dims[3];
-    float inv_unused;
-    float radius;  // cell edge
-};
+constexpr uint32_t kCellMask = 0x3fffffffu;
 
 // cell coordinate of a position: (int)floor(x / r), or the truncation toward
 // zero of HashedNeighborhoodSearch (2D) (HashedNeighborhoodSearch.cpp:108-115)
@@ -131,8 +117,8 @@ __global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* 
         int lx = local_cell(cell_coord<R>(p.x, r, trunc), origin[0], d0, cl);
         int ly = local_cell(cell_coord<R>(p.y, r, trunc), origin[1], d1, cl);
         int lz = local_cell(cell_coord<R>(p.z, r, trunc), origin[2], d2, cl);
-        uint32_t m = morton_spread10(lx) | (morton_spread10(ly) << 1) | (morton_spread10(lz) << 2);
-        key = (region_of(t, single_region) << 30) | m;
+        const uint32_t lin = (uint32_t)(((int64_t)lz * d1 + ly) * d0 + lx);
+        key = (region_of(t, single_region) << 30) | lin;
     }
     if (keys64) keys64[k] = ((unsigned long long)key << 32) | hidx[k];
     else keys[k] = key;
@@ -160,26 +146,23 @@ __global__ void k_reorder(int64_t n, const uint32_t* __restrict__ perm, const V4
     h1[k] = h0[s];
 }
 
-__device__ __forceinline__ int64_t lin_cell(uint32_t m, int d0, int d1) {
-    uint32_t lx = morton_compact10(m), ly = morton_compact10(m >> 1), lz = morton_compact10(m >> 2);
-    return ((int64_t)lz * d1 + ly) * d0 + lx;
-}
-
-// cell ranges: for region g and linear cell c, cell_range[g * cap + c] = [start, end)
-__global__ void k_cell_ranges(int64_t n_struct, const uint32_t* __restrict__ keys, const unsigned long long* __restrict__ keys64,
-                              int d0, int d1, int64_t cell_cap, uint2* __restrict__ cell_range) {
+// Per-cell particle counts of every region: the first particle of each run of
+// equal keys writes the run length (the table is zeroed before).
+__global__ void k_cell_counts(int64_t n_struct, const uint32_t* __restrict__ keys,
+                              const unsigned long long* __restrict__ keys64, int64_t cells,
+                              uint32_t* __restrict__ counts) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n_struct) return;
-    uint32_t key = keys64 ? (uint32_t)(keys64[k] >> 32) : keys[k];
-    uint32_t prev = k > 0 ? (keys64 ? (uint32_t)(keys64[k - 1] >> 32) : keys[k - 1]) : 0xffffffffu;
-    uint32_t next = k + 1 < n_struct ? (keys64 ? (uint32_t)(keys64[k + 1] >> 32) : keys[k + 1]) : 0xffffffffu;
-    int64_t c = (int64_t)(key >> 30) * cell_cap + lin_cell(key & 0x3fffffffu, d0, d1);
-    if (k == 0 || prev != key) cell_range[c].x = (uint32_t)k;
-    if (k + 1 == n_struct || next != key) cell_range[c].y = (uint32_t)(k + 1);
+    auto key_at = [&](int64_t q) -> uint32_t { return keys64 ? (uint32_t)(keys64[q] >> 32) : keys[q]; };
+    const uint32_t key = key_at(k);
+    if (k > 0 && key_at(k - 1) == key) return;
+    int64_t e = k + 1;
+    while (e < n_struct && key_at(e) == key) e++;
+    counts[(int64_t)(key >> 30) * (cells + 1) + (key & kCellMask)] = (uint32_t)(e - k);
 }
 
 // ---------------------------------------------------------------------------
-// the per-particle candidate walk shared by list building and position queries
+// candidate walks
 // ---------------------------------------------------------------------------
 struct WalkParams {
     float r;        // search radius
@@ -189,7 +172,7 @@ struct WalkParams {
     bool candidates_inactive;  // contract lists inactive neighbors
     bool trunc;                // cells by truncation toward zero (hashed 2D order)
     int d0, d1, d2;
-    int64_t cell_cap;
+    int64_t cells;  // d0 * d1 * d2; each region's table has cells + 1 entries
 };
 
 // predicate of the contract; d = x_i - x_j
@@ -204,11 +187,11 @@ template <typename R> __device__ __forceinline__ bool within(V3<R> d, const Walk
 
 // Visits the neighbors of position xi in HashedNeighborhoodSearch3D's order
 // (cells dx, dy, dz ascending with dx outermost; within a cell, sorted order).
-// f(j, entry) is called for every neighbor j; entry carries the boundary bit.
+// f(j, type_j) is called for every neighbor j.
 template <typename R, typename F>
-__device__ __forceinline__ void walk_neighbors(V3<R> xi, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                                               const uint2* __restrict__ cell_range, const int* __restrict__ origin,
-                                               const WalkParams& w, F&& f) {
+__device__ __forceinline__ void walk_cells(V3<R> xi, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
+                                           const uint32_t* __restrict__ cell_start, const int* __restrict__ origin,
+                                           const WalkParams& w, F&& f) {
     const int ci[3] = {cell_coord<R>(xi.x, w.r, w.trunc), cell_coord<R>(xi.y, w.r, w.trunc), cell_coord<R>(xi.z, w.r, w.trunc)};
     const int zr = w.dim == 2 ? 0 : 1;
     const int o0 = origin[0], o1 = origin[1], o2 = origin[2];
@@ -222,8 +205,9 @@ __device__ __forceinline__ void walk_neighbors(V3<R> xi, const V4<R>* __restrict
                 const int l2 = local_cell(c2, o2, w.d2, cl);
                 const int64_t lc = ((int64_t)l2 * w.d1 + l1) * w.d0 + l0;
                 for (int g = 0; g < w.regions; g++) {
-                    const uint2 rg = cell_range[g * w.cell_cap + lc];
-                    for (uint32_t j = rg.x; j < rg.y; j++) {
+                    const uint32_t* cs = cell_start + g * (w.cells + 1);
+                    const uint32_t b = cs[lc], e = cs[lc + 1];
+                    for (uint32_t j = b; j < e; j++) {
                         const V4<R> pj = pos[j];
                         if (cl) {
                             if (cell_coord<R>(pj.x, w.r, w.trunc) != c0 || cell_coord<R>(pj.y, w.r, w.trunc) != c1 ||
@@ -241,29 +225,76 @@ __device__ __forceinline__ void walk_neighbors(V3<R> xi, const V4<R>* __restrict
     }
 }
 
+// Fast walk for the solver lists (3D, fluid and boundary regions, no
+// inactive candidates): 9 contiguous row ranges per region. Returns false
+// (and visits nothing) for particles in or next to the grid border, which
+// take walk_cells instead.
+template <typename R, typename F>
+__device__ __forceinline__ bool walk_rows(V3<R> xi, const V4<R>* __restrict__ pos, const uint32_t* __restrict__ cell_start,
+                                          const int* __restrict__ origin, const WalkParams& w, F&& f) {
+    const int lx = cell_coord<R>(xi.x, w.r, false) - origin[0];
+    const int ly = cell_coord<R>(xi.y, w.r, false) - origin[1];
+    const int lz = cell_coord<R>(xi.z, w.r, false) - origin[2];
+    if (lx < 2 || ly < 2 || lz < 2 || lx > w.d0 - 3 || ly > w.d1 - 3 || lz > w.d2 - 3) return false;
+    const float r2 = w.r2;
+    const float x0 = (float)xi.x, x1 = (float)xi.y, x2 = (float)xi.z;
+#pragma unroll 1
+    for (int g = 0; g < 2; g++) {
+        const uint32_t* cs = cell_start + g * (w.cells + 1);
+#pragma unroll 1
+        for (int row = 0; row < 9; row++) {
+            const int64_t base = ((int64_t)(lz + row / 3 - 1) * w.d1 + (ly + row % 3 - 1)) * w.d0 + lx;
+            const uint32_t b = cs[base - 1], e = cs[base + 2];
+            for (uint32_t j = b; j < e; j++) {
+                const V4<R> pj = pos[j];
+                const float d0 = x0 - (float)pj.x, d1 = x1 - (float)pj.y, d2 = x2 - (float)pj.z;
+                if ((d0 * d0 + d1 * d1) + d2 * d2 <= r2) f(j, g);
+            }
+        }
+    }
+    return true;
+}
+
 // Solver lists: for owner k in [0, n_owners) with an owner type accepted by
-// owner_mask (bit per particle type), write up to K entries slot-major.
+// owner_mask (bit per particle type), write up to K entries slot-major. The
+// entry is the sorted index, with kBoundaryBit for boundary neighbors.
+// rows: use the 9-row walk (list order then differs from the reference's).
 template <typename R>
-__global__ void k_build_lists(int64_t n_owners, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                              const uint2* __restrict__ cell_range, const int* __restrict__ origin, WalkParams w,
-                              uint32_t owner_mask, bool solver_lists, uint32_t* __restrict__ nbr, int64_t stride, int K,
-                              uint32_t* __restrict__ count, int* __restrict__ status, StepScalars* __restrict__ sc) {
+__global__ void __launch_bounds__(128) k_build_lists(int64_t n_owners, const V4<R>* __restrict__ pos,
+                                                     const uint8_t* __restrict__ type,
+                                                     const uint32_t* __restrict__ cell_start,
+                                                     const int* __restrict__ origin, WalkParams w, uint32_t owner_mask,
+                                                     bool rows, uint32_t* __restrict__ nbr, int64_t stride, int K,
+                                                     uint32_t* __restrict__ count, int* __restrict__ status,
+                                                     StepScalars* __restrict__ sc) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n_owners) return;
     const uint8_t tk = type[k];
     uint32_t c = 0;
     if ((owner_mask >> tk) & 1u) {
         const V3<R> xi = xyz<R>(pos[k]);
-        walk_neighbors<R>(xi, pos, type, cell_range, origin, w, [&](uint32_t j, uint8_t tj) {
-            // solver lists never carry inactive particles (the solvers skip them)
-            if (solver_lists && tj == FS_TYPE_INACTIVE) return;
-            if ((int)c < K) nbr[(int64_t)c * stride + k] = j | (tj == FS_TYPE_BOUNDARY ? kBoundaryBit : 0u);
-            c++;
-        });
+        bool done = false;
+        if (rows) {
+            done = walk_rows<R>(xi, pos, cell_start, origin, w, [&](uint32_t j, int g) {
+                if ((int)c < K) nbr[(int64_t)c * stride + k] = j | (g == 1 ? kBoundaryBit : 0u);
+                c++;
+            });
+        }
+        if (!done) {
+            walk_cells<R>(xi, pos, type, cell_start, origin, w, [&](uint32_t j, uint8_t tj) {
+                // solver lists never carry inactive particles (the solvers skip them)
+                if (tj == FS_TYPE_INACTIVE) return;
+                if ((int)c < K) nbr[(int64_t)c * stride + k] = j | (tj == FS_TYPE_BOUNDARY ? kBoundaryBit : 0u);
+                c++;
+            });
+        }
     }
     count[k] = c;
     if ((int)c > K) raise_status(status, FS_ERR_CAPACITY);
-    atomicMax(&sc->max_neighbors, (int)c);
+    // warp-aggregated maximum
+    unsigned mx = c;
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(__activemask(), mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&sc->max_neighbors, (int)mx);
 }
 
 // Quadratic searches list neighbors by ascending index
@@ -291,35 +322,35 @@ __global__ void k_sort_lists_by_host(int64_t n_owners, uint32_t* __restrict__ nb
 // CSR export: counts (pass 1) and fill (pass 2) in sorted index space
 template <typename R>
 __global__ void k_csr_count(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                            const uint2* __restrict__ cell_range, const int* __restrict__ origin, WalkParams w,
+                            const uint32_t* __restrict__ cell_start, const int* __restrict__ origin, WalkParams w,
                             uint32_t owner_mask, uint32_t* __restrict__ count) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     uint32_t c = 0;
     if ((owner_mask >> type[k]) & 1u)
-        walk_neighbors<R>(xyz<R>(pos[k]), pos, type, cell_range, origin, w, [&](uint32_t, uint8_t) { c++; });
+        walk_cells<R>(xyz<R>(pos[k]), pos, type, cell_start, origin, w, [&](uint32_t, uint8_t) { c++; });
     count[k] = c;
 }
 
 template <typename R>
 __global__ void k_csr_fill(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                           const uint2* __restrict__ cell_range, const int* __restrict__ origin, WalkParams w,
+                           const uint32_t* __restrict__ cell_start, const int* __restrict__ origin, WalkParams w,
                            uint32_t owner_mask, const int64_t* __restrict__ offsets, uint32_t* __restrict__ out) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     if (!((owner_mask >> type[k]) & 1u)) return;
     int64_t o = offsets[k];
-    walk_neighbors<R>(xyz<R>(pos[k]), pos, type, cell_range, origin, w, [&](uint32_t j, uint8_t) { out[o++] = j; });
+    walk_cells<R>(xyz<R>(pos[k]), pos, type, cell_start, origin, w, [&](uint32_t j, uint8_t) { out[o++] = j; });
 }
 
 // neighbors of one arbitrary position (get_neighbors(vec)), sorted space
 template <typename R>
 __global__ void k_query_position(V3<R> x, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                                 const uint2* __restrict__ cell_range, const int* __restrict__ origin, WalkParams w,
+                                 const uint32_t* __restrict__ cell_start, const int* __restrict__ origin, WalkParams w,
                                  uint32_t* __restrict__ out, int64_t cap, unsigned long long* __restrict__ count) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     unsigned long long c = 0;
-    walk_neighbors<R>(x, pos, type, cell_range, origin, w, [&](uint32_t j, uint8_t) {
+    walk_cells<R>(x, pos, type, cell_start, origin, w, [&](uint32_t j, uint8_t) {
         if ((int64_t)c < cap) out[c] = j;
         c++;
     });

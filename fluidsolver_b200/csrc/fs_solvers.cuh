@@ -37,6 +37,32 @@ struct Lists {
     __device__ __forceinline__ uint32_t at(int64_t k, uint32_t s) const { return nbr[(int64_t)s * stride + k]; }
 };
 
+// Visits particle k's list in order, handing f(entry, position of the
+// neighbor). Entries and positions are loaded a batch at a time before any of
+// them is used, so that a thread keeps several independent gathers in flight
+// instead of one dependent load chain per neighbor. The summation order (list
+// order) is unchanged.
+constexpr int kBatch = 4;
+template <typename R, typename F>
+__device__ __forceinline__ void for_neighbors(const Lists& L, int64_t k, const V4<R>* __restrict__ pos, F&& f) {
+    const uint32_t n = L.size(k);
+    uint32_t q = 0;
+    for (; q + kBatch <= n; q += kBatch) {
+        uint32_t e[kBatch];
+        V4<R> p[kBatch];
+#pragma unroll
+        for (int b = 0; b < kBatch; b++) e[b] = __ldg(&L.nbr[(int64_t)(q + b) * L.stride + k]);
+#pragma unroll
+        for (int b = 0; b < kBatch; b++) p[b] = pos[e[b] & kIndexMask];
+#pragma unroll
+        for (int b = 0; b < kBatch; b++) f(e[b], p[b]);
+    }
+    for (; q < n; q++) {
+        const uint32_t e = __ldg(&L.nbr[(int64_t)q * L.stride + k]);
+        f(e, pos[e & kIndexMask]);
+    }
+}
+
 template <typename R> struct State {
     V4<R>* __restrict__ pos;
     V4<R>* __restrict__ vel;
@@ -85,20 +111,17 @@ template <typename R, bool KAHAN, typename RhoOf>
 __device__ __forceinline__ V3<R> viscosity(int64_t k, const State<R>& s, const Lists& L, const SolverConsts<R>& c,
                                            V3<R> xi, V3<R> vi, RhoOf&& rho_of) {
     Acc3<R, KAHAN> tmp;
-    const uint32_t n = L.size(k);
-    for (uint32_t q = 0; q < n; q++) {
-        const uint32_t e = L.at(k, q);
+    for_neighbors<R>(L, k, s.pos, [&](uint32_t e, const V4<R>& pj) {
         const uint32_t j = e & kIndexMask;
         const R rj = rho_of(j, e);
-        if (rj == R(0)) continue;
-        const V4<R> pj = s.pos[j];
+        if (rj == R(0)) return;
         const V4<R> vj = s.vel[j];
         const V3<R> vij = vi - xyz<R>(vj);
         const V3<R> xij = xi - xyz<R>(pj);
         const R f = KAHAN ? fdiv<true>(pj.w * dot(vij, xij), rj * (dot(xij, xij) + c.visc_eps))
                           : (pj.w / rj) * (dot(vij, xij) / (dot(xij, xij) + c.visc_eps));
         tmp.add(f * c.kern.template grad<KAHAN>(xij));
-    }
+    });
     return c.two_nu * tmp.get();
 }
 
@@ -152,14 +175,11 @@ __global__ void k_iisph3d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
     }
     if (!SPLIT) {
         Acc<R, KAHAN> rho;
-        const uint32_t nn = L.size(k);
-        for (uint32_t q = 0; q < nn; q++) {
-            const uint32_t e = L.at(k, q);
-            const V4<R> pj = s.pos[e & kIndexMask];
+        for_neighbors<R>(L, k, s.pos, [&](uint32_t e, const V4<R>& pj) {
             R m = pj.w;
             if (c.single_layer && (e & kBoundaryBit)) m = m * c.gamma1;
             rho.add(m * c.kern.template w<KAHAN>(xyz<R>(pk) - xyz<R>(pj)));
-        }
+        });
         s.rho[k] = rho.get();
     }
 }
@@ -209,15 +229,12 @@ __global__ void k_iisph3d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
     const V3<R> xk = xyz<R>(pk);
     const V4<R> vsk4 = s.vstar[k];
     const V3<R> vsk = xyz<R>(vsk4);
-    const uint32_t nn = L.size(k);
     Acc<R, KAHAN> contrib;
     Acc3<R, KAHAN> inner;
     Acc3<R, KAHAN> mg;    // sum_j m_j gradW      (single-pass a_ii)
     Acc<R, KAHAN> mg2;    // sum_fluid m_j |gradW|^2
-    for (uint32_t q = 0; q < nn; q++) {
-        const uint32_t e = L.at(k, q);
+    for_neighbors<R>(L, k, s.pos, [&](uint32_t e, const V4<R>& pj) {
         const uint32_t j = e & kIndexMask;
-        const V4<R> pj = s.pos[j];
         const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
         if (!(e & kBoundaryBit)) {
             const V3<R> vsj = xyz<R>(s.vstar[j]);
@@ -230,22 +247,19 @@ __global__ void k_iisph3d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
             inner.sub((KAHAN ? w * c.inv_rho0_sq : w / c.rho0_sq) * g);
         }
         if (!TWO_PASS) mg.add(pj.w * g);
-    }
+    });
     const R source = (c.rest_density - s.rho[k]) - dt * contrib.get();
     const V3<R> in = inner.get();
     R diag;
     if (TWO_PASS) {
         Acc<R, KAHAN> d;
         const R mi = pk.w / c.rho0_sq;
-        for (uint32_t q = 0; q < nn; q++) {
-            const uint32_t e = L.at(k, q);
-            const uint32_t j = e & kIndexMask;
-            const V4<R> pj = s.pos[j];
+        for_neighbors<R>(L, k, s.pos, [&](uint32_t e, const V4<R>& pj) {
             const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
             d.add(pj.w * dot(in, g));
             // gradW(x_j - x_i) == -gradW(x_i - x_j) bit for bit
             if (!(e & kBoundaryBit)) d.add(pj.w * dot(mi * (-g), g));
-        }
+        });
         diag = d.get() * (dt * dt);
     } else {
         diag = (dot(in, mg.get()) - (pk.w / c.rho0_sq) * mg2.get()) * (dt * dt);
@@ -267,12 +281,9 @@ __global__ void k_iisph3d_pressure_acc(int64_t n, State<R> s, Lists L, SolverCon
     if (s.type[k] != FS_TYPE_NORMAL) return;
     const V3<R> xk = xyz<R>(s.pos[k]);
     const R pk = s.p[k];
-    const uint32_t nn = L.size(k);
     Acc3<R, KAHAN> pa;
-    for (uint32_t q = 0; q < nn; q++) {
-        const uint32_t e = L.at(k, q);
+    for_neighbors<R>(L, k, s.pos, [&](uint32_t e, const V4<R>& pj) {
         const uint32_t j = e & kIndexMask;
-        const V4<R> pj = s.pos[j];
         const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
         if (KAHAN) {
             const R f = !(e & kBoundaryBit) ? pj.w * (pk + s.p[j])
@@ -285,7 +296,7 @@ __global__ void k_iisph3d_pressure_acc(int64_t n, State<R> s, Lists L, SolverCon
         } else {
             pa.sub((((pj.w * R(2)) * pk) / c.rho0_sq) * g);
         }
-    }
+    });
     s.acc[k] = v4<R>(pa.get(), R(0));
 }
 
@@ -306,16 +317,13 @@ __global__ void k_iisph3d_pressure_update(int64_t n, State<R> s, Lists L, Solver
         const R dt = (R)sc->dt;
         const V3<R> xk = xyz<R>(s.pos[k]);
         const V3<R> ak = xyz<R>(s.acc[k]);
-        const uint32_t nn = L.size(k);
         Acc<R, KAHAN> ap;
-        for (uint32_t q = 0; q < nn; q++) {
-            const uint32_t e = L.at(k, q);
+        for_neighbors<R>(L, k, s.pos, [&](uint32_t e, const V4<R>& pj) {
             const uint32_t j = e & kIndexMask;
-            const V4<R> pj = s.pos[j];
             const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
             if (!(e & kBoundaryBit)) ap.add(pj.w * dot(ak - xyz<R>(s.acc[j]), g));
             else ap.add(pj.w * dot(ak, g));
-        }
+        });
         const R Ap = ap.get() * (dt * dt);
         const V4<R> vs = s.vstar[k];   // w: source term
         const R aii = s.anp[k].w;

@@ -278,6 +278,14 @@ class FluidSolverBase:
         F.check(F.lib().fs_step(self._dev.ctx, float(dt), ctypes.byref(self.last_stats)))
         return self.last_stats
 
+    def run(self, steps: int, desired_dt: float | None = None) -> F.FsStepStats:
+        """`steps` steps without host synchronisation in between (fs_run);
+        returns the last step's statistics."""
+        self.initialize()
+        dt = self.timestep_generator.settings.timestep if desired_dt is None else desired_dt
+        F.check(F.lib().fs_run(self._dev.ctx, int(steps), float(dt), ctypes.byref(self.last_stats)))
+        return self.last_stats
+
     def phase_times(self) -> list[float]:
         out = np.zeros(5, np.float32)
         F.check(F.lib().fs_last_phase_times(self.ctx, out.ctypes.data))
