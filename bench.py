@@ -24,9 +24,8 @@ import ctypes
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
+import threading
 import time
 
 import numpy as np
@@ -58,57 +57,67 @@ def measured_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled through NVML every
+    few milliseconds while the timed region runs (read-only queries)."""
 
-    def __init__(self, device: int):
-        try:
-            import torch
-            self.index = "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
-        except Exception:
-            self.index = str(device)
-        self.proc = None
-        self.file = None
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
+
+    def __init__(self, device: int, period_s: float = 0.004):
+        self.device, self.period = device, period_s
+        self.samples, self.max_mhz, self.handle = [], None, None
+        self.nvml = None
+        self.stop = threading.Event()
+        self.thread = None
 
     def __enter__(self):
         try:
-            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index),
-                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+            self.handle = pynvml.nvmlDeviceGetHandleByUUID(uuid)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+            self.nvml = pynvml
         except Exception:
-            self.proc = None
+            self.nvml = None
+            return self
+        self.sample()
+        self.thread = threading.Thread(target=self.loop, daemon=True)
+        self.thread.start()
         return self
 
+    def sample(self):
+        N = self.nvml
+        try:
+            mhz = N.nvmlDeviceGetClockInfo(self.handle, N.NVML_CLOCK_SM)
+            bits = N.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+        except Exception:
+            return
+        self.samples.append((mhz, bits))
+
+    def loop(self):
+        while not self.stop.wait(self.period):
+            self.sample()
+
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            self.sample()
 
     def summary(self):
-        if self.proc is None:
+        if self.nvml is None or not self.samples:
             return None
-        self.file.flush()
-        rows = []
-        with open(self.file.name) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 8:
-                    rows.append(parts)
-        os.unlink(self.file.name)
-        if not rows:
-            return None
-        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        N = self.nvml
+        reasons = sorted({name for _, bits in self.samples for name, attr in self.REASONS
+                          if hasattr(N, attr) and bits & getattr(N, attr)})
+        return {"sm_mhz": statistics.median(m for m, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples), "source": "NVML, 4 ms period"}
 
 
 def make_solver(scene, device, precision="fp32-kahan"):
@@ -285,8 +294,9 @@ def run_e2e(solver, scene, steps, device, max_over_ranks):
            "type": pinned((n,), torch.uint8)}
     for k, a in inp.items():
         a[...] = getattr(src, k)
-    out = {"position": pinned((n, 3), torch.float32), "velocity": pinned((n, 3), torch.float32),
-           "density": pinned((n,), torch.float32), "pressure": pinned((n,), torch.float32)}
+    # the step's results land in the same pinned arrays the next upload reads
+    out = {"position": inp["position"], "velocity": inp["velocity"], "density": inp["density"],
+           "pressure": pinned((n,), torch.float32)}
     fin = F.FsParticles()
     fin.n = n
     for k, a in inp.items():
@@ -305,9 +315,6 @@ def run_e2e(solver, scene, steps, device, max_over_ranks):
         F.check(L.fs_upload(ctx, ctypes.byref(fin)))
         F.check(L.fs_step(ctx, ctypes.c_float(0.0), ctypes.byref(stats)))
         F.check(L.fs_download(ctx, ctypes.byref(fout)))
-        inp["position"][...] = out["position"]
-        inp["velocity"][...] = out["velocity"]
-        inp["density"][...] = out["density"]
     el = max_over_ranks(time.perf_counter() - t0)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     return {"value": scene.n_fluid * steps * world / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),

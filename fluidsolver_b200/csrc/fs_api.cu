@@ -136,10 +136,15 @@ template <typename R> SolverConsts<R> consts_of(fs_ctx* c) {
     return k;
 }
 
+// The compensated-sum (fast) mode stores every list entry's kernel-gradient
+// factor next to it; the exact modes evaluate the kernel in each pass.
+bool fast_lists(const fs_ctx* c) { return c->precision == FS_PRECISION_FP32_KAHAN && !c->reference_order; }
+
 Lists lists_of(fs_ctx* c) {
     Lists L;
     L.nbr = c->nbr;
     L.count = c->nbr_count;
+    L.grad = fast_lists(c) ? c->nbr_grad : nullptr;
     L.stride = c->nbr_stride;
     L.K = c->nbr_capacity;
     return L;
@@ -153,6 +158,9 @@ WalkParams walk_of(fs_ctx* c, bool for_solver) {
     w.regions = c->reference_order ? 1 : (c->include_inactive && !for_solver ? 3 : 2);
     w.candidates_inactive = c->include_inactive && !for_solver;
     w.trunc = c->truncate_cells;
+    w.length_test = c->dim == 2;
+    w.inv_h = 1.0f / c->kernel_h;
+    w.alpha_h = c->kernel_alpha * c->kernel_h;
     w.d0 = c->dims[0];
     w.d1 = c->dims[1];
     w.d2 = c->dims[2];
@@ -217,7 +225,7 @@ void clear_graphs(fs_ctx* c) {
 fs_status free_all(fs_ctx* c) {
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc[0], c->acc[1], c->ext[0], c->ext[1],
                     c->rho[0], c->rho[1], c->p[0], c->p[1], c->type[0], c->type[1], c->hidx[0], c->hidx[1],
-                    c->rho_prev, c->vstar, c->anp, c->err, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
+                    c->rho_prev, c->vstar, c->anp, c->err, c->nbr_grad, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
                     c->perm[0], c->perm[1], c->cub_temp, c->cell_start, c->cell_counts, c->bbox, c->origin, c->nbr, c->nbr_count,
                     c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->scalars};
     for (void* q : ptrs)
@@ -247,8 +255,11 @@ fs_status ensure_lists(fs_ctx* c, int K) {
     if (c->nbr && c->nbr_capacity >= K && c->nbr_stride == stride) return FS_OK;
     clear_graphs(c);
     if (c->nbr) cudaFree(c->nbr);
+    if (c->nbr_grad) cudaFree(c->nbr_grad);
     c->nbr = nullptr;
+    c->nbr_grad = nullptr;
     FS_TRY(dalloc(&c->nbr, (size_t)K * stride));
+    if (fast_lists(c)) FS_TRY(dalloc(&c->nbr_grad, (size_t)K * stride));
     c->nbr_capacity = K;
     c->nbr_stride = stride;
     return FS_OK;
@@ -256,20 +267,13 @@ fs_status ensure_lists(fs_ctx* c, int K) {
 
 // cell-grid dims from the host positions: bounding box + margin, clamped to
 // 1024 per axis and to a total table size
-void choose_dims(fs_ctx* c, const float* pos, const uint8_t* type, int64_t n) {
-    int lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+// Grid dims from the cell bounding box of the uploaded particles (lo > hi on
+// an axis: no finite coordinate there): the box plus a margin of a quarter
+// of its extent (at least 4 cells) on each side, shrunk until the grid has
+// at most max(4M, 8 * capacity) cells.
+void choose_dims(fs_ctx* c, const int* lo_in, const int* hi_in) {
     const int dim = c->dim;
-    for (int64_t i = 0; i < n; i++) {
-        if (!c->include_inactive && type && type[i] == FS_TYPE_INACTIVE) continue;
-        for (int a = 0; a < dim; a++) {
-            float x = pos[i * dim + a];
-            if (!(std::fabs(x) < 1e30f)) continue;
-            float q = std::floor(x / c->search_radius);
-            int cc = (int)std::max(-1.0e9f, std::min(1.0e9f, q));
-            lo[a] = std::min(lo[a], cc);
-            hi[a] = std::max(hi[a], cc);
-        }
-    }
+    int lo[3] = {lo_in[0], lo_in[1], lo_in[2]}, hi[3] = {hi_in[0], hi_in[1], hi_in[2]};
     int64_t ext[3] = {1, 1, 1};
     for (int a = 0; a < dim; a++) {
         if (lo[a] > hi[a]) { lo[a] = hi[a] = 0; }
@@ -364,34 +368,99 @@ __global__ void k_unpack(int64_t n, int dim, int field, State<R> s, float* __res
     }
 }
 
-template <typename R> fs_status upload_impl(fs_ctx* c, const fs_particles* in) {
+// Upload census over the staged host arrays: particles per type (index 3:
+// invalid types) and, per axis, the min/max of floor(x / r) over the finite
+// coordinates (|x| < 1e30, clamped to +-1e9) of the particles that take part
+// in the cell structure.
+struct UploadCensus {
+    unsigned long long counts[4];
+    int lo[3], hi[3];
+};
+
+__global__ void k_census(int64_t n, int dim, const float* __restrict__ pos, const uint8_t* __restrict__ type, float r,
+                         bool include_inactive, UploadCensus* __restrict__ out) {
+    unsigned int cnt[4] = {0, 0, 0, 0};
+    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint8_t t = type ? type[i] : (uint8_t)FS_TYPE_NORMAL;
+        cnt[t <= 2 ? t : 3]++;
+        if (!include_inactive && t == FS_TYPE_INACTIVE) continue;
+        for (int a = 0; a < dim; a++) {
+            const float x = pos[i * dim + a];
+            if (!(fabsf(x) < 1e30f)) continue;
+            const int cc = (int)fmaxf(-1.0e9f, fminf(1.0e9f, floorf(x / r)));
+            lo[a] = min(lo[a], cc);
+            hi[a] = max(hi[a], cc);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int t = 0; t < 4; t++) cnt[t] += __shfl_xor_sync(0xffffffffu, cnt[t], o);
+        for (int a = 0; a < 3; a++) {
+            lo[a] = min(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+            hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int t = 0; t < 4; t++)
+            if (cnt[t]) atomicAdd(&out->counts[t], (unsigned long long)cnt[t]);
+        for (int a = 0; a < 3; a++) {
+            if (lo[a] != INT_MAX) atomicMin(&out->lo[a], lo[a]);
+            if (hi[a] != INT_MIN) atomicMax(&out->hi[a], hi[a]);
+        }
+    }
+}
+
+// host arrays of one upload, staged in device memory
+struct StagedUpload {
+    const float *pos = nullptr, *vel = nullptr, *acc = nullptr, *ext = nullptr;
+    const float *mass = nullptr, *rho = nullptr, *p = nullptr;
+    const uint8_t* type = nullptr;
+    UploadCensus* census = nullptr;
+};
+
+fs_status stage_upload(fs_ctx* c, const fs_particles* in, StagedUpload& d, UploadCensus& h) {
     const int64_t n = in->n;
-    const int dim = c->dim;
-    const size_t vec = (size_t)n * dim * sizeof(float), sc = (size_t)n * sizeof(float);
-    FS_TRY(ensure_staging(c, 4 * vec + 3 * sc + (size_t)n + 64));
+    const size_t vec = (size_t)n * c->dim * sizeof(float), sc = (size_t)n * sizeof(float);
+    FS_TRY(ensure_staging(c, 4 * vec + 3 * sc + (size_t)n + 16 * 9 + sizeof(UploadCensus)));
     char* st = (char*)c->staging;
-    auto put = [&](const void* src, size_t bytes, size_t& off) -> const float* {
+    size_t off = 0;
+    cudaError_t e = cudaSuccess;
+    auto put = [&](const void* src, size_t bytes) -> const void* {
         if (!src) return nullptr;
         char* dst = st + off;
         off += (bytes + 15) & ~size_t(15);
-        if (cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess) return nullptr;
-        return (const float*)dst;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+        return dst;
     };
-    size_t off = 0;
-    const float* d_pos = put(in->position, vec, off);
-    if (!d_pos) return fail(FS_ERR_INVALID, "position is required for upload");
-    const float* d_vel = put(in->velocity, vec, off);
-    const float* d_acc = put(in->acceleration, vec, off);
-    const float* d_ext = put(in->external, vec, off);
-    const float* d_mass = put(in->mass, sc, off);
-    const float* d_rho = put(in->density, sc, off);
-    const float* d_p = put(in->pressure, sc, off);
-    const uint8_t* d_type = (const uint8_t*)put(in->type, (size_t)n, off);
-    FS_CUDA(cudaGetLastError());
+    d.pos = (const float*)put(in->position, vec);
+    d.vel = (const float*)put(in->velocity, vec);
+    d.acc = (const float*)put(in->acceleration, vec);
+    d.ext = (const float*)put(in->external, vec);
+    d.mass = (const float*)put(in->mass, sc);
+    d.rho = (const float*)put(in->density, sc);
+    d.p = (const float*)put(in->pressure, sc);
+    d.type = (const uint8_t*)put(in->type, (size_t)n);
+    d.census = (UploadCensus*)(st + off);
+    h = UploadCensus{{0, 0, 0, 0}, {INT_MAX, INT_MAX, INT_MAX}, {INT_MIN, INT_MIN, INT_MIN}};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d.census, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return fail(FS_ERR_CUDA, cudaGetErrorString(e));
+    if (n > 0) {
+        c->launches++;
+        k_census<<<(int)std::min<int64_t>((n + 255) / 256, 592), 256, 0, c->stream>>>(
+            n, c->dim, d.pos, d.type, c->search_radius, c->include_inactive, d.census);
+        FS_CUDA(cudaGetLastError());
+    }
+    FS_CUDA(cudaMemcpyAsync(&h, d.census, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    FS_CUDA(cudaStreamSynchronize(c->stream));
+    return FS_OK;
+}
+
+template <typename R> fs_status pack_upload(fs_ctx* c, const StagedUpload& d, int64_t n) {
     c->cur = 0;
+    if (n == 0) return FS_OK;
     State<R> s = state_of<R>(c);
     c->launches++;
-    k_pack<R><<<grid_for(n), kBlock, 0, c->stream>>>(n, dim, d_pos, d_vel, d_acc, d_ext, d_mass, d_rho, d_p, d_type,
+    k_pack<R><<<grid_for(n), kBlock, 0, c->stream>>>(n, c->dim, d.pos, d.vel, d.acc, d.ext, d.mass, d.rho, d.p, d.type,
                                                      c->prm.rest_density, s, c->type[0], c->hidx[0]);
     FS_CUDA(cudaGetLastError());
     FS_CUDA(cudaStreamSynchronize(c->stream));
@@ -436,6 +505,7 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     const bool single = c->reference_order;
     if (n == 0) {
         c->have_lists = solver_lists;
+        c->have_cells = true;
         return FS_OK;
     }
     State<R> s = state_of<R>(c);
@@ -490,7 +560,7 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
         const bool rows = !c->reference_order && c->dim == 3;
         c->launches++;
         k_build_lists<R><<<grid_for(c->n_owners), kBlock, 0, st>>>(c->n_owners, s.pos, s.type, c->cell_start, c->origin,
-                                                                    w, owners, rows, c->nbr, c->nbr_stride,
+                                                                    w, owners, rows, c->nbr, c->nbr_grad, c->nbr_stride,
                                                                     c->nbr_capacity, c->nbr_count, c->status, c->scalars);
         FS_CUDA(cudaGetLastError());
         if (c->sort_lists_by_host) {
@@ -501,26 +571,18 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
         }
         c->have_lists = true;
     }
+    c->have_cells = true;
     return FS_OK;
 }
 
 // layout bookkeeping after an upload: counts per type and owner range
-fs_status layout_from_types(fs_ctx* c, const uint8_t* type, int64_t n) {
-    int64_t nf = 0, nb = 0, ni = 0;
-    for (int64_t i = 0; i < n; i++) {
-        uint8_t t = type ? type[i] : (uint8_t)FS_TYPE_NORMAL;
-        if (t == FS_TYPE_NORMAL) nf++;
-        else if (t == FS_TYPE_BOUNDARY) nb++;
-        else if (t == FS_TYPE_INACTIVE) ni++;
-        else return fail(FS_ERR_INVALID, "particle type must be 0, 1 or 2");
-    }
+void set_layout(fs_ctx* c, int64_t n, int64_t nf, int64_t nb, int64_t ni) {
     c->n = n;
     c->n_fluid = nf;
     c->n_boundary = nb;
     c->n_inactive = ni;
     c->n_struct = c->include_inactive ? n : nf + nb;
     c->n_owners = c->reference_order ? c->n_struct : nf;
-    return FS_OK;
 }
 
 fs_status read_scalars(fs_ctx* c) {
@@ -1066,16 +1128,22 @@ fs_status fs_set_params(fs_ctx* c, const fs_params* p) {
 fs_status fs_upload(fs_ctx* c, const fs_particles* in) {
     if (!c || !in) return fail(FS_ERR_INVALID, "null argument");
     if (in->n < 0 || in->n > c->cap) return fail(FS_ERR_INVALID, "particle count exceeds the context capacity");
+    if (in->n > 0 && !in->position) return fail(FS_ERR_INVALID, "position is required for upload");
     FS_CUDA(cudaSetDevice(c->device));
+    StagedUpload d;
+    UploadCensus h;
+    FS_TRY(stage_upload(c, in, d, h));
+    if (h.counts[3]) return fail(FS_ERR_INVALID, "particle type must be 0, 1 or 2");
     const int64_t n_before = c->n, owners_before = c->n_owners;
-    FS_TRY(layout_from_types(c, in->type, in->n));
+    set_layout(c, in->n, (int64_t)h.counts[0], (int64_t)h.counts[1], (int64_t)h.counts[2]);
     if (c->n != n_before || c->n_owners != owners_before) clear_graphs(c);
-    choose_dims(c, in->position, in->type, in->n);
+    choose_dims(c, h.lo, h.hi);
     FS_TRY(ensure_cells(c));
-    fs_status r = c->precision == FS_PRECISION_FP64 ? upload_impl<double>(c, in) : upload_impl<float>(c, in);
+    fs_status r = c->precision == FS_PRECISION_FP64 ? pack_upload<double>(c, d, in->n) : pack_upload<float>(c, d, in->n);
     if (r != FS_OK) return r;
     c->have_state = true;
     c->have_lists = false;
+    c->have_cells = false;
     return FS_OK;
 }
 
@@ -1202,9 +1270,21 @@ fs_status fs_get_neighbors_csr(fs_ctx* c, int64_t* offsets, int64_t* indices, in
 
 fs_status fs_query_position(fs_ctx* c, const float* position, int64_t* out, int64_t cap, int64_t* count) {
     if (!c || !position) return fail(FS_ERR_INVALID, "null argument");
+    if (cap > 0 && !out) return fail(FS_ERR_INVALID, "out is null");
     if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    const int search = c->prm.search;
+    if (search == FS_SEARCH_COMPACT_2D)
+        return fail(FS_ERR_INVALID, "the compact-hashing contract has no position query (it throws \"Not implemented\")");
+    // the quadratic contracts test every particle; the others walk the cells
+    // of the last search (stale cells, current positions, as the reference)
+    const bool all = search == FS_SEARCH_QUADRATIC_2D || search == FS_SEARCH_QUADRATIC_3D;
+    if (!all && !c->have_cells) return fail(FS_ERR_STATE, "position queries need a neighborhood search after the upload");
+    if (count) *count = 0;
+    if (c->n == 0) return FS_OK;
     FS_CUDA(cudaSetDevice(c->device));
     WalkParams w = walk_of(c, false);
+    w.length_test = search != FS_SEARCH_COMPRESSED_3D;
+    const bool skip = search == FS_SEARCH_HASHED_3D;
     uint32_t* d_out = nullptr;
     unsigned long long* d_cnt = nullptr;
     const int64_t room = std::max<int64_t>(cap, 0);
@@ -1213,28 +1293,38 @@ fs_status fs_query_position(fs_ctx* c, const float* position, int64_t* out, int6
         cudaFree(d_out);
         return FS_ERR_CUDA;
     }
+    cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), c->stream);
     const float z = c->dim == 3 ? position[2] : 0.0f;
+    const int gq = (int)std::min<int64_t>((c->n + kBlock - 1) / kBlock, 1184);
     if (c->precision == FS_PRECISION_FP64) {
         State<double> s = state_of<double>(c);
-    c->launches++;
-        k_query_position<double><<<1, 32, 0, c->stream>>>(v3<double>(position[0], position[1], z), s.pos, s.type,
-                                                          c->cell_start, c->origin, w, d_out, room, d_cnt);
+        const V3<double> x = v3<double>(position[0], position[1], z);
+        c->launches++;
+        if (all) k_query_all<double><<<gq, kBlock, 0, c->stream>>>(x, c->n, s.pos, w, d_out, room, d_cnt);
+        else k_query_position<double><<<1, 32, 0, c->stream>>>(x, s.pos, s.type, s.hidx, c->cell_start, c->origin, w,
+                                                               skip, d_out, room, d_cnt);
     } else {
         State<float> s = state_of<float>(c);
-    c->launches++;
-        k_query_position<float><<<1, 32, 0, c->stream>>>(v3<float>(position[0], position[1], z), s.pos, s.type,
-                                                         c->cell_start, c->origin, w, d_out, room, d_cnt);
+        const V3<float> x = v3<float>(position[0], position[1], z);
+        c->launches++;
+        if (all) k_query_all<float><<<gq, kBlock, 0, c->stream>>>(x, c->n, s.pos, w, d_out, room, d_cnt);
+        else k_query_position<float><<<1, 32, 0, c->stream>>>(x, s.pos, s.type, s.hidx, c->cell_start, c->origin, w,
+                                                              skip, d_out, room, d_cnt);
     }
+    cudaError_t e = cudaGetLastError();
     unsigned long long cnt = 0;
     std::vector<uint32_t> tmp((size_t)room);
-    cudaMemcpyAsync(&cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream);
-    if (room) cudaMemcpyAsync(tmp.data(), d_out, sizeof(uint32_t) * room, cudaMemcpyDeviceToHost, c->stream);
     std::vector<uint32_t> hidx((size_t)c->n);
-    cudaMemcpyAsync(hidx.data(), c->hidx[c->cur], sizeof(uint32_t) * c->n, cudaMemcpyDeviceToHost, c->stream);
-    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && room)
+        e = cudaMemcpyAsync(tmp.data(), d_out, sizeof(uint32_t) * room, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hidx.data(), c->hidx[c->cur], sizeof(uint32_t) * c->n, cudaMemcpyDeviceToHost, c->stream);
+    const cudaError_t e2 = cudaStreamSynchronize(c->stream);
     cudaFree(d_out);
     cudaFree(d_cnt);
     if (e != cudaSuccess) return fail(FS_ERR_CUDA, cudaGetErrorString(e));
+    if (e2 != cudaSuccess) return fail(FS_ERR_CUDA, cudaGetErrorString(e2));
     const int64_t m = std::min<int64_t>((int64_t)cnt, room);
     for (int64_t q = 0; q < m; q++) out[q] = hidx[tmp[q]];
     std::sort(out, out + m);

@@ -130,6 +130,12 @@ template <> __device__ __forceinline__ double SplineKernel<double>::rsqrt_fast(d
 template <> __device__ __forceinline__ float SplineKernel<float>::sqrt_fast(float x) { return x > 0.f ? x * rsqrtf(x) : 0.f; }
 template <> __device__ __forceinline__ double SplineKernel<double>::sqrt_fast(double x) { return sqrt(x); }
 
+// dot product: glm's (x*x' + y*y') + z*z' in the exact modes, fused in the fast mode
+template <bool FAST, typename R> __device__ __forceinline__ R dotf(V3<R> a, V3<R> b) {
+    if (FAST) return SplineKernel<R>::fma_(a.z, b.z, SplineKernel<R>::fma_(a.y, b.y, a.x * b.x));
+    return dot(a, b);
+}
+
 // division: exact (reference order) or reciprocal-based (fast mode)
 template <bool FAST> __device__ __forceinline__ float fdiv(float a, float b) { return FAST ? __fdividef(a, b) : a / b; }
 template <bool FAST> __device__ __forceinline__ double fdiv(double a, double b) { return a / b; }

@@ -35,6 +35,7 @@ struct fs_ctx {
     int64_t n_struct = 0;     // particles that take part in the cell structure
     bool have_state = false;
     bool have_lists = false;
+    bool have_cells = false;        // cell tables describe the current sorted order
     float searched_dt = 0.f;
     bool reference_order = false;
     bool include_inactive = false;  // contract lists inactive particles (2D quadratic / hashed)
@@ -80,6 +81,7 @@ struct fs_ctx {
     int* bbox = nullptr;           // device: min xyz, max xyz (cell coordinates)
     int* origin = nullptr;         // device: cell-grid origin used this step
     uint32_t* nbr = nullptr;       // solver lists, slot-major: nbr[s * nbr_stride + k]
+    float* nbr_grad = nullptr;     // per entry: kernel-gradient factor f (gradW = f * (x_i - x_j)), fast mode
     uint32_t* nbr_count = nullptr;
     int nbr_capacity = 0;          // K
     int64_t nbr_stride = 0;

@@ -171,18 +171,22 @@ struct WalkParams {
     int regions;    // number of regions to visit (1 in single-region mode)
     bool candidates_inactive;  // contract lists inactive neighbors
     bool trunc;                // cells by truncation toward zero (hashed 2D order)
+    bool length_test;          // sqrt(dot) <= r instead of dot <= r * r
+    float inv_h, alpha_h;      // kernel constants for the stored gradient factors
     int d0, d1, d2;
     int64_t cells;  // d0 * d1 * d2; each region's table has cells + 1 entries
 };
 
-// predicate of the contract; d = x_i - x_j
+// predicate of the contract; d = x_i - x_j. The 2D searches and every
+// position query but the compressed one test glm::length(d) <= r
+// (HashedNeighborhoodSearch.cpp:56, HashedNeighborhoodSearch3D.cpp:335,
+// QuadraticNeighborhoodSearch3D.cpp:212); the 3D index lists and the
+// compressed position query test dot(d, d) <= r * r
+// (HashedNeighborhoodSearch3D.cpp:173, CompressedNeighbors.cpp:576). In 2D,
+// z == 0 adds an exact +0 to the sum.
 template <typename R> __device__ __forceinline__ bool within(V3<R> d, const WalkParams& w) {
-    if (w.dim == 2) {
-        float q = (float)d.x * (float)d.x + (float)d.y * (float)d.y;
-        return __fsqrt_rn(q) <= w.r;
-    }
-    float q = ((float)d.x * (float)d.x + (float)d.y * (float)d.y) + (float)d.z * (float)d.z;
-    return q <= w.r2;
+    const float q = ((float)d.x * (float)d.x + (float)d.y * (float)d.y) + (float)d.z * (float)d.z;
+    return w.length_test ? __fsqrt_rn(q) <= w.r : q <= w.r2;
 }
 
 // Visits the neighbors of position xi in HashedNeighborhoodSearch3D's order
@@ -248,7 +252,8 @@ __device__ __forceinline__ bool walk_rows(V3<R> xi, const V4<R>* __restrict__ po
             for (uint32_t j = b; j < e; j++) {
                 const V4<R> pj = pos[j];
                 const float d0 = x0 - (float)pj.x, d1 = x1 - (float)pj.y, d2 = x2 - (float)pj.z;
-                if ((d0 * d0 + d1 * d1) + d2 * d2 <= r2) f(j, g);
+                const float q2 = (d0 * d0 + d1 * d1) + d2 * d2;
+                if (q2 <= r2) f(j, g, q2);
             }
         }
     }
@@ -264,19 +269,35 @@ __global__ void __launch_bounds__(128) k_build_lists(int64_t n_owners, const V4<
                                                      const uint8_t* __restrict__ type,
                                                      const uint32_t* __restrict__ cell_start,
                                                      const int* __restrict__ origin, WalkParams w, uint32_t owner_mask,
-                                                     bool rows, uint32_t* __restrict__ nbr, int64_t stride, int K,
-                                                     uint32_t* __restrict__ count, int* __restrict__ status,
-                                                     StepScalars* __restrict__ sc) {
+                                                     bool rows, uint32_t* __restrict__ nbr, float* __restrict__ grad,
+                                                     int64_t stride, int K, uint32_t* __restrict__ count,
+                                                     int* __restrict__ status, StepScalars* __restrict__ sc) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n_owners) return;
     const uint8_t tk = type[k];
     uint32_t c = 0;
+    // the fast-mode kernel gradient factor of a neighbor at squared distance q2:
+    // gradW(d) = f d with f = alpha h poly(q) / |d| (SplineKernel::gradWf)
+    auto factor = [&](float q2) -> float {
+        if (!(q2 > kFltEps * kFltEps)) return 0.f;
+        const float inv = rsqrtf(q2);
+        const float q = q2 * inv * w.inv_h;
+        const float a = 2.f - q, b = 1.f - q;
+        float poly;
+        if (q < 1.f) poly = __fmaf_rn(12.f * b, b, -3.f * a * a);
+        else if (q < 2.f) poly = -3.f * a * a;
+        else return 0.f;
+        return w.alpha_h * poly * inv;
+    };
     if ((owner_mask >> tk) & 1u) {
         const V3<R> xi = xyz<R>(pos[k]);
         bool done = false;
         if (rows) {
-            done = walk_rows<R>(xi, pos, cell_start, origin, w, [&](uint32_t j, int g) {
-                if ((int)c < K) nbr[(int64_t)c * stride + k] = j | (g == 1 ? kBoundaryBit : 0u);
+            done = walk_rows<R>(xi, pos, cell_start, origin, w, [&](uint32_t j, int g, float q2) {
+                if ((int)c < K) {
+                    nbr[(int64_t)c * stride + k] = j | (g == 1 ? kBoundaryBit : 0u);
+                    if (grad) grad[(int64_t)c * stride + k] = factor(q2);
+                }
                 c++;
             });
         }
@@ -284,7 +305,15 @@ __global__ void __launch_bounds__(128) k_build_lists(int64_t n_owners, const V4<
             walk_cells<R>(xi, pos, type, cell_start, origin, w, [&](uint32_t j, uint8_t tj) {
                 // solver lists never carry inactive particles (the solvers skip them)
                 if (tj == FS_TYPE_INACTIVE) return;
-                if ((int)c < K) nbr[(int64_t)c * stride + k] = j | (tj == FS_TYPE_BOUNDARY ? kBoundaryBit : 0u);
+                if ((int)c < K) {
+                    nbr[(int64_t)c * stride + k] = j | (tj == FS_TYPE_BOUNDARY ? kBoundaryBit : 0u);
+                    if (grad) {
+                        const V4<R> pj = pos[j];
+                        const float d0 = (float)xi.x - (float)pj.x, d1 = (float)xi.y - (float)pj.y,
+                                    d2 = (float)xi.z - (float)pj.z;
+                        grad[(int64_t)c * stride + k] = factor((d0 * d0 + d1 * d1) + d2 * d2);
+                    }
+                }
                 c++;
             });
         }
@@ -343,18 +372,76 @@ __global__ void k_csr_fill(int64_t n, const V4<R>* __restrict__ pos, const uint8
     walk_cells<R>(xyz<R>(pos[k]), pos, type, cell_start, origin, w, [&](uint32_t j, uint8_t) { out[o++] = j; });
 }
 
-// neighbors of one arbitrary position (get_neighbors(vec)), sorted space
+// neighbors of one arbitrary position (get_neighbors(vec)), sorted space.
+// skip_cell_min reproduces HashedNeighborhoodSearch3D's position iterator
+// (HashedNeighborhoodSearch3D.cpp:279-344): when it moves on to the next
+// cell it sets the cell's set iterator to begin() and then advances it once
+// more before testing, so in every cell but the first one visited
+// (dx = dy = dz = -1) the member with the smallest particle index is never
+// tested. Members are the cell's non-inactive particles
+// (HashedNeighborhoodSearch3D.cpp:90-101); the index is the host index.
 template <typename R>
 __global__ void k_query_position(V3<R> x, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                                 const uint32_t* __restrict__ cell_start, const int* __restrict__ origin, WalkParams w,
+                                 const uint32_t* __restrict__ hidx, const uint32_t* __restrict__ cell_start,
+                                 const int* __restrict__ origin, WalkParams w, bool skip_cell_min,
                                  uint32_t* __restrict__ out, int64_t cap, unsigned long long* __restrict__ count) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     unsigned long long c = 0;
-    walk_cells<R>(x, pos, type, cell_start, origin, w, [&](uint32_t j, uint8_t) {
-        if ((int64_t)c < cap) out[c] = j;
-        c++;
-    });
+    const int ci[3] = {cell_coord<R>(x.x, w.r, w.trunc), cell_coord<R>(x.y, w.r, w.trunc), cell_coord<R>(x.z, w.r, w.trunc)};
+    const int zr = w.dim == 2 ? 0 : 1;
+    int ordinal = 0;
+    for (int dx = -1; dx <= 1; dx++) {
+        for (int dy = -1; dy <= 1; dy++) {
+            for (int dz = -zr; dz <= zr; dz++, ordinal++) {
+                const int c0 = ci[0] + dx, c1 = ci[1] + dy, c2 = ci[2] + dz;
+                bool cl = false;
+                const int l0 = local_cell(c0, origin[0], w.d0, cl);
+                const int l1 = local_cell(c1, origin[1], w.d1, cl);
+                const int l2 = local_cell(c2, origin[2], w.d2, cl);
+                const int64_t lc = ((int64_t)l2 * w.d1 + l1) * w.d0 + l0;
+                // visits the members of true cell (c0, c1, c2)
+                auto members = [&](auto&& f) {
+                    for (int g = 0; g < w.regions; g++) {
+                        const uint32_t* cs = cell_start + g * (w.cells + 1);
+                        for (uint32_t j = cs[lc], e = cs[lc + 1]; j < e; j++) {
+                            const V4<R> pj = pos[j];
+                            if (cl && (cell_coord<R>(pj.x, w.r, w.trunc) != c0 ||
+                                       cell_coord<R>(pj.y, w.r, w.trunc) != c1 ||
+                                       cell_coord<R>(pj.z, w.r, w.trunc) != c2))
+                                continue;
+                            if (!w.candidates_inactive && type[j] == FS_TYPE_INACTIVE) continue;
+                            f(j, pj);
+                        }
+                    }
+                };
+                uint32_t skip = 0xffffffffu;
+                if (skip_cell_min && ordinal > 0) {
+                    members([&](uint32_t j, const V4<R>&) { skip = min(skip, hidx[j]); });
+                }
+                members([&](uint32_t j, const V4<R>& pj) {
+                    if (hidx[j] == skip) return;
+                    if (!within<R>(x - xyz<R>(pj), w)) return;
+                    if ((int64_t)c < cap) out[c] = j;
+                    c++;
+                });
+            }
+        }
+    }
     *count = c;
+}
+
+// neighbors of one position over every particle, inactive ones included
+// (QuadraticNeighborhoodSearch3D.cpp:199-219,
+// QuadraticNeighborhoodSearchDynamicAllocated.cpp:190-225); unordered, the
+// host sorts. count must be zero before the launch.
+template <typename R>
+__global__ void k_query_all(V3<R> x, int64_t n, const V4<R>* __restrict__ pos, WalkParams w,
+                            uint32_t* __restrict__ out, int64_t cap, unsigned long long* __restrict__ count) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        if (!within<R>(x - xyz<R>(pos[j]), w)) continue;
+        const unsigned long long slot = atomicAdd(count, 1ull);
+        if ((int64_t)slot < cap) out[slot] = (uint32_t)j;
+    }
 }
 
 }  // namespace fsb

@@ -30,6 +30,7 @@ template <typename R> struct SolverConsts {
 
 struct Lists {
     const uint32_t* __restrict__ nbr;
+    const float* __restrict__ grad;  // gradient factors beside the entries (fast mode), or null
     const uint32_t* __restrict__ count;
     int64_t stride;
     int K;
@@ -61,6 +62,50 @@ __device__ __forceinline__ void for_neighbors(const Lists& L, int64_t k, const V
         const uint32_t e = __ldg(&L.nbr[(int64_t)q * L.stride + k]);
         f(e, pos[e & kIndexMask]);
     }
+}
+
+// As for_neighbors, also handing d = x_k - x_j and gradW(d). In the fast mode
+// the search stored the gradient factor f of every entry (gradW = f d), so no
+// pass evaluates the kernel again; otherwise gradW is evaluated here.
+template <typename R, bool FAST, typename F>
+__device__ __forceinline__ void for_neighbors_grad(const Lists& L, int64_t k, const V4<R>* __restrict__ pos, V3<R> xk,
+                                                   const SplineKernel<R>& kern, F&& f) {
+    if (FAST && L.grad != nullptr) {
+        const uint32_t n = L.size(k);
+        const uint32_t* __restrict__ ep = L.nbr + k;
+        const float* __restrict__ gp = L.grad + k;
+        const uint32_t st = (uint32_t)L.stride;
+        uint32_t q = 0;
+        for (; q + kBatch <= n; q += kBatch) {
+            uint32_t e[kBatch];
+            float fg[kBatch];
+            V4<R> p[kBatch];
+#pragma unroll
+            for (int b = 0; b < kBatch; b++) {
+                e[b] = __ldg(ep + (size_t)(q + b) * st);
+                fg[b] = __ldg(gp + (size_t)(q + b) * st);
+            }
+#pragma unroll
+            for (int b = 0; b < kBatch; b++) p[b] = pos[e[b] & kIndexMask];
+#pragma unroll
+            for (int b = 0; b < kBatch; b++) {
+                const V3<R> d = xk - xyz<R>(p[b]);
+                f(e[b], p[b], d, (R)fg[b] * d);
+            }
+        }
+        for (; q < n; q++) {
+            const uint32_t e = __ldg(ep + (size_t)q * st);
+            const R fg = (R)__ldg(gp + (size_t)q * st);
+            const V4<R> pj = pos[e & kIndexMask];
+            const V3<R> d = xk - xyz<R>(pj);
+            f(e, pj, d, fg * d);
+        }
+        return;
+    }
+    for_neighbors<R>(L, k, pos, [&](uint32_t e, const V4<R>& pj) {
+        const V3<R> d = xk - xyz<R>(pj);
+        f(e, pj, d, kern.template grad<FAST>(d));
+    });
 }
 
 template <typename R> struct State {
@@ -111,16 +156,15 @@ template <typename R, bool KAHAN, typename RhoOf>
 __device__ __forceinline__ V3<R> viscosity(int64_t k, const State<R>& s, const Lists& L, const SolverConsts<R>& c,
                                            V3<R> xi, V3<R> vi, RhoOf&& rho_of) {
     Acc3<R, KAHAN> tmp;
-    for_neighbors<R>(L, k, s.pos, [&](uint32_t e, const V4<R>& pj) {
+    for_neighbors_grad<R, KAHAN>(L, k, s.pos, xi, c.kern, [&](uint32_t e, const V4<R>& pj, V3<R> xij, V3<R> g) {
         const uint32_t j = e & kIndexMask;
         const R rj = rho_of(j, e);
         if (rj == R(0)) return;
         const V4<R> vj = s.vel[j];
         const V3<R> vij = vi - xyz<R>(vj);
-        const V3<R> xij = xi - xyz<R>(pj);
-        const R f = KAHAN ? fdiv<true>(pj.w * dot(vij, xij), rj * (dot(xij, xij) + c.visc_eps))
+        const R f = KAHAN ? fdiv<true>(pj.w * dotf<true>(vij, xij), rj * (dotf<true>(xij, xij) + c.visc_eps))
                           : (pj.w / rj) * (dot(vij, xij) / (dot(xij, xij) + c.visc_eps));
-        tmp.add(f * c.kern.template grad<KAHAN>(xij));
+        tmp.add(f * g);
     });
     return c.two_nu * tmp.get();
 }
@@ -233,16 +277,15 @@ __global__ void k_iisph3d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
     Acc3<R, KAHAN> inner;
     Acc3<R, KAHAN> mg;    // sum_j m_j gradW      (single-pass a_ii)
     Acc<R, KAHAN> mg2;    // sum_fluid m_j |gradW|^2
-    for_neighbors<R>(L, k, s.pos, [&](uint32_t e, const V4<R>& pj) {
+    for_neighbors_grad<R, KAHAN>(L, k, s.pos, xk, c.kern, [&](uint32_t e, const V4<R>& pj, V3<R>, V3<R> g) {
         const uint32_t j = e & kIndexMask;
-        const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
         if (!(e & kBoundaryBit)) {
             const V3<R> vsj = xyz<R>(s.vstar[j]);
-            contrib.add(pj.w * dot(vsk - vsj, g));
+            contrib.add(pj.w * dotf<KAHAN>(vsk - vsj, g));
             inner.sub((KAHAN ? pj.w * c.inv_rho0_sq : pj.w / c.rho0_sq) * g);
-            if (!TWO_PASS) mg2.add(pj.w * dot(g, g));
+            if (!TWO_PASS) mg2.add(pj.w * dotf<KAHAN>(g, g));
         } else {
-            contrib.add(pj.w * dot(vsk, g));
+            contrib.add(pj.w * dotf<KAHAN>(vsk, g));
             const R w = c.single_layer ? c.two_gamma * pj.w : R(2) * pj.w;
             inner.sub((KAHAN ? w * c.inv_rho0_sq : w / c.rho0_sq) * g);
         }
@@ -282,9 +325,8 @@ __global__ void k_iisph3d_pressure_acc(int64_t n, State<R> s, Lists L, SolverCon
     const V3<R> xk = xyz<R>(s.pos[k]);
     const R pk = s.p[k];
     Acc3<R, KAHAN> pa;
-    for_neighbors<R>(L, k, s.pos, [&](uint32_t e, const V4<R>& pj) {
+    for_neighbors_grad<R, KAHAN>(L, k, s.pos, xk, c.kern, [&](uint32_t e, const V4<R>& pj, V3<R>, V3<R> g) {
         const uint32_t j = e & kIndexMask;
-        const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
         if (KAHAN) {
             const R f = !(e & kBoundaryBit) ? pj.w * (pk + s.p[j])
                                             : (c.single_layer ? c.two_gamma : R(2)) * pj.w * pk;
@@ -318,11 +360,10 @@ __global__ void k_iisph3d_pressure_update(int64_t n, State<R> s, Lists L, Solver
         const V3<R> xk = xyz<R>(s.pos[k]);
         const V3<R> ak = xyz<R>(s.acc[k]);
         Acc<R, KAHAN> ap;
-        for_neighbors<R>(L, k, s.pos, [&](uint32_t e, const V4<R>& pj) {
+        for_neighbors_grad<R, KAHAN>(L, k, s.pos, xk, c.kern, [&](uint32_t e, const V4<R>& pj, V3<R>, V3<R> g) {
             const uint32_t j = e & kIndexMask;
-            const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
-            if (!(e & kBoundaryBit)) ap.add(pj.w * dot(ak - xyz<R>(s.acc[j]), g));
-            else ap.add(pj.w * dot(ak, g));
+            if (!(e & kBoundaryBit)) ap.add(pj.w * dotf<KAHAN>(ak - xyz<R>(s.acc[j]), g));
+            else ap.add(pj.w * dotf<KAHAN>(ak, g));
         });
         const R Ap = ap.get() * (dt * dt);
         const V4<R> vs = s.vstar[k];   // w: source term
@@ -529,12 +570,8 @@ __global__ void k_sesph_accel(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
     npa = npa + viscosity<R, KAHAN>(k, s, L, c, xk, xyz<R>(s.vel[k]),
                                     [&](uint32_t j, uint32_t) -> R { return s.rho[j]; });
     Acc3<R, KAHAN> pa;
-    const uint32_t nn = L.size(k);
-    for (uint32_t q = 0; q < nn; q++) {
-        const uint32_t e = L.at(k, q);
+    for_neighbors_grad<R, KAHAN>(L, k, s.pos, xk, c.kern, [&](uint32_t e, const V4<R>& pj, V3<R>, V3<R> g) {
         const uint32_t j = e & kIndexMask;
-        const V4<R> pj = s.pos[j];
-        const V3<R> g = c.kern.template grad<KAHAN>(xk - xyz<R>(pj));
         if (e & kBoundaryBit) {
             const R f = -pk.w * (pdd + pdd);
             if (c.single_layer) pa.add((f * g) * c.gamma2);
@@ -544,7 +581,7 @@ __global__ void k_sesph_accel(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
             const R pddj = rj == R(0) ? R(0) : fdiv<KAHAN>(s.p[j], rj * rj);
             pa.add((-pj.w * (pdd + pddj)) * g);
         }
-    }
+    });
     s.acc[k] = v4<R>(pa.get() + npa, R(0));
 }
 

@@ -311,10 +311,13 @@ class FluidSolverBase:
     def get_neighbors_of_position(self, position, cap: int = 4096) -> np.ndarray:
         pos = np.zeros(3, np.float32)
         pos[:self.DIM] = np.asarray(position, np.float32)[:self.DIM]
-        out = np.zeros(cap, np.int64)
         cnt = ctypes.c_int64()
-        F.check(F.lib().fs_query_position(self.ctx, pos.ctypes.data, out.ctypes.data, cap, ctypes.byref(cnt)))
-        return out[:min(cnt.value, cap)]
+        while True:
+            out = np.zeros(cap, np.int64)
+            F.check(F.lib().fs_query_position(self.ctx, pos.ctypes.data, out.ctypes.data, cap, ctypes.byref(cnt)))
+            if cnt.value <= cap:
+                return out[:cnt.value]
+            cap = cnt.value
 
     # ---- state ---------------------------------------------------------
     def collection(self, iisph: bool = False) -> ParticleCollection:

@@ -195,8 +195,16 @@ fs_status fs_find_neighbors(fs_ctx* ctx);
 /* Neighbor lists of the last search in host-index space, each list ascending:
  * offsets has n+1 entries; indices may be NULL to query *total first. */
 fs_status fs_get_neighbors_csr(fs_ctx* ctx, int64_t* offsets, int64_t* indices, int64_t* total);
-/* Neighbors of an arbitrary position (get_neighbors(vec)); ascending host indices.
- * Writes min(count, cap) indices and the full count to *count. */
+/* Neighbors of an arbitrary position (NeighborhoodInterface::get_neighbors(vec),
+ * NeighborhoodInterface.cpp:71-80); ascending host indices, per contract:
+ * hashed-3d walks the cells of the last search, skips inactive particles and,
+ * like HashedNeighborhoodSearch3D.cpp:279-344, the smallest-index member of
+ * every cell after the first; compressed-3d walks the cells, skips inactive
+ * particles and tests dot <= r*r; hashed-2d walks the cells; the quadratic
+ * contracts test every particle. compact-hashing-2d has none (FS_ERR_INVALID,
+ * as the reference throws). Writes min(count, cap) indices (which ones is
+ * unspecified when count > cap) and the full count to *count. The cell walks
+ * need a search after the last upload (FS_ERR_STATE otherwise). */
 fs_status fs_query_position(fs_ctx* ctx, const float* position, int64_t* out, int64_t cap, int64_t* count);
 
 /* The solver's timestep on the lists of the preceding fs_find_neighbors

@@ -75,6 +75,57 @@ def search(kind: str, position, radius: float, type_=None):
     return off, idx[:total], ok
 
 
+def query_position(kind: str, position, radius: float, q, type_=None) -> np.ndarray:
+    """Sorted host indices that NeighborhoodInterface::get_neighbors(position)
+    yields for query point q, per contract (float32 arithmetic throughout):
+
+    * hashed-3d (HashedNeighborhoodSearch3D.cpp:279-344): the 27 cells
+      around floor(q / r) (:63-66), members are the non-inactive particles of
+      a cell (:90-101), test glm::length(q - x_j) <= r (:335). Entering every
+      cell after the first one visited (dx = dy = dz = -1), the iterator is
+      advanced once more before its first test, so that cell's member with
+      the smallest index is skipped.
+    * quadratic-3d (QuadraticNeighborhoodSearch3D.cpp:199-219): every
+      particle, inactive ones included, length test.
+    * compressed-3d (CompressedNeighbors.cpp:536-590): non-inactive
+      particles (:177-178) of the 27 cells, dot(x_j - q, x_j - q) <= r * r.
+    * hashed-2d (HashedNeighborhoodSearch.cpp:290-340), quadratic-2d
+      (QuadraticNeighborhoodSearchDynamicAllocated.cpp:190-225): every
+      particle, inactive ones included, length test.
+    * compact-hashing-2d has none (CompactHashingNeighborhoodSearch.cpp:92-94
+      throws "Not implemented"): ValueError.
+    """
+    pos = np.ascontiguousarray(position, np.float32)
+    q = np.asarray(q, np.float32)
+    r = np.float32(radius)
+    n, dim = pos.shape
+    typ = np.zeros(n, np.uint8) if type_ is None else np.asarray(type_, np.uint8)
+    if kind == "compact-hashing-2d":
+        raise ValueError("compact hashing implements no position query")
+    d = pos - q[:dim]
+    dd = d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]
+    if dim == 3:
+        dd = dd + d[:, 2] * d[:, 2]
+    if kind == "compressed-3d":
+        hit = (dd <= r * r) & (typ != 2)
+    else:
+        hit = np.sqrt(dd) <= r
+    if kind == "hashed-3d":
+        hit &= typ != 2
+        cq = np.floor(q[:3] / r).astype(np.int64)
+        cell = np.floor(pos / r).astype(np.int64)
+        ordinal = 0
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    if ordinal > 0:
+                        m = np.nonzero((cell == cq + np.array([dx, dy, dz])).all(1) & (typ != 2))[0]
+                        if len(m):
+                            hit[m.min()] = False
+                    ordinal += 1
+    return np.nonzero(hit)[0].astype(np.int64)
+
+
 def config(solver: str, search: str, rest_density=1.0, gravity=9.81, particle_size=1.0, stiffness=1000.0,
            viscosity=0.01, single_layer=True, gamma1=1.1, gamma2=1.1, max_err=0.001, min_it=2, max_it=100, omega=0.5,
            gamma=0.7, timestep=0.005, lambda_v=0.4, lambda_a=0.25) -> np.ndarray:

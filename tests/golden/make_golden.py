@@ -171,13 +171,33 @@ def solver_fixture():
     np.savez_compressed(os.path.join(OUT, "solvers.npz"), **out)
 
 
+def position_query_fixture():
+    """NeighborhoodInterface::get_neighbors(position) of every contract that
+    has one, on random points with a third of them inactive."""
+    out = {}
+    rng = np.random.default_rng(14)
+    for dim, kinds in ((3, ("hashed-3d", "quadratic-3d", "compressed-3d")), (2, ("hashed-2d", "quadratic-2d"))):
+        pos = (rng.random((3000, dim)) * 10).astype(np.float32)
+        typ = rng.integers(0, 3, 3000).astype(np.uint8)
+        queries = (rng.random((40, dim)) * 10).astype(np.float32)
+        out[f"pos{dim}"], out[f"type{dim}"], out[f"queries{dim}"] = pos, typ, queries
+        for kind in kinds:
+            s = R.RefSearch(kind, pos, 1.0, typ)
+            assert s.find()
+            res = [np.sort(s.query(q)) for q in queries]
+            s.close()
+            out[f"{kind}/offsets"] = np.concatenate([[0], np.cumsum([len(a) for a in res])]).astype(np.int64)
+            out[f"{kind}/indices"] = np.concatenate(res).astype(np.int64)
+    np.savez_compressed(os.path.join(OUT, "position_queries.npz"), **out)
+
+
 if __name__ == "__main__":
     if not R.available():
         sys.exit("oracle/_ref is not built; run `make -C oracle/ref` where the reference checkout is available")
-    kernel_fixture()
-    cfl_fixture()
-    search_fixture()
-    solver_fixture()
+    fixtures = {"kernel": kernel_fixture, "cfl": cfl_fixture, "search": search_fixture, "solvers": solver_fixture,
+                "position_queries": position_query_fixture}
+    for name in sys.argv[1:] or fixtures:
+        fixtures[name]()
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")

@@ -140,15 +140,39 @@ def test_gaussian_blobs_match_oracle(c_oracle):
     assert np.array_equal(idx, sorted_csr(ro, ri)[1])
 
 
-def test_position_queries_match_oracle(c_oracle):
+@pytest.mark.parametrize("dim,kind", [(3, "hashed-3d"), (3, "quadratic-3d"), (3, "compressed-3d"), (2, "hashed-2d"),
+                                      (2, "quadratic-2d")])
+def test_position_queries_match_reference(golden, dim, kind):
+    """get_neighbors(position) of every contract against the reference's
+    (fixtures from its sources): inactive particles, the length/dot
+    predicates and hashed-3d's skipped cell minimum."""
+    g = golden["position_queries"]
+    pos, typ, queries = g[f"pos{dim}"], g[f"type{dim}"], g[f"queries{dim}"]
+    off, idx = g[f"{kind}/offsets"], g[f"{kind}/indices"]
+    ns = NeighborhoodSearch(kind, 1.0)
+    ns.data.collection = ParticleCollection(position=pos, type=typ)
+    ns.find_neighbors()
+    for i, q in enumerate(queries):
+        assert ns.get_neighbors_of_position(q).tolist() == idx[off[i]:off[i + 1]].tolist(), (kind, i)
+    ns.close()
+
+
+def test_position_queries_at_scale(c_oracle):
+    """20k points: the device query against the oracle's restatement."""
     rng = np.random.default_rng(4)
     pos = rng.random((20000, 3)).astype(np.float32)
     ns = NeighborhoodSearch("hashed-3d", 0.05)
     ns.data.collection = ParticleCollection(position=pos)
     ns.find_neighbors()
     for q in rng.random((20, 3)).astype(np.float32):
-        got = ns.get_neighbors_of_position(q)
-        d = pos - q
-        dd = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
-        assert got.tolist() == np.nonzero(dd <= np.float32(0.05) * np.float32(0.05))[0].tolist()
+        assert ns.get_neighbors_of_position(q).tolist() == c_oracle.query_position("hashed-3d", pos, 0.05, q).tolist()
+    ns.close()
+
+
+def test_compact_hashing_position_query_is_rejected():
+    ns = NeighborhoodSearch("compact-hashing-2d", 1.0)
+    ns.data.collection = ParticleCollection(position=np.zeros((4, 2), np.float32))
+    ns.find_neighbors()
+    with pytest.raises(FluidSolverError):
+        ns.get_neighbors_of_position(np.zeros(2, np.float32))
     ns.close()

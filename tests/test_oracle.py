@@ -198,3 +198,40 @@ def test_oracle_against_compiled_reference(ref_oracle, c_oracle):
         assert int(o[2]) == r["iterations"]
         for f in ("position", "velocity", "density", "pressure"):
             assert bits_equal(getattr(st, f), s[f]), f
+
+
+POSITION_QUERY_KINDS = [(3, "hashed-3d"), (3, "quadratic-3d"), (3, "compressed-3d"), (2, "hashed-2d"),
+                        (2, "quadratic-2d")]
+
+
+@pytest.mark.parametrize("dim,kind", POSITION_QUERY_KINDS)
+def test_position_query_oracle_matches_reference(golden, c_oracle, dim, kind):
+    """The oracle's get_neighbors(position) against the reference's, fixtures
+    made from the reference's sources: inactive particles, the length/dot
+    predicates and hashed-3d's skipped cell minimum."""
+    g = golden["position_queries"]
+    pos, typ, queries = g[f"pos{dim}"], g[f"type{dim}"], g[f"queries{dim}"]
+    off, idx = g[f"{kind}/offsets"], g[f"{kind}/indices"]
+    for i, q in enumerate(queries):
+        got = c_oracle.query_position(kind, pos, 1.0, q, typ)
+        assert got.tolist() == idx[off[i]:off[i + 1]].tolist(), (kind, i)
+
+
+def test_position_query_quirk_is_pinned(golden, c_oracle):
+    """hashed-3d drops members that a plain radius test keeps (and only
+    those): the fixture would not pin the quirk otherwise."""
+    g = golden["position_queries"]
+    pos, typ, queries = g["pos3"], g["type3"], g["queries3"]
+    off, idx = g["hashed-3d/offsets"], g["hashed-3d/indices"]
+    dropped = 0
+    for i, q in enumerate(queries):
+        full = set(c_oracle.query_position("compressed-3d", pos, 1.0, q, typ).tolist())
+        got = set(idx[off[i]:off[i + 1]].tolist())
+        assert got <= full
+        dropped += len(full - got)
+    assert dropped > 0
+
+
+def test_compact_hashing_has_no_position_query(c_oracle):
+    with pytest.raises(ValueError):
+        c_oracle.query_position("compact-hashing-2d", np.zeros((2, 2), np.float32), 1.0, np.zeros(2, np.float32))
