@@ -22,6 +22,8 @@ FS_ERR_CUDA = 5
 FS_ERR_NO_DEVICE = 6
 FS_ERR_STATE = 7
 
+FS_QUERY_NOALLOC_MAX = 65536  # include/fluidsolver_b200.h
+
 FS_SOLVER_NONE = 0
 FS_SOLVER_SESPH_2D = 1
 FS_SOLVER_SESPH_3D = 2
@@ -51,6 +53,7 @@ EXPORTED_SYMBOLS = (
     "fs_abi_version", "fs_last_error", "fs_params_default", "fs_create", "fs_destroy", "fs_set_params",
     "fs_upload", "fs_download", "fs_find_neighbors", "fs_get_neighbors_csr", "fs_query_position", "fs_solve_step", "fs_step",
     "fs_run", "fs_last_phase_times", "fs_stream", "fs_launch_count", "fs_batch_create", "fs_batch_run",
+    "fs_query_position_noalloc",
 )
 
 
@@ -119,6 +122,7 @@ def lib() -> ctypes.CDLL:
     L.fs_find_neighbors.argtypes = [ctx_p]
     L.fs_get_neighbors_csr.argtypes = [ctx_p, c_void_p, c_void_p, POINTER(c_int64)]
     L.fs_query_position.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
+    L.fs_query_position_noalloc.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
     L.fs_step.argtypes = [ctx_p, c_float, POINTER(FsStepStats)]
     L.fs_solve_step.argtypes = [ctx_p, c_float, POINTER(FsStepStats)]
     L.fs_run.argtypes = [ctx_p, c_int32, c_float, POINTER(FsStepStats)]
@@ -131,7 +135,7 @@ def lib() -> ctypes.CDLL:
     L.fs_batch_run.argtypes = [ctx_p, c_int32, c_float, c_void_p]
     for name in ("fs_create", "fs_destroy", "fs_set_params", "fs_upload", "fs_download", "fs_find_neighbors",
                  "fs_get_neighbors_csr", "fs_query_position", "fs_solve_step", "fs_step", "fs_run", "fs_last_phase_times",
-                 "fs_batch_create", "fs_batch_run"):
+                 "fs_batch_create", "fs_batch_run", "fs_query_position_noalloc"):
         getattr(L, name).restype = c_int32
     _lib = L
     return L

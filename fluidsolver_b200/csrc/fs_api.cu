@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -1379,3 +1380,164 @@ fs_status fs_batch_run(fs_ctx*, int32_t, float, fs_step_stats*) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Position query that allocates nothing (fs_query_position_noalloc).
+//
+// Who cannot allocate: code that asks for neighbors while a simulation is
+// running -- an entity or sensor hook between two steps, a render or
+// telemetry callback on its own thread. cudaFree waits for the whole device,
+// so it stalls a step queued on any stream, and cudaMalloc can do the same;
+// on a device whose memory is budgeted to the particle buffers a fresh
+// allocation can also just fail halfway through a run; and a host heap call
+// adds unbounded latency to a callback with a frame deadline. So this path
+// works from one fixed device array per device, compiled into the library,
+// and copies straight into the caller's buffer. It uses no cudaMalloc,
+// cudaFree or host-side allocation; even its error messages fit the error
+// string's inline storage.
+//
+// Shared state: one array per device, used by every context on it. Calls
+// that overlap in time on one device race on the array (the count and the
+// results). Set-up: the first call on a device, with that device current,
+// resolves the array's address with cudaGetSymbolAddress and keeps it; that
+// first call should come before any stream capture begins.
+// ---------------------------------------------------------------------------
+
+// [0]: neighbor count (zeroed before every launch); [1 ..]: host indices
+static __device__ __align__(256) unsigned long long g_query_scratch[1 + FS_QUERY_NOALLOC_MAX];
+
+namespace {
+
+constexpr int kNoAllocDevices = 64;
+std::mutex g_query_scratch_mutex;
+unsigned long long* g_query_scratch_ptr[kNoAllocDevices] = {};
+
+// k_query_position writing host indices into the fixed array
+template <typename R>
+__global__ void k_query_cells_noalloc(V3<R> x, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
+                                      const uint32_t* __restrict__ hidx, const uint32_t* __restrict__ cell_start,
+                                      const int* __restrict__ origin, WalkParams w, bool skip_cell_min,
+                                      unsigned long long* __restrict__ scratch, int64_t cap) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long c = 0;
+    const int ci[3] = {cell_coord<R>(x.x, w.r, w.trunc), cell_coord<R>(x.y, w.r, w.trunc), cell_coord<R>(x.z, w.r, w.trunc)};
+    const int zr = w.dim == 2 ? 0 : 1;
+    int ordinal = 0;
+    for (int dx = -1; dx <= 1; dx++) {
+        for (int dy = -1; dy <= 1; dy++) {
+            for (int dz = -zr; dz <= zr; dz++, ordinal++) {
+                const int c0 = ci[0] + dx, c1 = ci[1] + dy, c2 = ci[2] + dz;
+                bool cl = false;
+                const int l0 = local_cell(c0, origin[0], w.d0, cl);
+                const int l1 = local_cell(c1, origin[1], w.d1, cl);
+                const int l2 = local_cell(c2, origin[2], w.d2, cl);
+                const int64_t lc = ((int64_t)l2 * w.d1 + l1) * w.d0 + l0;
+                auto members = [&](auto&& f) {
+                    for (int g = 0; g < w.regions; g++) {
+                        const uint32_t* cs = cell_start + g * (w.cells + 1);
+                        for (uint32_t j = cs[lc], e = cs[lc + 1]; j < e; j++) {
+                            const V4<R> pj = pos[j];
+                            if (cl && (cell_coord<R>(pj.x, w.r, w.trunc) != c0 ||
+                                       cell_coord<R>(pj.y, w.r, w.trunc) != c1 ||
+                                       cell_coord<R>(pj.z, w.r, w.trunc) != c2))
+                                continue;
+                            if (!w.candidates_inactive && type[j] == FS_TYPE_INACTIVE) continue;
+                            f(j, pj);
+                        }
+                    }
+                };
+                uint32_t skip = 0xffffffffu;
+                if (skip_cell_min && ordinal > 0) members([&](uint32_t j, const V4<R>&) { skip = min(skip, hidx[j]); });
+                members([&](uint32_t j, const V4<R>& pj) {
+                    if (hidx[j] == skip || !within<R>(x - xyz<R>(pj), w)) return;
+                    if ((int64_t)c < cap) scratch[1 + c] = hidx[j];
+                    c++;
+                });
+            }
+        }
+    }
+    scratch[0] = c;
+}
+
+// k_query_all writing host indices into the fixed array; scratch[0] must be
+// zero at the launch
+template <typename R>
+__global__ void k_query_all_noalloc(V3<R> x, int64_t n, const V4<R>* __restrict__ pos,
+                                    const uint32_t* __restrict__ hidx, WalkParams w,
+                                    unsigned long long* __restrict__ scratch, int64_t cap) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        if (!within<R>(x - xyz<R>(pos[j]), w)) continue;
+        const unsigned long long slot = atomicAdd(&scratch[0], 1ull);
+        if ((int64_t)slot < cap) scratch[1 + slot] = hidx[j];
+    }
+}
+
+// the fixed array of the current device (resolved once per device)
+fs_status query_scratch(int device, unsigned long long** out) {
+    if (device < 0 || device >= kNoAllocDevices) return fail(FS_ERR_INVALID, "bad device");
+    std::lock_guard<std::mutex> lock(g_query_scratch_mutex);
+    if (!g_query_scratch_ptr[device]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_query_scratch) != cudaSuccess || !p) return fail(FS_ERR_CUDA, "CUDA symbol");
+        g_query_scratch_ptr[device] = (unsigned long long*)p;
+    }
+    *out = g_query_scratch_ptr[device];
+    return FS_OK;
+}
+
+template <typename R>
+bool launch_query_noalloc(fs_ctx* c, const float* position, const WalkParams& w, bool all, bool skip,
+                          unsigned long long* scratch, int64_t cap) {
+    const State<R> s = state_of<R>(c);
+    const V3<R> x = v3<R>(position[0], position[1], c->dim == 3 ? position[2] : 0.0f);
+    c->launches++;
+    if (all) {
+        const int g = (int)std::min<int64_t>((c->n + kBlock - 1) / kBlock, 1184);
+        k_query_all_noalloc<R><<<g, kBlock, 0, c->stream>>>(x, c->n, s.pos, s.hidx, w, scratch, cap);
+    } else {
+        k_query_cells_noalloc<R><<<1, 32, 0, c->stream>>>(x, s.pos, s.type, s.hidx, c->cell_start, c->origin, w, skip,
+                                                          scratch, cap);
+    }
+    return cudaGetLastError() == cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" fs_status fs_query_position_noalloc(fs_ctx* c, const float* position, int64_t* out, int64_t cap,
+                                               int64_t* count) {
+    // every message below fits std::string's inline buffer: no heap use
+    if (!c || !position || (cap > 0 && !out)) return fail(FS_ERR_INVALID, "null argument");
+    if (cap < 0) return fail(FS_ERR_INVALID, "cap < 0");
+    if (cap > FS_QUERY_NOALLOC_MAX) return fail(FS_ERR_INVALID, "cap > 65536");
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles");
+    const int search = c->prm.search;
+    if (search == FS_SEARCH_COMPACT_2D) return fail(FS_ERR_INVALID, "not supported");
+    const bool all = search == FS_SEARCH_QUADRATIC_2D || search == FS_SEARCH_QUADRATIC_3D;
+    if (!all && !c->have_cells) return fail(FS_ERR_STATE, "search first");
+    if (count) *count = 0;
+    if (c->n == 0) return FS_OK;
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(FS_ERR_CUDA, "CUDA device");
+    unsigned long long* scratch = nullptr;
+    FS_TRY(query_scratch(c->device, &scratch));
+    WalkParams w = walk_of(c, false);
+    w.length_test = search != FS_SEARCH_COMPRESSED_3D;
+    const bool skip = search == FS_SEARCH_HASHED_3D;
+    if (cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), c->stream) != cudaSuccess)
+        return fail(FS_ERR_CUDA, "CUDA memset");
+    const bool launched = c->precision == FS_PRECISION_FP64
+                              ? launch_query_noalloc<double>(c, position, w, all, skip, scratch, cap)
+                              : launch_query_noalloc<float>(c, position, w, all, skip, scratch, cap);
+    if (!launched) return fail(FS_ERR_CUDA, "CUDA launch");
+    unsigned long long cnt = 0;
+    if (cudaMemcpyAsync(&cnt, scratch, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return fail(FS_ERR_CUDA, "CUDA copy");
+    const int64_t m = std::min<int64_t>((int64_t)cnt, cap);
+    if (m > 0 && (cudaMemcpyAsync(out, scratch + 1, sizeof(int64_t) * (size_t)m, cudaMemcpyDeviceToHost,
+                                  c->stream) != cudaSuccess ||
+                  cudaStreamSynchronize(c->stream) != cudaSuccess))
+        return fail(FS_ERR_CUDA, "CUDA copy");
+    std::sort(out, out + m);
+    if (count) *count = (int64_t)cnt;
+    return FS_OK;
+}

@@ -207,6 +207,22 @@ fs_status fs_get_neighbors_csr(fs_ctx* ctx, int64_t* offsets, int64_t* indices, 
  * need a search after the last upload (FS_ERR_STATE otherwise). */
 fs_status fs_query_position(fs_ctx* ctx, const float* position, int64_t* out, int64_t cap, int64_t* count);
 
+/* fs_query_position without any allocation. It has no counterpart in the
+ * reference: libFluid's get_neighbors(vec) hands out a lazy iterator.
+ * Results and errors are those of fs_query_position. The difference is the
+ * working memory: one fixed device array per device (compiled into the
+ * library), and the caller's own buffer. Nothing goes through cudaMalloc,
+ * cudaFree or a host-side allocator. Limits:
+ *   - cap may be at most FS_QUERY_NOALLOC_MAX; a larger cap is rejected with
+ *     FS_ERR_INVALID before anything runs;
+ *   - the fixed array is shared by every context on a device, so calls that
+ *     overlap in time on one device (two host threads) race on it;
+ *   - the first call on each device resolves the array's address, so make
+ *     that first call before any stream capture begins. */
+#define FS_QUERY_NOALLOC_MAX 65536
+fs_status fs_query_position_noalloc(fs_ctx* ctx, const float* position, int64_t* out, int64_t cap,
+                                    int64_t* count);
+
 /* The solver's timestep on the lists of the preceding fs_find_neighbors
  * (IFluidSolverBase::execute_simulation_step, IFluidSolver.hpp:30); the
  * CFL-clamped time step is returned in stats->actual_dt. desired_dt <= 0 uses
