@@ -11,6 +11,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "fs_context.cuh"
@@ -139,16 +140,29 @@ template <typename R> SolverConsts<R> consts_of(fs_ctx* c) {
 
 // The compensated-sum (fast) mode stores every list entry's kernel-gradient
 // factor next to it; the exact modes evaluate the kernel in each pass.
-bool fast_lists(const fs_ctx* c) { return c->precision == FS_PRECISION_FP32_KAHAN && !c->reference_order; }
+// the 3D IISPH fast path runs on tile lists (fs_tiles.cuh)
+bool tiled_mode(const fs_ctx* c) {
+    return c->precision == FS_PRECISION_FP32_KAHAN && !c->reference_order && c->dim == 3 &&
+           c->prm.solver == FS_SOLVER_IISPH_3D;
+}
 
 Lists lists_of(fs_ctx* c) {
     Lists L;
     L.nbr = c->nbr;
     L.count = c->nbr_count;
-    L.grad = fast_lists(c) ? c->nbr_grad : nullptr;
     L.stride = c->nbr_stride;
     L.K = c->nbr_capacity;
     return L;
+}
+
+TileLists tile_lists_of(fs_ctx* c) {
+    TileLists T;
+    T.desc = c->tile_desc;
+    T.ent = c->tile_ent;
+    T.count = c->nbr_count;
+    T.stride = c->tile_stride;
+    T.K = c->nbr_capacity;
+    return T;
 }
 
 WalkParams walk_of(fs_ctx* c, bool for_solver) {
@@ -160,8 +174,6 @@ WalkParams walk_of(fs_ctx* c, bool for_solver) {
     w.candidates_inactive = c->include_inactive && !for_solver;
     w.trunc = c->truncate_cells;
     w.length_test = c->dim == 2;
-    w.inv_h = 1.0f / c->kernel_h;
-    w.alpha_h = c->kernel_alpha * c->kernel_h;
     w.d0 = c->dims[0];
     w.d1 = c->dims[1];
     w.d2 = c->dims[2];
@@ -226,7 +238,7 @@ void clear_graphs(fs_ctx* c) {
 fs_status free_all(fs_ctx* c) {
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc[0], c->acc[1], c->ext[0], c->ext[1],
                     c->rho[0], c->rho[1], c->p[0], c->p[1], c->type[0], c->type[1], c->hidx[0], c->hidx[1],
-                    c->rho_prev, c->vstar, c->anp, c->err, c->nbr_grad, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
+                    c->rho_prev, c->vstar, c->anp, c->err, c->tile_desc, c->tile_ent, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
                     c->perm[0], c->perm[1], c->cub_temp, c->cell_start, c->cell_counts, c->bbox, c->origin, c->nbr, c->nbr_count,
                     c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->scalars};
     for (void* q : ptrs)
@@ -253,21 +265,31 @@ fs_status ensure_staging(fs_ctx* c, size_t bytes) {
 
 fs_status ensure_lists(fs_ctx* c, int K) {
     const int64_t stride = ((c->cap + 31) / 32) * 32;
-    if (c->nbr && c->nbr_capacity >= K && c->nbr_stride == stride) return FS_OK;
+    const bool tiled = tiled_mode(c);
+    if (tiled) K = (K + 7) & ~7;   // tile lists hold octets of entries
+    if (c->nbr && c->nbr_capacity >= K && c->nbr_stride == stride && (!tiled || c->tile_ent)) return FS_OK;
     clear_graphs(c);
     if (c->nbr) cudaFree(c->nbr);
-    if (c->nbr_grad) cudaFree(c->nbr_grad);
+    if (c->tile_ent) cudaFree(c->tile_ent);
+    if (c->tile_desc) cudaFree(c->tile_desc);
     c->nbr = nullptr;
-    c->nbr_grad = nullptr;
+    c->tile_ent = nullptr;
+    c->tile_desc = nullptr;
     FS_TRY(dalloc(&c->nbr, (size_t)K * stride));
-    if (fast_lists(c)) FS_TRY(dalloc(&c->nbr_grad, (size_t)K * stride));
+    if (tiled) {
+        const int64_t tiles = (c->cap + kTileOwners - 1) / kTileOwners;
+        c->tile_stride = tiles * kTileOwners;
+        FS_TRY(dalloc(&c->tile_desc, (size_t)tiles));
+        FS_TRY(dalloc(&c->tile_ent, (size_t)(K / 8) * c->tile_stride));
+        FS_CUDA(cudaFuncSetAttribute(k_build_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tile_build_smem(K)));
+        FS_CUDA(set_tile_pass_smem(K));
+    }
     c->nbr_capacity = K;
     c->nbr_stride = stride;
     return FS_OK;
 }
 
-// cell-grid dims from the host positions: bounding box + margin, clamped to
-// 1024 per axis and to a total table size
 // Grid dims from the cell bounding box of the uploaded particles (lo > hi on
 // an axis: no finite coordinate there): the box plus a margin of a quarter
 // of its extent (at least 4 cells) on each side, shrunk until the grid has
@@ -559,10 +581,23 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
         WalkParams w = walk_of(c, true);
         const uint32_t owners = 1u << FS_TYPE_NORMAL;
         const bool rows = !c->reference_order && c->dim == 3;
-        c->launches++;
-        k_build_lists<R><<<grid_for(c->n_owners), kBlock, 0, st>>>(c->n_owners, s.pos, s.type, c->cell_start, c->origin,
-                                                                    w, owners, rows, c->nbr, c->nbr_grad, c->nbr_stride,
-                                                                    c->nbr_capacity, c->nbr_count, c->status, c->scalars);
+        bool built = false;
+        if constexpr (std::is_same<R, float>::value) {
+            if (tiled_mode(c) && c->n_owners > 0) {
+                const int64_t tiles = (c->n_owners + kTileOwners - 1) / kTileOwners;
+                c->launches++;
+                k_build_tiles<<<(unsigned)tiles, kTileOwners, tile_build_smem(c->nbr_capacity), st>>>(
+                    c->n_owners, s.pos, s.type, c->cell_start, c->origin, w, c->tile_desc, c->tile_ent,
+                    c->tile_stride, c->nbr, c->nbr_stride, c->nbr_capacity, c->nbr_count, c->status, c->scalars);
+                built = true;
+            }
+        }
+        if (!built) {
+            c->launches++;
+            k_build_lists<R><<<grid_for(c->n_owners), kBlock, 0, st>>>(
+                c->n_owners, s.pos, s.type, c->cell_start, c->origin, w, owners, rows, c->nbr, c->nbr_stride,
+                c->nbr_capacity, c->nbr_count, c->status, c->scalars);
+        }
         FS_CUDA(cudaGetLastError());
         if (c->sort_lists_by_host) {
     c->launches++;
@@ -672,7 +707,49 @@ fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_t
     return FS_OK;
 }
 
+// the IISPH 3D step on tile lists (fs_tiles.cuh)
+fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
+    cudaStream_t st = c->stream;
+    const int64_t n = c->n, nf = c->n_owners;
+    const unsigned tiles = (unsigned)((nf + kTileOwners - 1) / kTileOwners);
+    const unsigned rest = (unsigned)((n - nf + kPassThreads - 1) / kPassThreads);
+    const SolverConsts<float> k = consts_of<float>(c);
+    const Lists L = lists_of(c);
+    const TileLists T = tile_lists_of(c);
+    std::swap(c->rho[c->cur], c->rho_prev);
+    State<float> s = state_of<float>(c);
+    FS_TRY(mark(c, 1, st));
+    c->launches++;
+    k_tile_iisph3d_l1<<<tiles + rest, kPassThreads, tile_pass_smem(36, T.K), st>>>(nf, n, tiles, s, T, L, k, c->scalars,
+                                                                           c->status);
+    FS_CUDA(cudaGetLastError());
+    FS_TRY(mark(c, 2, st));
+    c->launches++;
+    k_tile_iisph3d_l2<<<tiles, kPassThreads, tile_pass_smem(32, T.K), st>>>(nf, s, T, L, k, c->scalars, c->status);
+    FS_CUDA(cudaGetLastError());
+    FS_TRY(mark(c, 3, st));
+    FS_TRY(enqueue_pressure_loop(c, capture, false, true, [&](cudaStream_t bs) {
+        c->launches += 2;
+        k_tile_iisph3d_pressure_acc<<<tiles, kPassThreads, tile_pass_smem(20, T.K), bs>>>(nf, s, T, L, k, c->scalars,
+                                                                                 c->status);
+        k_tile_iisph3d_pressure_update<<<tiles, kPassThreads, tile_pass_smem(32, T.K), bs>>>(nf, s, T, L, k, c->scalars,
+                                                                                    c->status);
+    }));
+    FS_TRY(mark(c, 4, st));
+    c->launches++;
+    k_cfl<<<1, 1, 0, st>>>(c->scalars, c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
+                           c->status);
+    c->launches++;
+    k_iisph3d_integrate<float><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
+    FS_CUDA(cudaGetLastError());
+    FS_TRY(mark(c, 5, st));
+    return FS_OK;
+}
+
 template <typename R, bool KAHAN> fs_status step_iisph3d(fs_ctx* c, bool capture) {
+    if constexpr (std::is_same<R, float>::value && KAHAN) {
+        if (tiled_mode(c) && c->n_owners > 0) return step_iisph3d_tiled(c, capture);
+    }
     cudaStream_t st = c->stream;
     const int64_t n = c->n, no = c->n_owners;
     const SolverConsts<R> k = consts_of<R>(c);
@@ -1071,7 +1148,7 @@ fs_status fs_create(const fs_params* p, fs_ctx** out) {
     FS_ALLOC(c->origin, 4);
     FS_ALLOC(c->status, 1);
     FS_ALLOC(c->scalars, 1);
-    FS_ALLOC(c->nbr_count, cap);
+    FS_ALLOC(c->nbr_count, (cap + kTileOwners - 1) / kTileOwners * kTileOwners);   // whole tiles
     if (cudaMallocHost((void**)&c->scalars_host, sizeof(StepScalars)) != cudaSuccess)
         return bail(fail(FS_ERR_CUDA, "cudaMallocHost failed"));
     // CUB temp storage for the largest sort

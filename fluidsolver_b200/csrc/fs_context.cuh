@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "fs_common.cuh"
+#include "fs_tiles.cuh"
 
 struct fs_ctx {
     fs_params prm{};
@@ -81,7 +82,9 @@ struct fs_ctx {
     int* bbox = nullptr;           // device: min xyz, max xyz (cell coordinates)
     int* origin = nullptr;         // device: cell-grid origin used this step
     uint32_t* nbr = nullptr;       // solver lists, slot-major: nbr[s * nbr_stride + k]
-    float* nbr_grad = nullptr;     // per entry: kernel-gradient factor f (gradW = f * (x_i - x_j)), fast mode
+    fsb::TileDesc* tile_desc = nullptr;  // tile lists (3D IISPH fast path): per tile of owners
+    uint4* tile_ent = nullptr;           // [K / 8][tile_stride] octets of 16-bit entries
+    int64_t tile_stride = 0;             // owners per octet plane (tiles * kTileOwners)
     uint32_t* nbr_count = nullptr;
     int nbr_capacity = 0;          // K
     int64_t nbr_stride = 0;

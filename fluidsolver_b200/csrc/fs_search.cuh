@@ -172,7 +172,6 @@ struct WalkParams {
     bool candidates_inactive;  // contract lists inactive neighbors
     bool trunc;                // cells by truncation toward zero (hashed 2D order)
     bool length_test;          // sqrt(dot) <= r instead of dot <= r * r
-    float inv_h, alpha_h;      // kernel constants for the stored gradient factors
     int d0, d1, d2;
     int64_t cells;  // d0 * d1 * d2; each region's table has cells + 1 entries
 };
@@ -260,70 +259,61 @@ __device__ __forceinline__ bool walk_rows(V3<R> xi, const V4<R>* __restrict__ po
     return true;
 }
 
+// One owner's solver list: up to K entries slot-major (nbr[s * stride + k]);
+// returns the neighbor count. rows: the 9-row walk where the owner is away
+// from the grid border (list order then differs from the reference's).
+template <typename R>
+__device__ __forceinline__ uint32_t build_list_one(int64_t k, const V4<R>* __restrict__ pos,
+                                                   const uint8_t* __restrict__ type,
+                                                   const uint32_t* __restrict__ cell_start,
+                                                   const int* __restrict__ origin, const WalkParams& w, bool rows,
+                                                   uint32_t* __restrict__ nbr, int64_t stride, int K) {
+    uint32_t c = 0;
+    const V3<R> xi = xyz<R>(pos[k]);
+    bool done = false;
+    if (rows) {
+        done = walk_rows<R>(xi, pos, cell_start, origin, w, [&](uint32_t j, int g, float) {
+            if ((int)c < K) nbr[(int64_t)c * stride + k] = j | (g == 1 ? kBoundaryBit : 0u);
+            c++;
+        });
+    }
+    if (!done) {
+        walk_cells<R>(xi, pos, type, cell_start, origin, w, [&](uint32_t j, uint8_t tj) {
+            // solver lists never carry inactive particles (the solvers skip them)
+            if (tj == FS_TYPE_INACTIVE) return;
+            if ((int)c < K) nbr[(int64_t)c * stride + k] = j | (tj == FS_TYPE_BOUNDARY ? kBoundaryBit : 0u);
+            c++;
+        });
+    }
+    return c;
+}
+
+// capacity status and the warp-aggregated maximum of a list length
+__device__ __forceinline__ void note_list_length(uint32_t c, int K, int* __restrict__ status,
+                                                 StepScalars* __restrict__ sc) {
+    if ((int)c > K) raise_status(status, FS_ERR_CAPACITY);
+    unsigned mx = c;
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(__activemask(), mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&sc->max_neighbors, (int)mx);
+}
+
 // Solver lists: for owner k in [0, n_owners) with an owner type accepted by
 // owner_mask (bit per particle type), write up to K entries slot-major. The
 // entry is the sorted index, with kBoundaryBit for boundary neighbors.
-// rows: use the 9-row walk (list order then differs from the reference's).
 template <typename R>
 __global__ void __launch_bounds__(128) k_build_lists(int64_t n_owners, const V4<R>* __restrict__ pos,
                                                      const uint8_t* __restrict__ type,
                                                      const uint32_t* __restrict__ cell_start,
                                                      const int* __restrict__ origin, WalkParams w, uint32_t owner_mask,
-                                                     bool rows, uint32_t* __restrict__ nbr, float* __restrict__ grad,
-                                                     int64_t stride, int K, uint32_t* __restrict__ count,
-                                                     int* __restrict__ status, StepScalars* __restrict__ sc) {
+                                                     bool rows, uint32_t* __restrict__ nbr, int64_t stride, int K,
+                                                     uint32_t* __restrict__ count, int* __restrict__ status,
+                                                     StepScalars* __restrict__ sc) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n_owners) return;
-    const uint8_t tk = type[k];
     uint32_t c = 0;
-    // the fast-mode kernel gradient factor of a neighbor at squared distance q2:
-    // gradW(d) = f d with f = alpha h poly(q) / |d| (SplineKernel::gradWf)
-    auto factor = [&](float q2) -> float {
-        if (!(q2 > kFltEps * kFltEps)) return 0.f;
-        const float inv = rsqrtf(q2);
-        const float q = q2 * inv * w.inv_h;
-        const float a = 2.f - q, b = 1.f - q;
-        float poly;
-        if (q < 1.f) poly = __fmaf_rn(12.f * b, b, -3.f * a * a);
-        else if (q < 2.f) poly = -3.f * a * a;
-        else return 0.f;
-        return w.alpha_h * poly * inv;
-    };
-    if ((owner_mask >> tk) & 1u) {
-        const V3<R> xi = xyz<R>(pos[k]);
-        bool done = false;
-        if (rows) {
-            done = walk_rows<R>(xi, pos, cell_start, origin, w, [&](uint32_t j, int g, float q2) {
-                if ((int)c < K) {
-                    nbr[(int64_t)c * stride + k] = j | (g == 1 ? kBoundaryBit : 0u);
-                    if (grad) grad[(int64_t)c * stride + k] = factor(q2);
-                }
-                c++;
-            });
-        }
-        if (!done) {
-            walk_cells<R>(xi, pos, type, cell_start, origin, w, [&](uint32_t j, uint8_t tj) {
-                // solver lists never carry inactive particles (the solvers skip them)
-                if (tj == FS_TYPE_INACTIVE) return;
-                if ((int)c < K) {
-                    nbr[(int64_t)c * stride + k] = j | (tj == FS_TYPE_BOUNDARY ? kBoundaryBit : 0u);
-                    if (grad) {
-                        const V4<R> pj = pos[j];
-                        const float d0 = (float)xi.x - (float)pj.x, d1 = (float)xi.y - (float)pj.y,
-                                    d2 = (float)xi.z - (float)pj.z;
-                        grad[(int64_t)c * stride + k] = factor((d0 * d0 + d1 * d1) + d2 * d2);
-                    }
-                }
-                c++;
-            });
-        }
-    }
+    if ((owner_mask >> type[k]) & 1u) c = build_list_one<R>(k, pos, type, cell_start, origin, w, rows, nbr, stride, K);
     count[k] = c;
-    if ((int)c > K) raise_status(status, FS_ERR_CAPACITY);
-    // warp-aggregated maximum
-    unsigned mx = c;
-    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(__activemask(), mx, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(&sc->max_neighbors, (int)mx);
+    note_list_length(c, K, status, sc);
 }
 
 // Quadratic searches list neighbors by ascending index

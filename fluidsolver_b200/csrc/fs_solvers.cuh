@@ -30,7 +30,6 @@ template <typename R> struct SolverConsts {
 
 struct Lists {
     const uint32_t* __restrict__ nbr;
-    const float* __restrict__ grad;  // gradient factors beside the entries (fast mode), or null
     const uint32_t* __restrict__ count;
     int64_t stride;
     int K;
@@ -64,44 +63,10 @@ __device__ __forceinline__ void for_neighbors(const Lists& L, int64_t k, const V
     }
 }
 
-// As for_neighbors, also handing d = x_k - x_j and gradW(d). In the fast mode
-// the search stored the gradient factor f of every entry (gradW = f d), so no
-// pass evaluates the kernel again; otherwise gradW is evaluated here.
+// As for_neighbors, also handing d = x_k - x_j and gradW(d).
 template <typename R, bool FAST, typename F>
 __device__ __forceinline__ void for_neighbors_grad(const Lists& L, int64_t k, const V4<R>* __restrict__ pos, V3<R> xk,
                                                    const SplineKernel<R>& kern, F&& f) {
-    if (FAST && L.grad != nullptr) {
-        const uint32_t n = L.size(k);
-        const uint32_t* __restrict__ ep = L.nbr + k;
-        const float* __restrict__ gp = L.grad + k;
-        const uint32_t st = (uint32_t)L.stride;
-        uint32_t q = 0;
-        for (; q + kBatch <= n; q += kBatch) {
-            uint32_t e[kBatch];
-            float fg[kBatch];
-            V4<R> p[kBatch];
-#pragma unroll
-            for (int b = 0; b < kBatch; b++) {
-                e[b] = __ldg(ep + (size_t)(q + b) * st);
-                fg[b] = __ldg(gp + (size_t)(q + b) * st);
-            }
-#pragma unroll
-            for (int b = 0; b < kBatch; b++) p[b] = pos[e[b] & kIndexMask];
-#pragma unroll
-            for (int b = 0; b < kBatch; b++) {
-                const V3<R> d = xk - xyz<R>(p[b]);
-                f(e[b], p[b], d, (R)fg[b] * d);
-            }
-        }
-        for (; q < n; q++) {
-            const uint32_t e = __ldg(ep + (size_t)q * st);
-            const R fg = (R)__ldg(gp + (size_t)q * st);
-            const V4<R> pj = pos[e & kIndexMask];
-            const V3<R> d = xk - xyz<R>(pj);
-            f(e, pj, d, fg * d);
-        }
-        return;
-    }
     for_neighbors<R>(L, k, pos, [&](uint32_t e, const V4<R>& pj) {
         const V3<R> d = xk - xyz<R>(pj);
         f(e, pj, d, kern.template grad<FAST>(d));
@@ -180,16 +145,13 @@ __device__ __forceinline__ V3<R> viscosity(int64_t k, const State<R>& s, const L
 //                loop produces (it overwrites densities while reading them).
 // ===========================================================================
 template <typename R, bool KAHAN, bool SPLIT>
-__global__ void k_iisph3d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* __restrict__ sc,
-                             const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || *status) return;
+__device__ __forceinline__ void iisph3d_l1_one(int64_t k, const State<R>& s, const Lists& L, const SolverConsts<R>& c,
+                                               R dt) {
     const uint8_t t = s.type[k];
     if (t == FS_TYPE_INACTIVE) {
         if (!SPLIT) s.rho[k] = s.rho_prev[k];  // carry the density through the double buffer
         return;
     }
-    const R dt = (R)sc->dt;
     const V4<R> pk = s.pos[k];
     const V4<R> vk = s.vel[k];
     s.p[k] = R(0);
@@ -228,6 +190,14 @@ __global__ void k_iisph3d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
     }
 }
 
+template <typename R, bool KAHAN, bool SPLIT>
+__global__ void k_iisph3d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* __restrict__ sc,
+                             const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    iisph3d_l1_one<R, KAHAN, SPLIT>(k, s, L, c, (R)sc->dt);
+}
+
 // density only (IISPHFluidSolver3D.hpp:184-210), for the split first loop
 template <typename R, bool KAHAN>
 __global__ void k_iisph3d_density(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* __restrict__ status) {
@@ -263,12 +233,8 @@ __global__ void k_iisph3d_density(int64_t n, State<R> s, Lists L, SolverConsts<R
 // regrouped, used with the compensated sums).
 // ===========================================================================
 template <typename R, bool KAHAN, bool TWO_PASS>
-__global__ void k_iisph3d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* __restrict__ sc,
-                             const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || *status) return;
-    if (s.type[k] != FS_TYPE_NORMAL) return;
-    const R dt = (R)sc->dt;
+__device__ __forceinline__ void iisph3d_l2_one(int64_t k, const State<R>& s, const Lists& L, const SolverConsts<R>& c,
+                                               R dt) {
     const V4<R> pk = s.pos[k];
     const V3<R> xk = xyz<R>(pk);
     const V4<R> vsk4 = s.vstar[k];
@@ -311,17 +277,23 @@ __global__ void k_iisph3d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
     s.anp[k].w = diag;
 }
 
+template <typename R, bool KAHAN, bool TWO_PASS>
+__global__ void k_iisph3d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* __restrict__ sc,
+                             const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    if (s.type[k] != FS_TYPE_NORMAL) return;
+    iisph3d_l2_one<R, KAHAN, TWO_PASS>(k, s, L, c, (R)sc->dt);
+}
+
 // ===========================================================================
 // IISPH 3D iteration (a): pressure acceleration (IISPHFluidSolver3D.hpp:348-397)
 //   a_i = - sum_fluid m_j (p_i/rho0^2 + p_j/rho0^2) gradW
 //         - sum_bdy (gamma m_j 2 p_i / rho0^2) gradW       (single layer; no gamma otherwise)
 // ===========================================================================
 template <typename R, bool KAHAN>
-__global__ void k_iisph3d_pressure_acc(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
-                                       const StepScalars* __restrict__ sc, const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || *status || sc->done) return;
-    if (s.type[k] != FS_TYPE_NORMAL) return;
+__device__ __forceinline__ void iisph3d_pressure_acc_one(int64_t k, const State<R>& s, const Lists& L,
+                                                         const SolverConsts<R>& c) {
     const V3<R> xk = xyz<R>(s.pos[k]);
     const R pk = s.p[k];
     Acc3<R, KAHAN> pa;
@@ -342,58 +314,77 @@ __global__ void k_iisph3d_pressure_acc(int64_t n, State<R> s, Lists L, SolverCon
     s.acc[k] = v4<R>(pa.get(), R(0));
 }
 
+template <typename R, bool KAHAN>
+__global__ void k_iisph3d_pressure_acc(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
+                                       const StepScalars* __restrict__ sc, const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status || sc->done) return;
+    if (s.type[k] != FS_TYPE_NORMAL) return;
+    iisph3d_pressure_acc_one<R, KAHAN>(k, s, L, c);
+}
+
 // ===========================================================================
 // IISPH 3D iteration (b): A p, relaxed Jacobi update and the per-particle
 // density error (IISPHFluidSolver3D.hpp:402-461), fused with the convergence
 // scan of :467-512 (block partial sums into StepScalars, FP64 residual).
 // ===========================================================================
-template <typename R, bool KAHAN>
-__global__ void k_iisph3d_pressure_update(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
-                                          StepScalars* __restrict__ sc, const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (*status || sc->done) return;
+// per-particle contribution to the convergence scan and the CFL maxima
+struct ErrPart {
     double e_sum = 0.0;
     unsigned int e_cnt = 0;
     float e_max = 0.f, a2 = 0.f, v2 = 0.f;
-    if (k < n && s.type[k] == FS_TYPE_NORMAL) {
-        const R dt = (R)sc->dt;
-        const V3<R> xk = xyz<R>(s.pos[k]);
-        const V3<R> ak = xyz<R>(s.acc[k]);
-        Acc<R, KAHAN> ap;
-        for_neighbors_grad<R, KAHAN>(L, k, s.pos, xk, c.kern, [&](uint32_t e, const V4<R>& pj, V3<R>, V3<R> g) {
-            const uint32_t j = e & kIndexMask;
-            if (!(e & kBoundaryBit)) ap.add(pj.w * dotf<KAHAN>(ak - xyz<R>(s.acc[j]), g));
-            else ap.add(pj.w * dotf<KAHAN>(ak, g));
-        });
-        const R Ap = ap.get() * (dt * dt);
-        const V4<R> vs = s.vstar[k];   // w: source term
-        const R aii = s.anp[k].w;
-        R p = s.p[k];
-        const bool has_diag = abs_(aii) > R(kFltEps);
-        if (has_diag) p = fmax_(R(0), p + c.omega * ((vs.w - Ap) / aii));
-        else p = R(0);
-        s.p[k] = p;
-        R perr = abs_(vs.w - Ap);
-        if (has_diag) {
-            if (abs_(p) <= R(kFltEps)) perr = R(0);
-            s.err[k] = perr;
-            e_sum = (double)perr;
-            e_cnt = 1;
-            e_max = (float)perr;
-        }
-        // max |a|^2 and |v* + dt a|^2 of the fluid particles (CFL input)
-        a2 = (float)dot(ak, ak);
-        const V3<R> vf = xyz<R>(vs) + dt * ak;
-        v2 = (float)dot(vf, vf);
-        if (!(a2 >= 0.f)) a2 = 0.f;
-        if (!(v2 >= 0.f)) v2 = 0.f;
-        if (!(e_max >= 0.f)) e_max = 0.f;
+};
+
+// the update of particle k given its pressure acceleration ak and the
+// neighbor sum sum_j m_j dot(a_k - a_j, gradW)
+// vs: v* with the source term in w; aii: diagonal element; p: current pressure
+template <typename R>
+__device__ __forceinline__ ErrPart iisph3d_pressure_update_tail(int64_t k, const State<R>& s, const SolverConsts<R>& c,
+                                                                R dt, V3<R> ak, R ap_sum, V4<R> vs, R aii, R p) {
+    ErrPart o;
+    const R Ap = ap_sum * (dt * dt);
+    const bool has_diag = abs_(aii) > R(kFltEps);
+    if (has_diag) p = fmax_(R(0), p + c.omega * ((vs.w - Ap) / aii));
+    else p = R(0);
+    s.p[k] = p;
+    R perr = abs_(vs.w - Ap);
+    if (has_diag) {
+        if (abs_(p) <= R(kFltEps)) perr = R(0);
+        s.err[k] = perr;
+        o.e_sum = (double)perr;
+        o.e_cnt = 1;
+        o.e_max = (float)perr;
     }
-    e_sum = warp_sum(e_sum);
-    e_cnt = warp_sum(e_cnt);
-    e_max = warp_max(e_max);
-    a2 = warp_max(a2);
-    v2 = warp_max(v2);
+    // max |a|^2 and |v* + dt a|^2 of the fluid particles (CFL input)
+    o.a2 = (float)dot(ak, ak);
+    const V3<R> vf = xyz<R>(vs) + dt * ak;
+    o.v2 = (float)dot(vf, vf);
+    if (!(o.a2 >= 0.f)) o.a2 = 0.f;
+    if (!(o.v2 >= 0.f)) o.v2 = 0.f;
+    if (!(o.e_max >= 0.f)) o.e_max = 0.f;
+    return o;
+}
+
+template <typename R, bool KAHAN>
+__device__ __forceinline__ ErrPart iisph3d_pressure_update_one(int64_t k, const State<R>& s, const Lists& L,
+                                                               const SolverConsts<R>& c, R dt) {
+    const V3<R> xk = xyz<R>(s.pos[k]);
+    const V3<R> ak = xyz<R>(s.acc[k]);
+    Acc<R, KAHAN> ap;
+    for_neighbors_grad<R, KAHAN>(L, k, s.pos, xk, c.kern, [&](uint32_t e, const V4<R>& pj, V3<R>, V3<R> g) {
+        const uint32_t j = e & kIndexMask;
+        if (!(e & kBoundaryBit)) ap.add(pj.w * dotf<KAHAN>(ak - xyz<R>(s.acc[j]), g));
+        else ap.add(pj.w * dotf<KAHAN>(ak, g));
+    });
+    return iisph3d_pressure_update_tail<R>(k, s, c, dt, ak, ap.get(), s.vstar[k], s.anp[k].w, s.p[k]);
+}
+
+// block reduction of the ErrParts into StepScalars (FP64 residual sum); every
+// thread of the block calls it
+__device__ __forceinline__ void reduce_err_parts(ErrPart o, StepScalars* __restrict__ sc) {
+    double e_sum = warp_sum(o.e_sum);
+    unsigned int e_cnt = warp_sum(o.e_cnt);
+    float e_max = warp_max(o.e_max), a2 = warp_max(o.a2), v2 = warp_max(o.v2);
     __shared__ double s_sum[32];
     __shared__ unsigned int s_cnt[32];
     __shared__ float s_max[3][32];
@@ -425,6 +416,16 @@ __global__ void k_iisph3d_pressure_update(int64_t n, State<R> s, Lists L, Solver
             atomic_max_nonneg(&sc->max_v2_bits, v2);
         }
     }
+}
+
+template <typename R, bool KAHAN>
+__global__ void k_iisph3d_pressure_update(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
+                                          StepScalars* __restrict__ sc, const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (*status || sc->done) return;
+    ErrPart o;
+    if (k < n && s.type[k] == FS_TYPE_NORMAL) o = iisph3d_pressure_update_one<R, KAHAN>(k, s, L, c, (R)sc->dt);
+    reduce_err_parts(o, sc);
 }
 
 // Convergence test after each iteration (IISPHFluidSolver3D.hpp:463-522) and

@@ -1,0 +1,673 @@
+// Tile lists: the neighbor lists of the 3D IISPH fast path (FP32 with
+// compensated sums, device order) and the kernels that walk them.
+//
+// A tile is kTileOwners consecutive fluid particles of the sorted order.
+// Sorted order is linear cell order (x fastest), so a tile's owners lie in a
+// few (y, z) rows of cells -- its "groups". The union of a group's 27-cell
+// neighborhoods is 9 contiguous ranges of the sorted fluid block plus 9 of
+// the sorted boundary block (rows y-1..y+1, z-1..z+1, cells from the group's
+// first x - 1 to its last x + 1). A pass copies those ranges of the arrays it
+// reads (position and mass, plus one per-neighbor field) into shared memory
+// with bulk copies, then every owner walks its own list, whose entries are
+// 16-bit offsets into the staged arrays. Neighbor data thus crosses the
+// memory system once per tile instead of once per pair, and an entry costs
+// 2 bytes instead of 4. Two threads share an owner in the passes (each takes
+// half of every octet of entries), which doubles the warps that the shared
+// memory of a tile feeds.
+//
+// A tile whose owners touch the grid's border cells, form more than
+// kTileGroups groups, or need more than kTileCap staged candidates is a
+// fallback tile: its owners get the ordinary 32-bit slot-major lists and the
+// passes run the per-pair gather code of fs_solvers.cuh for them.
+//
+// The neighbor sets are the contract's (hashed 3D: dot(d, d) <= r * r over
+// the 27 cells, fs_search.cuh); only the summation order differs from the
+// reference, which the compensated sums absorb.
+#pragma once
+
+#include "fs_common.cuh"
+#include "fs_search.cuh"
+#include "fs_solvers.cuh"
+
+namespace fsb {
+
+constexpr int kTileOwners = 128;
+constexpr int kPassThreads = 2 * kTileOwners;  // two threads per owner in the passes
+constexpr int kTileGroups = 4;
+constexpr int kTileRanges = 2 * 9 * kTileGroups;
+constexpr int kTileCap = 1536;                 // staged candidates
+constexpr uint32_t kTileFallback = 0xffffffffu;
+// entry: byte offset of the candidate's float4 in a staged array (index << 4),
+// bit 0 set for boundary neighbors
+constexpr uint32_t kEntOffset = 0xfff0u;
+constexpr uint32_t kEntBoundary = 0x1u;
+
+struct TileDesc {
+    uint32_t nranges;                  // non-empty candidate ranges, or kTileFallback
+    uint32_t staged;                   // candidates staged in total
+    uint32_t octets;                   // octets of entries of the tile's longest list
+    uint32_t start[kTileRanges];       // first sorted index of each range
+    uint32_t len_base[kTileRanges];    // length | (first staged slot << 16)
+};
+
+struct TileLists {
+    const TileDesc* __restrict__ desc;
+    const uint4* __restrict__ ent;     // [K / 8][stride]: 8 entries of 16 bits per owner and octet
+    const uint32_t* __restrict__ count;
+    int64_t stride;
+    int K;
+};
+
+// dynamic shared memory of the list builder and of the passes. A pass
+// stages its candidates (bytes per candidate: 36 for the first loop --
+// position, velocity, density --, 32 for position and a float4 field, 20 for
+// position and a float field), then the tile's entries and list lengths.
+inline size_t tile_build_smem(int K) { return (size_t)kTileCap * 16 + (size_t)kTileOwners * (K + 8) * 2; }
+inline size_t tile_pass_smem(int bytes_per_candidate, int K) {
+    return (size_t)kTileCap * bytes_per_candidate + (size_t)(K / 8) * kTileOwners * 16 + kTileOwners * 4;
+}
+
+// ---------------------------------------------------------------------------
+// list builder: one block of kTileOwners threads per tile
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
+    int64_t n_owners, const float4* __restrict__ pos, const uint8_t* __restrict__ type,
+    const uint32_t* __restrict__ cell_start, const int* __restrict__ origin, WalkParams w, TileDesc* __restrict__ desc,
+    uint4* __restrict__ ent, int64_t ent_stride, uint32_t* __restrict__ nbr, int64_t stride, int K,
+    uint32_t* __restrict__ count, int* __restrict__ status, StepScalars* __restrict__ sc) {
+    extern __shared__ float4 tile_smem[];
+    float4* sp = tile_smem;                                              // staged positions
+    uint16_t* sent = reinterpret_cast<uint16_t*>(tile_smem + kTileCap);  // [owner][K + 8] entries
+    const int KP = K + 8;
+    __shared__ int s_key[kTileOwners];
+    __shared__ uint32_t s_cnt[kTileOwners];
+    __shared__ int s_lead[kTileOwners / 32];
+    __shared__ int s_gy[kTileGroups], s_gz[kTileGroups], s_gx0[kTileGroups], s_gx1[kTileGroups];
+    __shared__ uint32_t s_start[kTileRanges], s_len[kTileRanges], s_base[kTileRanges];
+    __shared__ uint32_t s_total;
+
+    const int t = threadIdx.x, lane = t & 31;
+    const int64_t tile = blockIdx.x;
+    const int64_t k = tile * kTileOwners + t;
+    const bool valid = k < n_owners;
+    float4 pk = make_float4(0.f, 0.f, 0.f, 0.f);
+    int lx = 0, ly = 0, lz = 0, key = -1;
+    bool border = false;
+    if (valid) {
+        pk = pos[k];
+        lx = cell_coord<float>(pk.x, w.r, false) - origin[0];
+        ly = cell_coord<float>(pk.y, w.r, false) - origin[1];
+        lz = cell_coord<float>(pk.z, w.r, false) - origin[2];
+        border = lx < 2 || ly < 2 || lz < 2 || lx > w.d0 - 3 || ly > w.d1 - 3 || lz > w.d2 - 3;
+        key = border ? -2 : lz * w.d1 + ly;
+    }
+    s_key[t] = key;
+    const int any_border = __syncthreads_or(valid && border);
+    // groups: runs of equal (y, z) row keys (keys are non-decreasing in k)
+    const bool lead = valid && (t == 0 || s_key[t - 1] != key);
+    const unsigned bal = __ballot_sync(0xffffffffu, lead);
+    if (lane == 0) s_lead[t >> 5] = __popc(bal);
+    __syncthreads();
+    int G = 0, before = 0;
+#pragma unroll
+    for (int i = 0; i < kTileOwners / 32; i++) {
+        G += s_lead[i];
+        if (i < (t >> 5)) before += s_lead[i];
+    }
+    const int g = before + __popc(bal & ((1u << lane) - 1u)) + (lead ? 1 : 0) - 1;
+    bool fallback = any_border || G > kTileGroups;
+    int NR = 0;
+    if (!fallback) {
+        if (lead) {
+            s_gy[g] = ly;
+            s_gz[g] = lz;
+            s_gx0[g] = lx;
+        }
+        if (valid && (t == kTileOwners - 1 || s_key[t + 1] != key)) s_gx1[g] = lx;
+        __syncthreads();
+        NR = 18 * G;
+        if (t < NR) {
+            const int region = t / (9 * G), gg = (t % (9 * G)) / 9, r = t % 9;
+            const int64_t rb = ((int64_t)(s_gz[gg] + r / 3 - 1) * w.d1 + (s_gy[gg] + r % 3 - 1)) * w.d0;
+            const uint32_t* cs = cell_start + region * (w.cells + 1);
+            const uint32_t a = cs[rb + s_gx0[gg] - 1], b = cs[rb + s_gx1[gg] + 2];
+            s_start[t] = a;
+            s_len[t] = b - a;
+        }
+        __syncthreads();
+        if (t == 0) {
+            uint32_t tot = 0;
+            for (int q = 0; q < NR; q++) {
+                s_base[q] = tot;
+                tot += s_len[q];
+            }
+            s_total = tot;
+        }
+        __syncthreads();
+        fallback = s_total > (uint32_t)kTileCap;
+    }
+
+    if (fallback) {
+        // ordinary 32-bit lists for this tile's owners
+        if (t == 0) desc[tile].nranges = kTileFallback;
+        uint32_t c = 0;
+        if (valid) {
+            c = build_list_one<float>(k, pos, type, cell_start, origin, w, true, nbr, stride, K);
+            count[k] = c;
+        }
+        note_list_length(c, K, status, sc);
+        return;
+    }
+
+    // stage the candidates' positions (a warp per range)
+    for (int q = t >> 5; q < NR; q += kTileOwners / 32) {
+        const uint32_t a = s_start[q], len = s_len[q], base = s_base[q];
+        for (uint32_t i = lane; i < len; i += 32) sp[base + i] = pos[a + i];
+    }
+    __syncthreads();
+
+    // each owner tests the candidates of its own 27 cells: the 18 row bounds
+    // are loaded up front, candidates are tested two at a time
+    uint32_t c = 0;
+    if (valid) {
+        uint16_t* my = sent + t * KP;
+        uint32_t lo[18], hi[18];
+#pragma unroll
+        for (int q = 0; q < 18; q++) {
+            const uint32_t* cs = cell_start + (q / 9) * (w.cells + 1);
+            const int64_t rb = ((int64_t)(lz + (q % 9) / 3 - 1) * w.d1 + (ly + q % 3 - 1)) * w.d0;
+            lo[q] = cs[rb + lx - 1];
+            hi[q] = cs[rb + lx + 2];
+        }
+        auto test = [&](float4 pj, uint32_t entry) {
+            const float d0 = pk.x - pj.x, d1 = pk.y - pj.y, d2 = pk.z - pj.z;
+            if ((d0 * d0 + d1 * d1) + d2 * d2 <= w.r2) {
+                if ((int)c < K) my[c] = (uint16_t)entry;
+                c++;
+            }
+        };
+#pragma unroll
+        for (int q = 0; q < 18; q++) {
+            const int qq = ((q / 9) * G + g) * 9 + q % 9;
+            const uint32_t off = s_base[qq] - s_start[qq];
+            const uint32_t flag = q >= 9 ? kEntBoundary : 0u;
+            uint32_t i = lo[q] + off;
+            const uint32_t e = hi[q] + off;
+            for (; i + 2 <= e; i += 2) {
+                const float4 p0 = sp[i], p1 = sp[i + 1];
+                test(p0, (i << 4) | flag);
+                test(p1, ((i + 1) << 4) | flag);
+            }
+            if (i < e) test(sp[i], (i << 4) | flag);
+        }
+        count[k] = c;
+    }
+    s_cnt[t] = c;
+    note_list_length(c, K, status, sc);
+    __syncthreads();
+    if (t == 0) {
+        uint32_t mx = 0;
+        for (int i = 0; i < kTileOwners; i++) mx = max(mx, s_cnt[i]);
+        desc[tile].octets = (min(mx, (uint32_t)K) + 7) / 8;
+        uint32_t m = 0;
+        for (int q = 0; q < NR; q++) {
+            if (!s_len[q]) continue;
+            desc[tile].start[m] = s_start[q];
+            desc[tile].len_base[m] = s_len[q] | (s_base[q] << 16);
+            m++;
+        }
+        desc[tile].nranges = m;
+        desc[tile].staged = s_total;
+    }
+    // octets of entries, coalesced across the tile's owners
+    const int O = K / 8;
+    for (int idx = t; idx < kTileOwners * O; idx += kTileOwners) {
+        const int ow = idx % kTileOwners, o = idx / kTileOwners;
+        if ((uint32_t)o * 8 < min(s_cnt[ow], (uint32_t)K))
+            ent[(int64_t)o * ent_stride + tile * kTileOwners + ow] =
+                *reinterpret_cast<const uint4*>(sent + ow * KP + o * 8);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pass helpers: asynchronous staging
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// the mbarrier that a tile's bulk copies complete on
+struct TileStage {
+    uint64_t bar;
+};
+
+// Starts the copies of the tile's candidate ranges into shared memory. Each
+// float4 array (position and mass, and the pass's float4 field if any) is
+// copied range by range with bulk copies (the TMA engine; one thread per
+// range, completion counted in bytes on the mbarrier); a float field goes
+// through 4-byte cp.async copies, a warp per range.
+// Shared-memory view of a tile's lists: entries [octet][owner] and lengths.
+struct TileSlab {
+    uint4* ent;
+    uint32_t* count;
+};
+
+template <int NV4, typename Scalar>
+__device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* __restrict__ d, uint32_t nr,
+                                                 const float4* const (&src4)[NV4], float4* const (&dst4)[NV4],
+                                                 const Scalar* __restrict__ src1, Scalar* dst1, const TileLists& T,
+                                                 const TileSlab& slab) {
+    const int t = threadIdx.x, lane = t & 31;
+    const uint32_t octets = d->octets;
+    const int64_t first = (int64_t)blockIdx.x * kTileOwners;
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&st.bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (t == 0) {
+        const uint32_t bytes = d->staged * 16u * (uint32_t)NV4 + octets * (uint32_t)kTileOwners * 16u +
+                               (uint32_t)kTileOwners * 4u;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&st.bar)), "r"(bytes)
+                     : "memory");
+    }
+    // the tile's list lengths and its entry octets (one contiguous run of
+    // kTileOwners octets per slot group)
+    const int tb = blockDim.x - 1 - t;   // threads from the top of the block, clear of the range copies
+    if (tb == 0)
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_u32(slab.count)),
+            "l"(T.count + first), "r"((uint32_t)kTileOwners * 4u), "r"(smem_u32(&st.bar))
+            : "memory");
+    else if (tb <= (int)octets)
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_u32(slab.ent + (tb - 1) * kTileOwners)),
+            "l"(T.ent + (int64_t)(tb - 1) * T.stride + first), "r"((uint32_t)kTileOwners * 16u),
+            "r"(smem_u32(&st.bar))
+            : "memory");
+    if ((uint32_t)t < nr) {
+        const uint32_t a = d->start[t], lb = d->len_base[t];
+        const uint32_t len = lb & 0xffffu, base = lb >> 16;
+#pragma unroll
+        for (int v = 0; v < NV4; v++) {
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_u32(dst4[v] + base)),
+                "l"(src4[v] + a), "r"(len * 16u), "r"(smem_u32(&st.bar))
+                : "memory");
+        }
+    }
+    if (src1 != nullptr) {
+        for (uint32_t q = t >> 5; q < nr; q += blockDim.x / 32) {
+            const uint32_t a = d->start[q], lb = d->len_base[q];
+            const uint32_t len = lb & 0xffffu, base = lb >> 16;
+            for (uint32_t i = lane; i < len; i += 32)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst1 + base + i)),
+                             "l"(src1 + a + i)
+                             : "memory");
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t mbar_try_wait0(TileStage& st) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(&st.bar))
+        : "memory");
+    return ok;
+}
+
+// Waits for the staging to land, with a bounded number of tries. Returns
+// false, with FS_ERR_TIMEOUT raised, if the copies did not complete; the
+// caller then skips the tile (after a second bounded wait that gives copies
+// still in flight time to land before the block exits).
+__device__ __forceinline__ bool stage_tile_wait(TileStage& st, int* __restrict__ status) {
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    uint32_t ok = 0;
+    for (int it = 0; it < (1 << 16) && !ok; it++) ok = mbar_try_wait0(st);
+    const int late = __syncthreads_or(!ok);
+    if (late) {
+        if (threadIdx.x == 0) raise_status(status, FS_ERR_TIMEOUT);
+        for (int it = 0; it < (1 << 16) && !ok; it++) ok = mbar_try_wait0(st);
+        return false;
+    }
+    return true;
+}
+
+// Visits one half of local owner ol's entries (entries 4 half .. 4 half + 3
+// of every octet), staged in shared memory: f(byte offset into a staged
+// float4 array, boundary) for each, then flush() after every octet (where the
+// passes fold their partial sums into the compensated accumulators).
+template <typename F, typename Flush>
+__device__ __forceinline__ void for_tile_entries(const TileSlab& slab, int K, int ol, int half, F&& f, Flush&& flush) {
+    const uint32_t n = min(slab.count[ol], (uint32_t)K);
+    for (uint32_t o = 0; o * 8 < n; o++) {
+        const uint4 cur = slab.ent[o * kTileOwners + ol];
+        const uint32_t w0 = half ? cur.z : cur.x, w1 = half ? cur.w : cur.y;
+        const int m = (int)(n - o * 8) - 4 * half;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            if (i < m) {
+                const uint32_t v = ((i < 2 ? w0 : w1) >> ((i & 1) * 16)) & 0xffffu;
+                f(v & kEntOffset, (v & kEntBoundary) != 0u);
+            }
+        }
+        flush();
+    }
+}
+
+// the slab after a pass's staged candidates (bytes_per_candidate each)
+__device__ __forceinline__ TileSlab slab_at(float4* smem, int bytes_per_candidate, int K) {
+    char* b = reinterpret_cast<char*>(smem) + kTileCap * bytes_per_candidate;
+    return TileSlab{reinterpret_cast<uint4*>(b), reinterpret_cast<uint32_t*>(b + (K / 8) * kTileOwners * 16)};
+}
+
+template <typename T> __device__ __forceinline__ const T& at_offset(const T* base, uint32_t off) {
+    return *reinterpret_cast<const T*>(reinterpret_cast<const char*>(base) + off);
+}
+
+// value of a compensated accumulator, summed over the two threads of an owner
+__device__ __forceinline__ float pair_total(const Acc<float, true>& a) {
+    const float v = a.s - a.c;
+    return v + __shfl_xor_sync(0xffffffffu, v, 1);
+}
+__device__ __forceinline__ V3<float> pair_total(const Acc3<float, true>& a) {
+    return v3<float>(pair_total(a.x), pair_total(a.y), pair_total(a.z));
+}
+
+__device__ __forceinline__ V3<float> sub3(float4 a, float4 b) { return v3<float>(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float dot3(V3<float> a, V3<float> b) {
+    return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, a.x * b.x));
+}
+__device__ __forceinline__ float r2_of(V3<float> d) { return __fmaf_rn(d.z, d.z, __fmaf_rn(d.y, d.y, d.x * d.x)); }
+__device__ __forceinline__ V3<float> fma3(float s, V3<float> d, V3<float> acc) {
+    return v3<float>(__fmaf_rn(s, d.x, acc.x), __fmaf_rn(s, d.y, acc.y), __fmaf_rn(s, d.z, acc.z));
+}
+
+// The cubic spline of the fast mode, evaluated from a listed pair's squared
+// distance r2 (r2 <= (2h)^2). The reference's piecewise cubic
+// (CubicSplineKernel3D.cpp:7-66) with its polynomials expanded, q = |d| / h:
+//   W        = alpha (4 - 6 q^2 + 3 q^3)              q < 1
+//            = alpha (2 - q)^3                        1 <= q <= 2
+//   gradW(d) = f d,  f = alpha (9 q - 12)             q < 1
+//                    f = -3 alpha h (2 - q)^2 / |d|   1 <= q <= 2
+// (for q < 1 that is alpha h (-3 (2 - q)^2 + 12 (1 - q)^2) / |d| with
+// |d| = q h). One rsqrt per pair, no divisions, no branches. The self pair
+// (d = 0) gets the finite f = -12 alpha and so a zero gradient, as the
+// reference's |d| <= FLT_EPSILON test gives.
+struct FastSpline {
+    float a, inv_h, a9, a12, a3h;
+    __device__ explicit FastSpline(const SplineKernel<float>& k)
+        : a(k.alpha), inv_h(1.f / k.h), a9(9.f * k.alpha), a12(12.f * k.alpha), a3h(3.f * k.alpha * k.h) {}
+    __device__ __forceinline__ float grad(float r2) const {
+        const float inv = rsqrtf(r2);
+        const float q = (r2 > 0.f ? r2 * inv : 0.f) * inv_h;
+        const float t = fmaxf(2.f - q, 0.f);
+        return q < 1.f ? __fmaf_rn(a9, q, -a12) : -a3h * (t * t) * inv;
+    }
+    __device__ __forceinline__ void value_grad(float r2, float& w, float& f) const {
+        const float inv = rsqrtf(r2);
+        const float q = (r2 > 0.f ? r2 * inv : 0.f) * inv_h;
+        const float t = fmaxf(2.f - q, 0.f);
+        const bool inner = q < 1.f;
+        f = inner ? __fmaf_rn(a9, q, -a12) : -a3h * (t * t) * inv;
+        w = a * (inner ? __fmaf_rn(q * q, __fmaf_rn(3.f, q, -6.f), 4.f) : (t * t) * t);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// IISPH 3D passes on tile lists (the fast-mode formulas of the gather
+// kernels: IISPHFluidSolver3D.hpp:141-212, :216-339, :348-397, :402-461).
+// Blocks of kPassThreads threads: owner = threadIdx.x / 2, half =
+// threadIdx.x % 2; the even thread of a pair writes the owner's results.
+// ---------------------------------------------------------------------------
+
+// first loop. Blocks [0, n_tiles) are tiles of fluid owners; the blocks after
+// them take the boundary and inactive particles [n_fluid, n), which need no
+// neighbor sums.
+__global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l1(int64_t n_fluid, int64_t n, int64_t n_tiles,
+                                                                  State<float> s, TileLists T, Lists L,
+                                                                  SolverConsts<float> c,
+                                                                  const StepScalars* __restrict__ sc,
+                                                                  int* __restrict__ status) {
+    extern __shared__ float4 tile_smem[];
+    if (*status) return;
+    const float dt = sc->dt;
+    if (blockIdx.x >= n_tiles) {
+        const int64_t k = n_fluid + (blockIdx.x - n_tiles) * (int64_t)kPassThreads + threadIdx.x;
+        if (k < n) iisph3d_l1_one<float, true, false>(k, s, L, c, dt);
+        return;
+    }
+    const int half = threadIdx.x & 1;
+    const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
+    const TileDesc* d = T.desc + blockIdx.x;
+    const uint32_t nr = d->nranges;
+    if (nr == kTileFallback) {
+        if (k < n_fluid && !half) iisph3d_l1_one<float, true, false>(k, s, L, c, dt);
+        return;
+    }
+    float4* sp = tile_smem;
+    float4* sv = tile_smem + kTileCap;
+    float* sr = reinterpret_cast<float*>(tile_smem + 2 * kTileCap);
+    __shared__ TileStage stg;
+    const float4* src4[2] = {s.pos, s.vel};
+    float4* dst4[2] = {sp, sv};
+    const TileSlab slab = slab_at(tile_smem, 36, T.K);
+    stage_tile_async<2, float>(stg, d, nr, src4, dst4, s.rho_prev, sr, T, slab);
+    // owners past n_fluid (last tile) walk no entries but take part in the shuffles
+    const bool valid = k < n_fluid;
+    const int64_t kk = valid ? k : 0;
+    const float4 pk = s.pos[kk], vk = s.vel[kk], ek = s.ext[kk];
+    if (!stage_tile_wait(stg, status)) return;
+    const FastSpline S(c.kern);
+    Acc3<float, true> visc;
+    Acc<float, true> rho;
+    V3<float> vpart = v3<float>(0.f, 0.f, 0.f);
+    float rpart = 0.f;
+    const float gb = c.single_layer ? c.gamma1 : 1.f;
+    if (valid) for_tile_entries(slab, T.K, (int)(threadIdx.x >> 1), half, [&](uint32_t off, bool bnd) {
+        const float4 pj = at_offset(sp, off), vj = at_offset(sv, off);
+        const float rj = at_offset(sr, off >> 2);
+        const V3<float> xij = sub3(pk, pj);
+        const float r2 = r2_of(xij);
+        float w, f;
+        S.value_grad(r2, w, f);
+        rpart = __fmaf_rn(bnd ? pj.w * gb : pj.w, w, rpart);
+        if (rj != 0.f) {
+            const float cf = __fdividef(pj.w * dot3(sub3(vk, vj), xij), rj * (r2 + c.visc_eps)) * f;
+            vpart = fma3(cf, xij, vpart);
+        }
+    }, [&] {
+        visc.add(vpart);
+        rho.add(rpart);
+        vpart = v3<float>(0.f, 0.f, 0.f);
+        rpart = 0.f;
+    });
+    const V3<float> vs = pair_total(visc);
+    const float rk = pair_total(rho);
+    if (half || !valid) return;
+    s.p[k] = 0.f;
+    const V3<float> npa = v3<float>(ek.x, ek.y - c.gravity, ek.z) + c.two_nu * vs;
+    const V3<float> vstar = v3<float>(vk.x, vk.y, vk.z) + dt * npa;
+    s.vstar[k] = v4<float>(vstar, 0.f);
+    s.anp[k] = v4<float>(npa, 0.f);
+    s.ext[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    s.rho[k] = rk;
+}
+
+// second loop: source term and diagonal element (single-pass a_ii)
+__global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l2(int64_t n_fluid, State<float> s, TileLists T,
+                                                                  Lists L, SolverConsts<float> c,
+                                                                  const StepScalars* __restrict__ sc,
+                                                                  int* __restrict__ status) {
+    extern __shared__ float4 tile_smem[];
+    if (*status) return;
+    const float dt = sc->dt;
+    const int half = threadIdx.x & 1;
+    const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
+    const TileDesc* d = T.desc + blockIdx.x;
+    const uint32_t nr = d->nranges;
+    if (nr == kTileFallback) {
+        if (k < n_fluid && !half) iisph3d_l2_one<float, true, false>(k, s, L, c, dt);
+        return;
+    }
+    float4* sp = tile_smem;
+    float4* sa = tile_smem + kTileCap;
+    __shared__ TileStage stg;
+    const float4* src4[2] = {s.pos, s.vstar};
+    float4* dst4[2] = {sp, sa};
+    const TileSlab slab = slab_at(tile_smem, 32, T.K);
+    stage_tile_async<2, float>(stg, d, nr, src4, dst4, (const float*)nullptr, (float*)nullptr, T, slab);
+    const bool valid = k < n_fluid;
+    const int64_t kk = valid ? k : 0;
+    const float4 pk = s.pos[kk], vsk = s.vstar[kk];
+    const float rk = s.rho[kk];
+    if (!stage_tile_wait(stg, status)) return;
+    const FastSpline S(c.kern);
+    Acc<float, true> contrib, mg2;
+    Acc3<float, true> inner, mg;
+    float cpart = 0.f, g2part = 0.f;
+    V3<float> ipart = v3<float>(0.f, 0.f, 0.f), mpart = v3<float>(0.f, 0.f, 0.f);
+    const float wb = c.single_layer ? c.two_gamma : 2.f;
+    if (valid) for_tile_entries(slab, T.K, (int)(threadIdx.x >> 1), half, [&](uint32_t off, bool bnd) {
+        const float4 pj = at_offset(sp, off), vsj = at_offset(sa, off);
+        const V3<float> xij = sub3(pk, pj);
+        const float r2 = r2_of(xij);
+        const float f = S.grad(r2);
+        const float mf = pj.w * f;            // m_j gradW = mf d
+        const V3<float> dv = bnd ? v3<float>(vsk.x, vsk.y, vsk.z) : sub3(vsk, vsj);
+        cpart = __fmaf_rn(mf, dot3(dv, xij), cpart);
+        ipart = fma3(bnd ? -wb * mf : -mf, xij, ipart);
+        if (!bnd) g2part = __fmaf_rn(mf * f, r2, g2part);
+        mpart = fma3(mf, xij, mpart);
+    }, [&] {
+        contrib.add(cpart);
+        mg2.add(g2part);
+        inner.add(ipart);
+        mg.add(mpart);
+        cpart = g2part = 0.f;
+        ipart = mpart = v3<float>(0.f, 0.f, 0.f);
+    });
+    const float ct = pair_total(contrib), g2 = pair_total(mg2);
+    const V3<float> in = pair_total(inner), m = pair_total(mg);
+    if (half || !valid) return;
+    const float source = (c.rest_density - rk) - dt * ct;
+    const float diag = (c.inv_rho0_sq * dot(in, m) - (pk.w / c.rho0_sq) * g2) * (dt * dt);
+    s.vstar[k] = make_float4(vsk.x, vsk.y, vsk.z, source);
+    s.anp[k].w = diag;
+}
+
+// iteration (a): pressure acceleration
+__global__ void __launch_bounds__(kPassThreads, 4) k_tile_iisph3d_pressure_acc(int64_t n_fluid, State<float> s,
+                                                                            TileLists T, Lists L,
+                                                                            SolverConsts<float> c,
+                                                                            const StepScalars* __restrict__ sc,
+                                                                            int* __restrict__ status) {
+    extern __shared__ float4 tile_smem[];
+    if (*status || sc->done) return;
+    const int half = threadIdx.x & 1;
+    const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
+    const TileDesc* d = T.desc + blockIdx.x;
+    const uint32_t nr = d->nranges;
+    if (nr == kTileFallback) {
+        if (k < n_fluid && !half) iisph3d_pressure_acc_one<float, true>(k, s, L, c);
+        return;
+    }
+    float4* sp = tile_smem;
+    float* sa = reinterpret_cast<float*>(tile_smem + kTileCap);
+    __shared__ TileStage stg;
+    const float4* src4[1] = {s.pos};
+    float4* dst4[1] = {sp};
+    const TileSlab slab = slab_at(tile_smem, 20, T.K);
+    stage_tile_async<1, float>(stg, d, nr, src4, dst4, s.p, sa, T, slab);
+    const bool valid = k < n_fluid;
+    const int64_t kk = valid ? k : 0;
+    const float4 pk = s.pos[kk];
+    const float prk = s.p[kk];
+    if (!stage_tile_wait(stg, status)) return;
+    const FastSpline S(c.kern);
+    const float wb = (c.single_layer ? c.two_gamma : 2.f) * prk;
+    Acc3<float, true> pa;
+    V3<float> part = v3<float>(0.f, 0.f, 0.f);
+    if (valid) for_tile_entries(slab, T.K, (int)(threadIdx.x >> 1), half, [&](uint32_t off, bool bnd) {
+        const float4 pj = at_offset(sp, off);
+        const V3<float> xij = sub3(pk, pj);
+        const float coef = pj.w * (bnd ? wb : prk + at_offset(sa, off >> 2)) * S.grad(r2_of(xij));
+        part = fma3(-coef, xij, part);
+    }, [&] {
+        pa.add(part);
+        part = v3<float>(0.f, 0.f, 0.f);
+    });
+    const V3<float> a = pair_total(pa);
+    if (half || !valid) return;
+    s.acc[k] = v4<float>(c.inv_rho0_sq * a, 0.f);
+}
+
+// iteration (b): A p, relaxed Jacobi update, density error, fused scan
+__global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_pressure_update(int64_t n_fluid, State<float> s,
+                                                                               TileLists T, Lists L,
+                                                                               SolverConsts<float> c,
+                                                                               StepScalars* __restrict__ sc,
+                                                                               int* __restrict__ status) {
+    extern __shared__ float4 tile_smem[];
+    if (*status || sc->done) return;
+    const float dt = sc->dt;
+    const int half = threadIdx.x & 1;
+    const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
+    const TileDesc* d = T.desc + blockIdx.x;
+    const uint32_t nr = d->nranges;
+    ErrPart o;
+    if (nr == kTileFallback) {
+        if (k < n_fluid && !half) o = iisph3d_pressure_update_one<float, true>(k, s, L, c, dt);
+    } else {
+        float4* sp = tile_smem;
+        float4* sa = tile_smem + kTileCap;
+        __shared__ TileStage stg;
+        const float4* src4[2] = {s.pos, s.acc};
+        float4* dst4[2] = {sp, sa};
+        const TileSlab slab = slab_at(tile_smem, 32, T.K);
+        stage_tile_async<2, float>(stg, d, nr, src4, dst4, (const float*)nullptr, (float*)nullptr, T, slab);
+        // the owner's own data, loaded while the staging lands
+        const bool valid = k < n_fluid;
+        const int64_t kk = valid ? k : 0;
+        const float4 pk = s.pos[kk], ak = s.acc[kk], vsk = s.vstar[kk];
+        const float aii = s.anp[kk].w, prk = s.p[kk];
+        if (stage_tile_wait(stg, status)) {
+            const FastSpline S(c.kern);
+            Acc<float, true> ap;
+            float part = 0.f;
+            if (valid) for_tile_entries(slab, T.K, (int)(threadIdx.x >> 1), half, [&](uint32_t off, bool bnd) {
+                const float4 pj = at_offset(sp, off);
+                const V3<float> xij = sub3(pk, pj);
+                const V3<float> da = bnd ? v3<float>(ak.x, ak.y, ak.z) : sub3(ak, at_offset(sa, off));
+                part = __fmaf_rn(pj.w * S.grad(r2_of(xij)), dot3(da, xij), part);
+            }, [&] {
+                ap.add(part);
+                part = 0.f;
+            });
+            const float sum = pair_total(ap);
+            if (!half && valid)
+                o = iisph3d_pressure_update_tail<float>(k, s, c, dt, v3<float>(ak.x, ak.y, ak.z), sum, vsk, aii, prk);
+        }
+    }
+    reduce_err_parts(o, sc);
+}
+
+inline cudaError_t set_tile_pass_smem(int K) {
+    cudaError_t e = cudaFuncSetAttribute(k_tile_iisph3d_l1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)tile_pass_smem(36, K));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tile_iisph3d_l2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_pass_smem(32, K));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_acc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_pass_smem(20, K));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_pass_smem(32, K));
+    return e;
+}
+
+}  // namespace fsb
