@@ -120,10 +120,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples), "source": "NVML, 4 ms period"}
 
 
-def make_solver(scene, device, precision="fp32-kahan"):
+def make_solver(scene, device, precision="fp32-kahan", eager=False):
     from fluidsolver_b200 import IISPHFluidSolver3D
     from fluidsolver_b200.scenes import REFERENCE_UNITS_DT
-    s = IISPHFluidSolver3D(search="hashed-3d", precision=precision, device=device)
+    s = IISPHFluidSolver3D(search="hashed-3d", precision=precision, device=device, sync_each_iteration=eager)
     s.parameters.rest_density = scene.rest_density
     s.parameters.gravity = 9.81
     s.parameters.particle_size = scene.particle_size
@@ -201,7 +201,7 @@ def run_ours(args):
 
     scene = scenes.dam_1m(seed=5 + rank)
     n_active = scene.n_fluid + scene.n_boundary
-    solver = make_solver(scene, local, args.precision)
+    solver = make_solver(scene, local, args.precision, args.eager)
     L = F.lib()
     for _ in range(args.warmup):
         solver.step()
@@ -261,6 +261,8 @@ def run_ours(args):
                        "hashed-3d neighbor contract, dt 0.005 (reference units), single-layer boundary",
                        "fluid_particles_per_gpu": scene.n_fluid, "boundary_particles_per_gpu": scene.n_boundary,
                        "parallelism": f"replicas x{world} (independent scenes)",
+                       "mode": "eager (host-driven pressure loop, profiling only)" if args.eager else
+                       "whole step as one CUDA graph (pressure loop: conditional WHILE node)",
                        "l2": "inputs larger than L2 (~0.5 GB of particle state and lists per step)",
                        "iterations_mean": it_total / args.steps, "avg_density_error_max": max(errs),
                        "phase_ms_per_step": dict(zip(PHASES, (phase / args.steps).round(4).tolist())),
@@ -367,11 +369,14 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32-kahan", choices=["fp32", "fp32-kahan", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--eager", action="store_true",
+                    help="host-driven pressure loop instead of the whole-step CUDA graph: for kernel-level profiling "
+                         "(ncu cannot profile the kernels of a graph with conditional nodes); slower, not a bench value")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

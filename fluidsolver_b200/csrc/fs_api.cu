@@ -291,9 +291,11 @@ fs_status ensure_lists(fs_ctx* c, int K) {
 }
 
 // Grid dims from the cell bounding box of the uploaded particles (lo > hi on
-// an axis: no finite coordinate there): the box plus a margin of a quarter
-// of its extent (at least 4 cells) on each side, shrunk until the grid has
-// at most max(4M, 8 * capacity) cells.
+// an axis: no finite coordinate there): the box plus a margin of a sixteenth
+// of its extent (at least 2 cells, which the 9-row walk needs) on each side,
+// shrunk until the grid has at most max(4M, 8 * capacity) cells (2^30 at
+// most). Particles that later leave the grid are clamped into its border
+// cells and take the exact per-cell walk.
 void choose_dims(fs_ctx* c, const int* lo_in, const int* hi_in) {
     const int dim = c->dim;
     int lo[3] = {lo_in[0], lo_in[1], lo_in[2]}, hi[3] = {hi_in[0], hi_in[1], hi_in[2]};
@@ -301,10 +303,11 @@ void choose_dims(fs_ctx* c, const int* lo_in, const int* hi_in) {
     for (int a = 0; a < dim; a++) {
         if (lo[a] > hi[a]) { lo[a] = hi[a] = 0; }
         int64_t e = (int64_t)hi[a] - lo[a] + 1;
-        int64_t margin = std::max<int64_t>(4, e / 4);
+        int64_t margin = std::max<int64_t>(2, e / 16);
         ext[a] = std::min<int64_t>(int64_t(1) << 20, e + 2 * margin);
     }
-    const int64_t max_cells = std::max<int64_t>(int64_t(1) << 22, 8 * std::max<int64_t>(c->cap, 1));
+    const int64_t max_cells =
+        std::min<int64_t>(int64_t(1) << 30, std::max<int64_t>(int64_t(1) << 22, 8 * std::max<int64_t>(c->cap, 1)));
     while (ext[0] * ext[1] * ext[2] > max_cells) {
         int a = (ext[0] >= ext[1] && ext[0] >= ext[2]) ? 0 : (ext[1] >= ext[2] ? 1 : 2);
         ext[a] = std::max<int64_t>(1, (ext[a] * 3) / 4);
@@ -315,6 +318,8 @@ void choose_dims(fs_ctx* c, const int* lo_in, const int* hi_in) {
 // cell tables for the current dims (and the scan's temporary storage)
 fs_status ensure_cells(fs_ctx* c) {
     c->cells = (int64_t)c->dims[0] * c->dims[1] * c->dims[2];
+    c->key_bits = 1;
+    while ((int64_t(1) << c->key_bits) < c->cells) c->key_bits++;
     c->regions = c->reference_order ? 1 : (c->include_inactive ? 3 : 2);
     const int64_t need = c->cells + 1;
     if (!c->cell_start || c->cell_alloc < need) {
@@ -545,15 +550,16 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     unsigned long long* k64 = single ? c->keys64[0] : nullptr;
     c->launches++;
     k_keys<R><<<grid_for(n), kBlock, 0, st>>>(n, s.pos, s.type, s.hidx, c->include_inactive, single, c->search_radius,
-                                              c->truncate_cells, c->origin, c->dims[0], c->dims[1], c->dims[2], c->keys[0], k64, c->perm[0]);
+                                              c->truncate_cells, c->origin, c->dims[0], c->dims[1], c->dims[2], c->key_bits,
+                                              c->keys[0], k64, c->perm[0]);
     FS_CUDA(cudaGetLastError());
     size_t temp = c->cub_temp_bytes;
     if (single) {
         FS_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_temp, temp, c->keys64[0], c->keys64[1], c->perm[0], c->perm[1],
-                                                (int)n, 0, 64, st));
+                                                (int)n, 0, 32 + c->key_bits + 2, st));
     } else {
         FS_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_temp, temp, c->keys[0], c->keys[1], c->perm[0], c->perm[1],
-                                                (int)n, 0, 32, st));
+                                                (int)n, 0, c->key_bits + 2, st));
     }
     // gather every persistent field into the other buffer
     const int nx = c->cur ^ 1;
@@ -573,7 +579,8 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     FS_CUDA(cudaMemsetAsync(c->cell_counts, 0, sizeof(uint32_t) * table, st));
     c->launches++;
     k_cell_counts<<<grid_for(c->n_struct), kBlock, 0, st>>>(c->n_struct, single ? nullptr : c->keys[1],
-                                                            single ? c->keys64[1] : nullptr, c->cells, c->cell_counts);
+                                                            single ? c->keys64[1] : nullptr, c->cells, c->key_bits,
+                                                            c->cell_counts);
     FS_CUDA(cudaGetLastError());
     temp = c->cub_temp_bytes;
     FS_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_temp, temp, c->cell_counts, c->cell_start, (int)table, st));

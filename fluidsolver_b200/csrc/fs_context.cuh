@@ -76,6 +76,7 @@ struct fs_ctx {
     uint32_t* cell_start = nullptr;   // [regions][cells + 1] first sorted index of cell >= c
     uint32_t* cell_counts = nullptr;  // [regions][cells + 1] scratch for the scan
     int64_t cells = 0;                // dims[0] * dims[1] * dims[2]
+    int key_bits = 30;                // bits of the linear cell index in the sort keys
     int64_t cell_alloc = 0;           // entries allocated per table
     int regions = 2;                  // regions in the sorted layout
     int dims[3] = {1, 1, 1};

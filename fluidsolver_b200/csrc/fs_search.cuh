@@ -32,8 +32,11 @@
 
 namespace fsb {
 
-constexpr uint32_t kInactiveKey = 0xffffffffu;
-constexpr uint32_t kCellMask = 0x3fffffffu;
+// Sort keys: region (0 fluid, 1 boundary, 2 listed inactive, 3 excluded
+// inactive) in the two bits above the linear cell index, which takes
+// key_bits bits (the fewest that hold the grid's cells), so the radix sort
+// runs over key_bits + 2 bits only.
+__host__ __device__ __forceinline__ uint32_t inactive_key(int key_bits) { return 0xffffffffu >> (30 - key_bits); }
 
 // cell coordinate of a position: (int)floor(x / r), or the truncation toward
 // zero of HashedNeighborhoodSearch (2D) (HashedNeighborhoodSearch.cpp:108-115)
@@ -63,11 +66,30 @@ __global__ void k_bbox(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* 
             mx[a] = max(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
         }
     }
-    if ((threadIdx.x & 31) == 0) {
+    // block reduction, then one atomic per bound and block
+    __shared__ int s_b[6][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
 #pragma unroll
         for (int a = 0; a < 3; a++) {
-            if (mn[a] != INT_MAX) atomicMin(&bbox[a], mn[a]);
-            if (mx[a] != INT_MIN) atomicMax(&bbox[3 + a], mx[a]);
+            s_b[a][wid] = mn[a];
+            s_b[3 + a][wid] = mx[a];
+        }
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            int lo = lane < nw ? s_b[a][lane] : INT_MAX, hi = lane < nw ? s_b[3 + a][lane] : INT_MIN;
+            for (int o = 16; o > 0; o >>= 1) {
+                lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+            }
+            if (lane == 0) {
+                if (lo != INT_MAX) atomicMin(&bbox[a], lo);
+                if (hi != INT_MIN) atomicMax(&bbox[3 + a], hi);
+            }
         }
     }
 }
@@ -103,14 +125,15 @@ __device__ __forceinline__ uint32_t region_of(uint8_t t, bool single_region) {
 template <typename R>
 __global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
                        const uint32_t* __restrict__ hidx, bool include_inactive, bool single_region, float r,
-                       bool trunc, const int* __restrict__ origin, int d0, int d1, int d2, uint32_t* __restrict__ keys,
+                       bool trunc, const int* __restrict__ origin, int d0, int d1, int d2, int key_bits,
+                       uint32_t* __restrict__ keys,
                        unsigned long long* __restrict__ keys64, uint32_t* __restrict__ perm) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     uint8_t t = type[k];
     uint32_t key;
     if (!include_inactive && t == FS_TYPE_INACTIVE) {
-        key = kInactiveKey;
+        key = inactive_key(key_bits);
     } else {
         V4<R> p = pos[k];
         bool cl = false;
@@ -118,7 +141,7 @@ __global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* 
         int ly = local_cell(cell_coord<R>(p.y, r, trunc), origin[1], d1, cl);
         int lz = local_cell(cell_coord<R>(p.z, r, trunc), origin[2], d2, cl);
         const uint32_t lin = (uint32_t)(((int64_t)lz * d1 + ly) * d0 + lx);
-        key = (region_of(t, single_region) << 30) | lin;
+        key = (region_of(t, single_region) << key_bits) | lin;
     }
     if (keys64) keys64[k] = ((unsigned long long)key << 32) | hidx[k];
     else keys[k] = key;
@@ -149,7 +172,7 @@ __global__ void k_reorder(int64_t n, const uint32_t* __restrict__ perm, const V4
 // Per-cell particle counts of every region: the first particle of each run of
 // equal keys writes the run length (the table is zeroed before).
 __global__ void k_cell_counts(int64_t n_struct, const uint32_t* __restrict__ keys,
-                              const unsigned long long* __restrict__ keys64, int64_t cells,
+                              const unsigned long long* __restrict__ keys64, int64_t cells, int key_bits,
                               uint32_t* __restrict__ counts) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n_struct) return;
@@ -158,7 +181,7 @@ __global__ void k_cell_counts(int64_t n_struct, const uint32_t* __restrict__ key
     if (k > 0 && key_at(k - 1) == key) return;
     int64_t e = k + 1;
     while (e < n_struct && key_at(e) == key) e++;
-    counts[(int64_t)(key >> 30) * (cells + 1) + (key & kCellMask)] = (uint32_t)(e - k);
+    counts[(int64_t)(key >> key_bits) * (cells + 1) + (key & ((1u << key_bits) - 1u))] = (uint32_t)(e - k);
 }
 
 // ---------------------------------------------------------------------------
