@@ -44,6 +44,10 @@ BYTES_L2 = 44        # per fluid particle: read pos4 v*4 rho, write s a_ii
 BYTES_ITER = 84      # per fluid particle and iteration: pressure acceleration 36 + update 48
 BYTES_INTEGRATE = 96  # per active particle: read pos4 v*4 a_np4 a4, write pos4 vel4
 PHASES = ["search", "iisph_l1", "iisph_l2", "pressure_iterations", "integration"]
+PHASE_KERNELS = ["neighborhood search (sort, reorder, cell table, k_build_tiles)", "k_tile_iisph3d_l1",
+                 "k_tile_iisph3d_l2", "pressure iteration: k_tile_iisph3d_pressure_acc + k_tile_iisph3d_pressure_update",
+                 "k_cfl + k_iisph3d_integrate"]
+PHASE_UNITS = ["step", "launch", "launch", "iteration (two launches)", "step"]
 
 
 def measured_peak():
@@ -236,6 +240,9 @@ def run_ours(args):
     peak, peak_kind = measured_peak()
     achieved = phase_bytes[dom] / (phase[dom] / 1e3) / 1e9
     step_bytes = sum(phase_bytes) / args.steps
+    # the unit the roofline kernel's bytes and traffic are quoted per
+    units = [args.steps, args.steps, args.steps, max(it_total, 1.0), args.steps]
+    per_launch = phase_bytes[dom] / units[dom]
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
@@ -268,8 +275,10 @@ def run_ours(args):
                        "phase_ms_per_step": dict(zip(PHASES, (phase / args.steps).round(4).tolist())),
                        "algorithmic_bytes_per_step": step_bytes,
                        "step_fraction_of_hbm_roofline": step_bytes / (ms / args.steps / 1e3) / 1e9 / peak},
-            "roofline": {"bound": "hbm", "kernel": PHASES[dom], "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic},
+            "roofline": {"bound": "hbm", "kernel": PHASE_KERNELS[dom], "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": per_launch, "per": PHASE_UNITS[dom],
+                         "traffic_source": "profiles/traffic.json (ncu dram__bytes_read.sum + dram__bytes_write.sum)"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
         }
         print(json.dumps(out))
