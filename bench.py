@@ -124,13 +124,12 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples), "source": "NVML, 4 ms period"}
 
 
-def make_solver(scene, device, precision="fp32-kahan", eager=False):
-    from fluidsolver_b200 import IISPHFluidSolver3D
+def configure_iisph(s, rest_density=1.0, particle_size=1.0):
+    """The benchmark's IISPH parameters (reference units, see scenes.py)."""
     from fluidsolver_b200.scenes import REFERENCE_UNITS_DT
-    s = IISPHFluidSolver3D(search="hashed-3d", precision=precision, device=device, sync_each_iteration=eager)
-    s.parameters.rest_density = scene.rest_density
+    s.parameters.rest_density = rest_density
     s.parameters.gravity = 9.81
-    s.parameters.particle_size = scene.particle_size
+    s.parameters.particle_size = particle_size
     s.settings.viscosity = 0.01
     s.settings.single_layer_boundary = True
     s.settings.single_layer_boundary_gamma_1 = 1.1
@@ -140,6 +139,12 @@ def make_solver(scene, device, precision="fp32-kahan", eager=False):
     s.settings.omega = 0.5
     s.settings.gamma = 0.7
     s.timestep_generator.settings.timestep = REFERENCE_UNITS_DT
+
+
+def make_solver(scene, device, precision="fp32-kahan", eager=False):
+    from fluidsolver_b200 import IISPHFluidSolver3D
+    s = IISPHFluidSolver3D(search="hashed-3d", precision=precision, device=device, sync_each_iteration=eager)
+    configure_iisph(s, scene.rest_density, scene.particle_size)
     s.data.collection = scene.collection
     return s
 
@@ -251,11 +256,13 @@ def run_ours(args):
 
     # end to end through the public API: pinned host state in, step, state out
     e2e = run_e2e(solver, scene, min(args.steps, 5), local, max_over_ranks)
+    solver_state = solver.collection() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    solver.close()
+    batched = None if args.no_batched else run_batched(args, local, rank, world, max_over_ranks, barrier)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        state = solver.collection()
-        cpu = cpu_baseline_from_state(state, scene.n_fluid)
+    if solver_state is not None:
+        cpu = cpu_baseline_from_state(solver_state, scene.n_fluid)
 
     clocks = clk.summary()
     if rank == 0:
@@ -280,11 +287,66 @@ def run_ours(args):
                          "algorithmic_bytes_per_launch": per_launch, "per": PHASE_UNITS[dom],
                          "traffic_source": "profiles/traffic.json (ncu dram__bytes_read.sum + dram__bytes_write.sum)"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+            "batched": batched,
         }
         print(json.dumps(out))
-    solver.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_batched(args, device, rank, world, max_over_ranks, barrier):
+    """The batched breaking dams (256 scenes, seed 6; scenes i = rank mod N on
+    rank N): all of a rank's scenes in one batched context, timed with CUDA
+    events on the context's stream around fs_batch_run; at N = 1 the same
+    scenes also run one at a time through the single-scene path (fs_run of
+    the same steps per scene, events around each), the plain per-scene form."""
+    import torch
+    from fluidsolver_b200 import BatchedIISPHFluidSolver3D
+    from fluidsolver_b200 import _lib as F
+    from fluidsolver_b200 import scenes
+    L = F.lib()
+    allsc = scenes.batched_dams(256, seed=6)
+    mine = [s for i, s in enumerate(allsc) if i % world == rank]
+    batch = BatchedIISPHFluidSolver3D([s.collection for s in mine], device=device)
+    configure_iisph(batch)
+    batch.run(args.warmup)
+    stream = torch.cuda.ExternalStream(L.fs_stream(batch.ctx), device=torch.device("cuda", device))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    st = batch.run(args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    fluid_all = sum(s.n_fluid for s in allsc)
+    out = {"workload": f"{len(allsc)} breaking dams (seed 6): fluid {min(s.n_fluid for s in allsc):,}-"
+                       f"{max(s.n_fluid for s in allsc):,} per scene, {fluid_all:,} fluid + "
+                       f"{sum(s.n_boundary for s in allsc):,} boundary in total, one batched context per GPU",
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+           "value": fluid_all * args.steps / (ms / 1e3), "unit": UNIT,
+           "iterations_last_step": {"min": int(min(x.iterations for x in st)), "max": int(max(x.iterations for x in st))},
+           "avg_density_error_max": float(max(x.avg_density_error_fp64 for x in st))}
+    batch.close()
+    if world == 1:
+        total_ms = 0.0
+        for sc in allsc:
+            solver = make_solver(sc, device)
+            solver.run(args.warmup)
+            s2 = torch.cuda.ExternalStream(L.fs_stream(solver.ctx), device=torch.device("cuda", device))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record(s2)
+            solver.run(args.steps)
+            b.record(s2)
+            torch.cuda.synchronize()
+            total_ms += a.elapsed_time(b)
+            solver.close()
+        out["plain_per_scene_value"] = fluid_all * args.steps / (total_ms / 1e3)
+        out["plain_per_scene_ms_per_step"] = total_ms / args.steps
+        out["speedup_vs_plain_per_scene"] = out["value"] / out["plain_per_scene_value"]
+    return out
 
 
 def run_e2e(solver, scene, steps, device, max_over_ranks):
@@ -383,6 +445,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32-kahan", choices=["fp32", "fp32-kahan", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 256-scene batched measurement")
     ap.add_argument("--eager", action="store_true",
                     help="host-driven pressure loop instead of the whole-step CUDA graph: for kernel-level profiling "
                          "(ncu cannot profile the kernels of a graph with conditional nodes); slower, not a bench value")

@@ -3,6 +3,7 @@ search, SESPH and IISPH in 2D and 3D) behind a C-ABI; this package is the
 Python host mirror of libFluid's solver interfaces over that C-ABI."""
 from ._lib import FluidSolverError, lib  # noqa: F401
 from .solver import (  # noqa: F401
+    BatchedIISPHFluidSolver3D,
     IISPHFluidSolver,
     IISPHFluidSolver3D,
     NeighborhoodSearch,

@@ -97,6 +97,7 @@ template <typename R> State<R> state_of(fs_ctx* c) {
     s.err = (R*)c->err;
     s.type = c->type[c->cur];
     s.hidx = c->hidx[c->cur];
+    s.scene = c->scene_of[c->cur];
     return s;
 }
 
@@ -174,9 +175,8 @@ WalkParams walk_of(fs_ctx* c, bool for_solver) {
     w.candidates_inactive = c->include_inactive && !for_solver;
     w.trunc = c->truncate_cells;
     w.length_test = c->dim == 2;
-    w.d0 = c->dims[0];
-    w.d1 = c->dims[1];
-    w.d2 = c->dims[2];
+    w.grids = c->grids;
+    w.scene = c->scene_of[c->cur];
     w.cells = c->cells;
     return w;
 }
@@ -239,7 +239,8 @@ fs_status free_all(fs_ctx* c) {
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc[0], c->acc[1], c->ext[0], c->ext[1],
                     c->rho[0], c->rho[1], c->p[0], c->p[1], c->type[0], c->type[1], c->hidx[0], c->hidx[1],
                     c->rho_prev, c->vstar, c->anp, c->err, c->tile_desc, c->tile_ent, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
-                    c->perm[0], c->perm[1], c->cub_temp, c->cell_start, c->cell_counts, c->bbox, c->origin, c->nbr, c->nbr_count,
+                    c->perm[0], c->perm[1], c->cub_temp, c->cell_start, c->cell_counts, c->bbox, c->grids, c->nbr, c->nbr_count,
+                    c->scene_of[0], c->scene_of[1], c->d_scene_offsets,
                     c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->scalars};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -290,14 +291,13 @@ fs_status ensure_lists(fs_ctx* c, int K) {
     return FS_OK;
 }
 
-// Grid dims from the cell bounding box of the uploaded particles (lo > hi on
+// A scene's grid dims from the cell bounding box of its particles (lo > hi on
 // an axis: no finite coordinate there): the box plus a margin of a sixteenth
 // of its extent (at least 2 cells, which the 9-row walk needs) on each side,
-// shrunk until the grid has at most max(4M, 8 * capacity) cells (2^30 at
-// most). Particles that later leave the grid are clamped into its border
-// cells and take the exact per-cell walk.
-void choose_dims(fs_ctx* c, const int* lo_in, const int* hi_in) {
-    const int dim = c->dim;
+// shrunk until the grid has at most max_cells cells. Particles that later
+// leave the grid are clamped into its border cells and take the exact
+// per-cell walk.
+void choose_dims(int dim, int64_t max_cells, const int* lo_in, const int* hi_in, int* dims) {
     int lo[3] = {lo_in[0], lo_in[1], lo_in[2]}, hi[3] = {hi_in[0], hi_in[1], hi_in[2]};
     int64_t ext[3] = {1, 1, 1};
     for (int a = 0; a < dim; a++) {
@@ -306,18 +306,40 @@ void choose_dims(fs_ctx* c, const int* lo_in, const int* hi_in) {
         int64_t margin = std::max<int64_t>(2, e / 16);
         ext[a] = std::min<int64_t>(int64_t(1) << 20, e + 2 * margin);
     }
-    const int64_t max_cells =
-        std::min<int64_t>(int64_t(1) << 30, std::max<int64_t>(int64_t(1) << 22, 8 * std::max<int64_t>(c->cap, 1)));
     while (ext[0] * ext[1] * ext[2] > max_cells) {
         int a = (ext[0] >= ext[1] && ext[0] >= ext[2]) ? 0 : (ext[1] >= ext[2] ? 1 : 2);
         ext[a] = std::max<int64_t>(1, (ext[a] * 3) / 4);
     }
-    for (int a = 0; a < 3; a++) c->dims[a] = (int)ext[a];
+    for (int a = 0; a < 3; a++) dims[a] = (int)ext[a];
+}
+
+// every scene's grid from its box (lo[3 s + a], hi[3 s + a]); scene s may
+// hold up to max(4M, 8 * its particles) cells, and all scenes 2^30
+fs_status choose_grids(fs_ctx* c, const int* lo, const int* hi) {
+    const int S = c->nsc();
+    c->grids_host.assign(S, SceneGrid{});
+    int64_t base = 0;
+    for (int sidx = 0; sidx < S; sidx++) {
+        const int64_t np = c->scenes > 0 ? c->scene_offsets[sidx + 1] - c->scene_offsets[sidx] : c->cap;
+        const int64_t max_cells = std::max<int64_t>(int64_t(1) << 22, 8 * std::max<int64_t>(np, 1));
+        int d[3];
+        choose_dims(c->dim, max_cells, lo + 3 * sidx, hi + 3 * sidx, d);
+        SceneGrid& g = c->grids_host[sidx];
+        g.d0 = d[0];
+        g.d1 = d[1];
+        g.d2 = d[2];
+        g.base = base;
+        base += (int64_t)d[0] * d[1] * d[2];
+    }
+    if (base > (int64_t(1) << 30)) return fail(FS_ERR_INVALID, "the scenes' cell grids exceed 2^30 cells");
+    for (int a = 0; a < 3; a++) c->dims[a] = a == 0 ? c->grids_host[0].d0 : (a == 1 ? c->grids_host[0].d1 : c->grids_host[0].d2);
+    c->cells = base;
+    FS_CUDA(cudaMemcpyAsync(c->grids, c->grids_host.data(), sizeof(SceneGrid) * S, cudaMemcpyHostToDevice, c->stream));
+    return FS_OK;
 }
 
 // cell tables for the current dims (and the scan's temporary storage)
 fs_status ensure_cells(fs_ctx* c) {
-    c->cells = (int64_t)c->dims[0] * c->dims[1] * c->dims[2];
     c->key_bits = 1;
     while ((int64_t(1) << c->key_bits) < c->cells) c->key_bits++;
     c->regions = c->reference_order ? 1 : (c->include_inactive ? 3 : 2);
@@ -346,11 +368,23 @@ fs_status ensure_cells(fs_ctx* c) {
 // ---------------------------------------------------------------------------
 // upload / download
 // ---------------------------------------------------------------------------
+// scene of host particle i: the last s with offsets[s] <= i
+__device__ __forceinline__ int scene_of_host(const int64_t* __restrict__ offsets, int scenes, int64_t i) {
+    int lo = 0, hi = scenes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (offsets[mid] <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 template <typename R>
 __global__ void k_pack(int64_t n, int dim, const float* __restrict__ pos, const float* __restrict__ vel,
                        const float* __restrict__ acc, const float* __restrict__ ext, const float* __restrict__ mass,
                        const float* __restrict__ rho, const float* __restrict__ p, const uint8_t* __restrict__ type,
-                       float rest_density, State<R> s, uint8_t* __restrict__ type_out, uint32_t* __restrict__ hidx_out) {
+                       float rest_density, State<R> s, uint8_t* __restrict__ type_out, uint32_t* __restrict__ hidx_out,
+                       const int64_t* __restrict__ offsets, int scenes, uint16_t* __restrict__ scene_out) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     auto ld = [&](const float* a) -> V3<R> {
@@ -365,6 +399,7 @@ __global__ void k_pack(int64_t n, int dim, const float* __restrict__ pos, const 
     s.p[i] = p ? (R)p[i] : R(0);
     type_out[i] = type ? type[i] : (uint8_t)FS_TYPE_NORMAL;
     hidx_out[i] = (uint32_t)i;
+    if (scene_out) scene_out[i] = (uint16_t)scene_of_host(offsets, scenes, i);
 }
 
 // field f of the sorted state, scattered to host order
@@ -402,38 +437,70 @@ __global__ void k_unpack(int64_t n, int dim, int field, State<R> s, float* __res
 // in the cell structure.
 struct UploadCensus {
     unsigned long long counts[4];
-    int lo[3], hi[3];
 };
 
+// one particle per thread; per-scene boxes in bbox (mins [3 scenes], maxs
+// [3 scenes]), reduced per block when the block lies in one scene
 __global__ void k_census(int64_t n, int dim, const float* __restrict__ pos, const uint8_t* __restrict__ type, float r,
-                         bool include_inactive, UploadCensus* __restrict__ out) {
-    unsigned int cnt[4] = {0, 0, 0, 0};
+                         bool include_inactive, const int64_t* __restrict__ offsets, int scenes,
+                         UploadCensus* __restrict__ out, int* __restrict__ bbox) {
+    __shared__ unsigned int s_cnt[4];
+    __shared__ int s_first;
+    __shared__ int s_b[6][32];
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int sk = (i < n && offsets) ? scene_of_host(offsets, scenes, i) : 0;
+    if (threadIdx.x < 4) s_cnt[threadIdx.x] = 0;
+    if (threadIdx.x == 0) s_first = sk;
+    __syncthreads();
     int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i < n) {
         const uint8_t t = type ? type[i] : (uint8_t)FS_TYPE_NORMAL;
-        cnt[t <= 2 ? t : 3]++;
-        if (!include_inactive && t == FS_TYPE_INACTIVE) continue;
-        for (int a = 0; a < dim; a++) {
-            const float x = pos[i * dim + a];
-            if (!(fabsf(x) < 1e30f)) continue;
-            const int cc = (int)fmaxf(-1.0e9f, fminf(1.0e9f, floorf(x / r)));
-            lo[a] = min(lo[a], cc);
-            hi[a] = max(hi[a], cc);
+        atomicAdd(&s_cnt[t <= 2 ? t : 3], 1u);
+        if (include_inactive || t != FS_TYPE_INACTIVE) {
+            for (int a = 0; a < dim; a++) {
+                const float x = pos[i * dim + a];
+                if (!(fabsf(x) < 1e30f)) continue;
+                const int cc = (int)fmaxf(-1.0e9f, fminf(1.0e9f, floorf(x / r)));
+                lo[a] = cc;
+                hi[a] = cc;
+            }
         }
     }
+    const int s0 = s_first;
+    const bool uniform = __syncthreads_and(i >= n || sk == s0);
+    if (threadIdx.x < 4 && s_cnt[threadIdx.x]) atomicAdd(&out->counts[threadIdx.x], (unsigned long long)s_cnt[threadIdx.x]);
+    if (!uniform) {
+        for (int a = 0; a < 3; a++) {
+            if (lo[a] != INT_MAX) atomicMin(&bbox[3 * sk + a], lo[a]);
+            if (hi[a] != INT_MIN) atomicMax(&bbox[3 * scenes + 3 * sk + a], hi[a]);
+        }
+        return;
+    }
     for (int o = 16; o > 0; o >>= 1) {
-        for (int t = 0; t < 4; t++) cnt[t] += __shfl_xor_sync(0xffffffffu, cnt[t], o);
         for (int a = 0; a < 3; a++) {
             lo[a] = min(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
             hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
         }
     }
-    if ((threadIdx.x & 31) == 0) {
-        for (int t = 0; t < 4; t++)
-            if (cnt[t]) atomicAdd(&out->counts[t], (unsigned long long)cnt[t]);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0)
         for (int a = 0; a < 3; a++) {
-            if (lo[a] != INT_MAX) atomicMin(&out->lo[a], lo[a]);
-            if (hi[a] != INT_MIN) atomicMax(&out->hi[a], hi[a]);
+            s_b[a][wid] = lo[a];
+            s_b[3 + a][wid] = hi[a];
+        }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+        for (int a = 0; a < 3; a++) {
+            int l = lane < nw ? s_b[a][lane] : INT_MAX, h = lane < nw ? s_b[3 + a][lane] : INT_MIN;
+            for (int o = 16; o > 0; o >>= 1) {
+                l = min(l, __shfl_xor_sync(0xffffffffu, l, o));
+                h = max(h, __shfl_xor_sync(0xffffffffu, h, o));
+            }
+            if (lane == 0) {
+                if (l != INT_MAX) atomicMin(&bbox[3 * s0 + a], l);
+                if (h != INT_MIN) atomicMax(&bbox[3 * scenes + 3 * s0 + a], h);
+            }
         }
     }
 }
@@ -446,7 +513,16 @@ struct StagedUpload {
     UploadCensus* census = nullptr;
 };
 
-fs_status stage_upload(fs_ctx* c, const fs_particles* in, StagedUpload& d, UploadCensus& h) {
+// resets the per-scene box table (mins high, maxs low)
+fs_status reset_bbox(fs_ctx* c) {
+    const int S = c->nsc();
+    FS_CUDA(cudaMemsetAsync(c->bbox, 0x7f, 3 * S * sizeof(int), c->stream));
+    FS_CUDA(cudaMemsetAsync(c->bbox + 3 * S, 0x80, 3 * S * sizeof(int), c->stream));
+    return FS_OK;
+}
+
+// boxes: per-scene census box (mins [3 scenes], maxs [3 scenes])
+fs_status stage_upload(fs_ctx* c, const fs_particles* in, StagedUpload& d, UploadCensus& h, std::vector<int>& boxes) {
     const int64_t n = in->n;
     const size_t vec = (size_t)n * c->dim * sizeof(float), sc = (size_t)n * sizeof(float);
     FS_TRY(ensure_staging(c, 4 * vec + 3 * sc + (size_t)n + 16 * 9 + sizeof(UploadCensus)));
@@ -469,16 +545,21 @@ fs_status stage_upload(fs_ctx* c, const fs_particles* in, StagedUpload& d, Uploa
     d.p = (const float*)put(in->pressure, sc);
     d.type = (const uint8_t*)put(in->type, (size_t)n);
     d.census = (UploadCensus*)(st + off);
-    h = UploadCensus{{0, 0, 0, 0}, {INT_MAX, INT_MAX, INT_MAX}, {INT_MIN, INT_MIN, INT_MIN}};
+    h = UploadCensus{{0, 0, 0, 0}};
     if (e == cudaSuccess) e = cudaMemcpyAsync(d.census, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) return fail(FS_ERR_CUDA, cudaGetErrorString(e));
+    FS_TRY(reset_bbox(c));
+    const int S = c->nsc();
     if (n > 0) {
         c->launches++;
-        k_census<<<(int)std::min<int64_t>((n + 255) / 256, 592), 256, 0, c->stream>>>(
-            n, c->dim, d.pos, d.type, c->search_radius, c->include_inactive, d.census);
+        k_census<<<grid_for(n, 256), 256, 0, c->stream>>>(n, c->dim, d.pos, d.type, c->search_radius,
+                                                           c->include_inactive, c->d_scene_offsets, S, d.census,
+                                                           c->bbox);
         FS_CUDA(cudaGetLastError());
     }
+    boxes.assign(6 * (size_t)S, 0);
     FS_CUDA(cudaMemcpyAsync(&h, d.census, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    FS_CUDA(cudaMemcpyAsync(boxes.data(), c->bbox, sizeof(int) * 6 * S, cudaMemcpyDeviceToHost, c->stream));
     FS_CUDA(cudaStreamSynchronize(c->stream));
     return FS_OK;
 }
@@ -489,7 +570,8 @@ template <typename R> fs_status pack_upload(fs_ctx* c, const StagedUpload& d, in
     State<R> s = state_of<R>(c);
     c->launches++;
     k_pack<R><<<grid_for(n), kBlock, 0, c->stream>>>(n, c->dim, d.pos, d.vel, d.acc, d.ext, d.mass, d.rho, d.p, d.type,
-                                                     c->prm.rest_density, s, c->type[0], c->hidx[0]);
+                                                     c->prm.rest_density, s, c->type[0], c->hidx[0],
+                                                     c->d_scene_offsets, c->nsc(), c->scene_of[0]);
     FS_CUDA(cudaGetLastError());
     FS_CUDA(cudaStreamSynchronize(c->stream));
     return FS_OK;
@@ -538,20 +620,18 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     }
     State<R> s = state_of<R>(c);
     // bbox of the structure's cells -> grid origin
-    FS_CUDA(cudaMemsetAsync(c->bbox, 0x7f, 3 * sizeof(int), st));
-    FS_CUDA(cudaMemsetAsync(c->bbox + 3, 0x80, 3 * sizeof(int), st));
-    const unsigned gb = std::min<unsigned>(grid_for(n, 256), 148u * 8u);
+    FS_TRY(reset_bbox(c));
     c->launches++;
-    k_bbox<R><<<gb, 256, 0, st>>>(n, s.pos, s.type, c->include_inactive, c->search_radius, c->truncate_cells, c->bbox,
-                                  c->status);
+    k_bbox<R><<<grid_for(n, 256), 256, 0, st>>>(n, s.pos, s.type, s.scene, c->nsc(), c->include_inactive,
+                                                 c->search_radius, c->truncate_cells, c->bbox);
     c->launches++;
-    k_origin<<<1, 32, 0, st>>>(c->bbox, c->origin, c->dims[0], c->dims[1], c->dims[2]);
+    k_origin<<<grid_for(c->nsc(), 128), 128, 0, st>>>(c->bbox, c->grids, c->nsc());
     // keys + sort
     unsigned long long* k64 = single ? c->keys64[0] : nullptr;
     c->launches++;
     k_keys<R><<<grid_for(n), kBlock, 0, st>>>(n, s.pos, s.type, s.hidx, c->include_inactive, single, c->search_radius,
-                                              c->truncate_cells, c->origin, c->dims[0], c->dims[1], c->dims[2], c->key_bits,
-                                              c->keys[0], k64, c->perm[0]);
+                                              c->truncate_cells, c->grids, s.scene, c->key_bits, c->keys[0], k64,
+                                              c->perm[0]);
     FS_CUDA(cudaGetLastError());
     size_t temp = c->cub_temp_bytes;
     if (single) {
@@ -568,7 +648,7 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
         n, c->perm[1], (const V4<R>*)c->pos[c->cur], (V4<R>*)c->pos[nx], (const V4<R>*)c->vel[c->cur],
         (V4<R>*)c->vel[nx], (const V4<R>*)c->acc[c->cur], (V4<R>*)c->acc[nx], (const V4<R>*)c->ext[c->cur],
         (V4<R>*)c->ext[nx], (const R*)c->rho[c->cur], (R*)c->rho[nx], (const R*)c->p[c->cur], (R*)c->p[nx],
-        c->type[c->cur], c->type[nx], c->hidx[c->cur], c->hidx[nx]);
+        c->type[c->cur], c->type[nx], c->hidx[c->cur], c->hidx[nx], c->scene_of[c->cur], c->scene_of[nx]);
     FS_CUDA(cudaGetLastError());
     c->cur = nx;
     s = state_of<R>(c);
@@ -594,7 +674,7 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
                 const int64_t tiles = (c->n_owners + kTileOwners - 1) / kTileOwners;
                 c->launches++;
                 k_build_tiles<<<(unsigned)tiles, kTileOwners, tile_build_smem(c->nbr_capacity), st>>>(
-                    c->n_owners, s.pos, s.type, c->cell_start, c->origin, w, c->tile_desc, c->tile_ent,
+                    c->n_owners, s.pos, s.type, c->cell_start, w, c->tile_desc, c->tile_ent,
                     c->tile_stride, c->nbr, c->nbr_stride, c->nbr_capacity, c->nbr_count, c->status, c->scalars);
                 built = true;
             }
@@ -602,7 +682,7 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
         if (!built) {
             c->launches++;
             k_build_lists<R><<<grid_for(c->n_owners), kBlock, 0, st>>>(
-                c->n_owners, s.pos, s.type, c->cell_start, c->origin, w, owners, rows, c->nbr, c->nbr_stride,
+                c->n_owners, s.pos, s.type, c->cell_start, w, owners, rows, c->nbr, c->nbr_stride,
                 c->nbr_capacity, c->nbr_count, c->status, c->scalars);
         }
         FS_CUDA(cudaGetLastError());
@@ -629,7 +709,8 @@ void set_layout(fs_ctx* c, int64_t n, int64_t nf, int64_t nb, int64_t ni) {
 }
 
 fs_status read_scalars(fs_ctx* c) {
-    FS_CUDA(cudaMemcpyAsync(c->scalars_host, c->scalars, sizeof(StepScalars), cudaMemcpyDeviceToHost, c->stream));
+    FS_CUDA(cudaMemcpyAsync(c->scalars_host, c->scalars, sizeof(StepScalars) * c->nsc(), cudaMemcpyDeviceToHost,
+                            c->stream));
     FS_CUDA(cudaStreamSynchronize(c->stream));
     return FS_OK;
 }
@@ -653,12 +734,14 @@ fs_status mark(fs_ctx* c, int i, cudaStream_t st) {
 
 // resets the per-step scalars; keep_search keeps the statistics of the
 // search that precedes the solver phases
-__global__ void k_step_begin(StepScalars* sc, float desired_dt, bool keep_search) {
+__global__ void k_step_begin(StepScalars* sc, int scenes, float desired_dt, bool keep_search) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= scenes) return;
     StepScalars z{};
     z.desired_dt = desired_dt;
     z.dt = desired_dt;
-    if (keep_search) z.max_neighbors = sc->max_neighbors;
-    *sc = z;
+    if (keep_search) z.max_neighbors = sc[i].max_neighbors;
+    sc[i] = z;
 }
 
 // ---------------------------------------------------------------------------
@@ -678,11 +761,17 @@ fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_t
         for (int it = 0; it < max_it; it++) {
             body(st);
             c->launches++;
-            k_iisph_check<<<1, 1, 0, st>>>(c->scalars, c->prm.min_iterations, max_it, c->prm.max_density_error,
-                                           fp64_test, two_d, c->status, 0, false);
+            if (c->scenes > 0)
+                k_iisph_check_scenes<<<1, 256, 0, st>>>(c->scalars, c->scenes, c->prm.min_iterations, max_it,
+                                                        c->prm.max_density_error, c->status, 0, false);
+            else
+                k_iisph_check<<<1, 1, 0, st>>>(c->scalars, c->prm.min_iterations, max_it, c->prm.max_density_error,
+                                               fp64_test, two_d, c->status, 0, false);
             FS_CUDA(cudaGetLastError());
             FS_TRY(read_scalars(c));
-            if (c->scalars_host->done) break;
+            bool all_done = true;
+            for (int i = 0; i < c->nsc(); i++) all_done = all_done && c->scalars_host[i].done;
+            if (all_done) break;
         }
         return FS_OK;
     }
@@ -706,8 +795,12 @@ fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_t
                                           cudaStreamCaptureModeRelaxed));
     body(c->body_stream);
     c->launches++;
-    k_iisph_check<<<1, 1, 0, c->body_stream>>>(c->scalars, c->prm.min_iterations, max_it, c->prm.max_density_error,
-                                                fp64_test, two_d, c->status, handle, true);
+    if (c->scenes > 0)
+        k_iisph_check_scenes<<<1, 256, 0, c->body_stream>>>(c->scalars, c->scenes, c->prm.min_iterations, max_it,
+                                                            c->prm.max_density_error, c->status, handle, true);
+    else
+        k_iisph_check<<<1, 1, 0, c->body_stream>>>(c->scalars, c->prm.min_iterations, max_it,
+                                                    c->prm.max_density_error, fp64_test, two_d, c->status, handle, true);
     cudaError_t e = cudaGetLastError();
     cudaError_t e2 = cudaStreamEndCapture(c->body_stream, nullptr);
     if (e != cudaSuccess || e2 != cudaSuccess) return fail(FS_ERR_CUDA, "capture of the pressure loop failed");
@@ -744,7 +837,7 @@ fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
     }));
     FS_TRY(mark(c, 4, st));
     c->launches++;
-    k_cfl<<<1, 1, 0, st>>>(c->scalars, c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
+    k_cfl<<<1, 128, 0, st>>>(c->scalars, c->nsc(), c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
                            c->status);
     c->launches++;
     k_iisph3d_integrate<float><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
@@ -794,7 +887,7 @@ template <typename R, bool KAHAN> fs_status step_iisph3d(fs_ctx* c, bool capture
     }));
     FS_TRY(mark(c, 4, st));
     c->launches++;
-    k_cfl<<<1, 1, 0, st>>>(c->scalars, c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
+    k_cfl<<<1, 128, 0, st>>>(c->scalars, c->nsc(), c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
                            c->status);
     c->launches++;
     k_iisph3d_integrate<R><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
@@ -822,7 +915,7 @@ template <typename R, bool KAHAN> fs_status step_sesph(fs_ctx* c) {
     c->launches++;
         k_sesph_maxima_final<<<1, 1, 0, st>>>(c->scalars);
     c->launches++;
-        k_cfl<<<1, 1, 0, st>>>(c->scalars, c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
+        k_cfl<<<1, 128, 0, st>>>(c->scalars, c->nsc(), c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
                                c->status);
     }
     FS_TRY(mark(c, 4, st));
@@ -890,19 +983,23 @@ fs_status search_dispatch(fs_ctx* c, bool solver_lists) {
     return search_impl<float>(c, solver_lists);
 }
 
-fs_status fill_stats(fs_ctx* c, fs_step_stats* stats, int st) {
-    const StepScalars& h = *c->scalars_host;
-    if (stats) {
-        stats->desired_dt = h.desired_dt;
-        stats->actual_dt = h.dt;
-        stats->iterations = h.iteration;
-        stats->avg_density_error = h.avg_err;
-        stats->avg_density_error_fp64 = h.avg_err64;
-        stats->max_density_error = h.max_err;
-        stats->max_velocity = std::sqrt(h.final_max_v2);
-        stats->max_acceleration = std::sqrt(h.final_max_a2);
-        stats->status = st;
-        stats->max_neighbors = h.max_neighbors;
+// the statistics of scenes [0, entries) (the search's largest list is
+// counted in scene 0's scalars for all scenes)
+fs_status fill_stats(fs_ctx* c, fs_step_stats* stats, int st, int entries = 1) {
+    if (!stats) return FS_OK;
+    for (int i = 0; i < std::min(entries, c->nsc()); i++) {
+        const StepScalars& h = c->scalars_host[i];
+        fs_step_stats& o = stats[i];
+        o.desired_dt = h.desired_dt;
+        o.actual_dt = h.dt;
+        o.iterations = h.iteration;
+        o.avg_density_error = h.avg_err;
+        o.avg_density_error_fp64 = h.avg_err64;
+        o.max_density_error = h.max_err;
+        o.max_velocity = std::sqrt(h.final_max_v2);
+        o.max_acceleration = std::sqrt(h.final_max_a2);
+        o.status = st;
+        o.max_neighbors = c->scalars_host[0].max_neighbors;
     }
     return FS_OK;
 }
@@ -913,7 +1010,7 @@ fs_status fill_stats(fs_ctx* c, fs_step_stats* stats, int st) {
 fs_status search_for_step(fs_ctx* c, float dt) {
     for (int attempt = 0; attempt < 2; attempt++) {
         c->launches++;
-        k_step_begin<<<1, 1, 0, c->stream>>>(c->scalars, dt, false);
+        k_step_begin<<<grid_for(c->nsc(), 128), 128, 0, c->stream>>>(c->scalars, c->nsc(), dt, false);
         FS_CUDA(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
         cudaEventRecord(c->ev[0], c->stream);
         FS_TRY(search_dispatch(c, c->prm.solver != FS_SOLVER_NONE));
@@ -972,12 +1069,12 @@ fs_status solve_graph(fs_ctx* c, float dt, bool with_search = false) {
     fs_status r = FS_OK;
     if (with_search) {
         c->launches++;
-        k_step_begin<<<1, 1, 0, c->stream>>>(c->scalars, dt, false);
+        k_step_begin<<<grid_for(c->nsc(), 128), 128, 0, c->stream>>>(c->scalars, c->nsc(), dt, false);
         r = mark(c, 0, c->stream);
         if (r == FS_OK) r = search_dispatch(c, true);
     }
     c->launches++;
-    k_step_begin<<<1, 1, 0, c->stream>>>(c->scalars, dt, true);
+    k_step_begin<<<grid_for(c->nsc(), 128), 128, 0, c->stream>>>(c->scalars, c->nsc(), dt, true);
     if (r == FS_OK) r = step_dispatch_any(c, true);
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
@@ -1014,7 +1111,7 @@ fs_status solve_after_search(fs_ctx* c, float dt, fs_step_stats* stats) {
         FS_TRY(solve_graph(c, dt));
     } else {
         c->launches++;
-        k_step_begin<<<1, 1, 0, c->stream>>>(c->scalars, dt, true);
+        k_step_begin<<<grid_for(c->nsc(), 128), 128, 0, c->stream>>>(c->scalars, c->nsc(), dt, true);
         FS_TRY(step_dispatch_any(c, false));
     }
     c->have_lists = false;  // positions moved: the lists belong to the old positions
@@ -1104,7 +1201,9 @@ void fs_params_default(fs_params* p, int32_t dim, int32_t solver, int32_t search
     p->device = 0;
 }
 
-fs_status fs_create(const fs_params* p, fs_ctx** out) {
+// a context for one scene (scenes == 0) or for `scenes` batched scenes whose
+// host particles are [offsets[s], offsets[s + 1])
+static fs_status create_ctx(const fs_params* p, int32_t scenes, const int64_t* offsets, fs_ctx** out) {
     if (!out) return fail(FS_ERR_INVALID, "out is null");
     *out = nullptr;
     FS_TRY(check_params(p));
@@ -1121,6 +1220,11 @@ fs_status fs_create(const fs_params* p, fs_ctx** out) {
     c->device = p->device;
     derive(c);
     c->cap = p->max_particles;
+    if (scenes > 0) {
+        c->scenes = scenes;
+        c->scene_offsets.assign(offsets, offsets + scenes + 1);
+        c->cap = std::max<int64_t>(c->cap, offsets[scenes]);
+    }
     auto bail = [&](fs_status s) {
         free_all(c);
         delete c;
@@ -1151,12 +1255,21 @@ fs_status fs_create(const fs_params* p, fs_ctx** out) {
     FS_ALLOC(*(char**)&c->vstar, cap * v4);
     FS_ALLOC(*(char**)&c->anp, cap * v4);
     FS_ALLOC(*(char**)&c->err, cap * r1);
-    FS_ALLOC(c->bbox, 6);
-    FS_ALLOC(c->origin, 4);
+    const int S = c->nsc();
+    FS_ALLOC(c->bbox, 6 * S);
+    FS_ALLOC(c->grids, S);
     FS_ALLOC(c->status, 1);
-    FS_ALLOC(c->scalars, 1);
+    FS_ALLOC(c->scalars, S);
+    if (scenes > 0) {
+        FS_ALLOC(c->scene_of[0], cap);
+        FS_ALLOC(c->scene_of[1], cap);
+        FS_ALLOC(c->d_scene_offsets, scenes + 1);
+        if (cudaMemcpy(c->d_scene_offsets, offsets, sizeof(int64_t) * (scenes + 1), cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+            return bail(fail(FS_ERR_CUDA, "copy of the scene offsets failed"));
+    }
     FS_ALLOC(c->nbr_count, (cap + kTileOwners - 1) / kTileOwners * kTileOwners);   // whole tiles
-    if (cudaMallocHost((void**)&c->scalars_host, sizeof(StepScalars)) != cudaSuccess)
+    if (cudaMallocHost((void**)&c->scalars_host, sizeof(StepScalars) * S) != cudaSuccess)
         return bail(fail(FS_ERR_CUDA, "cudaMallocHost failed"));
     // CUB temp storage for the largest sort
     size_t temp = 0;
@@ -1186,6 +1299,8 @@ fs_status fs_create(const fs_params* p, fs_ctx** out) {
     return FS_OK;
 }
 
+fs_status fs_create(const fs_params* p, fs_ctx** out) { return create_ctx(p, 0, nullptr, out); }
+
 fs_status fs_destroy(fs_ctx* c) {
     if (!c) return FS_OK;
     cudaSetDevice(c->device);
@@ -1214,15 +1329,18 @@ fs_status fs_upload(fs_ctx* c, const fs_particles* in) {
     if (!c || !in) return fail(FS_ERR_INVALID, "null argument");
     if (in->n < 0 || in->n > c->cap) return fail(FS_ERR_INVALID, "particle count exceeds the context capacity");
     if (in->n > 0 && !in->position) return fail(FS_ERR_INVALID, "position is required for upload");
+    if (c->scenes > 0 && in->n != c->scene_offsets[c->scenes])
+        return fail(FS_ERR_INVALID, "a batched upload holds exactly the particles of every scene");
     FS_CUDA(cudaSetDevice(c->device));
     StagedUpload d;
     UploadCensus h;
-    FS_TRY(stage_upload(c, in, d, h));
+    std::vector<int> boxes;
+    FS_TRY(stage_upload(c, in, d, h, boxes));
     if (h.counts[3]) return fail(FS_ERR_INVALID, "particle type must be 0, 1 or 2");
     const int64_t n_before = c->n, owners_before = c->n_owners;
     set_layout(c, in->n, (int64_t)h.counts[0], (int64_t)h.counts[1], (int64_t)h.counts[2]);
     if (c->n != n_before || c->n_owners != owners_before) clear_graphs(c);
-    choose_dims(c, h.lo, h.hi);
+    FS_TRY(choose_grids(c, boxes.data(), boxes.data() + 3 * c->nsc()));
     FS_TRY(ensure_cells(c));
     fs_status r = c->precision == FS_PRECISION_FP64 ? pack_upload<double>(c, d, in->n) : pack_upload<float>(c, d, in->n);
     if (r != FS_OK) return r;
@@ -1287,12 +1405,12 @@ fs_status fs_get_neighbors_csr(fs_ctx* c, int64_t* offsets, int64_t* indices, in
     if (c->precision == FS_PRECISION_FP64) {
         State<double> s = state_of<double>(c);
     c->launches++;
-        k_csr_count<double><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_start, c->origin, w, mask,
+        k_csr_count<double><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_start, w, mask,
                                                              c->csr_counts);
     } else {
         State<float> s = state_of<float>(c);
     c->launches++;
-        k_csr_count<float><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_start, c->origin, w, mask,
+        k_csr_count<float><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_start, w, mask,
                                                             c->csr_counts);
     }
     FS_CUDA(cudaGetLastError());
@@ -1326,12 +1444,12 @@ fs_status fs_get_neighbors_csr(fs_ctx* c, int64_t* offsets, int64_t* indices, in
     if (c->precision == FS_PRECISION_FP64) {
         State<double> s = state_of<double>(c);
     c->launches++;
-        k_csr_fill<double><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_start, c->origin, w, mask,
+        k_csr_fill<double><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_start, w, mask,
                                                             c->csr_offsets, d_idx);
     } else {
         State<float> s = state_of<float>(c);
     c->launches++;
-        k_csr_fill<float><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_start, c->origin, w, mask,
+        k_csr_fill<float><<<grid_for(ns), kBlock, 0, st>>>(ns, s.pos, s.type, c->cell_start, w, mask,
                                                            c->csr_offsets, d_idx);
     }
     std::vector<uint32_t> idx((size_t)tot);
@@ -1357,6 +1475,7 @@ fs_status fs_query_position(fs_ctx* c, const float* position, int64_t* out, int6
     if (!c || !position) return fail(FS_ERR_INVALID, "null argument");
     if (cap > 0 && !out) return fail(FS_ERR_INVALID, "out is null");
     if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    if (c->scenes > 0) return fail(FS_ERR_INVALID, "a position query names no scene: not available on batched contexts");
     const int search = c->prm.search;
     if (search == FS_SEARCH_COMPACT_2D)
         return fail(FS_ERR_INVALID, "the compact-hashing contract has no position query (it throws \"Not implemented\")");
@@ -1386,14 +1505,14 @@ fs_status fs_query_position(fs_ctx* c, const float* position, int64_t* out, int6
         const V3<double> x = v3<double>(position[0], position[1], z);
         c->launches++;
         if (all) k_query_all<double><<<gq, kBlock, 0, c->stream>>>(x, c->n, s.pos, w, d_out, room, d_cnt);
-        else k_query_position<double><<<1, 32, 0, c->stream>>>(x, s.pos, s.type, s.hidx, c->cell_start, c->origin, w,
+        else k_query_position<double><<<1, 32, 0, c->stream>>>(x, s.pos, s.type, s.hidx, c->cell_start, w,
                                                                skip, d_out, room, d_cnt);
     } else {
         State<float> s = state_of<float>(c);
         const V3<float> x = v3<float>(position[0], position[1], z);
         c->launches++;
         if (all) k_query_all<float><<<gq, kBlock, 0, c->stream>>>(x, c->n, s.pos, w, d_out, room, d_cnt);
-        else k_query_position<float><<<1, 32, 0, c->stream>>>(x, s.pos, s.type, s.hidx, c->cell_start, c->origin, w,
+        else k_query_position<float><<<1, 32, 0, c->stream>>>(x, s.pos, s.type, s.hidx, c->cell_start, w,
                                                               skip, d_out, room, d_cnt);
     }
     cudaError_t e = cudaGetLastError();
@@ -1454,13 +1573,36 @@ void* fs_stream(fs_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 int64_t fs_launch_count(fs_ctx* c) { return c ? c->launches : 0; }
 
-fs_status fs_batch_create(const fs_params*, int32_t, const int64_t*, fs_ctx** out) {
+fs_status fs_batch_create(const fs_params* p, int32_t scenes, const int64_t* offsets, fs_ctx** out) {
     if (out) *out = nullptr;
-    return fail(FS_ERR_INVALID, "batched scenes are not available in this build");
+    if (!p || !offsets || !out) return fail(FS_ERR_INVALID, "null argument");
+    if (scenes < 1 || scenes > 65535) return fail(FS_ERR_INVALID, "scenes must be 1..65535");
+    if (offsets[0] != 0) return fail(FS_ERR_INVALID, "offsets[0] must be 0");
+    for (int32_t i = 0; i < scenes; i++)
+        if (offsets[i + 1] < offsets[i]) return fail(FS_ERR_INVALID, "offsets must not decrease");
+    if (p->solver != FS_SOLVER_IISPH_3D || p->search != FS_SEARCH_HASHED_3D ||
+        p->precision != FS_PRECISION_FP32_KAHAN || (p->flags & FS_FLAG_REFERENCE_ORDER))
+        return fail(FS_ERR_INVALID,
+                    "batched scenes run the 3D IISPH solver with the hashed-3d contract in FP32 + Kahan, device order");
+    return create_ctx(p, scenes, offsets, out);
 }
 
-fs_status fs_batch_run(fs_ctx*, int32_t, float, fs_step_stats*) {
-    return fail(FS_ERR_INVALID, "batched scenes are not available in this build");
+fs_status fs_batch_run(fs_ctx* c, int32_t steps, float desired_dt, fs_step_stats* stats) {
+    if (!c) return fail(FS_ERR_INVALID, "ctx is null");
+    if (c->scenes == 0) return fail(FS_ERR_INVALID, "not a batched context (fs_batch_create)");
+    if (steps < 0) return fail(FS_ERR_INVALID, "steps must be >= 0");
+    FS_CUDA(cudaSetDevice(c->device));
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    if (steps == 0) return FS_OK;
+    FS_TRY(one_step(c, desired_dt, nullptr));
+    if (steps > 1) {
+        const float dt = desired_dt > 0.0f ? desired_dt : c->prm.timestep;
+        FS_TRY(enqueue_steps(c, steps - 1, dt));
+        int st = 0;
+        FS_TRY(finish_steps(c, nullptr, &st));
+        if (st != FS_OK) return fail((fs_status)st, "device reported an error during fs_batch_run");
+    }
+    return fill_stats(c, stats, FS_OK, c->scenes);
 }
 
 }  // extern "C"
@@ -1500,7 +1642,7 @@ unsigned long long* g_query_scratch_ptr[kNoAllocDevices] = {};
 template <typename R>
 __global__ void k_query_cells_noalloc(V3<R> x, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
                                       const uint32_t* __restrict__ hidx, const uint32_t* __restrict__ cell_start,
-                                      const int* __restrict__ origin, WalkParams w, bool skip_cell_min,
+                                      WalkParams w, bool skip_cell_min,
                                       unsigned long long* __restrict__ scratch, int64_t cap) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     unsigned long long c = 0;
@@ -1512,10 +1654,11 @@ __global__ void k_query_cells_noalloc(V3<R> x, const V4<R>* __restrict__ pos, co
             for (int dz = -zr; dz <= zr; dz++, ordinal++) {
                 const int c0 = ci[0] + dx, c1 = ci[1] + dy, c2 = ci[2] + dz;
                 bool cl = false;
-                const int l0 = local_cell(c0, origin[0], w.d0, cl);
-                const int l1 = local_cell(c1, origin[1], w.d1, cl);
-                const int l2 = local_cell(c2, origin[2], w.d2, cl);
-                const int64_t lc = ((int64_t)l2 * w.d1 + l1) * w.d0 + l0;
+                const SceneGrid& gr = w.grids[0];
+                const int l0 = local_cell(c0, gr.o0, gr.d0, cl);
+                const int l1 = local_cell(c1, gr.o1, gr.d1, cl);
+                const int l2 = local_cell(c2, gr.o2, gr.d2, cl);
+                const int64_t lc = gr.base + ((int64_t)l2 * gr.d1 + l1) * gr.d0 + l0;
                 auto members = [&](auto&& f) {
                     for (int g = 0; g < w.regions; g++) {
                         const uint32_t* cs = cell_start + g * (w.cells + 1);
@@ -1579,7 +1722,7 @@ bool launch_query_noalloc(fs_ctx* c, const float* position, const WalkParams& w,
         const int g = (int)std::min<int64_t>((c->n + kBlock - 1) / kBlock, 1184);
         k_query_all_noalloc<R><<<g, kBlock, 0, c->stream>>>(x, c->n, s.pos, s.hidx, w, scratch, cap);
     } else {
-        k_query_cells_noalloc<R><<<1, 32, 0, c->stream>>>(x, s.pos, s.type, s.hidx, c->cell_start, c->origin, w, skip,
+        k_query_cells_noalloc<R><<<1, 32, 0, c->stream>>>(x, s.pos, s.type, s.hidx, c->cell_start, w, skip,
                                                           scratch, cap);
     }
     return cudaGetLastError() == cudaSuccess;
@@ -1594,6 +1737,7 @@ extern "C" fs_status fs_query_position_noalloc(fs_ctx* c, const float* position,
     if (cap < 0) return fail(FS_ERR_INVALID, "cap < 0");
     if (cap > FS_QUERY_NOALLOC_MAX) return fail(FS_ERR_INVALID, "cap > 65536");
     if (!c->have_state) return fail(FS_ERR_STATE, "no particles");
+    if (c->scenes > 0) return fail(FS_ERR_INVALID, "batched ctx");
     const int search = c->prm.search;
     if (search == FS_SEARCH_COMPACT_2D) return fail(FS_ERR_INVALID, "not supported");
     const bool all = search == FS_SEARCH_QUADRATIC_2D || search == FS_SEARCH_QUADRATIC_3D;

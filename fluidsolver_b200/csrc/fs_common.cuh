@@ -180,7 +180,15 @@ constexpr uint32_t kIndexMask = 0x7fffffffu;
 // device status word (first error wins)
 __device__ __forceinline__ void raise_status(int* status, int code) { atomicCAS(status, 0, code); }
 
-// per-step device scalars shared by the kernels of one step
+// One scene's cell grid: dims, this step's origin (cell coordinates) and the
+// offset of its cells in the concatenated cell tables.
+struct SceneGrid {
+    int d0, d1, d2;
+    int o0, o1, o2;
+    long long base;
+};
+
+// per-step device scalars shared by the kernels of one step (one set per scene)
 struct StepScalars {
     float desired_dt;        // Timepoint::desired_time_step
     float dt;                // current_timestep (after the CFL clamp: actual)

@@ -61,6 +61,7 @@ struct fs_ctx {
     void* p[2] = {};
     uint8_t* type[2] = {};
     uint32_t* hidx[2] = {};
+    uint16_t* scene_of[2] = {};      // per-particle scene (batched contexts only)
     int cur = 0;
     void* rho_prev = nullptr;
     void* vstar = nullptr;
@@ -79,9 +80,10 @@ struct fs_ctx {
     int key_bits = 30;                // bits of the linear cell index in the sort keys
     int64_t cell_alloc = 0;           // entries allocated per table
     int regions = 2;                  // regions in the sorted layout
-    int dims[3] = {1, 1, 1};
-    int* bbox = nullptr;           // device: min xyz, max xyz (cell coordinates)
-    int* origin = nullptr;         // device: cell-grid origin used this step
+    int dims[3] = {1, 1, 1};       // scene 0's grid dims
+    int* bbox = nullptr;           // device: per scene min xyz [3 scenes], then max xyz [3 scenes]
+    fsb::SceneGrid* grids = nullptr;            // device: per-scene grids (origins set every step)
+    std::vector<fsb::SceneGrid> grids_host;     // dims and bases
     uint32_t* nbr = nullptr;       // solver lists, slot-major: nbr[s * nbr_stride + k]
     fsb::TileDesc* tile_desc = nullptr;  // tile lists (3D IISPH fast path): per tile of owners
     uint4* tile_ent = nullptr;           // [K / 8][tile_stride] octets of 16-bit entries
@@ -136,7 +138,9 @@ struct fs_ctx {
     cudaEvent_t ev[6] = {};
     float phase_ms[5] = {};
 
-    // batched scenes
+    // batched scenes (0: a single-scene context)
     int32_t scenes = 0;
-    std::vector<int64_t> scene_offsets;
+    std::vector<int64_t> scene_offsets;   // host particles of scene s: [offsets[s], offsets[s+1])
+    int64_t* d_scene_offsets = nullptr;
+    int nsc() const { return scenes > 0 ? scenes : 1; }
 };

@@ -22,6 +22,11 @@
 // reference-order mode). cell_start[g][c] is the first sorted index of region
 // g whose cell is >= c (an exclusive scan of the per-cell counts).
 //
+// Scenes. A context holds one scene or many independent ones (batched mode).
+// Every scene has its own grid (SceneGrid: dims, this step's origin, and the
+// offset `base` of its cells in the concatenated cell tables), so particles
+// of different scenes never share a cell and never meet in a walk.
+//
 // A grid smaller than the bounding box is clamped: such particles go to border
 // cells. Particles in or next to border cells take a slow path that checks
 // every candidate's own cell; for all others no check is needed, because a
@@ -46,18 +51,39 @@ template <typename R> __device__ __forceinline__ int cell_coord(R x, float r, bo
 }
 
 // ---------------------------------------------------------------------------
-// bounding box of the cells of all particles in the structure
+// per-scene bounding box of the cells of the particles in the structure
 // ---------------------------------------------------------------------------
+// bbox[3 s .. 3 s + 2]: min xyz of scene s; bbox[3 scenes + 3 s ..]: its
+// max xyz (two memsets reset the table). scene: per-particle
+// scene ids (null: one scene). A block whose particles all belong to one
+// scene reduces first and issues one atomic per bound; a mixed block (a scene
+// boundary inside it) issues one per particle.
 template <typename R>
-__global__ void k_bbox(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type, bool include_inactive,
-                       float r, bool trunc, int* __restrict__ bbox, const int* __restrict__ status) {
+__global__ void k_bbox(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
+                       const uint16_t* __restrict__ scene, int scenes, bool include_inactive, float r, bool trunc,
+                       int* __restrict__ bbox) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        if (!include_inactive && type[k] == FS_TYPE_INACTIVE) continue;
-        V4<R> p = pos[k];
-        int c0 = cell_coord<R>(p.x, r, trunc), c1 = cell_coord<R>(p.y, r, trunc), c2 = cell_coord<R>(p.z, r, trunc);
-        mn[0] = min(mn[0], c0); mn[1] = min(mn[1], c1); mn[2] = min(mn[2], c2);
-        mx[0] = max(mx[0], c0); mx[1] = max(mx[1], c1); mx[2] = max(mx[2], c2);
+    const int sk = (k < n && scene) ? scene[k] : 0;
+    if (k < n && (include_inactive || type[k] != FS_TYPE_INACTIVE)) {
+        const V4<R> p = pos[k];
+        const int c[3] = {cell_coord<R>(p.x, r, trunc), cell_coord<R>(p.y, r, trunc), cell_coord<R>(p.z, r, trunc)};
+#pragma unroll
+        for (int a = 0; a < 3; a++) mn[a] = mx[a] = c[a];
+    }
+    __shared__ int s_first;
+    if (threadIdx.x == 0) s_first = sk;
+    __syncthreads();
+    const int s0 = s_first;
+    if (!__syncthreads_and(k >= n || sk == s0)) {
+        if (mn[0] != INT_MAX) {
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                atomicMin(&bbox[3 * sk + a], mn[a]);
+                atomicMax(&bbox[3 * scenes + 3 * sk + a], mx[a]);
+            }
+        }
+        return;
     }
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -66,7 +92,6 @@ __global__ void k_bbox(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* 
             mx[a] = max(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
         }
     }
-    // block reduction, then one atomic per bound and block
     __shared__ int s_b[6][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) {
@@ -87,25 +112,31 @@ __global__ void k_bbox(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* 
                 hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
             }
             if (lane == 0) {
-                if (lo != INT_MAX) atomicMin(&bbox[a], lo);
-                if (hi != INT_MIN) atomicMax(&bbox[3 + a], hi);
+                if (lo != INT_MAX) atomicMin(&bbox[3 * s0 + a], lo);
+                if (hi != INT_MIN) atomicMax(&bbox[3 * scenes + 3 * s0 + a], hi);
             }
         }
     }
 }
 
-// Grid origin for this step: the bbox minimum, shifted so that the box is
-// centred in the allocated dims when it is smaller.
-__global__ void k_origin(const int* __restrict__ bbox, int* __restrict__ origin, int d0, int d1, int d2) {
-    if (threadIdx.x != 0) return;
-    int d[3] = {d0, d1, d2};
+// Grid origin of every scene for this step: the bbox minimum, shifted so that
+// the box is centred in the scene's dims when it is smaller.
+__global__ void k_origin(const int* __restrict__ bbox, SceneGrid* __restrict__ grids, int scenes) {
+    const int sidx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sidx >= scenes) return;
+    SceneGrid& g = grids[sidx];
+    const int d[3] = {g.d0, g.d1, g.d2};
+    int o[3];
     for (int a = 0; a < 3; a++) {
-        int lo = bbox[a], hi = bbox[3 + a];
+        int lo = bbox[3 * sidx + a], hi = bbox[3 * scenes + 3 * sidx + a];
         if (lo > hi) { lo = 0; hi = 0; }
         long long ext = (long long)hi - lo + 1;
         long long slack = (long long)d[a] - ext;
-        origin[a] = (int)(slack > 0 ? (long long)lo - slack / 2 : (long long)lo);
+        o[a] = (int)(slack > 0 ? (long long)lo - slack / 2 : (long long)lo);
     }
+    g.o0 = o[0];
+    g.o1 = o[1];
+    g.o2 = o[2];
 }
 
 // clamped local cell of a cell coordinate; *clamped set when outside the grid
@@ -125,8 +156,8 @@ __device__ __forceinline__ uint32_t region_of(uint8_t t, bool single_region) {
 template <typename R>
 __global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
                        const uint32_t* __restrict__ hidx, bool include_inactive, bool single_region, float r,
-                       bool trunc, const int* __restrict__ origin, int d0, int d1, int d2, int key_bits,
-                       uint32_t* __restrict__ keys,
+                       bool trunc, const SceneGrid* __restrict__ grids, const uint16_t* __restrict__ scene,
+                       int key_bits, uint32_t* __restrict__ keys,
                        unsigned long long* __restrict__ keys64, uint32_t* __restrict__ perm) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -136,11 +167,12 @@ __global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* 
         key = inactive_key(key_bits);
     } else {
         V4<R> p = pos[k];
+        const SceneGrid g = grids[scene ? scene[k] : 0];
         bool cl = false;
-        int lx = local_cell(cell_coord<R>(p.x, r, trunc), origin[0], d0, cl);
-        int ly = local_cell(cell_coord<R>(p.y, r, trunc), origin[1], d1, cl);
-        int lz = local_cell(cell_coord<R>(p.z, r, trunc), origin[2], d2, cl);
-        const uint32_t lin = (uint32_t)(((int64_t)lz * d1 + ly) * d0 + lx);
+        int lx = local_cell(cell_coord<R>(p.x, r, trunc), g.o0, g.d0, cl);
+        int ly = local_cell(cell_coord<R>(p.y, r, trunc), g.o1, g.d1, cl);
+        int lz = local_cell(cell_coord<R>(p.z, r, trunc), g.o2, g.d2, cl);
+        const uint32_t lin = (uint32_t)(g.base + ((int64_t)lz * g.d1 + ly) * g.d0 + lx);
         key = (region_of(t, single_region) << key_bits) | lin;
     }
     if (keys64) keys64[k] = ((unsigned long long)key << 32) | hidx[k];
@@ -155,7 +187,7 @@ __global__ void k_reorder(int64_t n, const uint32_t* __restrict__ perm, const V4
                           V4<R>* __restrict__ acc1, const V4<R>* __restrict__ ext0, V4<R>* __restrict__ ext1,
                           const R* __restrict__ rho0, R* __restrict__ rho1, const R* __restrict__ p0, R* __restrict__ p1,
                           const uint8_t* __restrict__ t0, uint8_t* __restrict__ t1, const uint32_t* __restrict__ h0,
-                          uint32_t* __restrict__ h1) {
+                          uint32_t* __restrict__ h1, const uint16_t* __restrict__ sc0, uint16_t* __restrict__ sc1) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     uint32_t s = perm[k];
@@ -167,6 +199,7 @@ __global__ void k_reorder(int64_t n, const uint32_t* __restrict__ perm, const V4
     p1[k] = p0[s];
     t1[k] = t0[s];
     h1[k] = h0[s];
+    if (sc0) sc1[k] = sc0[s];
 }
 
 // Per-cell particle counts of every region: the first particle of each run of
@@ -195,8 +228,10 @@ struct WalkParams {
     bool candidates_inactive;  // contract lists inactive neighbors
     bool trunc;                // cells by truncation toward zero (hashed 2D order)
     bool length_test;          // sqrt(dot) <= r instead of dot <= r * r
-    int d0, d1, d2;
-    int64_t cells;  // d0 * d1 * d2; each region's table has cells + 1 entries
+    const SceneGrid* __restrict__ grids;  // per scene
+    const uint16_t* __restrict__ scene;   // per particle (null: one scene)
+    int64_t cells;  // cells of all scenes; each region's table has cells + 1 entries
+    __device__ __forceinline__ SceneGrid grid_of(int64_t k) const { return grids[scene ? scene[k] : 0]; }
 };
 
 // predicate of the contract; d = x_i - x_j. The 2D searches and every
@@ -216,20 +251,20 @@ template <typename R> __device__ __forceinline__ bool within(V3<R> d, const Walk
 // f(j, type_j) is called for every neighbor j.
 template <typename R, typename F>
 __device__ __forceinline__ void walk_cells(V3<R> xi, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                                           const uint32_t* __restrict__ cell_start, const int* __restrict__ origin,
+                                           const uint32_t* __restrict__ cell_start, const SceneGrid& gr,
                                            const WalkParams& w, F&& f) {
     const int ci[3] = {cell_coord<R>(xi.x, w.r, w.trunc), cell_coord<R>(xi.y, w.r, w.trunc), cell_coord<R>(xi.z, w.r, w.trunc)};
     const int zr = w.dim == 2 ? 0 : 1;
-    const int o0 = origin[0], o1 = origin[1], o2 = origin[2];
+    const int o0 = gr.o0, o1 = gr.o1, o2 = gr.o2;
     for (int dx = -1; dx <= 1; dx++) {
         for (int dy = -1; dy <= 1; dy++) {
             for (int dz = -zr; dz <= zr; dz++) {
                 const int c0 = ci[0] + dx, c1 = ci[1] + dy, c2 = ci[2] + dz;
                 bool cl = false;
-                const int l0 = local_cell(c0, o0, w.d0, cl);
-                const int l1 = local_cell(c1, o1, w.d1, cl);
-                const int l2 = local_cell(c2, o2, w.d2, cl);
-                const int64_t lc = ((int64_t)l2 * w.d1 + l1) * w.d0 + l0;
+                const int l0 = local_cell(c0, o0, gr.d0, cl);
+                const int l1 = local_cell(c1, o1, gr.d1, cl);
+                const int l2 = local_cell(c2, o2, gr.d2, cl);
+                const int64_t lc = gr.base + ((int64_t)l2 * gr.d1 + l1) * gr.d0 + l0;
                 for (int g = 0; g < w.regions; g++) {
                     const uint32_t* cs = cell_start + g * (w.cells + 1);
                     const uint32_t b = cs[lc], e = cs[lc + 1];
@@ -257,11 +292,11 @@ __device__ __forceinline__ void walk_cells(V3<R> xi, const V4<R>* __restrict__ p
 // take walk_cells instead.
 template <typename R, typename F>
 __device__ __forceinline__ bool walk_rows(V3<R> xi, const V4<R>* __restrict__ pos, const uint32_t* __restrict__ cell_start,
-                                          const int* __restrict__ origin, const WalkParams& w, F&& f) {
-    const int lx = cell_coord<R>(xi.x, w.r, false) - origin[0];
-    const int ly = cell_coord<R>(xi.y, w.r, false) - origin[1];
-    const int lz = cell_coord<R>(xi.z, w.r, false) - origin[2];
-    if (lx < 2 || ly < 2 || lz < 2 || lx > w.d0 - 3 || ly > w.d1 - 3 || lz > w.d2 - 3) return false;
+                                          const SceneGrid& gr, const WalkParams& w, F&& f) {
+    const int lx = cell_coord<R>(xi.x, w.r, false) - gr.o0;
+    const int ly = cell_coord<R>(xi.y, w.r, false) - gr.o1;
+    const int lz = cell_coord<R>(xi.z, w.r, false) - gr.o2;
+    if (lx < 2 || ly < 2 || lz < 2 || lx > gr.d0 - 3 || ly > gr.d1 - 3 || lz > gr.d2 - 3) return false;
     const float r2 = w.r2;
     const float x0 = (float)xi.x, x1 = (float)xi.y, x2 = (float)xi.z;
 #pragma unroll 1
@@ -269,7 +304,7 @@ __device__ __forceinline__ bool walk_rows(V3<R> xi, const V4<R>* __restrict__ po
         const uint32_t* cs = cell_start + g * (w.cells + 1);
 #pragma unroll 1
         for (int row = 0; row < 9; row++) {
-            const int64_t base = ((int64_t)(lz + row / 3 - 1) * w.d1 + (ly + row % 3 - 1)) * w.d0 + lx;
+            const int64_t base = gr.base + ((int64_t)(lz + row / 3 - 1) * gr.d1 + (ly + row % 3 - 1)) * gr.d0 + lx;
             const uint32_t b = cs[base - 1], e = cs[base + 2];
             for (uint32_t j = b; j < e; j++) {
                 const V4<R> pj = pos[j];
@@ -289,19 +324,20 @@ template <typename R>
 __device__ __forceinline__ uint32_t build_list_one(int64_t k, const V4<R>* __restrict__ pos,
                                                    const uint8_t* __restrict__ type,
                                                    const uint32_t* __restrict__ cell_start,
-                                                   const int* __restrict__ origin, const WalkParams& w, bool rows,
+                                                   const WalkParams& w, bool rows,
                                                    uint32_t* __restrict__ nbr, int64_t stride, int K) {
     uint32_t c = 0;
     const V3<R> xi = xyz<R>(pos[k]);
+    const SceneGrid gr = w.grid_of(k);
     bool done = false;
     if (rows) {
-        done = walk_rows<R>(xi, pos, cell_start, origin, w, [&](uint32_t j, int g, float) {
+        done = walk_rows<R>(xi, pos, cell_start, gr, w, [&](uint32_t j, int g, float) {
             if ((int)c < K) nbr[(int64_t)c * stride + k] = j | (g == 1 ? kBoundaryBit : 0u);
             c++;
         });
     }
     if (!done) {
-        walk_cells<R>(xi, pos, type, cell_start, origin, w, [&](uint32_t j, uint8_t tj) {
+        walk_cells<R>(xi, pos, type, cell_start, gr, w, [&](uint32_t j, uint8_t tj) {
             // solver lists never carry inactive particles (the solvers skip them)
             if (tj == FS_TYPE_INACTIVE) return;
             if ((int)c < K) nbr[(int64_t)c * stride + k] = j | (tj == FS_TYPE_BOUNDARY ? kBoundaryBit : 0u);
@@ -327,14 +363,14 @@ template <typename R>
 __global__ void __launch_bounds__(128) k_build_lists(int64_t n_owners, const V4<R>* __restrict__ pos,
                                                      const uint8_t* __restrict__ type,
                                                      const uint32_t* __restrict__ cell_start,
-                                                     const int* __restrict__ origin, WalkParams w, uint32_t owner_mask,
+                                                     WalkParams w, uint32_t owner_mask,
                                                      bool rows, uint32_t* __restrict__ nbr, int64_t stride, int K,
                                                      uint32_t* __restrict__ count, int* __restrict__ status,
                                                      StepScalars* __restrict__ sc) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n_owners) return;
     uint32_t c = 0;
-    if ((owner_mask >> type[k]) & 1u) c = build_list_one<R>(k, pos, type, cell_start, origin, w, rows, nbr, stride, K);
+    if ((owner_mask >> type[k]) & 1u) c = build_list_one<R>(k, pos, type, cell_start, w, rows, nbr, stride, K);
     count[k] = c;
     note_list_length(c, K, status, sc);
 }
@@ -364,25 +400,25 @@ __global__ void k_sort_lists_by_host(int64_t n_owners, uint32_t* __restrict__ nb
 // CSR export: counts (pass 1) and fill (pass 2) in sorted index space
 template <typename R>
 __global__ void k_csr_count(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                            const uint32_t* __restrict__ cell_start, const int* __restrict__ origin, WalkParams w,
+                            const uint32_t* __restrict__ cell_start, WalkParams w,
                             uint32_t owner_mask, uint32_t* __restrict__ count) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     uint32_t c = 0;
     if ((owner_mask >> type[k]) & 1u)
-        walk_cells<R>(xyz<R>(pos[k]), pos, type, cell_start, origin, w, [&](uint32_t, uint8_t) { c++; });
+        walk_cells<R>(xyz<R>(pos[k]), pos, type, cell_start, w.grid_of(k), w, [&](uint32_t, uint8_t) { c++; });
     count[k] = c;
 }
 
 template <typename R>
 __global__ void k_csr_fill(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                           const uint32_t* __restrict__ cell_start, const int* __restrict__ origin, WalkParams w,
+                           const uint32_t* __restrict__ cell_start, WalkParams w,
                            uint32_t owner_mask, const int64_t* __restrict__ offsets, uint32_t* __restrict__ out) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     if (!((owner_mask >> type[k]) & 1u)) return;
     int64_t o = offsets[k];
-    walk_cells<R>(xyz<R>(pos[k]), pos, type, cell_start, origin, w, [&](uint32_t j, uint8_t) { out[o++] = j; });
+    walk_cells<R>(xyz<R>(pos[k]), pos, type, cell_start, w.grid_of(k), w, [&](uint32_t j, uint8_t) { out[o++] = j; });
 }
 
 // neighbors of one arbitrary position (get_neighbors(vec)), sorted space.
@@ -396,7 +432,7 @@ __global__ void k_csr_fill(int64_t n, const V4<R>* __restrict__ pos, const uint8
 template <typename R>
 __global__ void k_query_position(V3<R> x, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
                                  const uint32_t* __restrict__ hidx, const uint32_t* __restrict__ cell_start,
-                                 const int* __restrict__ origin, WalkParams w, bool skip_cell_min,
+                                 WalkParams w, bool skip_cell_min,
                                  uint32_t* __restrict__ out, int64_t cap, unsigned long long* __restrict__ count) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     unsigned long long c = 0;
@@ -408,10 +444,11 @@ __global__ void k_query_position(V3<R> x, const V4<R>* __restrict__ pos, const u
             for (int dz = -zr; dz <= zr; dz++, ordinal++) {
                 const int c0 = ci[0] + dx, c1 = ci[1] + dy, c2 = ci[2] + dz;
                 bool cl = false;
-                const int l0 = local_cell(c0, origin[0], w.d0, cl);
-                const int l1 = local_cell(c1, origin[1], w.d1, cl);
-                const int l2 = local_cell(c2, origin[2], w.d2, cl);
-                const int64_t lc = ((int64_t)l2 * w.d1 + l1) * w.d0 + l0;
+                const SceneGrid& gr = w.grids[0];
+                const int l0 = local_cell(c0, gr.o0, gr.d0, cl);
+                const int l1 = local_cell(c1, gr.o1, gr.d1, cl);
+                const int l2 = local_cell(c2, gr.o2, gr.d2, cl);
+                const int64_t lc = gr.base + ((int64_t)l2 * gr.d1 + l1) * gr.d0 + l0;
                 // visits the members of true cell (c0, c1, c2)
                 auto members = [&](auto&& f) {
                     for (int g = 0; g < w.regions; g++) {

@@ -86,6 +86,8 @@ template <typename R> struct State {
     R* __restrict__ err;
     const uint8_t* __restrict__ type;
     const uint32_t* __restrict__ hidx;
+    const uint16_t* __restrict__ scene;  // per-particle scene (batched contexts), else null
+    __device__ __forceinline__ int scene_of(int64_t k) const { return scene ? scene[k] : 0; }
 };
 
 __device__ __forceinline__ float fmax_(float a, float b) { return fmaxf(a, b); }
@@ -379,9 +381,31 @@ __device__ __forceinline__ ErrPart iisph3d_pressure_update_one(int64_t k, const 
     return iisph3d_pressure_update_tail<R>(k, s, c, dt, ak, ap.get(), s.vstar[k], s.anp[k].w, s.p[k]);
 }
 
+// adds one thread's ErrPart to its scene's scalars
+__device__ __forceinline__ void add_err_part(const ErrPart& o, StepScalars* __restrict__ q) {
+    if (o.e_cnt) {
+        atomicAdd(&q->err_sum, o.e_sum);
+        atomicAdd(&q->err_count, (unsigned long long)o.e_cnt);
+    }
+    atomic_max_nonneg(&q->max_err_bits, o.e_max);
+    atomic_max_nonneg(&q->max_a2_bits, o.a2);
+    atomic_max_nonneg(&q->max_v2_bits, o.v2);
+}
+
 // block reduction of the ErrParts into StepScalars (FP64 residual sum); every
-// thread of the block calls it
-__device__ __forceinline__ void reduce_err_parts(ErrPart o, StepScalars* __restrict__ sc) {
+// thread of the block calls it. scene: the scene of the thread's particle.
+// A block whose threads all belong to one scene reduces first; a block that
+// spans scenes adds thread by thread.
+__device__ __forceinline__ void reduce_err_parts(ErrPart o, StepScalars* __restrict__ sc, int scene = 0) {
+    __shared__ int s_scene;
+    if (threadIdx.x == 0) s_scene = scene;
+    __syncthreads();
+    const int s0 = s_scene;
+    if (!__syncthreads_and(scene == s0)) {
+        add_err_part(o, sc + scene);
+        return;
+    }
+    sc += s0;
     double e_sum = warp_sum(o.e_sum);
     unsigned int e_cnt = warp_sum(o.e_cnt);
     float e_max = warp_max(o.e_max), a2 = warp_max(o.a2), v2 = warp_max(o.v2);
@@ -437,15 +461,10 @@ __global__ void k_iisph3d_pressure_update(int64_t n, State<R> s, Lists L, Solver
 // `handle`. The loop is bounded independently of the state: loop_guard counts
 // executions of the body and stops it after max_it, whatever the status word
 // or the residual say.
-__global__ void k_iisph_check(StepScalars* __restrict__ sc, int min_it, int max_it, float max_err, bool fp64_test,
-                              bool two_d, const int* __restrict__ status, cudaGraphConditionalHandle handle,
-                              bool set_condition) {
-    const int guard = ++sc->loop_guard;
-    bool stop = guard >= max_it;
-    if (*status || sc->done) {
-        if (set_condition) cudaGraphSetConditional(handle, 0u);
-        return;
-    }
+// One scene's test after an iteration; returns whether its loop is done and
+// resets the iteration's accumulators.
+__device__ __forceinline__ bool check_scene(StepScalars* __restrict__ sc, int min_it, int max_it, float max_err,
+                                            bool fp64_test, bool two_d) {
     const int it = sc->iteration;  // iterations completed before this one
     const unsigned long long cnt = sc->err_count;
     const double sum = sc->err_sum;
@@ -481,8 +500,42 @@ __global__ void k_iisph_check(StepScalars* __restrict__ sc, int min_it, int max_
     sc->max_err_bits = 0u;
     sc->max_a2_bits = 0u;
     sc->max_v2_bits = 0u;
-    stop = stop || done;
+    return done;
+}
+
+__global__ void k_iisph_check(StepScalars* __restrict__ sc, int min_it, int max_it, float max_err, bool fp64_test,
+                              bool two_d, const int* __restrict__ status, cudaGraphConditionalHandle handle,
+                              bool set_condition) {
+    const int guard = ++sc->loop_guard;
+    bool stop = guard >= max_it;
+    if (*status || sc->done) {
+        if (set_condition) cudaGraphSetConditional(handle, 0u);
+        return;
+    }
+    stop = check_scene(sc, min_it, max_it, max_err, fp64_test, two_d) || stop;
     if (set_condition) cudaGraphSetConditional(handle, stop ? 0u : 1u);
+}
+
+// Batched contexts: every scene still iterating is tested on its own (the
+// 3D test, FP64 average); the loop goes on while any scene iterates. One
+// block; the guard in scene 0 counts executions of the loop body.
+__global__ void k_iisph_check_scenes(StepScalars* __restrict__ sc, int scenes, int min_it, int max_it, float max_err,
+                                     const int* __restrict__ status, cudaGraphConditionalHandle handle,
+                                     bool set_condition) {
+    __shared__ int s_guard;
+    if (threadIdx.x == 0) s_guard = ++sc[0].loop_guard;
+    __syncthreads();
+    const bool stop_all = s_guard >= max_it || *status != 0;
+    int active = 0;
+    for (int i = threadIdx.x; i < scenes; i += blockDim.x) {
+        StepScalars* q = sc + i;
+        if (q->done) continue;
+        const bool done = check_scene(q, min_it, max_it, max_err, true, false) || stop_all;
+        q->done = done ? 1 : 0;
+        if (!done) active = 1;
+    }
+    const int any = __syncthreads_or(active);
+    if (threadIdx.x == 0 && set_condition) cudaGraphSetConditional(handle, any ? 1u : 0u);
 }
 
 // CFL clamp (IISPHFluidSolver3D.hpp:525-535, SESPHFluidSolver3D.hpp:109-116) with
@@ -490,9 +543,8 @@ __global__ void k_iisph_check(StepScalars* __restrict__ sc, int min_it, int max_
 // (ConstantTimestepGenerator.cpp:17-41). The reference evaluates
 // sqrt(size / a) * lambda_a in double (its unqualified sqrt is the C double
 // function) and rounds the product to float; the rest is float.
-__global__ void k_cfl(StepScalars* __restrict__ sc, float particle_size, float timestep, float lambda_v, float lambda_a,
-                      const int* __restrict__ status) {
-    if (*status) return;
+__device__ __forceinline__ void cfl_one(StepScalars* __restrict__ sc, float particle_size, float timestep,
+                                        float lambda_v, float lambda_a) {
     const float max_v = sqrtf(sc->final_max_v2);
     const float max_a = sqrtf(sc->final_max_a2);
     float dta = timestep, dtv = timestep;
@@ -501,6 +553,14 @@ __global__ void k_cfl(StepScalars* __restrict__ sc, float particle_size, float t
     float nt = fmaxf(fminf(dta, dtv), 0.000001f);
     nt = fminf(nt, sc->desired_dt);
     sc->dt = nt;
+}
+
+// the clamp for scenes [0, scenes) (one in a single-scene context)
+__global__ void k_cfl(StepScalars* __restrict__ sc, int scenes, float particle_size, float timestep, float lambda_v,
+                      float lambda_a, const int* __restrict__ status) {
+    if (*status) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < scenes; i += gridDim.x * blockDim.x)
+        cfl_one(sc + i, particle_size, timestep, lambda_v, lambda_a);
 }
 
 // ===========================================================================
@@ -514,9 +574,10 @@ __global__ void k_iisph3d_integrate(int64_t n, State<R> s, const StepScalars* __
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n || *status) return;
     if (s.type[k] == FS_TYPE_INACTIVE) return;
-    const R dt = (R)sc->dt, old = (R)sc->desired_dt;
+    const StepScalars* q = sc + s.scene_of(k);
+    const R dt = (R)q->dt, old = (R)q->desired_dt;
     V3<R> vs = xyz<R>(s.vstar[k]);
-    if (sc->dt != sc->desired_dt) {
+    if (q->dt != q->desired_dt) {
         const V3<R> a = xyz<R>(s.anp[k]);
         vs = (vs - old * a) + dt * a;
     }

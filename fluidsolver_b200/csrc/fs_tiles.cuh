@@ -72,17 +72,20 @@ inline size_t tile_pass_smem(int bytes_per_candidate, int K) {
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     int64_t n_owners, const float4* __restrict__ pos, const uint8_t* __restrict__ type,
-    const uint32_t* __restrict__ cell_start, const int* __restrict__ origin, WalkParams w, TileDesc* __restrict__ desc,
+    const uint32_t* __restrict__ cell_start, WalkParams w, TileDesc* __restrict__ desc,
     uint4* __restrict__ ent, int64_t ent_stride, uint32_t* __restrict__ nbr, int64_t stride, int K,
     uint32_t* __restrict__ count, int* __restrict__ status, StepScalars* __restrict__ sc) {
     extern __shared__ float4 tile_smem[];
     float4* sp = tile_smem;                                              // staged positions
     uint16_t* sent = reinterpret_cast<uint16_t*>(tile_smem + kTileCap);  // [owner][K + 8] entries
     const int KP = K + 8;
-    __shared__ int s_key[kTileOwners];
+    __shared__ long long s_key[kTileOwners];
     __shared__ uint32_t s_cnt[kTileOwners];
     __shared__ int s_lead[kTileOwners / 32];
-    __shared__ int s_gy[kTileGroups], s_gz[kTileGroups], s_gx0[kTileGroups], s_gx1[kTileGroups];
+    // per group: the first cell of its own row, the row and plane strides of
+    // its scene's grid, and its first and last x
+    __shared__ long long s_grow[kTileGroups];
+    __shared__ int s_gd0[kTileGroups], s_gd01[kTileGroups], s_gx0[kTileGroups], s_gx1[kTileGroups];
     __shared__ uint32_t s_start[kTileRanges], s_len[kTileRanges], s_base[kTileRanges];
     __shared__ uint32_t s_total;
 
@@ -91,19 +94,24 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     const int64_t k = tile * kTileOwners + t;
     const bool valid = k < n_owners;
     float4 pk = make_float4(0.f, 0.f, 0.f, 0.f);
-    int lx = 0, ly = 0, lz = 0, key = -1;
+    int lx = 0;
+    long long key = -1;   // first cell of the owner's own row (unique across scenes)
+    int d0 = 0, d01 = 0;
     bool border = false;
     if (valid) {
         pk = pos[k];
-        lx = cell_coord<float>(pk.x, w.r, false) - origin[0];
-        ly = cell_coord<float>(pk.y, w.r, false) - origin[1];
-        lz = cell_coord<float>(pk.z, w.r, false) - origin[2];
-        border = lx < 2 || ly < 2 || lz < 2 || lx > w.d0 - 3 || ly > w.d1 - 3 || lz > w.d2 - 3;
-        key = border ? -2 : lz * w.d1 + ly;
+        const SceneGrid gr = w.grid_of(k);
+        lx = cell_coord<float>(pk.x, w.r, false) - gr.o0;
+        const int ly = cell_coord<float>(pk.y, w.r, false) - gr.o1;
+        const int lz = cell_coord<float>(pk.z, w.r, false) - gr.o2;
+        border = lx < 2 || ly < 2 || lz < 2 || lx > gr.d0 - 3 || ly > gr.d1 - 3 || lz > gr.d2 - 3;
+        d0 = gr.d0;
+        d01 = gr.d0 * gr.d1;
+        key = border ? -2 : gr.base + ((long long)lz * gr.d1 + ly) * gr.d0;
     }
     s_key[t] = key;
     const int any_border = __syncthreads_or(valid && border);
-    // groups: runs of equal (y, z) row keys (keys are non-decreasing in k)
+    // groups: runs of equal row keys (non-decreasing in k: sorted order)
     const bool lead = valid && (t == 0 || s_key[t - 1] != key);
     const unsigned bal = __ballot_sync(0xffffffffu, lead);
     if (lane == 0) s_lead[t >> 5] = __popc(bal);
@@ -119,8 +127,9 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     int NR = 0;
     if (!fallback) {
         if (lead) {
-            s_gy[g] = ly;
-            s_gz[g] = lz;
+            s_grow[g] = key;
+            s_gd0[g] = d0;
+            s_gd01[g] = d01;
             s_gx0[g] = lx;
         }
         if (valid && (t == kTileOwners - 1 || s_key[t + 1] != key)) s_gx1[g] = lx;
@@ -128,7 +137,7 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
         NR = 18 * G;
         if (t < NR) {
             const int region = t / (9 * G), gg = (t % (9 * G)) / 9, r = t % 9;
-            const int64_t rb = ((int64_t)(s_gz[gg] + r / 3 - 1) * w.d1 + (s_gy[gg] + r % 3 - 1)) * w.d0;
+            const int64_t rb = s_grow[gg] + (int64_t)(r / 3 - 1) * s_gd01[gg] + (int64_t)(r % 3 - 1) * s_gd0[gg];
             const uint32_t* cs = cell_start + region * (w.cells + 1);
             const uint32_t a = cs[rb + s_gx0[gg] - 1], b = cs[rb + s_gx1[gg] + 2];
             s_start[t] = a;
@@ -152,7 +161,7 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
         if (t == 0) desc[tile].nranges = kTileFallback;
         uint32_t c = 0;
         if (valid) {
-            c = build_list_one<float>(k, pos, type, cell_start, origin, w, true, nbr, stride, K);
+            c = build_list_one<float>(k, pos, type, cell_start, w, true, nbr, stride, K);
             count[k] = c;
         }
         note_list_length(c, K, status, sc);
@@ -175,7 +184,7 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
 #pragma unroll
         for (int q = 0; q < 18; q++) {
             const uint32_t* cs = cell_start + (q / 9) * (w.cells + 1);
-            const int64_t rb = ((int64_t)(lz + (q % 9) / 3 - 1) * w.d1 + (ly + q % 3 - 1)) * w.d0;
+            const int64_t rb = key + (int64_t)((q % 9) / 3 - 1) * d01 + (int64_t)(q % 3 - 1) * d0;
             lo[q] = cs[rb + lx - 1];
             hi[q] = cs[rb + lx + 2];
         }
@@ -434,10 +443,9 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l1(int64_t n_f
                                                                   int* __restrict__ status) {
     extern __shared__ float4 tile_smem[];
     if (*status) return;
-    const float dt = sc->dt;
     if (blockIdx.x >= n_tiles) {
         const int64_t k = n_fluid + (blockIdx.x - n_tiles) * (int64_t)kPassThreads + threadIdx.x;
-        if (k < n) iisph3d_l1_one<float, true, false>(k, s, L, c, dt);
+        if (k < n) iisph3d_l1_one<float, true, false>(k, s, L, c, sc[s.scene_of(k)].dt);
         return;
     }
     const int half = threadIdx.x & 1;
@@ -445,7 +453,7 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l1(int64_t n_f
     const TileDesc* d = T.desc + blockIdx.x;
     const uint32_t nr = d->nranges;
     if (nr == kTileFallback) {
-        if (k < n_fluid && !half) iisph3d_l1_one<float, true, false>(k, s, L, c, dt);
+        if (k < n_fluid && !half) iisph3d_l1_one<float, true, false>(k, s, L, c, sc[s.scene_of(k)].dt);
         return;
     }
     float4* sp = tile_smem;
@@ -460,6 +468,7 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l1(int64_t n_f
     const bool valid = k < n_fluid;
     const int64_t kk = valid ? k : 0;
     const float4 pk = s.pos[kk], vk = s.vel[kk], ek = s.ext[kk];
+    const float dt = sc[s.scene_of(kk)].dt;
     if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     Acc3<float, true> visc;
@@ -504,13 +513,12 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l2(int64_t n_f
                                                                   int* __restrict__ status) {
     extern __shared__ float4 tile_smem[];
     if (*status) return;
-    const float dt = sc->dt;
     const int half = threadIdx.x & 1;
     const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
     const TileDesc* d = T.desc + blockIdx.x;
     const uint32_t nr = d->nranges;
     if (nr == kTileFallback) {
-        if (k < n_fluid && !half) iisph3d_l2_one<float, true, false>(k, s, L, c, dt);
+        if (k < n_fluid && !half) iisph3d_l2_one<float, true, false>(k, s, L, c, sc[s.scene_of(k)].dt);
         return;
     }
     float4* sp = tile_smem;
@@ -524,6 +532,7 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l2(int64_t n_f
     const int64_t kk = valid ? k : 0;
     const float4 pk = s.pos[kk], vsk = s.vstar[kk];
     const float rk = s.rho[kk];
+    const float dt = sc[s.scene_of(kk)].dt;
     if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     Acc<float, true> contrib, mg2;
@@ -566,13 +575,17 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_tile_iisph3d_pressure_acc(i
                                                                             const StepScalars* __restrict__ sc,
                                                                             int* __restrict__ status) {
     extern __shared__ float4 tile_smem[];
-    if (*status || sc->done) return;
+    if (*status) return;
     const int half = threadIdx.x & 1;
     const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
+    // owners of scenes whose loop has ended take no part; a tile without
+    // iterating owners ends at once
+    const bool live = k < n_fluid && !sc[s.scene_of(k)].done;
+    if (!__syncthreads_or(live)) return;
     const TileDesc* d = T.desc + blockIdx.x;
     const uint32_t nr = d->nranges;
     if (nr == kTileFallback) {
-        if (k < n_fluid && !half) iisph3d_pressure_acc_one<float, true>(k, s, L, c);
+        if (live && !half) iisph3d_pressure_acc_one<float, true>(k, s, L, c);
         return;
     }
     float4* sp = tile_smem;
@@ -582,7 +595,7 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_tile_iisph3d_pressure_acc(i
     float4* dst4[1] = {sp};
     const TileSlab slab = slab_at(tile_smem, 20, T.K);
     stage_tile_async<1, float>(stg, d, nr, src4, dst4, s.p, sa, T, slab);
-    const bool valid = k < n_fluid;
+    const bool valid = live;
     const int64_t kk = valid ? k : 0;
     const float4 pk = s.pos[kk];
     const float prk = s.p[kk];
@@ -612,15 +625,20 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_pressure_updat
                                                                                StepScalars* __restrict__ sc,
                                                                                int* __restrict__ status) {
     extern __shared__ float4 tile_smem[];
-    if (*status || sc->done) return;
-    const float dt = sc->dt;
+    if (*status) return;
     const int half = threadIdx.x & 1;
     const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
+    const int64_t kk = k < n_fluid ? k : 0;
+    const int scene = s.scene_of(kk);
+    const StepScalars* q = sc + scene;
+    const bool live = k < n_fluid && !q->done;
+    if (!__syncthreads_or(live)) return;
+    const float dt = q->dt;
     const TileDesc* d = T.desc + blockIdx.x;
     const uint32_t nr = d->nranges;
     ErrPart o;
     if (nr == kTileFallback) {
-        if (k < n_fluid && !half) o = iisph3d_pressure_update_one<float, true>(k, s, L, c, dt);
+        if (live && !half) o = iisph3d_pressure_update_one<float, true>(k, s, L, c, dt);
     } else {
         float4* sp = tile_smem;
         float4* sa = tile_smem + kTileCap;
@@ -630,8 +648,7 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_pressure_updat
         const TileSlab slab = slab_at(tile_smem, 32, T.K);
         stage_tile_async<2, float>(stg, d, nr, src4, dst4, (const float*)nullptr, (float*)nullptr, T, slab);
         // the owner's own data, loaded while the staging lands
-        const bool valid = k < n_fluid;
-        const int64_t kk = valid ? k : 0;
+        const bool valid = live;
         const float4 pk = s.pos[kk], ak = s.acc[kk], vsk = s.vstar[kk];
         const float aii = s.anp[kk].w, prk = s.p[kk];
         if (stage_tile_wait(stg, status)) {
@@ -652,7 +669,7 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_pressure_updat
                 o = iisph3d_pressure_update_tail<float>(k, s, c, dt, v3<float>(ak.x, ak.y, ak.z), sum, vsk, aii, prk);
         }
     }
-    reduce_err_parts(o, sc);
+    reduce_err_parts(o, sc, scene);
 }
 
 inline cudaError_t set_tile_pass_smem(int K) {

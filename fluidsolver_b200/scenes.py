@@ -105,6 +105,26 @@ def dam_1m(seed=5) -> Scene:
     return breaking_dam_3d(100, 100, 100, 1.0, tank=(320, 220, 150), seed=seed)
 
 
+def batched_dams(count=256, seed=6, f_min=2000, f_max=60000) -> list:
+    """The batched breaking dams: `count` scenes with fluid counts drawn
+    log-uniform in [f_min, f_max] and a block aspect ratio a ~ U(0.5, 2):
+    nx = round((F a)^(1/3)), ny = round(F^(1/3)), nz = max(1, round(F / (nx ny)))
+    (the actual count is nx ny nz). Each block sits in its own single-layer
+    tank with the 1M dam's proportions (3.2 nx x 2.2 ny x 1.5 nz spacings).
+    Scene i's jitter seed is seed * 100003 + i."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        f = int(round(np.exp(rng.uniform(np.log(f_min), np.log(f_max)))))
+        a = rng.uniform(0.5, 2.0)
+        nx = max(1, int(round((f * a) ** (1.0 / 3.0))))
+        ny = max(1, int(round(f ** (1.0 / 3.0))))
+        nz = max(1, int(round(f / (nx * ny))))
+        tank = (max(nx + 2, int(round(3.2 * nx))), max(ny + 2, int(round(2.2 * ny))), max(nz + 2, int(round(1.5 * nz))))
+        out.append(breaking_dam_3d(nx, ny, nz, 1.0, tank=tank, seed=seed * 100003 + i))
+    return out
+
+
 def breaking_dam_2d(nx=50, ny=50, spacing=1.0, width=150, height=120, layers=3, jitter=0.01, seed=1,
                     rest_density=1.0) -> Scene:
     """2D dam: nx x ny fluid block from (0,0) with uniform jitter, in a box

@@ -371,6 +371,83 @@ class IISPHFluidSolver3D(FluidSolverBase):
         p.single_layer_gamma_1 = s.single_layer_boundary_gamma_1
 
 
+class BatchedIISPHFluidSolver3D:
+    """Many independent 3D IISPH scenes advanced together (fs_batch_create,
+    fs_batch_run). One launch per sub-phase covers every scene. Each scene
+    keeps its own pressure-loop convergence test and its own CFL-clamped time
+    step, and particles of different scenes never interact. The physics of
+    each scene is IISPHFluidSolver3D's (same parameter and settings objects);
+    the reference has no batched form, it runs one solver object per scene.
+
+    scenes: one ParticleCollection per scene (host order within each)."""
+
+    def __init__(self, scenes: list, device: int = 0, neighbor_capacity: int = 0):
+        self._template = IISPHFluidSolver3D(search="hashed-3d", precision="fp32-kahan", device=device,
+                                            neighbor_capacity=neighbor_capacity)
+        self.parameters = self._template.parameters
+        self.settings = self._template.settings
+        self.timestep_generator = self._template.timestep_generator
+        self.scenes = [c.normalized() for c in scenes]
+        self.offsets = np.concatenate([[0], np.cumsum([len(c) for c in self.scenes])]).astype(np.int64)
+        self._ctx = None
+        self.last_stats = None
+
+    def initialize(self) -> None:
+        if self._ctx is not None:
+            return
+        n = int(self.offsets[-1])
+        p = self._template._params(n)
+        ctx = ctypes.c_void_p()
+        F.check(F.lib().fs_batch_create(ctypes.byref(p), len(self.scenes), self.offsets.ctypes.data, ctypes.byref(ctx)))
+        self._ctx = ctx
+        cat = lambda name: None if getattr(self.scenes[0], name) is None else \
+            np.ascontiguousarray(np.concatenate([getattr(c, name) for c in self.scenes]))
+        self._uploaded = ParticleCollection(**{name: cat(name) for name in (
+            "position", "velocity", "acceleration", "external", "mass", "density", "pressure", "type", "tag")})
+        F.check(F.lib().fs_upload(self._ctx, ctypes.byref(self._uploaded.as_fs())))
+
+    @property
+    def ctx(self):
+        self.initialize()
+        return self._ctx
+
+    def run(self, steps: int, desired_dt: float | None = None):
+        """`steps` steps of every scene; returns one FsStepStats per scene
+        (the last step's)."""
+        self.initialize()
+        dt = self.timestep_generator.settings.timestep if desired_dt is None else desired_dt
+        stats = (F.FsStepStats * len(self.scenes))()
+        F.check(F.lib().fs_batch_run(self._ctx, int(steps), float(dt), ctypes.cast(stats, ctypes.c_void_p)))
+        self.last_stats = list(stats)
+        return self.last_stats
+
+    def collections(self) -> list:
+        """Downloads every scene's state (host order within each scene)."""
+        self.initialize()
+        n, d = int(self.offsets[-1]), 3
+        out = ParticleCollection(
+            position=np.zeros((n, d), np.float32), velocity=np.zeros((n, d), np.float32),
+            acceleration=np.zeros((n, d), np.float32), external=np.zeros((n, d), np.float32),
+            mass=np.zeros(n, np.float32), density=np.zeros(n, np.float32), pressure=np.zeros(n, np.float32),
+            type=np.zeros(n, np.uint8), tag=np.zeros(n, np.uint32))
+        F.check(F.lib().fs_download(self._ctx, ctypes.byref(out.as_fs())))
+        res = []
+        for a, b in zip(self.offsets[:-1], self.offsets[1:]):
+            res.append(ParticleCollection(**{k: (None if v is None else v[a:b]) for k, v in out.__dict__.items()}))
+        return res
+
+    def close(self) -> None:
+        if self._ctx:
+            F.lib().fs_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class IISPHFluidSolver(FluidSolverBase):
     """IISPHFluidSolver, 2D (fluidSolver/solver/IISPHFluidSolver.hpp:21-548)."""
     DIM = 2

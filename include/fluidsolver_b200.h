@@ -247,11 +247,21 @@ void* fs_stream(fs_ctx* ctx);
 int64_t fs_launch_count(fs_ctx* ctx);
 
 /* ---- batched scenes -------------------------------------------------------
- * Many independent scenes of uneven size advance together: one launch per
- * sub-phase covers every scene, each scene keeps its own convergence test and
- * time step. Scene s owns host particles [offsets[s], offsets[s+1]). */
+ * Many independent scenes of uneven size advance together. This has no
+ * counterpart in the reference, which runs one solver object per scene (one
+ * IISPHFluidSolver3D per scenario). One launch per sub-phase covers every
+ * scene. Each scene keeps its own cell grid (particles of different scenes
+ * never interact), its own IISPH convergence test and its own CFL-clamped
+ * time step. Scene s owns host particles [offsets[s], offsets[s+1]) of the
+ * collection passed to fs_upload, which must hold exactly offsets[scenes]
+ * particles. Batched contexts run the 3D IISPH solver with the hashed-3d
+ * contract in FP32 + Kahan device order (FS_ERR_INVALID otherwise), up to
+ * 65,535 scenes; fs_query_position is not available on them (a position names
+ * no scene). fs_download, fs_get_neighbors_csr, fs_step and fs_run work as for
+ * one scene (fs_step/fs_run report scene 0's statistics). */
 fs_status fs_batch_create(const fs_params* p, int32_t scenes, const int64_t* offsets, fs_ctx** out);
-/* stats has one entry per scene. */
+/* `steps` steps of every scene (CUDA graphs, no host sync in between); stats
+ * has one entry per scene and receives each scene's last-step statistics. */
 fs_status fs_batch_run(fs_ctx* ctx, int32_t steps, float desired_dt, fs_step_stats* stats);
 
 #ifdef __cplusplus
