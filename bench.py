@@ -183,6 +183,24 @@ def cpu_baseline_from_state(state, n_fluid, seconds_budget=25.0):
                       f"iterations {iters}, {el:.1f} s"}
 
 
+def shard(items, rank: int, world: int) -> list:
+    """Rank `rank` of `world` takes items i with i mod world == rank."""
+    return [x for i, x in enumerate(items) if i % world == rank]
+
+
+def max_reducer(world: int, device):
+    """max over ranks of a float (torch.distributed, tensors on `device`)."""
+    def reduce(x: float) -> float:
+        if world == 1:
+            return x
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+    return reduce
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -201,12 +219,7 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = max_reducer(world, "cuda")
 
     scene = scenes.dam_1m(seed=5 + rank)
     n_active = scene.n_fluid + scene.n_boundary
@@ -306,7 +319,7 @@ def run_batched(args, device, rank, world, max_over_ranks, barrier):
     from fluidsolver_b200 import scenes
     L = F.lib()
     allsc = scenes.batched_dams(256, seed=6)
-    mine = [s for i, s in enumerate(allsc) if i % world == rank]
+    mine = shard(allsc, rank, world)
     batch = BatchedIISPHFluidSolver3D([s.collection for s in mine], device=device)
     configure_iisph(batch)
     batch.run(args.warmup)
