@@ -95,6 +95,7 @@ template <typename R> State<R> state_of(fs_ctx* c) {
     s.vstar = (V4<R>*)c->vstar;
     s.anp = (V4<R>*)c->anp;
     s.err = (R*)c->err;
+    s.gbnd = (V4<R>*)c->gbnd;
     s.type = c->type[c->cur];
     s.hidx = c->hidx[c->cur];
     s.scene = c->scene_of[c->cur];
@@ -238,7 +239,7 @@ void clear_graphs(fs_ctx* c) {
 fs_status free_all(fs_ctx* c) {
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc[0], c->acc[1], c->ext[0], c->ext[1],
                     c->rho[0], c->rho[1], c->p[0], c->p[1], c->type[0], c->type[1], c->hidx[0], c->hidx[1],
-                    c->rho_prev, c->vstar, c->anp, c->err, c->tile_desc, c->tile_ent, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
+                    c->rho_prev, c->vstar, c->anp, c->err, c->gbnd, c->tile_desc, c->tile_ent, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
                     c->perm[0], c->perm[1], c->cub_temp, c->cell_start, c->cell_counts, c->bbox, c->grids, c->nbr, c->nbr_count,
                     c->scene_of[0], c->scene_of[1], c->d_scene_offsets,
                     c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->scalars};
@@ -1255,6 +1256,7 @@ static fs_status create_ctx(const fs_params* p, int32_t scenes, const int64_t* o
     FS_ALLOC(*(char**)&c->vstar, cap * v4);
     FS_ALLOC(*(char**)&c->anp, cap * v4);
     FS_ALLOC(*(char**)&c->err, cap * r1);
+    FS_ALLOC(*(char**)&c->gbnd, cap * v4);
     const int S = c->nsc();
     FS_ALLOC(c->bbox, 6 * S);
     FS_ALLOC(c->grids, S);

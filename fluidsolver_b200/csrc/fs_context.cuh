@@ -67,6 +67,7 @@ struct fs_ctx {
     void* vstar = nullptr;
     void* anp = nullptr;
     void* err = nullptr;
+    void* gbnd = nullptr;     // V4: sum over boundary neighbors of m_j gradW (tile passes)
 
     // search
     uint32_t* keys[2] = {};

@@ -84,6 +84,7 @@ template <typename R> struct State {
     V4<R>* __restrict__ vstar; // w: source term
     V4<R>* __restrict__ anp;   // w: diagonal element
     R* __restrict__ err;
+    V4<R>* __restrict__ gbnd;  // sum over boundary neighbors of m_j gradW, from the second loop (tile passes)
     const uint8_t* __restrict__ type;
     const uint32_t* __restrict__ hidx;
     const uint16_t* __restrict__ scene;  // per-particle scene (batched contexts), else null

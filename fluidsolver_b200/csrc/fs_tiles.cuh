@@ -45,15 +45,18 @@ constexpr uint32_t kEntBoundary = 0x1u;
 struct TileDesc {
     uint32_t nranges;                  // non-empty candidate ranges, or kTileFallback
     uint32_t staged;                   // candidates staged in total
+    uint32_t staged_fluid;             // of them in fluid ranges
     uint32_t octets;                   // octets of entries of the tile's longest list
     uint32_t start[kTileRanges];       // first sorted index of each range
-    uint32_t len_base[kTileRanges];    // length | (first staged slot << 16)
+    uint32_t len_base[kTileRanges];    // length | kRangeBoundary for boundary ranges | (first staged slot << 16)
 };
+constexpr uint32_t kRangeBoundary = 0x8000u;
+constexpr uint32_t kRangeLen = 0x7fffu;
 
 struct TileLists {
     const TileDesc* __restrict__ desc;
     const uint4* __restrict__ ent;     // [K / 8][stride]: 8 entries of 16 bits per owner and octet
-    const uint32_t* __restrict__ count;
+    const uint32_t* __restrict__ count;  // per owner: entries | (fluid entries << 16); fluid entries come first
     int64_t stride;
     int K;
 };
@@ -195,8 +198,10 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
                 c++;
             }
         };
+        uint32_t cf = 0;
 #pragma unroll
         for (int q = 0; q < 18; q++) {
+            if (q == 9) cf = c;
             const int qq = ((q / 9) * G + g) * 9 + q % 9;
             const uint32_t off = s_base[qq] - s_start[qq];
             const uint32_t flag = q >= 9 ? kEntBoundary : 0u;
@@ -209,7 +214,7 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
             }
             if (i < e) test(sp[i], (i << 4) | flag);
         }
-        count[k] = c;
+        count[k] = min(c, 0xffffu) | (min(cf, 0xffffu) << 16);
     }
     s_cnt[t] = c;
     note_list_length(c, K, status, sc);
@@ -218,15 +223,18 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
         uint32_t mx = 0;
         for (int i = 0; i < kTileOwners; i++) mx = max(mx, s_cnt[i]);
         desc[tile].octets = (min(mx, (uint32_t)K) + 7) / 8;
-        uint32_t m = 0;
+        uint32_t m = 0, fl = 0;
         for (int q = 0; q < NR; q++) {
             if (!s_len[q]) continue;
+            const bool bnd = q >= 9 * G;
             desc[tile].start[m] = s_start[q];
-            desc[tile].len_base[m] = s_len[q] | (s_base[q] << 16);
+            desc[tile].len_base[m] = s_len[q] | (bnd ? kRangeBoundary : 0u) | (s_base[q] << 16);
+            if (!bnd) fl += s_len[q];
             m++;
         }
         desc[tile].nranges = m;
         desc[tile].staged = s_total;
+        desc[tile].staged_fluid = fl;
     }
     // octets of entries, coalesced across the tile's owners
     const int O = K / 8;
@@ -259,7 +267,7 @@ struct TileSlab {
     uint32_t* count;
 };
 
-template <int NV4, typename Scalar>
+template <int NV4, typename Scalar, bool FLUID_ONLY = false>
 __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* __restrict__ d, uint32_t nr,
                                                  const float4* const (&src4)[NV4], float4* const (&dst4)[NV4],
                                                  const Scalar* __restrict__ src1, Scalar* dst1, const TileLists& T,
@@ -273,8 +281,8 @@ __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* 
     }
     __syncthreads();
     if (t == 0) {
-        const uint32_t bytes = d->staged * 16u * (uint32_t)NV4 + octets * (uint32_t)kTileOwners * 16u +
-                               (uint32_t)kTileOwners * 4u;
+        const uint32_t bytes = (FLUID_ONLY ? d->staged_fluid : d->staged) * 16u * (uint32_t)NV4 +
+                               octets * (uint32_t)kTileOwners * 16u + (uint32_t)kTileOwners * 4u;
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&st.bar)), "r"(bytes)
                      : "memory");
     }
@@ -294,9 +302,9 @@ __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* 
             "l"(T.ent + (int64_t)(tb - 1) * T.stride + first), "r"((uint32_t)kTileOwners * 16u),
             "r"(smem_u32(&st.bar))
             : "memory");
-    if ((uint32_t)t < nr) {
+    if ((uint32_t)t < nr && !(FLUID_ONLY && (d->len_base[t] & kRangeBoundary))) {
         const uint32_t a = d->start[t], lb = d->len_base[t];
-        const uint32_t len = lb & 0xffffu, base = lb >> 16;
+        const uint32_t len = lb & kRangeLen, base = lb >> 16;
 #pragma unroll
         for (int v = 0; v < NV4; v++) {
             asm volatile(
@@ -309,7 +317,8 @@ __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* 
     if (src1 != nullptr) {
         for (uint32_t q = t >> 5; q < nr; q += blockDim.x / 32) {
             const uint32_t a = d->start[q], lb = d->len_base[q];
-            const uint32_t len = lb & 0xffffu, base = lb >> 16;
+            if (FLUID_ONLY && (lb & kRangeBoundary)) continue;
+            const uint32_t len = lb & kRangeLen, base = lb >> 16;
             for (uint32_t i = lane; i < len; i += 32)
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst1 + base + i)),
                              "l"(src1 + a + i)
@@ -349,9 +358,11 @@ __device__ __forceinline__ bool stage_tile_wait(TileStage& st, int* __restrict__
 // of every octet), staged in shared memory: f(byte offset into a staged
 // float4 array, boundary) for each, then flush() after every octet (where the
 // passes fold their partial sums into the compensated accumulators).
-template <typename F, typename Flush>
+template <bool FLUID_ONLY = false, typename F, typename Flush>
 __device__ __forceinline__ void for_tile_entries(const TileSlab& slab, int K, int ol, int half, F&& f, Flush&& flush) {
-    const uint32_t n = min(slab.count[ol], (uint32_t)K);
+    const uint32_t cnt = slab.count[ol];
+    const uint32_t all = min(cnt & 0xffffu, (uint32_t)K);
+    const uint32_t n = FLUID_ONLY ? min(cnt >> 16, all) : all;
     for (uint32_t o = 0; o * 8 < n; o++) {
         const uint4 cur = slab.ent[o * kTileOwners + ol];
         const uint32_t w0 = half ? cur.z : cur.x, w1 = half ? cur.w : cur.y;
@@ -536,9 +547,9 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l2(int64_t n_f
     if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     Acc<float, true> contrib, mg2;
-    Acc3<float, true> inner, mg;
+    Acc3<float, true> inner, mg, gb;
     float cpart = 0.f, g2part = 0.f;
-    V3<float> ipart = v3<float>(0.f, 0.f, 0.f), mpart = v3<float>(0.f, 0.f, 0.f);
+    V3<float> ipart = v3<float>(0.f, 0.f, 0.f), mpart = v3<float>(0.f, 0.f, 0.f), bpart = v3<float>(0.f, 0.f, 0.f);
     const float wb = c.single_layer ? c.two_gamma : 2.f;
     if (valid) for_tile_entries(slab, T.K, (int)(threadIdx.x >> 1), half, [&](uint32_t off, bool bnd) {
         const float4 pj = at_offset(sp, off), vsj = at_offset(sa, off);
@@ -550,18 +561,21 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l2(int64_t n_f
         cpart = __fmaf_rn(mf, dot3(dv, xij), cpart);
         ipart = fma3(bnd ? -wb * mf : -mf, xij, ipart);
         if (!bnd) g2part = __fmaf_rn(mf * f, r2, g2part);
+        else bpart = fma3(mf, xij, bpart);
         mpart = fma3(mf, xij, mpart);
     }, [&] {
         contrib.add(cpart);
         mg2.add(g2part);
         inner.add(ipart);
         mg.add(mpart);
+        gb.add(bpart);
         cpart = g2part = 0.f;
-        ipart = mpart = v3<float>(0.f, 0.f, 0.f);
+        ipart = mpart = bpart = v3<float>(0.f, 0.f, 0.f);
     });
     const float ct = pair_total(contrib), g2 = pair_total(mg2);
-    const V3<float> in = pair_total(inner), m = pair_total(mg);
+    const V3<float> in = pair_total(inner), m = pair_total(mg), gbt = pair_total(gb);
     if (half || !valid) return;
+    s.gbnd[k] = v4<float>(gbt, 0.f);   // sum_bnd m_j gradW, for the pressure iterations
     const float source = (c.rest_density - rk) - dt * ct;
     const float diag = (c.inv_rho0_sq * dot(in, m) - (pk.w / c.rho0_sq) * g2) * (dt * dt);
     s.vstar[k] = make_float4(vsk.x, vsk.y, vsk.z, source);
@@ -594,20 +608,21 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_tile_iisph3d_pressure_acc(i
     const float4* src4[1] = {s.pos};
     float4* dst4[1] = {sp};
     const TileSlab slab = slab_at(tile_smem, 20, T.K);
-    stage_tile_async<1, float>(stg, d, nr, src4, dst4, s.p, sa, T, slab);
+    // boundary neighbors enter through sum_bnd m_j gradW (second loop), so
+    // only the fluid candidates and entries are visited
+    stage_tile_async<1, float, true>(stg, d, nr, src4, dst4, s.p, sa, T, slab);
     const bool valid = live;
     const int64_t kk = valid ? k : 0;
-    const float4 pk = s.pos[kk];
+    const float4 pk = s.pos[kk], gbk = s.gbnd[kk];
     const float prk = s.p[kk];
     if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
-    const float wb = (c.single_layer ? c.two_gamma : 2.f) * prk;
     Acc3<float, true> pa;
     V3<float> part = v3<float>(0.f, 0.f, 0.f);
-    if (valid) for_tile_entries(slab, T.K, (int)(threadIdx.x >> 1), half, [&](uint32_t off, bool bnd) {
+    if (valid) for_tile_entries<true>(slab, T.K, (int)(threadIdx.x >> 1), half, [&](uint32_t off, bool) {
         const float4 pj = at_offset(sp, off);
         const V3<float> xij = sub3(pk, pj);
-        const float coef = pj.w * (bnd ? wb : prk + at_offset(sa, off >> 2)) * S.grad(r2_of(xij));
+        const float coef = pj.w * (prk + at_offset(sa, off >> 2)) * S.grad(r2_of(xij));
         part = fma3(-coef, xij, part);
     }, [&] {
         pa.add(part);
@@ -615,7 +630,9 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_tile_iisph3d_pressure_acc(i
     });
     const V3<float> a = pair_total(pa);
     if (half || !valid) return;
-    s.acc[k] = v4<float>(c.inv_rho0_sq * a, 0.f);
+    // boundary: - sum_bnd (lambda m_j p_i / rho0^2) gradW, lambda = 2 gamma (single layer) or 2
+    const float wb = (c.single_layer ? c.two_gamma : 2.f) * prk;
+    s.acc[k] = v4<float>(c.inv_rho0_sq * (a - wb * v3<float>(gbk.x, gbk.y, gbk.z)), 0.f);
 }
 
 // iteration (b): A p, relaxed Jacobi update, density error, fused scan
@@ -646,25 +663,26 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_pressure_updat
         const float4* src4[2] = {s.pos, s.acc};
         float4* dst4[2] = {sp, sa};
         const TileSlab slab = slab_at(tile_smem, 32, T.K);
-        stage_tile_async<2, float>(stg, d, nr, src4, dst4, (const float*)nullptr, (float*)nullptr, T, slab);
+        // boundary neighbors enter through sum_bnd m_j gradW (second loop)
+        stage_tile_async<2, float, true>(stg, d, nr, src4, dst4, (const float*)nullptr, (float*)nullptr, T, slab);
         // the owner's own data, loaded while the staging lands
         const bool valid = live;
-        const float4 pk = s.pos[kk], ak = s.acc[kk], vsk = s.vstar[kk];
+        const float4 pk = s.pos[kk], ak = s.acc[kk], vsk = s.vstar[kk], gbk = s.gbnd[kk];
         const float aii = s.anp[kk].w, prk = s.p[kk];
         if (stage_tile_wait(stg, status)) {
             const FastSpline S(c.kern);
             Acc<float, true> ap;
             float part = 0.f;
-            if (valid) for_tile_entries(slab, T.K, (int)(threadIdx.x >> 1), half, [&](uint32_t off, bool bnd) {
+            if (valid) for_tile_entries<true>(slab, T.K, (int)(threadIdx.x >> 1), half, [&](uint32_t off, bool) {
                 const float4 pj = at_offset(sp, off);
                 const V3<float> xij = sub3(pk, pj);
-                const V3<float> da = bnd ? v3<float>(ak.x, ak.y, ak.z) : sub3(ak, at_offset(sa, off));
-                part = __fmaf_rn(pj.w * S.grad(r2_of(xij)), dot3(da, xij), part);
+                part = __fmaf_rn(pj.w * S.grad(r2_of(xij)), dot3(sub3(ak, at_offset(sa, off)), xij), part);
             }, [&] {
                 ap.add(part);
                 part = 0.f;
             });
-            const float sum = pair_total(ap);
+            // boundary: sum_bnd m_j dot(a_i, gradW) = dot(a_i, sum_bnd m_j gradW)
+            const float sum = pair_total(ap) + dot3(v3<float>(ak.x, ak.y, ak.z), v3<float>(gbk.x, gbk.y, gbk.z));
             if (!half && valid)
                 o = iisph3d_pressure_update_tail<float>(k, s, c, dt, v3<float>(ak.x, ak.y, ak.z), sum, vsk, aii, prk);
         }
