@@ -272,6 +272,7 @@ def run_ours(args):
     solver_state = solver.collection() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     solver.close()
     batched = None if args.no_batched else run_batched(args, local, rank, world, max_over_ranks, barrier)
+    ns_micro = run_ns_microbench(args, local) if (rank == 0 and world == 1 and not args.no_batched) else None
 
     cpu = None
     if solver_state is not None:
@@ -300,7 +301,7 @@ def run_ours(args):
                          "algorithmic_bytes_per_launch": per_launch, "per": PHASE_UNITS[dom],
                          "traffic_source": "profiles/traffic.json (ncu dram__bytes_read.sum + dram__bytes_write.sum)"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
-            "batched": batched,
+            "batched": batched, "ns_microbench": ns_micro,
         }
         print(json.dumps(out))
     if world > 1:
@@ -360,6 +361,51 @@ def run_batched(args, device, rank, world, max_over_ranks, barrier):
         out["plain_per_scene_ms_per_step"] = total_ms / args.steps
         out["speedup_vs_plain_per_scene"] = out["value"] / out["plain_per_scene_value"]
     return out
+
+
+def run_ns_microbench(args, device):
+    """The 3D search microbenchmark: 10^6 uniform points in the unit cube
+    (seed 2), r = 0.02. (1) The device search as a solver step runs it (sort,
+    reorder, cell table and the neighbor lists of every point), timed with
+    the library's own events over --steps searches. (2) The contract's
+    neighbor sets exported in host index space (fs_get_neighbors_csr, both
+    calls, wall clock). Byte model: 96 B per point (keys, sort, permute of
+    the positions) + (4 n + 8) B of lists per point."""
+    from fluidsolver_b200 import IISPHFluidSolver3D, NeighborhoodSearch, ParticleCollection
+    from fluidsolver_b200 import _lib as F
+    pts = scenes_mod().ns_points_uniform()
+    col = ParticleCollection(position=pts)
+    s = IISPHFluidSolver3D(search="hashed-3d", precision="fp32-kahan", device=device)
+    s.parameters.particle_size = 0.01
+    s.data.collection = col
+    for _ in range(args.warmup):
+        s.execute_neighborhood_search()
+    ms = []
+    for _ in range(args.steps):
+        s.execute_neighborhood_search()
+        ms.append(s.phase_times()[0])
+    s.close()
+    ns = NeighborhoodSearch("hashed-3d", 0.02, device=device)
+    ns.data.collection = col
+    ns.find_neighbors()
+    t0 = time.perf_counter()
+    off, idx = ns.neighbor_lists()
+    export_s = time.perf_counter() - t0
+    ns.close()
+    nbar = len(idx) / len(pts)
+    per = statistics.median(ms)
+    bytes_ = (96 + 4 * nbar + 8) * len(pts)
+    peak, kind = measured_peak()
+    return {"workload": "10^6 uniform points in [0,1)^3 (seed 2), r = 0.02, hashed-3d contract",
+            "neighbors_mean": nbar, "search_with_lists_ms": per, "points_per_s": len(pts) / (per / 1e3),
+            "algorithmic_bytes": bytes_, "achieved_gbs": bytes_ / (per / 1e3) / 1e9,
+            "frac_of_hbm_peak": bytes_ / (per / 1e3) / 1e9 / peak,
+            "csr_export_s": export_s, "csr_export_path": "fs_get_neighbors_csr, sets in host index space, wall clock"}
+
+
+def scenes_mod():
+    from fluidsolver_b200 import scenes
+    return scenes
 
 
 def run_e2e(solver, scene, steps, device, max_over_ranks):
