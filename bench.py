@@ -273,6 +273,7 @@ def run_ours(args):
     solver.close()
     batched = None if args.no_batched else run_batched(args, local, rank, world, max_over_ranks, barrier)
     ns_micro = run_ns_microbench(args, local) if (rank == 0 and world == 1 and not args.no_batched) else None
+    configs = run_configs(args, local) if (rank == 0 and world == 1 and not args.no_batched) else None
 
     cpu = None
     if solver_state is not None:
@@ -301,7 +302,7 @@ def run_ours(args):
                          "algorithmic_bytes_per_launch": per_launch, "per": PHASE_UNITS[dom],
                          "traffic_source": "profiles/traffic.json (ncu dram__bytes_read.sum + dram__bytes_write.sum)"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
-            "batched": batched, "ns_microbench": ns_micro,
+            "batched": batched, "ns_microbench": ns_micro, "other_configs": configs,
         }
         print(json.dumps(out))
     if world > 1:
@@ -403,6 +404,93 @@ def run_ns_microbench(args, device):
             "csr_export_s": export_s, "csr_export_path": "fs_get_neighbors_csr, sets in host index space, wall clock"}
 
 
+def run_configs(args, device):
+    """The other configurations, each next to the reference's own CPU code
+    (oracle/_ref, bounded samples): the 2D SESPH dam (hashed-2d), the 100k 3D
+    IISPH dam, and the 1M dam in the two other precisions (plain FP32 in the
+    reference's operation order, FP64). GPU times are CUDA events around
+    fs_run on the library's stream."""
+    import torch
+    from fluidsolver_b200 import SESPHFluidSolver
+    from fluidsolver_b200 import _lib as F
+    from fluidsolver_b200.scenes import REFERENCE_UNITS_DT
+    sc = scenes_mod()
+    L = F.lib()
+
+    def gpu_time(solver, steps):
+        solver.run(args.warmup)
+        st = torch.cuda.ExternalStream(L.fs_stream(solver.ctx), device=torch.device("cuda", device))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(st)
+        stats = solver.run(steps)
+        b.record(st)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / steps, stats
+
+    def ref_time(solver_kind, search, scene, params, settings, gen, steps, budget_s):
+        from oracle import ref_oracle as R
+        variant = "omp" if R.available("omp") else ("serial" if R.available("serial") else None)
+        if variant is None:
+            return None
+        ref = R.RefSolver(solver_kind, search, scene.collection, params, settings, gen, variant=variant)
+        ref.step()
+        t0, k = time.perf_counter(), 0
+        while k < steps and time.perf_counter() - t0 < budget_s:
+            ref.step()
+            k += 1
+        el = time.perf_counter() - t0
+        ref.close()
+        return {"ms_per_step": el / k * 1e3, "steps": k, "cores": os.cpu_count() if variant == "omp" else 1,
+                "kind": "reference", "variant": "OpenMP over its 16-particle chunks" if variant == "omp" else "as built"}
+
+    out = {}
+    # 2D SESPH dam: 50 x 50 fluid, 3 boundary layers, k 1000, nu 0.01, dt 0.001 (no CFL clamp in 2D SESPH)
+    d2 = sc.breaking_dam_2d()
+    s2 = SESPHFluidSolver(search="hashed-2d", device=device)
+    s2.parameters.rest_density, s2.parameters.gravity, s2.parameters.particle_size = 1.0, 9.81, 1.0
+    s2.settings.StiffnessK, s2.settings.Viscosity = 1000.0, 0.01
+    s2.timestep_generator.settings.timestep = 0.001
+    s2.data.collection = d2.collection
+    ms2, _ = gpu_time(s2, 200)
+    s2.close()
+    out["sesph2d_dam"] = {"workload": f"2D SESPH dam, {d2.n_fluid} fluid + {d2.n_boundary} boundary, hashed-2d, "
+                                      "k 1000, nu 0.01, dt 0.001", "gpu_ms_per_step": ms2,
+                          "gpu_particle_steps_per_s": d2.n_fluid / (ms2 / 1e3),
+                          "cpu": None}
+    if not args.no_cpu_baseline:
+        from oracle import ref_oracle as R
+        cpu = ref_time("sesph-2d", "hashed-2d", d2, (1.0, 9.81, 1.0), R.sesph2d_settings(1000.0, 0.01),
+                       (0.001, 0.4, 0.25), 200, 10.0)
+        out["sesph2d_dam"]["cpu"] = cpu
+    # 3D IISPH 100k dam
+    d3 = sc.dam_100k()
+    s3 = make_solver(d3, device)
+    ms3, st3 = gpu_time(s3, 20)
+    s3.close()
+    out["iisph3d_dam_100k"] = {"workload": f"3D IISPH dam, {d3.n_fluid} fluid + {d3.n_boundary} boundary, hashed-3d, "
+                                           f"dt {REFERENCE_UNITS_DT}", "gpu_ms_per_step": ms3,
+                               "gpu_particle_steps_per_s": d3.n_fluid / (ms3 / 1e3),
+                               "iterations_last_step": int(st3.iterations), "cpu": None}
+    if not args.no_cpu_baseline:
+        params, settings, gen = reference_settings()
+        out["iisph3d_dam_100k"]["cpu"] = ref_time("iisph-3d", "hashed-3d", d3, params, settings, gen, 5, 15.0)
+    # 1M dam in the other precisions
+    d4 = sc.dam_1m(seed=5)
+    for prec in ("fp32", "fp64"):
+        s4 = make_solver(d4, device, prec)
+        if prec == "fp32":
+            s4.reference_order = True
+        ms4, st4 = gpu_time(s4, 5)
+        s4.close()
+        out[f"iisph3d_dam_1m_{prec}"] = {
+            "workload": "the 1M dam" + (" in FP32 with the reference's operation order and list order" if prec ==
+                                        "fp32" else " in FP64 (the error reference)"),
+            "gpu_ms_per_step": ms4, "gpu_particle_steps_per_s": d4.n_fluid / (ms4 / 1e3),
+            "iterations_last_step": int(st4.iterations), "avg_density_error_last_step": float(st4.avg_density_error_fp64)}
+    return out
+
+
 def scenes_mod():
     from fluidsolver_b200 import scenes
     return scenes
@@ -477,15 +565,19 @@ def run_reference(args):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         iters.append(ref.step()["iterations"])
+        if time.perf_counter() - t0 > 150.0:   # keep the run within a few minutes
+            break
     el = time.perf_counter() - t0
     ref.close()
-    value = scene.n_fluid * args.steps / el
+    done = len(iters)
+    value = scene.n_fluid * done / el
     cores = os.cpu_count() if variant == "omp" else 1
     sample = (f"100,000-fluid breaking dam (40x50x50 column, 59,684 boundary) of the same scene family, "
-              f"{args.steps} steps after {args.warmup} warm-up steps, mean iterations {np.mean(iters):.2f}")
+              f"{done} of {args.steps} steps (150 s budget) after {args.warmup} warm-up steps, "
+              f"mean iterations {np.mean(iters):.2f}")
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+        "steps": done, "warmup": args.warmup, "ms_per_step": el / done * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded breaking-dam scenes)",
         "impl": "reference",
         "config": {"workload": "3D IISPH breaking dam (bounded sample: 100k fluid), hashed-3d, dt 0.005",
