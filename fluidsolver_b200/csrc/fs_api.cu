@@ -632,7 +632,7 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     c->launches++;
     k_keys<R><<<grid_for(n), kBlock, 0, st>>>(n, s.pos, s.type, s.hidx, c->include_inactive, single, c->search_radius,
                                               c->truncate_cells, c->grids, s.scene, c->key_bits, c->keys[0], k64,
-                                              c->perm[0]);
+                                              c->perm[0], c->status);
     FS_CUDA(cudaGetLastError());
     size_t temp = c->cub_temp_bytes;
     if (single) {
@@ -1025,7 +1025,9 @@ fs_status search_for_step(fs_ctx* c, float dt) {
             FS_TRY(ensure_lists(c, K));
             continue;
         }
-        if (st != FS_OK) return fail((fs_status)st, "neighbor list capacity exceeded");
+        if (st != FS_OK)
+            return fail((fs_status)st, st == FS_ERR_CAPACITY ? "neighbor list capacity exceeded"
+                                                             : "device reported an error during the search");
         c->searched_dt = dt;
         return FS_OK;
     }

@@ -158,7 +158,8 @@ __global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* 
                        const uint32_t* __restrict__ hidx, bool include_inactive, bool single_region, float r,
                        bool trunc, const SceneGrid* __restrict__ grids, const uint16_t* __restrict__ scene,
                        int key_bits, uint32_t* __restrict__ keys,
-                       unsigned long long* __restrict__ keys64, uint32_t* __restrict__ perm) {
+                       unsigned long long* __restrict__ keys64, uint32_t* __restrict__ perm,
+                       int* __restrict__ status) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     uint8_t t = type[k];
@@ -167,6 +168,13 @@ __global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* 
         key = inactive_key(key_bits);
     } else {
         V4<R> p = pos[k];
+        if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) {
+            // a position that is NaN or infinite ends the step with FS_ERR_NAN
+            // (and stays out of the cell structure, which the rest of the
+            // step then no longer builds on)
+            raise_status(status, FS_ERR_NAN);
+            p.x = p.y = p.z = R(0);
+        }
         const SceneGrid g = grids[scene ? scene[k] : 0];
         bool cl = false;
         int lx = local_cell(cell_coord<R>(p.x, r, trunc), g.o0, g.d0, cl);
@@ -368,7 +376,7 @@ __global__ void __launch_bounds__(128) k_build_lists(int64_t n_owners, const V4<
                                                      uint32_t* __restrict__ count, int* __restrict__ status,
                                                      StepScalars* __restrict__ sc) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n_owners) return;
+    if (k >= n_owners || *status) return;
     uint32_t c = 0;
     if ((owner_mask >> type[k]) & 1u) c = build_list_one<R>(k, pos, type, cell_start, w, rows, nbr, stride, K);
     count[k] = c;

@@ -91,6 +91,7 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     __shared__ int s_gd0[kTileGroups], s_gd01[kTileGroups], s_gx0[kTileGroups], s_gx1[kTileGroups];
     __shared__ uint32_t s_start[kTileRanges], s_len[kTileRanges], s_base[kTileRanges];
     __shared__ uint32_t s_total;
+    if (*status) return;   // an earlier error (e.g. non-finite positions) ends the step
 
     const int t = threadIdx.x, lane = t & 31;
     const int64_t tile = blockIdx.x;

@@ -17,7 +17,7 @@ import pytest
 from conftest import bits_equal
 from fluidsolver_b200 import (IISPHFluidSolver, IISPHFluidSolver3D, SESPHFluidSolver, SESPHFluidSolver3D, Timepoint,
                               scenes)
-from fluidsolver_b200._lib import FS_ERR_STATE, FluidSolverError
+from fluidsolver_b200._lib import FS_ERR_NAN, FS_ERR_STATE, FluidSolverError
 from tests.golden.make_golden import SOLVER_CASES
 
 pytestmark = pytest.mark.gpu
@@ -248,4 +248,23 @@ def test_1m_dam_properties_at_full_size():
     # boundary particles do not move (zero velocity, zero acceleration)
     b = out.type == 1
     assert bits_equal(out.position[b], sc.collection.position[b])
+    s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp32-kahan", "fp32"])
+def test_non_finite_positions_end_the_step_with_a_nan_status(precision):
+    """A NaN position stops the step with FS_ERR_NAN: the particle is kept out
+    of the cell walks, and the list builders and solver phases skip their
+    work, so a broken state cannot turn the search quadratic."""
+    sc = scenes.breaking_dam_3d(12, 12, 12, 1.0, tank=(40, 30, 20), seed=3)
+    col = sc.collection
+    col.position = col.position.copy()
+    col.position[7, 1] = np.nan
+    s = IISPHFluidSolver3D(search="hashed-3d", precision=precision, reference_order=precision == "fp32")
+    s.parameters.rest_density, s.parameters.particle_size = 1.0, 1.0
+    s.timestep_generator.settings.timestep = 0.005
+    s.data.collection = col
+    with pytest.raises(FluidSolverError) as e:
+        s.step()
+    assert e.value.status == FS_ERR_NAN
     s.close()
