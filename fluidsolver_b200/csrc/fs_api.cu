@@ -754,25 +754,38 @@ __global__ void k_step_begin(StepScalars* sc, int scenes, float desired_dt, bool
 // convergence test, which ends the loop on the device (and always within
 // max_iterations executions, see k_iisph_check).
 template <typename Body>
-fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_test, Body&& body) {
+// first_done: the first iteration already ran fused into the preceding
+// phase (its scalars are accumulated); its test runs first, outside the loop.
+fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_test, Body&& body,
+                                bool first_done = false) {
     const int max_it = c->prm.max_iterations;
     if (max_it <= 0) return FS_OK;
     cudaStream_t st = c->stream;
+    auto check = [&](cudaStream_t s, cudaGraphConditionalHandle h, bool set) {
+        c->launches++;
+        if (c->scenes > 0)
+            k_iisph_check_scenes<<<1, 256, 0, s>>>(c->scalars, c->scenes, c->prm.min_iterations, max_it,
+                                                   c->prm.max_density_error, c->status, h, set);
+        else
+            k_iisph_check<<<1, 1, 0, s>>>(c->scalars, c->prm.min_iterations, max_it, c->prm.max_density_error,
+                                          fp64_test, two_d, c->status, h, set);
+    };
     if (!capture) {
-        for (int it = 0; it < max_it; it++) {
-            body(st);
-            c->launches++;
-            if (c->scenes > 0)
-                k_iisph_check_scenes<<<1, 256, 0, st>>>(c->scalars, c->scenes, c->prm.min_iterations, max_it,
-                                                        c->prm.max_density_error, c->status, 0, false);
-            else
-                k_iisph_check<<<1, 1, 0, st>>>(c->scalars, c->prm.min_iterations, max_it, c->prm.max_density_error,
-                                               fp64_test, two_d, c->status, 0, false);
+        auto all_done = [&]() -> fs_status {
             FS_CUDA(cudaGetLastError());
             FS_TRY(read_scalars(c));
-            bool all_done = true;
-            for (int i = 0; i < c->nsc(); i++) all_done = all_done && c->scalars_host[i].done;
-            if (all_done) break;
+            bool d = true;
+            for (int i = 0; i < c->nsc(); i++) d = d && c->scalars_host[i].done;
+            return d ? FS_ERR_STATE : FS_OK;   // FS_ERR_STATE here only means "stop"
+        };
+        if (first_done) {
+            check(st, 0, false);
+            if (all_done() != FS_OK) return FS_OK;
+        }
+        for (int it = first_done ? 1 : 0; it < max_it; it++) {
+            body(st);
+            check(st, 0, false);
+            if (all_done() != FS_OK) break;
         }
         return FS_OK;
     }
@@ -783,6 +796,12 @@ fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_t
     FS_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps));
     cudaGraphConditionalHandle handle;
     FS_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+    if (first_done) {
+        // the fused first iteration's test sets the loop's initial condition
+        check(st, handle, true);
+        FS_CUDA(cudaGetLastError());
+        FS_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps));
+    }
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = handle;
@@ -795,13 +814,7 @@ fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_t
     FS_CUDA(cudaStreamBeginCaptureToGraph(c->body_stream, body_graph, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
     body(c->body_stream);
-    c->launches++;
-    if (c->scenes > 0)
-        k_iisph_check_scenes<<<1, 256, 0, c->body_stream>>>(c->scalars, c->scenes, c->prm.min_iterations, max_it,
-                                                            c->prm.max_density_error, c->status, handle, true);
-    else
-        k_iisph_check<<<1, 1, 0, c->body_stream>>>(c->scalars, c->prm.min_iterations, max_it,
-                                                    c->prm.max_density_error, fp64_test, two_d, c->status, handle, true);
+    check(c->body_stream, handle, true);
     cudaError_t e = cudaGetLastError();
     cudaError_t e2 = cudaStreamEndCapture(c->body_stream, nullptr);
     if (e != cudaSuccess || e2 != cudaSuccess) return fail(FS_ERR_CUDA, "capture of the pressure loop failed");
@@ -829,13 +842,14 @@ fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
     k_tile_iisph3d_l2<<<tiles, kPassThreads, tile_pass_smem(32, T.K), st>>>(nf, s, T, L, k, c->scalars, c->status);
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 3, st));
+    // the second loop also ran the first pressure iteration (fs_tiles.cuh)
     FS_TRY(enqueue_pressure_loop(c, capture, false, true, [&](cudaStream_t bs) {
         c->launches += 2;
         k_tile_iisph3d_pressure_acc<<<tiles, kPassThreads, tile_pass_smem(20, T.K), bs>>>(nf, s, T, L, k, c->scalars,
                                                                                  c->status);
         k_tile_iisph3d_pressure_update<<<tiles, kPassThreads, tile_pass_smem(32, T.K), bs>>>(nf, s, T, L, k, c->scalars,
                                                                                     c->status);
-    }));
+    }, true));
     FS_TRY(mark(c, 4, st));
     c->launches++;
     k_cfl<<<1, 128, 0, st>>>(c->scalars, c->nsc(), c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,

@@ -393,6 +393,19 @@ __device__ __forceinline__ void add_err_part(const ErrPart& o, StepScalars* __re
     atomic_max_nonneg(&q->max_v2_bits, o.v2);
 }
 
+// The first pressure iteration without neighbor sums (fast mode). The first
+// loop sets every pressure to 0 (IISPHFluidSolver3D.hpp:141-212), so the
+// iteration's pressure accelerations are 0 (the sums of :348-397 over p = 0)
+// and so is A p (:402-461): the update is p = max(0, omega s / a_ii), the
+// error |s|, the acceleration 0. vs: v* with the source term in w; aii: the
+// diagonal element, as the second loop just computed them.
+template <typename R>
+__device__ __forceinline__ ErrPart iisph3d_first_iteration(int64_t k, const State<R>& s, const SolverConsts<R>& c,
+                                                           R dt, V4<R> vs, R aii) {
+    s.acc[k] = v4<R>(v3<R>(R(0), R(0), R(0)), R(0));
+    return iisph3d_pressure_update_tail<R>(k, s, c, dt, v3<R>(R(0), R(0), R(0)), R(0), vs, aii, R(0));
+}
+
 // block reduction of the ErrParts into StepScalars (FP64 residual sum); every
 // thread of the block calls it. scene: the scene of the thread's particle.
 // A block whose threads all belong to one scene reduces first; a block that

@@ -518,19 +518,30 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l1(int64_t n_f
     s.rho[k] = rk;
 }
 
-// second loop: source term and diagonal element (single-pass a_ii)
+// second loop: source term and diagonal element (single-pass a_ii), then
+// the first pressure iteration, which needs no neighbor sums
+// (iisph3d_first_iteration), with its part of the convergence scan
 __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l2(int64_t n_fluid, State<float> s, TileLists T,
                                                                   Lists L, SolverConsts<float> c,
-                                                                  const StepScalars* __restrict__ sc,
+                                                                  StepScalars* __restrict__ sc,
                                                                   int* __restrict__ status) {
     extern __shared__ float4 tile_smem[];
     if (*status) return;
     const int half = threadIdx.x & 1;
     const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
+    const bool valid = k < n_fluid;
+    const int64_t kk = valid ? k : 0;
+    const int scene = s.scene_of(kk);
+    const float dt = sc[scene].dt;
     const TileDesc* d = T.desc + blockIdx.x;
     const uint32_t nr = d->nranges;
+    ErrPart o;
     if (nr == kTileFallback) {
-        if (k < n_fluid && !half) iisph3d_l2_one<float, true, false>(k, s, L, c, sc[s.scene_of(k)].dt);
+        if (valid && !half) {
+            iisph3d_l2_one<float, true, false>(k, s, L, c, dt);
+            o = iisph3d_first_iteration<float>(k, s, c, dt, s.vstar[k], s.anp[k].w);
+        }
+        reduce_err_parts(o, sc, scene);
         return;
     }
     float4* sp = tile_smem;
@@ -540,11 +551,8 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l2(int64_t n_f
     float4* dst4[2] = {sp, sa};
     const TileSlab slab = slab_at(tile_smem, 32, T.K);
     stage_tile_async<2, float>(stg, d, nr, src4, dst4, (const float*)nullptr, (float*)nullptr, T, slab);
-    const bool valid = k < n_fluid;
-    const int64_t kk = valid ? k : 0;
     const float4 pk = s.pos[kk], vsk = s.vstar[kk];
     const float rk = s.rho[kk];
-    const float dt = sc[s.scene_of(kk)].dt;
     if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     Acc<float, true> contrib, mg2;
@@ -575,12 +583,16 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l2(int64_t n_f
     });
     const float ct = pair_total(contrib), g2 = pair_total(mg2);
     const V3<float> in = pair_total(inner), m = pair_total(mg), gbt = pair_total(gb);
-    if (half || !valid) return;
-    s.gbnd[k] = v4<float>(gbt, 0.f);   // sum_bnd m_j gradW, for the pressure iterations
-    const float source = (c.rest_density - rk) - dt * ct;
-    const float diag = (c.inv_rho0_sq * dot(in, m) - (pk.w / c.rho0_sq) * g2) * (dt * dt);
-    s.vstar[k] = make_float4(vsk.x, vsk.y, vsk.z, source);
-    s.anp[k].w = diag;
+    if (!half && valid) {
+        s.gbnd[k] = v4<float>(gbt, 0.f);   // sum_bnd m_j gradW, for the pressure iterations
+        const float source = (c.rest_density - rk) - dt * ct;
+        const float diag = (c.inv_rho0_sq * dot(in, m) - (pk.w / c.rho0_sq) * g2) * (dt * dt);
+        const float4 vs = make_float4(vsk.x, vsk.y, vsk.z, source);
+        s.vstar[k] = vs;
+        s.anp[k].w = diag;
+        o = iisph3d_first_iteration<float>(k, s, c, dt, vs, diag);
+    }
+    reduce_err_parts(o, sc, scene);
 }
 
 // iteration (a): pressure acceleration
