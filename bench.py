@@ -480,6 +480,28 @@ def run_configs(args, device):
     if not args.no_cpu_baseline:
         params, settings, gen = reference_settings()
         out["iisph3d_dam_100k"]["cpu"] = ref_time("iisph-3d", "hashed-3d", d3, params, settings, gen, 5, 15.0)
+    # the other solvers at a glance: 3D SESPH on the 100k dam, 2D IISPH on the 2D dam
+    from fluidsolver_b200 import IISPHFluidSolver, SESPHFluidSolver3D
+    s5 = SESPHFluidSolver3D(search="hashed-3d", device=device)
+    s5.parameters.rest_density, s5.parameters.gravity, s5.parameters.particle_size = 1.0, 9.81, 1.0
+    s5.settings.StiffnessK, s5.settings.Viscosity = 1000.0, 0.01
+    s5.settings.single_layer_boundary = True
+    s5.timestep_generator.settings.timestep = 0.001
+    s5.data.collection = d3.collection
+    ms5, _ = gpu_time(s5, 20)
+    s5.close()
+    out["sesph3d_dam_100k"] = {"workload": "3D SESPH on the 100k dam, hashed-3d, k 1000, nu 0.01, dt 0.001 (CFL-clamped)",
+                               "gpu_ms_per_step": ms5, "gpu_particle_steps_per_s": d3.n_fluid / (ms5 / 1e3)}
+    s6 = IISPHFluidSolver(search="hashed-2d", device=device)
+    s6.parameters.rest_density, s6.parameters.gravity, s6.parameters.particle_size = 1.0, 9.81, 1.0
+    s6.settings.Viscosity = 0.01
+    s6.timestep_generator.settings.timestep = 0.001
+    s6.data.collection = d2.collection
+    ms6, st6 = gpu_time(s6, 100)
+    s6.close()
+    out["iisph2d_dam"] = {"workload": f"2D IISPH dam, {d2.n_fluid} fluid + {d2.n_boundary} boundary, hashed-2d, dt 0.001",
+                          "gpu_ms_per_step": ms6, "gpu_particle_steps_per_s": d2.n_fluid / (ms6 / 1e3),
+                          "iterations_last_step": int(st6.iterations)}
     # 1M dam in the other precisions
     d4 = sc.dam_1m(seed=5)
     for prec in ("fp32", "fp64"):
