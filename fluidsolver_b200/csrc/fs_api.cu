@@ -623,7 +623,8 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     // bbox of the structure's cells -> grid origin
     FS_TRY(reset_bbox(c));
     c->launches++;
-    k_bbox<R><<<grid_for(n, 256), 256, 0, st>>>(n, s.pos, s.type, s.scene, c->nsc(), c->include_inactive,
+    const unsigned gb = c->scenes > 0 ? grid_for(n, 256) : std::min<unsigned>(grid_for(n, 256), 148u * 8u);
+    k_bbox<R><<<gb, 256, 0, st>>>(n, s.pos, s.type, s.scene, c->nsc(), c->include_inactive,
                                                  c->search_radius, c->truncate_cells, c->bbox);
     c->launches++;
     k_origin<<<grid_for(c->nsc(), 128), 128, 0, st>>>(c->bbox, c->grids, c->nsc());

@@ -13,7 +13,7 @@
 //   type  uint8, hidx uint32 (host index of the particle at this position)
 // Sorted order puts fluid particles first, then boundary particles, then the
 // inactive particles a contract still lists, then excluded inactive ones,
-// each block in Z-order of its cells (a single Z-ordered block in the
+// each block in linear cell order, x fastest (a single block in the
 // reference-order mode). Fluid-only phases run over [0, n_fluid).
 #pragma once
 

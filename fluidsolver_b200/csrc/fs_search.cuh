@@ -65,11 +65,18 @@ __global__ void k_bbox(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* 
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
     const int sk = (k < n && scene) ? scene[k] : 0;
-    if (k < n && (include_inactive || type[k] != FS_TYPE_INACTIVE)) {
-        const V4<R> p = pos[k];
+    // one scene: a grid-stride loop (a grid of a few blocks per SM); scenes:
+    // one particle per thread
+    const int64_t stride = scene ? n : (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = k; i < n; i += stride) {
+        if (!include_inactive && type[i] == FS_TYPE_INACTIVE) continue;
+        const V4<R> p = pos[i];
         const int c[3] = {cell_coord<R>(p.x, r, trunc), cell_coord<R>(p.y, r, trunc), cell_coord<R>(p.z, r, trunc)};
 #pragma unroll
-        for (int a = 0; a < 3; a++) mn[a] = mx[a] = c[a];
+        for (int a = 0; a < 3; a++) {
+            mn[a] = min(mn[a], c[a]);
+            mx[a] = max(mx[a], c[a]);
+        }
     }
     __shared__ int s_first;
     if (threadIdx.x == 0) s_first = sk;

@@ -71,6 +71,43 @@ inline size_t tile_pass_smem(int bytes_per_candidate, int K) {
 }
 
 // ---------------------------------------------------------------------------
+// asynchronous staging (the builder and the passes)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// the mbarrier that a tile's bulk copies complete on
+struct TileStage {
+    uint64_t bar;
+};
+
+__device__ __forceinline__ uint32_t mbar_try_wait0(TileStage& st) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(&st.bar))
+        : "memory");
+    return ok;
+}
+
+// Waits for the staging to land, with a bounded number of tries. Returns
+// false, with FS_ERR_TIMEOUT raised, if the copies did not complete; the
+// caller then skips the tile (after a second bounded wait that gives copies
+// still in flight time to land before the block exits).
+__device__ __forceinline__ bool stage_tile_wait(TileStage& st, int* __restrict__ status) {
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    uint32_t ok = 0;
+    for (int it = 0; it < (1 << 16) && !ok; it++) ok = mbar_try_wait0(st);
+    const int late = __syncthreads_or(!ok);
+    if (late) {
+        if (threadIdx.x == 0) raise_status(status, FS_ERR_TIMEOUT);
+        for (int it = 0; it < (1 << 16) && !ok; it++) ok = mbar_try_wait0(st);
+        return false;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
 // list builder: one block of kTileOwners threads per tile
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
@@ -172,12 +209,24 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
         return;
     }
 
-    // stage the candidates' positions (a warp per range)
-    for (int q = t >> 5; q < NR; q += kTileOwners / 32) {
-        const uint32_t a = s_start[q], len = s_len[q], base = s_base[q];
-        for (uint32_t i = lane; i < len; i += 32) sp[base + i] = pos[a + i];
+    // stage the candidates' positions: a bulk copy per range (the TMA engine)
+    __shared__ TileStage stg;
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&stg.bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    if (t == 0)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&stg.bar)),
+                     "r"(s_total * 16u)
+                     : "memory");
+    if (t < NR && s_len[t])
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_u32(sp + s_base[t])),
+            "l"(pos + s_start[t]), "r"(s_len[t] * 16u), "r"(smem_u32(&stg.bar))
+            : "memory");
+    if (!stage_tile_wait(stg, status)) return;
 
     // each owner tests the candidates of its own 27 cells: the 18 row bounds
     // are loaded up front, candidates are tested two at a time
@@ -247,27 +296,18 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     }
 }
 
-// ---------------------------------------------------------------------------
-// pass helpers: asynchronous staging
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// the mbarrier that a tile's bulk copies complete on
-struct TileStage {
-    uint64_t bar;
-};
-
-// Starts the copies of the tile's candidate ranges into shared memory. Each
-// float4 array (position and mass, and the pass's float4 field if any) is
-// copied range by range with bulk copies (the TMA engine; one thread per
-// range, completion counted in bytes on the mbarrier); a float field goes
-// through 4-byte cp.async copies, a warp per range.
 // Shared-memory view of a tile's lists: entries [octet][owner] and lengths.
 struct TileSlab {
     uint4* ent;
     uint32_t* count;
 };
 
+// Starts the copies of the tile's candidate ranges into shared memory. Each
+// float4 array (position and mass, and the pass's float4 field if any) is
+// copied range by range with bulk copies (the TMA engine; one thread per
+// range, completion counted in bytes on the mbarrier); a float field goes
+// through 4-byte cp.async copies, a warp per range. FLUID_ONLY skips the
+// boundary ranges.
 template <int NV4, typename Scalar, bool FLUID_ONLY = false>
 __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* __restrict__ d, uint32_t nr,
                                                  const float4* const (&src4)[NV4], float4* const (&dst4)[NV4],
@@ -326,33 +366,6 @@ __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* 
                              : "memory");
         }
     }
-}
-
-__device__ __forceinline__ uint32_t mbar_try_wait0(TileStage& st) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_u32(&st.bar))
-        : "memory");
-    return ok;
-}
-
-// Waits for the staging to land, with a bounded number of tries. Returns
-// false, with FS_ERR_TIMEOUT raised, if the copies did not complete; the
-// caller then skips the tile (after a second bounded wait that gives copies
-// still in flight time to land before the block exits).
-__device__ __forceinline__ bool stage_tile_wait(TileStage& st, int* __restrict__ status) {
-    asm volatile("cp.async.wait_all;" ::: "memory");
-    uint32_t ok = 0;
-    for (int it = 0; it < (1 << 16) && !ok; it++) ok = mbar_try_wait0(st);
-    const int late = __syncthreads_or(!ok);
-    if (late) {
-        if (threadIdx.x == 0) raise_status(status, FS_ERR_TIMEOUT);
-        for (int it = 0; it < (1 << 16) && !ok; it++) ok = mbar_try_wait0(st);
-        return false;
-    }
-    return true;
 }
 
 // Visits one half of local owner ol's entries (entries 4 half .. 4 half + 3

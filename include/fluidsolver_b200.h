@@ -65,7 +65,7 @@ typedef enum fs_solver_kind {
 
 /*
  * Neighbor-set contract of the reference search being replaced. One device
- * search (cell-key radix sort + Z-order reordering + cell table) serves all of
+ * search (cell-key radix sort + cell-order reordering + cell table) serves all of
  * them; the contract fixes the predicate, which particles own a list, which
  * particles may appear in one, and the capacity limit.
  */
