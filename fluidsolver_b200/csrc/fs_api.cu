@@ -835,21 +835,23 @@ fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
     State<float> s = state_of<float>(c);
     FS_TRY(mark(c, 1, st));
     c->launches++;
-    k_tile_iisph3d_l1<<<tiles + rest, kPassThreads, tile_pass_smem(36, T.K), st>>>(nf, n, tiles, s, T, L, k, c->scalars,
-                                                                           c->status);
+    k_tile_iisph3d_l1<<<tiles + rest, kPassThreads, tile_pass_smem(36, T.K, !kL1GlobalEntries), st>>>(
+        nf, n, tiles, s, T, L, k, c->scalars, c->status);
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 2, st));
     c->launches++;
-    k_tile_iisph3d_l2<<<tiles, kPassThreads, tile_pass_smem(32, T.K), st>>>(nf, s, T, L, k, c->scalars, c->status);
+    k_tile_iisph3d_l2<<<tiles, kPassThreads, tile_pass_smem(32, T.K, !kL2GlobalEntries), st>>>(
+        nf, s, T, L, k, c->scalars, c->status);
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 3, st));
     // the second loop also ran the first pressure iteration (fs_tiles.cuh)
     FS_TRY(enqueue_pressure_loop(c, capture, false, true, [&](cudaStream_t bs) {
         c->launches += 2;
-        k_tile_iisph3d_pressure_acc<<<tiles, kPassThreads, tile_pass_smem(20, T.K), bs>>>(nf, s, T, L, k, c->scalars,
-                                                                                 c->status);
-        k_tile_iisph3d_pressure_update<<<tiles, kPassThreads, tile_pass_smem(32, T.K), bs>>>(nf, s, T, L, k, c->scalars,
-                                                                                    c->status);
+        const bool slab = !kPressureGlobalEntries;
+        k_tile_iisph3d_pressure_acc<<<tiles, kPassThreads, tile_pass_smem(20, T.K, slab), bs>>>(nf, s, T, L, k,
+                                                                                       c->scalars, c->status);
+        k_tile_iisph3d_pressure_update<<<tiles, kPassThreads, tile_pass_smem(32, T.K, slab), bs>>>(nf, s, T, L, k,
+                                                                                          c->scalars, c->status);
     }, true));
     FS_TRY(mark(c, 4, st));
     c->launches++;

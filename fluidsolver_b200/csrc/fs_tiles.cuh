@@ -42,14 +42,31 @@ constexpr uint32_t kTileFallback = 0xffffffffu;
 constexpr uint32_t kEntOffset = 0xfff0u;
 constexpr uint32_t kEntBoundary = 0x1u;
 
-struct TileDesc {
+struct TileHead {
     uint32_t nranges;                  // non-empty candidate ranges, or kTileFallback
     uint32_t staged;                   // candidates staged in total
     uint32_t staged_fluid;             // of them in fluid ranges
     uint32_t octets;                   // octets of entries of the tile's longest list
+};
+struct alignas(16) TileDesc {
+    TileHead h;
     uint32_t start[kTileRanges];       // first sorted index of each range
     uint32_t len_base[kTileRanges];    // length | kRangeBoundary for boundary ranges | (first staged slot << 16)
 };
+
+__device__ __forceinline__ TileHead load_head(const TileDesc* d) {
+    const uint4 a = *reinterpret_cast<const uint4*>(d);
+    return TileHead{a.x, a.y, a.z, a.w};
+}
+
+// the range of thread t (t < kTileRanges), loaded before the tile's header
+// is known
+struct TileRange {
+    uint32_t start, len_base;
+};
+__device__ __forceinline__ TileRange load_range(const TileDesc* d, int t) {
+    return t < kTileRanges ? TileRange{d->start[t], d->len_base[t]} : TileRange{0u, 0u};
+}
 constexpr uint32_t kRangeBoundary = 0x8000u;
 constexpr uint32_t kRangeLen = 0x7fffu;
 
@@ -66,9 +83,17 @@ struct TileLists {
 // position, velocity, density --, 32 for position and a float4 field, 20 for
 // position and a float field), then the tile's entries and list lengths.
 inline size_t tile_build_smem(int K) { return (size_t)kTileCap * 16 + (size_t)kTileOwners * (K + 8) * 2; }
-inline size_t tile_pass_smem(int bytes_per_candidate, int K) {
-    return (size_t)kTileCap * bytes_per_candidate + (size_t)(K / 8) * kTileOwners * 16 + kTileOwners * 4;
+inline size_t tile_pass_smem(int bytes_per_candidate, int K, bool slab = true) {
+    return (size_t)kTileCap * bytes_per_candidate + (slab ? (size_t)(K / 8) * kTileOwners * 16 + kTileOwners * 4 : 0);
 }
+// Whether a pass reads its entries straight from the global octet planes
+// (one octet ahead of use) instead of staging them in shared memory. Without
+// the slab, the first loop and the pressure passes fit 4 and 4-5 blocks per
+// SM instead of 3 and were faster on the 1M-particle dam (B200); the second
+// loop would need more than the 64 registers that 4 blocks leave it.
+constexpr bool kL1GlobalEntries = true;
+constexpr bool kL2GlobalEntries = false;
+constexpr bool kPressureGlobalEntries = true;
 
 // ---------------------------------------------------------------------------
 // asynchronous staging (the builder and the passes)
@@ -199,7 +224,7 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
 
     if (fallback) {
         // ordinary 32-bit lists for this tile's owners
-        if (t == 0) desc[tile].nranges = kTileFallback;
+        if (t == 0) desc[tile].h.nranges = kTileFallback;
         uint32_t c = 0;
         if (valid) {
             c = build_list_one<float>(k, pos, type, cell_start, w, true, nbr, stride, K);
@@ -272,7 +297,6 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     if (t == 0) {
         uint32_t mx = 0;
         for (int i = 0; i < kTileOwners; i++) mx = max(mx, s_cnt[i]);
-        desc[tile].octets = (min(mx, (uint32_t)K) + 7) / 8;
         uint32_t m = 0, fl = 0;
         for (int q = 0; q < NR; q++) {
             if (!s_len[q]) continue;
@@ -282,9 +306,7 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
             if (!bnd) fl += s_len[q];
             m++;
         }
-        desc[tile].nranges = m;
-        desc[tile].staged = s_total;
-        desc[tile].staged_fluid = fl;
+        *reinterpret_cast<uint4*>(desc + tile) = make_uint4(m, s_total, fl, (min(mx, (uint32_t)K) + 7) / 8);
     }
     // octets of entries, coalesced across the tile's owners
     const int O = K / 8;
@@ -302,19 +324,22 @@ struct TileSlab {
     uint32_t* count;
 };
 
-// Starts the copies of the tile's candidate ranges into shared memory. Each
-// float4 array (position and mass, and the pass's float4 field if any) is
-// copied range by range with bulk copies (the TMA engine; one thread per
-// range, completion counted in bytes on the mbarrier); a float field goes
-// through 4-byte cp.async copies, a warp per range. FLUID_ONLY skips the
-// boundary ranges.
-template <int NV4, typename Scalar, bool FLUID_ONLY = false>
-__device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* __restrict__ d, uint32_t nr,
+// Starts the copies of the tile's candidate ranges into shared memory: a
+// bulk copy (the TMA engine) per range and float4 array, issued by the
+// range's thread, and one per octet plane of the tile's entries and for its
+// list lengths, issued by threads from the top of the block; completion is
+// counted in bytes on the mbarrier. A float array goes through 4-byte
+// cp.async copies, a warp per range (its ranges start at arbitrary floats,
+// which bulk copies cannot). h and rg are the tile's header and the calling
+// thread's range, loaded up front. FLUID_ONLY skips the boundary ranges;
+// SLAB false leaves the entries and list lengths in global memory.
+template <int NV4, bool FLUID_ONLY = false, bool SLAB = true>
+__device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* __restrict__ d, const TileHead& h,
+                                                 const TileRange& rg,
                                                  const float4* const (&src4)[NV4], float4* const (&dst4)[NV4],
-                                                 const Scalar* __restrict__ src1, Scalar* dst1, const TileLists& T,
+                                                 const float* __restrict__ src1, float* dst1, const TileLists& T,
                                                  const TileSlab& slab) {
-    const int t = threadIdx.x, lane = t & 31;
-    const uint32_t octets = d->octets;
+    const int t = threadIdx.x;
     const int64_t first = (int64_t)blockIdx.x * kTileOwners;
     if (t == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&st.bar)) : "memory");
@@ -322,30 +347,29 @@ __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* 
     }
     __syncthreads();
     if (t == 0) {
-        const uint32_t bytes = (FLUID_ONLY ? d->staged_fluid : d->staged) * 16u * (uint32_t)NV4 +
-                               octets * (uint32_t)kTileOwners * 16u + (uint32_t)kTileOwners * 4u;
+        const uint32_t bytes = (FLUID_ONLY ? h.staged_fluid : h.staged) * 16u * (uint32_t)NV4 +
+                               (SLAB ? h.octets * (uint32_t)kTileOwners * 16u + (uint32_t)kTileOwners * 4u : 0u);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&st.bar)), "r"(bytes)
                      : "memory");
     }
     // the tile's list lengths and its entry octets (one contiguous run of
     // kTileOwners octets per slot group)
-    const int tb = blockDim.x - 1 - t;   // threads from the top of the block, clear of the range copies
+    const int tb = SLAB ? (int)blockDim.x - 1 - t : -1;   // threads from the top of the block, clear of the range copies
     if (tb == 0)
         asm volatile(
             "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                 smem_u32(slab.count)),
             "l"(T.count + first), "r"((uint32_t)kTileOwners * 4u), "r"(smem_u32(&st.bar))
             : "memory");
-    else if (tb <= (int)octets)
+    else if (tb > 0 && tb <= (int)h.octets)
         asm volatile(
             "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                 smem_u32(slab.ent + (tb - 1) * kTileOwners)),
             "l"(T.ent + (int64_t)(tb - 1) * T.stride + first), "r"((uint32_t)kTileOwners * 16u),
             "r"(smem_u32(&st.bar))
             : "memory");
-    if ((uint32_t)t < nr && !(FLUID_ONLY && (d->len_base[t] & kRangeBoundary))) {
-        const uint32_t a = d->start[t], lb = d->len_base[t];
-        const uint32_t len = lb & kRangeLen, base = lb >> 16;
+    if ((uint32_t)t < h.nranges && !(FLUID_ONLY && (rg.len_base & kRangeBoundary))) {
+        const uint32_t a = rg.start, len = rg.len_base & kRangeLen, base = rg.len_base >> 16;
 #pragma unroll
         for (int v = 0; v < NV4; v++) {
             asm volatile(
@@ -356,7 +380,8 @@ __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* 
         }
     }
     if (src1 != nullptr) {
-        for (uint32_t q = t >> 5; q < nr; q += blockDim.x / 32) {
+        const int lane = t & 31;
+        for (uint32_t q = t >> 5; q < h.nranges; q += blockDim.x / 32) {
             const uint32_t a = d->start[q], lb = d->len_base[q];
             if (FLUID_ONLY && (lb & kRangeBoundary)) continue;
             const uint32_t len = lb & kRangeLen, base = lb >> 16;
@@ -368,27 +393,69 @@ __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* 
     }
 }
 
-// Visits one half of local owner ol's entries (entries 4 half .. 4 half + 3
-// of every octet), staged in shared memory: f(byte offset into a staged
-// float4 array, boundary) for each, then flush() after every octet (where the
-// passes fold their partial sums into the compensated accumulators).
-template <bool FLUID_ONLY = false, typename F, typename Flush>
-__device__ __forceinline__ void for_tile_entries(const TileSlab& slab, int K, int ol, int half, F&& f, Flush&& flush) {
-    const uint32_t cnt = slab.count[ol];
+// Where a pass reads a tile's entries from: the staged slab in shared memory
+// or the octet planes in global memory. o: octet index of the owner's list.
+struct SlabEntries {
+    const uint4* e;   // slab.ent + local owner
+    __device__ __forceinline__ uint4 operator()(uint32_t o) const { return e[o * kTileOwners]; }
+};
+struct GlobalEntries {
+    const uint4* __restrict__ e;   // T.ent + owner
+    int64_t stride;
+    __device__ __forceinline__ uint4 operator()(uint32_t o) const { return __ldg(e + o * stride); }
+};
+
+// Visits one half of an owner's list (entries 4 half .. 4 half + 3 of every
+// octet; cnt: the owner's packed list length): f(byte offset into a staged
+// float4 array, boundary) for each, and flush() after every second octet and
+// at the end (where the passes fold their partial sums into the compensated
+// accumulators). The next octet is loaded while the current one is visited.
+// FLUID_ONLY visits the fluid entries, which come first in a list and have
+// the boundary bit clear.
+template <bool FLUID_ONLY = false, typename Src, typename F, typename Flush>
+__device__ __forceinline__ void for_tile_entries(const Src& src, uint32_t cnt, int K, int half, F&& f,
+                                                 Flush&& flush) {
     const uint32_t all = min(cnt & 0xffffu, (uint32_t)K);
     const uint32_t n = FLUID_ONLY ? min(cnt >> 16, all) : all;
-    for (uint32_t o = 0; o * 8 < n; o++) {
-        const uint4 cur = slab.ent[o * kTileOwners + ol];
+    auto visit = [&](uint32_t v) {
+        if (FLUID_ONLY) f(v, false);
+        else f(v & kEntOffset, (v & kEntBoundary) != 0u);
+    };
+    const uint32_t full = n / 8, octets = (n + 7) / 8;
+    uint4 next = octets ? src(0) : make_uint4(0u, 0u, 0u, 0u);
+    uint32_t o = 0;
+    for (; o < full; o++) {
+        const uint4 cur = next;
+        if (o + 1 < octets) next = src(o + 1);
         const uint32_t w0 = half ? cur.z : cur.x, w1 = half ? cur.w : cur.y;
-        const int m = (int)(n - o * 8) - 4 * half;
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            if (i < m) {
-                const uint32_t v = ((i < 2 ? w0 : w1) >> ((i & 1) * 16)) & 0xffffu;
-                f(v & kEntOffset, (v & kEntBoundary) != 0u);
-            }
-        }
-        flush();
+        visit(w0 & 0xffffu);
+        visit(w0 >> 16);
+        visit(w1 & 0xffffu);
+        visit(w1 >> 16);
+        if (o & 1u) flush();
+    }
+    const int m = (int)(n - full * 8) - 4 * half;   // this half's entries of the last, partial octet
+    if (m > 0) {
+        const uint32_t w0 = half ? next.z : next.x, w1 = half ? next.w : next.y;
+        visit(w0 & 0xffffu);
+        if (m > 1) visit(w0 >> 16);
+        if (m > 2) visit(w1 & 0xffffu);
+        if (m > 3) visit(w1 >> 16);
+    }
+    flush();
+}
+
+// Walks one half of owner k's list (threadIdx.x / 2 within its tile) from
+// the global octet planes (GLOBAL; cnt: the owner's packed list length,
+// loaded by the caller) or from the staged slab.
+template <bool GLOBAL, bool FLUID_ONLY, typename F, typename Flush>
+__device__ __forceinline__ void walk_tile_list(const TileLists& T, const TileSlab& slab, int64_t k, uint32_t cnt,
+                                               int half, F&& f, Flush&& flush) {
+    if constexpr (GLOBAL) {
+        for_tile_entries<FLUID_ONLY>(GlobalEntries{T.ent + k, T.stride}, cnt, T.K, half, f, flush);
+    } else {
+        const int ol = (int)(threadIdx.x >> 1);
+        for_tile_entries<FLUID_ONLY>(SlabEntries{slab.ent + ol}, slab.count[ol], T.K, half, f, flush);
     }
 }
 
@@ -429,21 +496,23 @@ __device__ __forceinline__ V3<float> fma3(float s, V3<float> d, V3<float> acc) {
 //                    f = -3 alpha h (2 - q)^2 / |d|   1 <= q <= 2
 // (for q < 1 that is alpha h (-3 (2 - q)^2 + 12 (1 - q)^2) / |d| with
 // |d| = q h). One rsqrt per pair, no divisions, no branches. The self pair
-// (d = 0) gets the finite f = -12 alpha and so a zero gradient, as the
-// reference's |d| <= FLT_EPSILON test gives.
+// (d = 0; the rsqrt takes max(r2, 1e-30), so q = 0) gets the finite
+// f = -12 alpha and so a zero gradient, as the reference's |d| <= FLT_EPSILON
+// test gives.
 struct FastSpline {
+    static constexpr float kTiny = 1e-30f;   // r2 floor of the rsqrt: the self pair gets q = 0
     float a, inv_h, a9, a12, a3h;
     __device__ explicit FastSpline(const SplineKernel<float>& k)
         : a(k.alpha), inv_h(1.f / k.h), a9(9.f * k.alpha), a12(12.f * k.alpha), a3h(3.f * k.alpha * k.h) {}
     __device__ __forceinline__ float grad(float r2) const {
-        const float inv = rsqrtf(r2);
-        const float q = (r2 > 0.f ? r2 * inv : 0.f) * inv_h;
+        const float inv = rsqrtf(fmaxf(r2, kTiny));
+        const float q = (r2 * inv) * inv_h;
         const float t = fmaxf(2.f - q, 0.f);
         return q < 1.f ? __fmaf_rn(a9, q, -a12) : -a3h * (t * t) * inv;
     }
     __device__ __forceinline__ void value_grad(float r2, float& w, float& f) const {
-        const float inv = rsqrtf(r2);
-        const float q = (r2 > 0.f ? r2 * inv : 0.f) * inv_h;
+        const float inv = rsqrtf(fmaxf(r2, kTiny));
+        const float q = (r2 * inv) * inv_h;
         const float t = fmaxf(2.f - q, 0.f);
         const bool inner = q < 1.f;
         f = inner ? __fmaf_rn(a9, q, -a12) : -a3h * (t * t) * inv;
@@ -461,23 +530,27 @@ struct FastSpline {
 // first loop. Blocks [0, n_tiles) are tiles of fluid owners; the blocks after
 // them take the boundary and inactive particles [n_fluid, n), which need no
 // neighbor sums.
-__global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l1(int64_t n_fluid, int64_t n, int64_t n_tiles,
+__global__ void __launch_bounds__(kPassThreads, kL1GlobalEntries ? 4 : 3) k_tile_iisph3d_l1(int64_t n_fluid, int64_t n, int64_t n_tiles,
                                                                   State<float> s, TileLists T, Lists L,
                                                                   SolverConsts<float> c,
                                                                   const StepScalars* __restrict__ sc,
                                                                   int* __restrict__ status) {
     extern __shared__ float4 tile_smem[];
-    if (*status) return;
     if (blockIdx.x >= n_tiles) {
+        if (*status) return;
         const int64_t k = n_fluid + (blockIdx.x - n_tiles) * (int64_t)kPassThreads + threadIdx.x;
         if (k < n) iisph3d_l1_one<float, true, false>(k, s, L, c, sc[s.scene_of(k)].dt);
         return;
     }
     const int half = threadIdx.x & 1;
     const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
+    // the status word and the tile's header and ranges, loaded together
     const TileDesc* d = T.desc + blockIdx.x;
-    const uint32_t nr = d->nranges;
-    if (nr == kTileFallback) {
+    const int err = *status;
+    const TileHead h = load_head(d);
+    const TileRange rg = load_range(d, threadIdx.x);
+    if (__syncthreads_or(err)) return;   // one decision for the whole block
+    if (h.nranges == kTileFallback) {
         if (k < n_fluid && !half) iisph3d_l1_one<float, true, false>(k, s, L, c, sc[s.scene_of(k)].dt);
         return;
     }
@@ -488,12 +561,13 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l1(int64_t n_f
     const float4* src4[2] = {s.pos, s.vel};
     float4* dst4[2] = {sp, sv};
     const TileSlab slab = slab_at(tile_smem, 36, T.K);
-    stage_tile_async<2, float>(stg, d, nr, src4, dst4, s.rho_prev, sr, T, slab);
+    stage_tile_async<2, false, !kL1GlobalEntries>(stg, d, h, rg, src4, dst4, s.rho_prev, sr, T, slab);
     // owners past n_fluid (last tile) walk no entries but take part in the shuffles
     const bool valid = k < n_fluid;
     const int64_t kk = valid ? k : 0;
     const float4 pk = s.pos[kk], vk = s.vel[kk], ek = s.ext[kk];
     const float dt = sc[s.scene_of(kk)].dt;
+    const uint32_t cnt = kL1GlobalEntries ? T.count[kk] : 0u;
     if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     Acc3<float, true> visc;
@@ -501,7 +575,7 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l1(int64_t n_f
     V3<float> vpart = v3<float>(0.f, 0.f, 0.f);
     float rpart = 0.f;
     const float gb = c.single_layer ? c.gamma1 : 1.f;
-    if (valid) for_tile_entries(slab, T.K, (int)(threadIdx.x >> 1), half, [&](uint32_t off, bool bnd) {
+    if (valid) walk_tile_list<kL1GlobalEntries, false>(T, slab, k, cnt, half, [&](uint32_t off, bool bnd) {
         const float4 pj = at_offset(sp, off), vj = at_offset(sv, off);
         const float rj = at_offset(sr, off >> 2);
         const V3<float> xij = sub3(pk, pj);
@@ -534,22 +608,24 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l1(int64_t n_f
 // second loop: source term and diagonal element (single-pass a_ii), then
 // the first pressure iteration, which needs no neighbor sums
 // (iisph3d_first_iteration), with its part of the convergence scan
-__global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l2(int64_t n_fluid, State<float> s, TileLists T,
+__global__ void __launch_bounds__(kPassThreads, kL2GlobalEntries ? 4 : 3) k_tile_iisph3d_l2(int64_t n_fluid, State<float> s, TileLists T,
                                                                   Lists L, SolverConsts<float> c,
                                                                   StepScalars* __restrict__ sc,
                                                                   int* __restrict__ status) {
     extern __shared__ float4 tile_smem[];
-    if (*status) return;
     const int half = threadIdx.x & 1;
     const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
     const bool valid = k < n_fluid;
     const int64_t kk = valid ? k : 0;
-    const int scene = s.scene_of(kk);
-    const float dt = sc[scene].dt;
     const TileDesc* d = T.desc + blockIdx.x;
-    const uint32_t nr = d->nranges;
+    const int err = *status;
+    const TileHead h = load_head(d);
+    const TileRange rg = load_range(d, threadIdx.x);
+    const int scene = s.scene_of(kk);
+    if (__syncthreads_or(err)) return;   // one decision for the whole block
+    const float dt = sc[scene].dt;
     ErrPart o;
-    if (nr == kTileFallback) {
+    if (h.nranges == kTileFallback) {
         if (valid && !half) {
             iisph3d_l2_one<float, true, false>(k, s, L, c, dt);
             o = iisph3d_first_iteration<float>(k, s, c, dt, s.vstar[k], s.anp[k].w);
@@ -563,9 +639,10 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l2(int64_t n_f
     const float4* src4[2] = {s.pos, s.vstar};
     float4* dst4[2] = {sp, sa};
     const TileSlab slab = slab_at(tile_smem, 32, T.K);
-    stage_tile_async<2, float>(stg, d, nr, src4, dst4, (const float*)nullptr, (float*)nullptr, T, slab);
+    stage_tile_async<2, false, !kL2GlobalEntries>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
     const float4 pk = s.pos[kk], vsk = s.vstar[kk];
     const float rk = s.rho[kk];
+    const uint32_t cnt = kL2GlobalEntries ? T.count[kk] : 0u;
     if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     Acc<float, true> contrib, mg2;
@@ -573,7 +650,7 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l2(int64_t n_f
     float cpart = 0.f, g2part = 0.f;
     V3<float> ipart = v3<float>(0.f, 0.f, 0.f), mpart = v3<float>(0.f, 0.f, 0.f), bpart = v3<float>(0.f, 0.f, 0.f);
     const float wb = c.single_layer ? c.two_gamma : 2.f;
-    if (valid) for_tile_entries(slab, T.K, (int)(threadIdx.x >> 1), half, [&](uint32_t off, bool bnd) {
+    if (valid) walk_tile_list<kL2GlobalEntries, false>(T, slab, k, cnt, half, [&](uint32_t off, bool bnd) {
         const float4 pj = at_offset(sp, off), vsj = at_offset(sa, off);
         const V3<float> xij = sub3(pk, pj);
         const float r2 = r2_of(xij);
@@ -609,22 +686,23 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_l2(int64_t n_f
 }
 
 // iteration (a): pressure acceleration
-__global__ void __launch_bounds__(kPassThreads, 4) k_tile_iisph3d_pressure_acc(int64_t n_fluid, State<float> s,
+__global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) k_tile_iisph3d_pressure_acc(int64_t n_fluid, State<float> s,
                                                                             TileLists T, Lists L,
                                                                             SolverConsts<float> c,
                                                                             const StepScalars* __restrict__ sc,
                                                                             int* __restrict__ status) {
     extern __shared__ float4 tile_smem[];
-    if (*status) return;
     const int half = threadIdx.x & 1;
     const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
+    const TileDesc* d = T.desc + blockIdx.x;
+    const int err = *status;
+    const TileHead h = load_head(d);
+    const TileRange rg = load_range(d, threadIdx.x);
     // owners of scenes whose loop has ended take no part; a tile without
     // iterating owners ends at once
     const bool live = k < n_fluid && !sc[s.scene_of(k)].done;
-    if (!__syncthreads_or(live)) return;
-    const TileDesc* d = T.desc + blockIdx.x;
-    const uint32_t nr = d->nranges;
-    if (nr == kTileFallback) {
+    if (__syncthreads_or(err) || !__syncthreads_or(live)) return;
+    if (h.nranges == kTileFallback) {
         if (live && !half) iisph3d_pressure_acc_one<float, true>(k, s, L, c);
         return;
     }
@@ -636,24 +714,27 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_tile_iisph3d_pressure_acc(i
     const TileSlab slab = slab_at(tile_smem, 20, T.K);
     // boundary neighbors enter through sum_bnd m_j gradW (second loop), so
     // only the fluid candidates and entries are visited
-    stage_tile_async<1, float, true>(stg, d, nr, src4, dst4, s.p, sa, T, slab);
+    stage_tile_async<1, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, s.p, sa, T, slab);
     const bool valid = live;
     const int64_t kk = valid ? k : 0;
     const float4 pk = s.pos[kk], gbk = s.gbnd[kk];
     const float prk = s.p[kk];
+    const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
     if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     Acc3<float, true> pa;
     V3<float> part = v3<float>(0.f, 0.f, 0.f);
-    if (valid) for_tile_entries<true>(slab, T.K, (int)(threadIdx.x >> 1), half, [&](uint32_t off, bool) {
+    auto pair = [&](uint32_t off, bool) {
         const float4 pj = at_offset(sp, off);
         const V3<float> xij = sub3(pk, pj);
         const float coef = pj.w * (prk + at_offset(sa, off >> 2)) * S.grad(r2_of(xij));
         part = fma3(-coef, xij, part);
-    }, [&] {
+    };
+    auto flush = [&] {
         pa.add(part);
         part = v3<float>(0.f, 0.f, 0.f);
-    });
+    };
+    if (valid) walk_tile_list<kPressureGlobalEntries, true>(T, slab, k, cnt, half, pair, flush);
     const V3<float> a = pair_total(pa);
     if (half || !valid) return;
     // boundary: - sum_bnd (lambda m_j p_i / rho0^2) gradW, lambda = 2 gamma (single layer) or 2
@@ -662,25 +743,26 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_tile_iisph3d_pressure_acc(i
 }
 
 // iteration (b): A p, relaxed Jacobi update, density error, fused scan
-__global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_pressure_update(int64_t n_fluid, State<float> s,
+__global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) k_tile_iisph3d_pressure_update(int64_t n_fluid, State<float> s,
                                                                                TileLists T, Lists L,
                                                                                SolverConsts<float> c,
                                                                                StepScalars* __restrict__ sc,
                                                                                int* __restrict__ status) {
     extern __shared__ float4 tile_smem[];
-    if (*status) return;
     const int half = threadIdx.x & 1;
     const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
     const int64_t kk = k < n_fluid ? k : 0;
+    const TileDesc* d = T.desc + blockIdx.x;
+    const int err = *status;
+    const TileHead h = load_head(d);
+    const TileRange rg = load_range(d, threadIdx.x);
     const int scene = s.scene_of(kk);
     const StepScalars* q = sc + scene;
     const bool live = k < n_fluid && !q->done;
-    if (!__syncthreads_or(live)) return;
+    if (__syncthreads_or(err) || !__syncthreads_or(live)) return;
     const float dt = q->dt;
-    const TileDesc* d = T.desc + blockIdx.x;
-    const uint32_t nr = d->nranges;
     ErrPart o;
-    if (nr == kTileFallback) {
+    if (h.nranges == kTileFallback) {
         if (live && !half) o = iisph3d_pressure_update_one<float, true>(k, s, L, c, dt);
     } else {
         float4* sp = tile_smem;
@@ -690,23 +772,26 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_pressure_updat
         float4* dst4[2] = {sp, sa};
         const TileSlab slab = slab_at(tile_smem, 32, T.K);
         // boundary neighbors enter through sum_bnd m_j gradW (second loop)
-        stage_tile_async<2, float, true>(stg, d, nr, src4, dst4, (const float*)nullptr, (float*)nullptr, T, slab);
+        stage_tile_async<2, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
         // the owner's own data, loaded while the staging lands
         const bool valid = live;
         const float4 pk = s.pos[kk], ak = s.acc[kk], vsk = s.vstar[kk], gbk = s.gbnd[kk];
         const float aii = s.anp[kk].w, prk = s.p[kk];
+        const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
         if (stage_tile_wait(stg, status)) {
             const FastSpline S(c.kern);
             Acc<float, true> ap;
             float part = 0.f;
-            if (valid) for_tile_entries<true>(slab, T.K, (int)(threadIdx.x >> 1), half, [&](uint32_t off, bool) {
+            auto pair = [&](uint32_t off, bool) {
                 const float4 pj = at_offset(sp, off);
                 const V3<float> xij = sub3(pk, pj);
                 part = __fmaf_rn(pj.w * S.grad(r2_of(xij)), dot3(sub3(ak, at_offset(sa, off)), xij), part);
-            }, [&] {
+            };
+            auto flush = [&] {
                 ap.add(part);
                 part = 0.f;
-            });
+            };
+            if (valid) walk_tile_list<kPressureGlobalEntries, true>(T, slab, k, cnt, half, pair, flush);
             // boundary: sum_bnd m_j dot(a_i, gradW) = dot(a_i, sum_bnd m_j gradW)
             const float sum = pair_total(ap) + dot3(v3<float>(ak.x, ak.y, ak.z), v3<float>(gbk.x, gbk.y, gbk.z));
             if (!half && valid)
@@ -718,16 +803,16 @@ __global__ void __launch_bounds__(kPassThreads, 3) k_tile_iisph3d_pressure_updat
 
 inline cudaError_t set_tile_pass_smem(int K) {
     cudaError_t e = cudaFuncSetAttribute(k_tile_iisph3d_l1, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)tile_pass_smem(36, K));
+                                         (int)tile_pass_smem(36, K, !kL1GlobalEntries));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_tile_iisph3d_l2, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tile_pass_smem(32, K));
+                                 (int)tile_pass_smem(32, K, !kL2GlobalEntries));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_acc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tile_pass_smem(20, K));
+                                 (int)tile_pass_smem(20, K, !kPressureGlobalEntries));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tile_pass_smem(32, K));
+                                 (int)tile_pass_smem(32, K, !kPressureGlobalEntries));
     return e;
 }
 
