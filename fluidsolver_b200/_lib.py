@@ -53,7 +53,7 @@ EXPORTED_SYMBOLS = (
     "fs_abi_version", "fs_last_error", "fs_params_default", "fs_create", "fs_destroy", "fs_set_params",
     "fs_upload", "fs_download", "fs_find_neighbors", "fs_get_neighbors_csr", "fs_query_position", "fs_solve_step", "fs_step",
     "fs_run", "fs_last_phase_times", "fs_stream", "fs_launch_count", "fs_batch_create", "fs_batch_run",
-    "fs_query_position_noalloc",
+    "fs_query_position_noalloc", "fs_get_solver_lists_csr",
 )
 
 
@@ -121,6 +121,7 @@ def lib() -> ctypes.CDLL:
     L.fs_download.argtypes = [ctx_p, POINTER(FsParticles)]
     L.fs_find_neighbors.argtypes = [ctx_p]
     L.fs_get_neighbors_csr.argtypes = [ctx_p, c_void_p, c_void_p, POINTER(c_int64)]
+    L.fs_get_solver_lists_csr.argtypes = [ctx_p, c_void_p, c_void_p, POINTER(c_int64)]
     L.fs_query_position.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
     L.fs_query_position_noalloc.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
     L.fs_step.argtypes = [ctx_p, c_float, POINTER(FsStepStats)]
@@ -135,7 +136,7 @@ def lib() -> ctypes.CDLL:
     L.fs_batch_run.argtypes = [ctx_p, c_int32, c_float, c_void_p]
     for name in ("fs_create", "fs_destroy", "fs_set_params", "fs_upload", "fs_download", "fs_find_neighbors",
                  "fs_get_neighbors_csr", "fs_query_position", "fs_solve_step", "fs_step", "fs_run", "fs_last_phase_times",
-                 "fs_batch_create", "fs_batch_run", "fs_query_position_noalloc"):
+                 "fs_batch_create", "fs_batch_run", "fs_query_position_noalloc", "fs_get_solver_lists_csr"):
         getattr(L, name).restype = c_int32
     _lib = L
     return L

@@ -1492,6 +1492,103 @@ fs_status fs_get_neighbors_csr(fs_ctx* c, int64_t* offsets, int64_t* indices, in
     return over ? FS_ERR_CAPACITY : FS_OK;
 }
 
+fs_status fs_get_solver_lists_csr(fs_ctx* c, int64_t* offsets, int64_t* indices, int64_t* total) {
+    if (!c || !offsets) return fail(FS_ERR_INVALID, "null argument");
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    if (!c->have_lists) return fail(FS_ERR_STATE, "no solver lists: execute the neighborhood search first");
+    FS_CUDA(cudaSetDevice(c->device));
+    const int64_t n = c->n, no = c->n_owners;
+    cudaStream_t st = c->stream;
+    const bool tiled = tiled_mode(c) && no > 0;
+    std::vector<uint32_t> counts((size_t)std::max<int64_t>(no, 1), 0);
+    std::vector<int64_t> off_sorted((size_t)no + 1, 0);
+    uint32_t* d_counts = nullptr;
+    int64_t* d_off = nullptr;
+    uint32_t* d_idx = nullptr;
+    auto release = [&] {
+        if (d_counts) cudaFree(d_counts);
+        if (d_off) cudaFree(d_off);
+        if (d_idx) cudaFree(d_idx);
+    };
+    if (no > 0) {
+        if (dalloc(&d_counts, (size_t)no) != FS_OK || dalloc(&d_off, (size_t)no + 1) != FS_OK) {
+            release();
+            return fail(FS_ERR_CUDA, "allocation for the list export failed");
+        }
+        c->launches++;
+        k_export_solver_lists<<<grid_for(no), kBlock, 0, st>>>(no, tiled, tile_lists_of(c), lists_of(c), nullptr,
+                                                               d_counts, nullptr);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(counts.data(), d_counts, sizeof(uint32_t) * no, cudaMemcpyDeviceToHost, st) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            release();
+            return fail(FS_ERR_CUDA, "list export failed");
+        }
+        for (int64_t k = 0; k < no; k++) off_sorted[k + 1] = off_sorted[k] + counts[k];
+    }
+    std::vector<uint32_t> hidx((size_t)std::max<int64_t>(n, 1));
+    if (n > 0 && cudaMemcpy(hidx.data(), c->hidx[c->cur], sizeof(uint32_t) * n, cudaMemcpyDeviceToHost) !=
+                     cudaSuccess) {
+        release();
+        return fail(FS_ERR_CUDA, "list export failed");
+    }
+    std::vector<int64_t> cnt_host((size_t)n + 1, 0);
+    for (int64_t k = 0; k < no; k++) cnt_host[hidx[k]] = counts[k];
+    offsets[0] = 0;
+    for (int64_t h = 0; h < n; h++) offsets[h + 1] = offsets[h] + cnt_host[h];
+    const int64_t tot = off_sorted[no];
+    if (total) *total = tot;
+    if (!indices || tot == 0) {
+        release();
+        return FS_OK;
+    }
+    std::vector<uint32_t> idx((size_t)tot);
+    if (dalloc(&d_idx, (size_t)tot) != FS_OK ||
+        cudaMemcpyAsync(d_off, off_sorted.data(), sizeof(int64_t) * (no + 1), cudaMemcpyHostToDevice, st) !=
+            cudaSuccess) {
+        release();
+        return fail(FS_ERR_CUDA, "list export failed");
+    }
+    c->launches++;
+    k_export_solver_lists<<<grid_for(no), kBlock, 0, st>>>(no, tiled, tile_lists_of(c), lists_of(c), d_off, nullptr,
+                                                           d_idx);
+    const bool ok = cudaGetLastError() == cudaSuccess &&
+                    cudaMemcpyAsync(idx.data(), d_idx, sizeof(uint32_t) * tot, cudaMemcpyDeviceToHost, st) ==
+                        cudaSuccess &&
+                    cudaStreamSynchronize(st) == cudaSuccess;
+    release();
+    if (!ok) return fail(FS_ERR_CUDA, "list export failed");
+    for (int64_t k = 0; k < no; k++) {
+        const int64_t h = hidx[k];
+        int64_t o = offsets[h];
+        for (int64_t q = off_sorted[k]; q < off_sorted[k + 1]; q++) {
+            if (idx[q] >= (uint32_t)n) {
+                // report the entry and its tile's ranges
+                std::string msg = "solver list entry " + std::to_string(q - off_sorted[k]) + " of sorted owner " +
+                                  std::to_string(k) + " (of " + std::to_string(counts[k]) + ") maps to no particle";
+                if (tiled && (idx[q] >> 28) == 0xfu) {
+                    TileDesc dd;
+                    if (cudaMemcpy(&dd, c->tile_desc + k / kTileOwners, sizeof(dd), cudaMemcpyDeviceToHost) ==
+                        cudaSuccess) {
+                        msg += ": slot " + std::to_string(idx[q] & 0xffffu) + ", tile " +
+                               std::to_string(k / kTileOwners) + " with " + std::to_string(dd.h.nranges) +
+                               " ranges, " + std::to_string(dd.h.staged) + " staged:";
+                        for (uint32_t r = 0; r < dd.h.nranges && r < (uint32_t)kTileRanges; r++)
+                            msg += " [" + std::to_string(dd.start[r]) + "+" +
+                                   std::to_string(dd.len_base[r] & kRangeLen) + "@" +
+                                   std::to_string(dd.len_base[r] >> 16) + "]";
+                    }
+                }
+                return fail(FS_ERR_CUDA, msg);
+            }
+            indices[o++] = hidx[idx[q]];
+        }
+        std::sort(indices + offsets[h], indices + offsets[h + 1]);
+    }
+    return FS_OK;
+}
+
 fs_status fs_query_position(fs_ctx* c, const float* position, int64_t* out, int64_t cap, int64_t* count) {
     if (!c || !position) return fail(FS_ERR_INVALID, "null argument");
     if (cap > 0 && !out) return fail(FS_ERR_INVALID, "out is null");

@@ -151,8 +151,14 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     // its scene's grid, and its first and last x
     __shared__ long long s_grow[kTileGroups];
     __shared__ int s_gd0[kTileGroups], s_gd01[kTileGroups], s_gx0[kTileGroups], s_gx1[kTileGroups];
+    // s_base: first staged slot | (position among the non-empty ranges << 16)
     __shared__ uint32_t s_start[kTileRanges], s_len[kTileRanges], s_base[kTileRanges];
     __shared__ uint32_t s_total;
+    // per-warp partial results, in arrays whose contents are dead by then
+    // (static shared memory decides whether 5 blocks fit on an SM)
+    uint32_t* s_wlen = s_cnt;                                     // warp sums of the range scan
+    uint32_t* s_wne = s_cnt + kTileOwners / 32;
+    uint32_t* s_wmax = reinterpret_cast<uint32_t*>(s_lead);       // warp maxima of the list lengths
     if (*status) return;   // an earlier error (e.g. non-finite positions) ends the step
 
     const int t = threadIdx.x, lane = t & 31;
@@ -201,25 +207,47 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
         if (valid && (t == kTileOwners - 1 || s_key[t + 1] != key)) s_gx1[g] = lx;
         __syncthreads();
         NR = 18 * G;
+        uint32_t len = 0;
         if (t < NR) {
             const int region = t / (9 * G), gg = (t % (9 * G)) / 9, r = t % 9;
             const int64_t rb = s_grow[gg] + (int64_t)(r / 3 - 1) * s_gd01[gg] + (int64_t)(r % 3 - 1) * s_gd0[gg];
             const uint32_t* cs = cell_start + region * (w.cells + 1);
             const uint32_t a = cs[rb + s_gx0[gg] - 1], b = cs[rb + s_gx1[gg] + 2];
+            len = b - a;
             s_start[t] = a;
-            s_len[t] = b - a;
+            s_len[t] = len;
         }
-        __syncthreads();
-        if (t == 0) {
-            uint32_t tot = 0;
-            for (int q = 0; q < NR; q++) {
-                s_base[q] = tot;
-                tot += s_len[q];
+        // exclusive prefix sums over the ranges (thread t: range t) of their
+        // lengths -- first staged slots -- and of their non-emptiness --
+        // positions in the descriptor --, by warp scans
+        uint32_t incl = len, ne = len ? 1u : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t a = __shfl_up_sync(0xffffffffu, incl, o), b = __shfl_up_sync(0xffffffffu, ne, o);
+            if (lane >= o) {
+                incl += a;
+                ne += b;
             }
-            s_total = tot;
+        }
+        if (lane == 31) {
+            s_wlen[t >> 5] = incl;
+            s_wne[t >> 5] = ne;
         }
         __syncthreads();
-        fallback = s_total > (uint32_t)kTileCap;
+        uint32_t before = 0, before_ne = 0, tot = 0;
+#pragma unroll
+        for (int i = 0; i < kTileOwners / 32; i++) {
+            if (i < (t >> 5)) {
+                before += s_wlen[i];
+                before_ne += s_wne[i];
+            }
+            tot += s_wlen[i];
+        }
+        // (every thread has read the warp sums before s_cnt is reused)
+        if (t < NR) s_base[t] = (before + incl - len) | ((before_ne + ne - (len ? 1u : 0u)) << 16);
+        fallback = tot > (uint32_t)kTileCap;
+        if (t == 0) s_total = tot;
+        __syncthreads();
     }
 
     if (fallback) {
@@ -248,7 +276,7 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     if (t < NR && s_len[t])
         asm volatile(
             "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                smem_u32(sp + s_base[t])),
+                smem_u32(sp + (s_base[t] & 0xffffu))),
             "l"(pos + s_start[t]), "r"(s_len[t] * 16u), "r"(smem_u32(&stg.bar))
             : "memory");
     if (!stage_tile_wait(stg, status)) return;
@@ -278,7 +306,7 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
         for (int q = 0; q < 18; q++) {
             if (q == 9) cf = c;
             const int qq = ((q / 9) * G + g) * 9 + q % 9;
-            const uint32_t off = s_base[qq] - s_start[qq];
+            const uint32_t off = (s_base[qq] & 0xffffu) - s_start[qq];
             const uint32_t flag = q >= 9 ? kEntBoundary : 0u;
             uint32_t i = lo[q] + off;
             const uint32_t e = hi[q] + off;
@@ -293,20 +321,25 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     }
     s_cnt[t] = c;
     note_list_length(c, K, status, sc);
+    const uint32_t wmax = __reduce_max_sync(0xffffffffu, c);
+    if (lane == 0) s_wmax[t >> 5] = wmax;
+    // the descriptor: the non-empty ranges in order (thread t: range t), then
+    // the header
+    if (t < NR && s_len[t]) {
+        const uint32_t slot = s_base[t] >> 16;
+        desc[tile].start[slot] = s_start[t];
+        desc[tile].len_base[slot] = s_len[t] | (t >= 9 * G ? kRangeBoundary : 0u) | (s_base[t] << 16);
+    }
     __syncthreads();
     if (t == 0) {
         uint32_t mx = 0;
-        for (int i = 0; i < kTileOwners; i++) mx = max(mx, s_cnt[i]);
-        uint32_t m = 0, fl = 0;
-        for (int q = 0; q < NR; q++) {
-            if (!s_len[q]) continue;
-            const bool bnd = q >= 9 * G;
-            desc[tile].start[m] = s_start[q];
-            desc[tile].len_base[m] = s_len[q] | (bnd ? kRangeBoundary : 0u) | (s_base[q] << 16);
-            if (!bnd) fl += s_len[q];
-            m++;
-        }
-        *reinterpret_cast<uint4*>(desc + tile) = make_uint4(m, s_total, fl, (min(mx, (uint32_t)K) + 7) / 8);
+#pragma unroll
+        for (int i = 0; i < kTileOwners / 32; i++) mx = max(mx, s_wmax[i]);
+        const uint32_t last = NR - 1;
+        const uint32_t nonempty = (s_base[last] >> 16) + (s_len[last] ? 1u : 0u);
+        // fluid ranges come first: the first boundary range's slot is their total
+        *reinterpret_cast<uint4*>(desc + tile) =
+            make_uint4(nonempty, s_total, s_base[9 * G] & 0xffffu, (min(mx, (uint32_t)K) + 7) / 8);
     }
     // octets of entries, coalesced across the tile's owners
     const int O = K / 8;
@@ -799,6 +832,41 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
         }
     }
     reduce_err_parts(o, sc, scene);
+}
+
+// Export of the lists that the solver passes walk, as sorted indices: owner
+// k's list length (out == nullptr) or its entries from out[offsets[k]]. A
+// tile list entry is a staged slot, which the tile's ranges map back to a
+// sorted index; fallback tiles and untiled contexts hold slot-major 32-bit
+// lists (sorted index | kBoundaryBit).
+__global__ void k_export_solver_lists(int64_t n_owners, bool tiled, TileLists T, Lists L,
+                                      const int64_t* __restrict__ offsets, uint32_t* __restrict__ counts,
+                                      uint32_t* __restrict__ out) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n_owners) return;
+    const TileDesc* d = T.desc + k / kTileOwners;
+    const bool tile_list = tiled && d->h.nranges != kTileFallback;
+    const uint32_t n = tile_list ? min(T.count[k] & 0xffffu, (uint32_t)T.K) : min(L.count[k], (uint32_t)L.K);
+    if (out == nullptr) {
+        counts[k] = n;
+        return;
+    }
+    uint32_t* o = out + offsets[k];
+    for (uint32_t q = 0; q < n; q++) {
+        if (!tile_list) {
+            o[q] = L.nbr[(int64_t)q * L.stride + k] & kIndexMask;   // without the boundary bit
+            continue;
+        }
+        const uint4 oc = T.ent[(int64_t)(q / 8) * T.stride + k];
+        const uint32_t wd = (q & 7) < 2 ? oc.x : (q & 7) < 4 ? oc.y : (q & 7) < 6 ? oc.z : oc.w;
+        const uint32_t slot = ((wd >> ((q & 1) * 16)) & kEntOffset) >> 4;
+        uint32_t idx = 0xf0000000u | slot;   // no range holds the slot: a broken list (the slot, for the report)
+        for (uint32_t r = 0; r < d->h.nranges; r++) {
+            const uint32_t lb = d->len_base[r], base = lb >> 16;
+            if (slot - base < (lb & kRangeLen)) idx = d->start[r] + (slot - base);
+        }
+        o[q] = idx;
+    }
 }
 
 inline cudaError_t set_tile_pass_smem(int K) {

@@ -304,6 +304,17 @@ class FluidSolverBase:
         F.check(F.lib().fs_get_neighbors_csr(self.ctx, off.ctypes.data, idx.ctypes.data, ctypes.byref(tot)))
         return off, idx[:tot.value]
 
+    def solver_lists(self) -> tuple[np.ndarray, np.ndarray]:
+        """CSR (offsets, indices) of the lists the solver's passes walk (3D IISPH fast mode: the tile
+        lists), host index space, each list ascending. They must equal neighbor_lists() for the owners."""
+        n = len(self.data.collection)
+        off = np.zeros(n + 1, np.int64)
+        tot = ctypes.c_int64()
+        F.check(F.lib().fs_get_solver_lists_csr(self.ctx, off.ctypes.data, None, ctypes.byref(tot)))
+        idx = np.zeros(max(tot.value, 1), np.int64)
+        F.check(F.lib().fs_get_solver_lists_csr(self.ctx, off.ctypes.data, idx.ctypes.data, ctypes.byref(tot)))
+        return off, idx[:tot.value]
+
     def get_neighbors(self, index: int) -> np.ndarray:
         off, idx = self.neighbor_lists()
         return idx[off[index]:off[index + 1]]

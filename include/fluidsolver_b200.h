@@ -195,6 +195,13 @@ fs_status fs_find_neighbors(fs_ctx* ctx);
 /* Neighbor lists of the last search in host-index space, each list ascending:
  * offsets has n+1 entries; indices may be NULL to query *total first. */
 fs_status fs_get_neighbors_csr(fs_ctx* ctx, int64_t* offsets, int64_t* indices, int64_t* total);
+/* The lists that the solver's passes walk (3D IISPH fast mode: the tile lists),
+ * exported like fs_get_neighbors_csr: host-index space, each list ascending,
+ * indices NULL to query *total first. No reference counterpart (the
+ * reference's solvers walk the search's own lists); it lets a caller check
+ * that the solver sees the contract's neighbor sets. Needs a search since the
+ * last upload. */
+fs_status fs_get_solver_lists_csr(fs_ctx* ctx, int64_t* offsets, int64_t* indices, int64_t* total);
 /* Neighbors of an arbitrary position (NeighborhoodInterface::get_neighbors(vec),
  * NeighborhoodInterface.cpp:71-80); ascending host indices, per contract:
  * hashed-3d walks the cells of the last search, skips inactive particles and,
