@@ -4,6 +4,8 @@ Python host mirror of libFluid's solver interfaces over that C-ABI."""
 from ._lib import FluidSolverError, lib  # noqa: F401
 from .solver import (  # noqa: F401
     BatchedIISPHFluidSolver3D,
+    ConstantTimestepGenerator,
+    DynamicCflTimestepGenerator,
     IISPHFluidSolver,
     IISPHFluidSolver3D,
     NeighborhoodSearch,

@@ -30,6 +30,9 @@ FS_SOLVER_SESPH_3D = 2
 FS_SOLVER_IISPH_2D = 3
 FS_SOLVER_IISPH_3D = 4
 
+FS_TIMESTEP_CONSTANT = 0
+FS_TIMESTEP_DYNAMIC_CFL = 1
+
 FS_SEARCH_QUADRATIC_2D = 0
 FS_SEARCH_HASHED_2D = 1
 FS_SEARCH_COMPACT_2D = 2
@@ -67,7 +70,8 @@ class FsParams(ctypes.Structure):
         ("max_density_error", c_float), ("min_iterations", c_int32), ("max_iterations", c_int32),
         ("omega", c_float), ("gamma", c_float),
         ("timestep", c_float), ("lambda_v", c_float), ("lambda_a", c_float),
-        ("max_particles", c_int64), ("neighbor_capacity", c_int32), ("reserved", c_int32),
+        ("max_particles", c_int64), ("neighbor_capacity", c_int32),
+        ("timestep_generator", c_int32), ("min_timestep", c_float), ("max_timestep", c_float),
     ]
 
 

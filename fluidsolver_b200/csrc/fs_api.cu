@@ -205,8 +205,14 @@ fs_status check_params(const fs_params* p) {
             return fail(FS_ERR_INVALID, "MaxDensityErrorAllowed is smaller or equal to zero.");
         if (p->min_iterations < 0) return fail(FS_ERR_INVALID, "min iterations must be >= 0");
     }
-    if (p->solver != FS_SOLVER_NONE && !(p->timestep > 0.0f))
-        return fail(FS_ERR_INVALID, "Timestep is smaller or equal to zero.");
+    if (p->timestep_generator != FS_TIMESTEP_CONSTANT && p->timestep_generator != FS_TIMESTEP_DYNAMIC_CFL)
+        return fail(FS_ERR_INVALID, "unknown time step generator");
+    if (p->timestep_generator == FS_TIMESTEP_CONSTANT) {
+        if (p->solver != FS_SOLVER_NONE && !(p->timestep > 0.0f))
+            return fail(FS_ERR_INVALID, "Timestep is smaller or equal to zero.");
+    } else if (!(p->min_timestep > 0.0f) || !(p->max_timestep >= p->min_timestep)) {
+        return fail(FS_ERR_INVALID, "the dynamic time step bounds need 0 < min_timestep <= max_timestep");
+    }
     if (p->max_particles <= 0 || p->max_particles > (int64_t)0x7fffffff)
         return fail(FS_ERR_INVALID, "max_particles must be in [1, 2^31)");
     return FS_OK;
@@ -746,6 +752,40 @@ __global__ void k_step_begin(StepScalars* sc, int scenes, float desired_dt, bool
     sc[i] = z;
 }
 
+bool dynamic_timestep(const fs_ctx* c) { return c->prm.timestep_generator == FS_TIMESTEP_DYNAMIC_CFL; }
+
+// the desired time step a step call starts from: the caller's (or the
+// constant generator's); with the dynamic generator a placeholder, which the
+// device replaces (a fixed value, so that one CUDA graph serves every step)
+float desired_of(const fs_ctx* c, float desired_dt) {
+    if (dynamic_timestep(c)) return c->prm.max_timestep;
+    return desired_dt > 0.0f ? desired_dt : c->prm.timestep;
+}
+
+// the default of get_non_cfl_validating_timestep: the constant generator's
+// time step or the dynamic generator's max_timestep
+float cfl_default(const fs_ctx* c) { return dynamic_timestep(c) ? c->prm.max_timestep : c->prm.timestep; }
+
+// Resets the step scalars before the solver phases; with the dynamic
+// generator also chooses the desired time step from the state on the device
+// (Simulator.cpp:18-25 runs the generator before the step).
+fs_status begin_solver_phases(fs_ctx* c, float dt, cudaStream_t st) {
+    c->launches++;
+    k_step_begin<<<grid_for(c->nsc(), 128), 128, 0, st>>>(c->scalars, c->nsc(), dt, true);
+    FS_CUDA(cudaGetLastError());
+    if (!dynamic_timestep(c)) return FS_OK;
+    const fs_params& p = c->prm;
+    c->launches += 2;
+    if (c->precision == FS_PRECISION_FP64)
+        k_generator_max<double><<<grid_for(c->n, 256), 256, 0, st>>>(c->n, state_of<double>(c), c->scalars, c->status);
+    else
+        k_generator_max<float><<<grid_for(c->n, 256), 256, 0, st>>>(c->n, state_of<float>(c), c->scalars, c->status);
+    k_generator_finish<<<grid_for(c->nsc(), 128), 128, 0, st>>>(c->scalars, c->nsc(), p.particle_size, p.min_timestep,
+                                                                 p.max_timestep, p.lambda_v, p.lambda_a);
+    FS_CUDA(cudaGetLastError());
+    return FS_OK;
+}
+
 // ---------------------------------------------------------------------------
 // solver steps
 // ---------------------------------------------------------------------------
@@ -855,8 +895,8 @@ fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
     }, true));
     FS_TRY(mark(c, 4, st));
     c->launches++;
-    k_cfl<<<1, 128, 0, st>>>(c->scalars, c->nsc(), c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
-                           c->status);
+    k_cfl<<<1, 128, 0, st>>>(c->scalars, c->nsc(), c->prm.particle_size, cfl_default(c), c->prm.lambda_v,
+                             c->prm.lambda_a, c->status);
     c->launches++;
     k_iisph3d_integrate<float><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
     FS_CUDA(cudaGetLastError());
@@ -905,8 +945,8 @@ template <typename R, bool KAHAN> fs_status step_iisph3d(fs_ctx* c, bool capture
     }));
     FS_TRY(mark(c, 4, st));
     c->launches++;
-    k_cfl<<<1, 128, 0, st>>>(c->scalars, c->nsc(), c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
-                           c->status);
+    k_cfl<<<1, 128, 0, st>>>(c->scalars, c->nsc(), c->prm.particle_size, cfl_default(c), c->prm.lambda_v,
+                             c->prm.lambda_a, c->status);
     c->launches++;
     k_iisph3d_integrate<R><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
     FS_CUDA(cudaGetLastError());
@@ -933,8 +973,8 @@ template <typename R, bool KAHAN> fs_status step_sesph(fs_ctx* c) {
     c->launches++;
         k_sesph_maxima_final<<<1, 1, 0, st>>>(c->scalars);
     c->launches++;
-        k_cfl<<<1, 128, 0, st>>>(c->scalars, c->nsc(), c->prm.particle_size, c->prm.timestep, c->prm.lambda_v, c->prm.lambda_a,
-                               c->status);
+        k_cfl<<<1, 128, 0, st>>>(c->scalars, c->nsc(), c->prm.particle_size, cfl_default(c), c->prm.lambda_v,
+                                 c->prm.lambda_a, c->status);
     }
     FS_TRY(mark(c, 4, st));
     c->launches++;
@@ -1093,8 +1133,7 @@ fs_status solve_graph(fs_ctx* c, float dt, bool with_search = false) {
         r = mark(c, 0, c->stream);
         if (r == FS_OK) r = search_dispatch(c, true);
     }
-    c->launches++;
-    k_step_begin<<<grid_for(c->nsc(), 128), 128, 0, c->stream>>>(c->scalars, c->nsc(), dt, true);
+    if (r == FS_OK) r = begin_solver_phases(c, dt, c->stream);
     if (r == FS_OK) r = step_dispatch_any(c, true);
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
@@ -1130,8 +1169,7 @@ fs_status solve_after_search(fs_ctx* c, float dt, fs_step_stats* stats) {
     if (graphs) {
         FS_TRY(solve_graph(c, dt));
     } else {
-        c->launches++;
-        k_step_begin<<<grid_for(c->nsc(), 128), 128, 0, c->stream>>>(c->scalars, c->nsc(), dt, true);
+        FS_TRY(begin_solver_phases(c, dt, c->stream));
         FS_TRY(step_dispatch_any(c, false));
     }
     c->have_lists = false;  // positions moved: the lists belong to the old positions
@@ -1166,7 +1204,7 @@ fs_status finish_steps(fs_ctx* c, fs_step_stats* stats, int* st) {
 fs_status one_step(fs_ctx* c, float desired_dt, fs_step_stats* stats) {
     if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
     if (c->prm.solver == FS_SOLVER_NONE) return fail(FS_ERR_INVALID, "context has no solver");
-    const float dt = desired_dt > 0.0f ? desired_dt : c->prm.timestep;
+    const float dt = desired_of(c, desired_dt);
     if (!(c->prm.flags & FS_FLAG_SYNC_EACH_ITERATION)) {
         FS_TRY(enqueue_steps(c, 1, dt));
         int st = 0;
@@ -1216,6 +1254,9 @@ void fs_params_default(fs_params* p, int32_t dim, int32_t solver, int32_t search
     p->timestep = 0.001f;        // ConstantTimestepGenerator.hpp:8-13
     p->lambda_v = 0.4f;
     p->lambda_a = 0.25f;
+    p->timestep_generator = FS_TIMESTEP_CONSTANT;
+    p->min_timestep = 0.0001f;   // DynamicCflTimestepGenerator.hpp:11-18
+    p->max_timestep = 0.02f;
     p->max_particles = 0;
     p->neighbor_capacity = 0;
     p->device = 0;
@@ -1395,7 +1436,7 @@ fs_status fs_solve_step(fs_ctx* c, float desired_dt, fs_step_stats* stats) {
     if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
     if (c->prm.solver == FS_SOLVER_NONE) return fail(FS_ERR_INVALID, "context has no solver");
     FS_CUDA(cudaSetDevice(c->device));
-    const float dt = desired_dt > 0.0f ? desired_dt : c->prm.timestep;
+    const float dt = desired_of(c, desired_dt);
     return solve_after_search(c, dt, stats);
 }
 
@@ -1673,7 +1714,7 @@ fs_status fs_run(fs_ctx* c, int32_t steps, float desired_dt, fs_step_stats* stat
     }
     // one step first: it settles the list capacity (and captures the graph)
     FS_TRY(one_step(c, desired_dt, stats));
-    const float dt = desired_dt > 0.0f ? desired_dt : c->prm.timestep;
+    const float dt = desired_of(c, desired_dt);
     FS_TRY(enqueue_steps(c, steps - 1, dt));
     int st = 0;
     FS_TRY(finish_steps(c, stats, &st));
@@ -1714,7 +1755,7 @@ fs_status fs_batch_run(fs_ctx* c, int32_t steps, float desired_dt, fs_step_stats
     if (steps == 0) return FS_OK;
     FS_TRY(one_step(c, desired_dt, nullptr));
     if (steps > 1) {
-        const float dt = desired_dt > 0.0f ? desired_dt : c->prm.timestep;
+        const float dt = desired_of(c, desired_dt);
         FS_TRY(enqueue_steps(c, steps - 1, dt));
         int st = 0;
         FS_TRY(finish_steps(c, nullptr, &st));

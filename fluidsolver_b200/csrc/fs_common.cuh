@@ -206,6 +206,8 @@ struct StepScalars {
     float final_max_v2;
     int max_neighbors;
     int loop_guard;          // executions of the pressure-loop body this step
+    unsigned int gen_v2_bits;   // dynamic time step generator: largest |v|^2, |a|^2 at the step's start
+    unsigned int gen_a2_bits;
 };
 
 }  // namespace fsb

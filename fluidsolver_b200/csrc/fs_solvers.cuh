@@ -569,6 +569,71 @@ __device__ __forceinline__ void cfl_one(StepScalars* __restrict__ sc, float part
     sc->dt = nt;
 }
 
+// ---------------------------------------------------------------------------
+// DynamicCflTimestepGenerator (DynamicCflTimestepGenerator.cpp:6-61) on the
+// device, so that the time step is chosen inside the step's CUDA graph.
+// k_generator_max: the largest |v|^2 and |a|^2 (float, ((x x + y y) + z z),
+// glm::length's dot) over the particles that are not inactive -- boundary
+// included, as the reference's loop over the whole collection -- per scene,
+// as ordered bits. max |v| = sqrt(max |v|^2) since sqrt is monotonic and
+// correctly rounded. k_generator_finish: the generator's clamp, per scene.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void k_generator_max(int64_t n, State<R> s, StepScalars* __restrict__ sc,
+                                const int* __restrict__ status) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    float v2 = 0.f, a2 = 0.f;
+    int scene = 0;
+    const bool active = k < n && s.type[k] != FS_TYPE_INACTIVE;
+    if (active) {
+        const V4<R> v = s.vel[k], a = s.acc[k];
+        const float vx = (float)v.x, vy = (float)v.y, vz = (float)v.z;
+        const float ax = (float)a.x, ay = (float)a.y, az = (float)a.z;
+        v2 = (vx * vx + vy * vy) + vz * vz;
+        a2 = (ax * ax + ay * ay) + az * az;
+        scene = s.scene_of(k);
+    }
+    // one atomic per warp and quantity where the warp's particles share a scene
+    const int s0 = __shfl_sync(0xffffffffu, scene, 0);
+    if (__all_sync(0xffffffffu, scene == s0)) {
+        v2 = warp_max(v2);
+        a2 = warp_max(a2);
+        if ((threadIdx.x & 31) == 0 && !*status) {
+            atomic_max_nonneg(&sc[s0].gen_v2_bits, v2);
+            atomic_max_nonneg(&sc[s0].gen_a2_bits, a2);
+        }
+    } else if (active) {
+        atomic_max_nonneg(&sc[scene].gen_v2_bits, v2);
+        atomic_max_nonneg(&sc[scene].gen_a2_bits, a2);
+    }
+}
+
+// DynamicCflTimestepGenerator::generate_next_timestep (:45-59) and its
+// get_non_cfl_validating_timestep (:82-107), whose default is max_timestep
+__device__ __forceinline__ float dynamic_cfl_timestep(float max_v, float max_a, float particle_size, float min_ts,
+                                                      float max_ts, float lambda_v, float lambda_a) {
+    float ts = min_ts;
+    if (max_v > kFltEps && max_a > kFltEps) {
+        float dta = max_ts, dtv = max_ts;
+        if (max_a > 0.0f) dta = (float)(sqrt((double)(particle_size / max_a)) * (double)lambda_a);
+        if (max_v > 0.0f) dtv = particle_size / max_v * lambda_v;
+        const float allowed = fmaxf(fminf(dta, dtv), 0.000001f);
+        ts = fmaxf(ts, fminf(max_ts, allowed));
+    }
+    return ts;
+}
+
+__global__ void k_generator_finish(StepScalars* __restrict__ sc, int scenes, float particle_size, float min_ts,
+                                   float max_ts, float lambda_v, float lambda_a) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < scenes; i += gridDim.x * blockDim.x) {
+        const float max_v = sqrtf(__uint_as_float(sc[i].gen_v2_bits));
+        const float max_a = sqrtf(__uint_as_float(sc[i].gen_a2_bits));
+        const float ts = dynamic_cfl_timestep(max_v, max_a, particle_size, min_ts, max_ts, lambda_v, lambda_a);
+        sc[i].desired_dt = ts;
+        sc[i].dt = ts;
+    }
+}
+
 // the clamp for scenes [0, scenes) (one in a single-scene context)
 __global__ void k_cfl(StepScalars* __restrict__ sc, int scenes, float particle_size, float timestep, float lambda_v,
                       float lambda_a, const int* __restrict__ status) {

@@ -262,6 +262,18 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
         return;
     }
 
+    // the owner's 18 row bounds (its 27 cells), loaded while the staging lands
+    uint32_t lo[18], hi[18];
+    if (valid) {
+#pragma unroll
+        for (int q = 0; q < 18; q++) {
+            const uint32_t* cs = cell_start + (q / 9) * (w.cells + 1);
+            const int64_t rb = key + (int64_t)((q % 9) / 3 - 1) * d01 + (int64_t)(q % 3 - 1) * d0;
+            lo[q] = cs[rb + lx - 1];
+            hi[q] = cs[rb + lx + 2];
+        }
+    }
+
     // stage the candidates' positions: a bulk copy per range (the TMA engine)
     __shared__ TileStage stg;
     if (t == 0) {
@@ -281,19 +293,10 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
             : "memory");
     if (!stage_tile_wait(stg, status)) return;
 
-    // each owner tests the candidates of its own 27 cells: the 18 row bounds
-    // are loaded up front, candidates are tested two at a time
+    // each owner tests the candidates of its own 27 cells, two at a time
     uint32_t c = 0;
     if (valid) {
         uint16_t* my = sent + t * KP;
-        uint32_t lo[18], hi[18];
-#pragma unroll
-        for (int q = 0; q < 18; q++) {
-            const uint32_t* cs = cell_start + (q / 9) * (w.cells + 1);
-            const int64_t rb = key + (int64_t)((q % 9) / 3 - 1) * d01 + (int64_t)(q % 3 - 1) * d0;
-            lo[q] = cs[rb + lx - 1];
-            hi[q] = cs[rb + lx + 2];
-        }
         auto test = [&](float4 pj, uint32_t entry) {
             const float d0 = pk.x - pj.x, d1 = pk.y - pj.y, d2 = pk.z - pj.z;
             if ((d0 * d0 + d1 * d1) + d2 * d2 <= w.r2) {

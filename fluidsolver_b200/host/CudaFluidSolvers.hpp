@@ -28,6 +28,7 @@
 #include "fluidSolver/solver/settings/SESPHSettings.hpp"
 #include "fluidSolver/solver/settings/SESPHSettings3D.hpp"
 #include "time/ConstantTimestepGenerator.hpp"
+#include "time/DynamicCflTimestepGenerator.hpp"
 
 #include "fluidsolver_b200.h"
 
@@ -152,6 +153,7 @@ namespace LibFluid {
             void execute_simulation_step(Timepoint& timestep) override {
                 initialize();
                 check(fs_solve_step(ctx, timestep.desired_time_step, &last_stats), "fs_solve_step");
+                timestep.desired_time_step = last_stats.desired_dt;   // the generator's (device's with the dynamic one)
                 timestep.actual_time_step = last_stats.actual_dt;
                 if (sync_host_collection) download_collection();
             }
@@ -241,6 +243,15 @@ namespace LibFluid {
                     p.timestep = g->settings.timestep;
                     p.lambda_v = g->settings.lambda_v;
                     p.lambda_a = g->settings.lambda_a;
+                } else if (auto d = std::dynamic_pointer_cast<DynamicCflTimestepGenerator>(data.timestep_generator)) {
+                    // the device generates the time step inside the step (the value the
+                    // Simulator passes in is then ignored)
+                    p.timestep_generator = FS_TIMESTEP_DYNAMIC_CFL;
+                    p.min_timestep = d->settings.min_timestep;
+                    p.max_timestep = d->settings.max_timestep;
+                    p.timestep = d->settings.max_timestep;
+                    p.lambda_v = d->settings.lambda_v;
+                    p.lambda_a = d->settings.lambda_a;
                 }
                 fill_settings(p);
                 return p;

@@ -123,6 +123,53 @@ class ConstantTimestepGenerator:
 
 
 @dataclass
+class DynamicCflTimestepGeneratorSettings:
+    max_timestep: float = 0.02
+    min_timestep: float = 0.0001
+    cfl_number: float = 0.8      # a setting of the reference that its generator does not read
+    lambda_v: float = 0.4
+    lambda_a: float = 0.25
+
+
+@dataclass
+class DynamicCflTimestepGenerator:
+    """time/DynamicCflTimestepGenerator.hpp: the time step follows the largest velocity and
+    acceleration of the active particles (DynamicCflTimestepGenerator.cpp:45-59). The device
+    generates it at the start of every step, inside the step's CUDA graph; the step calls'
+    desired_dt is then ignored, and get_generated_timestep() returns the last step's choice."""
+    settings: DynamicCflTimestepGeneratorSettings = field(default_factory=DynamicCflTimestepGeneratorSettings)
+    generated_timestep: float = 0.0
+
+    def generate_next_timestep(self) -> None:
+        pass
+
+    def get_generated_timestep(self) -> float:
+        return self.generated_timestep if self.generated_timestep > 0 else self.settings.max_timestep
+
+
+def _generator_params(g, p) -> None:
+    """Copies a time step generator's settings into fs_params."""
+    if isinstance(g, DynamicCflTimestepGenerator):
+        st = g.settings
+        p.timestep_generator = F.FS_TIMESTEP_DYNAMIC_CFL
+        p.min_timestep, p.max_timestep = st.min_timestep, st.max_timestep
+        p.timestep, p.lambda_v, p.lambda_a = st.max_timestep, st.lambda_v, st.lambda_a
+    else:
+        st = g.settings
+        p.timestep_generator = F.FS_TIMESTEP_CONSTANT
+        p.timestep, p.lambda_v, p.lambda_a = st.timestep, st.lambda_v, st.lambda_a
+
+
+def _default_dt(g) -> float:
+    return g.settings.timestep if isinstance(g, ConstantTimestepGenerator) else g.settings.max_timestep
+
+
+def _note_generated(g, stats) -> None:
+    if isinstance(g, DynamicCflTimestepGenerator):
+        g.generated_timestep = float(stats.desired_dt)
+
+
+@dataclass
 class IISPHSettings3D:
     max_density_error_allowed: float = 0.001
     min_number_of_iterations: int = 2
@@ -227,8 +274,7 @@ class FluidSolverBase:
         p.rest_density = self.parameters.rest_density
         p.gravity = self.parameters.gravity
         p.particle_size = self.parameters.particle_size
-        g = self.timestep_generator.settings
-        p.timestep, p.lambda_v, p.lambda_a = g.timestep, g.lambda_v, g.lambda_a
+        _generator_params(self.timestep_generator, p)
         p.max_particles = max(n, 1)
         p.neighbor_capacity = self.neighbor_capacity
         self._fill_settings(p)
@@ -269,21 +315,26 @@ class FluidSolverBase:
     def execute_simulation_step(self, timepoint: Timepoint) -> None:
         self.initialize()
         F.check(F.lib().fs_solve_step(self._dev.ctx, float(timepoint.desired_time_step), ctypes.byref(self.last_stats)))
+        _note_generated(self.timestep_generator, self.last_stats)
+        if isinstance(self.timestep_generator, DynamicCflTimestepGenerator):
+            timepoint.desired_time_step = float(self.last_stats.desired_dt)
         timepoint.actual_time_step = float(self.last_stats.actual_dt)
 
     def step(self, desired_dt: float | None = None) -> F.FsStepStats:
         """Neighborhood search + step in one call (fs_step)."""
         self.initialize()
-        dt = self.timestep_generator.settings.timestep if desired_dt is None else desired_dt
+        dt = _default_dt(self.timestep_generator) if desired_dt is None else desired_dt
         F.check(F.lib().fs_step(self._dev.ctx, float(dt), ctypes.byref(self.last_stats)))
+        _note_generated(self.timestep_generator, self.last_stats)
         return self.last_stats
 
     def run(self, steps: int, desired_dt: float | None = None) -> F.FsStepStats:
         """`steps` steps without host synchronisation in between (fs_run);
         returns the last step's statistics."""
         self.initialize()
-        dt = self.timestep_generator.settings.timestep if desired_dt is None else desired_dt
+        dt = _default_dt(self.timestep_generator) if desired_dt is None else desired_dt
         F.check(F.lib().fs_run(self._dev.ctx, int(steps), float(dt), ctypes.byref(self.last_stats)))
+        _note_generated(self.timestep_generator, self.last_stats)
         return self.last_stats
 
     def phase_times(self) -> list[float]:
@@ -397,11 +448,19 @@ class BatchedIISPHFluidSolver3D:
                                             neighbor_capacity=neighbor_capacity)
         self.parameters = self._template.parameters
         self.settings = self._template.settings
-        self.timestep_generator = self._template.timestep_generator
         self.scenes = [c.normalized() for c in scenes]
         self.offsets = np.concatenate([[0], np.cumsum([len(c) for c in self.scenes])]).astype(np.int64)
         self._ctx = None
         self.last_stats = None
+
+    @property
+    def timestep_generator(self):
+        """ConstantTimestepGenerator or DynamicCflTimestepGenerator (per scene on the device)."""
+        return self._template.timestep_generator
+
+    @timestep_generator.setter
+    def timestep_generator(self, g) -> None:
+        self._template.timestep_generator = g
 
     def initialize(self) -> None:
         if self._ctx is not None:
@@ -426,7 +485,7 @@ class BatchedIISPHFluidSolver3D:
         """`steps` steps of every scene; returns one FsStepStats per scene
         (the last step's)."""
         self.initialize()
-        dt = self.timestep_generator.settings.timestep if desired_dt is None else desired_dt
+        dt = _default_dt(self.timestep_generator) if desired_dt is None else desired_dt
         stats = (F.FsStepStats * len(self.scenes))()
         F.check(F.lib().fs_batch_run(self._ctx, int(steps), float(dt), ctypes.cast(stats, ctypes.c_void_p)))
         self.last_stats = list(stats)

@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define FS_ABI_VERSION 1
+#define FS_ABI_VERSION 2
 
 typedef enum fs_status {
     FS_OK = 0,
@@ -96,6 +96,15 @@ typedef enum fs_precision {
 #define FS_TYPE_BOUNDARY 1
 #define FS_TYPE_INACTIVE 2
 
+/* Time step generator of the Simulator (time/TimestepGenerator.hpp:13-33). */
+typedef enum fs_timestep_kind {
+    FS_TIMESTEP_CONSTANT = 0,    /* ConstantTimestepGenerator.cpp:4-41: desired dt = timestep */
+    FS_TIMESTEP_DYNAMIC_CFL = 1  /* DynamicCflTimestepGenerator.cpp:6-97: desired dt from the
+                                    largest |v| and |a| of the active particles, computed on the
+                                    device at the start of every step; the desired_dt argument of
+                                    the step calls is then ignored */
+} fs_timestep_kind;
+
 typedef struct fs_params {
     int32_t dim;        /* 2 or 3 */
     int32_t solver;     /* fs_solver_kind */
@@ -124,7 +133,8 @@ typedef struct fs_params {
     float omega;
     float gamma;
 
-    /* ConstantTimestepGenerator settings (ConstantTimestepGenerator.hpp:8-13) */
+    /* ConstantTimestepGenerator settings (ConstantTimestepGenerator.hpp:8-13); with the
+     * dynamic generator, timestep is its max_timestep (the CFL clamp's default) */
     float timestep;
     float lambda_v;
     float lambda_a;
@@ -132,7 +142,12 @@ typedef struct fs_params {
     /* capacities */
     int64_t max_particles;      /* device arrays are sized for this many particles */
     int32_t neighbor_capacity;  /* per-particle list slots for the solver (0: chosen from the scene) */
-    int32_t reserved;
+
+    /* time step generator (fs_timestep_kind) and DynamicCflTimestepGenerator's
+     * bounds (DynamicCflTimestepGenerator.hpp:11-18); lambda_v / lambda_a above */
+    int32_t timestep_generator;
+    float min_timestep;
+    float max_timestep;
 } fs_params;
 
 /* Fills *p with libFluid's defaults for the given solver and dimension
@@ -233,7 +248,9 @@ fs_status fs_query_position_noalloc(fs_ctx* ctx, const float* position, int64_t*
 /* The solver's timestep on the lists of the preceding fs_find_neighbors
  * (IFluidSolverBase::execute_simulation_step, IFluidSolver.hpp:30); the
  * CFL-clamped time step is returned in stats->actual_dt. desired_dt <= 0 uses
- * p->timestep. */
+ * p->timestep. With FS_TIMESTEP_DYNAMIC_CFL the device generates the desired
+ * time step (stats->desired_dt) and desired_dt is ignored, here and in
+ * fs_step / fs_run. */
 fs_status fs_solve_step(fs_ctx* ctx, float desired_dt, fs_step_stats* stats);
 /* One solver step: neighborhood search + the solver's timestep, like
  * Simulator::execute_simulation_step (Simulator.cpp:7-57) without entities

@@ -36,6 +36,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_kernel_eval.argtypes = [c_int, c_float, c_int64, c_void_p, c_void_p, c_void_p]
         L.oracle_cfl.argtypes = [c_float] * 6
         L.oracle_cfl.restype = c_float
+        L.oracle_dynamic_timestep.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_void_p] + [c_float] * 5
+        L.oracle_dynamic_timestep.restype = c_float
         L.oracle_ns.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_float, c_void_p, c_void_p]
         L.oracle_ns.restype = c_int64
         L.oracle_run.argtypes = [c_void_p, c_int64, c_int] + [c_void_p] * 13 + [c_int, c_void_p, c_int]
@@ -58,6 +60,15 @@ def kernel_eval(dim, support, x):
 
 def cfl(timestep, lambda_v, lambda_a, particle_size, max_acc, max_vel) -> float:
     return lib().oracle_cfl(timestep, lambda_v, lambda_a, particle_size, max_acc, max_vel)
+
+
+def dynamic_timestep(vel, acc, type_, particle_size, min_ts, max_ts, lambda_v, lambda_a) -> float:
+    """DynamicCflTimestepGenerator's time step for one collection (vel, acc: n x dim)."""
+    vel = np.ascontiguousarray(vel, np.float32)
+    acc = np.ascontiguousarray(acc, np.float32)
+    type_ = np.ascontiguousarray(type_, np.uint8)
+    return lib().oracle_dynamic_timestep(vel.shape[1], len(vel), _p(vel), _p(acc), _p(type_), particle_size,
+                                         min_ts, max_ts, lambda_v, lambda_a)
 
 
 def search(kind: str, position, radius: float, type_=None):

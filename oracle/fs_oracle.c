@@ -121,6 +121,34 @@ float oracle_cfl(float timestep, float lambda_v, float lambda_a, float particle_
     return fmaxf(nt, 0.000001f);
 }
 
+/* DynamicCflTimestepGenerator (DynamicCflTimestepGenerator.cpp:6-61, 82-107):
+ * the largest |v| and |a| (glm::length: sqrt of ((x x + y y) + z z) in float)
+ * over the particles that are not inactive, then
+ *   dt = min_ts, or max(min_ts, min(max_ts, cfl)) when both maxima exceed
+ *   FLT_EPSILON, cfl = max(min(sqrt(size / a) lambda_a, size / v lambda_v), 1e-6)
+ * with max_ts in place of a bound whose maximum is 0, and sqrt in double as in
+ * oracle_cfl. vel, acc: dim floats per particle. */
+float oracle_dynamic_timestep(int dim, int64_t n, const float* vel, const float* acc, const uint8_t* type,
+                              float particle_size, float min_ts, float max_ts, float lambda_v, float lambda_a) {
+    float max_v = 0.0f, max_a = 0.0f;
+    for (int64_t i = 0; i < n; i++) {
+        if (type[i] == T_INACTIVE) continue;
+        const v3 v = load(vel, dim, i), a = load(acc, dim, i);
+        const float lv = sqrtf(dot3(v, v)), la = sqrtf(dot3(a, a));
+        max_v = fmaxf(max_v, lv);
+        max_a = fmaxf(max_a, la);
+    }
+    float ts = min_ts;
+    if (max_v > FLT_EPSILON && max_a > FLT_EPSILON) {
+        float dta = max_ts, dtv = max_ts;
+        if (max_a > 0.0f) dta = (float)(sqrt((double)(particle_size / max_a)) * (double)lambda_a);
+        if (max_v > 0.0f) dtv = particle_size / max_v * lambda_v;
+        const float allowed = fmaxf(fminf(dta, dtv), 0.000001f);
+        ts = fmaxf(ts, fminf(max_ts, allowed));
+    }
+    return ts;
+}
+
 /* ------------------------------------------------------------------------ */
 /* neighborhood search                                                       */
 /* ------------------------------------------------------------------------ */

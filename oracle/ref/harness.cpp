@@ -27,6 +27,7 @@
 #include "fluidSolver/solver/SESPHFluidSolver.hpp"
 #include "fluidSolver/solver/SESPHFluidSolver3D.hpp"
 #include "time/ConstantTimestepGenerator.hpp"
+#include "time/DynamicCflTimestepGenerator.hpp"
 
 #include <algorithm>
 #include <cstdint>
@@ -294,6 +295,40 @@ void ref_cfl_timestep(float timestep, float lambda_v, float lambda_a, float part
     g.parameters.particle_size = particle_size;
     for (int64_t i = 0; i < n; i++)
         out[i] = g.get_non_cfl_validating_timestep(max_acc[i], max_vel[i]);
+}
+
+// DynamicCflTimestepGenerator::generate_next_timestep
+// (DynamicCflTimestepGenerator.cpp:45-59) over one collection of n particles
+// (dim 2 or 3: MovementData or MovementData3D): its generated time step.
+float ref_dynamic_timestep(int dim, int64_t n, const float* vel, const float* acc, const uint8_t* type,
+                           float particle_size, float min_ts, float max_ts, float lambda_v, float lambda_a) {
+    auto c = std::make_shared<ParticleCollection>();
+    if (dim == 3) c->add_type<MovementData3D>();
+    else c->add_type<MovementData>();
+    c->add_type<ParticleInfo>();
+    for (int64_t i = 0; i < n; i++) {
+        const size_t k = c->add();
+        if (dim == 3) {
+            auto& m = c->get<MovementData3D>(k);
+            m.velocity = glm::vec3(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+            m.acceleration = glm::vec3(acc[3 * i], acc[3 * i + 1], acc[3 * i + 2]);
+        } else {
+            auto& m = c->get<MovementData>(k);
+            m.velocity = glm::vec2(vel[2 * i], vel[2 * i + 1]);
+            m.acceleration = glm::vec2(acc[2 * i], acc[2 * i + 1]);
+        }
+        c->get<ParticleInfo>(k).type = type[i];
+        c->get<ParticleInfo>(k).tag = (uint32_t)i;
+    }
+    DynamicCflTimestepGenerator g;
+    g.settings.min_timestep = min_ts;
+    g.settings.max_timestep = max_ts;
+    g.settings.lambda_v = lambda_v;
+    g.settings.lambda_a = lambda_a;
+    g.parameters.particle_size = particle_size;
+    g.parameters.particle_collection = c;
+    g.generate_next_timestep();
+    return g.get_generated_timestep();
 }
 
 // ---------------------------------------------------------------------------

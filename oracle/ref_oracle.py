@@ -39,6 +39,8 @@ def lib(variant: str = "serial") -> ctypes.CDLL:
     L.ref_last_error.restype = ctypes.c_char_p
     L.ref_kernel_eval.argtypes = [c_int, c_float, c_int64, c_void_p, c_void_p, c_void_p]
     L.ref_cfl_timestep.argtypes = [c_float] * 4 + [c_int64, c_void_p, c_void_p, c_void_p]
+    L.ref_dynamic_timestep.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_void_p] + [c_float] * 5
+    L.ref_dynamic_timestep.restype = c_float
     L.ref_ns_create.restype = c_void_p
     L.ref_ns_create.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_float]
     L.ref_ns_destroy.argtypes = [c_void_p]
@@ -79,6 +81,14 @@ def cfl_timestep(timestep, lambda_v, lambda_a, particle_size, max_acc, max_vel):
     out = np.zeros_like(a)
     lib().ref_cfl_timestep(timestep, lambda_v, lambda_a, particle_size, len(a), _p(a), _p(v), _p(out))
     return out
+
+
+def dynamic_timestep(vel, acc, type_, particle_size, min_ts, max_ts, lambda_v, lambda_a) -> float:
+    vel = np.ascontiguousarray(vel, np.float32)
+    acc = np.ascontiguousarray(acc, np.float32)
+    type_ = np.ascontiguousarray(type_, np.uint8)
+    return lib().ref_dynamic_timestep(vel.shape[1], len(vel), _p(vel), _p(acc), _p(type_), particle_size, min_ts,
+                                      max_ts, lambda_v, lambda_a)
 
 
 class RefSearch:

@@ -13,6 +13,7 @@
 #include "fluidSolver/kernel/CubicSplineKernel3D.hpp"
 #include "fluidSolver/neighborhoodSearch/HashedNeighborhoodSearch3D.hpp"
 #include "fluidSolver/solver/IISPHFluidSolver3D.hpp"
+#include "time/DynamicCflTimestepGenerator.hpp"
 
 #include <cmath>
 #include <cstdio>
@@ -154,6 +155,71 @@ int main() {
             if (compare(*c_ref, *c_gpu, true, st)) return 1;
         }
         std::printf("bit-exact: %d steps of %zu particles identical\n", steps, c_ref->size());
+    }
+    // ---- bit-exact with DynamicCflTimestepGenerator -------------------------
+    // The reference's generator runs on the host over the reference's
+    // collection (DynamicCflTimestepGenerator.cpp:45-59); the drop-in's device
+    // chooses the time step inside its step and reports it in the timepoint.
+    // Fluid particles start with velocities and accelerations, so that the
+    // generator's CFL bounds, not its min/max clamp, decide the first steps.
+    {
+        auto make = [](std::shared_ptr<ParticleCollection> c) {
+            auto g = std::make_shared<DynamicCflTimestepGenerator>();
+            g->settings.max_timestep = 0.2f;
+            g->settings.min_timestep = 0.0001f;
+            g->parameters.particle_size = 1.0f;
+            g->parameters.particle_collection = c;
+            return g;
+        };
+        auto c_ref = make_scene(5), c_gpu = make_scene(5);
+        for (auto c : {c_ref, c_gpu}) {
+            uint32_t s = 99;
+            auto rnd = [&]() {
+                s ^= s << 13;
+                s ^= s >> 17;
+                s ^= s << 5;
+                return (float)((double)s / 4294967296.0 * 2.0 - 1.0);
+            };
+            for (size_t i = 0; i < c->size(); i++) {
+                if (c->get<ParticleInfo>(i).type != ParticleTypeNormal) continue;
+                auto& m = c->get<MovementData3D>(i);
+                m.velocity = glm::vec3(2.0f * rnd(), 2.0f * rnd(), 2.0f * rnd());
+                m.acceleration = glm::vec3(0.5f * rnd(), -9.81f + 0.5f * rnd(), 0.5f * rnd());
+            }
+        }
+        auto gen_ref = make(c_ref), gen_gpu = make(c_gpu);
+        IISPHFluidSolver3D<CubicSplineKernel3D, HashedNeighborhoodSearch3D> ref;
+        Cuda::IISPHFluidSolver3D<FS_SEARCH_HASHED_3D> gpu;
+        gpu.precision = FS_PRECISION_FP32;
+        gpu.flags = FS_FLAG_REFERENCE_ORDER;
+        setup(ref, c_ref, gen_ref);
+        setup(gpu, c_gpu, gen_gpu);
+        float first = 0.0f;
+        for (int st = 0; st < steps; st++) {
+            Timepoint t1, t2;
+            gen_ref->generate_next_timestep();
+            t1.desired_time_step = t1.actual_time_step = gen_ref->get_generated_timestep();
+            t2.desired_time_step = t2.actual_time_step = 1.0f;   // not used: the device generates it
+            ref.execute_neighborhood_search();
+            gpu.execute_neighborhood_search();
+            ref.execute_simulation_step(t1);
+            gpu.execute_simulation_step(t2);
+            if (!same_bits(t1.desired_time_step, t2.desired_time_step) ||
+                !same_bits(t1.actual_time_step, t2.actual_time_step) ||
+                ref.stat_last_iteration_count != gpu.stat_last_iteration_count) {
+                std::printf("dynamic step %d: desired %.9g vs %.9g, actual %.9g vs %.9g, iterations %zu vs %zu\n", st,
+                            t1.desired_time_step, t2.desired_time_step, t1.actual_time_step, t2.actual_time_step,
+                            ref.stat_last_iteration_count, gpu.stat_last_iteration_count);
+                return 1;
+            }
+            if (st == 0) first = t1.desired_time_step;
+            if (compare(*c_ref, *c_gpu, true, st)) return 1;
+        }
+        if (!(first > 0.0001f && first < 0.2f)) {
+            std::printf("dynamic: first time step %g was clamped, the CFL bounds were not exercised\n", first);
+            return 1;
+        }
+        std::printf("dynamic CFL generator: %d steps bit-exact (first dt %g)\n", steps, first);
     }
     // ---- default mode within tolerance -------------------------------------
     {

@@ -67,6 +67,38 @@ def cfl_fixture():
     np.savez_compressed(os.path.join(OUT, "cfl.npz"), max_acc=a, max_vel=v, **out)
 
 
+def dynamic_timestep_fixture():
+    """DynamicCflTimestepGenerator on random collections: velocity and
+    acceleration magnitudes over many decades, zero fields, inactive
+    particles carrying the largest values, 2D and 3D."""
+    rng = np.random.default_rng(21)
+    cases = []
+    for c in range(64):
+        dim = 3 if c % 4 else 2
+        n = int(rng.integers(1, 400))
+        vel = (rng.standard_normal((n, dim)) * 10 ** rng.uniform(-4, 2)).astype(np.float32)
+        acc = (rng.standard_normal((n, dim)) * 10 ** rng.uniform(-4, 3)).astype(np.float32)
+        typ = rng.choice(np.array([0, 1, 2], np.uint8), n, p=[0.7, 0.2, 0.1])
+        if c % 7 == 0:
+            vel[:] = 0.0
+        if c % 11 == 0:
+            acc[:] = 0.0
+        if c % 5 == 0:   # the fastest particle is inactive
+            k = int(rng.integers(n))
+            typ[k] = 2
+            vel[k] = 1e3
+            acc[k] = 1e4
+        ps = float(rng.choice([1.0, 0.1, 0.01]))
+        lo, hi = float(10 ** rng.uniform(-6, -3)), float(10 ** rng.uniform(-3, 0))
+        lv, la = float(rng.uniform(0.1, 0.9)), float(rng.uniform(0.1, 0.9))
+        dt = R.dynamic_timestep(vel, acc, typ, ps, lo, hi, lv, la)
+        cases.append((dim, vel, acc, typ, np.array([ps, lo, hi, lv, la, dt], np.float32)))
+    out = {}
+    for i, (dim, vel, acc, typ, prm) in enumerate(cases):
+        out[f"c{i}_vel"], out[f"c{i}_acc"], out[f"c{i}_type"], out[f"c{i}_prm"] = vel, acc, typ, prm
+    np.savez_compressed(os.path.join(OUT, "dynamic_timestep.npz"), **out)
+
+
 def _lists(kind, pos, radius, typ, calls=1, moves=None):
     s = R.RefSearch(kind, pos, radius, typ)
     ok = s.find()
@@ -195,7 +227,7 @@ if __name__ == "__main__":
     if not R.available():
         sys.exit("oracle/_ref is not built; run `make -C oracle/ref` where the reference checkout is available")
     fixtures = {"kernel": kernel_fixture, "cfl": cfl_fixture, "search": search_fixture, "solvers": solver_fixture,
-                "position_queries": position_query_fixture}
+                "position_queries": position_query_fixture, "dynamic_timestep": dynamic_timestep_fixture}
     for name in sys.argv[1:] or fixtures:
         fixtures[name]()
     for f in sorted(os.listdir(OUT)):

@@ -4,6 +4,7 @@ rejects bad configurations before touching a device."""
 import ctypes
 import os
 import re
+import subprocess
 
 import pytest
 
@@ -38,7 +39,27 @@ def test_library_exports_every_declared_symbol(L):
 
 
 def test_abi_version(L):
-    assert L.fs_abi_version() == 1
+    assert L.fs_abi_version() == 2
+
+
+def test_structs_match_the_header(tmp_path):
+    """The ctypes mirrors have the C compiler's layout of the header's structs."""
+    src = tmp_path / "layout.c"
+    fields = {"fs_params": [f[0] for f in F.FsParams._fields_], "fs_step_stats": [f[0] for f in F.FsStepStats._fields_]}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "fluidsolver_b200.h"', "int main(void) {"]
+    for st, names in fields.items():
+        lines.append(f'printf("%zu\\n", sizeof({st}));')
+        lines += [f'printf("%zu\\n", offsetof({st}, {n}));' for n in names]
+    lines += ["return 0;", "}"]
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = []
+    for cls in (F.FsParams, F.FsStepStats):
+        want.append(ctypes.sizeof(cls))
+        want += [getattr(cls, f[0]).offset for f in cls._fields_]
+    assert got == want
 
 
 def test_params_default_are_libfluid_defaults(L):

@@ -51,6 +51,20 @@ def test_cfl_clamp_matches_reference(golden, c_oracle):
         assert bits_equal(mine, g[f"dt_la{la}"])
 
 
+def test_dynamic_timestep_generator_matches_reference(golden, c_oracle):
+    """DynamicCflTimestepGenerator::generate_next_timestep (DynamicCflTimestepGenerator.cpp:45-59)
+    restated in oracle/fs_oracle.c against the reference's own generator (tests/golden)."""
+    g = golden["dynamic_timestep"]
+    n = sum(1 for f in g.files if f.endswith("_prm"))
+    kinds = set()
+    for i in range(n):
+        ps, lo, hi, lv, la, dt = (float(x) for x in g[f"c{i}_prm"])
+        mine = c_oracle.dynamic_timestep(g[f"c{i}_vel"], g[f"c{i}_acc"], g[f"c{i}_type"], ps, lo, hi, lv, la)
+        assert bits_equal(np.float32(mine), np.float32(dt)), i
+        kinds.add("min" if dt == np.float32(lo) else "max" if dt == np.float32(hi) else "cfl")
+    assert kinds == {"min", "max", "cfl"}   # every branch of the generator is exercised
+
+
 # ---------------------------------------------------------------- searches
 def _expect_sets(off, idx, i, expected):
     assert sorted(idx[off[i]:off[i + 1]].tolist()) == sorted(expected)
