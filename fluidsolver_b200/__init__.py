@@ -4,6 +4,7 @@ Python host mirror of libFluid's solver interfaces over that C-ABI."""
 from ._lib import FluidSolverError, lib  # noqa: F401
 from .solver import (  # noqa: F401
     BatchedIISPHFluidSolver3D,
+    BoundaryPreprocessor,
     ConstantTimestepGenerator,
     DynamicCflTimestepGenerator,
     IISPHFluidSolver,

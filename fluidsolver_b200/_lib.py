@@ -56,7 +56,7 @@ EXPORTED_SYMBOLS = (
     "fs_abi_version", "fs_last_error", "fs_params_default", "fs_create", "fs_destroy", "fs_set_params",
     "fs_upload", "fs_download", "fs_find_neighbors", "fs_get_neighbors_csr", "fs_query_position", "fs_solve_step", "fs_step",
     "fs_run", "fs_last_phase_times", "fs_stream", "fs_launch_count", "fs_batch_create", "fs_batch_run",
-    "fs_query_position_noalloc", "fs_get_solver_lists_csr",
+    "fs_query_position_noalloc", "fs_get_solver_lists_csr", "fs_boundary_preprocess", "fs_global_statistics",
 )
 
 
@@ -95,6 +95,16 @@ class FsStepStats(ctypes.Structure):
     ]
 
 
+class FsGlobalStats(ctypes.Structure):
+    _fields_ = [
+        ("density_max", c_float), ("density_min", c_float), ("density_avg", c_float),
+        ("pressure_max", c_float), ("pressure_min", c_float), ("pressure_avg", c_float),
+        ("velocity_max", c_float), ("velocity_min", c_float), ("velocity_avg", c_float),
+        ("kinetic_energy", c_float), ("potential_energy", c_float), ("reserved", c_int32),
+        ("normal_particles", c_int64), ("boundary_particles", c_int64), ("inactive_particles", c_int64),
+    ]
+
+
 class FluidSolverError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"fluidsolver_b200 status {status}: {message}")
@@ -126,6 +136,8 @@ def lib() -> ctypes.CDLL:
     L.fs_find_neighbors.argtypes = [ctx_p]
     L.fs_get_neighbors_csr.argtypes = [ctx_p, c_void_p, c_void_p, POINTER(c_int64)]
     L.fs_get_solver_lists_csr.argtypes = [ctx_p, c_void_p, c_void_p, POINTER(c_int64)]
+    L.fs_boundary_preprocess.argtypes = [ctx_p]
+    L.fs_global_statistics.argtypes = [ctx_p, c_float, POINTER(FsGlobalStats)]
     L.fs_query_position.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
     L.fs_query_position_noalloc.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
     L.fs_step.argtypes = [ctx_p, c_float, POINTER(FsStepStats)]
@@ -140,7 +152,8 @@ def lib() -> ctypes.CDLL:
     L.fs_batch_run.argtypes = [ctx_p, c_int32, c_float, c_void_p]
     for name in ("fs_create", "fs_destroy", "fs_set_params", "fs_upload", "fs_download", "fs_find_neighbors",
                  "fs_get_neighbors_csr", "fs_query_position", "fs_solve_step", "fs_step", "fs_run", "fs_last_phase_times",
-                 "fs_batch_create", "fs_batch_run", "fs_query_position_noalloc", "fs_get_solver_lists_csr"):
+                 "fs_batch_create", "fs_batch_run", "fs_query_position_noalloc", "fs_get_solver_lists_csr",
+                 "fs_boundary_preprocess", "fs_global_statistics"):
         getattr(L, name).restype = c_int32
     _lib = L
     return L

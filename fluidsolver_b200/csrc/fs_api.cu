@@ -17,6 +17,7 @@
 #include "fs_context.cuh"
 #include "fs_search.cuh"
 #include "fs_solvers.cuh"
+#include "fs_entities.cuh"
 
 using namespace fsb;
 
@@ -248,7 +249,8 @@ fs_status free_all(fs_ctx* c) {
                     c->rho_prev, c->vstar, c->anp, c->err, c->gbnd, c->tile_desc, c->tile_ent, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
                     c->perm[0], c->perm[1], c->cub_temp, c->cell_start, c->cell_counts, c->bbox, c->grids, c->nbr, c->nbr_count,
                     c->scene_of[0], c->scene_of[1], c->d_scene_offsets,
-                    c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->scalars};
+                    c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->scalars,
+                    c->stats_parts, c->stats_out};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -1627,6 +1629,58 @@ fs_status fs_get_solver_lists_csr(fs_ctx* c, int64_t* offsets, int64_t* indices,
         }
         std::sort(indices + offsets[h], indices + offsets[h + 1]);
     }
+    return FS_OK;
+}
+
+fs_status fs_boundary_preprocess(fs_ctx* c) {
+    if (!c) return fail(FS_ERR_INVALID, "ctx is null");
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    if (c->dim != 3) return fail(FS_ERR_INVALID, "the boundary preprocessor needs 3D particles (MovementData3D)");
+    if (c->scenes > 0) return fail(FS_ERR_INVALID, "not available on batched contexts");
+    // the neighbor sets of the current positions: a search since the last step
+    if (c->prm.solver != FS_SOLVER_NONE ? !c->have_lists : !c->have_cells)
+        return fail(FS_ERR_STATE, "execute the neighborhood search first");
+    FS_CUDA(cudaSetDevice(c->device));
+    if (c->n == 0) return FS_OK;
+    const WalkParams w = walk_of(c, false);
+    c->launches++;
+    if (c->precision == FS_PRECISION_FP64) {
+        const SolverConsts<double> k = consts_of<double>(c);
+        k_boundary_mass<double><<<grid_for(c->n), kBlock, 0, c->stream>>>(
+            c->n, state_of<double>(c), c->cell_start, w, k.kern, (double)c->prm.rest_density,
+            (double)c->prm.particle_size);
+    } else {
+        const SolverConsts<float> k = consts_of<float>(c);
+        k_boundary_mass<float><<<grid_for(c->n), kBlock, 0, c->stream>>>(
+            c->n, state_of<float>(c), c->cell_start, w, k.kern, c->prm.rest_density, c->prm.particle_size);
+    }
+    FS_CUDA(cudaGetLastError());
+    FS_CUDA(cudaStreamSynchronize(c->stream));
+    return FS_OK;
+}
+
+static_assert(sizeof(StatsOut) == sizeof(fs_global_stats), "StatsOut mirrors fs_global_stats");
+
+fs_status fs_global_statistics(fs_ctx* c, float zero_height, fs_global_stats* out) {
+    if (!c || !out) return fail(FS_ERR_INVALID, "null argument");
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    FS_CUDA(cudaSetDevice(c->device));
+    if (!c->stats_parts) {
+        FS_TRY(dalloc(&c->stats_parts, (size_t)kStatsBlocks));
+        FS_TRY(dalloc(&c->stats_out, (size_t)1));
+    }
+    const int blocks = (int)std::min<int64_t>(kStatsBlocks, std::max<int64_t>(1, (c->n + kStatsThreads - 1) / kStatsThreads));
+    c->launches += 2;
+    if (c->precision == FS_PRECISION_FP64)
+        k_stats_partial<double><<<blocks, kStatsThreads, 0, c->stream>>>(c->n, state_of<double>(c), c->prm.gravity,
+                                                                          zero_height, c->stats_parts);
+    else
+        k_stats_partial<float><<<blocks, kStatsThreads, 0, c->stream>>>(c->n, state_of<float>(c), c->prm.gravity,
+                                                                         zero_height, c->stats_parts);
+    k_stats_finish<<<1, kStatsThreads, 0, c->stream>>>(c->stats_parts, blocks, c->stats_out);
+    FS_CUDA(cudaGetLastError());
+    FS_CUDA(cudaMemcpyAsync(out, c->stats_out, sizeof(fs_global_stats), cudaMemcpyDeviceToHost, c->stream));
+    FS_CUDA(cudaStreamSynchronize(c->stream));
     return FS_OK;
 }
 

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "fs_common.cuh"
+#include "fs_entities.cuh"
 #include "fs_tiles.cuh"
 
 struct fs_ctx {
@@ -108,6 +109,8 @@ struct fs_ctx {
     size_t pinned_bytes = 0;
 
     int* status = nullptr;                  // device status word
+    fsb::StatsPart* stats_parts = nullptr;  // global statistics: per-block partials and the result
+    fsb::StatsOut* stats_out = nullptr;
     fsb::StepScalars* scalars = nullptr;    // device
     fsb::StepScalars* scalars_host = nullptr;  // pinned mirror
 

@@ -169,6 +169,22 @@ def _note_generated(g, stats) -> None:
         g.generated_timestep = float(stats.desired_dt)
 
 
+class BoundaryPreprocessor:
+    """entities/BoundaryPreprocessor.hpp: an entity that runs before the solver and sets the mass of
+    every boundary particle from its boundary neighbors. This one runs on the device state of
+    `solver` (its last neighborhood search), so the collection need not come back to the host."""
+
+    execution_point = "BeforeSolver"
+
+    def __init__(self, solver):
+        self.solver = solver
+
+    def execute_simulation_step(self, timepoint: "Timepoint", before_solver: bool) -> None:
+        if not before_solver:
+            raise ValueError("It makes only sense to execute the preprocessor before the solver!")
+        self.solver.boundary_preprocess()
+
+
 @dataclass
 class IISPHSettings3D:
     max_density_error_allowed: float = 0.001
@@ -354,6 +370,18 @@ class FluidSolverBase:
         idx = np.zeros(max(tot.value, 1), np.int64)
         F.check(F.lib().fs_get_neighbors_csr(self.ctx, off.ctypes.data, idx.ctypes.data, ctypes.byref(tot)))
         return off, idx[:tot.value]
+
+    # ---- entities and sensors on the device ---------------------------
+    def boundary_preprocess(self) -> None:
+        """BoundaryPreprocessor::execute_simulation_step (BoundaryPreprocessor.cpp:7-48) on the device
+        state: boundary masses from the boundary neighbors of the last search (fs_boundary_preprocess)."""
+        F.check(F.lib().fs_boundary_preprocess(self.ctx))
+
+    def global_statistics(self, zero_height: float = 0.0) -> dict:
+        """The global sensors of ParticleStatistics.cpp:17-201 over the device state (fs_global_statistics)."""
+        st = F.FsGlobalStats()
+        F.check(F.lib().fs_global_statistics(self.ctx, float(zero_height), ctypes.byref(st)))
+        return {name: getattr(st, name) for name, _ in st._fields_ if name != "reserved"}
 
     def solver_lists(self) -> tuple[np.ndarray, np.ndarray]:
         """CSR (offsets, indices) of the lists the solver's passes walk (3D IISPH fast mode: the tile

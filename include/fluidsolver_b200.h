@@ -270,6 +270,37 @@ void* fs_stream(fs_ctx* ctx);
  * (library kernels such as the radix sort's are not counted). */
 int64_t fs_launch_count(fs_ctx* ctx);
 
+/* ---- entities and sensors on the device -----------------------------------
+ * Host-side entities and sensors of the Simulator read the whole collection;
+ * these run their arithmetic where the state lives, so that a step loop that
+ * keeps the state on the device (fs_run, or a caller that does not download
+ * every step) still gets them. */
+
+/* BoundaryPreprocessor::execute_simulation_step (BoundaryPreprocessor.cpp:7-48,
+ * the entity that runs before the solver): every boundary particle's mass
+ * becomes min(rho0 particle_size^3, rho0 gamma_1 / sum_b W(x_i - x_b)), the sum
+ * over its boundary neighbors in the neighbor-set contract (itself included),
+ * gamma_1 from a perfectly sampled plane (:104-119). rho0 and particle_size are
+ * the context's. Needs a search on the current positions (fs_find_neighbors);
+ * in the FP32 reference-order mode the sums run in the reference's list order. */
+fs_status fs_boundary_preprocess(fs_ctx* ctx);
+
+/* Global sensors of ParticleStatistics.cpp:17-201 over the device state.
+ * Maxima start at FLT_MIN and minima at FLT_MAX, as the reference's
+ * MaxMinAvgSensorData does. Averages and energies are summed in FP64 (the
+ * reference sums serially in float, whose own rounding they differ by).
+ * velocity: |v| of the normal particles (the reference's velocity and energy
+ * sensors read 2D MovementData; in 3D the same formulas use the 3D velocity). */
+typedef struct fs_global_stats {
+    float density_max, density_min, density_avg;     /* GlobalDensitySensor (:17-43) */
+    float pressure_max, pressure_min, pressure_avg;  /* GlobalPressureSensor (:59-85) */
+    float velocity_max, velocity_min, velocity_avg;  /* GlobalVelocitySensor (:101-128) */
+    float kinetic_energy, potential_energy;          /* GlobalEnergySensor (:143-167): relative to zero_height */
+    int32_t reserved;
+    int64_t normal_particles, boundary_particles, inactive_particles; /* GlobalParticleCountSensor (:181-201) */
+} fs_global_stats;
+fs_status fs_global_statistics(fs_ctx* ctx, float zero_height, fs_global_stats* out);
+
 /* ---- batched scenes -------------------------------------------------------
  * Many independent scenes of uneven size advance together. This has no
  * counterpart in the reference, which runs one solver object per scene (one

@@ -38,6 +38,9 @@ def lib() -> ctypes.CDLL:
         L.oracle_cfl.restype = c_float
         L.oracle_dynamic_timestep.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_void_p] + [c_float] * 5
         L.oracle_dynamic_timestep.restype = c_float
+        L.oracle_boundary_masses.argtypes = [c_int64, c_void_p, c_void_p, c_void_p, c_float, c_float, c_void_p,
+                                             c_void_p, c_void_p]
+        L.oracle_global_stats.argtypes = [c_int, c_int64] + [c_void_p] * 6 + [c_float, c_float, c_void_p, c_void_p]
         L.oracle_ns.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_float, c_void_p, c_void_p]
         L.oracle_ns.restype = c_int64
         L.oracle_run.argtypes = [c_void_p, c_int64, c_int] + [c_void_p] * 13 + [c_int, c_void_p, c_int]
@@ -69,6 +72,36 @@ def dynamic_timestep(vel, acc, type_, particle_size, min_ts, max_ts, lambda_v, l
     type_ = np.ascontiguousarray(type_, np.uint8)
     return lib().oracle_dynamic_timestep(vel.shape[1], len(vel), _p(vel), _p(acc), _p(type_), particle_size,
                                          min_ts, max_ts, lambda_v, lambda_a)
+
+
+def boundary_masses(position, mass, type_, particle_size, rest_density, kind="hashed-3d") -> np.ndarray:
+    """BoundaryPreprocessor's masses (3D) with the contract's lists in the reference's order."""
+    pos = np.ascontiguousarray(position, np.float32)
+    mass = np.ascontiguousarray(mass, np.float32)
+    type_ = np.ascontiguousarray(type_, np.uint8)
+    off, idx, ok = search(kind, pos, 2.0 * particle_size, type_)
+    assert ok
+    out = np.zeros_like(mass)
+    lib().oracle_boundary_masses(len(pos), _p(pos), _p(mass), _p(type_), particle_size, rest_density, _p(off),
+                                 _p(np.ascontiguousarray(idx, np.int64)), _p(out))
+    return out
+
+
+def global_stats(col, gravity: float, zero_height: float = 0.0) -> dict:
+    """The global sensors of ParticleStatistics.cpp as the reference computes them."""
+    pos = np.ascontiguousarray(col.position, np.float32)
+    vel = np.ascontiguousarray(col.velocity, np.float32)
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+    out = np.zeros(11, np.float32)
+    counts = np.zeros(3, np.int64)
+    lib().oracle_global_stats(pos.shape[1], len(pos), _p(pos), _p(vel), _p(f(col.mass)), _p(f(col.density)),
+                              _p(f(col.pressure)), _p(np.ascontiguousarray(col.type, np.uint8)), gravity, zero_height,
+                              _p(out), _p(counts))
+    names = ["density_max", "density_min", "density_avg", "pressure_max", "pressure_min", "pressure_avg",
+             "velocity_max", "velocity_min", "velocity_avg", "kinetic_energy", "potential_energy"]
+    d = {k: np.float32(v) for k, v in zip(names, out)}
+    d.update(normal_particles=int(counts[0]), boundary_particles=int(counts[1]), inactive_particles=int(counts[2]))
+    return d
 
 
 def search(kind: str, position, radius: float, type_=None):

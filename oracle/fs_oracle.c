@@ -149,6 +149,76 @@ float oracle_dynamic_timestep(int dim, int64_t n, const float* vel, const float*
     return ts;
 }
 
+/* BoundaryPreprocessor::execute_simulation_step (BoundaryPreprocessor.cpp:7-48)
+ * on 3D particles with the given neighbor lists (CSR, in the interface's list
+ * order; pass the reference's order for bit-identical sums): every boundary
+ * particle's mass becomes fmin(rho0 size^3, (rho0 gamma_1) / sum W(x_i - x_b))
+ * over its boundary neighbors b, gamma_1 = size^3 * (sum W over the plane x = 0,
+ * y, z in -2..2 spacings, y outer) (:104-122). Other masses are copied. */
+void oracle_boundary_masses(int64_t n, const float* pos, const float* mass, const uint8_t* type, float particle_size,
+                            float rest_density, const int64_t* offsets, const int64_t* idx, float* out) {
+    kern_t k = kern_make(3, particle_size * 2.0f);
+    float ideal = 0.0f;
+    for (int y = -2; y <= 2; y++)
+        for (int z = -2; z <= 2; z++)
+            ideal += kW(&k, mk(0.0f * particle_size, (float)y * particle_size, (float)z * particle_size));
+    const float size3 = (particle_size * particle_size) * particle_size;
+    const float gamma_1 = size3 * ideal;
+    const float max_mass = rest_density * size3;
+    for (int64_t i = 0; i < n; i++) {
+        out[i] = mass[i];
+        if (type[i] != T_BOUNDARY) continue;
+        const v3 xi = load(pos, 3, i);
+        float vr = 0.0f;
+        for (int64_t q = offsets[i]; q < offsets[i + 1]; q++) {
+            const int64_t j = idx[q];
+            if (type[j] != T_BOUNDARY) continue;
+            vr += kW(&k, sub(xi, load(pos, 3, j)));
+        }
+        const float corrected = rest_density * gamma_1 / vr;
+        out[i] = fminf(max_mass, corrected);
+    }
+}
+
+/* The global sensors of ParticleStatistics.cpp:17-201, as the reference
+ * computes them: serial float sums in collection order, maxima from FLT_MIN,
+ * minima from FLT_MAX (MaxMinAvgSensorData), average = sum / count in float.
+ * out: density max, min, avg; pressure max, min, avg; |v| max, min, avg;
+ * kinetic, potential energy. counts: normal, boundary, inactive. */
+void oracle_global_stats(int dim, int64_t n, const float* pos, const float* vel, const float* mass,
+                         const float* density, const float* pressure, const uint8_t* type, float gravity,
+                         float zero_height, float* out, int64_t* counts) {
+    float mx[3] = {FLT_MIN, FLT_MIN, FLT_MIN}, mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, avg[3] = {0.f, 0.f, 0.f};
+    float kin = 0.0f, pot = 0.0f;
+    int64_t cnt[3] = {0, 0, 0};
+    for (int64_t i = 0; i < n; i++) {
+        if (type[i] == T_BOUNDARY) { cnt[1]++; continue; }
+        if (type[i] == T_INACTIVE) { cnt[2]++; continue; }
+        if (type[i] != T_NORMAL) continue;
+        cnt[0]++;
+        const v3 v = load(vel, dim, i);
+        const float speed = sqrtf(dot3(v, v));
+        const float vals[3] = {density[i], pressure[i], speed};
+        for (int q = 0; q < 3; q++) {
+            avg[q] += vals[q];
+            mn[q] = vals[q] < mn[q] ? vals[q] : mn[q];   /* std::min(d.minimum, value) */
+            mx[q] = mx[q] < vals[q] ? vals[q] : mx[q];   /* std::max(d.maximum, value) */
+        }
+        const float h = load(pos, dim, i).y - zero_height;
+        kin += ((0.5f * mass[i]) * speed) * speed;
+        pot += (gravity * mass[i]) * h;
+    }
+    for (int q = 0; q < 3; q++) {
+        if (cnt[0] > 0) avg[q] = avg[q] / (float)cnt[0];
+        out[3 * q] = mx[q];
+        out[3 * q + 1] = mn[q];
+        out[3 * q + 2] = avg[q];
+    }
+    out[9] = kin;
+    out[10] = pot;
+    for (int q = 0; q < 3; q++) counts[q] = cnt[q];
+}
+
 /* ------------------------------------------------------------------------ */
 /* neighborhood search                                                       */
 /* ------------------------------------------------------------------------ */

@@ -28,6 +28,7 @@
 #include "fluidSolver/solver/SESPHFluidSolver3D.hpp"
 #include "time/ConstantTimestepGenerator.hpp"
 #include "time/DynamicCflTimestepGenerator.hpp"
+#include "entities/BoundaryPreprocessor.hpp"
 
 #include <algorithm>
 #include <cstdint>
@@ -70,12 +71,14 @@ namespace {
         // neighbors of the particle currently stored at collection index i
         virtual void neighbors_of(size_t i, std::vector<size_t>& out) = 0;
         virtual void neighbors_of_position(const float* p, std::vector<size_t>& out) = 0;
+        virtual std::shared_ptr<NeighborhoodInterface> interface() = 0;
     };
 
     template <typename NS>
     struct NsImpl : NsBase {
         NS search;
         void find() override { search.find_neighbors(); }
+        std::shared_ptr<NeighborhoodInterface> interface() override { return search.create_interface(); }
         void neighbors_of(size_t i, std::vector<size_t>& out) override {
             out.clear();
             auto nb = search.get_neighbors(i);
@@ -389,6 +392,31 @@ int ref_ns_find(void* h) {
         g_last_error = e.what();
         return -1;
     }
+    return 0;
+}
+
+// BoundaryPreprocessor::execute_simulation_step (BoundaryPreprocessor.cpp:7-48)
+// on search h's collection (3D) through the search's own neighborhood
+// interface, after ref_ns_find. mass: the masses to start from, by tag; out:
+// the masses afterwards, by tag. Returns 0, or -1 when the reference threw.
+int ref_boundary_preprocess(void* h, const float* mass, float particle_size, float rest_density, float* out) {
+    auto* ns = static_cast<NsBase*>(h);
+    auto& c = *ns->collection;
+    for (size_t i = 0; i < c.size(); i++) c.get<ParticleData>(i).mass = mass[c.get<ParticleInfo>(i).tag];
+    try {
+        BoundaryPreprocessor bp;
+        bp.simulation_data.collection = ns->collection;
+        bp.simulation_data.particle_size = particle_size;
+        bp.simulation_data.rest_density = rest_density;
+        bp.simulation_data.neighborhood_interface = ns->interface();
+        bp.simulation_data.notify_that_data_changed();
+        Timepoint t;
+        bp.execute_simulation_step(t, true);
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+    for (size_t i = 0; i < c.size(); i++) out[c.get<ParticleInfo>(i).tag] = c.get<ParticleData>(i).mass;
     return 0;
 }
 

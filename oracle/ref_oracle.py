@@ -41,6 +41,7 @@ def lib(variant: str = "serial") -> ctypes.CDLL:
     L.ref_cfl_timestep.argtypes = [c_float] * 4 + [c_int64, c_void_p, c_void_p, c_void_p]
     L.ref_dynamic_timestep.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_void_p] + [c_float] * 5
     L.ref_dynamic_timestep.restype = c_float
+    L.ref_boundary_preprocess.argtypes = [c_void_p, c_void_p, c_float, c_float, c_void_p]
     L.ref_ns_create.restype = c_void_p
     L.ref_ns_create.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_float]
     L.ref_ns_destroy.argtypes = [c_void_p]
@@ -129,6 +130,14 @@ class RefSearch:
         if c < 0:
             raise RuntimeError(self.L.ref_last_error().decode())
         return out[:min(c, cap)]
+
+    def boundary_preprocess(self, mass: np.ndarray, particle_size: float, rest_density: float) -> np.ndarray:
+        """BoundaryPreprocessor on this search's collection (after find()), through its own interface."""
+        mass = np.ascontiguousarray(mass, np.float32)
+        out = np.zeros_like(mass)
+        if self.L.ref_boundary_preprocess(self.h, _p(mass), particle_size, rest_density, _p(out)) != 0:
+            raise RuntimeError(self.L.ref_last_error().decode())
+        return out
 
     def close(self):
         if self.h:

@@ -99,6 +99,31 @@ def dynamic_timestep_fixture():
     np.savez_compressed(os.path.join(OUT, "dynamic_timestep.npz"), **out)
 
 
+def boundary_fixture():
+    """BoundaryPreprocessor (BoundaryPreprocessor.cpp:7-48) through the reference's
+    hashed-3d interface: single- and two-layer tanks, a jittered tank at another
+    particle size, and initial masses that differ from particle to particle."""
+    rng = np.random.default_rng(31)
+    out = {}
+    cases = [("one_layer", 1.0, 1, 0.0), ("two_layers", 1.0, 2, 0.0), ("jittered", 0.5, 1, 0.05)]
+    for name, ps, layers, jitter in cases:
+        sc = scenes.breaking_dam_3d(6, 5, 4, ps, tank=(14, 9, 8), layers=layers, seed=41)
+        col = sc.collection
+        pos = col.position.astype(np.float32)
+        if jitter:
+            pos = (pos + rng.uniform(-jitter, jitter, pos.shape) * ps).astype(np.float32)
+        mass = (col.mass * rng.uniform(0.5, 1.5, len(pos))).astype(np.float32)
+        typ = col.type.astype(np.uint8)
+        typ[rng.choice(len(typ), 5, replace=False)] = 2   # some inactive particles
+        s = R.RefSearch("hashed-3d", pos, 2.0 * ps, typ)
+        assert s.find()
+        res = s.boundary_preprocess(mass, ps, 1.0)
+        s.close()
+        out[f"{name}_pos"], out[f"{name}_mass"], out[f"{name}_type"] = pos, mass, typ
+        out[f"{name}_size"], out[f"{name}_out"] = np.float32(ps), res
+    np.savez_compressed(os.path.join(OUT, "boundary.npz"), **out)
+
+
 def _lists(kind, pos, radius, typ, calls=1, moves=None):
     s = R.RefSearch(kind, pos, radius, typ)
     ok = s.find()
@@ -227,7 +252,8 @@ if __name__ == "__main__":
     if not R.available():
         sys.exit("oracle/_ref is not built; run `make -C oracle/ref` where the reference checkout is available")
     fixtures = {"kernel": kernel_fixture, "cfl": cfl_fixture, "search": search_fixture, "solvers": solver_fixture,
-                "position_queries": position_query_fixture, "dynamic_timestep": dynamic_timestep_fixture}
+                "position_queries": position_query_fixture, "dynamic_timestep": dynamic_timestep_fixture,
+                "boundary": boundary_fixture}
     for name in sys.argv[1:] or fixtures:
         fixtures[name]()
     for f in sorted(os.listdir(OUT)):

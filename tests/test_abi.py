@@ -45,7 +45,8 @@ def test_abi_version(L):
 def test_structs_match_the_header(tmp_path):
     """The ctypes mirrors have the C compiler's layout of the header's structs."""
     src = tmp_path / "layout.c"
-    fields = {"fs_params": [f[0] for f in F.FsParams._fields_], "fs_step_stats": [f[0] for f in F.FsStepStats._fields_]}
+    classes = {"fs_params": F.FsParams, "fs_step_stats": F.FsStepStats, "fs_global_stats": F.FsGlobalStats}
+    fields = {name: [f[0] for f in cls._fields_] for name, cls in classes.items()}
     lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "fluidsolver_b200.h"', "int main(void) {"]
     for st, names in fields.items():
         lines.append(f'printf("%zu\\n", sizeof({st}));')
@@ -56,7 +57,7 @@ def test_structs_match_the_header(tmp_path):
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = []
-    for cls in (F.FsParams, F.FsStepStats):
+    for cls in classes.values():
         want.append(ctypes.sizeof(cls))
         want += [getattr(cls, f[0]).offset for f in cls._fields_]
     assert got == want

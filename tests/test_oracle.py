@@ -65,6 +65,16 @@ def test_dynamic_timestep_generator_matches_reference(golden, c_oracle):
     assert kinds == {"min", "max", "cfl"}   # every branch of the generator is exercised
 
 
+def test_boundary_preprocessor_matches_reference(golden, c_oracle):
+    """BoundaryPreprocessor (BoundaryPreprocessor.cpp:7-48) restated in oracle/fs_oracle.c against the
+    reference's own entity through its hashed-3d interface (tests/golden/boundary.npz)."""
+    g = golden["boundary"]
+    for name in ("one_layer", "two_layers", "jittered"):
+        ps = float(g[f"{name}_size"])
+        mine = c_oracle.boundary_masses(g[f"{name}_pos"], g[f"{name}_mass"], g[f"{name}_type"], ps, 1.0)
+        assert bits_equal(mine, g[f"{name}_out"]), name
+
+
 # ---------------------------------------------------------------- searches
 def _expect_sets(off, idx, i, expected):
     assert sorted(idx[off[i]:off[i + 1]].tolist()) == sorted(expected)
