@@ -29,6 +29,7 @@
 #include "fluidSolver/solver/settings/SESPHSettings3D.hpp"
 #include "time/ConstantTimestepGenerator.hpp"
 #include "time/DynamicCflTimestepGenerator.hpp"
+#include "entities/SimulationEntity.hpp"
 
 #include "fluidsolver_b200.h"
 
@@ -202,7 +203,6 @@ namespace LibFluid {
                 const size_t n = c.size();
                 host.resize(n);
                 fs_particles v = host.view(n);
-                v.mass = nullptr;
                 v.type = nullptr;
                 v.tag = nullptr;
                 check(fs_download(ctx, &v), "fs_download");
@@ -218,12 +218,28 @@ namespace LibFluid {
                         for (int a = 0; a < DIM; a++) e[a] = host.external[i * DIM + a];
                     }
                     auto& pd = c.template get<ParticleData>(i);
+                    pd.mass = host.mass[i];   // the boundary preprocessor changes it on the device
                     pd.density = host.density[i];
                     pd.pressure = host.pressure[i];
                 }
             }
 
             fs_ctx* context() const { return ctx; }
+
+            // BoundaryPreprocessor's arithmetic (BoundaryPreprocessor.cpp:7-48) on the device state,
+            // between the search and the step; the masses reach the collection with the next download
+            void boundary_preprocess() {
+                initialize();
+                check(fs_boundary_preprocess(ctx), "fs_boundary_preprocess");
+            }
+
+            // the global sensors of ParticleStatistics.cpp:17-201 over the device state
+            fs_global_stats global_statistics(float zero_height = 0.0f) {
+                initialize();
+                fs_global_stats st{};
+                check(fs_global_statistics(ctx, zero_height, &st), "fs_global_statistics");
+                return st;
+            }
 
           protected:
             virtual void fill_settings(fs_params& p) = 0;
@@ -424,6 +440,30 @@ namespace LibFluid {
                 p.viscosity = settings.Viscosity;
             }
             void settings_acknowledge() override { settings.acknowledge_data_change(); }
+        };
+
+        // BoundaryPreprocessor (entities/BoundaryPreprocessor.hpp:7-28) for a drop-in solver: the
+        // same entity, executed before the solver, on the device state of `solver`
+        template <class Solver>
+        class BoundaryPreprocessor final : public SimulationEntity {
+          public:
+            explicit BoundaryPreprocessor(Solver& s) : solver(s) {
+                settings.execution_point = EntityExecutionPoint::BeforeSolver;
+            }
+            void execute_simulation_step(const Timepoint&, bool before_solver) override {
+                if (!before_solver)
+                    throw Error(FS_ERR_INVALID, "It makes only sense to execute the preprocessor before the solver!");
+                solver.boundary_preprocess();
+            }
+            void initialize() override {}
+            void create_compatibility_report(CompatibilityReport& report) override {
+                report.begin_scope("Cuda::BoundaryPreprocessor");
+                if (solver.parameters.particle_size <= 0.0f) report.add_issue("Particle size is smaller or equal to zero!");
+                report.end_scope();
+            }
+
+          private:
+            Solver& solver;
         };
 
     } // namespace Cuda

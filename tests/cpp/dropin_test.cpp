@@ -14,6 +14,7 @@
 #include "fluidSolver/neighborhoodSearch/HashedNeighborhoodSearch3D.hpp"
 #include "fluidSolver/solver/IISPHFluidSolver3D.hpp"
 #include "time/DynamicCflTimestepGenerator.hpp"
+#include "entities/BoundaryPreprocessor.hpp"
 
 #include <cmath>
 #include <cstdio>
@@ -220,6 +221,51 @@ int main() {
             return 1;
         }
         std::printf("dynamic CFL generator: %d steps bit-exact (first dt %g)\n", steps, first);
+    }
+    // ---- bit-exact with the boundary preprocessor ----------------------------
+    // libFluid's BoundaryPreprocessor on the host collection through the
+    // reference solver's interface, and Cuda::BoundaryPreprocessor on the
+    // device state, each run between the search and the step as the Simulator
+    // does for entities executed before the solver (Simulator.cpp:28-36).
+    {
+        auto gen = std::make_shared<ConstantTimestepGenerator>();
+        gen->settings.timestep = 0.005f;
+        gen->parameters.particle_size = 1.0f;
+        auto c_ref = make_scene(11), c_gpu = make_scene(11);
+        IISPHFluidSolver3D<CubicSplineKernel3D, HashedNeighborhoodSearch3D> ref;
+        Cuda::IISPHFluidSolver3D<FS_SEARCH_HASHED_3D> gpu;
+        gpu.precision = FS_PRECISION_FP32;
+        gpu.flags = FS_FLAG_REFERENCE_ORDER;
+        setup(ref, c_ref, gen);
+        setup(gpu, c_gpu, gen);
+        BoundaryPreprocessor bp_ref;
+        bp_ref.simulation_data.collection = c_ref;
+        bp_ref.simulation_data.particle_size = 1.0f;
+        bp_ref.simulation_data.rest_density = 1.0f;
+        Cuda::BoundaryPreprocessor<Cuda::IISPHFluidSolver3D<FS_SEARCH_HASHED_3D>> bp_gpu(gpu);
+        for (int st = 0; st < 6; st++) {
+            Timepoint t1, t2;
+            gen->generate_next_timestep();
+            t1.desired_time_step = t1.actual_time_step = gen->get_generated_timestep();
+            t2 = t1;
+            ref.execute_neighborhood_search();
+            gpu.execute_neighborhood_search();
+            bp_ref.simulation_data.neighborhood_interface = ref.create_neighborhood_interface();
+            bp_ref.simulation_data.notify_that_data_changed();
+            bp_ref.execute_simulation_step(t1, true);
+            bp_gpu.execute_simulation_step(t2, true);
+            ref.execute_simulation_step(t1);
+            gpu.execute_simulation_step(t2);
+            int bad = 0;
+            for (size_t i = 0; i < c_ref->size(); i++)
+                if (!same_bits(c_ref->get<ParticleData>(i).mass, c_gpu->get<ParticleData>(i).mass)) bad++;
+            if (bad) {
+                std::printf("boundary preprocessor step %d: %d masses differ\n", st, bad);
+                return 1;
+            }
+            if (compare(*c_ref, *c_gpu, true, st)) return 1;
+        }
+        std::printf("boundary preprocessor: 6 steps bit-exact\n");
     }
     // ---- default mode within tolerance -------------------------------------
     {
