@@ -14,4 +14,6 @@ from .solver import (  # noqa: F401
     SESPHFluidSolver,
     SESPHFluidSolver3D,
     Timepoint,
+    read_particles,
+    write_particles,
 )

@@ -30,6 +30,13 @@ FS_SOLVER_SESPH_3D = 2
 FS_SOLVER_IISPH_2D = 3
 FS_SOLVER_IISPH_3D = 4
 
+FS_COMPONENT_MOVEMENT_2D = 1 << 1
+FS_COMPONENT_MOVEMENT_3D = 1 << 2
+FS_COMPONENT_INFO = 1 << 3
+FS_COMPONENT_DATA = 1 << 4
+FS_COMPONENT_EXTERNAL_2D = 1 << 5
+FS_COMPONENT_EXTERNAL_3D = 1 << 6
+
 FS_TIMESTEP_CONSTANT = 0
 FS_TIMESTEP_DYNAMIC_CFL = 1
 
@@ -57,6 +64,7 @@ EXPORTED_SYMBOLS = (
     "fs_upload", "fs_download", "fs_find_neighbors", "fs_get_neighbors_csr", "fs_query_position", "fs_solve_step", "fs_step",
     "fs_run", "fs_last_phase_times", "fs_stream", "fs_launch_count", "fs_batch_create", "fs_batch_run",
     "fs_query_position_noalloc", "fs_get_solver_lists_csr", "fs_boundary_preprocess", "fs_global_statistics",
+    "fs_particles_file_info", "fs_particles_file_read", "fs_particles_file_write", "fs_dump",
 )
 
 
@@ -137,6 +145,10 @@ def lib() -> ctypes.CDLL:
     L.fs_get_neighbors_csr.argtypes = [ctx_p, c_void_p, c_void_p, POINTER(c_int64)]
     L.fs_get_solver_lists_csr.argtypes = [ctx_p, c_void_p, c_void_p, POINTER(c_int64)]
     L.fs_boundary_preprocess.argtypes = [ctx_p]
+    L.fs_particles_file_info.argtypes = [ctypes.c_char_p, POINTER(c_int32), POINTER(c_int64), POINTER(ctypes.c_uint32)]
+    L.fs_particles_file_read.argtypes = [ctypes.c_char_p, POINTER(FsParticles)]
+    L.fs_particles_file_write.argtypes = [ctypes.c_char_p, c_int32, POINTER(FsParticles)]
+    L.fs_dump.argtypes = [ctx_p, ctypes.c_char_p]
     L.fs_global_statistics.argtypes = [ctx_p, c_float, POINTER(FsGlobalStats)]
     L.fs_query_position.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
     L.fs_query_position_noalloc.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
@@ -153,7 +165,8 @@ def lib() -> ctypes.CDLL:
     for name in ("fs_create", "fs_destroy", "fs_set_params", "fs_upload", "fs_download", "fs_find_neighbors",
                  "fs_get_neighbors_csr", "fs_query_position", "fs_solve_step", "fs_step", "fs_run", "fs_last_phase_times",
                  "fs_batch_create", "fs_batch_run", "fs_query_position_noalloc", "fs_get_solver_lists_csr",
-                 "fs_boundary_preprocess", "fs_global_statistics"):
+                 "fs_boundary_preprocess", "fs_global_statistics", "fs_particles_file_info",
+                 "fs_particles_file_read", "fs_particles_file_write", "fs_dump"):
         getattr(L, name).restype = c_int32
     _lib = L
     return L

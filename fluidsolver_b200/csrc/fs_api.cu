@@ -18,6 +18,7 @@
 #include "fs_search.cuh"
 #include "fs_solvers.cuh"
 #include "fs_entities.cuh"
+#include "fs_io.hpp"
 
 using namespace fsb;
 
@@ -1682,6 +1683,108 @@ fs_status fs_global_statistics(fs_ctx* c, float zero_height, fs_global_stats* ou
     FS_CUDA(cudaMemcpyAsync(out, c->stats_out, sizeof(fs_global_stats), cudaMemcpyDeviceToHost, c->stream));
     FS_CUDA(cudaStreamSynchronize(c->stream));
     return FS_OK;
+}
+
+fs_status fs_particles_file_info(const char* path, int32_t* dim, int64_t* n, uint32_t* components) {
+    if (!path) return fail(FS_ERR_INVALID, "path is null");
+    fsio::ParticleFile f;
+    const std::string e = fsio::read_particle_file(path, f);
+    if (!e.empty()) return fail(FS_ERR_INVALID, e);
+    if (dim) *dim = f.dim;
+    if (n) *n = (int64_t)f.n;
+    if (components) *components = f.components;
+    return FS_OK;
+}
+
+fs_status fs_particles_file_read(const char* path, fs_particles* out) {
+    if (!path || !out) return fail(FS_ERR_INVALID, "null argument");
+    fsio::ParticleFile f;
+    const std::string e = fsio::read_particle_file(path, f);
+    if (!e.empty()) return fail(FS_ERR_INVALID, e);
+    if (out->n != (int64_t)f.n)
+        return fail(FS_ERR_INVALID, "out->n is " + std::to_string(out->n) + ", the file holds " + std::to_string(f.n));
+    const size_t n = (size_t)f.n, d = (size_t)f.dim;
+    auto copy = [&](float* dst, const std::vector<float>& src, size_t per) {
+        if (!dst) return;
+        if (src.empty()) std::memset(dst, 0, sizeof(float) * n * per);
+        else std::memcpy(dst, src.data(), sizeof(float) * n * per);
+    };
+    copy(out->position, f.position, d);
+    copy(out->velocity, f.velocity, d);
+    copy(out->acceleration, f.acceleration, d);
+    copy(out->external, f.external, d);
+    copy(out->mass, f.mass, 1);
+    copy(out->density, f.density, 1);
+    copy(out->pressure, f.pressure, 1);
+    if (out->type) {
+        if (f.type.empty()) std::memset(out->type, 0, n);
+        else std::memcpy(out->type, f.type.data(), n);
+    }
+    if (out->tag)
+        for (size_t i = 0; i < n; i++) out->tag[i] = f.tag.empty() ? (uint32_t)i : f.tag[i];
+    return FS_OK;
+}
+
+fs_status fs_particles_file_write(const char* path, int32_t dim, const fs_particles* in) {
+    if (!path || !in) return fail(FS_ERR_INVALID, "null argument");
+    if (dim != 2 && dim != 3) return fail(FS_ERR_INVALID, "dim must be 2 or 3");
+    if (in->n < 0) return fail(FS_ERR_INVALID, "negative particle count");
+    fsio::ParticleFile f;
+    f.dim = dim;
+    f.n = (uint64_t)in->n;
+    const size_t n = (size_t)in->n;
+    auto take = [&](std::vector<float>& dst, const float* src, size_t per) {
+        if (src) dst.assign(src, src + n * per);
+    };
+    take(f.position, in->position, dim);
+    if (in->position) {
+        f.velocity.assign(n * dim, 0.0f);
+        f.acceleration.assign(n * dim, 0.0f);
+        take(f.velocity, in->velocity, dim);
+        take(f.acceleration, in->acceleration, dim);
+    }
+    take(f.external, in->external, dim);
+    if (in->mass || in->density || in->pressure) {
+        f.mass.assign(n, 0.0f);
+        f.density.assign(n, 0.0f);
+        f.pressure.assign(n, 0.0f);
+        take(f.mass, in->mass, 1);
+        take(f.density, in->density, 1);
+        take(f.pressure, in->pressure, 1);
+    }
+    if (in->type || in->tag) {
+        f.type.assign(n, 0);
+        f.tag.resize(n);
+        for (size_t i = 0; i < n; i++) {
+            f.type[i] = in->type ? in->type[i] : (uint8_t)FS_TYPE_NORMAL;
+            f.tag[i] = in->tag ? in->tag[i] : (uint32_t)i;
+        }
+    }
+    const std::string e = fsio::write_particle_file(path, f);
+    if (!e.empty()) return fail(FS_ERR_INVALID, e);
+    return FS_OK;
+}
+
+fs_status fs_dump(fs_ctx* c, const char* path) {
+    if (!c || !path) return fail(FS_ERR_INVALID, "null argument");
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    const size_t n = (size_t)c->n, d = (size_t)c->dim;
+    std::vector<float> pos(n * d), vel(n * d), acc(n * d), ext(n * d), mass(n), rho(n), p(n);
+    std::vector<uint8_t> type(n);
+    std::vector<uint32_t> tag(n);
+    fs_particles v{};
+    v.n = (int64_t)n;
+    v.position = pos.data();
+    v.velocity = vel.data();
+    v.acceleration = acc.data();
+    v.external = ext.data();
+    v.mass = mass.data();
+    v.density = rho.data();
+    v.pressure = p.data();
+    v.type = type.data();
+    v.tag = tag.data();
+    FS_TRY(fs_download(c, &v));
+    return fs_particles_file_write(path, c->dim, &v);
 }
 
 fs_status fs_query_position(fs_ctx* c, const float* position, int64_t* out, int64_t cap, int64_t* count) {

@@ -169,6 +169,35 @@ def _note_generated(g, stats) -> None:
         g.generated_timestep = float(stats.desired_dt)
 
 
+def read_particles(path: str) -> "ParticleCollection":
+    """A ParticleSerializer v1 particle file (ParticleSerializer.cpp:89-141; scenario .data files,
+    FluidConsole dumps) in host order. Components the file lacks come back as None."""
+    dim, n, comp = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_uint32()
+    F.check(F.lib().fs_particles_file_info(str(path).encode(), ctypes.byref(dim), ctypes.byref(n), ctypes.byref(comp)))
+    d, n, c = dim.value, n.value, comp.value
+    mv = c & (F.FS_COMPONENT_MOVEMENT_2D | F.FS_COMPONENT_MOVEMENT_3D)
+    ex = c & (F.FS_COMPONENT_EXTERNAL_2D | F.FS_COMPONENT_EXTERNAL_3D)
+    vec = lambda on: np.zeros((n, d), np.float32) if on else None
+    sca = lambda on: np.zeros(n, np.float32) if on else None
+    info, data = c & F.FS_COMPONENT_INFO, c & F.FS_COMPONENT_DATA
+    out = ParticleCollection(position=vec(mv), velocity=vec(mv), acceleration=vec(mv), external=vec(ex),
+                             mass=sca(data), density=sca(data), pressure=sca(data),
+                             type=np.zeros(n, np.uint8) if info else None, tag=np.zeros(n, np.uint32) if info else None)
+    view = F.FsParticles()
+    view.n = n
+    for name in ("position", "velocity", "acceleration", "external", "mass", "density", "pressure", "type", "tag"):
+        setattr(view, name, _ptr(getattr(out, name)))
+    F.check(F.lib().fs_particles_file_read(str(path).encode(), ctypes.byref(view)))
+    return out
+
+
+def write_particles(path: str, col: "ParticleCollection") -> None:
+    """Writes `col` as a ParticleSerializer v1 particle file (ParticleSerializer.cpp:41-84) with the
+    components it holds."""
+    c = col.normalized()
+    F.check(F.lib().fs_particles_file_write(str(path).encode(), c.dim, ctypes.byref(c.as_fs())))
+
+
 class BoundaryPreprocessor:
     """entities/BoundaryPreprocessor.hpp: an entity that runs before the solver and sets the mass of
     every boundary particle from its boundary neighbors. This one runs on the device state of
@@ -382,6 +411,10 @@ class FluidSolverBase:
         st = F.FsGlobalStats()
         F.check(F.lib().fs_global_statistics(self.ctx, float(zero_height), ctypes.byref(st)))
         return {name: getattr(st, name) for name, _ in st._fields_ if name != "reserved"}
+
+    def dump(self, path: str) -> None:
+        """The device state as a particle file (fs_dump), FluidConsole's particle dump."""
+        F.check(F.lib().fs_dump(self.ctx, str(path).encode()))
 
     def solver_lists(self) -> tuple[np.ndarray, np.ndarray]:
         """CSR (offsets, indices) of the lists the solver's passes walk (3D IISPH fast mode: the tile

@@ -301,6 +301,35 @@ typedef struct fs_global_stats {
 } fs_global_stats;
 fs_status fs_global_statistics(fs_ctx* ctx, float zero_height, fs_global_stats* out);
 
+/* ---- particle files ---------------------------------------------------------
+ * ParticleSerializer's version-1 files (ParticleSerializer.cpp:41-141): the
+ * scenario particle files (scenarios/** / *.data) and FluidConsole's particle
+ * dumps. The layout (little-endian): u32 version 1, u32 component count, u32
+ * component ids, u64 particle count, then per particle the components present
+ * in id order (1/2 MovementData 2D/3D: position, velocity, acceleration;
+ * 3 ParticleInfo: u8 type, u32 tag; 4 ParticleData: density, mass, pressure;
+ * 5/6 ExternalForces 2D/3D), all inside one LZ4 frame (the lz4 library's
+ * LZ4F format, Lz4CompressedStream.cpp:24-180), coded by this library itself.
+ * components: bit (1 << id) per component the file holds. */
+#define FS_COMPONENT_MOVEMENT_2D (1u << 1)
+#define FS_COMPONENT_MOVEMENT_3D (1u << 2)
+#define FS_COMPONENT_INFO (1u << 3)
+#define FS_COMPONENT_DATA (1u << 4)
+#define FS_COMPONENT_EXTERNAL_2D (1u << 5)
+#define FS_COMPONENT_EXTERNAL_3D (1u << 6)
+fs_status fs_particles_file_info(const char* path, int32_t* dim, int64_t* n, uint32_t* components);
+/* Reads a file into the non-NULL arrays of *out (out->n must be the file's
+ * count); arrays of components the file lacks are zeroed (tag: the index). */
+fs_status fs_particles_file_read(const char* path, fs_particles* out);
+/* Writes n particles (in->n) of dimension dim with the components whose
+ * arrays are non-NULL: movement if position is (velocity and acceleration
+ * NULL: zero), info if type or tag is, data if mass, density or pressure is,
+ * external forces if external is. */
+fs_status fs_particles_file_write(const char* path, int32_t dim, const fs_particles* in);
+/* The context's state in host order, every component, written as a particle
+ * file: FluidConsole's particle dump (fluidConsole/main.cpp:24-32, 150-184). */
+fs_status fs_dump(fs_ctx* ctx, const char* path);
+
 /* ---- batched scenes -------------------------------------------------------
  * Many independent scenes of uneven size advance together. This has no
  * counterpart in the reference, which runs one solver object per scene (one
