@@ -430,27 +430,34 @@ __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* 
 }
 
 // Where a pass reads a tile's entries from: the staged slab in shared memory
-// or the octet planes in global memory. o: octet index of the owner's list.
+// or the octet planes in global memory. src(o, half): half `half` of the
+// owner's octet o -- entries 4 half .. 4 half + 3, two 32-bit words, so the
+// two threads of an owner load disjoint 8 bytes.
 struct SlabEntries {
     const uint4* e;   // slab.ent + local owner
-    __device__ __forceinline__ uint4 operator()(uint32_t o) const { return e[o * kTileOwners]; }
+    __device__ __forceinline__ uint2 operator()(uint32_t o, int half) const {
+        return reinterpret_cast<const uint2*>(e + o * kTileOwners)[half];
+    }
 };
 struct GlobalEntries {
     const uint4* __restrict__ e;   // T.ent + owner
     int64_t stride;
-    __device__ __forceinline__ uint4 operator()(uint32_t o) const { return __ldg(e + o * stride); }
+    __device__ __forceinline__ uint2 operator()(uint32_t o, int half) const {
+        return __ldg(reinterpret_cast<const uint2*>(e + o * stride) + half);
+    }
 };
 
 // Visits one half of an owner's list (entries 4 half .. 4 half + 3 of every
 // octet; cnt: the owner's packed list length): f(byte offset into a staged
 // float4 array, boundary) for each, and flush() after every second octet and
 // at the end (where the passes fold their partial sums into the compensated
-// accumulators). The next octet is loaded while the current one is visited.
+// accumulators). The next AHEAD octets are loaded while one is visited.
 // FLUID_ONLY visits the fluid entries, which come first in a list and have
 // the boundary bit clear.
-template <bool FLUID_ONLY = false, typename Src, typename F, typename Flush>
+template <bool FLUID_ONLY, int AHEAD, typename Src, typename F, typename Flush>
 __device__ __forceinline__ void for_tile_entries(const Src& src, uint32_t cnt, int K, int half, F&& f,
                                                  Flush&& flush) {
+    constexpr int kEntryPrefetch = AHEAD;
     const uint32_t all = min(cnt & 0xffffu, (uint32_t)K);
     const uint32_t n = FLUID_ONLY ? min(cnt >> 16, all) : all;
     auto visit = [&](uint32_t v) {
@@ -458,25 +465,28 @@ __device__ __forceinline__ void for_tile_entries(const Src& src, uint32_t cnt, i
         else f(v & kEntOffset, (v & kEntBoundary) != 0u);
     };
     const uint32_t full = n / 8, octets = (n + 7) / 8;
-    uint4 next = octets ? src(0) : make_uint4(0u, 0u, 0u, 0u);
+    uint2 ahead[kEntryPrefetch];
+#pragma unroll
+    for (int d = 0; d < kEntryPrefetch; d++) ahead[d] = (uint32_t)d < octets ? src(d, half) : make_uint2(0u, 0u);
     uint32_t o = 0;
     for (; o < full; o++) {
-        const uint4 cur = next;
-        if (o + 1 < octets) next = src(o + 1);
-        const uint32_t w0 = half ? cur.z : cur.x, w1 = half ? cur.w : cur.y;
-        visit(w0 & 0xffffu);
-        visit(w0 >> 16);
-        visit(w1 & 0xffffu);
-        visit(w1 >> 16);
+        const uint2 cur = ahead[0];
+#pragma unroll
+        for (int d = 0; d + 1 < kEntryPrefetch; d++) ahead[d] = ahead[d + 1];
+        if (o + kEntryPrefetch < octets) ahead[kEntryPrefetch - 1] = src(o + kEntryPrefetch, half);
+        visit(cur.x & 0xffffu);
+        visit(cur.x >> 16);
+        visit(cur.y & 0xffffu);
+        visit(cur.y >> 16);
         if (o & 1u) flush();
     }
     const int m = (int)(n - full * 8) - 4 * half;   // this half's entries of the last, partial octet
     if (m > 0) {
-        const uint32_t w0 = half ? next.z : next.x, w1 = half ? next.w : next.y;
-        visit(w0 & 0xffffu);
-        if (m > 1) visit(w0 >> 16);
-        if (m > 2) visit(w1 & 0xffffu);
-        if (m > 3) visit(w1 >> 16);
+        const uint2 cur = ahead[0];
+        visit(cur.x & 0xffffu);
+        if (m > 1) visit(cur.x >> 16);
+        if (m > 2) visit(cur.y & 0xffffu);
+        if (m > 3) visit(cur.y >> 16);
     }
     flush();
 }
@@ -484,16 +494,22 @@ __device__ __forceinline__ void for_tile_entries(const Src& src, uint32_t cnt, i
 // Walks one half of owner k's list (threadIdx.x / 2 within its tile) from
 // the global octet planes (GLOBAL; cnt: the owner's packed list length,
 // loaded by the caller) or from the staged slab.
-template <bool GLOBAL, bool FLUID_ONLY, typename F, typename Flush>
+template <bool GLOBAL, bool FLUID_ONLY, int AHEAD, typename F, typename Flush>
 __device__ __forceinline__ void walk_tile_list(const TileLists& T, const TileSlab& slab, int64_t k, uint32_t cnt,
                                                int half, F&& f, Flush&& flush) {
     if constexpr (GLOBAL) {
-        for_tile_entries<FLUID_ONLY>(GlobalEntries{T.ent + k, T.stride}, cnt, T.K, half, f, flush);
+        for_tile_entries<FLUID_ONLY, AHEAD>(GlobalEntries{T.ent + k, T.stride}, cnt, T.K, half, f, flush);
     } else {
         const int ol = (int)(threadIdx.x >> 1);
-        for_tile_entries<FLUID_ONLY>(SlabEntries{slab.ent + ol}, slab.count[ol], T.K, half, f, flush);
+        for_tile_entries<FLUID_ONLY, AHEAD>(SlabEntries{slab.ent + ol}, slab.count[ol], T.K, half, f, flush);
     }
 }
+
+// octets a pass loads ahead of the one it visits (measured on the 1M dam):
+// the pressure passes hide more latency with 3; the loops, with more work per
+// entry and more registers, do best with 1
+constexpr int kLoopAhead = 1;
+constexpr int kPressureAhead = 3;
 
 // the slab after a pass's staged candidates (bytes_per_candidate each)
 __device__ __forceinline__ TileSlab slab_at(float4* smem, int bytes_per_candidate, int K) {
@@ -611,7 +627,7 @@ __global__ void __launch_bounds__(kPassThreads, kL1GlobalEntries ? 4 : 3) k_tile
     V3<float> vpart = v3<float>(0.f, 0.f, 0.f);
     float rpart = 0.f;
     const float gb = c.single_layer ? c.gamma1 : 1.f;
-    if (valid) walk_tile_list<kL1GlobalEntries, false>(T, slab, k, cnt, half, [&](uint32_t off, bool bnd) {
+    if (valid) walk_tile_list<kL1GlobalEntries, false, kLoopAhead>(T, slab, k, cnt, half, [&](uint32_t off, bool bnd) {
         const float4 pj = at_offset(sp, off), vj = at_offset(sv, off);
         const float rj = at_offset(sr, off >> 2);
         const V3<float> xij = sub3(pk, pj);
@@ -686,7 +702,7 @@ __global__ void __launch_bounds__(kPassThreads, kL2GlobalEntries ? 4 : 3) k_tile
     float cpart = 0.f, g2part = 0.f;
     V3<float> ipart = v3<float>(0.f, 0.f, 0.f), mpart = v3<float>(0.f, 0.f, 0.f), bpart = v3<float>(0.f, 0.f, 0.f);
     const float wb = c.single_layer ? c.two_gamma : 2.f;
-    if (valid) walk_tile_list<kL2GlobalEntries, false>(T, slab, k, cnt, half, [&](uint32_t off, bool bnd) {
+    if (valid) walk_tile_list<kL2GlobalEntries, false, kLoopAhead>(T, slab, k, cnt, half, [&](uint32_t off, bool bnd) {
         const float4 pj = at_offset(sp, off), vsj = at_offset(sa, off);
         const V3<float> xij = sub3(pk, pj);
         const float r2 = r2_of(xij);
@@ -770,7 +786,7 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
         pa.add(part);
         part = v3<float>(0.f, 0.f, 0.f);
     };
-    if (valid) walk_tile_list<kPressureGlobalEntries, true>(T, slab, k, cnt, half, pair, flush);
+    if (valid) walk_tile_list<kPressureGlobalEntries, true, kPressureAhead>(T, slab, k, cnt, half, pair, flush);
     const V3<float> a = pair_total(pa);
     if (half || !valid) return;
     // boundary: - sum_bnd (lambda m_j p_i / rho0^2) gradW, lambda = 2 gamma (single layer) or 2
@@ -827,7 +843,7 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
                 ap.add(part);
                 part = 0.f;
             };
-            if (valid) walk_tile_list<kPressureGlobalEntries, true>(T, slab, k, cnt, half, pair, flush);
+            if (valid) walk_tile_list<kPressureGlobalEntries, true, kPressureAhead>(T, slab, k, cnt, half, pair, flush);
             // boundary: sum_bnd m_j dot(a_i, gradW) = dot(a_i, sum_bnd m_j gradW)
             const float sum = pair_total(ap) + dot3(v3<float>(ak.x, ak.y, ak.z), v3<float>(gbk.x, gbk.y, gbk.z));
             if (!half && valid)
