@@ -406,12 +406,16 @@ __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* 
             : "memory");
     if ((uint32_t)t < h.nranges && !(FLUID_ONLY && (rg.len_base & kRangeBoundary))) {
         const uint32_t a = rg.start, len = rg.len_base & kRangeLen, base = rg.len_base >> 16;
+        // the candidates' arrays are re-read by the neighboring tiles and by the
+        // next pass: kept in L2 ahead of the streamed lists (evict_last)
+        uint64_t pol;
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
 #pragma unroll
         for (int v = 0; v < NV4; v++) {
             asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                    smem_u32(dst4[v] + base)),
-                "l"(src4[v] + a), "r"(len * 16u), "r"(smem_u32(&st.bar))
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], "
+                "%4;" ::"r"(smem_u32(dst4[v] + base)),
+                "l"(src4[v] + a), "r"(len * 16u), "r"(smem_u32(&st.bar)), "l"(pol)
                 : "memory");
         }
     }
