@@ -702,9 +702,9 @@ __global__ void __launch_bounds__(kPassThreads, kL2GlobalEntries ? 4 : 3) k_tile
     if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     Acc<float, true> contrib, mg2;
-    Acc3<float, true> inner, mg, gb;
+    Acc3<float, true> mg, gb;
     float cpart = 0.f, g2part = 0.f;
-    V3<float> ipart = v3<float>(0.f, 0.f, 0.f), mpart = v3<float>(0.f, 0.f, 0.f), bpart = v3<float>(0.f, 0.f, 0.f);
+    V3<float> mpart = v3<float>(0.f, 0.f, 0.f), bpart = v3<float>(0.f, 0.f, 0.f);
     const float wb = c.single_layer ? c.two_gamma : 2.f;
     if (valid) walk_tile_list<kL2GlobalEntries, false, kLoopAhead>(T, slab, k, cnt, half, [&](uint32_t off, bool bnd) {
         const float4 pj = at_offset(sp, off), vsj = at_offset(sa, off);
@@ -714,21 +714,22 @@ __global__ void __launch_bounds__(kPassThreads, kL2GlobalEntries ? 4 : 3) k_tile
         const float mf = pj.w * f;            // m_j gradW = mf d
         const V3<float> dv = bnd ? v3<float>(vsk.x, vsk.y, vsk.z) : sub3(vsk, vsj);
         cpart = __fmaf_rn(mf, dot3(dv, xij), cpart);
-        ipart = fma3(bnd ? -wb * mf : -mf, xij, ipart);
         if (!bnd) g2part = __fmaf_rn(mf * f, r2, g2part);
         else bpart = fma3(mf, xij, bpart);
         mpart = fma3(mf, xij, mpart);
     }, [&] {
         contrib.add(cpart);
         mg2.add(g2part);
-        inner.add(ipart);
         mg.add(mpart);
         gb.add(bpart);
         cpart = g2part = 0.f;
-        ipart = mpart = bpart = v3<float>(0.f, 0.f, 0.f);
+        mpart = bpart = v3<float>(0.f, 0.f, 0.f);
     });
     const float ct = pair_total(contrib), g2 = pair_total(mg2);
-    const V3<float> in = pair_total(inner), m = pair_total(mg), gbt = pair_total(gb);
+    const V3<float> m = pair_total(mg), gbt = pair_total(gb);
+    // the inner sum of d_ii, -sum_fluid m_j gradW - lambda sum_bnd m_j gradW, from the two sums above
+    const V3<float> in = v3<float>(__fmaf_rn(1.f - wb, gbt.x, -m.x), __fmaf_rn(1.f - wb, gbt.y, -m.y),
+                                   __fmaf_rn(1.f - wb, gbt.z, -m.z));
     if (!half && valid) {
         s.gbnd[k] = v4<float>(gbt, 0.f);   // sum_bnd m_j gradW, for the pressure iterations
         const float source = (c.rest_density - rk) - dt * ct;
