@@ -515,6 +515,31 @@ def run_configs(args, device):
                                         "fp32" else " in FP64 (the error reference)"),
             "gpu_ms_per_step": ms4, "gpu_particle_steps_per_s": d4.n_fluid / (ms4 / 1e3),
             "iterations_last_step": int(st4.iterations), "avg_density_error_last_step": float(st4.avg_density_error_fp64)}
+    out["error_vs_fp64"] = error_vs_fp64(sc.dam_1m(seed=5), device)
+    return out
+
+
+def error_vs_fp64(scene, device, steps=5):
+    """The state after `steps` steps of the 1M dam in the fast mode (FP32 + compensated sums) and in
+    FP32 with the reference's operation order, each against FP64 from the same start: the largest
+    position deviation (in particle sizes) and the largest relative density deviation."""
+    def run(prec, reference_order=False):
+        s = make_solver(scene, device, prec)
+        s.reference_order = reference_order
+        for _ in range(steps):
+            s.step()
+        c = s.collection()
+        s.close()
+        return c
+    ref = run("fp64")
+    out = {"steps": steps, "scene": "the 1M dam from its initial state"}
+    for name, (prec, order) in {"fast_mode": ("fp32-kahan", False), "reference_arithmetic_fp32": ("fp32", True)}.items():
+        c = run(prec, order)
+        fluid = ref.type == 0
+        out[name] = {
+            "position_max_abs": float(np.abs(c.position[fluid] - ref.position[fluid]).max() / scene.particle_size),
+            "density_max_rel": float((np.abs(c.density[fluid].astype(np.float64) - ref.density[fluid]) /
+                                      np.abs(ref.density[fluid].astype(np.float64))).max())}
     return out
 
 
