@@ -226,6 +226,8 @@ def run_ours(args):
     n_active = scene.n_fluid + scene.n_boundary
     solver = make_solver(scene, local, args.precision, args.eager)
     L = F.lib()
+    # the tile passes' prefetch depths, chosen on a copy of this scene (fs_autotune)
+    tuning = None if args.no_autotune else solver.autotune()
     for _ in range(args.warmup):
         solver.step()
     ctx = solver.ctx
@@ -276,7 +278,7 @@ def run_ours(args):
     e2e = run_e2e(solver, scene, min(args.steps, 5), local, max_over_ranks)
     solver_state = solver.collection() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     solver.close()
-    batched = None if args.no_batched else run_batched(args, local, rank, world, max_over_ranks, barrier)
+    batched = None if args.no_batched else run_batched(args, local, rank, world, max_over_ranks, barrier, tuning)
     ns_micro = run_ns_microbench(args, local) if (rank == 0 and world == 1 and not args.no_batched) else None
     configs = run_configs(args, local) if (rank == 0 and world == 1 and not args.no_batched) else None
 
@@ -298,6 +300,7 @@ def run_ours(args):
                        "mode": "eager (host-driven pressure loop, profiling only)" if args.eager else
                        "whole step as one CUDA graph (pressure loop: conditional WHILE node)",
                        "l2": "inputs larger than L2 (~0.5 GB of particle state and lists per step)",
+                       "tuning": tuning,
                        "iterations_mean": it_total / args.steps, "avg_density_error_max": max(errs),
                        "phase_ms_per_step": dict(zip(PHASES, (phase / args.steps).round(4).tolist())),
                        "algorithmic_bytes_per_step": step_bytes,
@@ -314,7 +317,7 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_batched(args, device, rank, world, max_over_ranks, barrier):
+def run_batched(args, device, rank, world, max_over_ranks, barrier, tuning=None):
     """The batched breaking dams (256 scenes, seed 6; scenes i = rank mod N on
     rank N): all of a rank's scenes in one batched context, timed with CUDA
     events on the context's stream around fs_batch_run; at N = 1 the same
@@ -329,6 +332,8 @@ def run_batched(args, device, rank, world, max_over_ranks, barrier):
     mine = shard(allsc, rank, world)
     batch = BatchedIISPHFluidSolver3D([s.collection for s in mine], device=device)
     configure_iisph(batch)
+    if tuning and tuning["tuned"]:   # the depths the 1M dam chose
+        batch.set_tuning(tuning["first_loop_prefetch"], tuning["pressure_prefetch"])
     batch.run(args.warmup)
     stream = torch.cuda.ExternalStream(L.fs_stream(batch.ctx), device=torch.device("cuda", device))
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -353,6 +358,8 @@ def run_batched(args, device, rank, world, max_over_ranks, barrier):
         total_ms = 0.0
         for sc in allsc:
             solver = make_solver(sc, device)
+            if tuning and tuning["tuned"]:
+                solver.set_tuning(tuning["first_loop_prefetch"], tuning["pressure_prefetch"])
             solver.run(args.warmup)
             s2 = torch.cuda.ExternalStream(L.fs_stream(solver.ctx), device=torch.device("cuda", device))
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -649,6 +656,7 @@ def main():
     ap.add_argument("--precision", default="fp32-kahan", choices=["fp32", "fp32-kahan", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-scene batched measurement")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default prefetch depths of the tile passes")
     ap.add_argument("--eager", action="store_true",
                     help="host-driven pressure loop instead of the whole-step CUDA graph: for kernel-level profiling "
                          "(ncu cannot profile the kernels of a graph with conditional nodes); slower, not a bench value")

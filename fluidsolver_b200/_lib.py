@@ -65,6 +65,7 @@ EXPORTED_SYMBOLS = (
     "fs_run", "fs_last_phase_times", "fs_stream", "fs_launch_count", "fs_batch_create", "fs_batch_run",
     "fs_query_position_noalloc", "fs_get_solver_lists_csr", "fs_boundary_preprocess", "fs_global_statistics",
     "fs_particles_file_info", "fs_particles_file_read", "fs_particles_file_write", "fs_dump",
+    "fs_autotune", "fs_set_tuning",
 )
 
 
@@ -113,6 +114,13 @@ class FsGlobalStats(ctypes.Structure):
     ]
 
 
+class FsTuning(ctypes.Structure):
+    _fields_ = [
+        ("tuned", c_int32), ("first_loop_prefetch", c_int32), ("pressure_prefetch", c_int32), ("reserved", c_int32),
+        ("first_loop_ms", c_float * 4), ("pressure_iteration_ms", c_float * 4),
+    ]
+
+
 class FluidSolverError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"fluidsolver_b200 status {status}: {message}")
@@ -149,6 +157,8 @@ def lib() -> ctypes.CDLL:
     L.fs_particles_file_read.argtypes = [ctypes.c_char_p, POINTER(FsParticles)]
     L.fs_particles_file_write.argtypes = [ctypes.c_char_p, c_int32, POINTER(FsParticles)]
     L.fs_dump.argtypes = [ctx_p, ctypes.c_char_p]
+    L.fs_autotune.argtypes = [ctx_p, POINTER(FsTuning)]
+    L.fs_set_tuning.argtypes = [ctx_p, POINTER(FsTuning)]
     L.fs_global_statistics.argtypes = [ctx_p, c_float, POINTER(FsGlobalStats)]
     L.fs_query_position.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
     L.fs_query_position_noalloc.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
@@ -166,7 +176,7 @@ def lib() -> ctypes.CDLL:
                  "fs_get_neighbors_csr", "fs_query_position", "fs_solve_step", "fs_step", "fs_run", "fs_last_phase_times",
                  "fs_batch_create", "fs_batch_run", "fs_query_position_noalloc", "fs_get_solver_lists_csr",
                  "fs_boundary_preprocess", "fs_global_statistics", "fs_particles_file_info",
-                 "fs_particles_file_read", "fs_particles_file_write", "fs_dump"):
+                 "fs_particles_file_read", "fs_particles_file_write", "fs_dump", "fs_autotune", "fs_set_tuning"):
         getattr(L, name).restype = c_int32
     _lib = L
     return L

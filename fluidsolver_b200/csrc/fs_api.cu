@@ -878,8 +878,9 @@ fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
     State<float> s = state_of<float>(c);
     FS_TRY(mark(c, 1, st));
     c->launches++;
-    k_tile_iisph3d_l1<<<tiles + rest, kPassThreads, tile_pass_smem(36, T.K, !kL1GlobalEntries), st>>>(
-        nf, n, tiles, s, T, L, k, c->scalars, c->status);
+    FSB_AHEAD_SWITCH(c->tuning.l1_ahead, k_tile_iisph3d_l1,
+                     <<<tiles + rest, kPassThreads, tile_pass_smem(36, T.K, !kL1GlobalEntries), st>>>(
+                         nf, n, tiles, s, T, L, k, c->scalars, c->status))
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 2, st));
     c->launches++;
@@ -891,10 +892,12 @@ fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
     FS_TRY(enqueue_pressure_loop(c, capture, false, true, [&](cudaStream_t bs) {
         c->launches += 2;
         const bool slab = !kPressureGlobalEntries;
-        k_tile_iisph3d_pressure_acc<<<tiles, kPassThreads, tile_pass_smem(20, T.K, slab), bs>>>(nf, s, T, L, k,
-                                                                                       c->scalars, c->status);
-        k_tile_iisph3d_pressure_update<<<tiles, kPassThreads, tile_pass_smem(32, T.K, slab), bs>>>(nf, s, T, L, k,
-                                                                                          c->scalars, c->status);
+        FSB_AHEAD_SWITCH(c->tuning.pressure_ahead, k_tile_iisph3d_pressure_acc,
+                         <<<tiles, kPassThreads, tile_pass_smem(20, T.K, slab), bs>>>(nf, s, T, L, k, c->scalars,
+                                                                                       c->status))
+        FSB_AHEAD_SWITCH(c->tuning.pressure_ahead, k_tile_iisph3d_pressure_update,
+                         <<<tiles, kPassThreads, tile_pass_smem(32, T.K, slab), bs>>>(nf, s, T, L, k, c->scalars,
+                                                                                       c->status))
     }, true));
     FS_TRY(mark(c, 4, st));
     c->launches++;
@@ -1876,6 +1879,99 @@ fs_status fs_run(fs_ctx* c, int32_t steps, float desired_dt, fs_step_stats* stat
     int st = 0;
     FS_TRY(finish_steps(c, stats, &st));
     if (st != FS_OK) return fail((fs_status)st, "device reported an error during fs_run");
+    return FS_OK;
+}
+
+// The tile passes' prefetch depths, chosen by timing whole steps on a copy of
+// the context: the same parameters and the same particles (downloaded from
+// the context, uploaded into the copy), so the caller's state and step count
+// stay as they were. Each trial runs 2 steps to capture its graph and settle,
+// then 4 timed steps; the first loop is timed as its phase, the pressure
+// passes per loop iteration (the first iteration runs inside the second loop).
+// Trials (pressure depth, first-loop depth): (1,1), (2,2), (3,1), (4,2); each
+// depth is judged by the mean over the trials that used it.
+fs_status fs_autotune(fs_ctx* c, fs_tuning* out) {
+    if (!c || !out) return fail(FS_ERR_INVALID, "null argument");
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    if (c->scenes > 0)
+        return fail(FS_ERR_INVALID, "tune a single-scene context and hand its result to fs_set_tuning");
+    *out = fs_tuning{};
+    out->first_loop_prefetch = c->tuning.l1_ahead;
+    out->pressure_prefetch = c->tuning.pressure_ahead;
+    if (!tiled_mode(c) || c->n_fluid == 0) return FS_OK;   // nothing tunable: the passes are not tiled
+    FS_CUDA(cudaSetDevice(c->device));
+    const size_t n = (size_t)c->n, d = (size_t)c->dim;
+    std::vector<float> pos(n * d), vel(n * d), acc(n * d), ext(n * d), mass(n), rho(n), p(n);
+    std::vector<uint8_t> type(n);
+    std::vector<uint32_t> tag(n);
+    fs_particles v{};
+    v.n = (int64_t)n;
+    v.position = pos.data();
+    v.velocity = vel.data();
+    v.acceleration = acc.data();
+    v.external = ext.data();
+    v.mass = mass.data();
+    v.density = rho.data();
+    v.pressure = p.data();
+    v.type = type.data();
+    v.tag = tag.data();
+    FS_TRY(fs_download(c, &v));
+    fs_ctx* t = nullptr;
+    FS_TRY(create_ctx(&c->prm, 0, nullptr, &t));
+    struct Guard {
+        fs_ctx* t;
+        ~Guard() { fs_destroy(t); }
+    } guard{t};
+    FS_TRY(fs_upload(t, &v));
+    const int trials[4][2] = {{1, 1}, {2, 2}, {3, 1}, {kMaxAhead, 2}};
+    double l1_sum[kMaxAhead + 1] = {}, pi_sum[kMaxAhead + 1] = {};
+    int l1_cnt[kMaxAhead + 1] = {}, pi_cnt[kMaxAhead + 1] = {};
+    fs_step_stats st{};
+    for (const auto& tr : trials) {
+        t->tuning.pressure_ahead = tr[0];
+        t->tuning.l1_ahead = tr[1];
+        clear_graphs(t);
+        for (int i = 0; i < 2; i++) FS_TRY(one_step(t, 0.0f, &st));
+        for (int i = 0; i < 4; i++) {
+            FS_TRY(one_step(t, 0.0f, &st));
+            l1_sum[tr[1]] += t->phase_ms[1];
+            l1_cnt[tr[1]]++;
+            if (st.iterations > 1) {
+                pi_sum[tr[0]] += t->phase_ms[3] / (st.iterations - 1);
+                pi_cnt[tr[0]]++;
+            }
+        }
+    }
+    int best_l1 = c->tuning.l1_ahead, best_pi = c->tuning.pressure_ahead;
+    double t_l1 = 1e30, t_pi = 1e30;
+    for (int a = 1; a <= kMaxAhead; a++) {
+        if (l1_cnt[a]) {
+            out->first_loop_ms[a - 1] = (float)(l1_sum[a] / l1_cnt[a]);
+            if (l1_sum[a] / l1_cnt[a] < t_l1) t_l1 = l1_sum[a] / l1_cnt[a], best_l1 = a;
+        }
+        if (pi_cnt[a]) {
+            out->pressure_iteration_ms[a - 1] = (float)(pi_sum[a] / pi_cnt[a]);
+            if (pi_sum[a] / pi_cnt[a] < t_pi) t_pi = pi_sum[a] / pi_cnt[a], best_pi = a;
+        }
+    }
+    out->tuned = 1;
+    out->first_loop_prefetch = best_l1;
+    out->pressure_prefetch = best_pi;
+    return fs_set_tuning(c, out);
+}
+
+fs_status fs_set_tuning(fs_ctx* c, const fs_tuning* in) {
+    if (!c || !in) return fail(FS_ERR_INVALID, "null argument");
+    if (in->first_loop_prefetch < 1 || in->first_loop_prefetch > kMaxAhead || in->pressure_prefetch < 1 ||
+        in->pressure_prefetch > kMaxAhead)
+        return fail(FS_ERR_INVALID, "prefetch depths must be in 1.." + std::to_string(kMaxAhead));
+    if (c->tuning.l1_ahead != in->first_loop_prefetch || c->tuning.pressure_ahead != in->pressure_prefetch) {
+        FS_CUDA(cudaSetDevice(c->device));
+        if (c->stream) FS_CUDA(cudaStreamSynchronize(c->stream));
+        clear_graphs(c);   // the captured steps launch the old instantiations
+        c->tuning.l1_ahead = in->first_loop_prefetch;
+        c->tuning.pressure_ahead = in->pressure_prefetch;
+    }
     return FS_OK;
 }
 

@@ -45,6 +45,7 @@ struct fs_ctx {
     bool sort_lists_by_host = false;  // quadratic list order (reference-order mode)
     int ns_owner_mode = 0;          // 0 all in structure, 1 fluid only, 2 active only
     int precision = FS_PRECISION_FP32_KAHAN;
+    fsb::TileTuning tuning;         // prefetch depths of the tile passes (fs_autotune)
     size_t real_size = 4;
 
     // derived constants (float, computed exactly as the reference does)

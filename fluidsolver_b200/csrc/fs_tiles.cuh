@@ -509,11 +509,16 @@ __device__ __forceinline__ void walk_tile_list(const TileLists& T, const TileSla
     }
 }
 
-// octets a pass loads ahead of the one it visits (measured on the 1M dam):
-// the pressure passes hide more latency with 3; the loops, with more work per
-// entry and more registers, do best with 1
-constexpr int kLoopAhead = 1;
-constexpr int kPressureAhead = 3;
+// Octets a pass loads ahead of the one it visits. The first loop's and the
+// pressure passes' depths are chosen per context by fs_autotune among
+// 1..kMaxAhead (defaults: what the 1M dam preferred on a B200, 1 and 3); the
+// second loop walks its staged slab with 1.
+constexpr int kMaxAhead = 4;
+constexpr int kL2Ahead = 1;
+struct TileTuning {
+    int l1_ahead = 1;
+    int pressure_ahead = 3;
+};
 
 // the slab after a pass's staged candidates (bytes_per_candidate each)
 __device__ __forceinline__ TileSlab slab_at(float4* smem, int bytes_per_candidate, int K) {
@@ -586,6 +591,7 @@ struct FastSpline {
 // first loop. Blocks [0, n_tiles) are tiles of fluid owners; the blocks after
 // them take the boundary and inactive particles [n_fluid, n), which need no
 // neighbor sums.
+template <int AHEAD>
 __global__ void __launch_bounds__(kPassThreads, kL1GlobalEntries ? 4 : 3) k_tile_iisph3d_l1(int64_t n_fluid, int64_t n, int64_t n_tiles,
                                                                   State<float> s, TileLists T, Lists L,
                                                                   SolverConsts<float> c,
@@ -631,7 +637,7 @@ __global__ void __launch_bounds__(kPassThreads, kL1GlobalEntries ? 4 : 3) k_tile
     V3<float> vpart = v3<float>(0.f, 0.f, 0.f);
     float rpart = 0.f;
     const float gb = c.single_layer ? c.gamma1 : 1.f;
-    if (valid) walk_tile_list<kL1GlobalEntries, false, kLoopAhead>(T, slab, k, cnt, half, [&](uint32_t off, bool bnd) {
+    if (valid) walk_tile_list<kL1GlobalEntries, false, AHEAD>(T, slab, k, cnt, half, [&](uint32_t off, bool bnd) {
         const float4 pj = at_offset(sp, off), vj = at_offset(sv, off);
         const float rj = at_offset(sr, off >> 2);
         const V3<float> xij = sub3(pk, pj);
@@ -706,7 +712,7 @@ __global__ void __launch_bounds__(kPassThreads, kL2GlobalEntries ? 4 : 3) k_tile
     float cpart = 0.f, g2part = 0.f;
     V3<float> mpart = v3<float>(0.f, 0.f, 0.f), bpart = v3<float>(0.f, 0.f, 0.f);
     const float wb = c.single_layer ? c.two_gamma : 2.f;
-    if (valid) walk_tile_list<kL2GlobalEntries, false, kLoopAhead>(T, slab, k, cnt, half, [&](uint32_t off, bool bnd) {
+    if (valid) walk_tile_list<kL2GlobalEntries, false, kL2Ahead>(T, slab, k, cnt, half, [&](uint32_t off, bool bnd) {
         const float4 pj = at_offset(sp, off), vsj = at_offset(sa, off);
         const V3<float> xij = sub3(pk, pj);
         const float r2 = r2_of(xij);
@@ -743,6 +749,7 @@ __global__ void __launch_bounds__(kPassThreads, kL2GlobalEntries ? 4 : 3) k_tile
 }
 
 // iteration (a): pressure acceleration
+template <int AHEAD>
 __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) k_tile_iisph3d_pressure_acc(int64_t n_fluid, State<float> s,
                                                                             TileLists T, Lists L,
                                                                             SolverConsts<float> c,
@@ -791,7 +798,7 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
         pa.add(part);
         part = v3<float>(0.f, 0.f, 0.f);
     };
-    if (valid) walk_tile_list<kPressureGlobalEntries, true, kPressureAhead>(T, slab, k, cnt, half, pair, flush);
+    if (valid) walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, pair, flush);
     const V3<float> a = pair_total(pa);
     if (half || !valid) return;
     // boundary: - sum_bnd (lambda m_j p_i / rho0^2) gradW, lambda = 2 gamma (single layer) or 2
@@ -800,6 +807,7 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
 }
 
 // iteration (b): A p, relaxed Jacobi update, density error, fused scan
+template <int AHEAD>
 __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) k_tile_iisph3d_pressure_update(int64_t n_fluid, State<float> s,
                                                                                TileLists T, Lists L,
                                                                                SolverConsts<float> c,
@@ -848,7 +856,7 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
                 ap.add(part);
                 part = 0.f;
             };
-            if (valid) walk_tile_list<kPressureGlobalEntries, true, kPressureAhead>(T, slab, k, cnt, half, pair, flush);
+            if (valid) walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, pair, flush);
             // boundary: sum_bnd m_j dot(a_i, gradW) = dot(a_i, sum_bnd m_j gradW)
             const float sum = pair_total(ap) + dot3(v3<float>(ak.x, ak.y, ak.z), v3<float>(gbk.x, gbk.y, gbk.z));
             if (!half && valid)
@@ -893,18 +901,34 @@ __global__ void k_export_solver_lists(int64_t n_owners, bool tiled, TileLists T,
     }
 }
 
-inline cudaError_t set_tile_pass_smem(int K) {
-    cudaError_t e = cudaFuncSetAttribute(k_tile_iisph3d_l1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+// the instantiation of a tuned kernel for a prefetch depth in 1..kMaxAhead
+#define FSB_AHEAD_SWITCH(ahead, KERNEL, ...)       \
+    switch (ahead) {                                  \
+        case 1: KERNEL<1> __VA_ARGS__; break;         \
+        case 2: KERNEL<2> __VA_ARGS__; break;         \
+        case 3: KERNEL<3> __VA_ARGS__; break;         \
+        default: KERNEL<kMaxAhead> __VA_ARGS__; break; \
+    }
+
+template <int AHEAD> inline cudaError_t set_tuned_pass_smem(int K) {
+    cudaError_t e = cudaFuncSetAttribute(k_tile_iisph3d_l1<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)tile_pass_smem(36, K, !kL1GlobalEntries));
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_tile_iisph3d_l2, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tile_pass_smem(32, K, !kL2GlobalEntries));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_acc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_acc<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)tile_pass_smem(20, K, !kPressureGlobalEntries));
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_update<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)tile_pass_smem(32, K, !kPressureGlobalEntries));
+    return e;
+}
+
+inline cudaError_t set_tile_pass_smem(int K) {
+    cudaError_t e = cudaFuncSetAttribute(k_tile_iisph3d_l2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)tile_pass_smem(32, K, !kL2GlobalEntries));
+    if (e == cudaSuccess) e = set_tuned_pass_smem<1>(K);
+    if (e == cudaSuccess) e = set_tuned_pass_smem<2>(K);
+    if (e == cudaSuccess) e = set_tuned_pass_smem<3>(K);
+    if (e == cudaSuccess) e = set_tuned_pass_smem<kMaxAhead>(K);
     return e;
 }
 

@@ -198,6 +198,12 @@ def write_particles(path: str, col: "ParticleCollection") -> None:
     F.check(F.lib().fs_particles_file_write(str(path).encode(), c.dim, ctypes.byref(c.as_fs())))
 
 
+def _tuning_dict(t) -> dict:
+    return {"tuned": bool(t.tuned), "first_loop_prefetch": t.first_loop_prefetch,
+            "pressure_prefetch": t.pressure_prefetch, "first_loop_ms": list(t.first_loop_ms),
+            "pressure_iteration_ms": list(t.pressure_iteration_ms)}
+
+
 class BoundaryPreprocessor:
     """entities/BoundaryPreprocessor.hpp: an entity that runs before the solver and sets the mass of
     every boundary particle from its boundary neighbors. This one runs on the device state of
@@ -412,6 +418,17 @@ class FluidSolverBase:
         F.check(F.lib().fs_global_statistics(self.ctx, float(zero_height), ctypes.byref(st)))
         return {name: getattr(st, name) for name, _ in st._fields_ if name != "reserved"}
 
+    def autotune(self) -> dict:
+        """Chooses the tile passes' prefetch depths by timing steps on a copy of this solver's device
+        context (fs_autotune); this solver's state is left as it was."""
+        t = F.FsTuning()
+        F.check(F.lib().fs_autotune(self.ctx, ctypes.byref(t)))
+        return _tuning_dict(t)
+
+    def set_tuning(self, first_loop_prefetch: int, pressure_prefetch: int) -> None:
+        t = F.FsTuning(first_loop_prefetch=first_loop_prefetch, pressure_prefetch=pressure_prefetch)
+        F.check(F.lib().fs_set_tuning(self.ctx, ctypes.byref(t)))
+
     def dump(self, path: str) -> None:
         """The device state as a particle file (fs_dump), FluidConsole's particle dump."""
         F.check(F.lib().fs_dump(self.ctx, str(path).encode()))
@@ -513,6 +530,12 @@ class BatchedIISPHFluidSolver3D:
         self.offsets = np.concatenate([[0], np.cumsum([len(c) for c in self.scenes])]).astype(np.int64)
         self._ctx = None
         self.last_stats = None
+
+    def set_tuning(self, first_loop_prefetch: int, pressure_prefetch: int) -> None:
+        """Prefetch depths of the tile passes, e.g. as IISPHFluidSolver3D.autotune() chose them on a
+        representative scene (fs_set_tuning)."""
+        t = F.FsTuning(first_loop_prefetch=first_loop_prefetch, pressure_prefetch=pressure_prefetch)
+        F.check(F.lib().fs_set_tuning(self.ctx, ctypes.byref(t)))
 
     @property
     def timestep_generator(self):

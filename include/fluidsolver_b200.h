@@ -270,6 +270,26 @@ void* fs_stream(fs_ctx* ctx);
  * (library kernels such as the radix sort's are not counted). */
 int64_t fs_launch_count(fs_ctx* ctx);
 
+/* ---- tuning ------------------------------------------------------------------
+ * How far ahead the 3D IISPH fast mode's tile passes load their neighbor lists
+ * (octets of 8 entries; 1..4). No reference counterpart: the reference's
+ * loops have nothing to tune. fs_autotune times whole steps with each choice
+ * on a copy of the context (same parameters and particles; the context's own
+ * state is left as it was), keeps the fastest for the context and reports the
+ * times. It allocates a second set of device buffers while it runs. Contexts
+ * whose passes are not tiled report tuned = 0. A batched context takes the
+ * result of a representative single scene through fs_set_tuning. */
+typedef struct fs_tuning {
+    int32_t tuned;                   /* 1 if fs_autotune measured */
+    int32_t first_loop_prefetch;     /* the depths in use */
+    int32_t pressure_prefetch;
+    int32_t reserved;
+    float first_loop_ms[4];          /* measured per depth 1..4 (0: not tried) */
+    float pressure_iteration_ms[4];  /* per pressure iteration, per depth 1..4 */
+} fs_tuning;
+fs_status fs_autotune(fs_ctx* ctx, fs_tuning* out);
+fs_status fs_set_tuning(fs_ctx* ctx, const fs_tuning* in);
+
 /* ---- entities and sensors on the device -----------------------------------
  * Host-side entities and sensors of the Simulator read the whole collection;
  * these run their arithmetic where the state lives, so that a step loop that

@@ -45,7 +45,8 @@ def test_abi_version(L):
 def test_structs_match_the_header(tmp_path):
     """The ctypes mirrors have the C compiler's layout of the header's structs."""
     src = tmp_path / "layout.c"
-    classes = {"fs_params": F.FsParams, "fs_step_stats": F.FsStepStats, "fs_global_stats": F.FsGlobalStats}
+    classes = {"fs_params": F.FsParams, "fs_step_stats": F.FsStepStats, "fs_global_stats": F.FsGlobalStats,
+               "fs_tuning": F.FsTuning}
     fields = {name: [f[0] for f in cls._fields_] for name, cls in classes.items()}
     lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "fluidsolver_b200.h"', "int main(void) {"]
     for st, names in fields.items():
