@@ -65,7 +65,7 @@ EXPORTED_SYMBOLS = (
     "fs_run", "fs_last_phase_times", "fs_stream", "fs_launch_count", "fs_batch_create", "fs_batch_run",
     "fs_query_position_noalloc", "fs_get_solver_lists_csr", "fs_boundary_preprocess", "fs_global_statistics",
     "fs_particles_file_info", "fs_particles_file_read", "fs_particles_file_write", "fs_dump",
-    "fs_autotune", "fs_set_tuning",
+    "fs_autotune", "fs_set_tuning", "fs_trace_rays", "fs_render_settings_default", "fs_render",
 )
 
 
@@ -121,6 +121,17 @@ class FsTuning(ctypes.Structure):
     ]
 
 
+class FsCamera(ctypes.Structure):
+    _fields_ = [("position", c_float * 3), ("view_direction", c_float * 3), ("view_up", c_float * 3),
+                ("field_of_view_x", c_float), ("width", c_int32), ("height", c_int32), ("flip_y", c_int32)]
+
+
+class FsRenderSettings(ctypes.Structure):
+    _fields_ = [("samples_per_pixel", c_int32), ("maximum_recursion_depth", c_int32),
+                ("output_normals_of_first_hit", c_int32), ("surface_density_fraction", c_float),
+                ("exposure", c_float), ("gamma", c_float), ("seed", ctypes.c_uint64)]
+
+
 class FluidSolverError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"fluidsolver_b200 status {status}: {message}")
@@ -158,6 +169,10 @@ def lib() -> ctypes.CDLL:
     L.fs_particles_file_write.argtypes = [ctypes.c_char_p, c_int32, POINTER(FsParticles)]
     L.fs_dump.argtypes = [ctx_p, ctypes.c_char_p]
     L.fs_autotune.argtypes = [ctx_p, POINTER(FsTuning)]
+    L.fs_trace_rays.argtypes = [ctx_p, c_float, c_int64] + [c_void_p] * 6
+    L.fs_render_settings_default.argtypes = [POINTER(FsRenderSettings)]
+    L.fs_render_settings_default.restype = None
+    L.fs_render.argtypes = [ctx_p, POINTER(FsCamera), POINTER(FsRenderSettings), c_void_p, c_void_p]
     L.fs_set_tuning.argtypes = [ctx_p, POINTER(FsTuning)]
     L.fs_global_statistics.argtypes = [ctx_p, c_float, POINTER(FsGlobalStats)]
     L.fs_query_position.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
@@ -176,7 +191,8 @@ def lib() -> ctypes.CDLL:
                  "fs_get_neighbors_csr", "fs_query_position", "fs_solve_step", "fs_step", "fs_run", "fs_last_phase_times",
                  "fs_batch_create", "fs_batch_run", "fs_query_position_noalloc", "fs_get_solver_lists_csr",
                  "fs_boundary_preprocess", "fs_global_statistics", "fs_particles_file_info",
-                 "fs_particles_file_read", "fs_particles_file_write", "fs_dump", "fs_autotune", "fs_set_tuning"):
+                 "fs_particles_file_read", "fs_particles_file_write", "fs_dump", "fs_autotune", "fs_set_tuning",
+                 "fs_trace_rays", "fs_render"):
         getattr(L, name).restype = c_int32
     _lib = L
     return L

@@ -19,6 +19,7 @@
 #include "fs_solvers.cuh"
 #include "fs_entities.cuh"
 #include "fs_io.hpp"
+#include "fs_render.cuh"
 
 using namespace fsb;
 
@@ -1971,6 +1972,179 @@ fs_status fs_set_tuning(fs_ctx* c, const fs_tuning* in) {
         clear_graphs(c);   // the captured steps launch the old instantiations
         c->tuning.l1_ahead = in->first_loop_prefetch;
         c->tuning.pressure_ahead = in->pressure_prefetch;
+    }
+    return FS_OK;
+}
+
+// the render scene of a 3D single-scene context: a fresh search (the cell
+// tables of the current positions) and the particles' box
+static fs_status render_scene_of(fs_ctx* c, float surface_fraction, RenderScene& rs) {
+    if (c->dim != 3) return fail(FS_ERR_INVALID, "the ray tracer renders 3D particles (MovementData3D)");
+    if (c->scenes > 0) return fail(FS_ERR_INVALID, "not available on batched contexts");
+    if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
+    if (!(surface_fraction > 0.0f)) return fail(FS_ERR_INVALID, "the surface density fraction must be positive");
+    FS_CUDA(cudaSetDevice(c->device));
+    FS_TRY(search_for_step(c, c->prm.timestep));
+    int* d_box = nullptr;
+    FS_TRY(dalloc(&d_box, 6));
+    const int init[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
+    int box[6];
+    cudaError_t e = cudaMemcpyAsync(d_box, init, sizeof(init), cudaMemcpyHostToDevice, c->stream);
+    c->launches++;
+    if (e == cudaSuccess) {
+        if (c->precision == FS_PRECISION_FP64)
+            k_particle_box<double><<<grid_for(c->n), kBlock, 0, c->stream>>>(c->n, state_of<double>(c), d_box);
+        else
+            k_particle_box<float><<<grid_for(c->n), kBlock, 0, c->stream>>>(c->n, state_of<float>(c), d_box);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(box, d_box, sizeof(box), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_box);
+    if (e != cudaSuccess) return fail(FS_ERR_CUDA, std::string("particle box: ") + cudaGetErrorString(e));
+    auto unord = [](int i) {
+        const int b = i >= 0 ? i : i ^ 0x7fffffff;
+        float f;
+        std::memcpy(&f, &b, sizeof(f));
+        return f;
+    };
+    const float ext = c->prm.particle_size * 2.0f;   // extended_in_all_directions_by(size * support factor)
+    for (int a = 0; a < 3; a++) {
+        rs.box_min[a] = box[a] == INT_MAX ? 0.0f : unord(box[a]) - ext;
+        rs.box_max[a] = box[3 + a] == INT_MIN ? -1.0f : unord(box[3 + a]) + ext;
+    }
+    rs.step = c->prm.particle_size / 2.0f;
+    rs.iso = surface_fraction * c->prm.rest_density;
+    rs.kern.h = c->kernel_h;
+    rs.kern.alpha = c->kernel_alpha;
+    rs.kern.inv_h = 1.0f / c->kernel_h;
+    rs.kern.alpha_h = c->kernel_alpha * c->kernel_h;
+    rs.w = walk_of(c, false);
+    return FS_OK;
+}
+
+fs_status fs_trace_rays(fs_ctx* c, float surface_fraction, int64_t n, const float* origins, const float* directions,
+                        int32_t* hit, float* point, float* normal, float* length) {
+    if (!c || (n > 0 && (!origins || !directions || !hit || !point || !normal || !length)))
+        return fail(FS_ERR_INVALID, "null argument");
+    if (n < 0) return fail(FS_ERR_INVALID, "negative ray count");
+    RenderScene rs;
+    FS_TRY(render_scene_of(c, surface_fraction, rs));
+    if (n == 0) return FS_OK;
+    float *d_in = nullptr, *d_out = nullptr;
+    int32_t* d_hit = nullptr;
+    FS_TRY(dalloc(&d_in, (size_t)n * 6));
+    if (dalloc(&d_out, (size_t)n * 7) != FS_OK || dalloc(&d_hit, (size_t)n) != FS_OK) {
+        cudaFree(d_in);
+        cudaFree(d_out);
+        return fail(FS_ERR_CUDA, "allocation for the rays failed");
+    }
+    cudaStream_t st = c->stream;
+    cudaError_t e = cudaMemcpyAsync(d_in, origins, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_in + 3 * n, directions, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        c->launches++;
+        if (c->precision == FS_PRECISION_FP64)
+            k_trace_rays<double><<<grid_for(n), kBlock, 0, st>>>(n, d_in, d_in + 3 * n, state_of<double>(c),
+                                                                 c->cell_start, rs, d_hit, d_out, d_out + 3 * n,
+                                                                 d_out + 6 * n);
+        else
+            k_trace_rays<float><<<grid_for(n), kBlock, 0, st>>>(n, d_in, d_in + 3 * n, state_of<float>(c),
+                                                                c->cell_start, rs, d_hit, d_out, d_out + 3 * n,
+                                                                d_out + 6 * n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hit, d_hit, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(point, d_out, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(normal, d_out + 3 * n, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(length, d_out + 6 * n, sizeof(float) * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d_in);
+    cudaFree(d_out);
+    cudaFree(d_hit);
+    if (e != cudaSuccess) return fail(FS_ERR_CUDA, std::string("ray tracing: ") + cudaGetErrorString(e));
+    return FS_OK;
+}
+
+void fs_render_settings_default(fs_render_settings* r) {
+    if (!r) return;
+    *r = fs_render_settings{};
+    r->samples_per_pixel = 50;         // Camera::SampleSettings (Camera.hpp:23-26)
+    r->maximum_recursion_depth = 10;   // FluidRaytracer3D::Settings (FluidRaytracer3D.hpp:22-25)
+    r->output_normals_of_first_hit = 0;
+    r->surface_density_fraction = 0.8f;   // ParticleIntersectionAccelerator.hpp:20
+    r->exposure = 0.2f;                   // ToneMapper::ToneMapperSettings (ToneMapper.hpp:11-20)
+    r->gamma = 2.2f;
+    r->seed = 1;
+}
+
+fs_status fs_render(fs_ctx* c, const fs_camera* cam, const fs_render_settings* r, float* radiance, uint8_t* rgba) {
+    if (!c || !cam || !r || !radiance) return fail(FS_ERR_INVALID, "null argument");
+    if (cam->width <= 0 || cam->height <= 0 || (int64_t)cam->width * cam->height > (int64_t)1 << 26)
+        return fail(FS_ERR_INVALID, "image size out of range");
+    if (r->samples_per_pixel <= 0 || r->maximum_recursion_depth < 0) return fail(FS_ERR_INVALID, "bad settings");
+    RenderScene rs;
+    FS_TRY(render_scene_of(c, r->surface_density_fraction, rs));
+    // the camera: glm::lookAt's basis (Camera.cpp:41-44); the ray direction is the inverse view
+    // rotation applied to the pixel's view-space direction
+    RenderCamera rc{};
+    const float* f0 = cam->view_direction;
+    const float fl = std::sqrt(f0[0] * f0[0] + f0[1] * f0[1] + f0[2] * f0[2]);
+    const float f[3] = {f0[0] / fl, f0[1] / fl, f0[2] / fl};
+    const float* up = cam->view_up;
+    float sv[3] = {f[1] * up[2] - f[2] * up[1], f[2] * up[0] - f[0] * up[2], f[0] * up[1] - f[1] * up[0]};
+    const float sl = std::sqrt(sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2]);
+    if (!(sl > 0.0f) || !(fl > 0.0f)) return fail(FS_ERR_INVALID, "view direction and up vector must span a plane");
+    for (int a = 0; a < 3; a++) sv[a] /= sl;
+    const float uv[3] = {sv[1] * f[2] - sv[2] * f[1], sv[2] * f[0] - sv[0] * f[2], sv[0] * f[1] - sv[1] * f[0]};
+    for (int a = 0; a < 3; a++) {
+        rc.pos[a] = cam->position[a];
+        rc.right[a] = sv[a];
+        rc.up[a] = uv[a];
+        rc.back[a] = -f[a];
+    }
+    rc.tan_half_fov = std::tan(cam->field_of_view_x / 2.0f);
+    rc.width = cam->width;
+    rc.height = cam->height;
+    rc.flip_y = cam->flip_y;
+    RenderShading sh{};
+    const float pi = 3.14159265358979323846f;
+    const float fc[3] = {0.1f, 0.15f, 0.5f}, bc[3] = {0.0f, 0.42f, 0.063f};   // FluidRaytracer3D.cpp:183-184
+    for (int a = 0; a < 3; a++) {
+        sh.fluid[a] = std::pow(fc[a], 2.2f) * (1.0f / pi);
+        sh.boundary[a] = std::pow(bc[a], 2.2f) * (1.0f / pi);
+    }
+    sh.samples = r->samples_per_pixel;
+    sh.max_depth = r->maximum_recursion_depth;
+    sh.normals_only = r->output_normals_of_first_hit != 0;
+    sh.seed = r->seed;
+    const int64_t np = (int64_t)cam->width * cam->height;
+    float* d_rad = nullptr;
+    FS_TRY(dalloc(&d_rad, (size_t)np * 3));
+    c->launches++;
+    if (c->precision == FS_PRECISION_FP64)
+        k_render<double><<<grid_for(np), kBlock, 0, c->stream>>>(state_of<double>(c), c->cell_start, rs, rc, sh, d_rad);
+    else
+        k_render<float><<<grid_for(np), kBlock, 0, c->stream>>>(state_of<float>(c), c->cell_start, rs, rc, sh, d_rad);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(radiance, d_rad, sizeof(float) * 3 * np, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_rad);
+    if (e != cudaSuccess) return fail(FS_ERR_CUDA, std::string("rendering: ") + cudaGetErrorString(e));
+    if (rgba) {   // ToneMapper::map_radiance_to_image_color (ToneMapper.cpp:79-102), exponential curve
+        auto byte = [](float v) { return (uint8_t)((v < 0.0f ? 0.0f : v > 1.0f ? 1.0f : v) * 255.0f); };
+        for (int64_t i = 0; i < np; i++) {
+            for (int a = 0; a < 3; a++) {
+                float v = radiance[3 * i + a] * r->exposure;
+                v = 1.0f - std::exp(-v);
+                v = v < 0.0f ? 0.0f : v > 1.0f ? 1.0f : v;
+                v = std::pow(v, 1.0f / r->gamma);
+                rgba[4 * i + a] = byte(v);
+            }
+            rgba[4 * i + 3] = 255;
+        }
     }
     return FS_OK;
 }

@@ -429,6 +429,39 @@ class FluidSolverBase:
         t = F.FsTuning(first_loop_prefetch=first_loop_prefetch, pressure_prefetch=pressure_prefetch)
         F.check(F.lib().fs_set_tuning(self.ctx, ctypes.byref(t)))
 
+    # ---- the fluid path tracer (visualizer/raytracer/FluidRaytracer3D) ----
+    def trace_rays(self, origins, directions, surface_density_fraction: float = 0.8) -> dict:
+        """First surface hits of rays through the SPH density (fs_trace_rays): hit (-1 none, 0/1 the
+        fluid surface from outside/inside, 2 a boundary), point, normal, length."""
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(directions, np.float32).reshape(-1, 3)
+        m = len(o)
+        out = {"hit": np.zeros(m, np.int32), "point": np.zeros((m, 3), np.float32),
+               "normal": np.zeros((m, 3), np.float32), "length": np.zeros(m, np.float32)}
+        F.check(F.lib().fs_trace_rays(self.ctx, float(surface_density_fraction), m, o.ctypes.data, d.ctypes.data,
+                                      out["hit"].ctypes.data, out["point"].ctypes.data, out["normal"].ctypes.data,
+                                      out["length"].ctypes.data))
+        return out
+
+    def render(self, position, view_direction, view_up=(0.0, 1.0, 0.0), width: int = 320, height: int = 240,
+               field_of_view_x: float = 90.0 / 360.0 * 2.0 * 3.1415, flip_y: bool = False, **settings):
+        """FluidRaytracer3D::render on the device state (fs_render): (radiance, rgba) arrays of
+        height x width x 3 floats and x 4 bytes. settings: samples_per_pixel, maximum_recursion_depth,
+        output_normals_of_first_hit, surface_density_fraction, exposure, gamma, seed."""
+        cam = F.FsCamera()
+        cam.position[:], cam.view_direction[:], cam.view_up[:] = position, view_direction, view_up
+        cam.field_of_view_x, cam.width, cam.height, cam.flip_y = field_of_view_x, width, height, int(flip_y)
+        rs = F.FsRenderSettings()
+        F.lib().fs_render_settings_default(ctypes.byref(rs))
+        for k, v in settings.items():
+            if not hasattr(rs, k):
+                raise TypeError(f"unknown render setting {k!r}")
+            setattr(rs, k, int(v) if isinstance(v, bool) else v)
+        rad = np.zeros((height, width, 3), np.float32)
+        rgba = np.zeros((height, width, 4), np.uint8)
+        F.check(F.lib().fs_render(self.ctx, ctypes.byref(cam), ctypes.byref(rs), rad.ctypes.data, rgba.ctypes.data))
+        return rad, rgba
+
     def dump(self, path: str) -> None:
         """The device state as a particle file (fs_dump), FluidConsole's particle dump."""
         F.check(F.lib().fs_dump(self.ctx, str(path).encode()))

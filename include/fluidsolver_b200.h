@@ -321,6 +321,46 @@ typedef struct fs_global_stats {
 } fs_global_stats;
 fs_status fs_global_statistics(fs_ctx* ctx, float zero_height, fs_global_stats* out);
 
+/* ---- the fluid path tracer ---------------------------------------------------
+ * libFluid's FluidRaytracer3D (visualizer/raytracer/) on the device state of a
+ * 3D single-scene context, rendering into host memory (no window or graphics
+ * API). Both calls first search the current positions; the density at a point
+ * sums the particles within the search radius (ParticleIntersectionAccelerator.cpp:76-126).
+ *
+ * fs_trace_rays: ParticleIntersectionAccelerator::is_intersecting_with_particles
+ * (:20-74) for n rays, without a random offset along them. hit: -1 none, 0 the
+ * fluid surface reached from outside, 1 from inside, 2 a boundary surface;
+ * point, normal (3 floats each) and length (the march distance to the hit). */
+fs_status fs_trace_rays(fs_ctx* ctx, float surface_density_fraction, int64_t n, const float* origins,
+                        const float* directions, int32_t* hit, float* point, float* normal, float* length);
+
+/* Camera::CameraSettings (Camera.hpp:13-21); field_of_view_x in radians. */
+typedef struct fs_camera {
+    float position[3];
+    float view_direction[3];
+    float view_up[3];
+    float field_of_view_x;
+    int32_t width, height;
+    int32_t flip_y;
+} fs_camera;
+typedef struct fs_render_settings {
+    int32_t samples_per_pixel;            /* Camera::SampleSettings::amount_of_samples */
+    int32_t maximum_recursion_depth;      /* FluidRaytracer3D::Settings */
+    int32_t output_normals_of_first_hit;
+    float surface_density_fraction;       /* of the rest density: the surface's iso density */
+    float exposure, gamma;                /* ToneMapper (exponential curve, gamma correction) */
+    uint64_t seed;                        /* of the per-pixel random streams */
+} fs_render_settings;
+void fs_render_settings_default(fs_render_settings* r);
+/* FluidRaytracer3D::render: radiance (width * height * 3 floats, row-major from
+ * the top-left pixel), the path tracer's estimate with a white sky
+ * (FluidRaytracer3D.cpp:70-165; Skybox without an image); rgba (width * height
+ * * 4 bytes, may be NULL): the tone-mapped image (ToneMapper.cpp:79-102). The
+ * random numbers come from per-pixel streams, so images match the reference's
+ * in distribution, not value by value. */
+fs_status fs_render(fs_ctx* ctx, const fs_camera* cam, const fs_render_settings* settings, float* radiance,
+                    uint8_t* rgba);
+
 /* ---- particle files ---------------------------------------------------------
  * ParticleSerializer's version-1 files (ParticleSerializer.cpp:41-141): the
  * scenario particle files (scenarios/** / *.data) and FluidConsole's particle

@@ -29,6 +29,7 @@
 #include "time/ConstantTimestepGenerator.hpp"
 #include "time/DynamicCflTimestepGenerator.hpp"
 #include "entities/BoundaryPreprocessor.hpp"
+#include "visualizer/raytracer/ParticleIntersectionAccelerator.hpp"
 
 #include <algorithm>
 #include <cstdint>
@@ -417,6 +418,44 @@ int ref_boundary_preprocess(void* h, const float* mass, float particle_size, flo
         return -1;
     }
     for (size_t i = 0; i < c.size(); i++) out[c.get<ParticleInfo>(i).tag] = c.get<ParticleData>(i).mass;
+    return 0;
+}
+
+// ParticleIntersectionAccelerator::is_intersecting_with_particles
+// (ParticleIntersectionAccelerator.cpp:20-74) after prepare() (:8-18), without
+// a sampler (no random offset along the ray): for each ray the hit type (-1:
+// none; 0/1: the fluid surface from outside/inside; 2: a boundary surface),
+// the point and normal of the intersection and length_until_hit.
+int ref_trace_rays(int64_t n, const float* pos, const float* mass, const uint8_t* type, float particle_size,
+                   float rest_density, int64_t nrays, const float* origins, const float* directions, int32_t* hit,
+                   float* point, float* normal, float* length) {
+    try {
+        auto c = std::make_shared<ParticleCollection>();
+        fill_collection(*c, 3, n, pos, type);
+        for (size_t i = 0; i < c->size(); i++) c->get<ParticleData>(i).mass = mass[c->get<ParticleInfo>(i).tag];
+        Raytracer::ParticleIntersectionAccelerator acc;
+        acc.particle_collection = c;
+        acc.particle_size = particle_size;
+        acc.rest_density = rest_density;
+        acc.sampler = nullptr;
+        acc.prepare();
+        for (int64_t r = 0; r < nrays; r++) {
+            Raytracer::Ray ray;
+            ray.starting_point = glm::vec3(origins[3 * r], origins[3 * r + 1], origins[3 * r + 2]);
+            ray.normalized_direction = glm::vec3(directions[3 * r], directions[3 * r + 1], directions[3 * r + 2]);
+            Raytracer::IntersectionResult res{};
+            const bool h = acc.is_intersecting_with_particles(ray, res);
+            hit[r] = h ? (int32_t)res.intersection_result_type : -1;
+            for (int a = 0; a < 3; a++) {
+                point[3 * r + a] = h ? res.point_of_intersection[a] : 0.0f;
+                normal[3 * r + a] = h ? res.normal_at_intersection[a] : 0.0f;
+            }
+            length[r] = h ? ray.length_until_hit : -1.0f;
+        }
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
     return 0;
 }
 

@@ -42,6 +42,7 @@ def lib(variant: str = "serial") -> ctypes.CDLL:
     L.ref_dynamic_timestep.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_void_p] + [c_float] * 5
     L.ref_dynamic_timestep.restype = c_float
     L.ref_boundary_preprocess.argtypes = [c_void_p, c_void_p, c_float, c_float, c_void_p]
+    L.ref_trace_rays.argtypes = [c_int64, c_void_p, c_void_p, c_void_p, c_float, c_float, c_int64] + [c_void_p] * 6
     L.ref_ns_create.restype = c_void_p
     L.ref_ns_create.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_float]
     L.ref_ns_destroy.argtypes = [c_void_p]
@@ -90,6 +91,20 @@ def dynamic_timestep(vel, acc, type_, particle_size, min_ts, max_ts, lambda_v, l
     type_ = np.ascontiguousarray(type_, np.uint8)
     return lib().ref_dynamic_timestep(vel.shape[1], len(vel), _p(vel), _p(acc), _p(type_), particle_size, min_ts,
                                       max_ts, lambda_v, lambda_a)
+
+
+def trace_rays(pos, mass, type_, particle_size, rest_density, origins, directions) -> dict:
+    """ParticleIntersectionAccelerator's first hits (no random offset along the rays)."""
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+    pos, mass, o, d = f(pos), f(mass), f(origins), f(directions)
+    t = np.ascontiguousarray(type_, np.uint8)
+    m = len(o)
+    out = {"hit": np.zeros(m, np.int32), "point": np.zeros((m, 3), np.float32),
+           "normal": np.zeros((m, 3), np.float32), "length": np.zeros(m, np.float32)}
+    if lib().ref_trace_rays(len(pos), _p(pos), _p(mass), _p(t), particle_size, rest_density, m, _p(o), _p(d),
+                            _p(out["hit"]), _p(out["point"]), _p(out["normal"]), _p(out["length"])) != 0:
+        raise RuntimeError(lib().ref_last_error().decode())
+    return out
 
 
 class RefSearch:

@@ -124,6 +124,42 @@ def boundary_fixture():
     np.savez_compressed(os.path.join(OUT, "boundary.npz"), **out)
 
 
+def camera_rays(position, target, width, height, fov_x=np.pi / 2):
+    """Pinhole rays through pixel centres (the construction of Camera.cpp:10-39, y flipped)."""
+    f = np.asarray(target, np.float64) - position
+    f /= np.linalg.norm(f)
+    up = np.array([0.0, 1.0, 0.0])
+    s = np.cross(f, up)
+    s /= np.linalg.norm(s)
+    u = np.cross(s, f)
+    x, y = np.meshgrid((np.arange(width) + 0.5) / width * 2 - 1, -((np.arange(height) + 0.5) / height * 2 - 1))
+    t = np.tan(fov_x / 2)
+    d = x[..., None] * t * s + y[..., None] * t * u + f
+    d /= np.linalg.norm(d, axis=-1, keepdims=True)
+    o = np.broadcast_to(np.asarray(position, np.float64), d.shape)
+    return o.reshape(-1, 3).astype(np.float32), d.reshape(-1, 3).astype(np.float32)
+
+
+def raytrace_fixture():
+    """ParticleIntersectionAccelerator (ParticleIntersectionAccelerator.cpp:8-206): first hits of camera
+    rays on a breaking dam in a tank (fluid from outside, walls, misses) and of rays that start inside
+    the fluid (the surface from inside)."""
+    sc = scenes.breaking_dam_3d(12, 10, 8, 1.0, tank=(24, 16, 14), seed=51, layers=2)
+    col = sc.collection
+    pos, mass, typ = col.position.astype(np.float32), col.mass.astype(np.float32), col.type.astype(np.uint8)
+    o1, d1 = camera_rays((30.0, 18.0, 28.0), (6.0, 4.0, 4.0), 48, 36, fov_x=0.7)
+    o3, d3 = camera_rays((6.5, 30.0, 5.5), (6.0, 4.0, 4.0), 32, 32, fov_x=0.9)   # from above the open tank
+    rng = np.random.default_rng(52)
+    fl = pos[typ == 0]
+    o2 = fl[rng.choice(len(fl), 200, replace=False)] + rng.uniform(-0.3, 0.3, (200, 3)).astype(np.float32)
+    d2 = rng.standard_normal((200, 3))
+    d2 = (d2 / np.linalg.norm(d2, axis=1, keepdims=True)).astype(np.float32)
+    o, d = np.concatenate([o1, o2, o3]), np.concatenate([d1, d2, d3])
+    res = R.trace_rays(pos, mass, typ, 1.0, 1.0, o, d)
+    np.savez_compressed(os.path.join(OUT, "raytrace.npz"), pos=pos, mass=mass, type=typ, origins=o, directions=d,
+                        **res)
+
+
 def _lists(kind, pos, radius, typ, calls=1, moves=None):
     s = R.RefSearch(kind, pos, radius, typ)
     ok = s.find()
@@ -253,7 +289,7 @@ if __name__ == "__main__":
         sys.exit("oracle/_ref is not built; run `make -C oracle/ref` where the reference checkout is available")
     fixtures = {"kernel": kernel_fixture, "cfl": cfl_fixture, "search": search_fixture, "solvers": solver_fixture,
                 "position_queries": position_query_fixture, "dynamic_timestep": dynamic_timestep_fixture,
-                "boundary": boundary_fixture}
+                "boundary": boundary_fixture, "raytrace": raytrace_fixture}
     for name in sys.argv[1:] or fixtures:
         fixtures[name]()
     for f in sorted(os.listdir(OUT)):

@@ -46,7 +46,7 @@ def test_structs_match_the_header(tmp_path):
     """The ctypes mirrors have the C compiler's layout of the header's structs."""
     src = tmp_path / "layout.c"
     classes = {"fs_params": F.FsParams, "fs_step_stats": F.FsStepStats, "fs_global_stats": F.FsGlobalStats,
-               "fs_tuning": F.FsTuning}
+               "fs_tuning": F.FsTuning, "fs_camera": F.FsCamera, "fs_render_settings": F.FsRenderSettings}
     fields = {name: [f[0] for f in cls._fields_] for name, cls in classes.items()}
     lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "fluidsolver_b200.h"', "int main(void) {"]
     for st, names in fields.items():
