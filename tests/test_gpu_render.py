@@ -2,11 +2,12 @@
 
 Ray queries are compared with the reference's own ParticleIntersectionAccelerator
 (visualizer/raytracer/ParticleIntersectionAccelerator.cpp, compiled in oracle/ref;
-tests/golden/raytrace.npz): the same hit type for at least 99 % of the rays, and
-for those the same march length, the intersection point within 1e-3 and the
-normal within 1e-3. The densities along a ray are float sums over the same
-particles in another order, which moves a hit only where the density at a
-march point lies within rounding of the surface density. The path tracer's
+tests/golden/raytrace.npz): the same hit type for at least 99.5 % of the rays
+(all 2,952 on a B200), and for those the same march length, the intersection
+point within 1e-4 (3.8e-6 measured) and the normal within 1e-5. The densities
+along a ray are float sums over the same particles in another order, which
+moves a hit only where the density at a march point lies within rounding of
+the surface density. The path tracer's
 images are random (the reference draws from per-thread engines in pixel
 order); they are checked for what holds for every sample: the white sky where
 rays miss, radiance below the sky's where they hit, the normal colours of the
@@ -38,13 +39,13 @@ def test_ray_hits_match_the_reference_accelerator(golden):
     s.close()
     want_hit = g["hit"]
     same = got["hit"] == want_hit
-    assert same.mean() >= 0.99, same.mean()
+    assert same.mean() >= 0.995, same.mean()
     assert (want_hit >= 0).sum() > 0.8 * len(want_hit)   # the fixture's rays mostly hit
     both = same & (want_hit >= 0)
-    assert np.mean(got["length"][both] == g["length"][both]) >= 0.99
-    np.testing.assert_allclose(got["point"][both], g["point"][both], atol=1e-3, rtol=0)
+    assert np.mean(got["length"][both] == g["length"][both]) >= 0.995
+    np.testing.assert_allclose(got["point"][both], g["point"][both], atol=1e-4, rtol=0)
     dots = np.sum(got["normal"][both] * g["normal"][both], axis=1)
-    assert np.all(dots > 1 - 1e-3)
+    assert np.all(dots > 1 - 1e-5)
     for t in (0, 1, 2):   # every kind of hit is exercised
         assert np.sum(want_hit == t) >= 5
 
