@@ -451,16 +451,26 @@ struct GlobalEntries {
     }
 };
 
+// The first AHEAD octets (this thread's halves) of an owner's list, loaded
+// before they are walked; octets are read up to `octets`, which may exceed
+// the owner's own list (the planes hold that many octets for every owner of
+// the tile) but never its plane count.
+template <int AHEAD, typename Src>
+__device__ __forceinline__ void load_entry_head(const Src& src, uint32_t octets, int half, uint2 (&ahead)[AHEAD]) {
+#pragma unroll
+    for (int d = 0; d < AHEAD; d++) ahead[d] = (uint32_t)d < octets ? src(d, half) : make_uint2(0u, 0u);
+}
+
 // Visits one half of an owner's list (entries 4 half .. 4 half + 3 of every
 // octet; cnt: the owner's packed list length): f(byte offset into a staged
 // float4 array, boundary) for each, and flush() after every second octet and
 // at the end (where the passes fold their partial sums into the compensated
-// accumulators). The next AHEAD octets are loaded while one is visited.
-// FLUID_ONLY visits the fluid entries, which come first in a list and have
-// the boundary bit clear.
+// accumulators). ahead holds the list's first AHEAD octets (load_entry_head);
+// the next AHEAD octets are loaded while one is visited. FLUID_ONLY visits the
+// fluid entries, which come first in a list and have the boundary bit clear.
 template <bool FLUID_ONLY, int AHEAD, typename Src, typename F, typename Flush>
-__device__ __forceinline__ void for_tile_entries(const Src& src, uint32_t cnt, int K, int half, F&& f,
-                                                 Flush&& flush) {
+__device__ __forceinline__ void for_tile_entries(const Src& src, uint32_t cnt, int K, int half, uint2 (&ahead)[AHEAD],
+                                                 F&& f, Flush&& flush) {
     constexpr int kEntryPrefetch = AHEAD;
     const uint32_t all = min(cnt & 0xffffu, (uint32_t)K);
     const uint32_t n = FLUID_ONLY ? min(cnt >> 16, all) : all;
@@ -469,9 +479,6 @@ __device__ __forceinline__ void for_tile_entries(const Src& src, uint32_t cnt, i
         else f(v & kEntOffset, (v & kEntBoundary) != 0u);
     };
     const uint32_t full = n / 8, octets = (n + 7) / 8;
-    uint2 ahead[kEntryPrefetch];
-#pragma unroll
-    for (int d = 0; d < kEntryPrefetch; d++) ahead[d] = (uint32_t)d < octets ? src(d, half) : make_uint2(0u, 0u);
     uint32_t o = 0;
     for (; o < full; o++) {
         const uint2 cur = ahead[0];
@@ -495,17 +502,31 @@ __device__ __forceinline__ void for_tile_entries(const Src& src, uint32_t cnt, i
     flush();
 }
 
+// The first AHEAD octets of owner k's list in the global octet planes, for
+// a pass that walks them from there (GLOBAL), issued before the tile's
+// staging has landed: the entries do not depend on it. h: the tile's header.
+template <bool GLOBAL, int AHEAD>
+__device__ __forceinline__ void prefetch_tile_list(const TileLists& T, const TileHead& h, int64_t k, int half,
+                                                   uint2 (&ahead)[AHEAD]) {
+    if constexpr (GLOBAL) load_entry_head(GlobalEntries{T.ent + k, T.stride}, h.octets, half, ahead);
+}
+
 // Walks one half of owner k's list (threadIdx.x / 2 within its tile) from
 // the global octet planes (GLOBAL; cnt: the owner's packed list length,
-// loaded by the caller) or from the staged slab.
+// loaded by the caller; ahead: from prefetch_tile_list) or from the staged
+// slab.
 template <bool GLOBAL, bool FLUID_ONLY, int AHEAD, typename F, typename Flush>
 __device__ __forceinline__ void walk_tile_list(const TileLists& T, const TileSlab& slab, int64_t k, uint32_t cnt,
-                                               int half, F&& f, Flush&& flush) {
+                                               int half, uint2 (&ahead)[AHEAD], F&& f, Flush&& flush) {
     if constexpr (GLOBAL) {
-        for_tile_entries<FLUID_ONLY, AHEAD>(GlobalEntries{T.ent + k, T.stride}, cnt, T.K, half, f, flush);
+        for_tile_entries<FLUID_ONLY, AHEAD>(GlobalEntries{T.ent + k, T.stride}, cnt, T.K, half, ahead, f, flush);
     } else {
         const int ol = (int)(threadIdx.x >> 1);
-        for_tile_entries<FLUID_ONLY, AHEAD>(SlabEntries{slab.ent + ol}, slab.count[ol], T.K, half, f, flush);
+        const SlabEntries src{slab.ent + ol};
+        const uint32_t c = slab.count[ol];
+        const uint32_t all = min(c & 0xffffu, (uint32_t)T.K);
+        load_entry_head(src, ((FLUID_ONLY ? min(c >> 16, all) : all) + 7) / 8, half, ahead);
+        for_tile_entries<FLUID_ONLY, AHEAD>(src, c, T.K, half, ahead, f, flush);
     }
 }
 
@@ -630,6 +651,8 @@ __global__ void __launch_bounds__(kPassThreads, kL1GlobalEntries ? 4 : 3) k_tile
     const float4 pk = s.pos[kk], vk = s.vel[kk], ek = s.ext[kk];
     const float dt = sc[s.scene_of(kk)].dt;
     const uint32_t cnt = kL1GlobalEntries ? T.count[kk] : 0u;
+    uint2 ahead[AHEAD];
+    prefetch_tile_list<kL1GlobalEntries>(T, h, k, half, ahead);
     if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     Acc3<float, true> visc;
@@ -637,7 +660,7 @@ __global__ void __launch_bounds__(kPassThreads, kL1GlobalEntries ? 4 : 3) k_tile
     V3<float> vpart = v3<float>(0.f, 0.f, 0.f);
     float rpart = 0.f;
     const float gb = c.single_layer ? c.gamma1 : 1.f;
-    if (valid) walk_tile_list<kL1GlobalEntries, false, AHEAD>(T, slab, k, cnt, half, [&](uint32_t off, bool bnd) {
+    if (valid) walk_tile_list<kL1GlobalEntries, false, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool bnd) {
         const float4 pj = at_offset(sp, off), vj = at_offset(sv, off);
         const float rj = at_offset(sr, off >> 2);
         const V3<float> xij = sub3(pk, pj);
@@ -712,7 +735,8 @@ __global__ void __launch_bounds__(kPassThreads, kL2GlobalEntries ? 4 : 3) k_tile
     float cpart = 0.f, g2part = 0.f;
     V3<float> mpart = v3<float>(0.f, 0.f, 0.f), bpart = v3<float>(0.f, 0.f, 0.f);
     const float wb = c.single_layer ? c.two_gamma : 2.f;
-    if (valid) walk_tile_list<kL2GlobalEntries, false, kL2Ahead>(T, slab, k, cnt, half, [&](uint32_t off, bool bnd) {
+    uint2 ahead[kL2Ahead];
+    if (valid) walk_tile_list<kL2GlobalEntries, false, kL2Ahead>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool bnd) {
         const float4 pj = at_offset(sp, off), vsj = at_offset(sa, off);
         const V3<float> xij = sub3(pk, pj);
         const float r2 = r2_of(xij);
@@ -784,6 +808,8 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
     const float4 pk = s.pos[kk], gbk = s.gbnd[kk];
     const float prk = s.p[kk];
     const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
+    uint2 ahead[AHEAD];
+    prefetch_tile_list<kPressureGlobalEntries>(T, h, k, half, ahead);
     if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     Acc3<float, true> pa;
@@ -798,7 +824,7 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
         pa.add(part);
         part = v3<float>(0.f, 0.f, 0.f);
     };
-    if (valid) walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, pair, flush);
+    if (valid) walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, pair, flush);
     const V3<float> a = pair_total(pa);
     if (half || !valid) return;
     // boundary: - sum_bnd (lambda m_j p_i / rho0^2) gradW, lambda = 2 gamma (single layer) or 2
@@ -843,6 +869,8 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
         const float4 pk = s.pos[kk], ak = s.acc[kk], vsk = s.vstar[kk], gbk = s.gbnd[kk];
         const float aii = s.anp[kk].w, prk = s.p[kk];
         const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
+        uint2 ahead[AHEAD];
+        prefetch_tile_list<kPressureGlobalEntries>(T, h, k, half, ahead);
         if (stage_tile_wait(stg, status)) {
             const FastSpline S(c.kern);
             Acc<float, true> ap;
@@ -856,7 +884,7 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
                 ap.add(part);
                 part = 0.f;
             };
-            if (valid) walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, pair, flush);
+            if (valid) walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, pair, flush);
             // boundary: sum_bnd m_j dot(a_i, gradW) = dot(a_i, sum_bnd m_j gradW)
             const float sum = pair_total(ap) + dot3(v3<float>(ak.x, ak.y, ak.z), v3<float>(gbk.x, gbk.y, gbk.z));
             if (!half && valid)
