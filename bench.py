@@ -268,11 +268,13 @@ def run_ours(args):
     # the unit the roofline kernel's bytes and traffic are quoted per
     units = [args.steps, args.steps, args.steps, max(it_total - args.steps, 1.0), args.steps]
     per_launch = phase_bytes[dom] / units[dom]
-    traffic = None
+    traffic, winst = None, None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(PHASES[dom])
+            tj = json.load(f)
+        traffic = tj.get(PHASES[dom])
+        winst = tj.get("warp_instructions", {}).get(PHASES[dom])
 
     # end to end through the public API: pinned host state in, step, state out
     e2e = run_e2e(solver, scene, min(args.steps, 5), local, max_over_ranks)
@@ -287,6 +289,19 @@ def run_ours(args):
         cpu = cpu_baseline_from_state(solver_state, scene.n_fluid)
 
     clocks = clk.summary()
+    # the same kernel against the SMs' instruction issue rate (one warp
+    # instruction per scheduler and cycle, 4 schedulers per SM, at the SM clock
+    # sampled in the timed region), which is what bounds it
+    issue = None
+    if winst and clocks and clocks.get("sm_mhz"):
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        unit_s = phase[dom] / 1e3 / units[dom]
+        peak_issue = sms * 4 * clocks["sm_mhz"] * 1e6
+        issue = {"kernel": PHASE_KERNELS[dom], "per": PHASE_UNITS[dom], "warp_instructions": winst,
+                 "achieved": winst / unit_s / 1e9, "peak": peak_issue / 1e9, "unit": "G warp instructions/s",
+                 "frac": winst / unit_s / peak_issue, "sms": sms, "sm_mhz": clocks["sm_mhz"],
+                 "source": "warp instructions per unit from profiles/traffic.json (ncu smsp__inst_executed.sum); "
+                           "the duration event-timed here"}
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -309,6 +324,7 @@ def run_ours(args):
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": per_launch, "per": PHASE_UNITS[dom],
                          "traffic_source": "profiles/traffic.json (ncu dram__bytes_read.sum + dram__bytes_write.sum)"},
+            "issue": issue,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
             "batched": batched, "ns_microbench": ns_micro, "other_configs": configs,
         }
