@@ -1890,7 +1890,7 @@ fs_status fs_run(fs_ctx* c, int32_t steps, float desired_dt, fs_step_stats* stat
 // then 4 timed steps; the first loop is timed as its phase, the pressure
 // passes per loop iteration (the first iteration runs inside the second loop).
 // Trials (pressure depth, first-loop depth): (1,1), (2,2), (3,1), (4,2); each
-// depth is judged by the mean over the trials that used it.
+// depth is rated by the mean over the trials that used it.
 fs_status fs_autotune(fs_ctx* c, fs_tuning* out) {
     if (!c || !out) return fail(FS_ERR_INVALID, "null argument");
     if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
