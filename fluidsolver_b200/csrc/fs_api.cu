@@ -148,7 +148,7 @@ template <typename R> SolverConsts<R> consts_of(fs_ctx* c) {
 // the 3D IISPH fast path runs on tile lists (fs_tiles.cuh)
 bool tiled_mode(const fs_ctx* c) {
     return c->precision == FS_PRECISION_FP32_KAHAN && !c->reference_order && c->dim == 3 &&
-           c->prm.solver == FS_SOLVER_IISPH_3D;
+           (c->prm.solver == FS_SOLVER_IISPH_3D || c->prm.solver == FS_SOLVER_SESPH_3D);
 }
 
 Lists lists_of(fs_ctx* c) {
@@ -961,7 +961,46 @@ template <typename R, bool KAHAN> fs_status step_iisph3d(fs_ctx* c, bool capture
     return FS_OK;
 }
 
+// 3D SESPH in the fast mode on tile lists (fs_tiles.cuh): the density and
+// acceleration passes; maxima, CFL clamp and integration as in step_sesph
+fs_status step_sesph3d_tiled(fs_ctx* c) {
+    cudaStream_t st = c->stream;
+    const int64_t n = c->n, nf = c->n_owners;
+    const unsigned tiles = (unsigned)((nf + kTileOwners - 1) / kTileOwners);
+    const SolverConsts<float> k = consts_of<float>(c);
+    const Lists L = lists_of(c);
+    const TileLists T = tile_lists_of(c);
+    State<float> s = state_of<float>(c);
+    FS_TRY(mark(c, 1, st));
+    c->launches++;
+    FSB_AHEAD_SWITCH(c->tuning.l1_ahead, k_tile_sesph3d_density,
+                     <<<tiles, kPassThreads, tile_pass_smem(16, T.K, false), st>>>(nf, s, T, L, k, c->status))
+    FS_CUDA(cudaGetLastError());
+    FS_TRY(mark(c, 2, st));
+    c->launches++;
+    FSB_AHEAD_SWITCH(c->tuning.l1_ahead, k_tile_sesph3d_accel,
+                     <<<tiles, kPassThreads, tile_pass_smem(36, T.K, false), st>>>(nf, s, T, L, k, c->status))
+    FS_CUDA(cudaGetLastError());
+    FS_TRY(mark(c, 3, st));
+    c->launches++;
+    k_sesph_maxima<float><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
+    c->launches++;
+    k_sesph_maxima_final<<<1, 1, 0, st>>>(c->scalars);
+    c->launches++;
+    k_cfl<<<1, 128, 0, st>>>(c->scalars, c->nsc(), c->prm.particle_size, cfl_default(c), c->prm.lambda_v,
+                             c->prm.lambda_a, c->status);
+    FS_TRY(mark(c, 4, st));
+    c->launches++;
+    k_sesph_integrate<float><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
+    FS_CUDA(cudaGetLastError());
+    FS_TRY(mark(c, 5, st));
+    return FS_OK;
+}
+
 template <typename R, bool KAHAN> fs_status step_sesph(fs_ctx* c) {
+    if constexpr (std::is_same<R, float>::value && KAHAN) {
+        if (tiled_mode(c) && c->n_owners > 0) return step_sesph3d_tiled(c);
+    }
     cudaStream_t st = c->stream;
     const int64_t n = c->n, no = c->n_owners;
     const SolverConsts<R> k = consts_of<R>(c);
@@ -1899,7 +1938,8 @@ fs_status fs_autotune(fs_ctx* c, fs_tuning* out) {
     *out = fs_tuning{};
     out->first_loop_prefetch = c->tuning.l1_ahead;
     out->pressure_prefetch = c->tuning.pressure_ahead;
-    if (!tiled_mode(c) || c->n_fluid == 0) return FS_OK;   // nothing tunable: the passes are not tiled
+    // nothing tunable unless the IISPH passes are tiled
+    if (!tiled_mode(c) || c->prm.solver != FS_SOLVER_IISPH_3D || c->n_fluid == 0) return FS_OK;
     FS_CUDA(cudaSetDevice(c->device));
     const size_t n = (size_t)c->n, d = (size_t)c->dim;
     std::vector<float> pos(n * d), vel(n * d), acc(n * d), ext(n * d), mass(n), rho(n), p(n);

@@ -674,10 +674,8 @@ __global__ void k_iisph3d_integrate(int64_t n, State<R> s, const StepScalars* __
 //   3D: boundary j contributes (gamma_1 m_j) W if single layer (:216-225)
 //   p = max(k (rho / rho0 - 1), 0)  (std::max: NaN propagates)
 template <typename R, bool KAHAN>
-__global__ void k_sesph_density(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || *status) return;
-    if (s.type[k] != FS_TYPE_NORMAL) return;
+__device__ __forceinline__ void sesph_density_one(int64_t k, const State<R>& s, const Lists& L,
+                                                  const SolverConsts<R>& c) {
     const V3<R> xk = xyz<R>(s.pos[k]);
     Acc<R, KAHAN> rho;
     const uint32_t nn = L.size(k);
@@ -694,15 +692,21 @@ __global__ void k_sesph_density(int64_t n, State<R> s, Lists L, SolverConsts<R> 
     s.p[k] = (pr < R(0)) ? R(0) : pr;
 }
 
+template <typename R, bool KAHAN>
+__global__ void k_sesph_density(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    if (s.type[k] != FS_TYPE_NORMAL) return;
+    sesph_density_one<R, KAHAN>(k, s, L, c);
+}
+
 // accelerations of fluid particles: a = pressure acc + (gravity + viscosity)
 //   pressure acc (:245-290): pdd = (rho == 0) ? 0 : p / rho^2
 //     fluid j   : += (-m_j (pdd_i + pdd_j)) gradW
 //     boundary j: += (-m_i (pdd_i + pdd_i)) gradW [* gamma_2 if single layer, 3D]
 template <typename R, bool KAHAN>
-__global__ void k_sesph_accel(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || *status) return;
-    if (s.type[k] != FS_TYPE_NORMAL) return;
+__device__ __forceinline__ void sesph_accel_one(int64_t k, const State<R>& s, const Lists& L,
+                                                const SolverConsts<R>& c) {
     const V4<R> pk = s.pos[k];
     const V3<R> xk = xyz<R>(pk);
     const R rk = s.rho[k];
@@ -724,6 +728,14 @@ __global__ void k_sesph_accel(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
         }
     });
     s.acc[k] = v4<R>(pa.get() + npa, R(0));
+}
+
+template <typename R, bool KAHAN>
+__global__ void k_sesph_accel(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* __restrict__ status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    if (s.type[k] != FS_TYPE_NORMAL) return;
+    sesph_accel_one<R, KAHAN>(k, s, L, c);
 }
 
 // max |a|^2, |v + dt a|^2 over ALL particles (SESPHFluidSolver3D.hpp:93-107)

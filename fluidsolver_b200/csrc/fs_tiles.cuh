@@ -1,4 +1,4 @@
-// Tile lists: the neighbor lists of the 3D IISPH fast path (FP32 with
+// Tile lists: the neighbor lists of the 3D IISPH and SESPH fast paths (FP32 with
 // compensated sums, device order) and the kernels that walk them.
 //
 // A tile is kTileOwners consecutive fluid particles of the sorted order.
@@ -894,6 +894,141 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
     reduce_err_parts(o, sc, scene);
 }
 
+// ---------------------------------------------------------------------------
+// SESPH 3D passes on tile lists (the fast-mode formulas of k_sesph_density
+// and k_sesph_accel: SESPHFluidSolver3D.hpp:49-130). Same block layout as the
+// IISPH passes; fallback tiles run the gather code.
+// ---------------------------------------------------------------------------
+
+// density and pressure of the fluid owners: rho = sum_j m_j W, boundary
+// neighbors weighted by gamma_1 in the single-layer model;
+// p = max(k (rho / rho0 - 1), 0). p / rho^2 goes to the velocity's unused w
+// component, where the acceleration pass finds it staged with the velocity.
+template <int AHEAD>
+__global__ void __launch_bounds__(kPassThreads, 5) k_tile_sesph3d_density(int64_t n_fluid, State<float> s,
+                                                                          TileLists T, Lists L, SolverConsts<float> c,
+                                                                          int* __restrict__ status) {
+    extern __shared__ float4 tile_smem[];
+    const int half = threadIdx.x & 1;
+    const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
+    const TileDesc* d = T.desc + blockIdx.x;
+    const int err = *status;
+    const TileHead h = load_head(d);
+    const TileRange rg = load_range(d, threadIdx.x);
+    if (__syncthreads_or(err)) return;   // one decision for the whole block
+    const bool valid = k < n_fluid;
+    auto pressure_terms = [&](float r) {
+        const float pr = c.stiffness * (r / c.rest_density - 1.f);
+        const float p = (pr < 0.f) ? 0.f : pr;
+        s.p[k] = p;
+        s.vel[k].w = r == 0.f ? 0.f : fdiv<true>(p, r * r);
+    };
+    if (h.nranges == kTileFallback) {
+        if (valid && !half) {
+            sesph_density_one<float, true>(k, s, L, c);
+            pressure_terms(s.rho[k]);
+        }
+        return;
+    }
+    float4* sp = tile_smem;
+    __shared__ TileStage stg;
+    const float4* src4[1] = {s.pos};
+    float4* dst4[1] = {sp};
+    const TileSlab none{nullptr, nullptr};
+    stage_tile_async<1, false, false>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, none);
+    const int64_t kk = valid ? k : 0;
+    const float4 pk = s.pos[kk];
+    const uint32_t cnt = T.count[kk];
+    uint2 ahead[AHEAD];
+    prefetch_tile_list<true>(T, h, k, half, ahead);
+    if (!stage_tile_wait(stg, status)) return;
+    const FastSpline S(c.kern);
+    const float gb = c.single_layer ? c.gamma1 : 1.f;
+    Acc<float, true> rho;
+    float part = 0.f;
+    if (valid) walk_tile_list<true, false, AHEAD>(T, none, k, cnt, half, ahead, [&](uint32_t off, bool bnd) {
+        const float4 pj = at_offset(sp, off);
+        float w, f;
+        S.value_grad(r2_of(sub3(pk, pj)), w, f);
+        part = __fmaf_rn(bnd ? pj.w * gb : pj.w, w, part);
+    }, [&] {
+        rho.add(part);
+        part = 0.f;
+    });
+    const float r = pair_total(rho);
+    if (half || !valid) return;
+    s.rho[k] = r;
+    pressure_terms(r);
+}
+
+// accelerations of the fluid owners: gravity + viscosity + pressure
+// acceleration. Fluid j: -m_j (p_i / rho_i^2 + p_j / rho_j^2) gradW;
+// boundary j: -m_i (2 p_i / rho_i^2) gradW, times gamma_2 in the single-layer
+// model; viscosity over every j of non-zero density, as k_sesph_accel.
+template <int AHEAD>
+__global__ void __launch_bounds__(kPassThreads, 4) k_tile_sesph3d_accel(int64_t n_fluid, State<float> s,
+                                                                        TileLists T, Lists L, SolverConsts<float> c,
+                                                                        int* __restrict__ status) {
+    extern __shared__ float4 tile_smem[];
+    const int half = threadIdx.x & 1;
+    const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
+    const TileDesc* d = T.desc + blockIdx.x;
+    const int err = *status;
+    const TileHead h = load_head(d);
+    const TileRange rg = load_range(d, threadIdx.x);
+    if (__syncthreads_or(err)) return;   // one decision for the whole block
+    const bool valid = k < n_fluid;
+    if (h.nranges == kTileFallback) {
+        if (valid && !half) sesph_accel_one<float, true>(k, s, L, c);
+        return;
+    }
+    float4* sp = tile_smem;
+    float4* sv = tile_smem + kTileCap;
+    float* sr = reinterpret_cast<float*>(tile_smem + 2 * kTileCap);
+    __shared__ TileStage stg;
+    const float4* src4[2] = {s.pos, s.vel};
+    float4* dst4[2] = {sp, sv};
+    const TileSlab none{nullptr, nullptr};
+    stage_tile_async<2, false, false>(stg, d, h, rg, src4, dst4, s.rho, sr, T, none);
+    const int64_t kk = valid ? k : 0;
+    const float4 pk = s.pos[kk], vk = s.vel[kk];
+    const float rk = s.rho[kk], prk = s.p[kk];
+    const uint32_t cnt = T.count[kk];
+    uint2 ahead[AHEAD];
+    prefetch_tile_list<true>(T, h, k, half, ahead);
+    if (!stage_tile_wait(stg, status)) return;
+    const FastSpline S(c.kern);
+    const float pdd = rk == 0.f ? 0.f : prk / (rk * rk);
+    // the boundary coefficient of gradW, the same for every boundary neighbor
+    const float cb = -pk.w * (pdd + pdd) * (c.single_layer ? c.gamma2 : 1.f);
+    Acc3<float, true> visc, pres;
+    V3<float> vpart = v3<float>(0.f, 0.f, 0.f), ppart = v3<float>(0.f, 0.f, 0.f);
+    if (valid) walk_tile_list<true, false, AHEAD>(T, none, k, cnt, half, ahead, [&](uint32_t off, bool bnd) {
+        const float4 pj = at_offset(sp, off), vj = at_offset(sv, off);
+        const float rj = at_offset(sr, off >> 2);
+        const V3<float> xij = sub3(pk, pj);
+        const float r2 = r2_of(xij);
+        const float f = S.grad(r2);
+        if (rj != 0.f) {
+            const float cf = __fdividef(pj.w * dot3(sub3(vk, vj), xij), rj * (r2 + c.visc_eps)) * f;
+            vpart = fma3(cf, xij, vpart);
+        }
+        // vj.w: p_j / rho_j^2 (k_tile_sesph3d_density)
+        const float cp = (bnd ? cb : -pj.w * (pdd + vj.w)) * f;
+        ppart = fma3(cp, xij, ppart);
+    }, [&] {
+        visc.add(vpart);
+        pres.add(ppart);
+        vpart = v3<float>(0.f, 0.f, 0.f);
+        ppart = v3<float>(0.f, 0.f, 0.f);
+    });
+    const V3<float> vs = pair_total(visc);
+    const V3<float> pa = pair_total(pres);
+    if (half || !valid) return;
+    const V3<float> npa = v3<float>(0.f, -c.gravity, 0.f) + c.two_nu * vs;
+    s.acc[k] = v4<float>(pa + npa, 0.f);
+}
+
 // Export of the lists that the solver passes walk, as sorted indices: owner
 // k's list length (out == nullptr) or its entries from out[offsets[k]]. A
 // tile list entry is a staged slot, which the tile's ranges map back to a
@@ -947,6 +1082,12 @@ template <int AHEAD> inline cudaError_t set_tuned_pass_smem(int K) {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_update<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)tile_pass_smem(32, K, !kPressureGlobalEntries));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tile_sesph3d_density<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_pass_smem(16, K, false));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tile_sesph3d_accel<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_pass_smem(36, K, false));
     return e;
 }
 
