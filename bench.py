@@ -515,6 +515,17 @@ def run_configs(args, device):
     s5.close()
     out["sesph3d_dam_100k"] = {"workload": "3D SESPH on the 100k dam, hashed-3d, k 1000, nu 0.01, dt 0.001 (CFL-clamped)",
                                "gpu_ms_per_step": ms5, "gpu_particle_steps_per_s": d3.n_fluid / (ms5 / 1e3)}
+    d1m = sc.dam_1m(seed=5)
+    s5 = SESPHFluidSolver3D(search="hashed-3d", device=device)
+    s5.parameters.rest_density, s5.parameters.gravity, s5.parameters.particle_size = 1.0, 9.81, 1.0
+    s5.settings.StiffnessK, s5.settings.Viscosity = 1000.0, 0.01
+    s5.settings.single_layer_boundary = True
+    s5.timestep_generator.settings.timestep = 0.001
+    s5.data.collection = d1m.collection
+    ms7, _ = gpu_time(s5, 20)
+    s5.close()
+    out["sesph3d_dam_1m"] = {"workload": "3D SESPH on the 1M dam, hashed-3d, k 1000, nu 0.01, dt 0.001 (CFL-clamped)",
+                             "gpu_ms_per_step": ms7, "gpu_particle_steps_per_s": d1m.n_fluid / (ms7 / 1e3)}
     s6 = IISPHFluidSolver(search="hashed-2d", device=device)
     s6.parameters.rest_density, s6.parameters.gravity, s6.parameters.particle_size = 1.0, 9.81, 1.0
     s6.settings.Viscosity = 0.01
