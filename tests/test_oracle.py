@@ -259,3 +259,14 @@ def test_position_query_quirk_is_pinned(golden, c_oracle):
 def test_compact_hashing_has_no_position_query(c_oracle):
     with pytest.raises(ValueError):
         c_oracle.query_position("compact-hashing-2d", np.zeros((2, 2), np.float32), 1.0, np.zeros(2, np.float32))
+
+
+def test_raytrace_fixture_is_the_reference_accelerator(golden, ref_oracle):
+    """tests/golden/raytrace.npz holds the first hits that the reference's own
+    ParticleIntersectionAccelerator (visualizer/raytracer/ParticleIntersectionAccelerator.cpp:8-206,
+    compiled in oracle/_ref) gives for its rays; the device tracer is checked against it."""
+    g = golden["raytrace"]
+    out = ref_oracle.trace_rays(g["pos"], g["mass"], g["type"], 1.0, 1.0, g["origins"], g["directions"])
+    for k in ("hit", "point", "normal", "length"):
+        assert bits_equal(out[k], g[k]), k
+    assert {int(t) for t in np.unique(g["hit"])} == {-1, 0, 1, 2}   # misses and every kind of hit
