@@ -89,3 +89,49 @@ def test_render_path_tracing(dam_solver):
     v = np.clip(1.0 - np.exp(-(rad.astype(np.float32) * np.float32(0.2))), 0, 1) ** (1 / 2.2)
     assert np.abs(rgba[..., :3].astype(int) - (v * 255).astype(int)).max() <= 1
     assert (rgba[..., 3] == 255).all()
+
+
+def test_render_rejects_bad_arguments(dam_solver):
+    from fluidsolver_b200._lib import FluidSolverError
+    with pytest.raises(FluidSolverError, match="image size"):
+        dam_solver.render(**dict(CAM, width=0))
+    with pytest.raises(FluidSolverError, match="bad settings"):
+        dam_solver.render(**CAM, samples_per_pixel=0)
+    with pytest.raises(FluidSolverError, match="surface density fraction"):
+        dam_solver.render(**CAM, surface_density_fraction=0.0)
+    with pytest.raises(FluidSolverError, match="view direction"):
+        dam_solver.render(**dict(CAM, view_direction=(0.0, 1.0, 0.0)))   # parallel to the up vector
+    with pytest.raises(TypeError):
+        dam_solver.render(**CAM, no_such_setting=1)
+    # no rays: nothing to trace, no error
+    out = dam_solver.trace_rays(np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32))
+    assert len(out["hit"]) == 0
+
+
+def test_render_needs_a_3d_context():
+    from fluidsolver_b200._lib import FluidSolverError
+    sc = scenes.breaking_dam_2d(10, 10, 1.0, seed=1)
+    s = make_solver("sesph-2d", "hashed-2d", [1000.0, 0.01], (0.001, 0.4, 0.25))
+    s.data.collection = sc.collection
+    with pytest.raises(FluidSolverError, match="3D"):
+        s.trace_rays(np.zeros((1, 3), np.float32), np.ones((1, 3), np.float32))
+    s.close()
+
+
+def test_trace_rays_in_fp64_matches_fp32(golden):
+    """The FP64 context marches the same points; its densities are double sums
+    rounded to float, so hits agree up to the same rounding margin."""
+    g = golden["raytrace"]
+    res = {}
+    for prec in ("fp32-kahan", "fp64"):
+        s = make_solver("iisph-3d", "hashed-3d", SETTINGS_3D, (0.005, 0.4, 0.25), precision=prec)
+        n = len(g["pos"])
+        s.data.collection = ParticleCollection(position=g["pos"], velocity=np.zeros_like(g["pos"]), mass=g["mass"],
+                                               density=np.ones(n, np.float32), type=g["type"])
+        res[prec] = s.trace_rays(g["origins"], g["directions"])
+        s.close()
+    a, b = res["fp32-kahan"], res["fp64"]
+    same = a["hit"] == b["hit"]
+    assert same.mean() >= 0.995
+    both = same & (a["hit"] >= 0)
+    np.testing.assert_allclose(a["point"][both], b["point"][both], atol=1e-3, rtol=0)
