@@ -114,6 +114,47 @@ def test_kahan_within_tolerance_of_reference(golden, name):
     assert np.max(np.abs(k.position - g[f"{name}_step0_position"])) <= TOL * _scale(g[f"{name}_step0_position"])
 
 
+@pytest.mark.parametrize("name", ["iisph3d_hashed", "iisph3d_multilayer", "sesph3d_hashed"])
+def test_fast_mode_step_by_step_from_the_reference_state(golden, name):
+    """Every step of the fast mode (FP32 + compensated sums, tile lists), started
+    from the reference's own state after the previous step (position, velocity,
+    and the density its viscosity reads): the IISPH iteration count within +-1
+    of the reference's, positions within 1e-5 of their scale, and velocity,
+    density and pressure within the reference's own FP32 distance to an FP64
+    step from the same state, plus 1e-5 of scale."""
+    import dataclasses
+    solver, search, build, gen, settings, steps = SOLVER_CASES[name]
+    g = golden["solvers"]
+    col0 = build().collection
+    TOL = 1e-5
+    for k in range(1, steps):
+        start = dataclasses.replace(col0, position=g[f"{name}_step{k - 1}_position"],
+                                    velocity=g[f"{name}_step{k - 1}_velocity"],
+                                    density=g[f"{name}_step{k - 1}_density"])
+        runs = {}
+        for prec in ("fp32-kahan", "fp64"):
+            s = make_solver(solver, search, g[f"{name}_settings"], g[f"{name}_generator"], precision=prec)
+            s.data.collection = start
+            tp = simulator_step(s)
+            its = s.stat_last_iteration_count if solver == "iisph-3d" else None
+            runs[prec] = (s.collection(), its, tp.actual_time_step)
+            s.close()
+        mine, its, dt = runs["fp32-kahan"]
+        exact = runs["fp64"][0]
+        ref = g[f"{name}_stats"][k]
+        # the CFL clamp sees the same velocities; its accelerations differ by rounding
+        assert abs(dt - float(ref[1])) <= 1e-5 * float(ref[1]), (name, k, dt, ref[1])
+        if its is not None:
+            assert abs(its - int(ref[2])) <= 1, (name, k, its, ref[2])
+        pos = g[f"{name}_step{k}_position"].astype(np.float64)
+        assert np.max(np.abs(mine.position - pos)) <= TOL * _scale(pos), (name, k)
+        for f in ("velocity", "density", "pressure"):
+            r = g[f"{name}_step{k}_{f}"].astype(np.float64)
+            e = getattr(exact, f).astype(np.float64)
+            envelope = np.max(np.abs(r - e))
+            assert np.max(np.abs(getattr(mine, f) - e)) <= envelope + TOL * _scale(r), (name, k, f)
+
+
 def test_kahan_is_closer_to_fp64_than_plain_fp32():
     sc = scenes.breaking_dam_3d(16, 20, 12, 1.0, tank=(30, 26, 18), seed=41)
     res = {}
