@@ -897,7 +897,8 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
 // ---------------------------------------------------------------------------
 // SESPH 3D passes on tile lists (the fast-mode formulas of k_sesph_density
 // and k_sesph_accel: SESPHFluidSolver3D.hpp:49-130). Same block layout as the
-// IISPH passes; fallback tiles run the gather code.
+// IISPH passes; in a fallback tile the two threads of an owner split its
+// 32-bit list, with the same pair arithmetic.
 // ---------------------------------------------------------------------------
 
 // density and pressure of the fluid owners: rho = sum_j m_j W, boundary
@@ -923,38 +924,45 @@ __global__ void __launch_bounds__(kPassThreads, 5) k_tile_sesph3d_density(int64_
         s.p[k] = p;
         s.vel[k].w = r == 0.f ? 0.f : fdiv<true>(p, r * r);
     };
-    if (h.nranges == kTileFallback) {
-        if (valid && !half) {
-            sesph_density_one<float, true>(k, s, L, c);
-            pressure_terms(s.rho[k]);
-        }
-        return;
-    }
-    float4* sp = tile_smem;
-    __shared__ TileStage stg;
-    const float4* src4[1] = {s.pos};
-    float4* dst4[1] = {sp};
-    const TileSlab none{nullptr, nullptr};
-    stage_tile_async<1, false, false>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, none);
     const int64_t kk = valid ? k : 0;
     const float4 pk = s.pos[kk];
-    const uint32_t cnt = T.count[kk];
-    uint2 ahead[AHEAD];
-    prefetch_tile_list<true>(T, h, k, half, ahead);
-    if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     const float gb = c.single_layer ? c.gamma1 : 1.f;
     Acc<float, true> rho;
     float part = 0.f;
-    if (valid) walk_tile_list<true, false, AHEAD>(T, none, k, cnt, half, ahead, [&](uint32_t off, bool bnd) {
-        const float4 pj = at_offset(sp, off);
+    auto pair = [&](const float4& pj, bool bnd) {
         float w, f;
         S.value_grad(r2_of(sub3(pk, pj)), w, f);
         part = __fmaf_rn(bnd ? pj.w * gb : pj.w, w, part);
-    }, [&] {
+    };
+    auto flush = [&] {
         rho.add(part);
         part = 0.f;
-    });
+    };
+    if (h.nranges == kTileFallback) {
+        // the owner's 32-bit list, split between its two threads
+        const uint32_t nn = valid ? L.size(k) : 0u;
+        for (uint32_t q = half; q < nn; q += 2) {
+            const uint32_t e = L.at(k, q);
+            pair(s.pos[e & kIndexMask], (e & kBoundaryBit) != 0u);
+            if ((q & 15u) >= 14u) flush();
+        }
+        flush();
+    } else {
+        float4* sp = tile_smem;
+        __shared__ TileStage stg;
+        const float4* src4[1] = {s.pos};
+        float4* dst4[1] = {sp};
+        const TileSlab none{nullptr, nullptr};
+        stage_tile_async<1, false, false>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, none);
+        const uint32_t cnt = T.count[kk];
+        uint2 ahead[AHEAD];
+        prefetch_tile_list<true>(T, h, k, half, ahead);
+        if (!stage_tile_wait(stg, status)) return;
+        if (valid)
+            walk_tile_list<true, false, AHEAD>(T, none, k, cnt, half, ahead,
+                                               [&](uint32_t off, bool bnd) { pair(at_offset(sp, off), bnd); }, flush);
+    }
     const float r = pair_total(rho);
     if (half || !valid) return;
     s.rho[k] = r;
@@ -978,34 +986,16 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_tile_sesph3d_accel(int64_t 
     const TileRange rg = load_range(d, threadIdx.x);
     if (__syncthreads_or(err)) return;   // one decision for the whole block
     const bool valid = k < n_fluid;
-    if (h.nranges == kTileFallback) {
-        if (valid && !half) sesph_accel_one<float, true>(k, s, L, c);
-        return;
-    }
-    float4* sp = tile_smem;
-    float4* sv = tile_smem + kTileCap;
-    float* sr = reinterpret_cast<float*>(tile_smem + 2 * kTileCap);
-    __shared__ TileStage stg;
-    const float4* src4[2] = {s.pos, s.vel};
-    float4* dst4[2] = {sp, sv};
-    const TileSlab none{nullptr, nullptr};
-    stage_tile_async<2, false, false>(stg, d, h, rg, src4, dst4, s.rho, sr, T, none);
     const int64_t kk = valid ? k : 0;
     const float4 pk = s.pos[kk], vk = s.vel[kk];
     const float rk = s.rho[kk], prk = s.p[kk];
-    const uint32_t cnt = T.count[kk];
-    uint2 ahead[AHEAD];
-    prefetch_tile_list<true>(T, h, k, half, ahead);
-    if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     const float pdd = rk == 0.f ? 0.f : prk / (rk * rk);
     // the boundary coefficient of gradW, the same for every boundary neighbor
     const float cb = -pk.w * (pdd + pdd) * (c.single_layer ? c.gamma2 : 1.f);
     Acc3<float, true> visc, pres;
     V3<float> vpart = v3<float>(0.f, 0.f, 0.f), ppart = v3<float>(0.f, 0.f, 0.f);
-    if (valid) walk_tile_list<true, false, AHEAD>(T, none, k, cnt, half, ahead, [&](uint32_t off, bool bnd) {
-        const float4 pj = at_offset(sp, off), vj = at_offset(sv, off);
-        const float rj = at_offset(sr, off >> 2);
+    auto pair = [&](const float4& pj, const float4& vj, float rj, bool bnd) {
         const V3<float> xij = sub3(pk, pj);
         const float r2 = r2_of(xij);
         const float f = S.grad(r2);
@@ -1016,12 +1006,41 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_tile_sesph3d_accel(int64_t 
         // vj.w: p_j / rho_j^2 (k_tile_sesph3d_density)
         const float cp = (bnd ? cb : -pj.w * (pdd + vj.w)) * f;
         ppart = fma3(cp, xij, ppart);
-    }, [&] {
+    };
+    auto flush = [&] {
         visc.add(vpart);
         pres.add(ppart);
         vpart = v3<float>(0.f, 0.f, 0.f);
         ppart = v3<float>(0.f, 0.f, 0.f);
-    });
+    };
+    if (h.nranges == kTileFallback) {
+        // the owner's 32-bit list, split between its two threads
+        const uint32_t nn = valid ? L.size(k) : 0u;
+        for (uint32_t q = half; q < nn; q += 2) {
+            const uint32_t e = L.at(k, q);
+            const uint32_t j = e & kIndexMask;
+            pair(s.pos[j], s.vel[j], s.rho[j], (e & kBoundaryBit) != 0u);
+            if ((q & 15u) >= 14u) flush();
+        }
+        flush();
+    } else {
+        float4* sp = tile_smem;
+        float4* sv = tile_smem + kTileCap;
+        float* sr = reinterpret_cast<float*>(tile_smem + 2 * kTileCap);
+        __shared__ TileStage stg;
+        const float4* src4[2] = {s.pos, s.vel};
+        float4* dst4[2] = {sp, sv};
+        const TileSlab none{nullptr, nullptr};
+        stage_tile_async<2, false, false>(stg, d, h, rg, src4, dst4, s.rho, sr, T, none);
+        const uint32_t cnt = T.count[kk];
+        uint2 ahead[AHEAD];
+        prefetch_tile_list<true>(T, h, k, half, ahead);
+        if (!stage_tile_wait(stg, status)) return;
+        if (valid)
+            walk_tile_list<true, false, AHEAD>(T, none, k, cnt, half, ahead, [&](uint32_t off, bool bnd) {
+                pair(at_offset(sp, off), at_offset(sv, off), at_offset(sr, off >> 2), bnd);
+            }, flush);
+    }
     const V3<float> vs = pair_total(visc);
     const V3<float> pa = pair_total(pres);
     if (half || !valid) return;
