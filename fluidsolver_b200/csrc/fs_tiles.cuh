@@ -530,6 +530,24 @@ __device__ __forceinline__ void walk_tile_list(const TileLists& T, const TileSla
     }
 }
 
+// Walks owner k's 32-bit list in a fallback tile, the entries of this half
+// of the owner's thread pair (half, half + 2, ...): f(sorted index, boundary)
+// for each (the fluid entries only with FLUID_ONLY), flush() after every 8
+// visits and at the end, as for_tile_entries does.
+template <bool FLUID_ONLY, typename F, typename Flush>
+__device__ __forceinline__ void walk_fallback_list(const Lists& L, int64_t k, int half, F&& f, Flush&& flush) {
+    const uint32_t nn = L.size(k);
+    uint32_t visited = 0;
+    for (uint32_t q = (uint32_t)half; q < nn; q += 2) {
+        const uint32_t e = L.at(k, q);
+        const bool bnd = (e & kBoundaryBit) != 0u;
+        if (FLUID_ONLY && bnd) continue;
+        f(e & kIndexMask, bnd);
+        if ((++visited & 7u) == 0u) flush();
+    }
+    flush();
+}
+
 // Octets a pass loads ahead of the one it visits. The first loop's and the
 // pressure passes' depths are chosen per context by fs_autotune among
 // 1..kMaxAhead (defaults: what the 1M dam preferred on a B200, 1 and 3); the
@@ -633,36 +651,18 @@ __global__ void __launch_bounds__(kPassThreads, kL1GlobalEntries ? 4 : 3) k_tile
     const TileHead h = load_head(d);
     const TileRange rg = load_range(d, threadIdx.x);
     if (__syncthreads_or(err)) return;   // one decision for the whole block
-    if (h.nranges == kTileFallback) {
-        if (k < n_fluid && !half) iisph3d_l1_one<float, true, false>(k, s, L, c, sc[s.scene_of(k)].dt);
-        return;
-    }
-    float4* sp = tile_smem;
-    float4* sv = tile_smem + kTileCap;
-    float* sr = reinterpret_cast<float*>(tile_smem + 2 * kTileCap);
-    __shared__ TileStage stg;
-    const float4* src4[2] = {s.pos, s.vel};
-    float4* dst4[2] = {sp, sv};
-    const TileSlab slab = slab_at(tile_smem, 36, T.K);
-    stage_tile_async<2, false, !kL1GlobalEntries>(stg, d, h, rg, src4, dst4, s.rho_prev, sr, T, slab);
     // owners past n_fluid (last tile) walk no entries but take part in the shuffles
     const bool valid = k < n_fluid;
     const int64_t kk = valid ? k : 0;
     const float4 pk = s.pos[kk], vk = s.vel[kk], ek = s.ext[kk];
     const float dt = sc[s.scene_of(kk)].dt;
-    const uint32_t cnt = kL1GlobalEntries ? T.count[kk] : 0u;
-    uint2 ahead[AHEAD];
-    prefetch_tile_list<kL1GlobalEntries>(T, h, k, half, ahead);
-    if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     Acc3<float, true> visc;
     Acc<float, true> rho;
     V3<float> vpart = v3<float>(0.f, 0.f, 0.f);
     float rpart = 0.f;
     const float gb = c.single_layer ? c.gamma1 : 1.f;
-    if (valid) walk_tile_list<kL1GlobalEntries, false, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool bnd) {
-        const float4 pj = at_offset(sp, off), vj = at_offset(sv, off);
-        const float rj = at_offset(sr, off >> 2);
+    auto pair = [&](const float4& pj, const float4& vj, float rj, bool bnd) {
         const V3<float> xij = sub3(pk, pj);
         const float r2 = r2_of(xij);
         float w, f;
@@ -672,12 +672,37 @@ __global__ void __launch_bounds__(kPassThreads, kL1GlobalEntries ? 4 : 3) k_tile
             const float cf = __fdividef(pj.w * dot3(sub3(vk, vj), xij), rj * (r2 + c.visc_eps)) * f;
             vpart = fma3(cf, xij, vpart);
         }
-    }, [&] {
+    };
+    auto flush = [&] {
         visc.add(vpart);
         rho.add(rpart);
         vpart = v3<float>(0.f, 0.f, 0.f);
         rpart = 0.f;
-    });
+    };
+    if (h.nranges == kTileFallback) {
+        // the owner's 32-bit list, split between its two threads
+        if (valid)
+            walk_fallback_list<false>(L, k, half, [&](uint32_t j, bool bnd) {
+                pair(s.pos[j], s.vel[j], s.rho_prev[j], bnd);
+            }, flush);
+    } else {
+        float4* sp = tile_smem;
+        float4* sv = tile_smem + kTileCap;
+        float* sr = reinterpret_cast<float*>(tile_smem + 2 * kTileCap);
+        __shared__ TileStage stg;
+        const float4* src4[2] = {s.pos, s.vel};
+        float4* dst4[2] = {sp, sv};
+        const TileSlab slab = slab_at(tile_smem, 36, T.K);
+        stage_tile_async<2, false, !kL1GlobalEntries>(stg, d, h, rg, src4, dst4, s.rho_prev, sr, T, slab);
+        const uint32_t cnt = kL1GlobalEntries ? T.count[kk] : 0u;
+        uint2 ahead[AHEAD];
+        prefetch_tile_list<kL1GlobalEntries>(T, h, k, half, ahead);
+        if (!stage_tile_wait(stg, status)) return;
+        if (valid)
+            walk_tile_list<kL1GlobalEntries, false, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool bnd) {
+                pair(at_offset(sp, off), at_offset(sv, off), at_offset(sr, off >> 2), bnd);
+            }, flush);
+    }
     const V3<float> vs = pair_total(visc);
     const float rk = pair_total(rho);
     if (half || !valid) return;
@@ -710,34 +735,15 @@ __global__ void __launch_bounds__(kPassThreads, kL2GlobalEntries ? 4 : 3) k_tile
     if (__syncthreads_or(err)) return;   // one decision for the whole block
     const float dt = sc[scene].dt;
     ErrPart o;
-    if (h.nranges == kTileFallback) {
-        if (valid && !half) {
-            iisph3d_l2_one<float, true, false>(k, s, L, c, dt);
-            o = iisph3d_first_iteration<float>(k, s, c, dt, s.vstar[k], s.anp[k].w);
-        }
-        reduce_err_parts(o, sc, scene);
-        return;
-    }
-    float4* sp = tile_smem;
-    float4* sa = tile_smem + kTileCap;
-    __shared__ TileStage stg;
-    const float4* src4[2] = {s.pos, s.vstar};
-    float4* dst4[2] = {sp, sa};
-    const TileSlab slab = slab_at(tile_smem, 32, T.K);
-    stage_tile_async<2, false, !kL2GlobalEntries>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
     const float4 pk = s.pos[kk], vsk = s.vstar[kk];
     const float rk = s.rho[kk];
-    const uint32_t cnt = kL2GlobalEntries ? T.count[kk] : 0u;
-    if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     Acc<float, true> contrib, mg2;
     Acc3<float, true> mg, gb;
     float cpart = 0.f, g2part = 0.f;
     V3<float> mpart = v3<float>(0.f, 0.f, 0.f), bpart = v3<float>(0.f, 0.f, 0.f);
     const float wb = c.single_layer ? c.two_gamma : 2.f;
-    uint2 ahead[kL2Ahead];
-    if (valid) walk_tile_list<kL2GlobalEntries, false, kL2Ahead>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool bnd) {
-        const float4 pj = at_offset(sp, off), vsj = at_offset(sa, off);
+    auto pair = [&](const float4& pj, const float4& vsj, bool bnd) {
         const V3<float> xij = sub3(pk, pj);
         const float r2 = r2_of(xij);
         const float f = S.grad(r2);
@@ -747,14 +753,37 @@ __global__ void __launch_bounds__(kPassThreads, kL2GlobalEntries ? 4 : 3) k_tile
         if (!bnd) g2part = __fmaf_rn(mf * f, r2, g2part);
         else bpart = fma3(mf, xij, bpart);
         mpart = fma3(mf, xij, mpart);
-    }, [&] {
+    };
+    auto flush = [&] {
         contrib.add(cpart);
         mg2.add(g2part);
         mg.add(mpart);
         gb.add(bpart);
         cpart = g2part = 0.f;
         mpart = bpart = v3<float>(0.f, 0.f, 0.f);
-    });
+    };
+    if (h.nranges == kTileFallback) {
+        // the owner's 32-bit list, split between its two threads; the same sums
+        // as a tiled owner's, so that gbnd is there for the pressure passes
+        if (valid)
+            walk_fallback_list<false>(L, k, half, [&](uint32_t j, bool bnd) { pair(s.pos[j], s.vstar[j], bnd); },
+                                      flush);
+    } else {
+        float4* sp = tile_smem;
+        float4* sa = tile_smem + kTileCap;
+        __shared__ TileStage stg;
+        const float4* src4[2] = {s.pos, s.vstar};
+        float4* dst4[2] = {sp, sa};
+        const TileSlab slab = slab_at(tile_smem, 32, T.K);
+        stage_tile_async<2, false, !kL2GlobalEntries>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
+        const uint32_t cnt = kL2GlobalEntries ? T.count[kk] : 0u;
+        if (!stage_tile_wait(stg, status)) return;
+        uint2 ahead[kL2Ahead];
+        if (valid)
+            walk_tile_list<kL2GlobalEntries, false, kL2Ahead>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool bnd) {
+                pair(at_offset(sp, off), at_offset(sa, off), bnd);
+            }, flush);
+    }
     const float ct = pair_total(contrib), g2 = pair_total(mg2);
     const V3<float> m = pair_total(mg), gbt = pair_total(gb);
     // the inner sum of d_ii, -sum_fluid m_j gradW - lambda sum_bnd m_j gradW, from the two sums above
@@ -790,41 +819,45 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
     // iterating owners ends at once
     const bool live = k < n_fluid && !sc[s.scene_of(k)].done;
     if (__syncthreads_or(err) || !__syncthreads_or(live)) return;
-    if (h.nranges == kTileFallback) {
-        if (live && !half) iisph3d_pressure_acc_one<float, true>(k, s, L, c);
-        return;
-    }
-    float4* sp = tile_smem;
-    float* sa = reinterpret_cast<float*>(tile_smem + kTileCap);
-    __shared__ TileStage stg;
-    const float4* src4[1] = {s.pos};
-    float4* dst4[1] = {sp};
-    const TileSlab slab = slab_at(tile_smem, 20, T.K);
-    // boundary neighbors enter through sum_bnd m_j gradW (second loop), so
-    // only the fluid candidates and entries are visited
-    stage_tile_async<1, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, s.p, sa, T, slab);
     const bool valid = live;
     const int64_t kk = valid ? k : 0;
     const float4 pk = s.pos[kk], gbk = s.gbnd[kk];
     const float prk = s.p[kk];
-    const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
-    uint2 ahead[AHEAD];
-    prefetch_tile_list<kPressureGlobalEntries>(T, h, k, half, ahead);
-    if (!stage_tile_wait(stg, status)) return;
     const FastSpline S(c.kern);
     Acc3<float, true> pa;
     V3<float> part = v3<float>(0.f, 0.f, 0.f);
-    auto pair = [&](uint32_t off, bool) {
-        const float4 pj = at_offset(sp, off);
+    auto pair = [&](const float4& pj, float prj) {
         const V3<float> xij = sub3(pk, pj);
-        const float coef = pj.w * (prk + at_offset(sa, off >> 2)) * S.grad(r2_of(xij));
+        const float coef = pj.w * (prk + prj) * S.grad(r2_of(xij));
         part = fma3(-coef, xij, part);
     };
     auto flush = [&] {
         pa.add(part);
         part = v3<float>(0.f, 0.f, 0.f);
     };
-    if (valid) walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, pair, flush);
+    // boundary neighbors enter through sum_bnd m_j gradW (second loop), so
+    // only the fluid candidates and entries are visited
+    if (h.nranges == kTileFallback) {
+        // the owner's 32-bit list, split between its two threads
+        if (valid)
+            walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.p[j]); }, flush);
+    } else {
+        float4* sp = tile_smem;
+        float* sa = reinterpret_cast<float*>(tile_smem + kTileCap);
+        __shared__ TileStage stg;
+        const float4* src4[1] = {s.pos};
+        float4* dst4[1] = {sp};
+        const TileSlab slab = slab_at(tile_smem, 20, T.K);
+        stage_tile_async<1, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, s.p, sa, T, slab);
+        const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
+        uint2 ahead[AHEAD];
+        prefetch_tile_list<kPressureGlobalEntries>(T, h, k, half, ahead);
+        if (!stage_tile_wait(stg, status)) return;
+        if (valid)
+            walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool) {
+                pair(at_offset(sp, off), at_offset(sa, off >> 2));
+            }, flush);
+    }
     const V3<float> a = pair_total(pa);
     if (half || !valid) return;
     // boundary: - sum_bnd (lambda m_j p_i / rho0^2) gradW, lambda = 2 gamma (single layer) or 2
@@ -853,8 +886,26 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
     if (__syncthreads_or(err) || !__syncthreads_or(live)) return;
     const float dt = q->dt;
     ErrPart o;
+    // the owner's own data, loaded while the staging lands
+    const bool valid = live;
+    const float4 pk = s.pos[kk], ak = s.acc[kk], vsk = s.vstar[kk], gbk = s.gbnd[kk];
+    const float aii = s.anp[kk].w, prk = s.p[kk];
+    const FastSpline S(c.kern);
+    Acc<float, true> ap;
+    float part = 0.f;
+    auto pair = [&](const float4& pj, const float4& aj) {
+        const V3<float> xij = sub3(pk, pj);
+        part = __fmaf_rn(pj.w * S.grad(r2_of(xij)), dot3(sub3(ak, aj), xij), part);
+    };
+    auto flush = [&] {
+        ap.add(part);
+        part = 0.f;
+    };
+    // boundary neighbors enter through sum_bnd m_j gradW (second loop)
+    bool done = true;
     if (h.nranges == kTileFallback) {
-        if (live && !half) o = iisph3d_pressure_update_one<float, true>(k, s, L, c, dt);
+        // the owner's 32-bit list, split between its two threads
+        if (valid) walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.acc[j]); }, flush);
     } else {
         float4* sp = tile_smem;
         float4* sa = tile_smem + kTileCap;
@@ -862,34 +913,21 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
         const float4* src4[2] = {s.pos, s.acc};
         float4* dst4[2] = {sp, sa};
         const TileSlab slab = slab_at(tile_smem, 32, T.K);
-        // boundary neighbors enter through sum_bnd m_j gradW (second loop)
         stage_tile_async<2, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
-        // the owner's own data, loaded while the staging lands
-        const bool valid = live;
-        const float4 pk = s.pos[kk], ak = s.acc[kk], vsk = s.vstar[kk], gbk = s.gbnd[kk];
-        const float aii = s.anp[kk].w, prk = s.p[kk];
         const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
         uint2 ahead[AHEAD];
         prefetch_tile_list<kPressureGlobalEntries>(T, h, k, half, ahead);
-        if (stage_tile_wait(stg, status)) {
-            const FastSpline S(c.kern);
-            Acc<float, true> ap;
-            float part = 0.f;
-            auto pair = [&](uint32_t off, bool) {
-                const float4 pj = at_offset(sp, off);
-                const V3<float> xij = sub3(pk, pj);
-                part = __fmaf_rn(pj.w * S.grad(r2_of(xij)), dot3(sub3(ak, at_offset(sa, off)), xij), part);
-            };
-            auto flush = [&] {
-                ap.add(part);
-                part = 0.f;
-            };
-            if (valid) walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, pair, flush);
-            // boundary: sum_bnd m_j dot(a_i, gradW) = dot(a_i, sum_bnd m_j gradW)
-            const float sum = pair_total(ap) + dot3(v3<float>(ak.x, ak.y, ak.z), v3<float>(gbk.x, gbk.y, gbk.z));
-            if (!half && valid)
-                o = iisph3d_pressure_update_tail<float>(k, s, c, dt, v3<float>(ak.x, ak.y, ak.z), sum, vsk, aii, prk);
-        }
+        done = stage_tile_wait(stg, status);
+        if (done && valid)
+            walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool) {
+                pair(at_offset(sp, off), at_offset(sa, off));
+            }, flush);
+    }
+    if (done) {
+        // boundary: sum_bnd m_j dot(a_i, gradW) = dot(a_i, sum_bnd m_j gradW)
+        const float sum = pair_total(ap) + dot3(v3<float>(ak.x, ak.y, ak.z), v3<float>(gbk.x, gbk.y, gbk.z));
+        if (!half && valid)
+            o = iisph3d_pressure_update_tail<float>(k, s, c, dt, v3<float>(ak.x, ak.y, ak.z), sum, vsk, aii, prk);
     }
     reduce_err_parts(o, sc, scene);
 }
