@@ -17,8 +17,9 @@
 //
 // A tile whose owners touch the grid's border cells, form more than
 // kTileGroups groups, or need more than kTileCap staged candidates is a
-// fallback tile: its owners get the ordinary 32-bit slot-major lists and the
-// passes run the per-pair gather code of fs_solvers.cuh for them.
+// fallback tile: its owners get the ordinary 32-bit slot-major lists, which
+// the two threads of an owner split in the passes, with the pair arithmetic
+// of the tiled owners and the neighbors' data read from global memory.
 //
 // The neighbor sets are the contract's (hashed 3D: dot(d, d) <= r * r over
 // the 27 cells, fs_search.cuh); only the summation order differs from the
