@@ -4,7 +4,10 @@
 // include/fluidsolver_b200.h. They mirror the reference solvers' public
 // surface -- `parameters`, `data`, `settings`, the IISPH statistics and the
 // neighborhood interface -- so that SolverSerializer, the Simulator, entities
-// and sensors use them unchanged (see INTEGRATION.md for the registration).
+// and sensors use them unchanged. To be selectable from scenario files they
+// are registered where the reference maps its type strings to solver types
+// (SolverSerializer.cpp:137-219 and the dynamic_pointer_cast chains of
+// :15-95, FluidSolverTypes.cpp, IisphSensor.cpp:61-78).
 //
 //   LibFluid::Cuda::IISPHFluidSolver3D   replaces IISPHFluidSolver3D<...>  (IISPHFluidSolver3D.hpp:22-610)
 //   LibFluid::Cuda::SESPHFluidSolver3D   replaces SESPHFluidSolver3D<...>  (SESPHFluidSolver3D.hpp:12-339)

@@ -286,7 +286,7 @@ def position_query_fixture():
 
 if __name__ == "__main__":
     if not R.available():
-        sys.exit("oracle/_ref is not built; run `make -C oracle/ref` where the reference checkout is available")
+        sys.exit("oracle/_ref is not built; run `make -C oracle/ref REF=<reference checkout>` where it is available")
     fixtures = {"kernel": kernel_fixture, "cfl": cfl_fixture, "search": search_fixture, "solvers": solver_fixture,
                 "position_queries": position_query_fixture, "dynamic_timestep": dynamic_timestep_fixture,
                 "boundary": boundary_fixture, "raytrace": raytrace_fixture}

@@ -18,7 +18,9 @@ from fluidsolver_b200 import _lib as F
 from fluidsolver_b200 import read_particles, write_particles
 from fluidsolver_b200.solver import ParticleCollection
 
-REFERENCE = "/root/reference"
+from oracle.reference_path import reference_dir
+
+REFERENCE = reference_dir()
 
 
 def _liblz4():
