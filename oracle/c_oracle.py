@@ -43,7 +43,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_global_stats.argtypes = [c_int, c_int64] + [c_void_p] * 6 + [c_float, c_float, c_void_p, c_void_p]
         L.oracle_ns.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_float, c_void_p, c_void_p]
         L.oracle_ns.restype = c_int64
-        L.oracle_run.argtypes = [c_void_p, c_int64, c_int] + [c_void_p] * 13 + [c_int, c_void_p, c_int]
+        L.oracle_run.argtypes = [c_void_p, c_int64, c_int] + [c_void_p] * 13 + [c_int, c_void_p, c_int] + \
+            [c_void_p] * 3
         L.oracle_run.restype = c_int
         _lib = L
     return _lib
@@ -198,6 +199,11 @@ class State:
         self.source_term = np.zeros(n, np.float32)
         self.diagonal_element = np.zeros(n, np.float32)
         self.density_error = np.zeros(n, np.float32)
+        # the 2D hashed grid's history across steps (HashedNeighborhoodSearch.cpp:117-151):
+        # each particle's cell (none yet) and the sequence number of its last insertion
+        self.h2d_cell = np.full((n, 2), np.iinfo(np.int32).max, np.int32)
+        self.h2d_seq = np.zeros(n, np.int64)
+        self.h2d_counter = np.zeros(1, np.int64)
 
     def run(self, cfg: np.ndarray, steps: int = 1, abs_int: bool = False) -> np.ndarray:
         """Advances `steps` steps; returns per-step {desired, actual dt, iterations, avg error}."""
@@ -205,7 +211,8 @@ class State:
         r = lib().oracle_run(_p(cfg), self.n, self.dim, _p(self.position), _p(self.velocity), _p(self.acceleration),
                              _p(self.external), _p(self.mass), _p(self.density), _p(self.pressure), _p(self.type),
                              _p(self.predicted_velocity), _p(self.non_pressure_acceleration), _p(self.source_term),
-                             _p(self.diagonal_element), _p(self.density_error), steps, _p(stats), 1 if abs_int else 0)
+                             _p(self.diagonal_element), _p(self.density_error), steps, _p(stats), 1 if abs_int else 0,
+                             _p(self.h2d_cell), _p(self.h2d_seq), _p(self.h2d_counter))
         if r != 0:
             raise RuntimeError("oracle_run failed")
         return stats

@@ -254,6 +254,7 @@ static int ns_within(int dim, v3 d, float r, float r2) {
 typedef struct {
     int c[3];
     int64_t i;
+    int64_t ord;   /* order within the cell: the index, or the hashed-2d insertion sequence */
 } cell_entry;
 
 typedef struct {
@@ -265,6 +266,23 @@ static int cellc(float x, float r) { return (int)floorf(x / r); }
 /* HashedNeighborhoodSearch (2D) truncates toward zero (HashedNeighborhoodSearch.cpp:108-115) */
 static int g_truncate_cells = 0;
 static int cellk(float x, float r) { return g_truncate_cells ? (int)(x / r) : (int)floorf(x / r); }
+
+/* The 2D hashed grid's history (HashedNeighborhoodSearch::UpdateGrid,
+ * HashedNeighborhoodSearch.cpp:117-151). Its cells are std::lists that the
+ * reference updates incrementally: for i ascending, a particle whose cell
+ * changed is removed from the old list and appended to the new one. So the
+ * order within a cell is the order of arrival: by the sequence number of
+ * the particle's last insertion, which a running counter hands out in that
+ * loop. cell[2 i], cell[2 i + 1] hold particle i's current cell (INT32_MAX
+ * before the first search, like currentStatus), seq[i] its sequence number;
+ * *counter is the next one. Without a history (NULL) the order is the first
+ * call's: ascending index. */
+typedef struct {
+    int32_t* cell;
+    int64_t* seq;
+    int64_t* counter;
+} h2d_history_t;
+static h2d_history_t g_h2d = {0, 0, 0};
 
 static int cell_cmp3(const int* a, const int* b) {
     for (int k = 2; k >= 0; k--) {
@@ -278,7 +296,7 @@ static int entry_cmp(const void* pa, const void* pb) {
     const cell_entry* b = (const cell_entry*)pb;
     int c = cell_cmp3(a->c, b->c);
     if (c) return c;
-    return a->i < b->i ? -1 : (a->i > b->i ? 1 : 0);
+    return a->ord < b->ord ? -1 : (a->ord > b->ord ? 1 : 0);
 }
 
 static void grid_build(grid_t* g, int dim, int64_t n, const float* pos, const uint8_t* type, int kind, float r) {
@@ -292,6 +310,16 @@ static void grid_build(grid_t* g, int dim, int64_t n, const float* pos, const ui
         e->c[1] = cellk(p.y, r);
         e->c[2] = dim == 3 ? cellk(p.z, r) : 0;
         e->i = i;
+        e->ord = i;
+        if (kind == NS_HASHED_2D && g_h2d.cell) {
+            int32_t* hc = g_h2d.cell + 2 * i;
+            if (hc[0] != e->c[0] || hc[1] != e->c[1]) {
+                hc[0] = e->c[0];
+                hc[1] = e->c[1];
+                g_h2d.seq[i] = (*g_h2d.counter)++;
+            }
+            e->ord = g_h2d.seq[i];
+        }
     }
     qsort(g->e, (size_t)g->m, sizeof(cell_entry), entry_cmp);
 }
@@ -833,10 +861,14 @@ static float step_iisph2d(const cfg_t* c, state_t* s, float desired, int* iterat
 /* Runs `steps` steps of solver c on the state arrays in place (input order;
  * vstar/anp: dim floats per particle, source/diag/err one float; any of the
  * IISPH arrays may be NULL). stats receives per step
- * {desired dt, actual dt, iterations, avg density error}. */
+ * {desired dt, actual dt, iterations, avg density error}. h2d_cell / h2d_seq /
+ * h2d_counter: the 2D hashed grid's history (h2d_history_t), kept by the
+ * caller across calls like the reference's search object keeps its grid
+ * across steps; NULL for a fresh grid at every step. */
 int oracle_run(const float* cfg, int64_t n, int dim, float* pos, float* vel, float* acc, float* ext, float* mass,
                float* density, float* pressure, uint8_t* type, float* vstar, float* anp, float* source, float* diag,
-               float* err, int steps, float* stats, int abs_int) {
+               float* err, int steps, float* stats, int abs_int, int32_t* h2d_cell, int64_t* h2d_seq,
+               int64_t* h2d_counter) {
     cfg_t c;
     c.solver = (int)cfg[0];
     c.ns_kind = (int)cfg[1];
@@ -873,6 +905,9 @@ int oracle_run(const float* cfg, int64_t n, int dim, float* pos, float* vel, flo
     s.source = source ? source : (own[2] = (float*)calloc((size_t)n, sizeof(float)));
     s.diag = diag ? diag : (own[3] = (float*)calloc((size_t)n, sizeof(float)));
     s.err = err ? err : (own[4] = (float*)calloc((size_t)n, sizeof(float)));
+    g_h2d.cell = h2d_cell;
+    g_h2d.seq = h2d_seq;
+    g_h2d.counter = h2d_counter;
     for (int st = 0; st < steps; st++) {
         int its = 0;
         float avg = 0.0f, dt = 0.0f;
@@ -892,5 +927,8 @@ int oracle_run(const float* cfg, int64_t n, int dim, float* pos, float* vel, flo
         }
     }
     for (int q = 0; q < 5; q++) free(own[q]);
+    g_h2d.cell = 0;
+    g_h2d.seq = 0;
+    g_h2d.counter = 0;
     return 0;
 }
