@@ -2,7 +2,6 @@
 // context management, host transfers, the neighborhood-search pipeline and
 // the per-solver step sequences.
 #include <cuda_runtime.h>
-#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -249,7 +248,7 @@ fs_status free_all(fs_ctx* c) {
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc[0], c->acc[1], c->ext[0], c->ext[1],
                     c->rho[0], c->rho[1], c->p[0], c->p[1], c->type[0], c->type[1], c->hidx[0], c->hidx[1],
                     c->rho_prev, c->vstar, c->anp, c->err, c->gbnd, c->tile_desc, c->tile_ent, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
-                    c->perm[0], c->perm[1], c->cub_temp, c->cell_start, c->cell_counts, c->bbox, c->grids, c->nbr, c->nbr_count,
+                    c->perm[0], c->perm[1], c->h2d_cell, c->h2d_rank, c->sort_hist, c->cell_start, c->bbox, c->grids, c->nbr, c->nbr_count,
                     c->scene_of[0], c->scene_of[1], c->d_scene_offsets,
                     c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->scalars,
                     c->stats_parts, c->stats_out};
@@ -349,7 +348,7 @@ fs_status choose_grids(fs_ctx* c, const int* lo, const int* hi) {
     return FS_OK;
 }
 
-// cell tables for the current dims (and the scan's temporary storage)
+// cell tables for the current dims
 fs_status ensure_cells(fs_ctx* c) {
     c->key_bits = 1;
     while ((int64_t(1) << c->key_bits) < c->cells) c->key_bits++;
@@ -358,20 +357,9 @@ fs_status ensure_cells(fs_ctx* c) {
     if (!c->cell_start || c->cell_alloc < need) {
         clear_graphs(c);
         if (c->cell_start) cudaFree(c->cell_start);
-        if (c->cell_counts) cudaFree(c->cell_counts);
-        c->cell_start = c->cell_counts = nullptr;
+        c->cell_start = nullptr;
         FS_TRY(dalloc(&c->cell_start, (size_t)3 * need));
-        FS_TRY(dalloc(&c->cell_counts, (size_t)3 * need));
         c->cell_alloc = need;
-    }
-    size_t temp = 0;
-    FS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, c->cell_counts, c->cell_start, (int)(3 * need), c->stream));
-    if (temp > c->cub_temp_bytes) {
-        clear_graphs(c);
-        if (c->cub_temp) cudaFree(c->cub_temp);
-        c->cub_temp = nullptr;
-        FS_CUDA(cudaMalloc(&c->cub_temp, temp));
-        c->cub_temp_bytes = temp;
     }
     return FS_OK;
 }
@@ -643,39 +631,47 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     c->launches++;
     k_keys<R><<<grid_for(n), kBlock, 0, st>>>(n, s.pos, s.type, s.hidx, c->include_inactive, single, c->search_radius,
                                               c->truncate_cells, c->grids, s.scene, c->key_bits, c->keys[0], k64,
-                                              c->perm[0], c->status);
+                                              c->perm[0], c->h2d_cell, c->h2d_rank, c->status);
     FS_CUDA(cudaGetLastError());
-    size_t temp = c->cub_temp_bytes;
+    // stable radix sort of (key, current index) over the key's bits (fs_sort.cuh)
+    uint32_t* const vals[2] = {c->perm[0], c->perm[1]};
+    int res;
     if (single) {
-        FS_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_temp, temp, c->keys64[0], c->keys64[1], c->perm[0], c->perm[1],
-                                                (int)n, 0, 32 + c->key_bits + 2, st));
+        unsigned long long* const kk[2] = {c->keys64[0], c->keys64[1]};
+        res = sort_pairs(n, 32 + c->key_bits + 2, kk, vals, c->sort_hist, st, c->launches);
     } else {
-        FS_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_temp, temp, c->keys[0], c->keys[1], c->perm[0], c->perm[1],
-                                                (int)n, 0, c->key_bits + 2, st));
+        uint32_t* const kk[2] = {c->keys[0], c->keys[1]};
+        res = sort_pairs(n, c->key_bits + 2, kk, vals, c->sort_hist, st, c->launches);
     }
+    FS_CUDA(cudaGetLastError());
     // gather every persistent field into the other buffer
     const int nx = c->cur ^ 1;
     c->launches++;
     k_reorder<R><<<grid_for(n), kBlock, 0, st>>>(
-        n, c->perm[1], (const V4<R>*)c->pos[c->cur], (V4<R>*)c->pos[nx], (const V4<R>*)c->vel[c->cur],
+        n, c->perm[res], (const V4<R>*)c->pos[c->cur], (V4<R>*)c->pos[nx], (const V4<R>*)c->vel[c->cur],
         (V4<R>*)c->vel[nx], (const V4<R>*)c->acc[c->cur], (V4<R>*)c->acc[nx], (const V4<R>*)c->ext[c->cur],
         (V4<R>*)c->ext[nx], (const R*)c->rho[c->cur], (R*)c->rho[nx], (const R*)c->p[c->cur], (R*)c->p[nx],
         c->type[c->cur], c->type[nx], c->hidx[c->cur], c->hidx[nx], c->scene_of[c->cur], c->scene_of[nx]);
     FS_CUDA(cudaGetLastError());
     c->cur = nx;
     s = state_of<R>(c);
-    // cell-start table: per-cell counts of every region, then one exclusive
-    // scan over the concatenated tables (regions are consecutive blocks of the
-    // sorted order, so region g's entries come out offset by its first index)
+    // cell-start table of the concatenated per-region tables, read off the
+    // sorted keys (regions are consecutive blocks of the sorted order)
     const int64_t table = (int64_t)c->regions * (c->cells + 1);
-    FS_CUDA(cudaMemsetAsync(c->cell_counts, 0, sizeof(uint32_t) * table, st));
     c->launches++;
-    k_cell_counts<<<grid_for(c->n_struct), kBlock, 0, st>>>(c->n_struct, single ? nullptr : c->keys[1],
-                                                            single ? c->keys64[1] : nullptr, c->cells, c->key_bits,
-                                                            c->cell_counts);
+    if (single)
+        k_cell_start_fill<unsigned long long><<<grid_for(c->n_struct + 1), kBlock, 0, st>>>(
+            c->n_struct, c->keys64[res], 32, c->key_bits, c->cells, table, c->cell_start);
+    else
+        k_cell_start_fill<uint32_t><<<grid_for(c->n_struct + 1), kBlock, 0, st>>>(
+            c->n_struct, c->keys[res], 0, c->key_bits, c->cells, table, c->cell_start);
     FS_CUDA(cudaGetLastError());
-    temp = c->cub_temp_bytes;
-    FS_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_temp, temp, c->cell_counts, c->cell_start, (int)table, st));
+    if (c->h2d_cell) {
+        c->launches++;
+        k_h2d_rank<<<grid_for(c->n_struct), kBlock, 0, st>>>(c->n_struct, c->keys64[res], c->cells, c->key_bits,
+                                                             c->cell_start, s.hidx, c->h2d_rank);
+        FS_CUDA(cudaGetLastError());
+    }
     if (solver_lists) {
         WalkParams w = walk_of(c, true);
         const uint32_t owners = 1u << FS_TYPE_NORMAL;
@@ -1358,6 +1354,10 @@ static fs_status create_ctx(const fs_params* p, int32_t scenes, const int64_t* o
         FS_ALLOC(c->perm[b], cap);
         if (c->reference_order) FS_ALLOC(c->keys64[b], cap);
     }
+    if (c->truncate_cells) {
+        FS_ALLOC(c->h2d_cell, cap);
+        FS_ALLOC(c->h2d_rank, cap);
+    }
     FS_ALLOC(*(char**)&c->rho_prev, cap * r1);
     FS_ALLOC(*(char**)&c->vstar, cap * v4);
     FS_ALLOC(*(char**)&c->anp, cap * v4);
@@ -1379,18 +1379,8 @@ static fs_status create_ctx(const fs_params* p, int32_t scenes, const int64_t* o
     FS_ALLOC(c->nbr_count, (cap + kTileOwners - 1) / kTileOwners * kTileOwners);   // whole tiles
     if (cudaMallocHost((void**)&c->scalars_host, sizeof(StepScalars) * S) != cudaSuccess)
         return bail(fail(FS_ERR_CUDA, "cudaMallocHost failed"));
-    // CUB temp storage for the largest sort
-    size_t temp = 0;
-    if (c->reference_order)
-        cub::DeviceRadixSort::SortPairs(nullptr, temp, c->keys64[0], c->keys64[1], c->perm[0], c->perm[1], (int)cap, 0,
-                                        64, c->stream);
-    else
-        cub::DeviceRadixSort::SortPairs(nullptr, temp, c->keys[0], c->keys[1], c->perm[0], c->perm[1], (int)cap, 0, 32,
-                                        c->stream);
-    size_t scan_temp = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, scan_temp, (uint32_t*)nullptr, (int64_t*)nullptr, (int)cap + 1, c->stream);
-    c->cub_temp_bytes = std::max(temp, scan_temp);
-    FS_ALLOC(*(char**)&c->cub_temp, c->cub_temp_bytes);
+    // the radix sort's per-tile digit counts for the largest sort
+    FS_ALLOC(c->sort_hist, (size_t)sort_hist_entries((int64_t)cap));
     int K = p->neighbor_capacity > 0 ? p->neighbor_capacity : (p->dim == 2 ? 32 : 64);
     if (contract_capacity(p->search) > 0) K = std::min(K, contract_capacity(p->search) + 1);
     {
@@ -1452,6 +1442,13 @@ fs_status fs_upload(fs_ctx* c, const fs_particles* in) {
     FS_TRY(ensure_cells(c));
     fs_status r = c->precision == FS_PRECISION_FP64 ? pack_upload<double>(c, d, in->n) : pack_upload<float>(c, d, in->n);
     if (r != FS_OK) return r;
+    // The 2D hashed grid's history lives as long as the context, like the
+    // reference's search object, whose grid survives changes of the
+    // collection's contents; a different particle count starts it afresh.
+    if (c->h2d_rank && c->h2d_n != in->n) {
+        FS_CUDA(cudaMemsetAsync(c->h2d_rank, 0xff, sizeof(uint32_t) * (size_t)c->cap, c->stream));
+        c->h2d_n = in->n;
+    }
     c->have_state = true;
     c->have_lists = false;
     c->have_cells = false;
@@ -1522,8 +1519,9 @@ fs_status fs_get_neighbors_csr(fs_ctx* c, int64_t* offsets, int64_t* indices, in
                                                             c->csr_counts);
     }
     FS_CUDA(cudaGetLastError());
-    size_t temp = c->cub_temp_bytes;
-    FS_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_temp, temp, c->csr_counts, c->csr_offsets, (int)(n + 1), st));
+    c->launches++;
+    k_scan_exclusive<uint32_t, int64_t><<<1, 1024, 0, st>>>(c->csr_counts, c->csr_offsets, n + 1);
+    FS_CUDA(cudaGetLastError());
     int64_t tot = 0;
     FS_CUDA(cudaMemcpyAsync(&tot, c->csr_offsets + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     FS_CUDA(cudaStreamSynchronize(st));

@@ -24,6 +24,7 @@
 
 #include "fs_common.cuh"
 #include "fs_entities.cuh"
+#include "fs_sort.cuh"
 #include "fs_tiles.cuh"
 
 struct fs_ctx {
@@ -75,10 +76,15 @@ struct fs_ctx {
     uint32_t* keys[2] = {};
     unsigned long long* keys64[2] = {};
     uint32_t* perm[2] = {};
-    void* cub_temp = nullptr;
-    size_t cub_temp_bytes = 0;
+    // the 2D hashed grid's history in the reference-order mode, per HOST index
+    // (HashedNeighborhoodSearch.cpp:117-151 keeps each cell's particles in
+    // order of arrival): the particle's last cell and its rank in the sorted
+    // order of that cell (0xffffffff: no cell yet, it arrives at the next search)
+    int2* h2d_cell = nullptr;
+    uint32_t* h2d_rank = nullptr;
+    int64_t h2d_n = -1;               // particle count the history belongs to
+    uint32_t* sort_hist = nullptr;    // per-tile digit counts of the radix sort (fs_sort.cuh)
     uint32_t* cell_start = nullptr;   // [regions][cells + 1] first sorted index of cell >= c
-    uint32_t* cell_counts = nullptr;  // [regions][cells + 1] scratch for the scan
     int64_t cells = 0;                // dims[0] * dims[1] * dims[2]
     int key_bits = 30;                // bits of the linear cell index in the sort keys
     int64_t cell_alloc = 0;           // entries allocated per table

@@ -160,17 +160,26 @@ __device__ __forceinline__ uint32_t region_of(uint8_t t, bool single_region) {
     return t == FS_TYPE_NORMAL ? 0u : (t == FS_TYPE_BOUNDARY ? 1u : 2u);
 }
 
+// Sort keys of every particle. keys64 (the reference-order mode) appends a
+// 32-bit order within the cell: the host index, or, with the 2D hashed grid's
+// history (h2d_cell / h2d_rank per host index, null otherwise), the arrival
+// order of HashedNeighborhoodSearch::UpdateGrid (HashedNeighborhoodSearch.cpp:117-151):
+// a particle that stays in its cell keeps its rank from the last search, and
+// one that arrives goes after every stayer, arrivals by ascending index (the
+// reference appends them to the cell's std::list in its i-ascending loop).
 template <typename R>
 __global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
                        const uint32_t* __restrict__ hidx, bool include_inactive, bool single_region, float r,
                        bool trunc, const SceneGrid* __restrict__ grids, const uint16_t* __restrict__ scene,
                        int key_bits, uint32_t* __restrict__ keys,
                        unsigned long long* __restrict__ keys64, uint32_t* __restrict__ perm,
+                       int2* __restrict__ h2d_cell, const uint32_t* __restrict__ h2d_rank,
                        int* __restrict__ status) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     uint8_t t = type[k];
     uint32_t key;
+    uint32_t order = keys64 ? hidx[k] : 0u;
     if (!include_inactive && t == FS_TYPE_INACTIVE) {
         key = inactive_key(key_bits);
     } else {
@@ -184,15 +193,42 @@ __global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* 
         }
         const SceneGrid g = grids[scene ? scene[k] : 0];
         bool cl = false;
-        int lx = local_cell(cell_coord<R>(p.x, r, trunc), g.o0, g.d0, cl);
-        int ly = local_cell(cell_coord<R>(p.y, r, trunc), g.o1, g.d1, cl);
+        const int cx = cell_coord<R>(p.x, r, trunc), cy = cell_coord<R>(p.y, r, trunc);
+        int lx = local_cell(cx, g.o0, g.d0, cl);
+        int ly = local_cell(cy, g.o1, g.d1, cl);
         int lz = local_cell(cell_coord<R>(p.z, r, trunc), g.o2, g.d2, cl);
         const uint32_t lin = (uint32_t)(g.base + ((int64_t)lz * g.d1 + ly) * g.d0 + lx);
         key = (region_of(t, single_region) << key_bits) | lin;
+        if (h2d_cell) {
+            const uint32_t h = order;
+            const int2 was = h2d_cell[h];
+            const uint32_t rank = h2d_rank[h];
+            if (rank != 0xffffffffu && was.x == cx && was.y == cy) {
+                order = rank;
+            } else {
+                order = 0x80000000u | h;
+                h2d_cell[h] = make_int2(cx, cy);
+            }
+        }
     }
-    if (keys64) keys64[k] = ((unsigned long long)key << 32) | hidx[k];
+    if (keys64) keys64[k] = ((unsigned long long)key << 32) | order;
     else keys[k] = key;
     perm[k] = (uint32_t)k;
+}
+
+// The 2D hashed grid's history after a sort (see k_keys): every particle's
+// rank within its cell of the new sorted order, stored by host index. Ranks
+// are relative to the device cell, which may hold several true cells of a
+// clamped grid; within each true cell they order its members as the
+// reference's list does, which is all the walks need.
+__global__ void k_h2d_rank(int64_t n_struct, const unsigned long long* __restrict__ keys64, int64_t cells,
+                           int key_bits, const uint32_t* __restrict__ cell_start, const uint32_t* __restrict__ hidx,
+                           uint32_t* __restrict__ h2d_rank) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n_struct) return;
+    const uint32_t key = (uint32_t)(keys64[k] >> 32);
+    const uint32_t first = cell_start[(int64_t)(key >> key_bits) * (cells + 1) + (key & ((1u << key_bits) - 1u))];
+    h2d_rank[hidx[k]] = (uint32_t)k - first;
 }
 
 // new[k] = old[perm[k]] for every persistent field
@@ -215,21 +251,6 @@ __global__ void k_reorder(int64_t n, const uint32_t* __restrict__ perm, const V4
     t1[k] = t0[s];
     h1[k] = h0[s];
     if (sc0) sc1[k] = sc0[s];
-}
-
-// Per-cell particle counts of every region: the first particle of each run of
-// equal keys writes the run length (the table is zeroed before).
-__global__ void k_cell_counts(int64_t n_struct, const uint32_t* __restrict__ keys,
-                              const unsigned long long* __restrict__ keys64, int64_t cells, int key_bits,
-                              uint32_t* __restrict__ counts) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n_struct) return;
-    auto key_at = [&](int64_t q) -> uint32_t { return keys64 ? (uint32_t)(keys64[q] >> 32) : keys[q]; };
-    const uint32_t key = key_at(k);
-    if (k > 0 && key_at(k - 1) == key) return;
-    int64_t e = k + 1;
-    while (e < n_struct && key_at(e) == key) e++;
-    counts[(int64_t)(key >> key_bits) * (cells + 1) + (key & ((1u << key_bits) - 1u))] = (uint32_t)(e - k);
 }
 
 // ---------------------------------------------------------------------------

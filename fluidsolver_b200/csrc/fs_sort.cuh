@@ -1,0 +1,272 @@
+// The search's sort, written for its keys: a stable least-significant-digit
+// radix sort of (key, value) pairs, and the cell-start table read straight
+// off the sorted keys.
+//
+// The reference sorts its particle collection with a quick sort over 64-bit
+// Morton keys that permutes every component through ParticleCollection::swap
+// (ParticleCollectionAlgorithm.hpp:28-133). Here the keys are the bounded
+// (region, linear cell) indices of fs_search.cuh (key_bits + 2 bits; in the
+// reference-order mode 32 more bits of order within a cell), the values the
+// particles' current positions in the array, and the permutation is applied
+// afterwards by one gather of every field (k_reorder).
+//
+// One pass per 8-bit digit, three kernels each:
+//   k_sort_hist     per-tile digit counts, stored digit-major (hist[d][tile]);
+//   k_sort_rowscan  one block per digit turns its row into exclusive offsets
+//                   over the tiles and stores the digit's total;
+//   k_sort_scatter  every tile takes the digits' first slots (a scan of the
+//                   256 totals) plus its row offsets, ranks its keys per digit
+//                   in input order (warps own consecutive 512-key runs and
+//                   count with match_any) and writes each pair to its slot.
+// Tiles are 4,096 consecutive keys (8 warps x 32 lanes x 16). Because ranks
+// follow input order within a tile and the slots follow tile order, every
+// pass is stable, which makes the whole sort stable: keys that compare equal
+// keep their input order. The searches feed it the previous step's sorted
+// order, so a particle that stays in its cell keeps its place among the
+// cell's particles from step to step.
+#pragma once
+
+#include <algorithm>
+
+#include "fs_common.cuh"
+
+namespace fsb {
+
+constexpr int kSortWarps = 8;
+constexpr int kSortThreads = 32 * kSortWarps;
+constexpr int kSortPerLane = 16;
+constexpr int kSortWarpKeys = 32 * kSortPerLane;            // consecutive keys per warp
+constexpr int kSortTile = kSortWarps * kSortWarpKeys;       // consecutive keys per block
+constexpr int kSortDigits = 256;
+
+inline int64_t sort_tiles(int64_t n) { return (n + kSortTile - 1) / kSortTile; }
+// entries of the per-tile histogram matrix, followed by the 256 digit totals
+inline int64_t sort_hist_entries(int64_t n) {
+    return (int64_t)kSortDigits * std::max<int64_t>(sort_tiles(n), 1) + kSortDigits;
+}
+
+template <typename K> __device__ __forceinline__ uint32_t digit_of(K key, int shift) {
+    return (uint32_t)(key >> shift) & (kSortDigits - 1u);
+}
+
+// hist[d * tiles + t] = keys of tile t whose digit at `shift` is d
+template <typename K>
+__global__ void __launch_bounds__(kSortThreads) k_sort_hist(int64_t n, const K* __restrict__ keys, int shift,
+                                                            int64_t tiles, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[kSortDigits];
+    h[threadIdx.x] = 0u;
+    __syncthreads();
+    const int64_t base = blockIdx.x * (int64_t)kSortTile;
+    const int lane = threadIdx.x & 31;
+#pragma unroll 4
+    for (int r = 0; r < kSortTile / kSortThreads; r++) {
+        const int64_t i = base + r * kSortThreads + threadIdx.x;
+        const bool v = i < n;
+        const uint32_t d = v ? digit_of<K>(keys[i], shift) : 0u;
+        const unsigned act = __ballot_sync(0xffffffffu, v);
+        if (v) {
+            // one shared-memory atomic per run of equal digits in the warp
+            const unsigned peers = __match_any_sync(act, d);
+            if (lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
+        }
+    }
+    __syncthreads();
+    hist[(int64_t)threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Row d of the histogram matrix (block d) into exclusive offsets over the
+// tiles, in place; totals[d] = the digit's keys in all tiles.
+__global__ void __launch_bounds__(kSortThreads) k_sort_rowscan(uint32_t* __restrict__ hist, int64_t tiles,
+                                                               uint32_t* __restrict__ totals) {
+    __shared__ uint32_t s_warp[kSortWarps];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    uint32_t* row = hist + (int64_t)blockIdx.x * tiles;
+    uint32_t carry = 0u;
+    for (int64_t a = 0; a < tiles; a += kSortThreads) {
+        const int64_t i = a + t;
+        const uint32_t v = i < tiles ? row[i] : 0u;
+        uint32_t incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_warp[w] = incl;
+        __syncthreads();
+        uint32_t before = 0u, chunk = 0u;
+#pragma unroll
+        for (int q = 0; q < kSortWarps; q++) {
+            const uint32_t x = s_warp[q];
+            if (q < w) before += x;
+            chunk += x;
+        }
+        if (i < tiles) row[i] = carry + before + incl - v;
+        carry += chunk;
+        __syncthreads();
+    }
+    if (t == 0) totals[blockIdx.x] = carry;
+}
+
+// Exclusive scan of m counts by one block of 1024 threads (each scans a
+// contiguous run, the runs' sums are scanned across the block); used for
+// list exports. out may alias in when both have one type.
+template <typename In, typename Out>
+__global__ void __launch_bounds__(1024) k_scan_exclusive(const In* in, Out* out, int64_t m) {
+    __shared__ Out s_warp[32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int64_t per = (m + 1023) / 1024;
+    const int64_t lo = min(m, (int64_t)t * per), hi = min(m, lo + per);
+    Out sum = 0;
+    for (int64_t i = lo; i < hi; i++) sum += (Out)in[i];
+    // inclusive warp scan, then the warps' totals
+    Out incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const Out y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        Out x = s_warp[lane];
+        Out xi = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Out y = __shfl_up_sync(0xffffffffu, xi, o);
+            if (lane >= o) xi += y;
+        }
+        s_warp[lane] = xi - x;   // exclusive over warps
+    }
+    __syncthreads();
+    Out run = s_warp[w] + incl - sum;
+    for (int64_t i = lo; i < hi; i++) {
+        const Out v = (Out)in[i];
+        out[i] = run;
+        run += v;
+    }
+}
+
+// Scatters tile blockIdx.x of (kin, vin) to its slots: slot of a key =
+// (keys of smaller digits, from totals) + offs[d * tiles + tile] (the row
+// scan of k_sort_hist) + keys of digit d before it in the tile. Warp w ranks
+// its own 512 consecutive keys, 32 at a time in lane order, with a per-warp
+// counter per digit; then the counters turn into each warp's first slot per
+// digit.
+template <typename K>
+__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(int64_t n, const K* __restrict__ kin,
+                                                               const uint32_t* __restrict__ vin, K* __restrict__ kout,
+                                                               uint32_t* __restrict__ vout, int shift, int64_t tiles,
+                                                               const uint32_t* __restrict__ offs,
+                                                               const uint32_t* __restrict__ totals) {
+    __shared__ uint32_t wh[kSortWarps][kSortDigits];
+    __shared__ uint32_t s_base[kSortWarps];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    // first slot of every digit: exclusive scan of the totals (thread d: digit d)
+    uint32_t digit_base;
+    {
+        const uint32_t v = totals[threadIdx.x];
+        uint32_t incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_base[w] = incl;
+        __syncthreads();
+        uint32_t before = 0u;
+#pragma unroll
+        for (int q = 0; q < kSortWarps; q++)
+            if (q < w) before += s_base[q];
+        digit_base = before + incl - v;
+    }
+    for (int d = lane; d < kSortDigits; d += 32) wh[w][d] = 0u;
+    __syncwarp();
+    const int64_t base = blockIdx.x * (int64_t)kSortTile + (int64_t)w * kSortWarpKeys;
+    const unsigned below = (1u << lane) - 1u;
+    K key[kSortPerLane];
+    uint32_t val[kSortPerLane], rank[kSortPerLane];
+#pragma unroll
+    for (int j = 0; j < kSortPerLane; j++) {
+        const int64_t i = base + j * 32 + lane;
+        const bool v = i < n;
+        key[j] = v ? kin[i] : K(0);
+        val[j] = v ? vin[i] : 0u;
+        rank[j] = 0u;
+        const unsigned act = __ballot_sync(0xffffffffu, v);
+        if (v) {
+            const uint32_t d = digit_of<K>(key[j], shift);
+            const unsigned peers = __match_any_sync(act, d);
+            const uint32_t before = wh[w][d];
+            __syncwarp(act);   // every peer has read the counter before the leader moves it
+            rank[j] = before + (uint32_t)__popc(peers & below);
+            if (lane == __ffs(peers) - 1) wh[w][d] = before + (uint32_t)__popc(peers);
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    // per digit: the tile's first slot, then each warp's, in warp order
+    {
+        const int d = threadIdx.x;
+        uint32_t run = digit_base + offs[(int64_t)d * tiles + blockIdx.x];
+#pragma unroll
+        for (int q = 0; q < kSortWarps; q++) {
+            const uint32_t c = wh[q][d];
+            wh[q][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kSortPerLane; j++) {
+        const int64_t i = base + j * 32 + lane;
+        if (i < n) {
+            const uint32_t pos = wh[w][digit_of<K>(key[j], shift)] + rank[j];
+            kout[pos] = key[j];
+            vout[pos] = val[j];
+        }
+    }
+}
+
+// Cell-start table from the sorted keys of the particles in the structure
+// ([0, n_struct)): entry t of the concatenated per-region tables (region g,
+// cell c at t = g (cells + 1) + c; entry g (cells + 1) + cells ends region
+// g) is the first sorted index whose key's entry is >= t. Thread k fills the
+// entries between its predecessor's key and its own; thread n_struct the
+// rest, so every entry is written exactly once and no scan is needed.
+template <typename K>
+__global__ void k_cell_start_fill(int64_t n_struct, const K* __restrict__ keys, int key_shift, int key_bits,
+                                  int64_t cells, int64_t table, uint32_t* __restrict__ cell_start) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k > n_struct) return;
+    auto entry = [&](int64_t q) -> int64_t {
+        const uint32_t key = (uint32_t)(keys[q] >> key_shift);
+        return (int64_t)(key >> key_bits) * (cells + 1) + (key & ((1u << key_bits) - 1u));
+    };
+    const int64_t from = k > 0 ? entry(k - 1) + 1 : 0;
+    const int64_t to = k < n_struct ? entry(k) : table - 1;
+    for (int64_t t = from; t <= to; t++) cell_start[t] = (uint32_t)k;
+}
+
+// Sorts n (key, value) pairs over bits [0, bits) with the passes above,
+// ping-ponging between buffers 0 and 1 of keys and vals. Returns the buffer
+// that holds the result. hist holds sort_hist_entries(n) counters (capacity
+// for at least n keys).
+template <typename K>
+inline int sort_pairs(int64_t n, int bits, K* const (&keys)[2], uint32_t* const (&vals)[2], uint32_t* hist,
+                      cudaStream_t st, int64_t& launches) {
+    const int64_t tiles = sort_tiles(n);
+    uint32_t* totals = hist + (int64_t)kSortDigits * tiles;
+    int cur = 0;
+    if (n <= 1) return cur;
+    for (int shift = 0; shift < bits; shift += 8) {
+        k_sort_hist<K><<<(unsigned)tiles, kSortThreads, 0, st>>>(n, keys[cur], shift, tiles, hist);
+        k_sort_rowscan<<<kSortDigits, kSortThreads, 0, st>>>(hist, tiles, totals);
+        k_sort_scatter<K><<<(unsigned)tiles, kSortThreads, 0, st>>>(n, keys[cur], vals[cur], keys[cur ^ 1],
+                                                                    vals[cur ^ 1], shift, tiles, hist, totals);
+        launches += 3;
+        cur ^= 1;
+    }
+    return cur;
+}
+
+}  // namespace fsb
