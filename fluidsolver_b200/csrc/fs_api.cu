@@ -1999,6 +1999,15 @@ fs_status fs_autotune(fs_ctx* c, fs_tuning* out) {
     return fs_set_tuning(c, out);
 }
 
+fs_status fs_set_tile_wait_limit(fs_ctx* c, int32_t tries) {
+    if (!c) return fail(FS_ERR_INVALID, "ctx is null");
+    FS_CUDA(cudaSetDevice(c->device));
+    const int v = tries < 0 ? kTileWaitTries : tries;
+    FS_CUDA(cudaStreamSynchronize(c->stream));
+    FS_CUDA(cudaMemcpyToSymbol(g_tile_wait_tries, &v, sizeof(int)));
+    return FS_OK;
+}
+
 fs_status fs_set_tuning(fs_ctx* c, const fs_tuning* in) {
     if (!c || !in) return fail(FS_ERR_INVALID, "null argument");
     if (in->first_loop_prefetch < 1 || in->first_loop_prefetch > kMaxAhead || in->pressure_prefetch < 1 ||

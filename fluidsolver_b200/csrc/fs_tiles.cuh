@@ -116,18 +116,30 @@ __device__ __forceinline__ uint32_t mbar_try_wait0(TileStage& st) {
     return ok;
 }
 
+// Tries of the first wait for a tile's staging (each mbarrier.try_wait may
+// suspend the thread for a while). fs_set_tile_wait_limit lowers it so that
+// a test can make the wait run out and check the error path; it is
+// kTileWaitTries otherwise.
+constexpr int kTileWaitTries = 1 << 16;
+constexpr int kTileDrainTries = 1 << 20;
+static __device__ int g_tile_wait_tries = kTileWaitTries;
+
 // Waits for the staging to land, with a bounded number of tries. Returns
 // false, with FS_ERR_TIMEOUT raised, if the copies did not complete; the
-// caller then skips the tile (after a second bounded wait that gives copies
-// still in flight time to land before the block exits).
+// caller then skips the tile. Before that, a second, longer bounded wait
+// (kTileDrainTries, independent of the first's limit) lets copies still in
+// flight land, so that none writes into shared memory after the block has
+// left it.
 __device__ __forceinline__ bool stage_tile_wait(TileStage& st, int* __restrict__ status) {
     asm volatile("cp.async.wait_all;" ::: "memory");
     uint32_t ok = 0;
-    for (int it = 0; it < (1 << 16) && !ok; it++) ok = mbar_try_wait0(st);
+    const int tries = g_tile_wait_tries;
+    for (int it = 0; it < tries && !ok; it++) ok = mbar_try_wait0(st);
     const int late = __syncthreads_or(!ok);
     if (late) {
         if (threadIdx.x == 0) raise_status(status, FS_ERR_TIMEOUT);
-        for (int it = 0; it < (1 << 16) && !ok; it++) ok = mbar_try_wait0(st);
+        for (int it = 0; it < kTileDrainTries && !ok; it++) ok = mbar_try_wait0(st);
+        __syncthreads();
         return false;
     }
     return true;

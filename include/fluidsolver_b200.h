@@ -240,7 +240,10 @@ fs_status fs_query_position(fs_ctx* ctx, const float* position, int64_t* out, in
  *   - the fixed array is shared by every context on a device, so calls that
  *     overlap in time on one device (two host threads) race on it;
  *   - the first call on each device resolves the array's address, so make
- *     that first call before any stream capture begins. */
+ *     that first call before any stream capture begins;
+ *   - that address is kept for the rest of the process: after a
+ *     cudaDeviceReset of the device (which also ends every context on it)
+ *     this entry point must not be called on that device again. */
 #define FS_QUERY_NOALLOC_MAX 65536
 fs_status fs_query_position_noalloc(fs_ctx* ctx, const float* position, int64_t* out, int64_t cap,
                                     int64_t* count);
@@ -289,6 +292,15 @@ typedef struct fs_tuning {
 } fs_tuning;
 fs_status fs_autotune(fs_ctx* ctx, fs_tuning* out);
 fs_status fs_set_tuning(fs_ctx* ctx, const fs_tuning* in);
+
+/* Test hook for the bounded waits: how many times the tile passes try the
+ * wait for a tile's staged copies before they give up with FS_ERR_TIMEOUT
+ * (the step then returns it and leaves the state as the last finished phase
+ * left it). No reference counterpart: it exists so that the error path of a
+ * wait that runs out can be exercised on a GPU without faulting it. tries < 0
+ * restores the default (65,536); 0 makes every wait give up at once. The
+ * limit is one per device, shared by every context on the context's device. */
+fs_status fs_set_tile_wait_limit(fs_ctx* ctx, int32_t tries);
 
 /* ---- entities and sensors on the device -----------------------------------
  * Host-side entities and sensors of the Simulator read the whole collection;

@@ -52,6 +52,28 @@ def test_noalloc_query_equals_allocating_query(kind, dim):
     ns.close()
 
 
+@pytest.mark.parametrize("kind", ["hashed-3d", "quadratic-3d"])
+@pytest.mark.parametrize("precision,reference_order", [("fp32-kahan", False), ("fp32", True), ("fp64", False)])
+def test_noalloc_query_in_every_precision(kind, precision, reference_order):
+    """The same equality in the three precision modes (FP64 positions take the
+    double-precision walk) and with the reference-order layout."""
+    rng = np.random.default_rng(22)
+    n = 20000 if kind == "hashed-3d" else 4000
+    pos = (rng.random((n, 3)) * 15).astype(np.float32)
+    typ = rng.integers(0, 3, n).astype(np.uint8)
+    ns = NeighborhoodSearch(kind, 1.0, precision=precision, reference_order=reference_order)
+    ns.data.collection = ParticleCollection(position=pos, type=typ)
+    ns.find_neighbors()
+    total = 0
+    for q in (rng.random((6, 3)) * 15).astype(np.float32):
+        for call in range(2):
+            a, ca, b, cb = _both(ns, q)
+            assert ca == cb and a.tolist() == b.tolist(), (kind, precision, call)
+            total += cb
+    assert total > 0
+    ns.close()
+
+
 def test_noalloc_rejects_caps_beyond_the_fixed_array():
     ns = NeighborhoodSearch("compressed-3d", 1.0)
     ns.data.collection = ParticleCollection(position=np.zeros((4, 3), np.float32))
