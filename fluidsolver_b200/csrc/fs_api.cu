@@ -181,6 +181,8 @@ WalkParams walk_of(fs_ctx* c, bool for_solver) {
     w.grids = c->grids;
     w.scene = c->scene_of[c->cur];
     w.cells = c->cells;
+    w.table = c->hash_table;
+    w.table_mask = c->hash_mask;
     return w;
 }
 
@@ -248,7 +250,7 @@ fs_status free_all(fs_ctx* c) {
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc[0], c->acc[1], c->ext[0], c->ext[1],
                     c->rho[0], c->rho[1], c->p[0], c->p[1], c->type[0], c->type[1], c->hidx[0], c->hidx[1],
                     c->rho_prev, c->vstar, c->anp, c->err, c->gbnd, c->tile_desc, c->tile_ent, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
-                    c->perm[0], c->perm[1], c->h2d_cell, c->h2d_rank, c->sort_hist, c->cell_start, c->bbox, c->grids, c->nbr, c->nbr_count,
+                    c->perm[0], c->perm[1], c->h2d_cell, c->h2d_rank, c->sort_hist, c->hash_table, c->cell_start, c->bbox, c->grids, c->nbr, c->nbr_count,
                     c->scene_of[0], c->scene_of[1], c->d_scene_offsets,
                     c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->scalars,
                     c->stats_parts, c->stats_out};
@@ -608,6 +610,47 @@ template <typename R> fs_status download_impl(fs_ctx* c, fs_particles* out) {
 // ---------------------------------------------------------------------------
 // neighborhood search
 // ---------------------------------------------------------------------------
+// Compact hashing (2D): sort by the full (region, cell) key, gather, and
+// enter the occupied cells into the hashed table (fs_search.cuh); the walks
+// then look cells up by key, with no dense grid to clamp into.
+template <typename R> fs_status compact_search_impl(fs_ctx* c, State<R> s, bool solver_lists) {
+    const int64_t n = c->n;
+    cudaStream_t st = c->stream;
+    c->launches++;
+    k_compact_keys<R><<<grid_for(n), kBlock, 0, st>>>(n, s.pos, s.type, c->include_inactive, c->reference_order,
+                                                      c->search_radius, c->keys64[0], c->perm[0], c->status);
+    FS_CUDA(cudaGetLastError());
+    uint32_t* const vals[2] = {c->perm[0], c->perm[1]};
+    unsigned long long* const kk[2] = {c->keys64[0], c->keys64[1]};
+    const int res = sort_pairs(n, 64, kk, vals, c->sort_hist, st, c->launches);
+    FS_CUDA(cudaGetLastError());
+    const int nx = c->cur ^ 1;
+    c->launches++;
+    k_reorder<R><<<grid_for(n), kBlock, 0, st>>>(
+        n, c->perm[res], (const V4<R>*)c->pos[c->cur], (V4<R>*)c->pos[nx], (const V4<R>*)c->vel[c->cur],
+        (V4<R>*)c->vel[nx], (const V4<R>*)c->acc[c->cur], (V4<R>*)c->acc[nx], (const V4<R>*)c->ext[c->cur],
+        (V4<R>*)c->ext[nx], (const R*)c->rho[c->cur], (R*)c->rho[nx], (const R*)c->p[c->cur], (R*)c->p[nx],
+        c->type[c->cur], c->type[nx], c->hidx[c->cur], c->hidx[nx], c->scene_of[c->cur], c->scene_of[nx]);
+    FS_CUDA(cudaGetLastError());
+    c->cur = nx;
+    s = state_of<R>(c);
+    FS_CUDA(cudaMemsetAsync(c->hash_table, 0xff, sizeof(HashCell) * ((size_t)c->hash_mask + 1), st));
+    c->launches++;
+    k_hash_insert<<<grid_for(c->n_struct), kBlock, 0, st>>>(c->n_struct, c->keys64[res], c->hash_table, c->hash_mask);
+    FS_CUDA(cudaGetLastError());
+    if (solver_lists) {
+        WalkParams w = walk_of(c, true);
+        c->launches++;
+        k_build_lists<R><<<grid_for(c->n_owners), kBlock, 0, st>>>(
+            c->n_owners, s.pos, s.type, c->cell_start, w, 1u << FS_TYPE_NORMAL, false, c->nbr, c->nbr_stride,
+            c->nbr_capacity, c->nbr_count, c->status, c->scalars);
+        FS_CUDA(cudaGetLastError());
+        c->have_lists = true;
+    }
+    c->have_cells = true;
+    return FS_OK;
+}
+
 template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     const int64_t n = c->n;
     cudaStream_t st = c->stream;
@@ -618,6 +661,7 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
         return FS_OK;
     }
     State<R> s = state_of<R>(c);
+    if (c->hash_table) return compact_search_impl<R>(c, s, solver_lists);
     // bbox of the structure's cells -> grid origin
     FS_TRY(reset_bbox(c));
     c->launches++;
@@ -1352,7 +1396,13 @@ static fs_status create_ctx(const fs_params* p, int32_t scenes, const int64_t* o
         FS_ALLOC(c->hidx[b], cap);
         FS_ALLOC(c->keys[b], cap);
         FS_ALLOC(c->perm[b], cap);
-        if (c->reference_order) FS_ALLOC(c->keys64[b], cap);
+        if (c->reference_order || p->search == FS_SEARCH_COMPACT_2D) FS_ALLOC(c->keys64[b], cap);
+    }
+    if (p->search == FS_SEARCH_COMPACT_2D) {
+        uint32_t slots = 64;
+        while ((uint64_t)slots < 2 * (uint64_t)cap) slots <<= 1;
+        FS_ALLOC(c->hash_table, slots);
+        c->hash_mask = slots - 1;
     }
     if (c->truncate_cells) {
         FS_ALLOC(c->h2d_cell, cap);

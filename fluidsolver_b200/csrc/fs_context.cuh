@@ -84,6 +84,9 @@ struct fs_ctx {
     uint32_t* h2d_rank = nullptr;
     int64_t h2d_n = -1;               // particle count the history belongs to
     uint32_t* sort_hist = nullptr;    // per-tile digit counts of the radix sort (fs_sort.cuh)
+    // compact hashing (2D): the hashed table of occupied cells instead of the dense grid
+    fsb::HashCell* hash_table = nullptr;
+    uint32_t hash_mask = 0;           // slots - 1 (a power of two, >= 2 x capacity)
     uint32_t* cell_start = nullptr;   // [regions][cells + 1] first sorted index of cell >= c
     int64_t cells = 0;                // dims[0] * dims[1] * dims[2]
     int key_bits = 30;                // bits of the linear cell index in the sort keys

@@ -256,6 +256,104 @@ __global__ void k_reorder(int64_t n, const uint32_t* __restrict__ perm, const V4
 // ---------------------------------------------------------------------------
 // candidate walks
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// compact hashing: a hashed cell table for sparse domains
+// ---------------------------------------------------------------------------
+// CompactHashingNeighborhoodSearch (CompactHashingNeighborhoodSearch.cpp:99-107,
+// 342-349) finds a cell's particles through an open-addressing hash table of
+// the occupied cells, so memory follows the particles, not the domain's
+// extent. Here: particles are sorted by their full (region, cell) key -- no
+// dense grid, so no cell is ever clamped however far apart the particles
+// lie --, every run of equal keys (one occupied cell of one region) is entered
+// into a table of at least twice as many slots as particles, and a walk looks
+// each of its cells up by key. The slot of a cell is the spatial hash the
+// reference uses (Teschner et al., primes 73856093 and 19349663, here with
+// 83492791 for the region) over a power-of-two table, probed linearly.
+// Entries are only looked up by their full key, so which slot a cell takes
+// (which can depend on the order of concurrent insertions) never changes
+// a result.
+struct HashCell {
+    unsigned long long key;   // kHashEmpty: free slot
+    uint32_t start, end;      // the cell's run in the sorted order
+};
+constexpr unsigned long long kHashEmpty = ~0ull;
+constexpr int kHashCoordBits = 31;   // per cell coordinate, biased by 2^30
+
+__device__ __forceinline__ int clamp_cell_coord(int c) { return min(max(c, -(1 << 30)), (1 << 30) - 1); }
+// 2 region bits, then the biased x and y cell coordinates (31 bits each)
+__device__ __forceinline__ unsigned long long compact_cell_key(uint32_t region, int cx, int cy) {
+    const unsigned long long bx = (unsigned long long)(clamp_cell_coord(cx) + (1 << 30));
+    const unsigned long long by = (unsigned long long)(clamp_cell_coord(cy) + (1 << 30));
+    return ((unsigned long long)region << (2 * kHashCoordBits)) | (bx << kHashCoordBits) | by;
+}
+__device__ __forceinline__ uint32_t compact_hash(uint32_t region, int cx, int cy, uint32_t mask) {
+    return ((uint32_t)clamp_cell_coord(cx) * 73856093u ^ (uint32_t)clamp_cell_coord(cy) * 19349663u ^
+            region * 83492791u) & mask;
+}
+// the run of key in the table, or false; at most mask + 1 probes
+__device__ __forceinline__ bool hash_lookup(const HashCell* __restrict__ table, uint32_t mask, uint32_t slot,
+                                            unsigned long long key, uint32_t& start, uint32_t& end) {
+    for (uint32_t probe = 0; probe <= mask; probe++, slot = (slot + 1) & mask) {
+        const unsigned long long k = table[slot].key;
+        if (k == key) {
+            start = table[slot].start;
+            end = table[slot].end;
+            return true;
+        }
+        if (k == kHashEmpty) return false;
+    }
+    return false;
+}
+
+// Compact hashing's sort keys (2D): (region, cell x, cell y) of every
+// particle in the structure; excluded inactive particles sort last.
+template <typename R>
+__global__ void k_compact_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
+                               bool include_inactive, bool single_region, float r,
+                               unsigned long long* __restrict__ keys, uint32_t* __restrict__ perm,
+                               int* __restrict__ status) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint8_t t = type[k];
+    unsigned long long key = kHashEmpty;
+    if (include_inactive || t != FS_TYPE_INACTIVE) {
+        V4<R> p = pos[k];
+        if (!(isfinite(p.x) && isfinite(p.y))) {
+            raise_status(status, FS_ERR_NAN);
+            p.x = p.y = R(0);
+        }
+        key = compact_cell_key(region_of(t, single_region), cell_coord<R>(p.x, r, false),
+                               cell_coord<R>(p.y, r, false));
+    }
+    keys[k] = key;
+    perm[k] = (uint32_t)k;
+}
+
+// Enters every run of equal sorted keys (one occupied cell of one region)
+// into the cleared table: the run's first particle probes from the cell's
+// hash for a free slot (at most mask + 1 probes; the table has at least
+// twice as many slots as particles, so one is always free).
+__global__ void k_hash_insert(int64_t n_struct, const unsigned long long* __restrict__ keys,
+                              HashCell* __restrict__ table, uint32_t mask) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n_struct) return;
+    const unsigned long long key = keys[k];
+    if (k > 0 && keys[k - 1] == key) return;
+    int64_t e = k + 1;
+    while (e < n_struct && keys[e] == key) e++;
+    const uint32_t region = (uint32_t)(key >> (2 * kHashCoordBits));
+    const int cx = (int)((key >> kHashCoordBits) & ((1ull << kHashCoordBits) - 1)) - (1 << 30);
+    const int cy = (int)(key & ((1ull << kHashCoordBits) - 1)) - (1 << 30);
+    uint32_t slot = compact_hash(region, cx, cy, mask);
+    for (uint32_t probe = 0; probe <= mask; probe++, slot = (slot + 1) & mask) {
+        if (atomicCAS(&table[slot].key, kHashEmpty, key) == kHashEmpty) {
+            table[slot].start = (uint32_t)k;
+            table[slot].end = (uint32_t)e;
+            return;
+        }
+    }
+}
+
 struct WalkParams {
     float r;        // search radius
     float r2;       // r * r
@@ -267,6 +365,8 @@ struct WalkParams {
     const SceneGrid* __restrict__ grids;  // per scene
     const uint16_t* __restrict__ scene;   // per particle (null: one scene)
     int64_t cells;  // cells of all scenes; each region's table has cells + 1 entries
+    const HashCell* table = nullptr;      // compact hashing (2D): cells by key instead of the dense grid
+    uint32_t table_mask = 0;
     __device__ __forceinline__ SceneGrid grid_of(int64_t k) const { return grids[scene ? scene[k] : 0]; }
 };
 
@@ -290,6 +390,25 @@ __device__ __forceinline__ void walk_cells(V3<R> xi, const V4<R>* __restrict__ p
                                            const uint32_t* __restrict__ cell_start, const SceneGrid& gr,
                                            const WalkParams& w, F&& f) {
     const int ci[3] = {cell_coord<R>(xi.x, w.r, w.trunc), cell_coord<R>(xi.y, w.r, w.trunc), cell_coord<R>(xi.z, w.r, w.trunc)};
+    if (w.table) {
+        // compact hashing (2D): the 3 x 3 cells looked up by key
+        for (int dx = -1; dx <= 1; dx++) {
+            for (int dy = -1; dy <= 1; dy++) {
+                for (int g = 0; g < w.regions; g++) {
+                    uint32_t b, e;
+                    if (!hash_lookup(w.table, w.table_mask, compact_hash(g, ci[0] + dx, ci[1] + dy, w.table_mask),
+                                     compact_cell_key(g, ci[0] + dx, ci[1] + dy), b, e))
+                        continue;
+                    for (uint32_t j = b; j < e; j++) {
+                        const uint8_t tj = type[j];
+                        if (!w.candidates_inactive && tj == FS_TYPE_INACTIVE) continue;
+                        if (within<R>(xi - xyz<R>(pos[j]), w)) f(j, tj);
+                    }
+                }
+            }
+        }
+        return;
+    }
     const int zr = w.dim == 2 ? 0 : 1;
     const int o0 = gr.o0, o1 = gr.o1, o2 = gr.o2;
     for (int dx = -1; dx <= 1; dx++) {

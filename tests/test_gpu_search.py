@@ -120,6 +120,33 @@ def test_far_apart_clusters_exceed_the_cell_grid(c_oracle):
     assert same_sets(off, idx, ro, ri)
 
 
+def test_compact_hashing_on_a_sparse_domain(c_oracle):
+    """Compact hashing's hashed cell table (CompactHashingNeighborhoodSearch.cpp:342-349):
+    four clusters millions of radii apart, with boundary and inactive
+    particles. A dense grid over that extent would clamp nearly every
+    particle into a border cell; the table holds only the occupied cells, and
+    the sets equal the oracle's (active owners and candidates, <= 40)."""
+    rng = np.random.default_rng(10)
+    a = (rng.random((4000, 2)) * 30).astype(np.float32)
+    pos = np.concatenate([a, a + np.float32(3.0e6), a - np.float32(5.0e5),
+                          a + np.array([1.0e6, -2.0e6], np.float32)]).astype(np.float32)
+    typ = rng.choice(np.array([0, 0, 0, 1, 2], np.uint8), len(pos))
+    off, idx = run_search("compact-hashing-2d", pos, 1.0, typ)
+    ro, ri, ok = c_oracle.search("compact-hashing-2d", pos, 1.0, typ)
+    assert ok
+    assert np.array_equal(off, ro)
+    assert np.array_equal(idx, sorted_csr(ro, ri)[1])
+    assert off[-1] > 5 * len(pos)
+
+
+def test_compact_hashing_capacity_is_reported():
+    # more than 40 neighbors: the reference throws (CompactHashingNeighborhoodSearch.cpp:5, 210-247)
+    pos = (np.random.default_rng(11).random((200, 2)) * 2).astype(np.float32)
+    with pytest.raises(FluidSolverError) as e:
+        run_search("compact-hashing-2d", pos, 1.0)
+    assert e.value.status == FS_ERR_CAPACITY
+
+
 @pytest.mark.parametrize("kind", ["hashed-3d", "compressed-3d"])
 def test_uniform_1m_points_match_oracle(c_oracle, kind):
     # the 3D search microbenchmark's uniform case at full size: 1,000,000 points
