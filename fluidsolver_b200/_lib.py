@@ -117,9 +117,15 @@ class FsGlobalStats(ctypes.Structure):
 
 class FsTuning(ctypes.Structure):
     _fields_ = [
-        ("tuned", c_int32), ("first_loop_prefetch", c_int32), ("pressure_prefetch", c_int32), ("reserved", c_int32),
-        ("first_loop_ms", c_float * 4), ("pressure_iteration_ms", c_float * 4),
+        ("tuned", c_int32), ("first_loop_prefetch", c_int32), ("pressure_prefetch", c_int32), ("tile_cap", c_int32),
+        ("block_size", c_int32), ("reserved", c_int32),
+        ("first_loop_ms", c_float * 4), ("pressure_iteration_ms", c_float * 4), ("step_ms_by_tile_cap", c_float * 4),
+        ("step_ms_by_block_size", c_float * 3), ("fallback_tiles_by_tile_cap", c_float * 4),
     ]
+
+
+TILE_CAPS = (1024, 1536, 2048, 3072)   # include/fluidsolver_b200.h, fs_tuning
+BLOCK_SIZES = (128, 256, 512)
 
 
 class FsCamera(ctypes.Structure):

@@ -166,6 +166,7 @@ TileLists tile_lists_of(fs_ctx* c) {
     T.count = c->nbr_count;
     T.stride = c->tile_stride;
     T.K = c->nbr_capacity;
+    T.cap = c->tuning.cap;
     return T;
 }
 
@@ -280,6 +281,8 @@ fs_status ensure_lists(fs_ctx* c, int K) {
     const int64_t stride = ((c->cap + 31) / 32) * 32;
     const bool tiled = tiled_mode(c);
     if (tiled) K = (K + 7) & ~7;   // tile lists hold octets of entries
+    if (tiled && tile_build_smem(K, kTileCapMax) > (size_t)227 * 1024)
+        return fail(FS_ERR_CAPACITY, "more neighbors per particle than the fast mode's list builder holds (704)");
     if (c->nbr && c->nbr_capacity >= K && c->nbr_stride == stride && (!tiled || c->tile_ent)) return FS_OK;
     clear_graphs(c);
     if (c->nbr) cudaFree(c->nbr);
@@ -295,7 +298,7 @@ fs_status ensure_lists(fs_ctx* c, int K) {
         FS_TRY(dalloc(&c->tile_desc, (size_t)tiles));
         FS_TRY(dalloc(&c->tile_ent, (size_t)(K / 8) * c->tile_stride));
         FS_CUDA(cudaFuncSetAttribute(k_build_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)tile_build_smem(K)));
+                                     (int)tile_build_smem(K, kTileCapMax)));
         FS_CUDA(set_tile_pass_smem(K));
     }
     c->nbr_capacity = K;
@@ -672,8 +675,9 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     k_origin<<<grid_for(c->nsc(), 128), 128, 0, st>>>(c->bbox, c->grids, c->nsc());
     // keys + sort
     unsigned long long* k64 = single ? c->keys64[0] : nullptr;
+    const int pb = c->tuning.block;   // the per-particle kernels' block size (fs_autotune)
     c->launches++;
-    k_keys<R><<<grid_for(n), kBlock, 0, st>>>(n, s.pos, s.type, s.hidx, c->include_inactive, single, c->search_radius,
+    k_keys<R><<<grid_for(n, pb), pb, 0, st>>>(n, s.pos, s.type, s.hidx, c->include_inactive, single, c->search_radius,
                                               c->truncate_cells, c->grids, s.scene, c->key_bits, c->keys[0], k64,
                                               c->perm[0], c->h2d_cell, c->h2d_rank, c->status);
     FS_CUDA(cudaGetLastError());
@@ -691,7 +695,7 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     // gather every persistent field into the other buffer
     const int nx = c->cur ^ 1;
     c->launches++;
-    k_reorder<R><<<grid_for(n), kBlock, 0, st>>>(
+    k_reorder<R><<<grid_for(n, pb), pb, 0, st>>>(
         n, c->perm[res], (const V4<R>*)c->pos[c->cur], (V4<R>*)c->pos[nx], (const V4<R>*)c->vel[c->cur],
         (V4<R>*)c->vel[nx], (const V4<R>*)c->acc[c->cur], (V4<R>*)c->acc[nx], (const V4<R>*)c->ext[c->cur],
         (V4<R>*)c->ext[nx], (const R*)c->rho[c->cur], (R*)c->rho[nx], (const R*)c->p[c->cur], (R*)c->p[nx],
@@ -704,10 +708,10 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     const int64_t table = (int64_t)c->regions * (c->cells + 1);
     c->launches++;
     if (single)
-        k_cell_start_fill<unsigned long long><<<grid_for(c->n_struct + 1), kBlock, 0, st>>>(
+        k_cell_start_fill<unsigned long long><<<grid_for(c->n_struct + 1, pb), pb, 0, st>>>(
             c->n_struct, c->keys64[res], 32, c->key_bits, c->cells, table, c->cell_start);
     else
-        k_cell_start_fill<uint32_t><<<grid_for(c->n_struct + 1), kBlock, 0, st>>>(
+        k_cell_start_fill<uint32_t><<<grid_for(c->n_struct + 1, pb), pb, 0, st>>>(
             c->n_struct, c->keys[res], 0, c->key_bits, c->cells, table, c->cell_start);
     FS_CUDA(cudaGetLastError());
     if (c->h2d_cell) {
@@ -725,9 +729,9 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
             if (tiled_mode(c) && c->n_owners > 0) {
                 const int64_t tiles = (c->n_owners + kTileOwners - 1) / kTileOwners;
                 c->launches++;
-                k_build_tiles<<<(unsigned)tiles, kTileOwners, tile_build_smem(c->nbr_capacity), st>>>(
-                    c->n_owners, s.pos, s.type, c->cell_start, w, c->tile_desc, c->tile_ent,
-                    c->tile_stride, c->nbr, c->nbr_stride, c->nbr_capacity, c->nbr_count, c->status, c->scalars);
+                k_build_tiles<<<(unsigned)tiles, kTileOwners, tile_build_smem(c->nbr_capacity, c->tuning.cap), st>>>(
+                    c->n_owners, s.pos, s.type, c->cell_start, w, c->tile_desc, c->tile_ent, c->tile_stride, c->nbr,
+                    c->nbr_stride, c->nbr_capacity, c->tuning.cap, c->nbr_count, c->status, c->scalars);
                 built = true;
             }
         }
@@ -920,12 +924,12 @@ fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
     FS_TRY(mark(c, 1, st));
     c->launches++;
     FSB_AHEAD_SWITCH(c->tuning.l1_ahead, k_tile_iisph3d_l1,
-                     <<<tiles + rest, kPassThreads, tile_pass_smem(36, T.K, !kL1GlobalEntries), st>>>(
+                     <<<tiles + rest, kPassThreads, tile_pass_smem(36, T.K, !kL1GlobalEntries, T.cap), st>>>(
                          nf, n, tiles, s, T, L, k, c->scalars, c->status))
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 2, st));
     c->launches++;
-    k_tile_iisph3d_l2<<<tiles, kPassThreads, tile_pass_smem(32, T.K, !kL2GlobalEntries), st>>>(
+    k_tile_iisph3d_l2<<<tiles, kPassThreads, tile_pass_smem(32, T.K, !kL2GlobalEntries, T.cap), st>>>(
         nf, s, T, L, k, c->scalars, c->status);
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 3, st));
@@ -934,10 +938,10 @@ fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
         c->launches += 2;
         const bool slab = !kPressureGlobalEntries;
         FSB_AHEAD_SWITCH(c->tuning.pressure_ahead, k_tile_iisph3d_pressure_acc,
-                         <<<tiles, kPassThreads, tile_pass_smem(20, T.K, slab), bs>>>(nf, s, T, L, k, c->scalars,
+                         <<<tiles, kPassThreads, tile_pass_smem(20, T.K, slab, T.cap), bs>>>(nf, s, T, L, k, c->scalars,
                                                                                        c->status))
         FSB_AHEAD_SWITCH(c->tuning.pressure_ahead, k_tile_iisph3d_pressure_update,
-                         <<<tiles, kPassThreads, tile_pass_smem(32, T.K, slab), bs>>>(nf, s, T, L, k, c->scalars,
+                         <<<tiles, kPassThreads, tile_pass_smem(32, T.K, slab, T.cap), bs>>>(nf, s, T, L, k, c->scalars,
                                                                                        c->status))
     }, true));
     FS_TRY(mark(c, 4, st));
@@ -945,7 +949,7 @@ fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
     k_cfl<<<1, 128, 0, st>>>(c->scalars, c->nsc(), c->prm.particle_size, cfl_default(c), c->prm.lambda_v,
                              c->prm.lambda_a, c->status);
     c->launches++;
-    k_iisph3d_integrate<float><<<grid_for(n), kBlock, 0, st>>>(n, s, c->scalars, c->status);
+    k_iisph3d_integrate<float><<<grid_for(n, c->tuning.block), c->tuning.block, 0, st>>>(n, s, c->scalars, c->status);
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 5, st));
     return FS_OK;
@@ -1014,12 +1018,12 @@ fs_status step_sesph3d_tiled(fs_ctx* c) {
     FS_TRY(mark(c, 1, st));
     c->launches++;
     FSB_AHEAD_SWITCH(c->tuning.l1_ahead, k_tile_sesph3d_density,
-                     <<<tiles, kPassThreads, tile_pass_smem(16, T.K, false), st>>>(nf, s, T, L, k, c->status))
+                     <<<tiles, kPassThreads, tile_pass_smem(16, T.K, false, T.cap), st>>>(nf, s, T, L, k, c->status))
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 2, st));
     c->launches++;
     FSB_AHEAD_SWITCH(c->tuning.l1_ahead, k_tile_sesph3d_accel,
-                     <<<tiles, kPassThreads, tile_pass_smem(36, T.K, false), st>>>(nf, s, T, L, k, c->status))
+                     <<<tiles, kPassThreads, tile_pass_smem(36, T.K, false, T.cap), st>>>(nf, s, T, L, k, c->status))
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 3, st));
     c->launches++;
@@ -1970,14 +1974,55 @@ fs_status fs_run(fs_ctx* c, int32_t steps, float desired_dt, fs_step_stats* stat
     return FS_OK;
 }
 
-// The tile passes' prefetch depths, chosen by timing whole steps on a copy of
+// mean whole-step time of `steps` steps after `warm` (graphs re-captured);
+// the step is the sum of the five phase times the events measure
+static fs_status time_steps(fs_ctx* t, int warm, int steps, double& step_ms, double& l1_ms, double& iter_ms,
+                            int& iter_samples) {
+    fs_step_stats st{};
+    clear_graphs(t);
+    for (int i = 0; i < warm; i++) FS_TRY(one_step(t, 0.0f, &st));
+    step_ms = l1_ms = iter_ms = 0.0;
+    iter_samples = 0;
+    for (int i = 0; i < steps; i++) {
+        FS_TRY(one_step(t, 0.0f, &st));
+        double sum = 0.0;
+        for (int q = 0; q < 5; q++) sum += t->phase_ms[q];
+        step_ms += sum / steps;
+        l1_ms += t->phase_ms[1] / steps;
+        if (st.iterations > 1) {
+            iter_ms += t->phase_ms[3] / (st.iterations - 1);
+            iter_samples++;
+        }
+    }
+    if (iter_samples) iter_ms /= iter_samples;
+    return FS_OK;
+}
+
+// fraction of the tiles of the last search that fell back to 32-bit lists
+static fs_status fallback_fraction(fs_ctx* t, float& frac) {
+    const int64_t tiles = (t->n_owners + kTileOwners - 1) / kTileOwners;
+    frac = 0.f;
+    if (tiles == 0) return FS_OK;
+    std::vector<TileDesc> d((size_t)tiles);
+    FS_CUDA(cudaMemcpy(d.data(), t->tile_desc, sizeof(TileDesc) * tiles, cudaMemcpyDeviceToHost));
+    int64_t fb = 0;
+    for (const TileDesc& x : d) fb += x.h.nranges == kTileFallback ? 1 : 0;
+    frac = (float)fb / (float)tiles;
+    return FS_OK;
+}
+
+// The fast mode's launch shapes, chosen by timing whole steps on a copy of
 // the context: the same parameters and the same particles (downloaded from
-// the context, uploaded into the copy), so the caller's state and step count
-// stay as they were. Each trial runs 2 steps to capture its graph and settle,
-// then 4 timed steps; the first loop is timed as its phase, the pressure
-// passes per loop iteration (the first iteration runs inside the second loop).
-// Trials (pressure depth, first-loop depth): (1,1), (2,2), (3,1), (4,2); each
-// depth is rated by the mean over the trials that used it.
+// the context, uploaded into the copy before every trial), so the caller's
+// state and step count stay as they were. A coordinate search, one axis
+// after the other, each trial 2 steps to capture its graph and settle, then
+// 4 timed steps:
+//   1. prefetch depths, trials (pressure, first loop) (1,1), (2,2), (3,1),
+//      (4,2); the first loop is rated by its phase time, the pressure passes
+//      per loop iteration (the first iteration runs inside the second loop),
+//      each depth by the mean over the trials that used it;
+//   2. the staging cap per tile, 1024 / 1536 / 2048 / 3072, by whole steps;
+//   3. the per-particle kernels' block size, 128 / 256 / 512, by whole steps.
 fs_status fs_autotune(fs_ctx* c, fs_tuning* out) {
     if (!c || !out) return fail(FS_ERR_INVALID, "null argument");
     if (!c->have_state) return fail(FS_ERR_STATE, "no particles uploaded");
@@ -1986,6 +2031,8 @@ fs_status fs_autotune(fs_ctx* c, fs_tuning* out) {
     *out = fs_tuning{};
     out->first_loop_prefetch = c->tuning.l1_ahead;
     out->pressure_prefetch = c->tuning.pressure_ahead;
+    out->tile_cap = c->tuning.cap;
+    out->block_size = c->tuning.block;
     // nothing tunable unless the IISPH passes are tiled
     if (!tiled_mode(c) || c->prm.solver != FS_SOLVER_IISPH_3D || c->n_fluid == 0) return FS_OK;
     FS_CUDA(cudaSetDevice(c->device));
@@ -2011,24 +2058,23 @@ fs_status fs_autotune(fs_ctx* c, fs_tuning* out) {
         fs_ctx* t;
         ~Guard() { fs_destroy(t); }
     } guard{t};
-    FS_TRY(fs_upload(t, &v));
+    t->tuning = c->tuning;
+    double step_ms, l1_ms, iter_ms;
+    int samples;
+    // 1. prefetch depths
     const int trials[4][2] = {{1, 1}, {2, 2}, {3, 1}, {kMaxAhead, 2}};
     double l1_sum[kMaxAhead + 1] = {}, pi_sum[kMaxAhead + 1] = {};
     int l1_cnt[kMaxAhead + 1] = {}, pi_cnt[kMaxAhead + 1] = {};
-    fs_step_stats st{};
     for (const auto& tr : trials) {
+        FS_TRY(fs_upload(t, &v));
         t->tuning.pressure_ahead = tr[0];
         t->tuning.l1_ahead = tr[1];
-        clear_graphs(t);
-        for (int i = 0; i < 2; i++) FS_TRY(one_step(t, 0.0f, &st));
-        for (int i = 0; i < 4; i++) {
-            FS_TRY(one_step(t, 0.0f, &st));
-            l1_sum[tr[1]] += t->phase_ms[1];
-            l1_cnt[tr[1]]++;
-            if (st.iterations > 1) {
-                pi_sum[tr[0]] += t->phase_ms[3] / (st.iterations - 1);
-                pi_cnt[tr[0]]++;
-            }
+        FS_TRY(time_steps(t, 2, 4, step_ms, l1_ms, iter_ms, samples));
+        l1_sum[tr[1]] += l1_ms;
+        l1_cnt[tr[1]]++;
+        if (samples) {
+            pi_sum[tr[0]] += iter_ms;
+            pi_cnt[tr[0]]++;
         }
     }
     int best_l1 = c->tuning.l1_ahead, best_pi = c->tuning.pressure_ahead;
@@ -2043,9 +2089,37 @@ fs_status fs_autotune(fs_ctx* c, fs_tuning* out) {
             if (pi_sum[a] / pi_cnt[a] < t_pi) t_pi = pi_sum[a] / pi_cnt[a], best_pi = a;
         }
     }
+    t->tuning.l1_ahead = best_l1;
+    t->tuning.pressure_ahead = best_pi;
+    // 2. staging cap
+    const int caps[4] = {1024, 1536, 2048, 3072};
+    double best = 1e30;
+    int best_cap = t->tuning.cap;
+    for (int q = 0; q < 4; q++) {
+        FS_TRY(fs_upload(t, &v));
+        t->tuning.cap = caps[q];
+        FS_TRY(time_steps(t, 2, 4, step_ms, l1_ms, iter_ms, samples));
+        out->step_ms_by_tile_cap[q] = (float)step_ms;
+        FS_TRY(fallback_fraction(t, out->fallback_tiles_by_tile_cap[q]));
+        if (step_ms < best) best = step_ms, best_cap = caps[q];
+    }
+    t->tuning.cap = best_cap;
+    // 3. block size of the per-particle kernels
+    const int blocks[3] = {128, 256, 512};
+    best = 1e30;
+    int best_block = t->tuning.block;
+    for (int q = 0; q < 3; q++) {
+        FS_TRY(fs_upload(t, &v));
+        t->tuning.block = blocks[q];
+        FS_TRY(time_steps(t, 2, 4, step_ms, l1_ms, iter_ms, samples));
+        out->step_ms_by_block_size[q] = (float)step_ms;
+        if (step_ms < best) best = step_ms, best_block = blocks[q];
+    }
     out->tuned = 1;
     out->first_loop_prefetch = best_l1;
     out->pressure_prefetch = best_pi;
+    out->tile_cap = best_cap;
+    out->block_size = best_block;
     return fs_set_tuning(c, out);
 }
 
@@ -2063,12 +2137,22 @@ fs_status fs_set_tuning(fs_ctx* c, const fs_tuning* in) {
     if (in->first_loop_prefetch < 1 || in->first_loop_prefetch > kMaxAhead || in->pressure_prefetch < 1 ||
         in->pressure_prefetch > kMaxAhead)
         return fail(FS_ERR_INVALID, "prefetch depths must be in 1.." + std::to_string(kMaxAhead));
-    if (c->tuning.l1_ahead != in->first_loop_prefetch || c->tuning.pressure_ahead != in->pressure_prefetch) {
+    if (in->tile_cap != 0 && (in->tile_cap < 256 || in->tile_cap > kTileCapMax || in->tile_cap % 4 != 0))
+        return fail(FS_ERR_INVALID, "tile_cap must be 0 or a multiple of 4 in 256.." + std::to_string(kTileCapMax));
+    if (in->block_size != 0 && (in->block_size < 32 || in->block_size > 1024 || in->block_size % 32 != 0))
+        return fail(FS_ERR_INVALID, "block_size must be 0 or a multiple of 32 in 32..1024");
+    TileTuning next = c->tuning;
+    next.l1_ahead = in->first_loop_prefetch;
+    next.pressure_ahead = in->pressure_prefetch;
+    if (in->tile_cap) next.cap = in->tile_cap;
+    if (in->block_size) next.block = in->block_size;
+    if (next.l1_ahead != c->tuning.l1_ahead || next.pressure_ahead != c->tuning.pressure_ahead ||
+        next.cap != c->tuning.cap || next.block != c->tuning.block) {
         FS_CUDA(cudaSetDevice(c->device));
         if (c->stream) FS_CUDA(cudaStreamSynchronize(c->stream));
-        clear_graphs(c);   // the captured steps launch the old instantiations
-        c->tuning.l1_ahead = in->first_loop_prefetch;
-        c->tuning.pressure_ahead = in->pressure_prefetch;
+        clear_graphs(c);   // the captured steps launch the old instantiations and shapes
+        c->tuning = next;
+        c->have_lists = false;   // tile lists are built for one cap: search again before solving
     }
     return FS_OK;
 }

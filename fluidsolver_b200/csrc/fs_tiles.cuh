@@ -16,7 +16,7 @@
 // memory of a tile feeds.
 //
 // A tile whose owners touch the grid's border cells, form more than
-// kTileGroups groups, or need more than kTileCap staged candidates is a
+// kTileGroups groups, or need more than the staging cap (TileLists::cap) of candidates is a
 // fallback tile: its owners get the ordinary 32-bit slot-major lists, which
 // the two threads of an owner split in the passes, with the pair arithmetic
 // of the tiled owners and the neighbors' data read from global memory.
@@ -36,7 +36,8 @@ constexpr int kTileOwners = 128;
 constexpr int kPassThreads = 2 * kTileOwners;  // two threads per owner in the passes
 constexpr int kTileGroups = 4;
 constexpr int kTileRanges = 2 * 9 * kTileGroups;
-constexpr int kTileCap = 1536;                 // staged candidates
+constexpr int kTileCap = 1536;                 // staged candidates per tile (default; fs_autotune may change it)
+constexpr int kTileCapMax = 3072;              // the largest cap (entries address up to 4,096 staged candidates)
 constexpr uint32_t kTileFallback = 0xffffffffu;
 // entry: byte offset of the candidate's float4 in a staged array (index << 4),
 // bit 0 set for boundary neighbors
@@ -77,15 +78,16 @@ struct TileLists {
     const uint32_t* __restrict__ count;  // per owner: entries | (fluid entries << 16); fluid entries come first
     int64_t stride;
     int K;
+    int cap;                           // staged candidates per tile the lists were built for
 };
 
 // dynamic shared memory of the list builder and of the passes. A pass
 // stages its candidates (bytes per candidate: 36 for the first loop --
 // position, velocity, density --, 32 for position and a float4 field, 20 for
 // position and a float field), then the tile's entries and list lengths.
-inline size_t tile_build_smem(int K) { return (size_t)kTileCap * 16 + (size_t)kTileOwners * (K + 8) * 2; }
-inline size_t tile_pass_smem(int bytes_per_candidate, int K, bool slab = true) {
-    return (size_t)kTileCap * bytes_per_candidate + (slab ? (size_t)(K / 8) * kTileOwners * 16 + kTileOwners * 4 : 0);
+inline size_t tile_build_smem(int K, int cap) { return (size_t)cap * 16 + (size_t)kTileOwners * (K + 8) * 2; }
+inline size_t tile_pass_smem(int bytes_per_candidate, int K, bool slab, int cap) {
+    return (size_t)cap * bytes_per_candidate + (slab ? (size_t)(K / 8) * kTileOwners * 16 + kTileOwners * 4 : 0);
 }
 // Whether a pass reads its entries straight from the global octet planes
 // (one octet ahead of use) instead of staging them in shared memory. Without
@@ -151,11 +153,11 @@ __device__ __forceinline__ bool stage_tile_wait(TileStage& st, int* __restrict__
 __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     int64_t n_owners, const float4* __restrict__ pos, const uint8_t* __restrict__ type,
     const uint32_t* __restrict__ cell_start, WalkParams w, TileDesc* __restrict__ desc,
-    uint4* __restrict__ ent, int64_t ent_stride, uint32_t* __restrict__ nbr, int64_t stride, int K,
+    uint4* __restrict__ ent, int64_t ent_stride, uint32_t* __restrict__ nbr, int64_t stride, int K, int cap,
     uint32_t* __restrict__ count, int* __restrict__ status, StepScalars* __restrict__ sc) {
     extern __shared__ float4 tile_smem[];
-    float4* sp = tile_smem;                                              // staged positions
-    uint16_t* sent = reinterpret_cast<uint16_t*>(tile_smem + kTileCap);  // [owner][K + 8] entries
+    float4* sp = tile_smem;                                          // staged positions
+    uint16_t* sent = reinterpret_cast<uint16_t*>(tile_smem + cap);   // [owner][K + 8] entries
     const int KP = K + 8;
     __shared__ long long s_key[kTileOwners];
     __shared__ uint32_t s_cnt[kTileOwners];
@@ -258,7 +260,7 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
         }
         // (every thread has read the warp sums before s_cnt is reused)
         if (t < NR) s_base[t] = (before + incl - len) | ((before_ne + ne - (len ? 1u : 0u)) << 16);
-        fallback = tot > (uint32_t)kTileCap;
+        fallback = tot > (uint32_t)cap;
         if (t == 0) s_total = tot;
         __syncthreads();
     }
@@ -570,11 +572,13 @@ constexpr int kL2Ahead = 1;
 struct TileTuning {
     int l1_ahead = 1;
     int pressure_ahead = 3;
+    int cap = kTileCap;   // staged candidates per tile
+    int block = 128;      // threads per block of the step's per-particle kernels (keys, reorder, integration)
 };
 
 // the slab after a pass's staged candidates (bytes_per_candidate each)
-__device__ __forceinline__ TileSlab slab_at(float4* smem, int bytes_per_candidate, int K) {
-    char* b = reinterpret_cast<char*>(smem) + kTileCap * bytes_per_candidate;
+__device__ __forceinline__ TileSlab slab_at(float4* smem, int bytes_per_candidate, int K, int cap) {
+    char* b = reinterpret_cast<char*>(smem) + cap * bytes_per_candidate;
     return TileSlab{reinterpret_cast<uint4*>(b), reinterpret_cast<uint32_t*>(b + (K / 8) * kTileOwners * 16)};
 }
 
@@ -700,12 +704,12 @@ __global__ void __launch_bounds__(kPassThreads, kL1GlobalEntries ? 4 : 3) k_tile
             }, flush);
     } else {
         float4* sp = tile_smem;
-        float4* sv = tile_smem + kTileCap;
-        float* sr = reinterpret_cast<float*>(tile_smem + 2 * kTileCap);
+        float4* sv = tile_smem + T.cap;
+        float* sr = reinterpret_cast<float*>(tile_smem + 2 * T.cap);
         __shared__ TileStage stg;
         const float4* src4[2] = {s.pos, s.vel};
         float4* dst4[2] = {sp, sv};
-        const TileSlab slab = slab_at(tile_smem, 36, T.K);
+        const TileSlab slab = slab_at(tile_smem, 36, T.K, T.cap);
         stage_tile_async<2, false, !kL1GlobalEntries>(stg, d, h, rg, src4, dst4, s.rho_prev, sr, T, slab);
         const uint32_t cnt = kL1GlobalEntries ? T.count[kk] : 0u;
         uint2 ahead[AHEAD];
@@ -783,11 +787,11 @@ __global__ void __launch_bounds__(kPassThreads, kL2GlobalEntries ? 4 : 3) k_tile
                                       flush);
     } else {
         float4* sp = tile_smem;
-        float4* sa = tile_smem + kTileCap;
+        float4* sa = tile_smem + T.cap;
         __shared__ TileStage stg;
         const float4* src4[2] = {s.pos, s.vstar};
         float4* dst4[2] = {sp, sa};
-        const TileSlab slab = slab_at(tile_smem, 32, T.K);
+        const TileSlab slab = slab_at(tile_smem, 32, T.K, T.cap);
         stage_tile_async<2, false, !kL2GlobalEntries>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
         const uint32_t cnt = kL2GlobalEntries ? T.count[kk] : 0u;
         if (!stage_tile_wait(stg, status)) return;
@@ -856,11 +860,11 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
             walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.p[j]); }, flush);
     } else {
         float4* sp = tile_smem;
-        float* sa = reinterpret_cast<float*>(tile_smem + kTileCap);
+        float* sa = reinterpret_cast<float*>(tile_smem + T.cap);
         __shared__ TileStage stg;
         const float4* src4[1] = {s.pos};
         float4* dst4[1] = {sp};
-        const TileSlab slab = slab_at(tile_smem, 20, T.K);
+        const TileSlab slab = slab_at(tile_smem, 20, T.K, T.cap);
         stage_tile_async<1, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, s.p, sa, T, slab);
         const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
         uint2 ahead[AHEAD];
@@ -921,11 +925,11 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
         if (valid) walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.acc[j]); }, flush);
     } else {
         float4* sp = tile_smem;
-        float4* sa = tile_smem + kTileCap;
+        float4* sa = tile_smem + T.cap;
         __shared__ TileStage stg;
         const float4* src4[2] = {s.pos, s.acc};
         float4* dst4[2] = {sp, sa};
-        const TileSlab slab = slab_at(tile_smem, 32, T.K);
+        const TileSlab slab = slab_at(tile_smem, 32, T.K, T.cap);
         stage_tile_async<2, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
         const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
         uint2 ahead[AHEAD];
@@ -1076,8 +1080,8 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_tile_sesph3d_accel(int64_t 
         flush();
     } else {
         float4* sp = tile_smem;
-        float4* sv = tile_smem + kTileCap;
-        float* sr = reinterpret_cast<float*>(tile_smem + 2 * kTileCap);
+        float4* sv = tile_smem + T.cap;
+        float* sr = reinterpret_cast<float*>(tile_smem + 2 * T.cap);
         __shared__ TileStage stg;
         const float4* src4[2] = {s.pos, s.vel};
         float4* dst4[2] = {sp, sv};
@@ -1145,25 +1149,25 @@ __global__ void k_export_solver_lists(int64_t n_owners, bool tiled, TileLists T,
 
 template <int AHEAD> inline cudaError_t set_tuned_pass_smem(int K) {
     cudaError_t e = cudaFuncSetAttribute(k_tile_iisph3d_l1<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)tile_pass_smem(36, K, !kL1GlobalEntries));
+                                         (int)tile_pass_smem(36, K, !kL1GlobalEntries, kTileCapMax));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_acc<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tile_pass_smem(20, K, !kPressureGlobalEntries));
+                                 (int)tile_pass_smem(20, K, !kPressureGlobalEntries, kTileCapMax));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_update<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tile_pass_smem(32, K, !kPressureGlobalEntries));
+                                 (int)tile_pass_smem(32, K, !kPressureGlobalEntries, kTileCapMax));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_tile_sesph3d_density<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tile_pass_smem(16, K, false));
+                                 (int)tile_pass_smem(16, K, false, kTileCapMax));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_tile_sesph3d_accel<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tile_pass_smem(36, K, false));
+                                 (int)tile_pass_smem(36, K, false, kTileCapMax));
     return e;
 }
 
 inline cudaError_t set_tile_pass_smem(int K) {
     cudaError_t e = cudaFuncSetAttribute(k_tile_iisph3d_l2, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)tile_pass_smem(32, K, !kL2GlobalEntries));
+                                         (int)tile_pass_smem(32, K, !kL2GlobalEntries, kTileCapMax));
     if (e == cudaSuccess) e = set_tuned_pass_smem<1>(K);
     if (e == cudaSuccess) e = set_tuned_pass_smem<2>(K);
     if (e == cudaSuccess) e = set_tuned_pass_smem<3>(K);

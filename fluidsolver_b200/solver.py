@@ -199,9 +199,15 @@ def write_particles(path: str, col: "ParticleCollection") -> None:
 
 
 def _tuning_dict(t) -> dict:
+    """fs_tuning as a dict: the values in use and every measured time, keyed by the value tried."""
     return {"tuned": bool(t.tuned), "first_loop_prefetch": t.first_loop_prefetch,
-            "pressure_prefetch": t.pressure_prefetch, "first_loop_ms": list(t.first_loop_ms),
-            "pressure_iteration_ms": list(t.pressure_iteration_ms)}
+            "pressure_prefetch": t.pressure_prefetch, "tile_cap": t.tile_cap, "block_size": t.block_size,
+            "first_loop_ms": {d + 1: v for d, v in enumerate(t.first_loop_ms) if v > 0},
+            "pressure_iteration_ms": {d + 1: v for d, v in enumerate(t.pressure_iteration_ms) if v > 0},
+            "step_ms_by_tile_cap": {c: v for c, v in zip(F.TILE_CAPS, t.step_ms_by_tile_cap) if v > 0},
+            "fallback_tiles_by_tile_cap": {c: v for c, v, m in zip(F.TILE_CAPS, t.fallback_tiles_by_tile_cap,
+                                                                   t.step_ms_by_tile_cap) if m > 0},
+            "step_ms_by_block_size": {b: v for b, v in zip(F.BLOCK_SIZES, t.step_ms_by_block_size) if v > 0}}
 
 
 class BoundaryPreprocessor:
@@ -419,14 +425,18 @@ class FluidSolverBase:
         return {name: getattr(st, name) for name, _ in st._fields_ if name != "reserved"}
 
     def autotune(self) -> dict:
-        """Chooses the tile passes' prefetch depths by timing steps on a copy of this solver's device
-        context (fs_autotune); this solver's state is left as it was."""
+        """Chooses the fast mode's launch shapes (prefetch depths, staging cap, block size) by timing
+        steps on a copy of this solver's device context (fs_autotune); this solver's state is left as
+        it was. Returns every measured time."""
         t = F.FsTuning()
         F.check(F.lib().fs_autotune(self.ctx, ctypes.byref(t)))
         return _tuning_dict(t)
 
-    def set_tuning(self, first_loop_prefetch: int, pressure_prefetch: int) -> None:
-        t = F.FsTuning(first_loop_prefetch=first_loop_prefetch, pressure_prefetch=pressure_prefetch)
+    def set_tuning(self, first_loop_prefetch: int, pressure_prefetch: int, tile_cap: int = 0,
+                   block_size: int = 0) -> None:
+        """The fast mode's launch shapes (0 keeps the current cap / block size)."""
+        t = F.FsTuning(first_loop_prefetch=first_loop_prefetch, pressure_prefetch=pressure_prefetch,
+                       tile_cap=tile_cap, block_size=block_size)
         F.check(F.lib().fs_set_tuning(self.ctx, ctypes.byref(t)))
 
     # ---- the fluid path tracer (visualizer/raytracer/FluidRaytracer3D) ----
@@ -564,10 +574,12 @@ class BatchedIISPHFluidSolver3D:
         self._ctx = None
         self.last_stats = None
 
-    def set_tuning(self, first_loop_prefetch: int, pressure_prefetch: int) -> None:
-        """Prefetch depths of the tile passes, e.g. as IISPHFluidSolver3D.autotune() chose them on a
-        representative scene (fs_set_tuning)."""
-        t = F.FsTuning(first_loop_prefetch=first_loop_prefetch, pressure_prefetch=pressure_prefetch)
+    def set_tuning(self, first_loop_prefetch: int, pressure_prefetch: int, tile_cap: int = 0,
+                   block_size: int = 0) -> None:
+        """The fast mode's launch shapes, e.g. as IISPHFluidSolver3D.autotune() chose them on a
+        representative scene (fs_set_tuning); 0 keeps the current cap / block size."""
+        t = F.FsTuning(first_loop_prefetch=first_loop_prefetch, pressure_prefetch=pressure_prefetch,
+                       tile_cap=tile_cap, block_size=block_size)
         F.check(F.lib().fs_set_tuning(self.ctx, ctypes.byref(t)))
 
     @property

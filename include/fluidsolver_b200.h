@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define FS_ABI_VERSION 2
+#define FS_ABI_VERSION 3
 
 typedef enum fs_status {
     FS_OK = 0,
@@ -274,21 +274,38 @@ void* fs_stream(fs_ctx* ctx);
 int64_t fs_launch_count(fs_ctx* ctx);
 
 /* ---- tuning ------------------------------------------------------------------
- * How far ahead the 3D IISPH fast mode's tile passes load their neighbor lists
- * (octets of 8 entries; 1..4). No reference counterpart: the reference's
- * loops have nothing to tune. fs_autotune times whole steps with each choice
- * on a copy of the context (same parameters and particles; the context's own
- * state is left as it was), keeps the fastest for the context and reports the
- * times. It allocates a second set of device buffers while it runs. Contexts
- * whose passes are not tiled report tuned = 0. A batched context takes the
- * result of a representative single scene through fs_set_tuning. */
+ * The 3D fast mode's launch shapes (no reference counterpart: the reference's
+ * loops have nothing to tune). fs_autotune times whole steps on a copy of
+ * the context (same parameters and particles; the context's own state is
+ * left as it was) along each axis in turn, keeping the fastest value of one
+ * axis before trying the next, keeps the best for the context and reports
+ * every time it measured:
+ *   - how far ahead the tile passes load their neighbor lists (octets of 8
+ *     entries, 1..4; the first loop's and the pressure passes' depths);
+ *   - the staged candidates per tile (1024, 1536, 2048, 3072): tiles whose
+ *     neighborhood holds more fall back to 32-bit lists read from global
+ *     memory; a larger cap leaves fewer fallback tiles but takes more shared
+ *     memory per block, so fewer blocks fit on an SM;
+ *   - the block size of the step's per-particle kernels (sort keys, reorder,
+ *     cell table, integration): 128, 256, 512 threads.
+ * The tile passes' own shape (128 owners per tile, two threads per owner)
+ * and the cell edge (the search radius, which the tiles' 27-cell ranges
+ * assume) are fixed by the tile design. fs_autotune allocates a second set
+ * of device buffers while it runs. Contexts whose passes are not tiled report
+ * tuned = 0. A batched context takes the result of a representative single
+ * scene through fs_set_tuning. */
 typedef struct fs_tuning {
     int32_t tuned;                   /* 1 if fs_autotune measured */
-    int32_t first_loop_prefetch;     /* the depths in use */
+    int32_t first_loop_prefetch;     /* the values in use */
     int32_t pressure_prefetch;
+    int32_t tile_cap;                /* fs_set_tuning: 0 keeps the current one */
+    int32_t block_size;              /* fs_set_tuning: 0 keeps the current one */
     int32_t reserved;
     float first_loop_ms[4];          /* measured per depth 1..4 (0: not tried) */
     float pressure_iteration_ms[4];  /* per pressure iteration, per depth 1..4 */
+    float step_ms_by_tile_cap[4];    /* whole step, caps 1024, 1536, 2048, 3072 */
+    float step_ms_by_block_size[3];  /* whole step, block sizes 128, 256, 512 */
+    float fallback_tiles_by_tile_cap[4]; /* fraction of tiles on 32-bit lists, per cap */
 } fs_tuning;
 fs_status fs_autotune(fs_ctx* ctx, fs_tuning* out);
 fs_status fs_set_tuning(fs_ctx* ctx, const fs_tuning* in);

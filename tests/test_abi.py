@@ -39,7 +39,7 @@ def test_library_exports_every_declared_symbol(L):
 
 
 def test_abi_version(L):
-    assert L.fs_abi_version() == 2
+    assert L.fs_abi_version() == 3
 
 
 def test_structs_match_the_header(tmp_path):

@@ -1,11 +1,16 @@
-"""The tile passes' prefetch depths (fs_autotune, fs_set_tuning): tuning
-leaves the tuned context's state as it was, and the depth changes only when
-the list entries are loaded, never the arithmetic, so steps with any depths
-are bit-identical."""
+"""The fast mode's launch shapes (fs_autotune, fs_set_tuning): tuning leaves
+the tuned context's state as it was and reports a time for every value it
+tried. The prefetch depth changes only when list entries are loaded, and the
+per-particle kernels' block size only how they are launched, never the
+arithmetic: steps are bit-identical under any of them. The staging cap
+decides which tiles fall back to 32-bit lists, whose owners split their
+lists between their two threads differently: the neighbor sets stay the
+contract's and the results agree to rounding."""
 import numpy as np
 import pytest
 
 from conftest import bits_equal
+from fluidsolver_b200 import _lib as F
 from fluidsolver_b200 import scenes
 from test_gpu_solvers import make_solver, simulator_step
 
@@ -30,7 +35,12 @@ def test_autotune_keeps_the_state_and_picks_valid_depths():
     for f in FIELDS:
         assert bits_equal(getattr(before, f), getattr(after, f)), f
     assert t["tuned"] and 1 <= t["first_loop_prefetch"] <= 4 and 1 <= t["pressure_prefetch"] <= 4
-    assert all(x > 0 for x in t["pressure_iteration_ms"]) and sum(x > 0 for x in t["first_loop_ms"]) == 2
+    assert sorted(t["pressure_iteration_ms"]) == [1, 2, 3, 4] and sorted(t["first_loop_ms"]) == [1, 2]
+    assert all(v > 0 for v in t["pressure_iteration_ms"].values())
+    assert t["tile_cap"] in F.TILE_CAPS and sorted(t["step_ms_by_tile_cap"]) == list(F.TILE_CAPS)
+    assert t["block_size"] in F.BLOCK_SIZES and sorted(t["step_ms_by_block_size"]) == list(F.BLOCK_SIZES)
+    fb = [t["fallback_tiles_by_tile_cap"][c] for c in F.TILE_CAPS]
+    assert all(0.0 <= x <= 1.0 for x in fb) and fb == sorted(fb, reverse=True)
     simulator_step(s)   # the tuned context steps on
     s.close()
 
@@ -48,6 +58,50 @@ def test_prefetch_depths_do_not_change_results():
     for other in runs[1:]:
         for f in FIELDS:
             assert bits_equal(getattr(runs[0], f), getattr(other, f)), f
+
+
+def test_block_size_does_not_change_results():
+    runs = []
+    for b in F.BLOCK_SIZES:
+        s = make_solver("iisph-3d", "hashed-3d", SETTINGS_3D, (0.005, 0.4, 0.25))
+        s.data.collection = dam()
+        s.set_tuning(1, 3, block_size=b)
+        for _ in range(3):
+            s.step()
+        runs.append(s.collection())
+        s.close()
+    for other in runs[1:]:
+        for f in FIELDS:
+            assert bits_equal(getattr(runs[0], f), getattr(other, f)), f
+
+
+def test_tile_cap_keeps_the_sets_and_the_results_to_rounding():
+    runs, lists = [], []
+    for cap in F.TILE_CAPS:
+        s = make_solver("iisph-3d", "hashed-3d", SETTINGS_3D, (0.005, 0.4, 0.25))
+        s.data.collection = dam()
+        s.set_tuning(1, 3, tile_cap=cap)
+        s.step()
+        lists.append(s.solver_lists())
+        for _ in range(2):
+            s.step()
+        runs.append(s.collection())
+        s.close()
+    for (o, i) in lists[1:]:
+        assert np.array_equal(o, lists[0][0]) and np.array_equal(i, lists[0][1])
+    for other in runs[1:]:
+        for f in ("position", "density"):
+            a, b = getattr(runs[0], f).astype(np.float64), getattr(other, f).astype(np.float64)
+            assert np.max(np.abs(a - b)) <= 1e-5 * np.max(np.abs(a)), f
+
+
+def test_invalid_shapes_are_rejected():
+    s = make_solver("iisph-3d", "hashed-3d", SETTINGS_3D, (0.005, 0.4, 0.25))
+    s.data.collection = dam()
+    for kw in ({"tile_cap": 100}, {"tile_cap": 4096}, {"tile_cap": 1030}, {"block_size": 48}, {"block_size": 2048}):
+        with pytest.raises(Exception):
+            s.set_tuning(1, 3, **kw)
+    s.close()
 
 
 def test_untiled_modes_report_nothing_to_tune():
