@@ -49,6 +49,12 @@ PHASE_KERNELS = ["neighborhood search (sort, reorder, cell table, k_build_tiles)
                  "pressure iteration 2..I: k_tile_iisph3d_pressure_acc + k_tile_iisph3d_pressure_update",
                  "k_cfl + k_iisph3d_integrate"]
 PHASE_UNITS = ["step", "launch", "launch", "iteration (two launches)", "step"]
+# The timed window starts PREROLL_STEPS steps into the dam's run, inside its
+# collapse, so that it needs as many pressure iterations per step as the
+# configuration's whole run of FULL_RUN_STEPS steps does on average (its
+# first steps, from rest, need the minimum of 2).
+PREROLL_STEPS = 1000
+FULL_RUN_STEPS = 2000
 
 
 def measured_peak():
@@ -158,15 +164,30 @@ def reference_settings():
             (REFERENCE_UNITS_DT, 0.4, 0.25))
 
 
-def cpu_baseline_from_state(state, n_fluid, seconds_budget=25.0):
-    """The reference's own CPU code (oracle/_ref, all host cores) continuing
-    from the GPU's state: bounded to ~one or two steps of the same scene."""
+def ref_variant():
     from oracle import ref_oracle as R
-    variant = "omp" if R.available("omp") else ("serial" if R.available("serial") else None)
+    return "omp" if R.available("omp") else ("serial" if R.available("serial") else None)
+
+
+def variant_text(variant):
+    return "OpenMP over its 16-particle chunks" if variant == "omp" else "as built, serial"
+
+
+def cpu_baseline_from_state(state, n_fluid, seconds_budget=20.0):
+    """The reference's own CPU code (oracle/_ref, all host cores) continuing
+    from the GPU's state at the end of the timed window: one untimed step
+    first (the reference's first search sorts the whole collection and builds
+    its grid, HashedNeighborhoodSearch3D.cpp:82-131, 187-217), then timed
+    steps until the budget is spent (at least one, at most three)."""
+    from oracle import ref_oracle as R
+    variant = ref_variant()
     if variant is None:
         return None
     params, settings, gen = reference_settings()
     ref = R.RefSolver("iisph-3d", "hashed-3d", state, params, settings, gen, variant=variant)
+    t_cold = time.perf_counter()
+    ref.step()
+    t_cold = time.perf_counter() - t_cold
     steps, t0 = 0, time.perf_counter()
     iters = []
     while True:
@@ -178,15 +199,41 @@ def cpu_baseline_from_state(state, n_fluid, seconds_budget=25.0):
     ref.close()
     cores = os.cpu_count() if variant == "omp" else 1
     return {"value": n_fluid * steps / el, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"{steps} step(s) of the same 1M-fluid scene continuing from the GPU state, "
-                      f"reference libFluid IISPHFluidSolver3D<CubicSplineKernel3D, HashedNeighborhoodSearch3D> "
-                      f"({'OpenMP over its 16-particle chunks' if variant == 'omp' else 'as built, serial'}), "
-                      f"iterations {iters}, {el:.1f} s"}
+            "sample": f"{steps} timed step(s) of the same 1M-fluid scene continuing from the GPU state at the end of "
+                      f"the timed window, after 1 untimed step ({t_cold:.1f} s: the first search's sort and grid "
+                      f"build); reference libFluid IISPHFluidSolver3D<CubicSplineKernel3D, HashedNeighborhoodSearch3D> "
+                      f"({variant_text(variant)}), iterations {iters}, {el:.1f} s timed"}
 
 
-def shard(items, rank: int, world: int) -> list:
-    """Rank `rank` of `world` takes items i with i mod world == rank."""
-    return [x for i, x in enumerate(items) if i % world == rank]
+# iterations per step assumed for every scene when the batched scenes are
+# dealt out (the cost estimate of scene_cost; the measured means lie near 2-4)
+COST_ITERATIONS = 3.0
+
+
+def scene_cost(n_fluid: int, n_boundary: int, iterations: float = COST_ITERATIONS) -> float:
+    """Estimated cost of one step of a scene: its algorithmic bytes
+    (144 per active particle for the search, 216 + 84 I per fluid particle
+    for the IISPH phases), i.e. F * I plus the terms that do not iterate."""
+    return BYTES_SEARCH * (n_fluid + n_boundary) + n_fluid * (BYTES_L1 + BYTES_L2 + BYTES_INTEGRATE + BYTES_ITER * iterations)
+
+
+def shard(items, rank: int, world: int, cost=None) -> list:
+    """The items that rank `rank` of `world` takes: longest processing time
+    first. Items go in order of decreasing cost (ties by index) to the rank
+    with the least cost so far (ties by rank), so every rank's total is at
+    most the mean plus the largest item's cost. Without costs every item
+    costs 1. The assignment depends on the items only, so every rank computes
+    the same split without exchanging anything."""
+    costs = [1.0] * len(items) if cost is None else [float(cost(x)) for x in items]
+    order = sorted(range(len(items)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    mine = []
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += costs[i]
+        if r == rank:
+            mine.append(i)
+    return [items[i] for i in sorted(mine)]
 
 
 def max_reducer(world: int, device):
@@ -226,10 +273,15 @@ def run_ours(args):
     n_active = scene.n_fluid + scene.n_boundary
     solver = make_solver(scene, local, args.precision, args.eager)
     L = F.lib()
-    # the tile passes' prefetch depths, chosen on a copy of this scene (fs_autotune)
+    # the fast mode's launch shapes, chosen on a copy of this scene (fs_autotune)
     tuning = None if args.no_autotune else solver.autotune()
+    # advance the dam into its collapse, where a run of the configuration's
+    # length spends its steps, before warming up and timing
+    run_its = []
+    for _ in range(args.preroll):
+        run_its.append(int(solver.step().iterations))
     for _ in range(args.warmup):
-        solver.step()
+        run_its.append(int(solver.step().iterations))
     ctx = solver.ctx
     stream = torch.cuda.ExternalStream(L.fs_stream(ctx), device=torch.device("cuda", local))
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -276,9 +328,16 @@ def run_ours(args):
         traffic = tj.get(PHASES[dom])
         winst = tj.get("warp_instructions", {}).get(PHASES[dom])
 
+    run_its += iters
+    # the state at the end of the window: where the end-to-end run and the
+    # CPU baseline continue from
+    window_state = solver.collection()
+    # the rest of a run of the configuration's length, for its mean iteration count
+    while len(run_its) < args.full_run:
+        run_its.append(int(solver.step().iterations))
     # end to end through the public API: pinned host state in, step, state out
-    e2e = run_e2e(solver, scene, min(args.steps, 5), local, max_over_ranks)
-    solver_state = solver.collection() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    e2e = run_e2e(solver, window_state, scene.n_fluid, min(args.steps, 5), local, max_over_ranks)
+    solver_state = window_state if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     solver.close()
     batched = None if args.no_batched else run_batched(args, local, rank, world, max_over_ranks, barrier, tuning)
     ns_micro = run_ns_microbench(args, local) if (rank == 0 and world == 1 and not args.no_batched) else None
@@ -297,11 +356,11 @@ def run_ours(args):
         sms = torch.cuda.get_device_properties(local).multi_processor_count
         unit_s = phase[dom] / 1e3 / units[dom]
         peak_issue = sms * 4 * clocks["sm_mhz"] * 1e6
-        issue = {"kernel": PHASE_KERNELS[dom], "per": PHASE_UNITS[dom], "warp_instructions": winst,
-                 "achieved": winst / unit_s / 1e9, "peak": peak_issue / 1e9, "unit": "G warp instructions/s",
-                 "frac": winst / unit_s / peak_issue, "sms": sms, "sm_mhz": clocks["sm_mhz"],
-                 "source": "warp instructions per unit from profiles/traffic.json (ncu smsp__inst_executed.sum); "
-                           "the duration event-timed here"}
+        issue = {"issue_achieved": winst / unit_s / 1e9, "issue_peak": peak_issue / 1e9,
+                 "issue_unit": "G warp instructions/s", "issue_frac": winst / unit_s / peak_issue,
+                 "warp_instructions_per_unit": winst, "sms": sms, "sm_mhz": clocks["sm_mhz"],
+                 "issue_source": "warp instructions per unit from profiles/traffic.json (ncu "
+                                 "smsp__inst_executed.sum); the duration event-timed here"}
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -316,15 +375,20 @@ def run_ours(args):
                        "whole step as one CUDA graph (pressure loop: conditional WHILE node)",
                        "l2": "inputs larger than L2 (~0.5 GB of particle state and lists per step)",
                        "tuning": tuning,
-                       "iterations_mean": it_total / args.steps, "avg_density_error_max": max(errs),
+                       "preroll_steps": args.preroll,
+                       "window": f"steps {args.preroll + args.warmup + 1}-{args.preroll + args.warmup + args.steps} "
+                                 f"of the dam (after {args.preroll} pre-roll and {args.warmup} warm-up steps)",
+                       "iterations_mean": it_total / args.steps,
+                       "iterations_mean_full_run": float(np.mean(run_its)), "full_run_steps": len(run_its),
+                       "avg_density_error_max": max(errs),
                        "phase_ms_per_step": dict(zip(PHASES, (phase / args.steps).round(4).tolist())),
                        "algorithmic_bytes_per_step": step_bytes,
                        "step_fraction_of_hbm_roofline": step_bytes / (ms / args.steps / 1e3) / 1e9 / peak},
-            "roofline": {"bound": "hbm", "kernel": PHASE_KERNELS[dom], "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": per_launch, "per": PHASE_UNITS[dom],
-                         "traffic_source": "profiles/traffic.json (ncu dram__bytes_read.sum + dram__bytes_write.sum)"},
-            "issue": issue,
+            "roofline": dict({"bound": "hbm", "kernel": PHASE_KERNELS[dom], "achieved": achieved, "peak": peak,
+                              "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                              "algorithmic_bytes_per_launch": per_launch, "per": PHASE_UNITS[dom],
+                              "traffic_source": "profiles/traffic.json (ncu dram__bytes_read.sum + "
+                                                "dram__bytes_write.sum)"}, **(issue or {})),
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
             "batched": batched, "ns_microbench": ns_micro, "other_configs": configs,
         }
@@ -334,8 +398,8 @@ def run_ours(args):
 
 
 def run_batched(args, device, rank, world, max_over_ranks, barrier, tuning=None):
-    """The batched breaking dams (256 scenes, seed 6; scenes i = rank mod N on
-    rank N): all of a rank's scenes in one batched context, timed with CUDA
+    """The batched breaking dams (256 scenes, seed 6, dealt out over the ranks
+    by estimated cost, see shard): all of a rank's scenes in one batched context, timed with CUDA
     events on the context's stream around fs_batch_run; at N = 1 the same
     scenes also run one at a time through the single-scene path (fs_run of
     the same steps per scene, events around each), the plain per-scene form."""
@@ -345,11 +409,12 @@ def run_batched(args, device, rank, world, max_over_ranks, barrier, tuning=None)
     from fluidsolver_b200 import scenes
     L = F.lib()
     allsc = scenes.batched_dams(256, seed=6)
-    mine = shard(allsc, rank, world)
+    mine = shard(allsc, rank, world, cost=lambda sc: scene_cost(sc.n_fluid, sc.n_boundary))
     batch = BatchedIISPHFluidSolver3D([s.collection for s in mine], device=device)
     configure_iisph(batch)
-    if tuning and tuning["tuned"]:   # the depths the 1M dam chose
-        batch.set_tuning(tuning["first_loop_prefetch"], tuning["pressure_prefetch"])
+    if tuning and tuning["tuned"]:   # the shapes the 1M dam chose
+        batch.set_tuning(tuning["first_loop_prefetch"], tuning["pressure_prefetch"], tuning["tile_cap"],
+                         tuning["block_size"])
     batch.run(args.warmup)
     stream = torch.cuda.ExternalStream(L.fs_stream(batch.ctx), device=torch.device("cuda", device))
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -375,7 +440,8 @@ def run_batched(args, device, rank, world, max_over_ranks, barrier, tuning=None)
         for sc in allsc:
             solver = make_solver(sc, device)
             if tuning and tuning["tuned"]:
-                solver.set_tuning(tuning["first_loop_prefetch"], tuning["pressure_prefetch"])
+                solver.set_tuning(tuning["first_loop_prefetch"], tuning["pressure_prefetch"], tuning["tile_cap"],
+                                  tuning["block_size"])
             solver.run(args.warmup)
             s2 = torch.cuda.ExternalStream(L.fs_stream(solver.ctx), device=torch.device("cuda", device))
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -389,47 +455,129 @@ def run_batched(args, device, rank, world, max_over_ranks, barrier, tuning=None)
         out["plain_per_scene_value"] = fluid_all * args.steps / (total_ms / 1e3)
         out["plain_per_scene_ms_per_step"] = total_ms / args.steps
         out["speedup_vs_plain_per_scene"] = out["value"] / out["plain_per_scene_value"]
+        if not args.no_cpu_baseline:
+            out["cpu"] = batched_cpu_baseline(allsc)
     return out
 
 
+def batched_cpu_baseline(allsc, sample=16, steps=2):
+    """The reference scene by scene (it has no batching; one
+    IISPHFluidSolver3D per scene, oracle/_ref on all host cores) on a
+    sample of the batched dams: `sample` scenes evenly spaced in fluid count,
+    each 1 untimed + `steps` timed steps. The value is the sample's fluid
+    particle-steps over its total time; the 256 scenes' time follows from it
+    (their fluid total over that rate)."""
+    from oracle import ref_oracle as R
+    variant = ref_variant()
+    if variant is None:
+        return None
+    params, settings, gen = reference_settings()
+    order = sorted(range(len(allsc)), key=lambda i: allsc[i].n_fluid)
+    pick = [order[int(round(q * (len(order) - 1) / (sample - 1)))] for q in range(sample)]
+    fluid_steps, el = 0, 0.0
+    for i in pick:
+        sc = allsc[i]
+        ref = R.RefSolver("iisph-3d", "hashed-3d", sc.collection, params, settings, gen, variant=variant)
+        ref.step()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            ref.step()
+        el += time.perf_counter() - t0
+        fluid_steps += sc.n_fluid * steps
+        ref.close()
+    rate = fluid_steps / el
+    fluid_all = sum(x.n_fluid for x in allsc)
+    return {"value": rate, "unit": UNIT, "ms_per_step_all_scenes": fluid_all / rate * 1e3,
+            "cores": os.cpu_count() if variant == "omp" else 1, "kind": "reference",
+            "sample": f"{sample} of the {len(allsc)} scenes, evenly spaced in fluid count "
+                      f"({min(allsc[i].n_fluid for i in pick):,}-{max(allsc[i].n_fluid for i in pick):,}), "
+                      f"scene by scene, 1 untimed + {steps} timed steps each, {el:.1f} s timed",
+            "variant": variant_text(variant)}
+
+
+def ref_search_time(kind, pts, radius, calls=10, budget_s=15.0):
+    """The reference's own search (oracle/_ref) on the same points: one
+    untimed call (the first builds the grid and, for hashed-3d, sorts the
+    collection), then up to `calls` timed find_neighbors calls within the
+    budget; ms per call (wall clock) and the calls made."""
+    from oracle import ref_oracle as R
+    variant = ref_variant()
+    if variant is None:
+        return None
+    rs = R.RefSearch(kind, pts, radius, variant=variant)
+    t_cold = time.perf_counter()
+    ok = rs.find()
+    t_cold = time.perf_counter() - t_cold
+    if not ok:
+        rs.close()
+        return {"error": "the reference's search threw (a list above its capacity)"}
+    k, t0 = 0, time.perf_counter()
+    while k < calls and (k == 0 or time.perf_counter() - t0 < budget_s):
+        rs.find()
+        k += 1
+    el = time.perf_counter() - t0
+    rs.close()
+    return {"ms_per_search": el / k * 1e3, "calls": k, "first_call_s": t_cold,
+            "points_per_s": len(pts) / (el / k), "cores": os.cpu_count() if variant == "omp" else 1,
+            "kind": "reference", "variant": variant_text(variant)}
+
+
 def run_ns_microbench(args, device):
-    """The 3D search microbenchmark: 10^6 uniform points in the unit cube
-    (seed 2), r = 0.02. (1) The device search as a solver step runs it (sort,
-    reorder, cell table and the neighbor lists of every point), timed with
-    the library's own events over --steps searches. (2) The contract's
-    neighbor sets exported in host index space (fs_get_neighbors_csr, both
-    calls, wall clock). Byte model: 96 B per point (keys, sort, permute of
-    the positions) + (4 n + 8) B of lists per point."""
+    """The 3D search microbenchmark: 10^6 points in the unit cube, r = 0.02,
+    uniform (seed 2) and 64 Gaussian blobs (sigma 0.03, seed 3). (1) The
+    device search as a solver step runs it (sort, reorder, cell table and the
+    neighbor lists of every point), timed with the library's own events over
+    --steps searches: the fast mode's tile lists on the uniform points; on
+    the blobs, whose cores hold over a thousand neighbors per point, the
+    32-bit lists of the FP32 mode. (2) The contract's neighbor sets exported
+    in host index space (fs_get_neighbors_csr, both calls, wall clock).
+    (3) The reference's own searches on the same points (oracle/_ref):
+    HashedNeighborhoodSearch3D on both sets, CompressedNeighborhoodSearch on
+    the uniform points (it throws above 97 neighbors, which the blobs' cores
+    exceed). Byte model: 96 B per point (keys, sort, permute of the
+    positions) + (4 n + 8) B of lists per point."""
     from fluidsolver_b200 import IISPHFluidSolver3D, NeighborhoodSearch, ParticleCollection
-    from fluidsolver_b200 import _lib as F
-    pts = scenes_mod().ns_points_uniform()
-    col = ParticleCollection(position=pts)
-    s = IISPHFluidSolver3D(search="hashed-3d", precision="fp32-kahan", device=device)
-    s.parameters.particle_size = 0.01
-    s.data.collection = col
-    for _ in range(args.warmup):
-        s.execute_neighborhood_search()
-    ms = []
-    for _ in range(args.steps):
-        s.execute_neighborhood_search()
-        ms.append(s.phase_times()[0])
-    s.close()
-    ns = NeighborhoodSearch("hashed-3d", 0.02, device=device)
-    ns.data.collection = col
-    ns.find_neighbors()
-    t0 = time.perf_counter()
-    off, idx = ns.neighbor_lists()
-    export_s = time.perf_counter() - t0
-    ns.close()
-    nbar = len(idx) / len(pts)
-    per = statistics.median(ms)
-    bytes_ = (96 + 4 * nbar + 8) * len(pts)
+    sc = scenes_mod()
     peak, kind = measured_peak()
-    return {"workload": "10^6 uniform points in [0,1)^3 (seed 2), r = 0.02, hashed-3d contract",
-            "neighbors_mean": nbar, "search_with_lists_ms": per, "points_per_s": len(pts) / (per / 1e3),
-            "algorithmic_bytes": bytes_, "achieved_gbs": bytes_ / (per / 1e3) / 1e9,
-            "frac_of_hbm_peak": bytes_ / (per / 1e3) / 1e9 / peak,
-            "csr_export_s": export_s, "csr_export_path": "fs_get_neighbors_csr, sets in host index space, wall clock"}
+    out = {}
+    for case, pts in (("uniform", sc.ns_points_uniform()), ("blobs", sc.ns_points_blobs())):
+        col = ParticleCollection(position=pts)
+        s = IISPHFluidSolver3D(search="hashed-3d", precision="fp32-kahan" if case == "uniform" else "fp32",
+                               device=device)
+        s.parameters.particle_size = 0.01
+        s.data.collection = col
+        for _ in range(args.warmup):
+            s.execute_neighborhood_search()
+        ms = []
+        for _ in range(args.steps):
+            s.execute_neighborhood_search()
+            ms.append(s.phase_times()[0])
+        s.close()
+        ns = NeighborhoodSearch("hashed-3d", 0.02, device=device)
+        ns.data.collection = col
+        ns.find_neighbors()
+        t0 = time.perf_counter()
+        off, idx = ns.neighbor_lists()
+        export_s = time.perf_counter() - t0
+        ns.close()
+        nbar = len(idx) / len(pts)
+        nmax = int(np.max(np.diff(off)))
+        del off, idx
+        per = statistics.median(ms)
+        bytes_ = (96 + 4 * nbar + 8) * len(pts)
+        r = {"workload": f"10^6 {'uniform points' if case == 'uniform' else 'points in 64 Gaussian blobs (sigma 0.03)'}"
+                         f" in [0,1)^3 (seed {2 if case == 'uniform' else 3}), r = 0.02, hashed-3d contract",
+             "neighbors_mean": nbar, "neighbors_max": nmax, "search_with_lists_ms": per,
+             "lists": "tile lists (fast mode)" if case == "uniform" else "32-bit lists (FP32 mode)",
+             "points_per_s": len(pts) / (per / 1e3), "algorithmic_bytes": bytes_,
+             "achieved_gbs": bytes_ / (per / 1e3) / 1e9, "frac_of_hbm_peak": bytes_ / (per / 1e3) / 1e9 / peak,
+             "csr_export_s": export_s, "csr_export_path": "fs_get_neighbors_csr, sets in host index space, wall clock"}
+        if not args.no_cpu_baseline:
+            r["cpu_hashed_3d"] = ref_search_time("hashed-3d", pts, 0.02)
+            if case == "uniform":
+                r["cpu_compressed_3d"] = ref_search_time("compressed-3d", pts, 0.02)
+        out[case] = r
+    return out
 
 
 def run_configs(args, device):
@@ -491,6 +639,22 @@ def run_configs(args, device):
         cpu = ref_time("sesph-2d", "hashed-2d", d2, (1.0, 9.81, 1.0), R.sesph2d_settings(1000.0, 0.01),
                        (0.001, 0.4, 0.25), 200, 10.0)
         out["sesph2d_dam"]["cpu"] = cpu
+    # the same dam on the quadratic-dynamic-allocated contract (every pair tested)
+    s2q = SESPHFluidSolver(search="quadratic-2d", device=device)
+    s2q.parameters.rest_density, s2q.parameters.gravity, s2q.parameters.particle_size = 1.0, 9.81, 1.0
+    s2q.settings.StiffnessK, s2q.settings.Viscosity = 1000.0, 0.01
+    s2q.timestep_generator.settings.timestep = 0.001
+    s2q.data.collection = d2.collection
+    ms2q, _ = gpu_time(s2q, 200)
+    s2q.close()
+    out["sesph2d_dam_quadratic"] = {"workload": f"2D SESPH dam, {d2.n_fluid} fluid + {d2.n_boundary} boundary, "
+                                                "quadratic-2d (QuadraticNeighborhoodSearchDynamicAllocated), k 1000, "
+                                                "nu 0.01, dt 0.001", "gpu_ms_per_step": ms2q,
+                                    "gpu_particle_steps_per_s": d2.n_fluid / (ms2q / 1e3), "cpu": None}
+    if not args.no_cpu_baseline:
+        out["sesph2d_dam_quadratic"]["cpu"] = ref_time(
+            "sesph-2d", "quadratic-2d", d2, (1.0, 9.81, 1.0), R.sesph2d_settings(1000.0, 0.01),
+            (0.001, 0.4, 0.25), 100, 10.0)
     # 3D IISPH 100k dam
     d3 = sc.dam_100k()
     s3 = make_solver(d3, device)
@@ -582,19 +746,19 @@ def scenes_mod():
     return scenes
 
 
-def run_e2e(solver, scene, steps, device, max_over_ranks):
+def run_e2e(solver, src, n_fluid, steps, device, max_over_ranks):
     """Per step: upload the state from pinned host memory, search + step,
     download the state to pinned host memory (the host collection stays
-    authoritative, as when entities or sensors touch it every step)."""
+    authoritative, as when entities or sensors touch it every step). src:
+    the collection the run starts from."""
     import torch
     from fluidsolver_b200 import _lib as F
     L = F.lib()
-    n = len(scene.collection)
+    n = len(src)
 
     def pinned(shape, dtype):
         return torch.empty(shape, dtype=dtype, pin_memory=True).numpy()
 
-    src = scene.collection
     inp = {"position": pinned((n, 3), torch.float32), "velocity": pinned((n, 3), torch.float32),
            "mass": pinned((n,), torch.float32), "density": pinned((n,), torch.float32),
            "type": pinned((n,), torch.uint8)}
@@ -623,30 +787,43 @@ def run_e2e(solver, scene, steps, device, max_over_ranks):
         F.check(L.fs_download(ctx, ctypes.byref(fout)))
     el = max_over_ranks(time.perf_counter() - t0)
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    return {"value": scene.n_fluid * steps * world / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+    return {"value": n_fluid * steps * world / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "steps": steps,
             "path": "fs_upload (pinned host) -> fs_step -> fs_download (pinned host), wall clock"}
 
 
 def run_reference(args):
     """The reference's own CPU implementation (libFluid sources compiled
-    unmodified in oracle/_ref) on all host cores, on a bounded sample of the
-    workload: the 100k-fluid breaking dam of the same scene family."""
+    unmodified in oracle/_ref) on all host cores, on the benchmark's own
+    scene: the 1M-fluid breaking dam with the same parameters, through the
+    reference's solver interface (RefSolver drives its
+    execute_neighborhood_search + execute_simulation_step). Each step is a
+    whole reference step; the run is bounded in time: the first warm-up step
+    (the first search sorts the whole collection and builds the grid) and at
+    most 60 s of further warm-up steps, then timed steps until --steps or
+    150 s, whichever comes first. The reference starts from the dam at rest,
+    where a step needs the fewest pressure iterations (this arm's window lies
+    earlier in the run than the GPU arm's, which favours the reference)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle import ref_oracle as R
     from fluidsolver_b200 import scenes
-    variant = "omp" if R.available("omp") else ("serial" if R.available("serial") else None)
+    variant = ref_variant()
     if variant is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (needs the reference "
                           "checkout at build time)"}))
         return
-    scene = scenes.dam_100k()
+    scene = scenes.dam_1m() if args.scene == "1m" else scenes.dam_100k()
     params, settings, gen = reference_settings()
     ref = R.RefSolver("iisph-3d", "hashed-3d", scene.collection, params, settings, gen, variant=variant)
+    t_w = time.perf_counter()
+    warm = 0
     for _ in range(args.warmup):
         ref.step()
+        warm += 1
+        if time.perf_counter() - t_w > 60.0:
+            break
     iters = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
@@ -658,18 +835,22 @@ def run_reference(args):
     done = len(iters)
     value = scene.n_fluid * done / el
     cores = os.cpu_count() if variant == "omp" else 1
-    sample = (f"100,000-fluid breaking dam (40x50x50 column, 59,684 boundary) of the same scene family, "
-              f"{done} of {args.steps} steps (150 s budget) after {args.warmup} warm-up steps, "
-              f"mean iterations {np.mean(iters):.2f}")
+    desc = (f"{scene.n_fluid:,}-fluid breaking dam ({scene.n_boundary:,} boundary), steps {warm + 1}-{warm + done} "
+            f"from rest: {done} of {args.steps} timed steps (150 s budget) after {warm} of {args.warmup} warm-up "
+            f"steps (60 s budget), mean iterations {np.mean(iters):.2f}")
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
-        "steps": done, "warmup": args.warmup, "ms_per_step": el / done * 1e3, "higher_is_better": True,
+        "steps": done, "warmup": warm, "ms_per_step": el / done * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded breaking-dam scenes)",
         "impl": "reference",
-        "config": {"workload": "3D IISPH breaking dam (bounded sample: 100k fluid), hashed-3d, dt 0.005",
+        "config": {"workload": "3D IISPH breaking dam, " + (
+                       "1,000,000 fluid + 256,624 boundary particles (the benchmark's scene)" if args.scene == "1m"
+                       else "100,000 fluid + 59,684 boundary particles") +
+                   ", hashed-3d neighbor contract, dt 0.005 (reference units), single-layer boundary",
+                   "same_config": args.scene == "1m",
                    "implementation": "libFluid IISPHFluidSolver3D<CubicSplineKernel3D, HashedNeighborhoodSearch3D>, "
-                                     + ("OpenMP over its 16-particle chunks" if variant == "omp" else "as built")},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+                                     + variant_text(variant)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -683,7 +864,13 @@ def main():
     ap.add_argument("--precision", default="fp32-kahan", choices=["fp32", "fp32-kahan", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-scene batched measurement")
-    ap.add_argument("--no-autotune", action="store_true", help="keep the default prefetch depths of the tile passes")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes of the fast mode")
+    ap.add_argument("--preroll", type=int, default=PREROLL_STEPS,
+                    help="steps the dam advances before the warm-up (into its collapse)")
+    ap.add_argument("--full-run", type=int, default=FULL_RUN_STEPS,
+                    help="steps of the whole run whose mean iteration count is reported (untimed)")
+    ap.add_argument("--scene", default="1m", choices=["1m", "100k"],
+                    help="reference arm only: the dam it times (1m: the benchmark's own scene)")
     ap.add_argument("--eager", action="store_true",
                     help="host-driven pressure loop instead of the whole-step CUDA graph: for kernel-level profiling "
                          "(ncu cannot profile the kernels of a graph with conditional nodes); slower, not a bench value")
