@@ -15,5 +15,6 @@ from .solver import (  # noqa: F401
     SESPHFluidSolver3D,
     Timepoint,
     read_particles,
+    tone_map,
     write_particles,
 )

@@ -66,7 +66,7 @@ EXPORTED_SYMBOLS = (
     "fs_query_position_noalloc", "fs_get_solver_lists_csr", "fs_boundary_preprocess", "fs_global_statistics",
     "fs_particles_file_info", "fs_particles_file_read", "fs_particles_file_write", "fs_dump",
     "fs_autotune", "fs_set_tuning", "fs_trace_rays", "fs_render_settings_default", "fs_render",
-    "fs_set_tile_wait_limit",
+    "fs_set_tile_wait_limit", "fs_tone_map",
 )
 
 
@@ -136,7 +136,8 @@ class FsCamera(ctypes.Structure):
 class FsRenderSettings(ctypes.Structure):
     _fields_ = [("samples_per_pixel", c_int32), ("maximum_recursion_depth", c_int32),
                 ("output_normals_of_first_hit", c_int32), ("surface_density_fraction", c_float),
-                ("exposure", c_float), ("gamma", c_float), ("seed", ctypes.c_uint64)]
+                ("exposure", c_float), ("gamma", c_float), ("seed", ctypes.c_uint64), ("tone_mapper", c_int32),
+                ("gamma_correction", c_int32)]
 
 
 class FluidSolverError(RuntimeError):
@@ -182,6 +183,7 @@ def lib() -> ctypes.CDLL:
     L.fs_render.argtypes = [ctx_p, POINTER(FsCamera), POINTER(FsRenderSettings), c_void_p, c_void_p]
     L.fs_set_tuning.argtypes = [ctx_p, POINTER(FsTuning)]
     L.fs_set_tile_wait_limit.argtypes = [ctx_p, c_int32]
+    L.fs_tone_map.argtypes = [c_void_p, c_int64, POINTER(FsRenderSettings), c_void_p]
     L.fs_global_statistics.argtypes = [ctx_p, c_float, POINTER(FsGlobalStats)]
     L.fs_query_position.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
     L.fs_query_position_noalloc.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
@@ -200,7 +202,7 @@ def lib() -> ctypes.CDLL:
                  "fs_batch_create", "fs_batch_run", "fs_query_position_noalloc", "fs_get_solver_lists_csr",
                  "fs_boundary_preprocess", "fs_global_statistics", "fs_particles_file_info",
                  "fs_particles_file_read", "fs_particles_file_write", "fs_dump", "fs_autotune", "fs_set_tuning",
-                 "fs_trace_rays", "fs_render", "fs_set_tile_wait_limit"):
+                 "fs_trace_rays", "fs_render", "fs_set_tile_wait_limit", "fs_tone_map"):
         getattr(L, name).restype = c_int32
     _lib = L
     return L

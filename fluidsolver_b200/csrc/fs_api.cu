@@ -2258,10 +2258,45 @@ void fs_render_settings_default(fs_render_settings* r) {
     r->exposure = 0.2f;                   // ToneMapper::ToneMapperSettings (ToneMapper.hpp:11-20)
     r->gamma = 2.2f;
     r->seed = 1;
+    r->tone_mapper = 0;                   // ToneMapperFunction::Exponential
+    r->gamma_correction = 1;
+}
+
+// ToneMapper's mapping of one radiance value to a byte colour
+// (ToneMapper.cpp:7-102), in the reference's float operations: exposure,
+// the exponential 1 - exp(-v) or the ACES filmic curve (with its clamp),
+// the clamp to [0, 1], the gamma correction pow(v, 1 / gamma), and the
+// byte (clamp(v) * 255, truncated).
+static float tone_clamp(float v) { return v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v); }
+static void tone_map_pixels(const float* radiance, int64_t np, const fs_render_settings* r, uint8_t* rgba) {
+    const float gpow = 1.0f / r->gamma;
+    for (int64_t i = 0; i < np; i++) {
+        for (int a = 0; a < 3; a++) {
+            float v = radiance[3 * i + a] * r->exposure;
+            if (r->tone_mapper == 1) {
+                const float ka = 2.51f, kb = 0.03f, kc = 2.43f, kd = 0.59f, ke = 0.14f;
+                v = tone_clamp((v * (ka * v + kb)) / (v * (kc * v + kd) + ke));
+            } else {
+                v = 1.0f - std::exp(-v);
+            }
+            v = tone_clamp(v);
+            if (r->gamma_correction) v = std::pow(v, gpow);
+            rgba[4 * i + a] = (uint8_t)(tone_clamp(v) * 255.0f);
+        }
+        rgba[4 * i + 3] = 255;
+    }
+}
+
+fs_status fs_tone_map(const float* radiance, int64_t pixels, const fs_render_settings* r, uint8_t* rgba) {
+    if (!radiance || !r || !rgba || pixels < 0) return fail(FS_ERR_INVALID, "null argument or negative size");
+    if (r->tone_mapper != 0 && r->tone_mapper != 1) return fail(FS_ERR_INVALID, "tone_mapper must be 0 or 1");
+    tone_map_pixels(radiance, pixels, r, rgba);
+    return FS_OK;
 }
 
 fs_status fs_render(fs_ctx* c, const fs_camera* cam, const fs_render_settings* r, float* radiance, uint8_t* rgba) {
     if (!c || !cam || !r || !radiance) return fail(FS_ERR_INVALID, "null argument");
+    if (r->tone_mapper != 0 && r->tone_mapper != 1) return fail(FS_ERR_INVALID, "tone_mapper must be 0 or 1");
     if (cam->width <= 0 || cam->height <= 0 || (int64_t)cam->width * cam->height > (int64_t)1 << 26)
         return fail(FS_ERR_INVALID, "image size out of range");
     if (r->samples_per_pixel <= 0 || r->maximum_recursion_depth < 0) return fail(FS_ERR_INVALID, "bad settings");
@@ -2314,19 +2349,7 @@ fs_status fs_render(fs_ctx* c, const fs_camera* cam, const fs_render_settings* r
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     cudaFree(d_rad);
     if (e != cudaSuccess) return fail(FS_ERR_CUDA, std::string("rendering: ") + cudaGetErrorString(e));
-    if (rgba) {   // ToneMapper::map_radiance_to_image_color (ToneMapper.cpp:79-102), exponential curve
-        auto byte = [](float v) { return (uint8_t)((v < 0.0f ? 0.0f : v > 1.0f ? 1.0f : v) * 255.0f); };
-        for (int64_t i = 0; i < np; i++) {
-            for (int a = 0; a < 3; a++) {
-                float v = radiance[3 * i + a] * r->exposure;
-                v = 1.0f - std::exp(-v);
-                v = v < 0.0f ? 0.0f : v > 1.0f ? 1.0f : v;
-                v = std::pow(v, 1.0f / r->gamma);
-                rgba[4 * i + a] = byte(v);
-            }
-            rgba[4 * i + 3] = 255;
-        }
-    }
+    if (rgba) tone_map_pixels(radiance, np, r, rgba);   // ToneMapper::map_render_target_to_image
     return FS_OK;
 }
 

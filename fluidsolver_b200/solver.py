@@ -198,6 +198,20 @@ def write_particles(path: str, col: "ParticleCollection") -> None:
     F.check(F.lib().fs_particles_file_write(str(path).encode(), c.dim, ctypes.byref(c.as_fs())))
 
 
+def tone_map(radiance, exposure: float = 0.2, gamma: float = 2.2, filmic: bool = False,
+             gamma_correction: bool = True) -> np.ndarray:
+    """ToneMapper::map_render_target_to_image (ToneMapper.cpp:71-102) on radiance of shape (..., 3):
+    bytes of shape (..., 4) (fs_tone_map, host code; the mapping fs_render applies)."""
+    rad = np.ascontiguousarray(radiance, np.float32)
+    n = rad.size // 3
+    rs = F.FsRenderSettings()
+    F.lib().fs_render_settings_default(ctypes.byref(rs))
+    rs.exposure, rs.gamma, rs.tone_mapper, rs.gamma_correction = exposure, gamma, int(filmic), int(gamma_correction)
+    out = np.zeros(rad.shape[:-1] + (4,), np.uint8)
+    F.check(F.lib().fs_tone_map(rad.ctypes.data, n, ctypes.byref(rs), out.ctypes.data))
+    return out
+
+
 def _tuning_dict(t) -> dict:
     """fs_tuning as a dict: the values in use and every measured time, keyed by the value tried."""
     return {"tuned": bool(t.tuned), "first_loop_prefetch": t.first_loop_prefetch,
@@ -457,7 +471,8 @@ class FluidSolverBase:
                field_of_view_x: float = 90.0 / 360.0 * 2.0 * 3.1415, flip_y: bool = False, **settings):
         """FluidRaytracer3D::render on the device state (fs_render): (radiance, rgba) arrays of
         height x width x 3 floats and x 4 bytes. settings: samples_per_pixel, maximum_recursion_depth,
-        output_normals_of_first_hit, surface_density_fraction, exposure, gamma, seed."""
+        output_normals_of_first_hit, surface_density_fraction, exposure, gamma, seed, tone_mapper (0
+        exponential, 1 filmic), gamma_correction."""
         cam = F.FsCamera()
         cam.position[:], cam.view_direction[:], cam.view_up[:] = position, view_direction, view_up
         cam.field_of_view_x, cam.width, cam.height, cam.flip_y = field_of_view_x, width, height, int(flip_y)

@@ -377,10 +377,17 @@ typedef struct fs_render_settings {
     int32_t maximum_recursion_depth;      /* FluidRaytracer3D::Settings */
     int32_t output_normals_of_first_hit;
     float surface_density_fraction;       /* of the rest density: the surface's iso density */
-    float exposure, gamma;                /* ToneMapper (exponential curve, gamma correction) */
+    float exposure, gamma;                /* ToneMapper::ToneMapperSettings (ToneMapper.hpp:9-20) */
     uint64_t seed;                        /* of the per-pixel random streams */
+    int32_t tone_mapper;                  /* 0 exponential (the default), 1 filmic (the ACES curve) */
+    int32_t gamma_correction;             /* 1: the gamma correction is applied (the default) */
 } fs_render_settings;
 void fs_render_settings_default(fs_render_settings* r);
+/* ToneMapper::map_render_target_to_image (ToneMapper.cpp:71-102) on host
+ * radiance, without a context: exposure, the settings' tone mapping curve,
+ * the gamma correction when enabled, bytes; rgba receives 4 bytes per pixel
+ * (alpha 255). fs_render applies the same mapping. Host code only. */
+fs_status fs_tone_map(const float* radiance, int64_t pixels, const fs_render_settings* settings, uint8_t* rgba);
 /* FluidRaytracer3D::render: radiance (width * height * 3 floats, row-major from
  * the top-left pixel), the path tracer's estimate with a white sky
  * (FluidRaytracer3D.cpp:70-165; Skybox without an image); rgba (width * height

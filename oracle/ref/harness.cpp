@@ -30,6 +30,7 @@
 #include "time/DynamicCflTimestepGenerator.hpp"
 #include "entities/BoundaryPreprocessor.hpp"
 #include "visualizer/raytracer/ParticleIntersectionAccelerator.hpp"
+#include "visualizer/raytracer/ToneMapper.hpp"
 
 #include <algorithm>
 #include <cstdint>
@@ -462,6 +463,44 @@ int ref_trace_rays(int64_t n, const float* pos, const float* mass, const uint8_t
 // Neighbor lists in tag space, in the reference's own list order: for tag t,
 // idx[offsets[t] .. offsets[t+1]) are the tags of its neighbors. With
 // idx == nullptr only offsets are filled. Returns the total count.
+// ToneMapper::map_render_target_to_image (ToneMapper.cpp:71-102) on a w x h
+// render target of radiance (3 floats per pixel, row-major from the top-left
+// pixel); rgba receives the image's 4 bytes per pixel. filmic selects the
+// ACES curve instead of the exponential one.
+int ref_tone_map(int64_t w, int64_t h, const float* radiance, float exposure, float gamma, int gamma_enabled,
+                 int filmic, uint8_t* rgba) {
+    try {
+        Raytracer::RenderTarget target;
+        target.set_size((size_t)w, (size_t)h);
+        for (int64_t y = 0; y < h; y++)
+            for (int64_t x = 0; x < w; x++) {
+                const float* v = radiance + 3 * (y * w + x);
+                target.set((size_t)x, (size_t)y, glm::vec3(v[0], v[1], v[2]));
+            }
+        Image image((size_t)w, (size_t)h);
+        Raytracer::ToneMapper tm;
+        tm.settings.exposure = exposure;
+        tm.settings.gamma = gamma;
+        tm.settings.gamma_correction_enabled = gamma_enabled != 0;
+        tm.settings.tone_mapper_function = filmic ? Raytracer::ToneMapper::ToneMapperSettings::ToneMapperFunction::Filmic
+                                                  : Raytracer::ToneMapper::ToneMapperSettings::ToneMapperFunction::Exponential;
+        tm.map_render_target_to_image(target, image);
+        for (int64_t y = 0; y < h; y++)
+            for (int64_t x = 0; x < w; x++) {
+                const Image::Color c = image.get((size_t)x, (size_t)y);
+                uint8_t* o = rgba + 4 * (y * w + x);
+                o[0] = c.r;
+                o[1] = c.g;
+                o[2] = c.b;
+                o[3] = c.a;
+            }
+        return 0;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
 int64_t ref_ns_lists(void* h, int64_t* offsets, int64_t* idx) {
     auto* ns = static_cast<NsBase*>(h);
     auto& c = *ns->collection;

@@ -1,6 +1,7 @@
 // Minimal stand-in for the parts of the glm vector-math library that
 // libFluid's hot-path sources use (vec2/vec3 arithmetic, dot, length,
-// normalize, isnan, any). Test infrastructure only: it lets the oracle build
+// normalize, isnan, any; vec4 and the r/g/b/a colour names for the image
+// types of the tone mapper). Test infrastructure only: it lets the oracle build
 // compile the reference solver sources unmodified.
 //
 // Arithmetic follows glm's scalar (non-SIMD) code path:
@@ -43,16 +44,30 @@ namespace glm {
     };
 
     struct vec3 {
-        float x, y, z;
+        // r, g, b name the same components (glm's colour aliases)
+        union { float x, r; };
+        union { float y, g; };
+        union { float z, b; };
         vec3() = default;
         constexpr explicit vec3(float s) : x(s), y(s), z(s) {}
-        constexpr vec3(float a, float b, float c) : x(a), y(b), z(c) {}
+        constexpr vec3(float a0, float a1, float a2) : x(a0), y(a1), z(a2) {}
         float& operator[](std::size_t i) { return i == 0 ? x : (i == 1 ? y : z); }
         const float& operator[](std::size_t i) const { return i == 0 ? x : (i == 1 ? y : z); }
         vec3& operator+=(const vec3& o) { x = x + o.x; y = y + o.y; z = z + o.z; return *this; }
         vec3& operator-=(const vec3& o) { x = x - o.x; y = y - o.y; z = z - o.z; return *this; }
         vec3& operator*=(float s) { x = x * s; y = y * s; z = z * s; return *this; }
         vec3& operator/=(float s) { x = x / s; y = y / s; z = z / s; return *this; }
+    };
+
+    struct vec4 {
+        union { float x, r; };
+        union { float y, g; };
+        union { float z, b; };
+        union { float w, a; };
+        vec4() = default;
+        constexpr explicit vec4(float s) : x(s), y(s), z(s), w(s) {}
+        constexpr vec4(float a0, float a1, float a2, float a3) : x(a0), y(a1), z(a2), w(a3) {}
+        constexpr vec4(const vec3& v, float a3) : x(v.x), y(v.y), z(v.z), w(a3) {}
     };
 
     // ---- vec2 ----

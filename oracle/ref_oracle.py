@@ -43,6 +43,7 @@ def lib(variant: str = "serial") -> ctypes.CDLL:
     L.ref_dynamic_timestep.restype = c_float
     L.ref_boundary_preprocess.argtypes = [c_void_p, c_void_p, c_float, c_float, c_void_p]
     L.ref_trace_rays.argtypes = [c_int64, c_void_p, c_void_p, c_void_p, c_float, c_float, c_int64] + [c_void_p] * 6
+    L.ref_tone_map.argtypes = [c_int64, c_int64, c_void_p, c_float, c_float, c_int, c_int, c_void_p]
     L.ref_ns_create.restype = c_void_p
     L.ref_ns_create.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_float]
     L.ref_ns_destroy.argtypes = [c_void_p]
@@ -103,6 +104,18 @@ def trace_rays(pos, mass, type_, particle_size, rest_density, origins, direction
            "normal": np.zeros((m, 3), np.float32), "length": np.zeros(m, np.float32)}
     if lib().ref_trace_rays(len(pos), _p(pos), _p(mass), _p(t), particle_size, rest_density, m, _p(o), _p(d),
                             _p(out["hit"]), _p(out["point"]), _p(out["normal"]), _p(out["length"])) != 0:
+        raise RuntimeError(lib().ref_last_error().decode())
+    return out
+
+
+def tone_map(radiance, exposure=0.2, gamma=2.2, filmic=False, gamma_correction=True) -> np.ndarray:
+    """The reference's ToneMapper (map_render_target_to_image) on radiance of shape (h, w, 3):
+    (h, w, 4) bytes."""
+    rad = np.ascontiguousarray(radiance, np.float32)
+    h, w = rad.shape[0], rad.shape[1]
+    out = np.zeros((h, w, 4), np.uint8)
+    if lib().ref_tone_map(w, h, _p(rad), exposure, gamma, 1 if gamma_correction else 0, 1 if filmic else 0,
+                          _p(out)) != 0:
         raise RuntimeError(lib().ref_last_error().decode())
     return out
 

@@ -284,12 +284,39 @@ def position_query_fixture():
     np.savez_compressed(os.path.join(OUT, "position_queries.npz"), **out)
 
 
+TONE_CASES = {"exponential": dict(exposure=0.2, gamma=2.2, filmic=False, gamma_correction=True),
+              "filmic": dict(exposure=0.7, gamma=2.2, filmic=True, gamma_correction=True),
+              "exponential_linear": dict(exposure=1.5, gamma=1.0, filmic=False, gamma_correction=False),
+              "filmic_linear": dict(exposure=0.05, gamma=1.8, filmic=True, gamma_correction=False)}
+
+
+def tone_radiance():
+    """Fixed radiance for the tone mapper: log-spread values over 1e-4..1e3,
+    zeros, negatives, values at the byte boundaries, one infinity."""
+    rng = np.random.default_rng(15)
+    r = np.exp(rng.uniform(np.log(1e-4), np.log(1e3), (48, 64, 3))).astype(np.float32)
+    r[0, :8] = 0.0
+    r[1, :8] = -rng.uniform(0, 5, (8, 3))
+    r[2, :16] = (np.arange(16 * 3).reshape(16, 3) / 47.0 * 20.0).astype(np.float32)
+    r[3, 0] = np.inf
+    return r
+
+
+def tonemap_fixture():
+    """ToneMapper::map_render_target_to_image (ToneMapper.cpp:71-102) through the reference's own class."""
+    rad = tone_radiance()
+    out = {"radiance": rad}
+    for name, kw in TONE_CASES.items():
+        out[name] = R.tone_map(rad, **kw)
+    np.savez_compressed(os.path.join(OUT, "tonemap.npz"), **out)
+
+
 if __name__ == "__main__":
     if not R.available():
         sys.exit("oracle/_ref is not built; run `make -C oracle/ref REF=<reference checkout>` where it is available")
     fixtures = {"kernel": kernel_fixture, "cfl": cfl_fixture, "search": search_fixture, "solvers": solver_fixture,
                 "position_queries": position_query_fixture, "dynamic_timestep": dynamic_timestep_fixture,
-                "boundary": boundary_fixture, "raytrace": raytrace_fixture}
+                "boundary": boundary_fixture, "raytrace": raytrace_fixture, "tonemap": tonemap_fixture}
     for name in sys.argv[1:] or fixtures:
         fixtures[name]()
     for f in sorted(os.listdir(OUT)):

@@ -13,6 +13,8 @@ order); they are checked for what holds for every sample: the white sky where
 rays miss, radiance below the sky's where they hit, the normal colours of the
 first hits, the tone mapping, and the same image for the same seed."""
 import numpy as np
+
+from fluidsolver_b200 import tone_map
 import pytest
 
 from fluidsolver_b200 import scenes
@@ -89,6 +91,11 @@ def test_render_path_tracing(dam_solver):
     v = np.clip(1.0 - np.exp(-(rad.astype(np.float32) * np.float32(0.2))), 0, 1) ** (1 / 2.2)
     assert np.abs(rgba[..., :3].astype(int) - (v * 255).astype(int)).max() <= 1
     assert (rgba[..., 3] == 255).all()
+    # exactly the mapping fs_tone_map applies, which tests/test_tonemap.py pins to the
+    # reference's ToneMapper byte for byte; the filmic curve through the render settings too
+    assert np.array_equal(rgba, tone_map(rad))
+    rad_f, rgba_f = dam_solver.render(**CAM, samples_per_pixel=16, seed=5, tone_mapper=1, exposure=0.6)
+    assert np.array_equal(rad_f, rad) and np.array_equal(rgba_f, tone_map(rad, exposure=0.6, filmic=True))
 
 
 def test_render_rejects_bad_arguments(dam_solver):
