@@ -31,6 +31,7 @@
 #include "entities/BoundaryPreprocessor.hpp"
 #include "visualizer/raytracer/ParticleIntersectionAccelerator.hpp"
 #include "visualizer/raytracer/ToneMapper.hpp"
+#include "sensors/ParticleStatistics.hpp"
 
 #include <algorithm>
 #include <cstdint>
@@ -497,6 +498,66 @@ int ref_tone_map(int64_t w, int64_t h, const float* radiance, float exposure, fl
         return 0;
     } catch (const std::exception& e) {
         g_last_error = e.what();
+        return -1;
+    }
+}
+
+// The global sensors of ParticleStatistics.cpp through their own
+// calculate_for_timepoint: out = {density max, min, avg, pressure max, min,
+// avg, velocity max, min, avg, kinetic energy, potential energy}, counts =
+// {normal, boundary, inactive}. The velocity and energy sensors read the 2D
+// MovementData (ParticleStatistics.cpp:101-167); for dim 3 they are not run
+// and their entries are NaN.
+int ref_global_stats(int dim, int64_t n, const float* pos, const float* vel, const float* mass, const float* density,
+                     const float* pressure, const uint8_t* type, float gravity, float zero_height, float* out,
+                     int64_t* counts) {
+    try {
+        auto c = std::make_shared<ParticleCollection>();
+        fill_collection(*c, dim, n, pos, type);
+        for (int64_t i = 0; i < n; i++) {
+            if (dim == 2) c->get<MovementData>(i).velocity = glm::vec2(vel[2 * i], vel[2 * i + 1]);
+            else c->get<MovementData3D>(i).velocity = glm::vec3(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+            auto& pd = c->get<ParticleData>(i);
+            pd.mass = mass[i];
+            pd.density = density[i];
+            pd.pressure = pressure[i];
+        }
+        Timepoint tp;
+        Sensors::GlobalDensitySensor ds;
+        ds.simulator_data.collection = c;
+        const auto d = ds.calculate_for_timepoint(tp);
+        Sensors::GlobalPressureSensor ps;
+        ps.simulator_data.collection = c;
+        const auto p = ps.calculate_for_timepoint(tp);
+        Sensors::GlobalParticleCountSensor cs;
+        cs.simulator_data.collection = c;
+        const auto k = cs.calculate_for_timepoint(tp);
+        const float nan = std::numeric_limits<float>::quiet_NaN();
+        float v[3] = {nan, nan, nan}, e[2] = {nan, nan};
+        if (dim == 2) {
+            Sensors::GlobalVelocitySensor vs;
+            vs.simulator_data.collection = c;
+            const auto vd = vs.calculate_for_timepoint(tp);
+            v[0] = vd.maximum;
+            v[1] = vd.minimum;
+            v[2] = vd.average;
+            Sensors::GlobalEnergySensor es;
+            es.simulator_data.collection = c;
+            es.simulator_parameters.gravity = gravity;
+            es.settings.relative_zero_height = zero_height;
+            const auto ed = es.calculate_for_timepoint(tp);
+            e[0] = ed.kinetic;
+            e[1] = ed.potential;
+        }
+        const float vals[11] = {d.maximum, d.minimum, d.average, p.maximum, p.minimum, p.average,
+                                v[0], v[1], v[2], e[0], e[1]};
+        std::memcpy(out, vals, sizeof(vals));
+        counts[0] = (int64_t)k.normal_particles;
+        counts[1] = (int64_t)k.boundary_particles;
+        counts[2] = (int64_t)k.inactive_particles;
+        return 0;
+    } catch (const std::exception& ex) {
+        g_last_error = ex.what();
         return -1;
     }
 }

@@ -44,6 +44,7 @@ def lib(variant: str = "serial") -> ctypes.CDLL:
     L.ref_boundary_preprocess.argtypes = [c_void_p, c_void_p, c_float, c_float, c_void_p]
     L.ref_trace_rays.argtypes = [c_int64, c_void_p, c_void_p, c_void_p, c_float, c_float, c_int64] + [c_void_p] * 6
     L.ref_tone_map.argtypes = [c_int64, c_int64, c_void_p, c_float, c_float, c_int, c_int, c_void_p]
+    L.ref_global_stats.argtypes = [c_int, c_int64] + [c_void_p] * 6 + [c_float, c_float, c_void_p, c_void_p]
     L.ref_ns_create.restype = c_void_p
     L.ref_ns_create.argtypes = [c_int, c_int64, c_void_p, c_void_p, c_float]
     L.ref_ns_destroy.argtypes = [c_void_p]
@@ -118,6 +119,28 @@ def tone_map(radiance, exposure=0.2, gamma=2.2, filmic=False, gamma_correction=T
                           _p(out)) != 0:
         raise RuntimeError(lib().ref_last_error().decode())
     return out
+
+
+STAT_NAMES = ["density_max", "density_min", "density_avg", "pressure_max", "pressure_min", "pressure_avg",
+              "velocity_max", "velocity_min", "velocity_avg", "kinetic_energy", "potential_energy"]
+
+
+def global_stats(col, gravity: float, zero_height: float = 0.0) -> dict:
+    """The reference's global sensors (ParticleStatistics.cpp: density, pressure,
+    velocity, energy, particle counts) through their calculate_for_timepoint.
+    Velocity and energy are NaN for 3D collections (the reference's sensors
+    read 2D MovementData)."""
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+    pos, vel = f(col.position), f(col.velocity)
+    out = np.zeros(11, np.float32)
+    counts = np.zeros(3, np.int64)
+    if lib().ref_global_stats(pos.shape[1], len(pos), _p(pos), _p(vel), _p(f(col.mass)), _p(f(col.density)),
+                              _p(f(col.pressure)), _p(np.ascontiguousarray(col.type, np.uint8)), gravity, zero_height,
+                              _p(out), _p(counts)) != 0:
+        raise RuntimeError(lib().ref_last_error().decode())
+    d = {k: np.float32(v) for k, v in zip(STAT_NAMES, out)}
+    d.update(normal_particles=int(counts[0]), boundary_particles=int(counts[1]), inactive_particles=int(counts[2]))
+    return d
 
 
 class RefSearch:

@@ -1,7 +1,8 @@
 """Entities and sensors on the device: the boundary preprocessor
 (BoundaryPreprocessor.cpp:7-48) against the reference's own entity (golden
 fixtures, bit for bit in the FP32 reference-order mode) and the global
-sensors (ParticleStatistics.cpp:17-201) against the oracle's restatement."""
+sensors (ParticleStatistics.cpp:17-201) against the oracle's restatement and
+against the reference's own sensor classes compiled in oracle/_ref."""
 import numpy as np
 import pytest
 
@@ -104,6 +105,50 @@ def test_global_statistics_2d(c_oracle):
     want = c_oracle.global_stats(out, 9.81, 0.0)
     _check_stats(got, want, out, out.type == 0, 9.81, 0.0)
     s.close()
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_global_statistics_against_the_reference_sensors(ref_oracle, dim):
+    """fs_global_statistics against the reference's own sensor classes
+    (ParticleStatistics.cpp:17-201, compiled in oracle/_ref) on the device
+    state after a few steps: maxima, minima and counts bit for bit; averages
+    and energies, which the device sums in FP64 and the reference serially in
+    float, within the float sum's own error bound (n - 1) u sum|x_i|, u = 2^-24.
+    Velocity and energy in 2D only (the reference's sensors read 2D MovementData)."""
+    if dim == 3:
+        sc = scenes.breaking_dam_3d(16, 14, 12, 1.0, tank=(50, 30, 25), seed=8)
+        col = sc.collection
+        col.type[::97] = 2
+        s = make_solver("iisph-3d", "hashed-3d", SETTINGS_3D, (0.005, 0.4, 0.25))
+    else:
+        col = scenes.breaking_dam_2d(30, 20, seed=4).collection
+        s = make_solver("sesph-2d", "hashed-2d", [1000.0, 0.01], (0.001, 0.4, 0.25))
+    s.data.collection = col
+    for _ in range(4):
+        simulator_step(s)
+    got = s.global_statistics(zero_height=2.0)
+    out = s.collection()
+    want = ref_oracle.global_stats(out, 9.81, 2.0)
+    s.close()
+    fields = ("density", "pressure", "velocity") if dim == 2 else ("density", "pressure")
+    for k in fields:
+        assert bits_equal(np.float32(got[f"{k}_max"]), want[f"{k}_max"]), k
+        assert bits_equal(np.float32(got[f"{k}_min"]), want[f"{k}_min"]), k
+    for k in ("normal_particles", "boundary_particles", "inactive_particles"):
+        assert got[k] == want[k], k
+    fluid = out.type == 0
+    nf = int(fluid.sum())
+    u = 2.0 ** -24
+    v = out.velocity.astype(np.float64)
+    speed = np.sqrt((v ** 2).sum(1))
+    terms = {"density_avg": np.abs(out.density[fluid]).sum() / nf, "pressure_avg": np.abs(out.pressure[fluid]).sum() / nf}
+    if dim == 2:
+        m = out.mass[fluid].astype(np.float64)
+        terms.update(velocity_avg=speed[fluid].sum() / nf, kinetic_energy=(0.5 * m * speed[fluid] ** 2).sum(),
+                     potential_energy=np.abs(9.81 * m * (out.position[fluid, 1] - 2.0)).sum())
+    for k, mag in terms.items():
+        bound = (nf - 1) * u * mag + 4 * np.spacing(np.float32(abs(float(want[k]))))
+        assert abs(got[k] - float(want[k])) <= bound, (k, got[k], want[k], bound)
 
 
 def test_global_statistics_quirks():

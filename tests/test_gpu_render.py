@@ -13,11 +13,9 @@ order); they are checked for what holds for every sample: the white sky where
 rays miss, radiance below the sky's where they hit, the normal colours of the
 first hits, the tone mapping, and the same image for the same seed."""
 import numpy as np
-
-from fluidsolver_b200 import tone_map
 import pytest
 
-from fluidsolver_b200 import scenes
+from fluidsolver_b200 import scenes, tone_map
 from fluidsolver_b200.solver import ParticleCollection
 from test_gpu_solvers import make_solver
 

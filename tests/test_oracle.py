@@ -304,3 +304,44 @@ def test_hashed_2d_insertion_order_over_the_2d_dam(ref_oracle, c_oracle):
             differs = True
             break
     assert differs
+
+
+def _stats_collections():
+    """Collections for the global sensors: a moving 2D dam, a 3D dam with
+    inactive particles, all-negative pressures, and one without normal
+    particles."""
+    from fluidsolver_b200 import ParticleCollection
+    rng = np.random.default_rng(31)
+    out = []
+    for dim, n in ((2, 3000), (3, 4000)):
+        pos = rng.uniform(-5, 40, (n, dim)).astype(np.float32)
+        typ = rng.choice(np.array([0, 0, 0, 1, 2], np.uint8), n)
+        out.append(ParticleCollection(position=pos, velocity=rng.normal(0, 3, (n, dim)).astype(np.float32),
+                                      mass=rng.uniform(0.5, 1.5, n).astype(np.float32),
+                                      density=rng.uniform(0.9, 1.1, n).astype(np.float32),
+                                      pressure=rng.uniform(-2, 50, n).astype(np.float32), type=typ))
+    neg = ParticleCollection(position=np.zeros((64, 2), np.float32), velocity=np.zeros((64, 2), np.float32),
+                             mass=np.ones(64, np.float32), density=np.ones(64, np.float32),
+                             pressure=-np.ones(64, np.float32), type=np.zeros(64, np.uint8))
+    none = ParticleCollection(position=np.zeros((16, 2), np.float32), velocity=np.ones((16, 2), np.float32),
+                              mass=np.ones(16, np.float32), density=np.ones(16, np.float32),
+                              pressure=np.ones(16, np.float32), type=np.ones(16, np.uint8))
+    return out + [neg, none]
+
+
+def test_global_sensors_oracle_equals_the_compiled_reference(ref_oracle, c_oracle):
+    """The C restatement of the global sensors (ParticleStatistics.cpp:17-201)
+    against the reference's own sensor classes, bit for bit: maxima starting at
+    FLT_MIN, minima at FLT_MAX, averages and energies as serial float sums in
+    index order, the counts. Velocity and energy in 2D only (the reference's
+    sensors read 2D MovementData)."""
+    for col in _stats_collections():
+        dim = col.position.shape[1]
+        ref = ref_oracle.global_stats(col, 9.81, 1.5)
+        mine = c_oracle.global_stats(col, 9.81, 1.5)
+        keys = ref_oracle.STAT_NAMES if dim == 2 else [k for k in ref_oracle.STAT_NAMES
+                                                       if k.startswith(("density", "pressure"))]
+        for k in keys:
+            assert bits_equal(np.float32(mine[k]), ref[k]), (dim, k, mine[k], ref[k])
+        for k in ("normal_particles", "boundary_particles", "inactive_particles"):
+            assert mine[k] == ref[k], k
