@@ -1435,6 +1435,7 @@ static fs_status create_ctx(const fs_params* p, int32_t scenes, const int64_t* o
         return bail(fail(FS_ERR_CUDA, "cudaMallocHost failed"));
     // the radix sort's per-tile digit counts for the largest sort
     FS_ALLOC(c->sort_hist, (size_t)sort_hist_entries((int64_t)cap));
+    if (prepare_small_sort() != cudaSuccess) return bail(fail(FS_ERR_CUDA, "small-sort shared memory"));
     int K = p->neighbor_capacity > 0 ? p->neighbor_capacity : (p->dim == 2 ? 32 : 64);
     if (contract_capacity(p->search) > 0) K = std::min(K, contract_capacity(p->search) + 1);
     {

@@ -247,10 +247,114 @@ __global__ void k_cell_start_fill(int64_t n_struct, const K* __restrict__ keys, 
     for (int64_t t = from; t <= to; t++) cell_start[t] = (uint32_t)k;
 }
 
+// Small sorts (n <= kSmallSortMax, e.g. a 2D dam of a few thousand
+// particles) in one block and one launch: the same stable passes, with the
+// keys in shared memory between them, so that a scene whose whole step lasts
+// a few microseconds does not pay three launches per digit. 32 warps own 128
+// consecutive keys each; the result lands in buffer 1.
+constexpr int kSmallSortThreads = 1024;
+constexpr int kSmallSortWarps = kSmallSortThreads / 32;
+constexpr int kSmallSortPerLane = 4;
+constexpr int kSmallSortMax = kSmallSortThreads * kSmallSortPerLane;
+template <typename K> constexpr size_t small_sort_smem() {
+    return (size_t)2 * kSmallSortMax * (sizeof(K) + sizeof(uint32_t)) + (size_t)kSmallSortWarps * kSortDigits * 4;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kSmallSortThreads) k_sort_small(int64_t n, int bits, const K* __restrict__ kin,
+                                                                  const uint32_t* __restrict__ vin,
+                                                                  K* __restrict__ kout, uint32_t* __restrict__ vout) {
+    extern __shared__ __align__(16) unsigned char sort_smem[];
+    K* sk[2] = {reinterpret_cast<K*>(sort_smem), reinterpret_cast<K*>(sort_smem) + kSmallSortMax};
+    uint32_t* sv[2] = {reinterpret_cast<uint32_t*>(sk[1] + kSmallSortMax),
+                       reinterpret_cast<uint32_t*>(sk[1] + kSmallSortMax) + kSmallSortMax};
+    uint32_t(*wh)[kSortDigits] = reinterpret_cast<uint32_t(*)[kSortDigits]>(sv[1] + kSmallSortMax);
+    __shared__ uint32_t s_tot[kSortDigits / 32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    for (int i = t; i < n; i += kSmallSortThreads) {
+        sk[0][i] = kin[i];
+        sv[0][i] = vin[i];
+    }
+    int cur = 0;
+    for (int shift = 0; shift < bits; shift += 8) {
+        for (int d = lane; d < kSortDigits; d += 32) wh[w][d] = 0u;
+        __syncthreads();
+        uint32_t rank[kSmallSortPerLane];
+#pragma unroll
+        for (int j = 0; j < kSmallSortPerLane; j++) {
+            const int i = w * (32 * kSmallSortPerLane) + j * 32 + lane;
+            const bool v = i < n;
+            rank[j] = 0u;
+            const unsigned act = __ballot_sync(0xffffffffu, v);
+            if (v) {
+                const uint32_t d = digit_of<K>(sk[cur][i], shift);
+                const unsigned peers = __match_any_sync(act, d);
+                const uint32_t before = wh[w][d];
+                __syncwarp(act);
+                rank[j] = before + (uint32_t)__popc(peers & below);
+                if (lane == __ffs(peers) - 1) wh[w][d] = before + (uint32_t)__popc(peers);
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        // per digit (threads 0..255): its total over the warps, the digits'
+        // exclusive scan, then each warp's first slot
+        uint32_t total = 0u, incl = 0u;
+        if (t < kSortDigits) {
+            for (int q = 0; q < kSmallSortWarps; q++) total += wh[q][t];
+            incl = total;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane == 31) s_tot[w] = incl;
+        }
+        __syncthreads();
+        if (t < kSortDigits) {
+            uint32_t run = incl - total;
+            for (int q = 0; q < w; q++) run += s_tot[q];
+            for (int q = 0; q < kSmallSortWarps; q++) {
+                const uint32_t c = wh[q][t];
+                wh[q][t] = run;
+                run += c;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kSmallSortPerLane; j++) {
+            const int i = w * (32 * kSmallSortPerLane) + j * 32 + lane;
+            if (i < n) {
+                const K key = sk[cur][i];
+                const uint32_t pos = wh[w][digit_of<K>(key, shift)] + rank[j];
+                sk[cur ^ 1][pos] = key;
+                sv[cur ^ 1][pos] = sv[cur][i];
+            }
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+    for (int i = t; i < n; i += kSmallSortThreads) {
+        kout[i] = sk[cur][i];
+        vout[i] = sv[cur][i];
+    }
+}
+
+// the small sort's shared memory, set once per process and device
+inline cudaError_t prepare_small_sort() {
+    cudaError_t e = cudaFuncSetAttribute(k_sort_small<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)small_sort_smem<uint32_t>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sort_small<unsigned long long>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)small_sort_smem<unsigned long long>());
+    return e;
+}
+
 // Sorts n (key, value) pairs over bits [0, bits) with the passes above,
-// ping-ponging between buffers 0 and 1 of keys and vals. Returns the buffer
-// that holds the result. hist holds sort_hist_entries(n) counters (capacity
-// for at least n keys).
+// ping-ponging between buffers 0 and 1 of keys and vals (or, for n <=
+// kSmallSortMax, in one block). Returns the buffer that holds the result.
+// hist holds sort_hist_entries(n) counters (capacity for at least n keys).
 template <typename K>
 inline int sort_pairs(int64_t n, int bits, K* const (&keys)[2], uint32_t* const (&vals)[2], uint32_t* hist,
                       cudaStream_t st, int64_t& launches) {
@@ -258,6 +362,11 @@ inline int sort_pairs(int64_t n, int bits, K* const (&keys)[2], uint32_t* const 
     uint32_t* totals = hist + (int64_t)kSortDigits * tiles;
     int cur = 0;
     if (n <= 1) return cur;
+    if (n <= kSmallSortMax) {
+        k_sort_small<K><<<1, kSmallSortThreads, small_sort_smem<K>(), st>>>(n, bits, keys[0], vals[0], keys[1], vals[1]);
+        launches += 1;
+        return 1;
+    }
     for (int shift = 0; shift < bits; shift += 8) {
         k_sort_hist<K><<<(unsigned)tiles, kSortThreads, 0, st>>>(n, keys[cur], shift, tiles, hist);
         k_sort_rowscan<<<kSortDigits, kSortThreads, 0, st>>>(hist, tiles, totals);
