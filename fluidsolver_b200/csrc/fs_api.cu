@@ -251,7 +251,7 @@ fs_status free_all(fs_ctx* c) {
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc[0], c->acc[1], c->ext[0], c->ext[1],
                     c->rho[0], c->rho[1], c->p[0], c->p[1], c->type[0], c->type[1], c->hidx[0], c->hidx[1],
                     c->rho_prev, c->vstar, c->anp, c->err, c->gbnd, c->tile_desc, c->tile_ent, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
-                    c->perm[0], c->perm[1], c->h2d_cell, c->h2d_rank, c->sort_hist, c->hash_table, c->cell_start, c->bbox, c->grids, c->nbr, c->nbr_count,
+                    c->perm[0], c->perm[1], c->h2d_cell, c->h2d_rank, c->sort_hist, c->hash_table, c->cell_start, c->cell_partials, c->bbox, c->grids, c->nbr, c->nbr_count,
                     c->scene_of[0], c->scene_of[1], c->d_scene_offsets,
                     c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->scalars,
                     c->stats_parts, c->stats_out};
@@ -362,8 +362,10 @@ fs_status ensure_cells(fs_ctx* c) {
     if (!c->cell_start || c->cell_alloc < need) {
         clear_graphs(c);
         if (c->cell_start) cudaFree(c->cell_start);
-        c->cell_start = nullptr;
+        if (c->cell_partials) cudaFree(c->cell_partials);
+        c->cell_start = c->cell_partials = nullptr;
         FS_TRY(dalloc(&c->cell_start, (size_t)3 * need));
+        FS_TRY(dalloc(&c->cell_partials, (size_t)scan_tiles(3 * need)));
         c->cell_alloc = need;
     }
     return FS_OK;
@@ -706,13 +708,12 @@ template <typename R> fs_status search_impl(fs_ctx* c, bool solver_lists) {
     // cell-start table of the concatenated per-region tables, read off the
     // sorted keys (regions are consecutive blocks of the sorted order)
     const int64_t table = (int64_t)c->regions * (c->cells + 1);
-    c->launches++;
     if (single)
-        k_cell_start_fill<unsigned long long><<<grid_for(c->n_struct + 1, pb), pb, 0, st>>>(
-            c->n_struct, c->keys64[res], 32, c->key_bits, c->cells, table, c->cell_start);
+        cell_start_table<unsigned long long>(c->n_struct, c->keys64[res], 32, c->key_bits, c->cells, table,
+                                             c->cell_start, c->cell_partials, pb, st, c->launches);
     else
-        k_cell_start_fill<uint32_t><<<grid_for(c->n_struct + 1, pb), pb, 0, st>>>(
-            c->n_struct, c->keys[res], 0, c->key_bits, c->cells, table, c->cell_start);
+        cell_start_table<uint32_t>(c->n_struct, c->keys[res], 0, c->key_bits, c->cells, table, c->cell_start,
+                                   c->cell_partials, pb, st, c->launches);
     FS_CUDA(cudaGetLastError());
     if (c->h2d_cell) {
         c->launches++;
@@ -1156,7 +1157,7 @@ fs_status fill_stats(fs_ctx* c, fs_step_stats* stats, int st, int entries = 1) {
 // every later kernel (they check the status word); with an automatic
 // capacity the lists are grown and the search is repeated once.
 fs_status search_for_step(fs_ctx* c, float dt) {
-    for (int attempt = 0; attempt < 2; attempt++) {
+    for (int attempt = 0; attempt < 3; attempt++) {
         c->launches++;
         k_step_begin<<<grid_for(c->nsc(), 128), 128, 0, c->stream>>>(c->scalars, c->nsc(), dt, false);
         FS_CUDA(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
@@ -1164,7 +1165,7 @@ fs_status search_for_step(fs_ctx* c, float dt) {
         FS_TRY(search_dispatch(c, c->prm.solver != FS_SOLVER_NONE));
         int st = 0;
         FS_TRY(read_status(c, &st));
-        if (st == FS_ERR_CAPACITY && attempt == 0 && c->prm.neighbor_capacity == 0 &&
+        if (st == FS_ERR_CAPACITY && attempt < 2 && c->prm.neighbor_capacity == 0 &&
             c->prm.solver != FS_SOLVER_NONE) {
             FS_TRY(read_scalars(c));
             int K = 32;

@@ -88,6 +88,7 @@ struct fs_ctx {
     fsb::HashCell* hash_table = nullptr;
     uint32_t hash_mask = 0;           // slots - 1 (a power of two, >= 2 x capacity)
     uint32_t* cell_start = nullptr;   // [regions][cells + 1] first sorted index of cell >= c
+    uint32_t* cell_partials = nullptr;  // tile totals of the cell table's scan
     int64_t cells = 0;                // dims[0] * dims[1] * dims[2]
     int key_bits = 30;                // bits of the linear cell index in the sort keys
     int64_t cell_alloc = 0;           // entries allocated per table

@@ -523,7 +523,10 @@ __global__ void __launch_bounds__(128) k_build_lists(int64_t n_owners, const V4<
                                                      uint32_t* __restrict__ count, int* __restrict__ status,
                                                      StepScalars* __restrict__ sc) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n_owners || *status) return;
+    if (k >= n_owners) return;
+    // an overflow elsewhere does not stop the counting: the largest list decides how far the lists grow
+    const int err = *status;
+    if (err && err != FS_ERR_CAPACITY) return;
     uint32_t c = 0;
     if ((owner_mask >> type[k]) & 1u) c = build_list_one<R>(k, pos, type, cell_start, w, rows, nbr, stride, K);
     count[k] = c;

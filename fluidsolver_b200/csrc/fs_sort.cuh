@@ -228,23 +228,98 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(int64_t n, const 
 }
 
 // Cell-start table from the sorted keys of the particles in the structure
-// ([0, n_struct)): entry t of the concatenated per-region tables (region g,
+// ([0, n_struct)). Entry t of the concatenated per-region tables (region g,
 // cell c at t = g (cells + 1) + c; entry g (cells + 1) + cells ends region
-// g) is the first sorted index whose key's entry is >= t. Thread k fills the
-// entries between its predecessor's key and its own; thread n_struct the
-// rest, so every entry is written exactly once and no scan is needed.
+// g) is the first sorted index whose key's entry is >= t: the exclusive scan
+// of the per-entry counts. k_cell_counts writes, for the first particle of
+// every run of equal keys, the run's length (the table is zeroed before);
+// the scan runs in place.
 template <typename K>
-__global__ void k_cell_start_fill(int64_t n_struct, const K* __restrict__ keys, int key_shift, int key_bits,
-                                  int64_t cells, int64_t table, uint32_t* __restrict__ cell_start) {
+__global__ void k_cell_counts(int64_t n_struct, const K* __restrict__ keys, int key_shift, int key_bits,
+                              int64_t cells, uint32_t* __restrict__ counts) {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k > n_struct) return;
-    auto entry = [&](int64_t q) -> int64_t {
-        const uint32_t key = (uint32_t)(keys[q] >> key_shift);
-        return (int64_t)(key >> key_bits) * (cells + 1) + (key & ((1u << key_bits) - 1u));
-    };
-    const int64_t from = k > 0 ? entry(k - 1) + 1 : 0;
-    const int64_t to = k < n_struct ? entry(k) : table - 1;
-    for (int64_t t = from; t <= to; t++) cell_start[t] = (uint32_t)k;
+    if (k >= n_struct) return;
+    const uint32_t key = (uint32_t)(keys[k] >> key_shift);
+    if (k > 0 && (uint32_t)(keys[k - 1] >> key_shift) == key) return;
+    int64_t e = k + 1;
+    while (e < n_struct && (uint32_t)(keys[e] >> key_shift) == key) e++;
+    counts[(int64_t)(key >> key_bits) * (cells + 1) + (key & ((1u << key_bits) - 1u))] = (uint32_t)(e - k);
+}
+
+// Device-wide exclusive scan of m counts, in place, in three launches:
+// k_scan_tiles scans every tile of kScanTile entries and stores the tile's
+// total, one block scans the totals (k_scan_exclusive), k_scan_add adds each
+// tile's offset.
+constexpr int kScanThreads = 1024;
+constexpr int kScanPerThread = 8;
+constexpr int kScanTile = kScanThreads * kScanPerThread;
+inline int64_t scan_tiles(int64_t m) { return (m + kScanTile - 1) / kScanTile; }
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(uint32_t* __restrict__ a, int64_t m,
+                                                             uint32_t* __restrict__ partials) {
+    __shared__ uint32_t tile[kScanTile];
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int64_t base = blockIdx.x * (int64_t)kScanTile;
+    for (int i = t; i < kScanTile; i += kScanThreads) tile[i] = base + i < m ? a[base + i] : 0u;
+    __syncthreads();
+    uint32_t v[kScanPerThread], sum = 0u;
+#pragma unroll
+    for (int j = 0; j < kScanPerThread; j++) {
+        v[j] = tile[t * kScanPerThread + j];
+        sum += v[j];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        const uint32_t x = s_warp[lane];
+        uint32_t xi = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, xi, o);
+            if (lane >= o) xi += y;
+        }
+        s_warp[lane] = xi - x;
+        if (lane == 31) partials[blockIdx.x] = xi;
+    }
+    __syncthreads();
+    uint32_t run = s_warp[w] + incl - sum;
+#pragma unroll
+    for (int j = 0; j < kScanPerThread; j++) {
+        tile[t * kScanPerThread + j] = run;
+        run += v[j];
+    }
+    __syncthreads();
+    for (int i = t; i < kScanTile; i += kScanThreads)
+        if (base + i < m) a[base + i] = tile[i];
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ a, int64_t m, const uint32_t* __restrict__ partials) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+        a[i] += partials[i / kScanTile];
+}
+
+// the cell-start table of n_struct sorted keys: zero, count, scan in place;
+// partials holds scan_tiles(table) entries
+template <typename K>
+inline void cell_start_table(int64_t n_struct, const K* keys, int key_shift, int key_bits, int64_t cells,
+                             int64_t table, uint32_t* cell_start, uint32_t* partials, int block, cudaStream_t st,
+                             int64_t& launches) {
+    cudaMemsetAsync(cell_start, 0, sizeof(uint32_t) * (size_t)table, st);
+    if (n_struct > 0)
+        k_cell_counts<K><<<(unsigned)((n_struct + block - 1) / block), block, 0, st>>>(n_struct, keys, key_shift,
+                                                                                       key_bits, cells, cell_start);
+    const int64_t tiles = scan_tiles(table);
+    k_scan_tiles<<<(unsigned)tiles, kScanThreads, 0, st>>>(cell_start, table, partials);
+    k_scan_exclusive<uint32_t, uint32_t><<<1, 1024, 0, st>>>(partials, partials, tiles);
+    k_scan_add<<<(unsigned)std::min<int64_t>((table + 255) / 256, 148 * 8), 256, 0, st>>>(cell_start, table, partials);
+    launches += 4;
 }
 
 // Small sorts (n <= kSmallSortMax, e.g. a 2D dam of a few thousand

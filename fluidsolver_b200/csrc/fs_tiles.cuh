@@ -174,7 +174,12 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     uint32_t* s_wlen = s_cnt;                                     // warp sums of the range scan
     uint32_t* s_wne = s_cnt + kTileOwners / 32;
     uint32_t* s_wmax = reinterpret_cast<uint32_t*>(s_lead);       // warp maxima of the list lengths
-    if (*status) return;   // an earlier error (e.g. non-finite positions) ends the step
+    {
+        // an earlier error (e.g. non-finite positions) ends the step; an overflow
+        // elsewhere does not stop the counting (the largest list decides the growth)
+        const int err = *status;
+        if (err && err != FS_ERR_CAPACITY) return;
+    }
 
     const int t = threadIdx.x, lane = t & 31;
     const int64_t tile = blockIdx.x;
