@@ -1,9 +1,10 @@
 """Parity at the benchmark configurations, against the reference's own code.
 
 The reference here is libFluid's hot path compiled from its own sources
-(oracle/_ref, OpenMP variant: the same arithmetic per particle, its loops
-spread over the host cores). Every case runs at the configuration's full
-size:
+(oracle/_ref): the OpenMP variant (the same arithmetic per particle, its
+loops spread over the host cores) for the searches and the 2D dam, the
+serial build for the 3D IISPH dams, whose first loop depends on the loop
+order. Every case runs at the configuration's full size:
 
 * 2D SESPH dam (2,500 fluid + 1,188 boundary, k 1000, nu 0.01, dt 0.001):
   all 1,000 steps in the FP32 reference-order mode, bit for bit, on the
@@ -134,8 +135,12 @@ def test_sesph2d_dam_1000_steps_bit_exact(ref_oracle, search):
 # 3D IISPH dams
 # ---------------------------------------------------------------------------
 def _iisph3d_exact_vs_reference(ref_oracle, col, steps, name):
+    # The reference as built (serial loops): its first loop reads neighbor
+    # densities while it overwrites them (IISPHFluidSolver3D.hpp:60-64 vs
+    # :210), so its result depends on the loop order, which only the serial
+    # build fixes; the OpenMP variant races there once velocities are nonzero.
     ref = ref_oracle.RefSolver("iisph-3d", "hashed-3d", col, (1.0, 9.81, 1.0), IISPH3D_SETTINGS, IISPH3D_GENERATOR,
-                               variant="omp")
+                               variant="serial")
     s = make_solver("iisph-3d", "hashed-3d", IISPH3D_SETTINGS, IISPH3D_GENERATOR, precision="fp32",
                     reference_order=True)
     s.data.collection = col

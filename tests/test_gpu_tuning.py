@@ -81,9 +81,9 @@ def test_tile_cap_keeps_the_sets_and_the_results_to_rounding():
         s = make_solver("iisph-3d", "hashed-3d", SETTINGS_3D, (0.005, 0.4, 0.25))
         s.data.collection = dam()
         s.set_tuning(1, 3, tile_cap=cap)
-        s.step()
+        s.execute_neighborhood_search()
         lists.append(s.solver_lists())
-        for _ in range(2):
+        for _ in range(3):
             s.step()
         runs.append(s.collection())
         s.close()
