@@ -254,6 +254,7 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanPerThread = 8;
 constexpr int kScanTile = kScanThreads * kScanPerThread;
 inline int64_t scan_tiles(int64_t m) { return (m + kScanTile - 1) / kScanTile; }
+constexpr int64_t kSmallScanMax = 65536;   // tables scanned by one block in one launch
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(uint32_t* __restrict__ a, int64_t m,
                                                              uint32_t* __restrict__ partials) {
@@ -315,6 +316,11 @@ inline void cell_start_table(int64_t n_struct, const K* keys, int key_shift, int
     if (n_struct > 0)
         k_cell_counts<K><<<(unsigned)((n_struct + block - 1) / block), block, 0, st>>>(n_struct, keys, key_shift,
                                                                                        key_bits, cells, cell_start);
+    if (table <= kSmallScanMax) {   // small tables: one block, one launch
+        k_scan_exclusive<uint32_t, uint32_t><<<1, 1024, 0, st>>>(cell_start, cell_start, table);
+        launches += 2;
+        return;
+    }
     const int64_t tiles = scan_tiles(table);
     k_scan_tiles<<<(unsigned)tiles, kScanThreads, 0, st>>>(cell_start, table, partials);
     k_scan_exclusive<uint32_t, uint32_t><<<1, 1024, 0, st>>>(partials, partials, tiles);
