@@ -16,9 +16,9 @@
 //                   over the tiles and stores the digit's total;
 //   k_sort_scatter  every tile takes the digits' first slots (a scan of the
 //                   256 totals) plus its row offsets, ranks its keys per digit
-//                   in input order (warps own consecutive 512-key runs and
+//                   in input order (warps own consecutive 128-key runs and
 //                   count with match_any) and writes each pair to its slot.
-// Tiles are 4,096 consecutive keys (8 warps x 32 lanes x 16). Because ranks
+// Tiles are 1,024 consecutive keys (8 warps x 32 lanes x 4). Because ranks
 // follow input order within a tile and the slots follow tile order, every
 // pass is stable, which makes the whole sort stable: keys that compare equal
 // keep their input order. The searches feed it the previous step's sorted
@@ -34,7 +34,7 @@ namespace fsb {
 
 constexpr int kSortWarps = 8;
 constexpr int kSortThreads = 32 * kSortWarps;
-constexpr int kSortPerLane = 16;
+constexpr int kSortPerLane = 4;   // 1,024-key tiles: enough blocks to fill the SMs at a million keys
 constexpr int kSortWarpKeys = 32 * kSortPerLane;            // consecutive keys per warp
 constexpr int kSortTile = kSortWarps * kSortWarpKeys;       // consecutive keys per block
 constexpr int kSortDigits = 256;
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(1024) k_scan_exclusive(const In* in, Out* out,
 // Scatters tile blockIdx.x of (kin, vin) to its slots: slot of a key =
 // (keys of smaller digits, from totals) + offs[d * tiles + tile] (the row
 // scan of k_sort_hist) + keys of digit d before it in the tile. Warp w ranks
-// its own 512 consecutive keys, 32 at a time in lane order, with a per-warp
+// its own 128 consecutive keys, 32 at a time in lane order, with a per-warp
 // counter per digit; then the counters turn into each warp's first slot per
 // digit.
 template <typename K>
