@@ -66,7 +66,7 @@ EXPORTED_SYMBOLS = (
     "fs_query_position_noalloc", "fs_get_solver_lists_csr", "fs_boundary_preprocess", "fs_global_statistics",
     "fs_particles_file_info", "fs_particles_file_read", "fs_particles_file_write", "fs_dump",
     "fs_autotune", "fs_set_tuning", "fs_trace_rays", "fs_render_settings_default", "fs_render",
-    "fs_set_tile_wait_limit", "fs_tone_map",
+    "fs_set_tile_wait_limit", "fs_tone_map", "fs_sort_keys",
 )
 
 
@@ -184,6 +184,7 @@ def lib() -> ctypes.CDLL:
     L.fs_set_tuning.argtypes = [ctx_p, POINTER(FsTuning)]
     L.fs_set_tile_wait_limit.argtypes = [ctx_p, c_int32]
     L.fs_tone_map.argtypes = [c_void_p, c_int64, POINTER(FsRenderSettings), c_void_p]
+    L.fs_sort_keys.argtypes = [c_int32, c_void_p, c_int32, c_int64, c_int32, c_void_p, c_void_p]
     L.fs_global_statistics.argtypes = [ctx_p, c_float, POINTER(FsGlobalStats)]
     L.fs_query_position.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
     L.fs_query_position_noalloc.argtypes = [ctx_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
@@ -202,7 +203,7 @@ def lib() -> ctypes.CDLL:
                  "fs_batch_create", "fs_batch_run", "fs_query_position_noalloc", "fs_get_solver_lists_csr",
                  "fs_boundary_preprocess", "fs_global_statistics", "fs_particles_file_info",
                  "fs_particles_file_read", "fs_particles_file_write", "fs_dump", "fs_autotune", "fs_set_tuning",
-                 "fs_trace_rays", "fs_render", "fs_set_tile_wait_limit", "fs_tone_map"):
+                 "fs_trace_rays", "fs_render", "fs_set_tile_wait_limit", "fs_tone_map", "fs_sort_keys"):
         getattr(L, name).restype = c_int32
     _lib = L
     return L

@@ -2138,6 +2138,75 @@ fs_status fs_set_tile_wait_limit(fs_ctx* c, int32_t tries) {
     return FS_OK;
 }
 
+extern "C++" {
+namespace {
+// the search's sort on caller keys (fs_sort_keys): device buffers for both
+// ping-pong halves, values = input positions, sort_pairs as the search runs it
+template <typename K>
+fs_status sort_keys_impl(int32_t device, const K* keys, int64_t n, int32_t bits, K* sorted, uint32_t* order) {
+    for (int64_t i = 0; i < n; i++)
+        if (bits < (int)(8 * sizeof(K)) && (keys[i] >> bits) != 0)
+            return fail(FS_ERR_INVALID, "key " + std::to_string(i) + " has bits at or above `bits`");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FS_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(FS_ERR_INVALID, "device ordinal out of range");
+    FS_CUDA(cudaSetDevice(device));
+    if (n == 0) return FS_OK;
+    std::vector<uint32_t> iota((size_t)n);
+    for (int64_t i = 0; i < n; i++) iota[(size_t)i] = (uint32_t)i;
+    K* dk = nullptr;
+    uint32_t *dv = nullptr, *hist = nullptr;
+    cudaStream_t st = nullptr;
+    auto release = [&](fs_status s) {
+        cudaFree(dk);
+        cudaFree(dv);
+        cudaFree(hist);
+        if (st) cudaStreamDestroy(st);
+        return s;
+    };
+    if (dalloc(&dk, (size_t)(2 * n)) != FS_OK || dalloc(&dv, (size_t)(2 * n)) != FS_OK ||
+        dalloc(&hist, (size_t)sort_hist_entries(n)) != FS_OK)
+        return release(FS_ERR_CUDA);
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = prepare_small_sort();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dk, keys, sizeof(K) * (size_t)n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dv, iota.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, st);
+    int64_t launches = 0;
+    int res = 0;
+    if (e == cudaSuccess) {
+        K* const kb[2] = {dk, dk + n};
+        uint32_t* const vb[2] = {dv, dv + n};
+        res = sort_pairs<K>(n, bits, kb, vb, hist, st, launches);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && sorted)
+        e = cudaMemcpyAsync(sorted, dk + res * n, sizeof(K) * (size_t)n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && order)
+        e = cudaMemcpyAsync(order, dv + res * n, 4 * (size_t)n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return release(fail(FS_ERR_CUDA, std::string("fs_sort_keys: ") + cudaGetErrorString(e)));
+    return release(FS_OK);
+}
+}  // namespace
+}  // extern "C++"
+
+fs_status fs_sort_keys(int32_t device, const void* keys, int32_t key_bytes, int64_t n, int32_t bits, void* sorted,
+                       uint32_t* order) {
+    if ((!keys && n > 0) || n < 0) return fail(FS_ERR_INVALID, "null keys or negative count");
+    if (n > (int64_t)0xffffffffu) return fail(FS_ERR_INVALID, "more keys than 32-bit positions hold");
+    if (key_bytes == 4) {
+        if (bits < 1 || bits > 32) return fail(FS_ERR_INVALID, "bits must be in 1..32 for 4-byte keys");
+        return sort_keys_impl<uint32_t>(device, static_cast<const uint32_t*>(keys), n, bits,
+                                        static_cast<uint32_t*>(sorted), order);
+    }
+    if (key_bytes == 8) {
+        if (bits < 1 || bits > 64) return fail(FS_ERR_INVALID, "bits must be in 1..64 for 8-byte keys");
+        return sort_keys_impl<unsigned long long>(device, static_cast<const unsigned long long*>(keys), n, bits,
+                                                  static_cast<unsigned long long*>(sorted), order);
+    }
+    return fail(FS_ERR_INVALID, "key_bytes must be 4 or 8");
+}
+
 fs_status fs_set_tuning(fs_ctx* c, const fs_tuning* in) {
     if (!c || !in) return fail(FS_ERR_INVALID, "null argument");
     if (in->first_loop_prefetch < 1 || in->first_loop_prefetch > kMaxAhead || in->pressure_prefetch < 1 ||

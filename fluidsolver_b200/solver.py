@@ -212,6 +212,19 @@ def tone_map(radiance, exposure: float = 0.2, gamma: float = 2.2, filmic: bool =
     return out
 
 
+def sort_keys(keys, bits: int, device: int = 0):
+    """The searches' stable radix sort on keys (uint32 or uint64, each below 2**bits), on the
+    device (fs_sort_keys): (sorted keys, input position of each); equal keys keep input order."""
+    k = np.ascontiguousarray(keys)
+    if k.dtype not in (np.uint32, np.uint64):
+        raise TypeError("keys must be uint32 or uint64")
+    n = k.size
+    out = np.empty_like(k)
+    order = np.empty(n, np.uint32)
+    F.check(F.lib().fs_sort_keys(device, k.ctypes.data, k.itemsize, n, bits, out.ctypes.data, order.ctypes.data))
+    return out, order
+
+
 def _tuning_dict(t) -> dict:
     """fs_tuning as a dict: the values in use and every measured time, keyed by the value tried."""
     return {"tuned": bool(t.tuned), "first_loop_prefetch": t.first_loop_prefetch,

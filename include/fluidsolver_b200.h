@@ -319,6 +319,20 @@ fs_status fs_set_tuning(fs_ctx* ctx, const fs_tuning* in);
  * limit is one per device, shared by every context on the context's device. */
 fs_status fs_set_tile_wait_limit(fs_ctx* ctx, int32_t tries);
 
+/* The searches' own sort on caller keys, for tests of the sort alone: the
+ * stable least-significant-digit radix sort that orders the particles by
+ * (region, cell) key every search (and, in the reference-order mode, by the
+ * 64-bit key with the order inside a cell), run on `device` over n host keys
+ * of key_bytes 4 or 8 bytes. Every key must be below 2^bits (1 <= bits <=
+ * 8 * key_bytes). sorted (n keys, may be null) receives the keys in
+ * ascending order; order (n, may be null) the input position of each, equal
+ * keys in input order. No reference counterpart: the reference sorts its
+ * collection with a quick sort over Morton keys
+ * (ParticleCollectionAlgorithm.hpp:28-133), whose order of equal keys is not
+ * defined. */
+fs_status fs_sort_keys(int32_t device, const void* keys, int32_t key_bytes, int64_t n, int32_t bits, void* sorted,
+                       uint32_t* order);
+
 /* ---- entities and sensors on the device -----------------------------------
  * Host-side entities and sensors of the Simulator read the whole collection;
  * these run their arithmetic where the state lives, so that a step loop that

@@ -6,6 +6,7 @@ import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 from conftest import ROOT, gpu_available
@@ -109,3 +110,29 @@ def test_null_arguments(L):
     assert L.fs_destroy(None) == F.FS_OK
     assert L.fs_upload(None, None) == F.FS_ERR_INVALID
     assert L.fs_step(None, ctypes.c_float(0.0), None) == F.FS_ERR_INVALID
+
+
+def test_sort_keys_validates_its_arguments(L):
+    """fs_sort_keys rejects bad widths and keys at or above 2^bits before it touches a device."""
+    k = np.array([1, 2, 300], np.uint32)
+    out = np.empty_like(k)
+    order = np.empty(3, np.uint32)
+    args = (out.ctypes.data, order.ctypes.data)
+    assert L.fs_sort_keys(0, k.ctypes.data, 2, 3, 16, *args) == F.FS_ERR_INVALID       # key_bytes
+    assert L.fs_sort_keys(0, k.ctypes.data, 4, 3, 0, *args) == F.FS_ERR_INVALID        # bits
+    assert L.fs_sort_keys(0, k.ctypes.data, 4, 3, 33, *args) == F.FS_ERR_INVALID
+    assert L.fs_sort_keys(0, k.ctypes.data, 4, 3, 8, *args) == F.FS_ERR_INVALID        # 300 >= 2^8
+    assert b"bits" in L.fs_last_error()
+    assert L.fs_sort_keys(0, None, 4, 3, 16, *args) == F.FS_ERR_INVALID
+    assert L.fs_sort_keys(0, k.ctypes.data, 4, -1, 16, *args) == F.FS_ERR_INVALID
+    k8 = np.array([1, 2, 1 << 40], np.uint64)
+    assert L.fs_sort_keys(0, k8.ctypes.data, 8, 3, 65, *args) == F.FS_ERR_INVALID
+    assert L.fs_sort_keys(0, k8.ctypes.data, 8, 3, 40, *args) == F.FS_ERR_INVALID      # 2^40 >= 2^40
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-device path")
+def test_sort_keys_without_a_device_fails_loudly(L):
+    k = np.array([3, 1, 2], np.uint32)
+    out = np.empty_like(k)
+    order = np.empty(3, np.uint32)
+    assert L.fs_sort_keys(0, k.ctypes.data, 4, 3, 8, out.ctypes.data, order.ctypes.data) == F.FS_ERR_NO_DEVICE
