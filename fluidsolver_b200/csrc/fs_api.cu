@@ -167,7 +167,6 @@ TileLists tile_lists_of(fs_ctx* c) {
     T.stride = c->tile_stride;
     T.K = c->nbr_capacity;
     T.cap = c->tuning.cap;
-    T.fac = c->tile_fac;
     return T;
 }
 
@@ -251,7 +250,7 @@ void clear_graphs(fs_ctx* c) {
 fs_status free_all(fs_ctx* c) {
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc[0], c->acc[1], c->ext[0], c->ext[1],
                     c->rho[0], c->rho[1], c->p[0], c->p[1], c->type[0], c->type[1], c->hidx[0], c->hidx[1],
-                    c->rho_prev, c->vstar, c->anp, c->err, c->gbnd, c->tile_desc, c->tile_ent, c->tile_fac, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
+                    c->rho_prev, c->vstar, c->anp, c->err, c->gbnd, c->tile_desc, c->tile_ent, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
                     c->perm[0], c->perm[1], c->h2d_cell, c->h2d_rank, c->sort_hist, c->hash_table, c->cell_start, c->cell_partials, c->bbox, c->grids, c->nbr, c->nbr_count,
                     c->scene_of[0], c->scene_of[1], c->d_scene_offsets,
                     c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->scalars,
@@ -288,11 +287,9 @@ fs_status ensure_lists(fs_ctx* c, int K) {
     clear_graphs(c);
     if (c->nbr) cudaFree(c->nbr);
     if (c->tile_ent) cudaFree(c->tile_ent);
-    if (c->tile_fac) cudaFree(c->tile_fac);
     if (c->tile_desc) cudaFree(c->tile_desc);
     c->nbr = nullptr;
     c->tile_ent = nullptr;
-    c->tile_fac = nullptr;
     c->tile_desc = nullptr;
     FS_TRY(dalloc(&c->nbr, (size_t)K * stride));
     if (tiled) {
@@ -300,7 +297,6 @@ fs_status ensure_lists(fs_ctx* c, int K) {
         c->tile_stride = tiles * kTileOwners;
         FS_TRY(dalloc(&c->tile_desc, (size_t)tiles));
         FS_TRY(dalloc(&c->tile_ent, (size_t)(K / 8) * c->tile_stride));
-        FS_TRY(dalloc(&c->tile_fac, (size_t)(K / 8) * c->tile_stride * 2));
         FS_CUDA(cudaFuncSetAttribute(k_build_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)tile_build_smem(K, kTileCapMax)));
         FS_CUDA(set_tile_pass_smem(K));

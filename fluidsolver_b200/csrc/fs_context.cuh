@@ -100,7 +100,6 @@ struct fs_ctx {
     uint32_t* nbr = nullptr;       // solver lists, slot-major: nbr[s * nbr_stride + k]
     fsb::TileDesc* tile_desc = nullptr;  // tile lists (3D IISPH fast path): per tile of owners
     uint4* tile_ent = nullptr;           // [K / 8][tile_stride] octets of 16-bit entries
-    float4* tile_fac = nullptr;          // [K / 8][tile_stride] x 2: the pairs' gradient factors (TileLists::fac)
     int64_t tile_stride = 0;             // owners per octet plane (tiles * kTileOwners)
     uint32_t* nbr_count = nullptr;
     int nbr_capacity = 0;          // K

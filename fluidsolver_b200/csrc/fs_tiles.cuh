@@ -79,13 +79,6 @@ struct TileLists {
     int64_t stride;
     int K;
     int cap;                           // staged candidates per tile the lists were built for
-    // The kernel-gradient factor f of every listed pair (gradW(d) = f d), in
-    // the layout of the entry planes: [K / 8][stride] of 8 floats, the two
-    // halves of an owner's octet as two float4. The first loop writes them
-    // (it evaluates the spline anyway); the pressure passes, which run twice
-    // per iteration on the same positions, read them instead of evaluating
-    // the spline again: the same floats, so the results do not change.
-    float4* fac;
 };
 
 // dynamic shared memory of the list builder and of the passes. A pass
@@ -529,86 +522,6 @@ __device__ __forceinline__ void for_tile_entries(const Src& src, uint32_t cnt, i
     flush();
 }
 
-// for_tile_entries for a walk that also writes the factor planes: f(byte
-// offset, boundary) returns the pair's gradient factor, and the four of this
-// half of every octet go to fac[o * fstride] (float4; fac: the owner's first
-// half-slot, fstride: two per owner of a plane). Slots past the list are 0.
-template <int AHEAD, typename Src, typename F, typename Flush>
-__device__ __forceinline__ void for_tile_entries_store(const Src& src, uint32_t cnt, int K, int half,
-                                                       uint2 (&ahead)[AHEAD], float4* __restrict__ fac,
-                                                       int64_t fstride, F&& f, Flush&& flush) {
-    const uint32_t n = min(cnt & 0xffffu, (uint32_t)K);
-    auto visit = [&](uint32_t v) -> float { return f(v & kEntOffset, (v & kEntBoundary) != 0u); };
-    const uint32_t full = n / 8, octets = (n + 7) / 8;
-    uint32_t o = 0;
-    for (; o < full; o++) {
-        const uint2 cur = ahead[0];
-#pragma unroll
-        for (int d = 0; d + 1 < AHEAD; d++) ahead[d] = ahead[d + 1];
-        if (o + AHEAD < octets) ahead[AHEAD - 1] = src(o + AHEAD, half);
-        float4 fv;
-        fv.x = visit(cur.x & 0xffffu);
-        fv.y = visit(cur.x >> 16);
-        fv.z = visit(cur.y & 0xffffu);
-        fv.w = visit(cur.y >> 16);
-        fac[(int64_t)o * fstride] = fv;
-        if (o & 1u) flush();
-    }
-    const int m = (int)(n - full * 8) - 4 * half;   // this half's entries of the last, partial octet
-    if (o < octets) {
-        const uint2 cur = ahead[0];
-        float4 fv = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (m > 0) fv.x = visit(cur.x & 0xffffu);
-        if (m > 1) fv.y = visit(cur.x >> 16);
-        if (m > 2) fv.z = visit(cur.y & 0xffffu);
-        if (m > 3) fv.w = visit(cur.y >> 16);
-        fac[(int64_t)o * fstride] = fv;
-    }
-    flush();
-}
-
-// for_tile_entries over the fluid entries for a pass that reads the factor
-// planes: f(byte offset, gradient factor) for each; the factors of an octet
-// are loaded one octet ahead of their use.
-template <int AHEAD, typename Src, typename F, typename Flush>
-__device__ __forceinline__ void for_tile_entries_load(const Src& src, uint32_t cnt, int K, int half,
-                                                      uint2 (&ahead)[AHEAD], const float4* __restrict__ fac,
-                                                      int64_t fstride, F&& f, Flush&& flush) {
-    const uint32_t all = min(cnt & 0xffffu, (uint32_t)K);
-    const uint32_t n = min(cnt >> 16, all);
-    const uint32_t full = n / 8, octets = (n + 7) / 8;
-    float4 fnext = octets > 0 ? fac[0] : make_float4(0.f, 0.f, 0.f, 0.f);
-    uint32_t o = 0;
-    for (; o < full; o++) {
-        const uint2 cur = ahead[0];
-#pragma unroll
-        for (int d = 0; d + 1 < AHEAD; d++) ahead[d] = ahead[d + 1];
-        if (o + AHEAD < octets) ahead[AHEAD - 1] = src(o + AHEAD, half);
-        const float4 fv = fnext;
-        if (o + 1 < octets) fnext = fac[(int64_t)(o + 1) * fstride];
-        f(cur.x & 0xffffu, fv.x);
-        f(cur.x >> 16, fv.y);
-        f(cur.y & 0xffffu, fv.z);
-        f(cur.y >> 16, fv.w);
-        if (o & 1u) flush();
-    }
-    const int m = (int)(n - full * 8) - 4 * half;
-    if (m > 0) {
-        const uint2 cur = ahead[0];
-        const float4 fv = fnext;
-        f(cur.x & 0xffffu, fv.x);
-        if (m > 1) f(cur.x >> 16, fv.y);
-        if (m > 2) f(cur.y & 0xffffu, fv.z);
-        if (m > 3) f(cur.y >> 16, fv.w);
-    }
-    flush();
-}
-
-// the factor planes' first half-slot of owner k (half `half`) and their stride
-__device__ __forceinline__ float4* factor_slot(const TileLists& T, int64_t k, int half) {
-    return T.fac + k * 2 + half;
-}
-
 // The first AHEAD octets of owner k's list in the global octet planes, for
 // a pass that walks them from there (GLOBAL), issued before the tile's
 // staging has landed: the entries do not depend on it. h: the tile's header.
@@ -771,7 +684,7 @@ __global__ void __launch_bounds__(kPassThreads, kL1GlobalEntries ? 4 : 3) k_tile
     V3<float> vpart = v3<float>(0.f, 0.f, 0.f);
     float rpart = 0.f;
     const float gb = c.single_layer ? c.gamma1 : 1.f;
-    auto pair = [&](const float4& pj, const float4& vj, float rj, bool bnd) -> float {
+    auto pair = [&](const float4& pj, const float4& vj, float rj, bool bnd) {
         const V3<float> xij = sub3(pk, pj);
         const float r2 = r2_of(xij);
         float w, f;
@@ -781,7 +694,6 @@ __global__ void __launch_bounds__(kPassThreads, kL1GlobalEntries ? 4 : 3) k_tile
             const float cf = __fdividef(pj.w * dot3(sub3(vk, vj), xij), rj * (r2 + c.visc_eps)) * f;
             vpart = fma3(cf, xij, vpart);
         }
-        return f;
     };
     auto flush = [&] {
         visc.add(vpart);
@@ -803,16 +715,14 @@ __global__ void __launch_bounds__(kPassThreads, kL1GlobalEntries ? 4 : 3) k_tile
         const float4* src4[2] = {s.pos, s.vel};
         float4* dst4[2] = {sp, sv};
         const TileSlab slab = slab_at(tile_smem, 36, T.K, T.cap);
-        static_assert(kL1GlobalEntries, "the first loop writes the factor planes while it walks the global entries");
-        stage_tile_async<2, false, false>(stg, d, h, rg, src4, dst4, s.rho_prev, sr, T, slab);
-        const uint32_t cnt = T.count[kk];
+        stage_tile_async<2, false, !kL1GlobalEntries>(stg, d, h, rg, src4, dst4, s.rho_prev, sr, T, slab);
+        const uint32_t cnt = kL1GlobalEntries ? T.count[kk] : 0u;
         uint2 ahead[AHEAD];
-        prefetch_tile_list<true>(T, h, k, half, ahead);
+        prefetch_tile_list<kL1GlobalEntries>(T, h, k, half, ahead);
         if (!stage_tile_wait(stg, status)) return;
         if (valid)
-            for_tile_entries_store<AHEAD>(GlobalEntries{T.ent + k, T.stride}, cnt, T.K, half, ahead,
-                                          factor_slot(T, k, half), 2 * T.stride, [&](uint32_t off, bool bnd) -> float {
-                return pair(at_offset(sp, off), at_offset(sv, off), at_offset(sr, off >> 2), bnd);
+            walk_tile_list<kL1GlobalEntries, false, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool bnd) {
+                pair(at_offset(sp, off), at_offset(sv, off), at_offset(sr, off >> 2), bnd);
             }, flush);
     }
     const V3<float> vs = pair_total(visc);
@@ -938,10 +848,9 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
     const FastSpline S(c.kern);
     Acc3<float, true> pa;
     V3<float> part = v3<float>(0.f, 0.f, 0.f);
-    // fgrad: the pair's gradient factor (the factor planes, or the spline in a fallback tile)
-    auto pair = [&](const float4& pj, float prj, float fgrad) {
+    auto pair = [&](const float4& pj, float prj) {
         const V3<float> xij = sub3(pk, pj);
-        const float coef = pj.w * (prk + prj) * fgrad;
+        const float coef = pj.w * (prk + prj) * S.grad(r2_of(xij));
         part = fma3(-coef, xij, part);
     };
     auto flush = [&] {
@@ -953,27 +862,22 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
     if (h.nranges == kTileFallback) {
         // the owner's 32-bit list, split between its two threads
         if (valid)
-            walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) {
-                const float4 pj = s.pos[j];
-                pair(pj, s.p[j], S.grad(r2_of(sub3(pk, pj))));
-            }, flush);
+            walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.p[j]); }, flush);
     } else {
-        static_assert(kPressureGlobalEntries, "the pressure passes read the factor planes beside the global entries");
         float4* sp = tile_smem;
         float* sa = reinterpret_cast<float*>(tile_smem + T.cap);
         __shared__ TileStage stg;
         const float4* src4[1] = {s.pos};
         float4* dst4[1] = {sp};
         const TileSlab slab = slab_at(tile_smem, 20, T.K, T.cap);
-        stage_tile_async<1, true, false>(stg, d, h, rg, src4, dst4, s.p, sa, T, slab);
-        const uint32_t cnt = T.count[kk];
+        stage_tile_async<1, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, s.p, sa, T, slab);
+        const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
         uint2 ahead[AHEAD];
-        prefetch_tile_list<true>(T, h, k, half, ahead);
+        prefetch_tile_list<kPressureGlobalEntries>(T, h, k, half, ahead);
         if (!stage_tile_wait(stg, status)) return;
         if (valid)
-            for_tile_entries_load<AHEAD>(GlobalEntries{T.ent + k, T.stride}, cnt, T.K, half, ahead,
-                                         factor_slot(T, k, half), 2 * T.stride, [&](uint32_t off, float fg) {
-                pair(at_offset(sp, off), at_offset(sa, off >> 2), fg);
+            walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool) {
+                pair(at_offset(sp, off), at_offset(sa, off >> 2));
             }, flush);
     }
     const V3<float> a = pair_total(pa);
@@ -1011,9 +915,9 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
     const FastSpline S(c.kern);
     Acc<float, true> ap;
     float part = 0.f;
-    auto pair = [&](const float4& pj, const float4& aj, float fgrad) {
+    auto pair = [&](const float4& pj, const float4& aj) {
         const V3<float> xij = sub3(pk, pj);
-        part = __fmaf_rn(pj.w * fgrad, dot3(sub3(ak, aj), xij), part);
+        part = __fmaf_rn(pj.w * S.grad(r2_of(xij)), dot3(sub3(ak, aj), xij), part);
     };
     auto flush = [&] {
         ap.add(part);
@@ -1023,11 +927,7 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
     bool done = true;
     if (h.nranges == kTileFallback) {
         // the owner's 32-bit list, split between its two threads
-        if (valid)
-            walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) {
-                const float4 pj = s.pos[j];
-                pair(pj, s.acc[j], S.grad(r2_of(sub3(pk, pj))));
-            }, flush);
+        if (valid) walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.acc[j]); }, flush);
     } else {
         float4* sp = tile_smem;
         float4* sa = tile_smem + T.cap;
@@ -1035,15 +935,14 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
         const float4* src4[2] = {s.pos, s.acc};
         float4* dst4[2] = {sp, sa};
         const TileSlab slab = slab_at(tile_smem, 32, T.K, T.cap);
-        stage_tile_async<2, true, false>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
-        const uint32_t cnt = T.count[kk];
+        stage_tile_async<2, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
+        const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
         uint2 ahead[AHEAD];
-        prefetch_tile_list<true>(T, h, k, half, ahead);
+        prefetch_tile_list<kPressureGlobalEntries>(T, h, k, half, ahead);
         done = stage_tile_wait(stg, status);
         if (done && valid)
-            for_tile_entries_load<AHEAD>(GlobalEntries{T.ent + k, T.stride}, cnt, T.K, half, ahead,
-                                         factor_slot(T, k, half), 2 * T.stride, [&](uint32_t off, float fg) {
-                pair(at_offset(sp, off), at_offset(sa, off), fg);
+            walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool) {
+                pair(at_offset(sp, off), at_offset(sa, off));
             }, flush);
     }
     if (done) {
