@@ -2,8 +2,10 @@
 
     python -m fluidsolver_b200.build
 
-fluidsolver_b200/lib/libfluidsolver_b200.so is compiled from csrc/fs_api.cu
-(and the host-only particle-file code, csrc/fs_lz4.cpp and csrc/fs_io.cpp) with nvcc (-gencode arch=compute_100a,code=sm_100a). -fmad=false keeps every
+fluidsolver_b200/lib/libfluidsolver_b200.so is compiled from csrc/fs_api.cu and
+csrc/fs_small.cu (the small-scene step kernel, a translation unit of its own
+with coherent loads only), and the host-only particle-file code,
+csrc/fs_lz4.cpp and csrc/fs_io.cpp, with nvcc (-gencode arch=compute_100a,code=sm_100a). -fmad=false keeps every
 float operation separately rounded, which the FP32 precision mode needs to
 reproduce the reference's arithmetic bit for bit.
 """
@@ -18,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libfluidsolver_b200.so")
-SOURCES = ["fs_api.cu", "fs_lz4.cpp", "fs_io.cpp"]
+SOURCES = ["fs_api.cu", "fs_small.cu", "fs_lz4.cpp", "fs_io.cpp"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-fmad=false",
               "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-warn-spills"]
 

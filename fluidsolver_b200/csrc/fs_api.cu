@@ -19,6 +19,7 @@
 #include "fs_entities.cuh"
 #include "fs_io.hpp"
 #include "fs_render.cuh"
+#include "fs_small.cuh"
 
 using namespace fsb;
 
@@ -253,7 +254,7 @@ fs_status free_all(fs_ctx* c) {
                     c->rho_prev, c->vstar, c->anp, c->err, c->gbnd, c->tile_desc, c->tile_ent, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
                     c->perm[0], c->perm[1], c->h2d_cell, c->h2d_rank, c->sort_hist, c->hash_table, c->cell_start, c->cell_partials, c->bbox, c->grids, c->nbr, c->nbr_count,
                     c->scene_of[0], c->scene_of[1], c->d_scene_offsets,
-                    c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->scalars,
+                    c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->loop_ticket, c->small_stamps, c->scalars,
                     c->stats_parts, c->stats_out};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -846,6 +847,9 @@ fs_status begin_solver_phases(fs_ctx* c, float dt, cudaStream_t st) {
 template <typename Body>
 // first_done: the first iteration already ran fused into the preceding
 // phase (its scalars are accumulated); its test runs first, outside the loop.
+// body(stream, handle, set_condition) enqueues one iteration and returns
+// whether its last kernel ran the convergence test itself (LoopCheck);
+// otherwise k_iisph_check follows it.
 fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_test, Body&& body,
                                 bool first_done = false) {
     const int max_it = c->prm.max_iterations;
@@ -873,8 +877,7 @@ fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_t
             if (all_done() != FS_OK) return FS_OK;
         }
         for (int it = first_done ? 1 : 0; it < max_it; it++) {
-            body(st);
-            check(st, 0, false);
+            if (!body(st, cudaGraphConditionalHandle{}, false)) check(st, 0, false);
             if (all_done() != FS_OK) break;
         }
         return FS_OK;
@@ -903,8 +906,7 @@ fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_t
     FS_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
     FS_CUDA(cudaStreamBeginCaptureToGraph(c->body_stream, body_graph, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
-    body(c->body_stream);
-    check(c->body_stream, handle, true);
+    if (!body(c->body_stream, handle, true)) check(c->body_stream, handle, true);
     cudaError_t e = cudaGetLastError();
     cudaError_t e2 = cudaStreamEndCapture(c->body_stream, nullptr);
     if (e != cudaSuccess || e2 != cudaSuccess) return fail(FS_ERR_CUDA, "capture of the pressure loop failed");
@@ -935,15 +937,20 @@ fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 3, st));
     // the second loop also ran the first pressure iteration (fs_tiles.cuh)
-    FS_TRY(enqueue_pressure_loop(c, capture, false, true, [&](cudaStream_t bs) {
+    FS_TRY(enqueue_pressure_loop(c, capture, false, true, [&](cudaStream_t bs, cudaGraphConditionalHandle h,
+                                                              bool set) {
         c->launches += 2;
         const bool slab = !kPressureGlobalEntries;
+        // the update's last block runs the iteration's test (in place of k_iisph_check)
+        const LoopCheck chk{c->loop_ticket, c->scenes, c->prm.min_iterations, c->prm.max_iterations,
+                            c->prm.max_density_error, true, false, h, set};
         FSB_AHEAD_SWITCH(c->tuning.pressure_ahead, k_tile_iisph3d_pressure_acc,
                          <<<tiles, kPassThreads, tile_pass_smem(20, T.K, slab, T.cap), bs>>>(nf, s, T, L, k, c->scalars,
                                                                                        c->status))
         FSB_AHEAD_SWITCH(c->tuning.pressure_ahead, k_tile_iisph3d_pressure_update,
                          <<<tiles, kPassThreads, tile_pass_smem(32, T.K, slab, T.cap), bs>>>(nf, s, T, L, k, c->scalars,
-                                                                                       c->status))
+                                                                                       c->status, chk))
+        return true;
     }, true));
     FS_TRY(mark(c, 4, st));
     c->launches++;
@@ -990,10 +997,11 @@ template <typename R, bool KAHAN> fs_status step_iisph3d(fs_ctx* c, bool capture
     }
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 3, st));
-    FS_TRY(enqueue_pressure_loop(c, capture, false, !fp32, [&](cudaStream_t bs) {
+    FS_TRY(enqueue_pressure_loop(c, capture, false, !fp32, [&](cudaStream_t bs, cudaGraphConditionalHandle, bool) {
         c->launches += 2;
         k_iisph3d_pressure_acc<R, KAHAN><<<grid_for(no), kBlock, 0, bs>>>(no, s, L, k, c->scalars, c->status);
         k_iisph3d_pressure_update<R, KAHAN><<<grid_for(no), kBlock, 0, bs>>>(no, s, L, k, c->scalars, c->status);
+        return false;
     }));
     FS_TRY(mark(c, 4, st));
     c->launches++;
@@ -1098,10 +1106,12 @@ template <typename R, bool KAHAN> fs_status step_iisph2d(fs_ctx* c, bool capture
     k_iisph2d_l2<R, KAHAN><<<grid_for(no), kBlock, 0, st>>>(no, s, L, k, c->scalars, c->status);
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 3, st));
-    FS_TRY(enqueue_pressure_loop(c, capture, true, c->precision != FS_PRECISION_FP32, [&](cudaStream_t bs) {
+    FS_TRY(enqueue_pressure_loop(c, capture, true, c->precision != FS_PRECISION_FP32,
+                                 [&](cudaStream_t bs, cudaGraphConditionalHandle, bool) {
         c->launches += 2;
         k_iisph2d_pressure_acc<R, KAHAN><<<grid_for(no), kBlock, 0, bs>>>(no, s, L, k, c->scalars, c->status);
         k_iisph2d_pressure_update<R, KAHAN><<<grid_for(no), kBlock, 0, bs>>>(no, s, L, k, c->scalars, c->status);
+        return false;
     }));
     FS_TRY(mark(c, 4, st));
     c->launches++;
@@ -1264,6 +1274,7 @@ fs_status solve_after_search(fs_ctx* c, float dt, fs_step_stats* stats) {
         FS_TRY(step_dispatch_any(c, false));
     }
     c->have_lists = false;  // positions moved: the lists belong to the old positions
+    c->small_last = false;
     FS_TRY(read_scalars(c));
     int st = 0;
     FS_TRY(read_status(c, &st));
@@ -1277,17 +1288,127 @@ fs_status solve_after_search(fs_ctx* c, float dt, fs_step_stats* stats) {
 // no host synchronisation in between. The status word is cleared once: after
 // a failure every later step skips its solver phases, leaving the state as
 // the last successful step left it (up to the search's reordering).
+// Whether whole steps of this context run in the small-scene kernel
+// (fs_small.cuh): one scene of at most kSmallMax particles on the per-owner
+// lists, with the dense cell grid.
+bool small_eligible(const fs_ctx* c) {
+    return c->scenes == 0 && c->n > 0 && c->n <= kSmallMax && !tiled_mode(c) && !c->hash_table &&
+           c->prm.solver != FS_SOLVER_NONE && !(c->prm.flags & FS_FLAG_SYNC_EACH_ITERATION) &&
+           (int64_t)c->regions * (c->cells + 1) <= kSmallMaxTable;
+}
+
+template <typename R, bool KAHAN>
+fs_status launch_small(fs_ctx* c, int32_t steps, float dt) {
+    SmallStepArgs<R> a{};
+    a.steps = steps;
+    a.dim = c->dim;
+    a.split = c->reference_order;
+    a.fp32 = c->precision == FS_PRECISION_FP32;
+    a.n = c->n;
+    a.n_struct = c->n_struct;
+    a.n_owners = c->n_owners;
+    a.cur = c->cur;
+    for (int b = 0; b < 2; b++)
+        a.buf[b] = SmallBuffers{c->pos[b], c->vel[b], c->acc[b], c->ext[b], c->rho[b], c->p[b], c->type[b], c->hidx[b]};
+    a.rho_prev = (R*)c->rho_prev;
+    a.vstar = c->vstar;
+    a.anp = c->anp;
+    a.err = c->err;
+    a.gbnd = c->gbnd;
+    a.include_inactive = c->include_inactive;
+    a.single_region = c->reference_order;
+    a.trunc = c->truncate_cells;
+    a.rows = !c->reference_order && c->dim == 3;
+    a.sort_by_host = c->sort_lists_by_host;
+    a.radius = c->search_radius;
+    a.radius2 = c->radius2;
+    a.key_bits = c->key_bits;
+    a.regions = c->regions;
+    a.cells = c->cells;
+    a.grids = c->grids;
+    a.bbox = c->bbox;
+    for (int b = 0; b < 2; b++) {
+        a.keys[b] = c->keys[b];
+        a.keys64[b] = c->reference_order ? c->keys64[b] : nullptr;
+        a.perm[b] = c->perm[b];
+    }
+    a.h2d_cell = c->h2d_cell;
+    a.h2d_rank = c->h2d_rank;
+    a.cell_start = c->cell_start;
+    a.owner_mask = 1u << FS_TYPE_NORMAL;
+    a.nbr = c->nbr;
+    a.count = c->nbr_count;
+    a.stride = c->nbr_stride;
+    a.K = c->nbr_capacity;
+    a.c = consts_of<R>(c);
+    a.sc = c->scalars;
+    a.status = c->status;
+    a.desired_dt = dt;
+    a.dynamic_generator = dynamic_timestep(c);
+    a.particle_size = c->prm.particle_size;
+    a.min_ts = c->prm.min_timestep;
+    a.max_ts = c->prm.max_timestep;
+    a.lambda_v = c->prm.lambda_v;
+    a.lambda_a = c->prm.lambda_a;
+    a.cfl_timestep = cfl_default(c);
+    a.min_it = c->prm.min_iterations;
+    a.max_it = c->prm.max_iterations;
+    a.max_err = c->prm.max_density_error;
+    a.stamps = c->small_stamps;
+    cudaError_t e;
+    switch (c->prm.solver) {
+        case FS_SOLVER_IISPH_3D: e = launch_small_steps<R, KAHAN, kSmallIISPH3D>(a, c->stream); break;
+        case FS_SOLVER_IISPH_2D: e = launch_small_steps<R, KAHAN, kSmallIISPH2D>(a, c->stream); break;
+        default: e = launch_small_steps<R, KAHAN, kSmallSESPH>(a, c->stream); break;
+    }
+    if (e != cudaSuccess) return fail(FS_ERR_CUDA, std::string("small-scene steps: ") + cudaGetErrorString(e));
+    c->launches++;
+    // the buffer rotation the kernel applied, step by step: the search's
+    // reordering, then (IISPH) the density double buffer
+    const bool iisph = c->prm.solver == FS_SOLVER_IISPH_3D || c->prm.solver == FS_SOLVER_IISPH_2D;
+    for (int32_t i = 0; i < steps; i++) {
+        c->cur ^= 1;
+        if (iisph) std::swap(c->rho[c->cur], c->rho_prev);
+    }
+    return FS_OK;
+}
+
+fs_status enqueue_small_steps(fs_ctx* c, int32_t steps, float dt) {
+    if (c->precision == FS_PRECISION_FP64) return launch_small<double, false>(c, steps, dt);
+    if (c->precision == FS_PRECISION_FP32) return launch_small<float, false>(c, steps, dt);
+    return launch_small<float, true>(c, steps, dt);
+}
+
 fs_status enqueue_steps(fs_ctx* c, int32_t steps, float dt) {
     FS_CUDA(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
-    for (int32_t i = 0; i < steps; i++) FS_TRY(solve_graph(c, dt, true));
+    c->small_last = small_eligible(c);
+    if (c->small_last) {
+        if (steps > 0) FS_TRY(enqueue_small_steps(c, steps, dt));
+    } else {
+        for (int32_t i = 0; i < steps; i++) FS_TRY(solve_graph(c, dt, true));
+    }
     c->have_lists = false;
+    return FS_OK;
+}
+
+// the phase times of the last step (search, first loop, second loop,
+// pressure iterations, integration): from the events of the step-by-step
+// path or the small-scene kernel's timestamps
+fs_status read_phase_times(fs_ctx* c) {
+    if (!c->small_last) {
+        for (int i = 0; i < 5; i++) cudaEventElapsedTime(&c->phase_ms[i], c->ev[i], c->ev[i + 1]);
+        return FS_OK;
+    }
+    unsigned long long t[6];
+    FS_CUDA(cudaMemcpy(t, c->small_stamps, sizeof(t), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < 5; i++) c->phase_ms[i] = t[i + 1] >= t[i] ? (float)((double)(t[i + 1] - t[i]) * 1e-6) : 0.f;
     return FS_OK;
 }
 
 fs_status finish_steps(fs_ctx* c, fs_step_stats* stats, int* st) {
     FS_TRY(read_scalars(c));
     FS_TRY(read_status(c, st));
-    for (int i = 0; i < 5; i++) cudaEventElapsedTime(&c->phase_ms[i], c->ev[i], c->ev[i + 1]);
+    FS_TRY(read_phase_times(c));
     fill_stats(c, stats, *st);
     return FS_OK;
 }
@@ -1392,11 +1513,13 @@ static fs_status create_ctx(const fs_params* p, int32_t scenes, const int64_t* o
         return bail(fail(FS_ERR_CUDA, "cudaStreamCreate failed"));
     const size_t cap = (size_t)c->cap;
     const size_t v4 = c->real_size * 4, r1 = c->real_size;
+    // scalar fields that the tile passes stage: readable up to a multiple of 4 entries
+    const size_t cap4 = (cap + 3) & ~(size_t)3;
     for (int b = 0; b < 2; b++) {
         char** fields[] = {(char**)&c->pos[b], (char**)&c->vel[b], (char**)&c->acc[b], (char**)&c->ext[b]};
         for (char** f : fields) FS_ALLOC(*f, cap * v4);
-        FS_ALLOC(*(char**)&c->rho[b], cap * r1);
-        FS_ALLOC(*(char**)&c->p[b], cap * r1);
+        FS_ALLOC(*(char**)&c->rho[b], cap4 * r1);
+        FS_ALLOC(*(char**)&c->p[b], cap4 * r1);
         FS_ALLOC(c->type[b], cap);
         FS_ALLOC(c->hidx[b], cap);
         FS_ALLOC(c->keys[b], cap);
@@ -1413,7 +1536,7 @@ static fs_status create_ctx(const fs_params* p, int32_t scenes, const int64_t* o
         FS_ALLOC(c->h2d_cell, cap);
         FS_ALLOC(c->h2d_rank, cap);
     }
-    FS_ALLOC(*(char**)&c->rho_prev, cap * r1);
+    FS_ALLOC(*(char**)&c->rho_prev, cap4 * r1);
     FS_ALLOC(*(char**)&c->vstar, cap * v4);
     FS_ALLOC(*(char**)&c->anp, cap * v4);
     FS_ALLOC(*(char**)&c->err, cap * r1);
@@ -1422,6 +1545,8 @@ static fs_status create_ctx(const fs_params* p, int32_t scenes, const int64_t* o
     FS_ALLOC(c->bbox, 6 * S);
     FS_ALLOC(c->grids, S);
     FS_ALLOC(c->status, 1);
+    FS_ALLOC(c->loop_ticket, 1);
+    FS_ALLOC(c->small_stamps, 8);
     FS_ALLOC(c->scalars, S);
     if (scenes > 0) {
         FS_ALLOC(c->scene_of[0], cap);
@@ -1446,6 +1571,7 @@ static fs_status create_ctx(const fs_params* p, int32_t scenes, const int64_t* o
     for (auto& e : c->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return bail(fail(FS_ERR_CUDA, "cudaEventCreate failed"));
     if (cudaMemsetAsync(c->status, 0, sizeof(int), c->stream) != cudaSuccess ||
+        cudaMemsetAsync(c->loop_ticket, 0, sizeof(unsigned int), c->stream) != cudaSuccess ||
         cudaStreamSynchronize(c->stream) != cudaSuccess)
         return bail(fail(FS_ERR_CUDA, "initialisation failed"));
 #undef FS_ALLOC
@@ -1714,7 +1840,7 @@ fs_status fs_get_solver_lists_csr(fs_ctx* c, int64_t* offsets, int64_t* indices,
                         cudaSuccess) {
                         msg += ": slot " + std::to_string(idx[q] & 0xffffu) + ", tile " +
                                std::to_string(k / kTileOwners) + " with " + std::to_string(dd.h.nranges) +
-                               " ranges, " + std::to_string(dd.h.staged) + " staged:";
+                               " ranges, " + std::to_string(dd.h.staged & 0xffffu) + " staged:";
                         for (uint32_t r = 0; r < dd.h.nranges && r < (uint32_t)kTileRanges; r++)
                             msg += " [" + std::to_string(dd.start[r]) + "+" +
                                    std::to_string(dd.len_base[r] & kRangeLen) + "@" +

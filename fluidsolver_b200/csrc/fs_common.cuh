@@ -14,6 +14,19 @@
 
 #include "../../include/fluidsolver_b200.h"
 
+// Pointer qualifiers of the search and solver code. FSB_R is __restrict__
+// and FSB_LDG a read-only-cache load, except in a translation unit that
+// defines FSB_COHERENT_LOADS first: there kernels read data that earlier
+// phases of the same kernel wrote (the small-scene step kernel), which the
+// non-coherent read-only path must not serve, so both become plain.
+#ifdef FSB_COHERENT_LOADS
+#define FSB_R
+#define FSB_LDG(p) (*(p))
+#else
+#define FSB_R __restrict__
+#define FSB_LDG(p) __ldg(p)
+#endif
+
 namespace fsb {
 
 // ---------------------------------------------------------------------------

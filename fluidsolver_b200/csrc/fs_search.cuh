@@ -59,9 +59,9 @@ template <typename R> __device__ __forceinline__ int cell_coord(R x, float r, bo
 // scene reduces first and issues one atomic per bound; a mixed block (a scene
 // boundary inside it) issues one per particle.
 template <typename R>
-__global__ void k_bbox(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                       const uint16_t* __restrict__ scene, int scenes, bool include_inactive, float r, bool trunc,
-                       int* __restrict__ bbox) {
+__global__ void k_bbox(int64_t n, const V4<R>* FSB_R pos, const uint8_t* FSB_R type,
+                       const uint16_t* FSB_R scene, int scenes, bool include_inactive, float r, bool trunc,
+                       int* FSB_R bbox) {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
     const int sk = (k < n && scene) ? scene[k] : 0;
@@ -128,9 +128,7 @@ __global__ void k_bbox(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* 
 
 // Grid origin of every scene for this step: the bbox minimum, shifted so that
 // the box is centred in the scene's dims when it is smaller.
-__global__ void k_origin(const int* __restrict__ bbox, SceneGrid* __restrict__ grids, int scenes) {
-    const int sidx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (sidx >= scenes) return;
+__device__ __forceinline__ void grid_origin_at(int sidx, const int* FSB_R bbox, SceneGrid* FSB_R grids, int scenes) {
     SceneGrid& g = grids[sidx];
     const int d[3] = {g.d0, g.d1, g.d2};
     int o[3];
@@ -144,6 +142,11 @@ __global__ void k_origin(const int* __restrict__ bbox, SceneGrid* __restrict__ g
     g.o0 = o[0];
     g.o1 = o[1];
     g.o2 = o[2];
+}
+static __global__ void k_origin(const int* FSB_R bbox, SceneGrid* FSB_R grids, int scenes) {
+    const int sidx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sidx >= scenes) return;
+    grid_origin_at(sidx, bbox, grids, scenes);
 }
 
 // clamped local cell of a cell coordinate; *clamped set when outside the grid
@@ -168,15 +171,13 @@ __device__ __forceinline__ uint32_t region_of(uint8_t t, bool single_region) {
 // one that arrives goes after every stayer, arrivals by ascending index (the
 // reference appends them to the cell's std::list in its i-ascending loop).
 template <typename R>
-__global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                       const uint32_t* __restrict__ hidx, bool include_inactive, bool single_region, float r,
-                       bool trunc, const SceneGrid* __restrict__ grids, const uint16_t* __restrict__ scene,
-                       int key_bits, uint32_t* __restrict__ keys,
-                       unsigned long long* __restrict__ keys64, uint32_t* __restrict__ perm,
-                       int2* __restrict__ h2d_cell, const uint32_t* __restrict__ h2d_rank,
-                       int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n) return;
+__device__ __forceinline__ void keys_at(int64_t k, const V4<R>* FSB_R pos, const uint8_t* FSB_R type,
+                                        const uint32_t* FSB_R hidx, bool include_inactive, bool single_region,
+                                        float r, bool trunc, const SceneGrid* FSB_R grids,
+                                        const uint16_t* FSB_R scene, int key_bits, uint32_t* FSB_R keys,
+                                        unsigned long long* FSB_R keys64, uint32_t* FSB_R perm,
+                                        int2* FSB_R h2d_cell, const uint32_t* FSB_R h2d_rank,
+                                        int* FSB_R status) {
     uint8_t t = type[k];
     uint32_t key;
     uint32_t order = keys64 ? hidx[k] : 0u;
@@ -215,33 +216,52 @@ __global__ void k_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* 
     else keys[k] = key;
     perm[k] = (uint32_t)k;
 }
+template <typename R>
+__global__ void k_keys(int64_t n, const V4<R>* FSB_R pos, const uint8_t* FSB_R type,
+                       const uint32_t* FSB_R hidx, bool include_inactive, bool single_region, float r,
+                       bool trunc, const SceneGrid* FSB_R grids, const uint16_t* FSB_R scene,
+                       int key_bits, uint32_t* FSB_R keys,
+                       unsigned long long* FSB_R keys64, uint32_t* FSB_R perm,
+                       int2* FSB_R h2d_cell, const uint32_t* FSB_R h2d_rank,
+                       int* FSB_R status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    keys_at<R>(k, pos, type, hidx, include_inactive, single_region, r, trunc, grids, scene, key_bits, keys, keys64,
+               perm, h2d_cell, h2d_rank, status);
+}
 
 // The 2D hashed grid's history after a sort (see k_keys): every particle's
 // rank within its cell of the new sorted order, stored by host index. Ranks
 // are relative to the device cell, which may hold several true cells of a
 // clamped grid; within each true cell they order its members as the
 // reference's list does, which is all the walks need.
-__global__ void k_h2d_rank(int64_t n_struct, const unsigned long long* __restrict__ keys64, int64_t cells,
-                           int key_bits, const uint32_t* __restrict__ cell_start, const uint32_t* __restrict__ hidx,
-                           uint32_t* __restrict__ h2d_rank) {
-    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n_struct) return;
-    const uint32_t key = (uint32_t)(keys64[k] >> 32);
+// (key_shift: where the cell key starts in the 64-bit sort key)
+__device__ __forceinline__ void h2d_rank_at(int64_t k, const unsigned long long* FSB_R keys64, int64_t cells,
+                                            int key_bits, const uint32_t* FSB_R cell_start,
+                                            const uint32_t* FSB_R hidx, uint32_t* FSB_R h2d_rank,
+                                            int key_shift = 32) {
+    const uint32_t key = (uint32_t)(keys64[k] >> key_shift);
     const uint32_t first = cell_start[(int64_t)(key >> key_bits) * (cells + 1) + (key & ((1u << key_bits) - 1u))];
     h2d_rank[hidx[k]] = (uint32_t)k - first;
+}
+static __global__ void k_h2d_rank(int64_t n_struct, const unsigned long long* FSB_R keys64, int64_t cells,
+                           int key_bits, const uint32_t* FSB_R cell_start, const uint32_t* FSB_R hidx,
+                           uint32_t* FSB_R h2d_rank) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n_struct) return;
+    h2d_rank_at(k, keys64, cells, key_bits, cell_start, hidx, h2d_rank);
 }
 
 // new[k] = old[perm[k]] for every persistent field
 template <typename R>
-__global__ void k_reorder(int64_t n, const uint32_t* __restrict__ perm, const V4<R>* __restrict__ pos0, V4<R>* __restrict__ pos1,
-                          const V4<R>* __restrict__ vel0, V4<R>* __restrict__ vel1, const V4<R>* __restrict__ acc0,
-                          V4<R>* __restrict__ acc1, const V4<R>* __restrict__ ext0, V4<R>* __restrict__ ext1,
-                          const R* __restrict__ rho0, R* __restrict__ rho1, const R* __restrict__ p0, R* __restrict__ p1,
-                          const uint8_t* __restrict__ t0, uint8_t* __restrict__ t1, const uint32_t* __restrict__ h0,
-                          uint32_t* __restrict__ h1, const uint16_t* __restrict__ sc0, uint16_t* __restrict__ sc1) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    uint32_t s = perm[k];
+__device__ __forceinline__ void reorder_at(int64_t k, const uint32_t* FSB_R perm, const V4<R>* FSB_R pos0,
+                                           V4<R>* FSB_R pos1, const V4<R>* FSB_R vel0, V4<R>* FSB_R vel1,
+                                           const V4<R>* FSB_R acc0, V4<R>* FSB_R acc1, const V4<R>* FSB_R ext0,
+                                           V4<R>* FSB_R ext1, const R* FSB_R rho0, R* FSB_R rho1,
+                                           const R* FSB_R p0, R* FSB_R p1, const uint8_t* FSB_R t0,
+                                           uint8_t* FSB_R t1, const uint32_t* FSB_R h0, uint32_t* FSB_R h1,
+                                           const uint16_t* FSB_R sc0, uint16_t* FSB_R sc1) {
+    const uint32_t s = perm[k];
     pos1[k] = pos0[s];
     vel1[k] = vel0[s];
     acc1[k] = acc0[s];
@@ -251,6 +271,18 @@ __global__ void k_reorder(int64_t n, const uint32_t* __restrict__ perm, const V4
     t1[k] = t0[s];
     h1[k] = h0[s];
     if (sc0) sc1[k] = sc0[s];
+}
+template <typename R>
+__global__ void k_reorder(int64_t n, const uint32_t* FSB_R perm, const V4<R>* FSB_R pos0, V4<R>* FSB_R pos1,
+                          const V4<R>* FSB_R vel0, V4<R>* FSB_R vel1, const V4<R>* FSB_R acc0,
+                          V4<R>* FSB_R acc1, const V4<R>* FSB_R ext0, V4<R>* FSB_R ext1,
+                          const R* FSB_R rho0, R* FSB_R rho1, const R* FSB_R p0, R* FSB_R p1,
+                          const uint8_t* FSB_R t0, uint8_t* FSB_R t1, const uint32_t* FSB_R h0,
+                          uint32_t* FSB_R h1, const uint16_t* FSB_R sc0, uint16_t* FSB_R sc1) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    reorder_at<R>(k, perm, pos0, pos1, vel0, vel1, acc0, acc1, ext0, ext1, rho0, rho1, p0, p1, t0, t1, h0, h1, sc0,
+                  sc1);
 }
 
 // ---------------------------------------------------------------------------
@@ -291,7 +323,7 @@ __device__ __forceinline__ uint32_t compact_hash(uint32_t region, int cx, int cy
             region * 83492791u) & mask;
 }
 // the run of key in the table, or false; at most mask + 1 probes
-__device__ __forceinline__ bool hash_lookup(const HashCell* __restrict__ table, uint32_t mask, uint32_t slot,
+__device__ __forceinline__ bool hash_lookup(const HashCell* FSB_R table, uint32_t mask, uint32_t slot,
                                             unsigned long long key, uint32_t& start, uint32_t& end) {
     for (uint32_t probe = 0; probe <= mask; probe++, slot = (slot + 1) & mask) {
         const unsigned long long k = table[slot].key;
@@ -308,10 +340,10 @@ __device__ __forceinline__ bool hash_lookup(const HashCell* __restrict__ table, 
 // Compact hashing's sort keys (2D): (region, cell x, cell y) of every
 // particle in the structure; excluded inactive particles sort last.
 template <typename R>
-__global__ void k_compact_keys(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
+__global__ void k_compact_keys(int64_t n, const V4<R>* FSB_R pos, const uint8_t* FSB_R type,
                                bool include_inactive, bool single_region, float r,
-                               unsigned long long* __restrict__ keys, uint32_t* __restrict__ perm,
-                               int* __restrict__ status) {
+                               unsigned long long* FSB_R keys, uint32_t* FSB_R perm,
+                               int* FSB_R status) {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     const uint8_t t = type[k];
@@ -333,8 +365,8 @@ __global__ void k_compact_keys(int64_t n, const V4<R>* __restrict__ pos, const u
 // into the cleared table: the run's first particle probes from the cell's
 // hash for a free slot (at most mask + 1 probes; the table has at least
 // twice as many slots as particles, so one is always free).
-__global__ void k_hash_insert(int64_t n_struct, const unsigned long long* __restrict__ keys,
-                              HashCell* __restrict__ table, uint32_t mask) {
+static __global__ void k_hash_insert(int64_t n_struct, const unsigned long long* FSB_R keys,
+                              HashCell* FSB_R table, uint32_t mask) {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n_struct) return;
     const unsigned long long key = keys[k];
@@ -362,8 +394,8 @@ struct WalkParams {
     bool candidates_inactive;  // contract lists inactive neighbors
     bool trunc;                // cells by truncation toward zero (hashed 2D order)
     bool length_test;          // sqrt(dot) <= r instead of dot <= r * r
-    const SceneGrid* __restrict__ grids;  // per scene
-    const uint16_t* __restrict__ scene;   // per particle (null: one scene)
+    const SceneGrid* FSB_R grids;  // per scene
+    const uint16_t* FSB_R scene;   // per particle (null: one scene)
     int64_t cells;  // cells of all scenes; each region's table has cells + 1 entries
     const HashCell* table = nullptr;      // compact hashing (2D): cells by key instead of the dense grid
     uint32_t table_mask = 0;
@@ -386,8 +418,8 @@ template <typename R> __device__ __forceinline__ bool within(V3<R> d, const Walk
 // (cells dx, dy, dz ascending with dx outermost; within a cell, sorted order).
 // f(j, type_j) is called for every neighbor j.
 template <typename R, typename F>
-__device__ __forceinline__ void walk_cells(V3<R> xi, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                                           const uint32_t* __restrict__ cell_start, const SceneGrid& gr,
+__device__ __forceinline__ void walk_cells(V3<R> xi, const V4<R>* FSB_R pos, const uint8_t* FSB_R type,
+                                           const uint32_t* FSB_R cell_start, const SceneGrid& gr,
                                            const WalkParams& w, F&& f) {
     const int ci[3] = {cell_coord<R>(xi.x, w.r, w.trunc), cell_coord<R>(xi.y, w.r, w.trunc), cell_coord<R>(xi.z, w.r, w.trunc)};
     if (w.table) {
@@ -446,7 +478,7 @@ __device__ __forceinline__ void walk_cells(V3<R> xi, const V4<R>* __restrict__ p
 // (and visits nothing) for particles in or next to the grid border, which
 // take walk_cells instead.
 template <typename R, typename F>
-__device__ __forceinline__ bool walk_rows(V3<R> xi, const V4<R>* __restrict__ pos, const uint32_t* __restrict__ cell_start,
+__device__ __forceinline__ bool walk_rows(V3<R> xi, const V4<R>* FSB_R pos, const uint32_t* FSB_R cell_start,
                                           const SceneGrid& gr, const WalkParams& w, F&& f) {
     const int lx = cell_coord<R>(xi.x, w.r, false) - gr.o0;
     const int ly = cell_coord<R>(xi.y, w.r, false) - gr.o1;
@@ -476,11 +508,11 @@ __device__ __forceinline__ bool walk_rows(V3<R> xi, const V4<R>* __restrict__ po
 // returns the neighbor count. rows: the 9-row walk where the owner is away
 // from the grid border (list order then differs from the reference's).
 template <typename R>
-__device__ __forceinline__ uint32_t build_list_one(int64_t k, const V4<R>* __restrict__ pos,
-                                                   const uint8_t* __restrict__ type,
-                                                   const uint32_t* __restrict__ cell_start,
+__device__ __forceinline__ uint32_t build_list_one(int64_t k, const V4<R>* FSB_R pos,
+                                                   const uint8_t* FSB_R type,
+                                                   const uint32_t* FSB_R cell_start,
                                                    const WalkParams& w, bool rows,
-                                                   uint32_t* __restrict__ nbr, int64_t stride, int K) {
+                                                   uint32_t* FSB_R nbr, int64_t stride, int K) {
     uint32_t c = 0;
     const V3<R> xi = xyz<R>(pos[k]);
     const SceneGrid gr = w.grid_of(k);
@@ -503,43 +535,51 @@ __device__ __forceinline__ uint32_t build_list_one(int64_t k, const V4<R>* __res
 }
 
 // capacity status and the warp-aggregated maximum of a list length
-__device__ __forceinline__ void note_list_length(uint32_t c, int K, int* __restrict__ status,
-                                                 StepScalars* __restrict__ sc) {
+__device__ __forceinline__ void note_list_length(uint32_t c, int K, int* FSB_R status,
+                                                 StepScalars* FSB_R sc) {
     if ((int)c > K) raise_status(status, FS_ERR_CAPACITY);
-    unsigned mx = c;
-    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(__activemask(), mx, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(&sc->max_neighbors, (int)mx);
+    // the maximum over the warp's active lanes (a partial warp at the end of
+    // the owners, or of a block-stride loop), issued by its first active lane
+    const unsigned act = __activemask();
+    const unsigned mx = __reduce_max_sync(act, c);
+    if ((threadIdx.x & 31) == __ffs(act) - 1) atomicMax(&sc->max_neighbors, (int)mx);
 }
 
 // Solver lists: for owner k in [0, n_owners) with an owner type accepted by
 // owner_mask (bit per particle type), write up to K entries slot-major. The
 // entry is the sorted index, with kBoundaryBit for boundary neighbors.
 template <typename R>
-__global__ void __launch_bounds__(128) k_build_lists(int64_t n_owners, const V4<R>* __restrict__ pos,
-                                                     const uint8_t* __restrict__ type,
-                                                     const uint32_t* __restrict__ cell_start,
-                                                     WalkParams w, uint32_t owner_mask,
-                                                     bool rows, uint32_t* __restrict__ nbr, int64_t stride, int K,
-                                                     uint32_t* __restrict__ count, int* __restrict__ status,
-                                                     StepScalars* __restrict__ sc) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n_owners) return;
-    // an overflow elsewhere does not stop the counting: the largest list decides how far the lists grow
-    const int err = *status;
-    if (err && err != FS_ERR_CAPACITY) return;
+__device__ __forceinline__ void list_owner_at(int64_t k, const V4<R>* FSB_R pos, const uint8_t* FSB_R type,
+                                              const uint32_t* FSB_R cell_start, const WalkParams& w,
+                                              uint32_t owner_mask, bool rows, uint32_t* FSB_R nbr, int64_t stride,
+                                              int K, uint32_t* FSB_R count, int* FSB_R status,
+                                              StepScalars* FSB_R sc) {
     uint32_t c = 0;
     if ((owner_mask >> type[k]) & 1u) c = build_list_one<R>(k, pos, type, cell_start, w, rows, nbr, stride, K);
     count[k] = c;
     note_list_length(c, K, status, sc);
 }
+template <typename R>
+__global__ void __launch_bounds__(128) k_build_lists(int64_t n_owners, const V4<R>* FSB_R pos,
+                                                     const uint8_t* FSB_R type,
+                                                     const uint32_t* FSB_R cell_start,
+                                                     WalkParams w, uint32_t owner_mask,
+                                                     bool rows, uint32_t* FSB_R nbr, int64_t stride, int K,
+                                                     uint32_t* FSB_R count, int* FSB_R status,
+                                                     StepScalars* FSB_R sc) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n_owners) return;
+    // an overflow elsewhere does not stop the counting: the largest list decides how far the lists grow
+    const int err = *status;
+    if (err && err != FS_ERR_CAPACITY) return;
+    list_owner_at<R>(k, pos, type, cell_start, w, owner_mask, rows, nbr, stride, K, count, status, sc);
+}
 
 // Quadratic searches list neighbors by ascending index
 // (QuadraticNeighborhoodSearch3D.cpp:52-66); with the reference's summation
 // order requested, each solver list is sorted by host index.
-__global__ void k_sort_lists_by_host(int64_t n_owners, uint32_t* __restrict__ nbr, int64_t stride, int K,
-                                     const uint32_t* __restrict__ count, const uint32_t* __restrict__ hidx) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n_owners) return;
+__device__ __forceinline__ void sort_list_by_host_at(int64_t k, uint32_t* FSB_R nbr, int64_t stride, int K,
+                                                     const uint32_t* FSB_R count, const uint32_t* FSB_R hidx) {
     const int c = min((int)count[k], K);
     for (int a = 1; a < c; a++) {
         const uint32_t e = nbr[(int64_t)a * stride + k];
@@ -554,12 +594,18 @@ __global__ void k_sort_lists_by_host(int64_t n_owners, uint32_t* __restrict__ nb
         nbr[(int64_t)(b + 1) * stride + k] = e;
     }
 }
+static __global__ void k_sort_lists_by_host(int64_t n_owners, uint32_t* FSB_R nbr, int64_t stride, int K,
+                                     const uint32_t* FSB_R count, const uint32_t* FSB_R hidx) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n_owners) return;
+    sort_list_by_host_at(k, nbr, stride, K, count, hidx);
+}
 
 // CSR export: counts (pass 1) and fill (pass 2) in sorted index space
 template <typename R>
-__global__ void k_csr_count(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                            const uint32_t* __restrict__ cell_start, WalkParams w,
-                            uint32_t owner_mask, uint32_t* __restrict__ count) {
+__global__ void k_csr_count(int64_t n, const V4<R>* FSB_R pos, const uint8_t* FSB_R type,
+                            const uint32_t* FSB_R cell_start, WalkParams w,
+                            uint32_t owner_mask, uint32_t* FSB_R count) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     uint32_t c = 0;
@@ -569,9 +615,9 @@ __global__ void k_csr_count(int64_t n, const V4<R>* __restrict__ pos, const uint
 }
 
 template <typename R>
-__global__ void k_csr_fill(int64_t n, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                           const uint32_t* __restrict__ cell_start, WalkParams w,
-                           uint32_t owner_mask, const int64_t* __restrict__ offsets, uint32_t* __restrict__ out) {
+__global__ void k_csr_fill(int64_t n, const V4<R>* FSB_R pos, const uint8_t* FSB_R type,
+                           const uint32_t* FSB_R cell_start, WalkParams w,
+                           uint32_t owner_mask, const int64_t* FSB_R offsets, uint32_t* FSB_R out) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
     if (!((owner_mask >> type[k]) & 1u)) return;
@@ -588,10 +634,10 @@ __global__ void k_csr_fill(int64_t n, const V4<R>* __restrict__ pos, const uint8
 // tested. Members are the cell's non-inactive particles
 // (HashedNeighborhoodSearch3D.cpp:90-101); the index is the host index.
 template <typename R>
-__global__ void k_query_position(V3<R> x, const V4<R>* __restrict__ pos, const uint8_t* __restrict__ type,
-                                 const uint32_t* __restrict__ hidx, const uint32_t* __restrict__ cell_start,
+__global__ void k_query_position(V3<R> x, const V4<R>* FSB_R pos, const uint8_t* FSB_R type,
+                                 const uint32_t* FSB_R hidx, const uint32_t* FSB_R cell_start,
                                  WalkParams w, bool skip_cell_min,
-                                 uint32_t* __restrict__ out, int64_t cap, unsigned long long* __restrict__ count) {
+                                 uint32_t* FSB_R out, int64_t cap, unsigned long long* FSB_R count) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     unsigned long long c = 0;
     const int ci[3] = {cell_coord<R>(x.x, w.r, w.trunc), cell_coord<R>(x.y, w.r, w.trunc), cell_coord<R>(x.z, w.r, w.trunc)};
@@ -643,8 +689,8 @@ __global__ void k_query_position(V3<R> x, const V4<R>* __restrict__ pos, const u
 // QuadraticNeighborhoodSearchDynamicAllocated.cpp:190-225); unordered, the
 // host sorts. count must be zero before the launch.
 template <typename R>
-__global__ void k_query_all(V3<R> x, int64_t n, const V4<R>* __restrict__ pos, WalkParams w,
-                            uint32_t* __restrict__ out, int64_t cap, unsigned long long* __restrict__ count) {
+__global__ void k_query_all(V3<R> x, int64_t n, const V4<R>* FSB_R pos, WalkParams w,
+                            uint32_t* FSB_R out, int64_t cap, unsigned long long* FSB_R count) {
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
         if (!within<R>(x - xyz<R>(pos[j]), w)) continue;
         const unsigned long long slot = atomicAdd(count, 1ull);

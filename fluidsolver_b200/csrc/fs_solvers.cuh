@@ -29,8 +29,8 @@ template <typename R> struct SolverConsts {
 };
 
 struct Lists {
-    const uint32_t* __restrict__ nbr;
-    const uint32_t* __restrict__ count;
+    const uint32_t* FSB_R nbr;
+    const uint32_t* FSB_R count;
     int64_t stride;
     int K;
     __device__ __forceinline__ uint32_t size(int64_t k) const { return min(count[k], (uint32_t)K); }
@@ -44,28 +44,28 @@ struct Lists {
 // order) is unchanged.
 constexpr int kBatch = 4;
 template <typename R, typename F>
-__device__ __forceinline__ void for_neighbors(const Lists& L, int64_t k, const V4<R>* __restrict__ pos, F&& f) {
+__device__ __forceinline__ void for_neighbors(const Lists& L, int64_t k, const V4<R>* FSB_R pos, F&& f) {
     const uint32_t n = L.size(k);
     uint32_t q = 0;
     for (; q + kBatch <= n; q += kBatch) {
         uint32_t e[kBatch];
         V4<R> p[kBatch];
 #pragma unroll
-        for (int b = 0; b < kBatch; b++) e[b] = __ldg(&L.nbr[(int64_t)(q + b) * L.stride + k]);
+        for (int b = 0; b < kBatch; b++) e[b] = FSB_LDG(&L.nbr[(int64_t)(q + b) * L.stride + k]);
 #pragma unroll
         for (int b = 0; b < kBatch; b++) p[b] = pos[e[b] & kIndexMask];
 #pragma unroll
         for (int b = 0; b < kBatch; b++) f(e[b], p[b]);
     }
     for (; q < n; q++) {
-        const uint32_t e = __ldg(&L.nbr[(int64_t)q * L.stride + k]);
+        const uint32_t e = FSB_LDG(&L.nbr[(int64_t)q * L.stride + k]);
         f(e, pos[e & kIndexMask]);
     }
 }
 
 // As for_neighbors, also handing d = x_k - x_j and gradW(d).
 template <typename R, bool FAST, typename F>
-__device__ __forceinline__ void for_neighbors_grad(const Lists& L, int64_t k, const V4<R>* __restrict__ pos, V3<R> xk,
+__device__ __forceinline__ void for_neighbors_grad(const Lists& L, int64_t k, const V4<R>* FSB_R pos, V3<R> xk,
                                                    const SplineKernel<R>& kern, F&& f) {
     for_neighbors<R>(L, k, pos, [&](uint32_t e, const V4<R>& pj) {
         const V3<R> d = xk - xyz<R>(pj);
@@ -74,20 +74,20 @@ __device__ __forceinline__ void for_neighbors_grad(const Lists& L, int64_t k, co
 }
 
 template <typename R> struct State {
-    V4<R>* __restrict__ pos;
-    V4<R>* __restrict__ vel;
-    V4<R>* __restrict__ acc;
-    V4<R>* __restrict__ ext;
-    R* __restrict__ rho;       // density of this step (written by the density phase)
-    R* __restrict__ rho_prev;  // density read by the viscosity term
-    R* __restrict__ p;
-    V4<R>* __restrict__ vstar; // w: source term
-    V4<R>* __restrict__ anp;   // w: diagonal element
-    R* __restrict__ err;
-    V4<R>* __restrict__ gbnd;  // sum over boundary neighbors of m_j gradW, from the second loop (tile passes)
-    const uint8_t* __restrict__ type;
-    const uint32_t* __restrict__ hidx;
-    const uint16_t* __restrict__ scene;  // per-particle scene (batched contexts), else null
+    V4<R>* FSB_R pos;
+    V4<R>* FSB_R vel;
+    V4<R>* FSB_R acc;
+    V4<R>* FSB_R ext;
+    R* FSB_R rho;       // density of this step (written by the density phase)
+    R* FSB_R rho_prev;  // density read by the viscosity term
+    R* FSB_R p;
+    V4<R>* FSB_R vstar; // w: source term
+    V4<R>* FSB_R anp;   // w: diagonal element
+    R* FSB_R err;
+    V4<R>* FSB_R gbnd;  // xyz: sum over boundary neighbors of m_j gradW, w: diagonal a_ii (second loop, tile passes)
+    const uint8_t* FSB_R type;
+    const uint32_t* FSB_R hidx;
+    const uint16_t* FSB_R scene;  // per-particle scene (batched contexts), else null
     __device__ __forceinline__ int scene_of(int64_t k) const { return scene ? scene[k] : 0; }
 };
 
@@ -194,8 +194,8 @@ __device__ __forceinline__ void iisph3d_l1_one(int64_t k, const State<R>& s, con
 }
 
 template <typename R, bool KAHAN, bool SPLIT>
-__global__ void k_iisph3d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* __restrict__ sc,
-                             const int* __restrict__ status) {
+__global__ void k_iisph3d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* FSB_R sc,
+                             const int* FSB_R status) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n || *status) return;
     iisph3d_l1_one<R, KAHAN, SPLIT>(k, s, L, c, (R)sc->dt);
@@ -203,9 +203,8 @@ __global__ void k_iisph3d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
 
 // density only (IISPHFluidSolver3D.hpp:184-210), for the split first loop
 template <typename R, bool KAHAN>
-__global__ void k_iisph3d_density(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || *status) return;
+__device__ __forceinline__ void iisph3d_density_at(int64_t k, const State<R>& s, const Lists& L,
+                                                   const SolverConsts<R>& c) {
     const uint8_t t = s.type[k];
     if (t != FS_TYPE_NORMAL) {
         s.rho[k] = s.rho_prev[k];
@@ -222,6 +221,12 @@ __global__ void k_iisph3d_density(int64_t n, State<R> s, Lists L, SolverConsts<R
         rho.add(m * c.kern.template w<KAHAN>(xk - xyz<R>(pj)));
     }
     s.rho[k] = rho.get();
+}
+template <typename R, bool KAHAN>
+__global__ void k_iisph3d_density(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* FSB_R status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    iisph3d_density_at<R, KAHAN>(k, s, L, c);
 }
 
 // ===========================================================================
@@ -281,8 +286,8 @@ __device__ __forceinline__ void iisph3d_l2_one(int64_t k, const State<R>& s, con
 }
 
 template <typename R, bool KAHAN, bool TWO_PASS>
-__global__ void k_iisph3d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* __restrict__ sc,
-                             const int* __restrict__ status) {
+__global__ void k_iisph3d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* FSB_R sc,
+                             const int* FSB_R status) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n || *status) return;
     if (s.type[k] != FS_TYPE_NORMAL) return;
@@ -319,7 +324,7 @@ __device__ __forceinline__ void iisph3d_pressure_acc_one(int64_t k, const State<
 
 template <typename R, bool KAHAN>
 __global__ void k_iisph3d_pressure_acc(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
-                                       const StepScalars* __restrict__ sc, const int* __restrict__ status) {
+                                       const StepScalars* FSB_R sc, const int* FSB_R status) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n || *status || sc->done) return;
     if (s.type[k] != FS_TYPE_NORMAL) return;
@@ -383,7 +388,7 @@ __device__ __forceinline__ ErrPart iisph3d_pressure_update_one(int64_t k, const 
 }
 
 // adds one thread's ErrPart to its scene's scalars
-__device__ __forceinline__ void add_err_part(const ErrPart& o, StepScalars* __restrict__ q) {
+__device__ __forceinline__ void add_err_part(const ErrPart& o, StepScalars* FSB_R q) {
     if (o.e_cnt) {
         atomicAdd(&q->err_sum, o.e_sum);
         atomicAdd(&q->err_count, (unsigned long long)o.e_cnt);
@@ -410,13 +415,14 @@ __device__ __forceinline__ ErrPart iisph3d_first_iteration(int64_t k, const Stat
 // thread of the block calls it. scene: the scene of the thread's particle.
 // A block whose threads all belong to one scene reduces first; a block that
 // spans scenes adds thread by thread.
-__device__ __forceinline__ void reduce_err_parts(ErrPart o, StepScalars* __restrict__ sc, int scene = 0) {
+__device__ __forceinline__ void reduce_err_parts(ErrPart o, StepScalars* FSB_R sc, int scene = 0) {
     __shared__ int s_scene;
     if (threadIdx.x == 0) s_scene = scene;
     __syncthreads();
     const int s0 = s_scene;
     if (!__syncthreads_and(scene == s0)) {
         add_err_part(o, sc + scene);
+        __threadfence();   // before a ticket taken after this reduction (iisph_end_of_iteration)
         return;
     }
     sc += s0;
@@ -458,7 +464,7 @@ __device__ __forceinline__ void reduce_err_parts(ErrPart o, StepScalars* __restr
 
 template <typename R, bool KAHAN>
 __global__ void k_iisph3d_pressure_update(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
-                                          StepScalars* __restrict__ sc, const int* __restrict__ status) {
+                                          StepScalars* FSB_R sc, const int* FSB_R status) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (*status || sc->done) return;
     ErrPart o;
@@ -477,11 +483,15 @@ __global__ void k_iisph3d_pressure_update(int64_t n, State<R> s, Lists L, Solver
 // or the residual say.
 // One scene's test after an iteration; returns whether its loop is done and
 // resets the iteration's accumulators.
-__device__ __forceinline__ bool check_scene(StepScalars* __restrict__ sc, int min_it, int max_it, float max_err,
+// The accumulators are read through volatile loads: when the test runs in
+// the last block of the iteration's own update kernel (iisph_end_of_iteration),
+// the other blocks' atomics reached L2 after this SM may have cached the line.
+__device__ __forceinline__ bool check_scene(StepScalars* FSB_R sc, int min_it, int max_it, float max_err,
                                             bool fp64_test, bool two_d) {
-    const int it = sc->iteration;  // iterations completed before this one
-    const unsigned long long cnt = sc->err_count;
-    const double sum = sc->err_sum;
+    const volatile StepScalars* v = sc;
+    const int it = v->iteration;  // iterations completed before this one
+    const unsigned long long cnt = v->err_count;
+    const double sum = v->err_sum;
     float avg = 0.f;
     double avg64 = 0.0;
     if (cnt > 0) {
@@ -490,9 +500,9 @@ __device__ __forceinline__ bool check_scene(StepScalars* __restrict__ sc, int mi
     }
     sc->avg_err = avg;
     sc->avg_err64 = avg64;
-    sc->max_err = __uint_as_float(sc->max_err_bits);
-    sc->final_max_a2 = __uint_as_float(sc->max_a2_bits);
-    sc->final_max_v2 = __uint_as_float(sc->max_v2_bits);
+    sc->max_err = __uint_as_float(v->max_err_bits);
+    sc->final_max_a2 = __uint_as_float(v->max_a2_bits);
+    sc->final_max_v2 = __uint_as_float(v->max_v2_bits);
     const int done_it = it + 1;
     sc->iteration = done_it;
     bool done = false;
@@ -517,12 +527,13 @@ __device__ __forceinline__ bool check_scene(StepScalars* __restrict__ sc, int mi
     return done;
 }
 
-__global__ void k_iisph_check(StepScalars* __restrict__ sc, int min_it, int max_it, float max_err, bool fp64_test,
-                              bool two_d, const int* __restrict__ status, cudaGraphConditionalHandle handle,
-                              bool set_condition) {
+// The test of a single-scene context (one thread).
+__device__ __forceinline__ void iisph_check_one(StepScalars* FSB_R sc, int min_it, int max_it, float max_err,
+                                                bool fp64_test, bool two_d, const int* FSB_R status,
+                                                cudaGraphConditionalHandle handle, bool set_condition) {
     const int guard = ++sc->loop_guard;
     bool stop = guard >= max_it;
-    if (*status || sc->done) {
+    if (*(const volatile int*)status || sc->done) {
         if (set_condition) cudaGraphSetConditional(handle, 0u);
         return;
     }
@@ -531,15 +542,16 @@ __global__ void k_iisph_check(StepScalars* __restrict__ sc, int min_it, int max_
 }
 
 // Batched contexts: every scene still iterating is tested on its own (the
-// 3D test, FP64 average); the loop goes on while any scene iterates. One
-// block; the guard in scene 0 counts executions of the loop body.
-__global__ void k_iisph_check_scenes(StepScalars* __restrict__ sc, int scenes, int min_it, int max_it, float max_err,
-                                     const int* __restrict__ status, cudaGraphConditionalHandle handle,
-                                     bool set_condition) {
+// 3D test, FP64 average); the loop goes on while any scene iterates. Every
+// thread of one block calls it; the guard in scene 0 counts executions of
+// the loop body.
+__device__ __forceinline__ void iisph_check_scenes_block(StepScalars* FSB_R sc, int scenes, int min_it,
+                                                         int max_it, float max_err, const int* FSB_R status,
+                                                         cudaGraphConditionalHandle handle, bool set_condition) {
     __shared__ int s_guard;
     if (threadIdx.x == 0) s_guard = ++sc[0].loop_guard;
     __syncthreads();
-    const bool stop_all = s_guard >= max_it || *status != 0;
+    const bool stop_all = s_guard >= max_it || *(const volatile int*)status != 0;
     int active = 0;
     for (int i = threadIdx.x; i < scenes; i += blockDim.x) {
         StepScalars* q = sc + i;
@@ -552,12 +564,62 @@ __global__ void k_iisph_check_scenes(StepScalars* __restrict__ sc, int scenes, i
     if (threadIdx.x == 0 && set_condition) cudaGraphSetConditional(handle, any ? 1u : 0u);
 }
 
+static __global__ void k_iisph_check(StepScalars* FSB_R sc, int min_it, int max_it, float max_err, bool fp64_test,
+                              bool two_d, const int* FSB_R status, cudaGraphConditionalHandle handle,
+                              bool set_condition) {
+    iisph_check_one(sc, min_it, max_it, max_err, fp64_test, two_d, status, handle, set_condition);
+}
+
+static __global__ void k_iisph_check_scenes(StepScalars* FSB_R sc, int scenes, int min_it, int max_it, float max_err,
+                                     const int* FSB_R status, cudaGraphConditionalHandle handle,
+                                     bool set_condition) {
+    iisph_check_scenes_block(sc, scenes, min_it, max_it, max_err, status, handle, set_condition);
+}
+
+// The convergence test folded into the last block of an iteration's update
+// kernel, in place of a k_iisph_check launch: every block takes a ticket
+// after its contributions to the scalars; the block that takes the last one
+// (all others' atomics are then in L2) resets the ticket and runs the test.
+struct LoopCheck {
+    unsigned int* ticket;              // zero between launches
+    int scenes;                        // 0: single-scene context
+    int min_it, max_it;
+    float max_err;
+    bool fp64_test, two_d;
+    cudaGraphConditionalHandle handle;
+    bool set_condition;                // inside the captured loop: end it through handle
+};
+
+// every thread of every block calls it once, after reduce_err_parts
+__device__ __forceinline__ void iisph_end_of_iteration(const LoopCheck& chk, StepScalars* FSB_R sc,
+                                                       const int* FSB_R status) {
+    __shared__ int s_last;
+    // the block's atomics (thread 0's, or each thread's fenced ones in a
+    // block that spans scenes) come before its ticket
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(chk.ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (chk.scenes > 0) {
+        iisph_check_scenes_block(sc, chk.scenes, chk.min_it, chk.max_it, chk.max_err, status, chk.handle,
+                                 chk.set_condition);
+    } else if (threadIdx.x == 0) {
+        iisph_check_one(sc, chk.min_it, chk.max_it, chk.max_err, chk.fp64_test, chk.two_d, status, chk.handle,
+                        chk.set_condition);
+    }
+    if (threadIdx.x == 0) *chk.ticket = 0u;
+}
+
 // CFL clamp (IISPHFluidSolver3D.hpp:525-535, SESPHFluidSolver3D.hpp:109-116) with
 // ConstantTimestepGenerator::get_non_cfl_validating_timestep
 // (ConstantTimestepGenerator.cpp:17-41). The reference evaluates
 // sqrt(size / a) * lambda_a in double (its unqualified sqrt is the C double
 // function) and rounds the product to float; the rest is float.
-__device__ __forceinline__ void cfl_one(StepScalars* __restrict__ sc, float particle_size, float timestep,
+__device__ __forceinline__ void cfl_one(StepScalars* FSB_R sc, float particle_size, float timestep,
                                         float lambda_v, float lambda_a) {
     const float max_v = sqrtf(sc->final_max_v2);
     const float max_a = sqrtf(sc->final_max_a2);
@@ -578,21 +640,25 @@ __device__ __forceinline__ void cfl_one(StepScalars* __restrict__ sc, float part
 // as ordered bits. max |v| = sqrt(max |v|^2) since sqrt is monotonic and
 // correctly rounded. k_generator_finish: the generator's clamp, per scene.
 // ---------------------------------------------------------------------------
+// |v|^2 and |a|^2 of particle k as the generator computes them (0 when inactive)
 template <typename R>
-__global__ void k_generator_max(int64_t n, State<R> s, StepScalars* __restrict__ sc,
-                                const int* __restrict__ status) {
+__device__ __forceinline__ bool generator_at(int64_t k, const State<R>& s, float& v2, float& a2) {
+    if (s.type[k] == FS_TYPE_INACTIVE) return false;
+    const V4<R> v = s.vel[k], a = s.acc[k];
+    const float vx = (float)v.x, vy = (float)v.y, vz = (float)v.z;
+    const float ax = (float)a.x, ay = (float)a.y, az = (float)a.z;
+    v2 = (vx * vx + vy * vy) + vz * vz;
+    a2 = (ax * ax + ay * ay) + az * az;
+    return true;
+}
+template <typename R>
+__global__ void k_generator_max(int64_t n, State<R> s, StepScalars* FSB_R sc,
+                                const int* FSB_R status) {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     float v2 = 0.f, a2 = 0.f;
     int scene = 0;
-    const bool active = k < n && s.type[k] != FS_TYPE_INACTIVE;
-    if (active) {
-        const V4<R> v = s.vel[k], a = s.acc[k];
-        const float vx = (float)v.x, vy = (float)v.y, vz = (float)v.z;
-        const float ax = (float)a.x, ay = (float)a.y, az = (float)a.z;
-        v2 = (vx * vx + vy * vy) + vz * vz;
-        a2 = (ax * ax + ay * ay) + az * az;
-        scene = s.scene_of(k);
-    }
+    const bool active = k < n && generator_at<R>(k, s, v2, a2);
+    if (active) scene = s.scene_of(k);
     // one atomic per warp and quantity where the warp's particles share a scene
     const int s0 = __shfl_sync(0xffffffffu, scene, 0);
     if (__all_sync(0xffffffffu, scene == s0)) {
@@ -623,20 +689,26 @@ __device__ __forceinline__ float dynamic_cfl_timestep(float max_v, float max_a, 
     return ts;
 }
 
-__global__ void k_generator_finish(StepScalars* __restrict__ sc, int scenes, float particle_size, float min_ts,
+// (the maxima come from atomics: read through volatile loads, as the small-scene
+// step kernel runs this in the kernel that issued them)
+__device__ __forceinline__ void generator_finish_one(StepScalars* FSB_R q, float particle_size, float min_ts,
+                                                     float max_ts, float lambda_v, float lambda_a) {
+    const volatile StepScalars* v = q;
+    const float max_v = sqrtf(__uint_as_float(v->gen_v2_bits));
+    const float max_a = sqrtf(__uint_as_float(v->gen_a2_bits));
+    const float ts = dynamic_cfl_timestep(max_v, max_a, particle_size, min_ts, max_ts, lambda_v, lambda_a);
+    q->desired_dt = ts;
+    q->dt = ts;
+}
+static __global__ void k_generator_finish(StepScalars* FSB_R sc, int scenes, float particle_size, float min_ts,
                                    float max_ts, float lambda_v, float lambda_a) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < scenes; i += gridDim.x * blockDim.x) {
-        const float max_v = sqrtf(__uint_as_float(sc[i].gen_v2_bits));
-        const float max_a = sqrtf(__uint_as_float(sc[i].gen_a2_bits));
-        const float ts = dynamic_cfl_timestep(max_v, max_a, particle_size, min_ts, max_ts, lambda_v, lambda_a);
-        sc[i].desired_dt = ts;
-        sc[i].dt = ts;
-    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < scenes; i += gridDim.x * blockDim.x)
+        generator_finish_one(sc + i, particle_size, min_ts, max_ts, lambda_v, lambda_a);
 }
 
 // the clamp for scenes [0, scenes) (one in a single-scene context)
-__global__ void k_cfl(StepScalars* __restrict__ sc, int scenes, float particle_size, float timestep, float lambda_v,
-                      float lambda_a, const int* __restrict__ status) {
+static __global__ void k_cfl(StepScalars* FSB_R sc, int scenes, float particle_size, float timestep, float lambda_v,
+                      float lambda_a, const int* FSB_R status) {
     if (*status) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < scenes; i += gridDim.x * blockDim.x)
         cfl_one(sc + i, particle_size, timestep, lambda_v, lambda_a);
@@ -648,10 +720,7 @@ __global__ void k_cfl(StepScalars* __restrict__ sc, int scenes, float particle_s
 //   v = v* + dt a ;  x = x + dt v
 // ===========================================================================
 template <typename R>
-__global__ void k_iisph3d_integrate(int64_t n, State<R> s, const StepScalars* __restrict__ sc,
-                                    const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || *status) return;
+__device__ __forceinline__ void iisph3d_integrate_at(int64_t k, const State<R>& s, const StepScalars* FSB_R sc) {
     if (s.type[k] == FS_TYPE_INACTIVE) return;
     const StepScalars* q = sc + s.scene_of(k);
     const R dt = (R)q->dt, old = (R)q->desired_dt;
@@ -665,6 +734,13 @@ __global__ void k_iisph3d_integrate(int64_t n, State<R> s, const StepScalars* __
     const V3<R> x = xyz<R>(p) + dt * v;
     s.vel[k] = v4<R>(v, s.vel[k].w);
     s.pos[k] = v4<R>(x, p.w);
+}
+template <typename R>
+__global__ void k_iisph3d_integrate(int64_t n, State<R> s, const StepScalars* FSB_R sc,
+                                    const int* FSB_R status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    iisph3d_integrate_at<R>(k, s, sc);
 }
 
 // ===========================================================================
@@ -693,7 +769,7 @@ __device__ __forceinline__ void sesph_density_one(int64_t k, const State<R>& s, 
 }
 
 template <typename R, bool KAHAN>
-__global__ void k_sesph_density(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* __restrict__ status) {
+__global__ void k_sesph_density(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* FSB_R status) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n || *status) return;
     if (s.type[k] != FS_TYPE_NORMAL) return;
@@ -731,7 +807,7 @@ __device__ __forceinline__ void sesph_accel_one(int64_t k, const State<R>& s, co
 }
 
 template <typename R, bool KAHAN>
-__global__ void k_sesph_accel(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* __restrict__ status) {
+__global__ void k_sesph_accel(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* FSB_R status) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n || *status) return;
     if (s.type[k] != FS_TYPE_NORMAL) return;
@@ -740,19 +816,22 @@ __global__ void k_sesph_accel(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
 
 // max |a|^2, |v + dt a|^2 over ALL particles (SESPHFluidSolver3D.hpp:93-107)
 template <typename R>
-__global__ void k_sesph_maxima(int64_t n, State<R> s, StepScalars* __restrict__ sc, const int* __restrict__ status) {
+__device__ __forceinline__ void sesph_maxima_at(int64_t k, const State<R>& s, const StepScalars* FSB_R sc, float& a2,
+                                                float& v2) {
+    const R dt = (R)sc->desired_dt;
+    const V3<R> a = xyz<R>(s.acc[k]);
+    a2 = (float)dot(a, a);
+    const V3<R> v = xyz<R>(s.vel[k]) + dt * a;
+    v2 = (float)dot(v, v);
+    if (!(a2 >= 0.f)) a2 = 0.f;
+    if (!(v2 >= 0.f)) v2 = 0.f;
+}
+template <typename R>
+__global__ void k_sesph_maxima(int64_t n, State<R> s, StepScalars* FSB_R sc, const int* FSB_R status) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (*status) return;
     float a2 = 0.f, v2 = 0.f;
-    if (k < n) {
-        const R dt = (R)sc->desired_dt;
-        const V3<R> a = xyz<R>(s.acc[k]);
-        a2 = (float)dot(a, a);
-        const V3<R> v = xyz<R>(s.vel[k]) + dt * a;
-        v2 = (float)dot(v, v);
-        if (!(a2 >= 0.f)) a2 = 0.f;
-        if (!(v2 >= 0.f)) v2 = 0.f;
-    }
+    if (k < n) sesph_maxima_at<R>(k, s, sc, a2, v2);
     a2 = warp_max(a2);
     v2 = warp_max(v2);
     if ((threadIdx.x & 31) == 0) {
@@ -761,19 +840,18 @@ __global__ void k_sesph_maxima(int64_t n, State<R> s, StepScalars* __restrict__ 
     }
 }
 
-__global__ void k_sesph_maxima_final(StepScalars* __restrict__ sc) {
-    sc->final_max_a2 = __uint_as_float(sc->max_a2_bits);
-    sc->final_max_v2 = __uint_as_float(sc->max_v2_bits);
+__device__ __forceinline__ void sesph_maxima_final_one(StepScalars* FSB_R sc) {
+    const volatile StepScalars* v = sc;   // maxima from atomics (see generator_finish_one)
+    sc->final_max_a2 = __uint_as_float(v->max_a2_bits);
+    sc->final_max_v2 = __uint_as_float(v->max_v2_bits);
     sc->max_a2_bits = 0u;
     sc->max_v2_bits = 0u;
 }
+static __global__ void k_sesph_maxima_final(StepScalars* FSB_R sc) { sesph_maxima_final_one(sc); }
 
 // Euler-Cromer for every active particle: v += dt a; x += dt v
 template <typename R>
-__global__ void k_sesph_integrate(int64_t n, State<R> s, const StepScalars* __restrict__ sc,
-                                  const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || *status) return;
+__device__ __forceinline__ void sesph_integrate_at(int64_t k, const State<R>& s, const StepScalars* FSB_R sc) {
     if (s.type[k] == FS_TYPE_INACTIVE) return;
     const R dt = (R)sc->dt;
     const V4<R> vv = s.vel[k];
@@ -781,6 +859,13 @@ __global__ void k_sesph_integrate(int64_t n, State<R> s, const StepScalars* __re
     const V4<R> p = s.pos[k];
     s.vel[k] = v4<R>(v, vv.w);
     s.pos[k] = v4<R>(xyz<R>(p) + dt * v, p.w);
+}
+template <typename R>
+__global__ void k_sesph_integrate(int64_t n, State<R> s, const StepScalars* FSB_R sc,
+                                  const int* FSB_R status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    sesph_integrate_at<R>(k, s, sc);
 }
 
 // ===========================================================================
@@ -790,16 +875,13 @@ __global__ void k_sesph_integrate(int64_t n, State<R> s, const StepScalars* __re
 // acceleration + v* (all active); viscosity reads neighbor densities as in the
 // 3D first loop (SPLIT selects the serial-order emulation).
 template <typename R, bool KAHAN, bool SPLIT>
-__global__ void k_iisph2d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* __restrict__ sc,
-                             const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || *status) return;
+__device__ __forceinline__ void iisph2d_l1_at(int64_t k, const State<R>& s, const Lists& L, const SolverConsts<R>& c,
+                                              R dt) {
     const uint8_t t = s.type[k];
     if (t == FS_TYPE_INACTIVE) {
         if (!SPLIT) s.rho[k] = s.rho_prev[k];  // carry the density through the double buffer
         return;
     }
-    const R dt = (R)sc->dt;
     const V4<R> pk = s.pos[k];
     const V4<R> vk = s.vel[k];
     R rho_k = s.rho_prev[k];
@@ -835,12 +917,18 @@ __global__ void k_iisph2d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
     s.ext[k] = v4<R>(v3<R>(R(0), R(0), R(0)), R(0));
     if (!SPLIT) s.rho[k] = rho_k;
 }
+template <typename R, bool KAHAN, bool SPLIT>
+__global__ void k_iisph2d_l1(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* FSB_R sc,
+                             const int* FSB_R status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    iisph2d_l1_at<R, KAHAN, SPLIT>(k, s, L, c, (R)sc->dt);
+}
 
 // density for the split 2D first loop
 template <typename R, bool KAHAN>
-__global__ void k_iisph2d_density(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || *status) return;
+__device__ __forceinline__ void iisph2d_density_at(int64_t k, const State<R>& s, const Lists& L,
+                                                   const SolverConsts<R>& c) {
     if (s.type[k] != FS_TYPE_NORMAL) {
         s.rho[k] = s.rho_prev[k];
         return;
@@ -854,17 +942,20 @@ __global__ void k_iisph2d_density(int64_t n, State<R> s, Lists L, SolverConsts<R
     }
     s.rho[k] = rho.get();
 }
+template <typename R, bool KAHAN>
+__global__ void k_iisph2d_density(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const int* FSB_R status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    iisph2d_density_at<R, KAHAN>(k, s, L, c);
+}
 
 // second loop (:170-180, 280-376): source term, diagonal element, p = 0.
 // The reference's O(n^2) diagonal recomputes the same inner sum for every
 // outer neighbor; it is computed once here (the value is identical).
 template <typename R, bool KAHAN>
-__global__ void k_iisph2d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* __restrict__ sc,
-                             const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || *status) return;
+__device__ __forceinline__ void iisph2d_l2_at(int64_t k, const State<R>& s, const Lists& L, const SolverConsts<R>& c,
+                                              R dt) {
     if (s.type[k] != FS_TYPE_NORMAL) return;
-    const R dt = (R)sc->dt;
     const V4<R> pk = s.pos[k];
     const V3<R> xk = xyz<R>(pk);
     const V3<R> vsk = xyz<R>(s.vstar[k]);
@@ -899,13 +990,18 @@ __global__ void k_iisph2d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, 
     s.anp[k] = v4<R>(v3<R>(R(0), R(0), R(0)), (dt * dt) * d.get());
     s.p[k] = R(0);
 }
+template <typename R, bool KAHAN>
+__global__ void k_iisph2d_l2(int64_t n, State<R> s, Lists L, SolverConsts<R> c, const StepScalars* FSB_R sc,
+                             const int* FSB_R status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    iisph2d_l2_at<R, KAHAN>(k, s, L, c, (R)sc->dt);
+}
 
 // 2D iteration (a) (:408-444): a_i = -sum
 template <typename R, bool KAHAN>
-__global__ void k_iisph2d_pressure_acc(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
-                                       const StepScalars* __restrict__ sc, const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || *status || sc->done) return;
+__device__ __forceinline__ void iisph2d_pressure_acc_at(int64_t k, const State<R>& s, const Lists& L,
+                                                        const SolverConsts<R>& c) {
     if (s.type[k] != FS_TYPE_NORMAL) return;
     const V3<R> xk = xyz<R>(s.pos[k]);
     const R pk = s.p[k];
@@ -922,17 +1018,21 @@ __global__ void k_iisph2d_pressure_acc(int64_t n, State<R> s, Lists L, SolverCon
     }
     s.acc[k] = v4<R>(-sum.get(), R(0));
 }
+template <typename R, bool KAHAN>
+__global__ void k_iisph2d_pressure_acc(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
+                                       const StepScalars* FSB_R sc, const int* FSB_R status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status || sc->done) return;
+    iisph2d_pressure_acc_at<R, KAHAN>(k, s, L, c);
+}
 
 // 2D iteration (b) (:447-511): Ap = dt^2 sum, update, density error
+// particle k's update; adds its error to e_sum / e_cnt
 template <typename R, bool KAHAN>
-__global__ void k_iisph2d_pressure_update(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
-                                          StepScalars* __restrict__ sc, const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (*status || sc->done) return;
-    double e_sum = 0.0;
-    unsigned int e_cnt = 0;
-    if (k < n && s.type[k] == FS_TYPE_NORMAL) {
-        const R dt = (R)sc->dt;
+__device__ __forceinline__ void iisph2d_pressure_update_at(int64_t k, const State<R>& s, const Lists& L,
+                                                           const SolverConsts<R>& c, R dt, double& e_sum,
+                                                           unsigned int& e_cnt) {
+    if (s.type[k] == FS_TYPE_NORMAL) {
         const V3<R> xk = xyz<R>(s.pos[k]);
         const V3<R> ak = xyz<R>(s.acc[k]);
         const uint32_t nn = L.size(k);
@@ -956,10 +1056,19 @@ __global__ void k_iisph2d_pressure_update(int64_t n, State<R> s, Lists L, Solver
         R perr = abs_(src - Ap);
         if (has_diag) {
             if (abs_(p) <= R(kFltEps)) perr = R(0);
-            e_sum = (double)perr;
-            e_cnt = 1;
+            e_sum += (double)perr;
+            e_cnt += 1;
         }
     }
+}
+template <typename R, bool KAHAN>
+__global__ void k_iisph2d_pressure_update(int64_t n, State<R> s, Lists L, SolverConsts<R> c,
+                                          StepScalars* FSB_R sc, const int* FSB_R status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (*status || sc->done) return;
+    double e_sum = 0.0;
+    unsigned int e_cnt = 0;
+    if (k < n) iisph2d_pressure_update_at<R, KAHAN>(k, s, L, c, (R)sc->dt, e_sum, e_cnt);
     e_sum = warp_sum(e_sum);
     e_cnt = warp_sum(e_cnt);
     if ((threadIdx.x & 31) == 0 && e_cnt) {
@@ -970,16 +1079,20 @@ __global__ void k_iisph2d_pressure_update(int64_t n, State<R> s, Lists L, Solver
 
 // 2D integration (:379-392): v = v* + dt a; x += dt v (no CFL clamp)
 template <typename R>
-__global__ void k_iisph2d_integrate(int64_t n, State<R> s, const StepScalars* __restrict__ sc,
-                                    const int* __restrict__ status) {
-    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || *status) return;
+__device__ __forceinline__ void iisph2d_integrate_at(int64_t k, const State<R>& s, const StepScalars* FSB_R sc) {
     if (s.type[k] == FS_TYPE_INACTIVE) return;
     const R dt = (R)sc->dt;
     const V3<R> v = xyz<R>(s.vstar[k]) + dt * xyz<R>(s.acc[k]);
     const V4<R> p = s.pos[k];
     s.vel[k] = v4<R>(v, s.vel[k].w);
     s.pos[k] = v4<R>(xyz<R>(p) + dt * v, p.w);
+}
+template <typename R>
+__global__ void k_iisph2d_integrate(int64_t n, State<R> s, const StepScalars* FSB_R sc,
+                                    const int* FSB_R status) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || *status) return;
+    iisph2d_integrate_at<R>(k, s, sc);
 }
 
 }  // namespace fsb

@@ -51,8 +51,8 @@ template <typename K> __device__ __forceinline__ uint32_t digit_of(K key, int sh
 
 // hist[d * tiles + t] = keys of tile t whose digit at `shift` is d
 template <typename K>
-__global__ void __launch_bounds__(kSortThreads) k_sort_hist(int64_t n, const K* __restrict__ keys, int shift,
-                                                            int64_t tiles, uint32_t* __restrict__ hist) {
+__global__ void __launch_bounds__(kSortThreads) k_sort_hist(int64_t n, const K* FSB_R keys, int shift,
+                                                            int64_t tiles, uint32_t* FSB_R hist) {
     __shared__ uint32_t h[kSortDigits];
     h[threadIdx.x] = 0u;
     __syncthreads();
@@ -76,8 +76,8 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_hist(int64_t n, const K* 
 
 // Row d of the histogram matrix (block d) into exclusive offsets over the
 // tiles, in place; totals[d] = the digit's keys in all tiles.
-__global__ void __launch_bounds__(kSortThreads) k_sort_rowscan(uint32_t* __restrict__ hist, int64_t tiles,
-                                                               uint32_t* __restrict__ totals) {
+static __global__ void __launch_bounds__(kSortThreads) k_sort_rowscan(uint32_t* FSB_R hist, int64_t tiles,
+                                                               uint32_t* FSB_R totals) {
     __shared__ uint32_t s_warp[kSortWarps];
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     uint32_t* row = hist + (int64_t)blockIdx.x * tiles;
@@ -109,9 +109,10 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_rowscan(uint32_t* __restr
 
 // Exclusive scan of m counts by one block of 1024 threads (each scans a
 // contiguous run, the runs' sums are scanned across the block); used for
-// list exports. out may alias in when both have one type.
+// list exports and small cell tables. out may alias in when both have one
+// type. Every thread of the block calls scan_exclusive_block.
 template <typename In, typename Out>
-__global__ void __launch_bounds__(1024) k_scan_exclusive(const In* in, Out* out, int64_t m) {
+__device__ __forceinline__ void scan_exclusive_block(const In* in, Out* out, int64_t m) {
     __shared__ Out s_warp[32];
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int64_t per = (m + 1023) / 1024;
@@ -145,6 +146,10 @@ __global__ void __launch_bounds__(1024) k_scan_exclusive(const In* in, Out* out,
         run += v;
     }
 }
+template <typename In, typename Out>
+__global__ void __launch_bounds__(1024) k_scan_exclusive(const In* in, Out* out, int64_t m) {
+    scan_exclusive_block<In, Out>(in, out, m);
+}
 
 // Scatters tile blockIdx.x of (kin, vin) to its slots: slot of a key =
 // (keys of smaller digits, from totals) + offs[d * tiles + tile] (the row
@@ -153,11 +158,11 @@ __global__ void __launch_bounds__(1024) k_scan_exclusive(const In* in, Out* out,
 // counter per digit; then the counters turn into each warp's first slot per
 // digit.
 template <typename K>
-__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(int64_t n, const K* __restrict__ kin,
-                                                               const uint32_t* __restrict__ vin, K* __restrict__ kout,
-                                                               uint32_t* __restrict__ vout, int shift, int64_t tiles,
-                                                               const uint32_t* __restrict__ offs,
-                                                               const uint32_t* __restrict__ totals) {
+__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(int64_t n, const K* FSB_R kin,
+                                                               const uint32_t* FSB_R vin, K* FSB_R kout,
+                                                               uint32_t* FSB_R vout, int shift, int64_t tiles,
+                                                               const uint32_t* FSB_R offs,
+                                                               const uint32_t* FSB_R totals) {
     __shared__ uint32_t wh[kSortWarps][kSortDigits];
     __shared__ uint32_t s_base[kSortWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -235,15 +240,20 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(int64_t n, const 
 // every run of equal keys, the run's length (the table is zeroed before);
 // the scan runs in place.
 template <typename K>
-__global__ void k_cell_counts(int64_t n_struct, const K* __restrict__ keys, int key_shift, int key_bits,
-                              int64_t cells, uint32_t* __restrict__ counts) {
-    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n_struct) return;
+__device__ __forceinline__ void cell_count_at(int64_t k, int64_t n_struct, const K* FSB_R keys, int key_shift,
+                                              int key_bits, int64_t cells, uint32_t* FSB_R counts) {
     const uint32_t key = (uint32_t)(keys[k] >> key_shift);
     if (k > 0 && (uint32_t)(keys[k - 1] >> key_shift) == key) return;
     int64_t e = k + 1;
     while (e < n_struct && (uint32_t)(keys[e] >> key_shift) == key) e++;
     counts[(int64_t)(key >> key_bits) * (cells + 1) + (key & ((1u << key_bits) - 1u))] = (uint32_t)(e - k);
+}
+template <typename K>
+__global__ void k_cell_counts(int64_t n_struct, const K* FSB_R keys, int key_shift, int key_bits,
+                              int64_t cells, uint32_t* FSB_R counts) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n_struct) return;
+    cell_count_at<K>(k, n_struct, keys, key_shift, key_bits, cells, counts);
 }
 
 // Device-wide exclusive scan of m counts, in place, in three launches:
@@ -256,8 +266,8 @@ constexpr int kScanTile = kScanThreads * kScanPerThread;
 inline int64_t scan_tiles(int64_t m) { return (m + kScanTile - 1) / kScanTile; }
 constexpr int64_t kSmallScanMax = 65536;   // tables scanned by one block in one launch
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(uint32_t* __restrict__ a, int64_t m,
-                                                             uint32_t* __restrict__ partials) {
+static __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(uint32_t* FSB_R a, int64_t m,
+                                                             uint32_t* FSB_R partials) {
     __shared__ uint32_t tile[kScanTile];
     __shared__ uint32_t s_warp[kScanThreads / 32];
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
@@ -301,7 +311,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(uint32_t* __restric
         if (base + i < m) a[base + i] = tile[i];
 }
 
-__global__ void k_scan_add(uint32_t* __restrict__ a, int64_t m, const uint32_t* __restrict__ partials) {
+static __global__ void k_scan_add(uint32_t* FSB_R a, int64_t m, const uint32_t* FSB_R partials) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
         a[i] += partials[i / kScanTile];
 }
@@ -341,11 +351,11 @@ template <typename K> constexpr size_t small_sort_smem() {
     return (size_t)2 * kSmallSortMax * (sizeof(K) + sizeof(uint32_t)) + (size_t)kSmallSortWarps * kSortDigits * 4;
 }
 
+// the whole small sort by one block of kSmallSortThreads threads;
+// sort_smem: small_sort_smem<K>() bytes of shared memory
 template <typename K>
-__global__ void __launch_bounds__(kSmallSortThreads) k_sort_small(int64_t n, int bits, const K* __restrict__ kin,
-                                                                  const uint32_t* __restrict__ vin,
-                                                                  K* __restrict__ kout, uint32_t* __restrict__ vout) {
-    extern __shared__ __align__(16) unsigned char sort_smem[];
+__device__ __forceinline__ void sort_small_block(int64_t n, int bits, const K* FSB_R kin, const uint32_t* FSB_R vin,
+                                                 K* FSB_R kout, uint32_t* FSB_R vout, unsigned char* sort_smem) {
     K* sk[2] = {reinterpret_cast<K*>(sort_smem), reinterpret_cast<K*>(sort_smem) + kSmallSortMax};
     uint32_t* sv[2] = {reinterpret_cast<uint32_t*>(sk[1] + kSmallSortMax),
                        reinterpret_cast<uint32_t*>(sk[1] + kSmallSortMax) + kSmallSortMax};
@@ -420,6 +430,13 @@ __global__ void __launch_bounds__(kSmallSortThreads) k_sort_small(int64_t n, int
         kout[i] = sk[cur][i];
         vout[i] = sv[cur][i];
     }
+}
+template <typename K>
+__global__ void __launch_bounds__(kSmallSortThreads) k_sort_small(int64_t n, int bits, const K* FSB_R kin,
+                                                                  const uint32_t* FSB_R vin,
+                                                                  K* FSB_R kout, uint32_t* FSB_R vout) {
+    extern __shared__ __align__(16) unsigned char sort_smem[];
+    sort_small_block<K>(n, bits, kin, vin, kout, vout, sort_smem);
 }
 
 // the small sort's shared memory, set once per process and device

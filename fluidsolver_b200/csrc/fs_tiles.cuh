@@ -44,21 +44,40 @@ constexpr uint32_t kTileFallback = 0xffffffffu;
 constexpr uint32_t kEntOffset = 0xfff0u;
 constexpr uint32_t kEntBoundary = 0x1u;
 
-struct TileHead {
+// Staged slots: range r of a tile occupies slots [base_r, base_r + len_r) of
+// every staged array. In the padded layout base_r is congruent to the range's
+// first sorted index modulo 4 and at least the previous range's end rounded up
+// to a multiple of 4: a float array's range then starts and ends, rounded
+// outwards to 4 floats, on 16-byte boundaries in global and in shared memory
+// alike, so it is staged by one bulk copy, as the float4 arrays are; the
+// rounding lands in padding slots that no entry addresses. A tile whose
+// padded layout exceeds the staging cap but whose candidates fit keeps the
+// packed layout (base_r = the lengths before r), and its float arrays go
+// through 4-byte copies. The range's padded extent:
+__host__ __device__ __forceinline__ uint32_t padded_slots(uint32_t start, uint32_t len) {
+    return len ? ((start + len + 3u) & ~3u) - (start & ~3u) : 0u;
+}
+
+// a tile's header as stored (TileDesc::h)
+struct TileHeadRaw {
     uint32_t nranges;                  // non-empty candidate ranges, or kTileFallback
-    uint32_t staged;                   // candidates staged in total
-    uint32_t staged_fluid;             // of them in fluid ranges
+    uint32_t staged;                   // candidates staged in total | (of them in fluid ranges << 16)
+    uint32_t slots;                    // padded layout: slots in total | (of them in fluid ranges << 16); 0: packed
     uint32_t octets;                   // octets of entries of the tile's longest list
 };
+// the header as the passes use it
+struct TileHead {
+    uint32_t nranges, staged, staged_fluid, slots, slots_fluid, octets;
+};
 struct alignas(16) TileDesc {
-    TileHead h;
+    TileHeadRaw h;
     uint32_t start[kTileRanges];       // first sorted index of each range
     uint32_t len_base[kTileRanges];    // length | kRangeBoundary for boundary ranges | (first staged slot << 16)
 };
 
 __device__ __forceinline__ TileHead load_head(const TileDesc* d) {
     const uint4 a = *reinterpret_cast<const uint4*>(d);
-    return TileHead{a.x, a.y, a.z, a.w};
+    return TileHead{a.x, a.y & 0xffffu, a.y >> 16, a.z & 0xffffu, a.z >> 16, a.w};
 }
 
 // the range of thread t (t < kTileRanges), loaded before the tile's header
@@ -108,22 +127,26 @@ struct TileStage {
     uint64_t bar;
 };
 
+// One try of the wait for phase 0: the thread sleeps until the phase
+// completes or kTileWaitHintNs pass (the try's time limit), so that waiting
+// warps issue no instructions while the copies land.
+constexpr uint32_t kTileWaitHintNs = 20000;
 __device__ __forceinline__ uint32_t mbar_try_wait0(TileStage& st) {
     uint32_t ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0, %2;\n selp.u32 %0, 1, 0, p;\n}"
         : "=r"(ok)
-        : "r"(smem_u32(&st.bar))
+        : "r"(smem_u32(&st.bar)), "r"(kTileWaitHintNs)
         : "memory");
     return ok;
 }
 
-// Tries of the first wait for a tile's staging (each mbarrier.try_wait may
-// suspend the thread for a while). fs_set_tile_wait_limit lowers it so that
-// a test can make the wait run out and check the error path; it is
+// Tries of the first wait for a tile's staging (each try sleeps up to
+// kTileWaitHintNs: about 1.3 s in all). fs_set_tile_wait_limit lowers it so
+// that a test can make the wait run out and check the error path; it is
 // kTileWaitTries otherwise.
 constexpr int kTileWaitTries = 1 << 16;
-constexpr int kTileDrainTries = 1 << 20;
+constexpr int kTileDrainTries = 1 << 16;
 static __device__ int g_tile_wait_tries = kTileWaitTries;
 
 // Waits for the staging to land, with a bounded number of tries. Returns
@@ -133,7 +156,7 @@ static __device__ int g_tile_wait_tries = kTileWaitTries;
 // flight land, so that none writes into shared memory after the block has
 // left it.
 __device__ __forceinline__ bool stage_tile_wait(TileStage& st, int* __restrict__ status) {
-    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("cp.async.wait_all;" ::: "memory");   // the packed layout's 4-byte copies
     uint32_t ok = 0;
     const int tries = g_tile_wait_tries;
     for (int it = 0; it < tries && !ok; it++) ok = mbar_try_wait0(st);
@@ -168,11 +191,13 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     __shared__ int s_gd0[kTileGroups], s_gd01[kTileGroups], s_gx0[kTileGroups], s_gx1[kTileGroups];
     // s_base: first staged slot | (position among the non-empty ranges << 16)
     __shared__ uint32_t s_start[kTileRanges], s_len[kTileRanges], s_base[kTileRanges];
-    __shared__ uint32_t s_total;
     // per-warp partial results, in arrays whose contents are dead by then
     // (static shared memory decides whether 5 blocks fit on an SM)
-    uint32_t* s_wlen = s_cnt;                                     // warp sums of the range scan
+    uint32_t* s_wlen = s_cnt;                                     // warp sums of the range scans
     uint32_t* s_wne = s_cnt + kTileOwners / 32;
+    uint32_t* s_wl = s_cnt + 2 * (kTileOwners / 32);              // warp sums of the header's totals
+    uint32_t* s_wlf = s_cnt + 3 * (kTileOwners / 32);
+    uint32_t* s_wpf = s_cnt + 4 * (kTileOwners / 32);
     uint32_t* s_wmax = reinterpret_cast<uint32_t*>(s_lead);       // warp maxima of the list lengths
     {
         // an earlier error (e.g. non-finite positions) ends the step; an overflow
@@ -217,6 +242,9 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     const int g = before + __popc(bal & ((1u << lane) - 1u)) + (lead ? 1 : 0) - 1;
     bool fallback = any_border || G > kTileGroups;
     int NR = 0;
+    // the header's totals: candidates and padded slots, all and in fluid ranges
+    uint32_t tot_len = 0, tot_len_fluid = 0, tot_slots = 0, tot_slots_fluid = 0;
+    bool padded = false;
     if (!fallback) {
         if (lead) {
             s_grow[g] = key;
@@ -227,46 +255,65 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
         if (valid && (t == kTileOwners - 1 || s_key[t + 1] != key)) s_gx1[g] = lx;
         __syncthreads();
         NR = 18 * G;
-        uint32_t len = 0;
+        uint32_t len = 0, a = 0;
         if (t < NR) {
             const int region = t / (9 * G), gg = (t % (9 * G)) / 9, r = t % 9;
             const int64_t rb = s_grow[gg] + (int64_t)(r / 3 - 1) * s_gd01[gg] + (int64_t)(r % 3 - 1) * s_gd0[gg];
             const uint32_t* cs = cell_start + region * (w.cells + 1);
-            const uint32_t a = cs[rb + s_gx0[gg] - 1], b = cs[rb + s_gx1[gg] + 2];
-            len = b - a;
+            a = cs[rb + s_gx0[gg] - 1];
+            len = cs[rb + s_gx1[gg] + 2] - a;
             s_start[t] = a;
             s_len[t] = len;
         }
         // exclusive prefix sums over the ranges (thread t: range t) of their
-        // lengths -- first staged slots -- and of their non-emptiness --
-        // positions in the descriptor --, by warp scans
-        uint32_t incl = len, ne = len ? 1u : 0u;
+        // padded extents -- first staged slots -- and of their non-emptiness
+        // -- positions in the descriptor --, by warp scans; and the header's
+        // totals (fluid ranges, t < 9 G, come first)
+        const uint32_t ps = padded_slots(a, len);
+        const bool fluid_range = t < 9 * G;
+        uint32_t incl = ps, incl_len = len, ne = len ? 1u : 0u;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t a = __shfl_up_sync(0xffffffffu, incl, o), b = __shfl_up_sync(0xffffffffu, ne, o);
+            const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o), y = __shfl_up_sync(0xffffffffu, ne, o);
+            const uint32_t z = __shfl_up_sync(0xffffffffu, incl_len, o);
             if (lane >= o) {
-                incl += a;
-                ne += b;
+                incl += x;
+                ne += y;
+                incl_len += z;
             }
         }
+        const uint32_t wl = __reduce_add_sync(0xffffffffu, len);
+        const uint32_t wlf = __reduce_add_sync(0xffffffffu, fluid_range ? len : 0u);
+        const uint32_t wpf = __reduce_add_sync(0xffffffffu, fluid_range ? ps : 0u);
         if (lane == 31) {
             s_wlen[t >> 5] = incl;
             s_wne[t >> 5] = ne;
         }
+        if (lane == 0) {
+            s_wl[t >> 5] = wl;
+            s_wlf[t >> 5] = wlf;
+            s_wpf[t >> 5] = wpf;
+        }
         __syncthreads();
-        uint32_t before = 0, before_ne = 0, tot = 0;
+        uint32_t before = 0, before_ne = 0, before_len = 0;
 #pragma unroll
         for (int i = 0; i < kTileOwners / 32; i++) {
             if (i < (t >> 5)) {
                 before += s_wlen[i];
                 before_ne += s_wne[i];
+                before_len += s_wl[i];
             }
-            tot += s_wlen[i];
+            tot_slots += s_wlen[i];
+            tot_len += s_wl[i];
+            tot_len_fluid += s_wlf[i];
+            tot_slots_fluid += s_wpf[i];
         }
+        // the padded layout where it fits the cap, else the packed one
         // (every thread has read the warp sums before s_cnt is reused)
-        if (t < NR) s_base[t] = (before + incl - len) | ((before_ne + ne - (len ? 1u : 0u)) << 16);
-        fallback = tot > (uint32_t)cap;
-        if (t == 0) s_total = tot;
+        padded = tot_slots <= (uint32_t)cap;
+        const uint32_t slot = padded ? before + incl - ps + (a & 3u) : before_len + incl_len - len;
+        if (t < NR) s_base[t] = slot | ((before_ne + ne - (len ? 1u : 0u)) << 16);
+        fallback = !padded && tot_len > (uint32_t)cap;
         __syncthreads();
     }
 
@@ -303,7 +350,7 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
     __syncthreads();
     if (t == 0)
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&stg.bar)),
-                     "r"(s_total * 16u)
+                     "r"(tot_len * 16u)
                      : "memory");
     if (t < NR && s_len[t])
         asm volatile(
@@ -362,7 +409,8 @@ __global__ void __launch_bounds__(kTileOwners, 4) k_build_tiles(
         const uint32_t nonempty = (s_base[last] >> 16) + (s_len[last] ? 1u : 0u);
         // fluid ranges come first: the first boundary range's slot is their total
         *reinterpret_cast<uint4*>(desc + tile) =
-            make_uint4(nonempty, s_total, s_base[9 * G] & 0xffffu, (min(mx, (uint32_t)K) + 7) / 8);
+            make_uint4(nonempty, tot_len | (tot_len_fluid << 16), padded ? tot_slots | (tot_slots_fluid << 16) : 0u,
+                       (min(mx, (uint32_t)K) + 7) / 8);
     }
     // octets of entries, coalesced across the tile's owners
     const int O = K / 8;
@@ -384,11 +432,13 @@ struct TileSlab {
 // bulk copy (the TMA engine) per range and float4 array, issued by the
 // range's thread, and one per octet plane of the tile's entries and for its
 // list lengths, issued by threads from the top of the block; completion is
-// counted in bytes on the mbarrier. A float array goes through 4-byte
-// cp.async copies, a warp per range (its ranges start at arbitrary floats,
-// which bulk copies cannot). h and rg are the tile's header and the calling
+// counted in bytes on the mbarrier. In the padded layout a float array's
+// range is copied rounded outwards to 16-byte boundaries into its padded
+// slots (padded_slots); in the packed layout it goes through 4-byte cp.async
+// copies, a warp per range. h and rg are the tile's header and the calling
 // thread's range, loaded up front. FLUID_ONLY skips the boundary ranges;
-// SLAB false leaves the entries and list lengths in global memory.
+// SLAB false leaves the entries and list lengths in global memory. A float
+// array (src1) must be readable up to its length rounded up to a multiple of 4.
 template <int NV4, bool FLUID_ONLY = false, bool SLAB = true>
 __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* __restrict__ d, const TileHead& h,
                                                  const TileRange& rg,
@@ -404,6 +454,7 @@ __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* 
     __syncthreads();
     if (t == 0) {
         const uint32_t bytes = (FLUID_ONLY ? h.staged_fluid : h.staged) * 16u * (uint32_t)NV4 +
+                               (src1 != nullptr ? (FLUID_ONLY ? h.slots_fluid : h.slots) * 4u : 0u) +   // 0: packed
                                (SLAB ? h.octets * (uint32_t)kTileOwners * 16u + (uint32_t)kTileOwners * 4u : 0u);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&st.bar)), "r"(bytes)
                      : "memory");
@@ -438,8 +489,16 @@ __device__ __forceinline__ void stage_tile_async(TileStage& st, const TileDesc* 
                 "l"(src4[v] + a), "r"(len * 16u), "r"(smem_u32(&st.bar)), "l"(pol)
                 : "memory");
         }
+        if (src1 != nullptr && h.slots) {
+            // base is congruent to a modulo 4: both ends round to 16-byte boundaries
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], "
+                "%4;" ::"r"(smem_u32(dst1 + (base - (a & 3u)))),
+                "l"(src1 + (a & ~3u)), "r"(padded_slots(a, len) * 4u), "r"(smem_u32(&st.bar)), "l"(pol)
+                : "memory");
+        }
     }
-    if (src1 != nullptr) {
+    if (src1 != nullptr && !h.slots) {
         const int lane = t & 31;
         for (uint32_t q = t >> 5; q < h.nranges; q += blockDim.x / 32) {
             const uint32_t a = d->start[q], lb = d->len_base[q];
@@ -812,9 +871,11 @@ __global__ void __launch_bounds__(kPassThreads, kL2GlobalEntries ? 4 : 3) k_tile
     const V3<float> in = v3<float>(__fmaf_rn(1.f - wb, gbt.x, -m.x), __fmaf_rn(1.f - wb, gbt.y, -m.y),
                                    __fmaf_rn(1.f - wb, gbt.z, -m.z));
     if (!half && valid) {
-        s.gbnd[k] = v4<float>(gbt, 0.f);   // sum_bnd m_j gradW, for the pressure iterations
         const float source = (c.rest_density - rk) - dt * ct;
         const float diag = (c.inv_rho0_sq * dot(in, m) - (pk.w / c.rho0_sq) * g2) * (dt * dt);
+        // sum_bnd m_j gradW for the pressure iterations, with the diagonal beside it
+        // (one float4 read per owner instead of two in the update pass)
+        s.gbnd[k] = v4<float>(gbt, diag);
         const float4 vs = make_float4(vsk.x, vsk.y, vsk.z, source);
         s.vstar[k] = vs;
         s.anp[k].w = diag;
@@ -887,13 +948,14 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
     s.acc[k] = v4<float>(c.inv_rho0_sq * (a - wb * v3<float>(gbk.x, gbk.y, gbk.z)), 0.f);
 }
 
-// iteration (b): A p, relaxed Jacobi update, density error, fused scan
+// iteration (b): A p, relaxed Jacobi update, density error, fused scan; the
+// block that finishes last runs the iteration's convergence test (chk)
 template <int AHEAD>
 __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) k_tile_iisph3d_pressure_update(int64_t n_fluid, State<float> s,
                                                                                TileLists T, Lists L,
                                                                                SolverConsts<float> c,
                                                                                StepScalars* __restrict__ sc,
-                                                                               int* __restrict__ status) {
+                                                                               int* __restrict__ status, LoopCheck chk) {
     extern __shared__ float4 tile_smem[];
     const int half = threadIdx.x & 1;
     const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
@@ -905,53 +967,56 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
     const int scene = s.scene_of(kk);
     const StepScalars* q = sc + scene;
     const bool live = k < n_fluid && !q->done;
-    if (__syncthreads_or(err) || !__syncthreads_or(live)) return;
-    const float dt = q->dt;
-    ErrPart o;
-    // the owner's own data, loaded while the staging lands
-    const bool valid = live;
-    const float4 pk = s.pos[kk], ak = s.acc[kk], vsk = s.vstar[kk], gbk = s.gbnd[kk];
-    const float aii = s.anp[kk].w, prk = s.p[kk];
-    const FastSpline S(c.kern);
-    Acc<float, true> ap;
-    float part = 0.f;
-    auto pair = [&](const float4& pj, const float4& aj) {
-        const V3<float> xij = sub3(pk, pj);
-        part = __fmaf_rn(pj.w * S.grad(r2_of(xij)), dot3(sub3(ak, aj), xij), part);
-    };
-    auto flush = [&] {
-        ap.add(part);
-        part = 0.f;
-    };
-    // boundary neighbors enter through sum_bnd m_j gradW (second loop)
-    bool done = true;
-    if (h.nranges == kTileFallback) {
-        // the owner's 32-bit list, split between its two threads
-        if (valid) walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.acc[j]); }, flush);
-    } else {
-        float4* sp = tile_smem;
-        float4* sa = tile_smem + T.cap;
-        __shared__ TileStage stg;
-        const float4* src4[2] = {s.pos, s.acc};
-        float4* dst4[2] = {sp, sa};
-        const TileSlab slab = slab_at(tile_smem, 32, T.K, T.cap);
-        stage_tile_async<2, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
-        const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
-        uint2 ahead[AHEAD];
-        prefetch_tile_list<kPressureGlobalEntries>(T, h, k, half, ahead);
-        done = stage_tile_wait(stg, status);
-        if (done && valid)
-            walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool) {
-                pair(at_offset(sp, off), at_offset(sa, off));
-            }, flush);
+    // a block with nothing to do still takes its ticket for the test
+    if (!__syncthreads_or(err) && __syncthreads_or(live)) {
+        const float dt = q->dt;
+        ErrPart o;
+        // the owner's own data, loaded while the staging lands
+        const bool valid = live;
+        const float4 pk = s.pos[kk], ak = s.acc[kk], vsk = s.vstar[kk], gbk = s.gbnd[kk];
+        const float aii = gbk.w, prk = s.p[kk];   // gbnd.w: the diagonal (second loop)
+        const FastSpline S(c.kern);
+        Acc<float, true> ap;
+        float part = 0.f;
+        auto pair = [&](const float4& pj, const float4& aj) {
+            const V3<float> xij = sub3(pk, pj);
+            part = __fmaf_rn(pj.w * S.grad(r2_of(xij)), dot3(sub3(ak, aj), xij), part);
+        };
+        auto flush = [&] {
+            ap.add(part);
+            part = 0.f;
+        };
+        // boundary neighbors enter through sum_bnd m_j gradW (second loop)
+        bool done = true;
+        if (h.nranges == kTileFallback) {
+            // the owner's 32-bit list, split between its two threads
+            if (valid) walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.acc[j]); }, flush);
+        } else {
+            float4* sp = tile_smem;
+            float4* sa = tile_smem + T.cap;
+            __shared__ TileStage stg;
+            const float4* src4[2] = {s.pos, s.acc};
+            float4* dst4[2] = {sp, sa};
+            const TileSlab slab = slab_at(tile_smem, 32, T.K, T.cap);
+            stage_tile_async<2, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
+            const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
+            uint2 ahead[AHEAD];
+            prefetch_tile_list<kPressureGlobalEntries>(T, h, k, half, ahead);
+            done = stage_tile_wait(stg, status);
+            if (done && valid)
+                walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool) {
+                    pair(at_offset(sp, off), at_offset(sa, off));
+                }, flush);
+        }
+        if (done) {
+            // boundary: sum_bnd m_j dot(a_i, gradW) = dot(a_i, sum_bnd m_j gradW)
+            const float sum = pair_total(ap) + dot3(v3<float>(ak.x, ak.y, ak.z), v3<float>(gbk.x, gbk.y, gbk.z));
+            if (!half && valid)
+                o = iisph3d_pressure_update_tail<float>(k, s, c, dt, v3<float>(ak.x, ak.y, ak.z), sum, vsk, aii, prk);
+        }
+        reduce_err_parts(o, sc, scene);
     }
-    if (done) {
-        // boundary: sum_bnd m_j dot(a_i, gradW) = dot(a_i, sum_bnd m_j gradW)
-        const float sum = pair_total(ap) + dot3(v3<float>(ak.x, ak.y, ak.z), v3<float>(gbk.x, gbk.y, gbk.z));
-        if (!half && valid)
-            o = iisph3d_pressure_update_tail<float>(k, s, c, dt, v3<float>(ak.x, ak.y, ak.z), sum, vsk, aii, prk);
-    }
-    reduce_err_parts(o, sc, scene);
+    iisph_end_of_iteration(chk, sc, status);
 }
 
 // ---------------------------------------------------------------------------

@@ -27,8 +27,8 @@ SOLVER_CLASSES = {"iisph-3d": IISPHFluidSolver3D, "sesph-3d": SESPHFluidSolver3D
 
 
 def make_solver(solver, search, settings, gen, precision="fp32-kahan", reference_order=False, rest_density=1.0,
-                particle_size=1.0):
-    s = SOLVER_CLASSES[solver](search=search, precision=precision, reference_order=reference_order)
+                particle_size=1.0, **kw):
+    s = SOLVER_CLASSES[solver](search=search, precision=precision, reference_order=reference_order, **kw)
     s.parameters.rest_density = rest_density
     s.parameters.gravity = 9.81
     s.parameters.particle_size = particle_size
