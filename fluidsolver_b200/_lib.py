@@ -53,6 +53,7 @@ FS_PRECISION_FP64 = 2
 
 FS_FLAG_REFERENCE_ORDER = 0x1
 FS_FLAG_SYNC_EACH_ITERATION = 0x2
+FS_FLAG_ONE_KERNEL_STEPS = 0x4
 
 FS_TYPE_NORMAL = 0
 FS_TYPE_BOUNDARY = 1

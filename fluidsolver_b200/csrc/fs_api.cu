@@ -254,7 +254,7 @@ fs_status free_all(fs_ctx* c) {
                     c->rho_prev, c->vstar, c->anp, c->err, c->gbnd, c->tile_desc, c->tile_ent, c->keys[0], c->keys[1], c->keys64[0], c->keys64[1],
                     c->perm[0], c->perm[1], c->h2d_cell, c->h2d_rank, c->sort_hist, c->hash_table, c->cell_start, c->cell_partials, c->bbox, c->grids, c->nbr, c->nbr_count,
                     c->scene_of[0], c->scene_of[1], c->d_scene_offsets,
-                    c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->loop_ticket, c->small_stamps, c->scalars,
+                    c->csr_offsets, c->csr_indices, c->csr_counts, c->staging, c->status, c->small_stamps, c->scalars,
                     c->stats_parts, c->stats_out};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -839,6 +839,25 @@ fs_status begin_solver_phases(fs_ctx* c, float dt, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // solver steps
 // ---------------------------------------------------------------------------
+// Launches kernel<<<grid, block, smem, st>>>(args...), as a programmatic
+// dependent of the kernel before it on st when pdl is set (the kernel then
+// calls grid_dependency_wait before it reads that kernel's results).
+template <typename... KArgs, typename... Args>
+void launch_pdl(bool pdl, void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+                Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // The IISPH pressure iterations. Eagerly, the host reads the exit flag after
 // every iteration. While the stream is being captured, the loop becomes a
 // conditional WHILE node: its body is the iteration followed by the
@@ -847,22 +866,22 @@ fs_status begin_solver_phases(fs_ctx* c, float dt, cudaStream_t st) {
 template <typename Body>
 // first_done: the first iteration already ran fused into the preceding
 // phase (its scalars are accumulated); its test runs first, outside the loop.
-// body(stream, handle, set_condition) enqueues one iteration and returns
-// whether its last kernel ran the convergence test itself (LoopCheck);
-// otherwise k_iisph_check follows it.
+// body(stream) enqueues one iteration and returns whether the convergence
+// test (k_iisph_check, which follows it) may start as a programmatic
+// dependent of the iteration's last kernel (launch_pdl).
 fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_test, Body&& body,
                                 bool first_done = false) {
     const int max_it = c->prm.max_iterations;
     if (max_it <= 0) return FS_OK;
     cudaStream_t st = c->stream;
-    auto check = [&](cudaStream_t s, cudaGraphConditionalHandle h, bool set) {
+    auto check = [&](cudaStream_t s, cudaGraphConditionalHandle h, bool set, bool pdl = false) {
         c->launches++;
         if (c->scenes > 0)
-            k_iisph_check_scenes<<<1, 256, 0, s>>>(c->scalars, c->scenes, c->prm.min_iterations, max_it,
-                                                   c->prm.max_density_error, c->status, h, set);
+            launch_pdl(pdl, k_iisph_check_scenes, 1, 256, 0, s, c->scalars, c->scenes, c->prm.min_iterations, max_it,
+                       c->prm.max_density_error, (const int*)c->status, h, set);
         else
-            k_iisph_check<<<1, 1, 0, s>>>(c->scalars, c->prm.min_iterations, max_it, c->prm.max_density_error,
-                                          fp64_test, two_d, c->status, h, set);
+            launch_pdl(pdl, k_iisph_check, 1, 1, 0, s, c->scalars, c->prm.min_iterations, max_it,
+                       c->prm.max_density_error, fp64_test, two_d, (const int*)c->status, h, set);
     };
     if (!capture) {
         auto all_done = [&]() -> fs_status {
@@ -877,7 +896,8 @@ fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_t
             if (all_done() != FS_OK) return FS_OK;
         }
         for (int it = first_done ? 1 : 0; it < max_it; it++) {
-            if (!body(st, cudaGraphConditionalHandle{}, false)) check(st, 0, false);
+            const bool pdl = body(st);
+            check(st, 0, false, pdl);
             if (all_done() != FS_OK) break;
         }
         return FS_OK;
@@ -906,7 +926,8 @@ fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_t
     FS_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
     FS_CUDA(cudaStreamBeginCaptureToGraph(c->body_stream, body_graph, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
-    if (!body(c->body_stream, handle, true)) check(c->body_stream, handle, true);
+    const bool pdl = body(c->body_stream);
+    check(c->body_stream, handle, true, pdl);
     cudaError_t e = cudaGetLastError();
     cudaError_t e2 = cudaStreamEndCapture(c->body_stream, nullptr);
     if (e != cudaSuccess || e2 != cudaSuccess) return fail(FS_ERR_CUDA, "capture of the pressure loop failed");
@@ -937,19 +958,21 @@ fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 3, st));
     // the second loop also ran the first pressure iteration (fs_tiles.cuh)
-    FS_TRY(enqueue_pressure_loop(c, capture, false, true, [&](cudaStream_t bs, cudaGraphConditionalHandle h,
-                                                              bool set) {
+    FS_TRY(enqueue_pressure_loop(c, capture, false, true, [&](cudaStream_t bs) {
         c->launches += 2;
         const bool slab = !kPressureGlobalEntries;
-        // the update's last block runs the iteration's test (in place of k_iisph_check)
-        const LoopCheck chk{c->loop_ticket, c->scenes, c->prm.min_iterations, c->prm.max_iterations,
-                            c->prm.max_density_error, true, false, h, set};
         FSB_AHEAD_SWITCH(c->tuning.pressure_ahead, k_tile_iisph3d_pressure_acc,
                          <<<tiles, kPassThreads, tile_pass_smem(20, T.K, slab, T.cap), bs>>>(nf, s, T, L, k, c->scalars,
                                                                                        c->status))
-        FSB_AHEAD_SWITCH(c->tuning.pressure_ahead, k_tile_iisph3d_pressure_update,
-                         <<<tiles, kPassThreads, tile_pass_smem(32, T.K, slab, T.cap), bs>>>(nf, s, T, L, k, c->scalars,
-                                                                                       c->status, chk))
+        // the update starts as a programmatic dependent of the acceleration pass (it
+        // reads what that pass does not write before it waits), and so does the test
+        const size_t usm = tile_pass_smem(32, T.K, slab, T.cap);
+        switch (c->tuning.pressure_ahead) {
+            case 1: launch_pdl(true, k_tile_iisph3d_pressure_update<1>, tiles, kPassThreads, usm, bs, nf, s, T, L, k, c->scalars, c->status); break;
+            case 2: launch_pdl(true, k_tile_iisph3d_pressure_update<2>, tiles, kPassThreads, usm, bs, nf, s, T, L, k, c->scalars, c->status); break;
+            case 3: launch_pdl(true, k_tile_iisph3d_pressure_update<3>, tiles, kPassThreads, usm, bs, nf, s, T, L, k, c->scalars, c->status); break;
+            default: launch_pdl(true, k_tile_iisph3d_pressure_update<kMaxAhead>, tiles, kPassThreads, usm, bs, nf, s, T, L, k, c->scalars, c->status); break;
+        }
         return true;
     }, true));
     FS_TRY(mark(c, 4, st));
@@ -997,7 +1020,7 @@ template <typename R, bool KAHAN> fs_status step_iisph3d(fs_ctx* c, bool capture
     }
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 3, st));
-    FS_TRY(enqueue_pressure_loop(c, capture, false, !fp32, [&](cudaStream_t bs, cudaGraphConditionalHandle, bool) {
+    FS_TRY(enqueue_pressure_loop(c, capture, false, !fp32, [&](cudaStream_t bs) {
         c->launches += 2;
         k_iisph3d_pressure_acc<R, KAHAN><<<grid_for(no), kBlock, 0, bs>>>(no, s, L, k, c->scalars, c->status);
         k_iisph3d_pressure_update<R, KAHAN><<<grid_for(no), kBlock, 0, bs>>>(no, s, L, k, c->scalars, c->status);
@@ -1107,7 +1130,7 @@ template <typename R, bool KAHAN> fs_status step_iisph2d(fs_ctx* c, bool capture
     FS_CUDA(cudaGetLastError());
     FS_TRY(mark(c, 3, st));
     FS_TRY(enqueue_pressure_loop(c, capture, true, c->precision != FS_PRECISION_FP32,
-                                 [&](cudaStream_t bs, cudaGraphConditionalHandle, bool) {
+                                 [&](cudaStream_t bs) {
         c->launches += 2;
         k_iisph2d_pressure_acc<R, KAHAN><<<grid_for(no), kBlock, 0, bs>>>(no, s, L, k, c->scalars, c->status);
         k_iisph2d_pressure_update<R, KAHAN><<<grid_for(no), kBlock, 0, bs>>>(no, s, L, k, c->scalars, c->status);
@@ -1292,7 +1315,7 @@ fs_status solve_after_search(fs_ctx* c, float dt, fs_step_stats* stats) {
 // (fs_small.cuh): one scene of at most kSmallMax particles on the per-owner
 // lists, with the dense cell grid.
 bool small_eligible(const fs_ctx* c) {
-    return c->scenes == 0 && c->n > 0 && c->n <= kSmallMax && !tiled_mode(c) && !c->hash_table &&
+    return (c->prm.flags & FS_FLAG_ONE_KERNEL_STEPS) && c->scenes == 0 && c->n > 0 && c->n <= kSmallMax && !tiled_mode(c) && !c->hash_table &&
            c->prm.solver != FS_SOLVER_NONE && !(c->prm.flags & FS_FLAG_SYNC_EACH_ITERATION) &&
            (int64_t)c->regions * (c->cells + 1) <= kSmallMaxTable;
 }
@@ -1545,7 +1568,6 @@ static fs_status create_ctx(const fs_params* p, int32_t scenes, const int64_t* o
     FS_ALLOC(c->bbox, 6 * S);
     FS_ALLOC(c->grids, S);
     FS_ALLOC(c->status, 1);
-    FS_ALLOC(c->loop_ticket, 1);
     FS_ALLOC(c->small_stamps, 8);
     FS_ALLOC(c->scalars, S);
     if (scenes > 0) {
@@ -1571,7 +1593,6 @@ static fs_status create_ctx(const fs_params* p, int32_t scenes, const int64_t* o
     for (auto& e : c->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return bail(fail(FS_ERR_CUDA, "cudaEventCreate failed"));
     if (cudaMemsetAsync(c->status, 0, sizeof(int), c->stream) != cudaSuccess ||
-        cudaMemsetAsync(c->loop_ticket, 0, sizeof(unsigned int), c->stream) != cudaSuccess ||
         cudaStreamSynchronize(c->stream) != cudaSuccess)
         return bail(fail(FS_ERR_CUDA, "initialisation failed"));
 #undef FS_ALLOC

@@ -193,6 +193,14 @@ constexpr uint32_t kIndexMask = 0x7fffffffu;
 // device status word (first error wins)
 __device__ __forceinline__ void raise_status(int* status, int code) { atomicCAS(status, 0, code); }
 
+// Programmatic dependent launch (a kernel launched with programmatic stream
+// serialization may start while the kernel before it still runs):
+// grid_dependency_wait blocks until that kernel has completed and its writes
+// are visible (at once when launched without the attribute);
+// launch_dependents lets the next such kernel start early.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // One scene's cell grid: dims, this step's origin (cell coordinates) and the
 // offset of its cells in the concatenated cell tables.
 struct SceneGrid {

@@ -120,7 +120,6 @@ struct fs_ctx {
     size_t pinned_bytes = 0;
 
     int* status = nullptr;                  // device status word
-    unsigned int* loop_ticket = nullptr;    // blocks of the running pressure update done (LoopCheck); 0 between launches
     unsigned long long* small_stamps = nullptr;  // phase boundaries of the small-scene kernel's last step (ns)
     bool small_last = false;                // the last steps ran in the small-scene kernel
     fsb::StatsPart* stats_parts = nullptr;  // global statistics: per-block partials and the result

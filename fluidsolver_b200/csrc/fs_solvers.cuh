@@ -422,7 +422,6 @@ __device__ __forceinline__ void reduce_err_parts(ErrPart o, StepScalars* FSB_R s
     const int s0 = s_scene;
     if (!__syncthreads_and(scene == s0)) {
         add_err_part(o, sc + scene);
-        __threadfence();   // before a ticket taken after this reduction (iisph_end_of_iteration)
         return;
     }
     sc += s0;
@@ -483,9 +482,9 @@ __global__ void k_iisph3d_pressure_update(int64_t n, State<R> s, Lists L, Solver
 // or the residual say.
 // One scene's test after an iteration; returns whether its loop is done and
 // resets the iteration's accumulators.
-// The accumulators are read through volatile loads: when the test runs in
-// the last block of the iteration's own update kernel (iisph_end_of_iteration),
-// the other blocks' atomics reached L2 after this SM may have cached the line.
+// The accumulators are read through volatile loads: the small-scene kernel
+// runs the test in the kernel whose atomics produced them, where this SM may
+// hold an older copy of the line.
 __device__ __forceinline__ bool check_scene(StepScalars* FSB_R sc, int min_it, int max_it, float max_err,
                                             bool fp64_test, bool two_d) {
     const volatile StepScalars* v = sc;
@@ -567,51 +566,15 @@ __device__ __forceinline__ void iisph_check_scenes_block(StepScalars* FSB_R sc, 
 static __global__ void k_iisph_check(StepScalars* FSB_R sc, int min_it, int max_it, float max_err, bool fp64_test,
                               bool two_d, const int* FSB_R status, cudaGraphConditionalHandle handle,
                               bool set_condition) {
+    grid_dependency_wait();
     iisph_check_one(sc, min_it, max_it, max_err, fp64_test, two_d, status, handle, set_condition);
 }
 
 static __global__ void k_iisph_check_scenes(StepScalars* FSB_R sc, int scenes, int min_it, int max_it, float max_err,
                                      const int* FSB_R status, cudaGraphConditionalHandle handle,
                                      bool set_condition) {
+    grid_dependency_wait();
     iisph_check_scenes_block(sc, scenes, min_it, max_it, max_err, status, handle, set_condition);
-}
-
-// The convergence test folded into the last block of an iteration's update
-// kernel, in place of a k_iisph_check launch: every block takes a ticket
-// after its contributions to the scalars; the block that takes the last one
-// (all others' atomics are then in L2) resets the ticket and runs the test.
-struct LoopCheck {
-    unsigned int* ticket;              // zero between launches
-    int scenes;                        // 0: single-scene context
-    int min_it, max_it;
-    float max_err;
-    bool fp64_test, two_d;
-    cudaGraphConditionalHandle handle;
-    bool set_condition;                // inside the captured loop: end it through handle
-};
-
-// every thread of every block calls it once, after reduce_err_parts
-__device__ __forceinline__ void iisph_end_of_iteration(const LoopCheck& chk, StepScalars* FSB_R sc,
-                                                       const int* FSB_R status) {
-    __shared__ int s_last;
-    // the block's atomics (thread 0's, or each thread's fenced ones in a
-    // block that spans scenes) come before its ticket
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        s_last = atomicAdd(chk.ticket, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    if (chk.scenes > 0) {
-        iisph_check_scenes_block(sc, chk.scenes, chk.min_it, chk.max_it, chk.max_err, status, chk.handle,
-                                 chk.set_condition);
-    } else if (threadIdx.x == 0) {
-        iisph_check_one(sc, chk.min_it, chk.max_it, chk.max_err, chk.fp64_test, chk.two_d, status, chk.handle,
-                        chk.set_condition);
-    }
-    if (threadIdx.x == 0) *chk.ticket = 0u;
 }
 
 // CFL clamp (IISPHFluidSolver3D.hpp:525-535, SESPHFluidSolver3D.hpp:109-116) with

@@ -892,6 +892,7 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
                                                                             const StepScalars* __restrict__ sc,
                                                                             int* __restrict__ status) {
     extern __shared__ float4 tile_smem[];
+    launch_dependents();   // the update pass may be scheduled while this grid runs
     const int half = threadIdx.x & 1;
     const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
     const TileDesc* d = T.desc + blockIdx.x;
@@ -948,15 +949,17 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
     s.acc[k] = v4<float>(c.inv_rho0_sq * (a - wb * v3<float>(gbk.x, gbk.y, gbk.z)), 0.f);
 }
 
-// iteration (b): A p, relaxed Jacobi update, density error, fused scan; the
-// block that finishes last runs the iteration's convergence test (chk)
+// iteration (b): A p, relaxed Jacobi update, density error, fused scan.
+// Launched as a programmatic dependent of the acceleration pass: it reads
+// what that pass does not write before waiting for it.
 template <int AHEAD>
 __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) k_tile_iisph3d_pressure_update(int64_t n_fluid, State<float> s,
                                                                                TileLists T, Lists L,
                                                                                SolverConsts<float> c,
                                                                                StepScalars* __restrict__ sc,
-                                                                               int* __restrict__ status, LoopCheck chk) {
+                                                                               int* __restrict__ status) {
     extern __shared__ float4 tile_smem[];
+    launch_dependents();   // the convergence test may be scheduled while this grid runs
     const int half = threadIdx.x & 1;
     const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
     const int64_t kk = k < n_fluid ? k : 0;
@@ -967,56 +970,55 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
     const int scene = s.scene_of(kk);
     const StepScalars* q = sc + scene;
     const bool live = k < n_fluid && !q->done;
-    // a block with nothing to do still takes its ticket for the test
-    if (!__syncthreads_or(err) && __syncthreads_or(live)) {
-        const float dt = q->dt;
-        ErrPart o;
-        // the owner's own data, loaded while the staging lands
-        const bool valid = live;
-        const float4 pk = s.pos[kk], ak = s.acc[kk], vsk = s.vstar[kk], gbk = s.gbnd[kk];
-        const float aii = gbk.w, prk = s.p[kk];   // gbnd.w: the diagonal (second loop)
-        const FastSpline S(c.kern);
-        Acc<float, true> ap;
-        float part = 0.f;
-        auto pair = [&](const float4& pj, const float4& aj) {
-            const V3<float> xij = sub3(pk, pj);
-            part = __fmaf_rn(pj.w * S.grad(r2_of(xij)), dot3(sub3(ak, aj), xij), part);
-        };
-        auto flush = [&] {
-            ap.add(part);
-            part = 0.f;
-        };
-        // boundary neighbors enter through sum_bnd m_j gradW (second loop)
-        bool done = true;
-        if (h.nranges == kTileFallback) {
-            // the owner's 32-bit list, split between its two threads
-            if (valid) walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.acc[j]); }, flush);
-        } else {
-            float4* sp = tile_smem;
-            float4* sa = tile_smem + T.cap;
-            __shared__ TileStage stg;
-            const float4* src4[2] = {s.pos, s.acc};
-            float4* dst4[2] = {sp, sa};
-            const TileSlab slab = slab_at(tile_smem, 32, T.K, T.cap);
-            stage_tile_async<2, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
-            const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
-            uint2 ahead[AHEAD];
-            prefetch_tile_list<kPressureGlobalEntries>(T, h, k, half, ahead);
-            done = stage_tile_wait(stg, status);
-            if (done && valid)
-                walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool) {
-                    pair(at_offset(sp, off), at_offset(sa, off));
-                }, flush);
-        }
-        if (done) {
-            // boundary: sum_bnd m_j dot(a_i, gradW) = dot(a_i, sum_bnd m_j gradW)
-            const float sum = pair_total(ap) + dot3(v3<float>(ak.x, ak.y, ak.z), v3<float>(gbk.x, gbk.y, gbk.z));
-            if (!half && valid)
-                o = iisph3d_pressure_update_tail<float>(k, s, c, dt, v3<float>(ak.x, ak.y, ak.z), sum, vsk, aii, prk);
-        }
-        reduce_err_parts(o, sc, scene);
+    if (__syncthreads_or(err) || !__syncthreads_or(live)) return;
+    const float dt = q->dt;
+    ErrPart o;
+    // the owner's own data, loaded while the staging lands
+    const bool valid = live;
+    const float4 pk = s.pos[kk], vsk = s.vstar[kk], gbk = s.gbnd[kk];
+    const float aii = gbk.w, prk = s.p[kk];   // gbnd.w: the diagonal (second loop)
+    const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
+    grid_dependency_wait();   // the accelerations of this iteration
+    const float4 ak = s.acc[kk];
+    const FastSpline S(c.kern);
+    Acc<float, true> ap;
+    float part = 0.f;
+    auto pair = [&](const float4& pj, const float4& aj) {
+        const V3<float> xij = sub3(pk, pj);
+        part = __fmaf_rn(pj.w * S.grad(r2_of(xij)), dot3(sub3(ak, aj), xij), part);
+    };
+    auto flush = [&] {
+        ap.add(part);
+        part = 0.f;
+    };
+    // boundary neighbors enter through sum_bnd m_j gradW (second loop)
+    bool done = true;
+    if (h.nranges == kTileFallback) {
+        // the owner's 32-bit list, split between its two threads
+        if (valid) walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.acc[j]); }, flush);
+    } else {
+        float4* sp = tile_smem;
+        float4* sa = tile_smem + T.cap;
+        __shared__ TileStage stg;
+        const float4* src4[2] = {s.pos, s.acc};
+        float4* dst4[2] = {sp, sa};
+        const TileSlab slab = slab_at(tile_smem, 32, T.K, T.cap);
+        stage_tile_async<2, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
+        uint2 ahead[AHEAD];
+        prefetch_tile_list<kPressureGlobalEntries>(T, h, k, half, ahead);
+        done = stage_tile_wait(stg, status);
+        if (done && valid)
+            walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool) {
+                pair(at_offset(sp, off), at_offset(sa, off));
+            }, flush);
     }
-    iisph_end_of_iteration(chk, sc, status);
+    if (done) {
+        // boundary: sum_bnd m_j dot(a_i, gradW) = dot(a_i, sum_bnd m_j gradW)
+        const float sum = pair_total(ap) + dot3(v3<float>(ak.x, ak.y, ak.z), v3<float>(gbk.x, gbk.y, gbk.z));
+        if (!half && valid)
+            o = iisph3d_pressure_update_tail<float>(k, s, c, dt, v3<float>(ak.x, ak.y, ak.z), sum, vsk, aii, prk);
+    }
+    reduce_err_parts(o, sc, scene);
 }
 
 // ---------------------------------------------------------------------------

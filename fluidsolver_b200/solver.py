@@ -328,13 +328,15 @@ class FluidSolverBase:
     DEFAULT_SEARCH = "hashed-3d"
 
     def __init__(self, search: str | None = None, precision: str = "fp32-kahan", reference_order: bool = False,
-                 device: int = 0, neighbor_capacity: int = 0, sync_each_iteration: bool = False):
+                 device: int = 0, neighbor_capacity: int = 0, sync_each_iteration: bool = False,
+                 one_kernel_steps: bool = False):
         self.search = search or self.DEFAULT_SEARCH
         if self.search not in SEARCH_KINDS:
             raise ValueError(f"unknown neighborhood search {self.search!r}")
         self.precision = precision
         self.reference_order = reference_order
         self.sync_each_iteration = sync_each_iteration
+        self.one_kernel_steps = one_kernel_steps   # FS_FLAG_ONE_KERNEL_STEPS
         self.device = device
         self.neighbor_capacity = neighbor_capacity
         self.parameters = SimulationParameters()
@@ -353,7 +355,8 @@ class FluidSolverBase:
         F.lib().fs_params_default(ctypes.byref(p), self.DIM, self.SOLVER, SEARCH_KINDS[self.search])
         p.precision = PRECISIONS[self.precision]
         p.flags = (F.FS_FLAG_REFERENCE_ORDER if self.reference_order else 0) | \
-            (F.FS_FLAG_SYNC_EACH_ITERATION if self.sync_each_iteration else 0)
+            (F.FS_FLAG_SYNC_EACH_ITERATION if self.sync_each_iteration else 0) | \
+            (F.FS_FLAG_ONE_KERNEL_STEPS if self.one_kernel_steps else 0)
         p.device = self.device
         p.rest_density = self.parameters.rest_density
         p.gravity = self.parameters.gravity

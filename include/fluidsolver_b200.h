@@ -90,6 +90,10 @@ typedef enum fs_precision {
                                          (IISPHFluidSolver3D.hpp:60-64 vs :210); for bit-level parity runs */
 #define FS_FLAG_SYNC_EACH_ITERATION 0x2u /* host-driven IISPH loop (one readback per iteration) instead of the
                                             device-side early exit inside a CUDA graph */
+#define FS_FLAG_ONE_KERNEL_STEPS 0x4u  /* fs_step / fs_run of a single scene of at most 4,096 particles (not
+                                          the 3D fast mode, not compact hashing) run whole steps in one launch
+                                          of one block instead of a CUDA graph of per-phase kernels; the same
+                                          results bit for bit */
 
 /* Particle types (Particle.hpp:7-12). */
 #define FS_TYPE_NORMAL 0

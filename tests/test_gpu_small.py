@@ -1,11 +1,11 @@
-"""The small-scene step kernel (csrc/fs_small.cu): fs_step / fs_run of a
-single scene of at most 4,096 particles run whole steps in one launch of one
-block. Its phases call the per-particle functions of the step-by-step kernels
-in the same order, so it must give the same state bit for bit as the
-host-driven step-by-step path (FS_FLAG_SYNC_EACH_ITERATION) in every
-precision mode, solver and contract it serves; the reference-order mode's
-1000-step 2D dam against the reference itself runs through it as well
-(tests/test_gpu_configs.py::test_sesph2d_dam_1000_steps_bit_exact)."""
+"""The small-scene step kernel (csrc/fs_small.cu): with FS_FLAG_ONE_KERNEL_STEPS,
+fs_step / fs_run of a single scene of at most 4,096 particles run whole steps
+in one launch of one block. Its phases call the per-particle functions of the
+step-by-step kernels in the same order, so it must give the same state bit
+for bit as the host-driven step-by-step path (FS_FLAG_SYNC_EACH_ITERATION) in
+every precision mode, solver and contract it serves (and so, in the
+reference-order mode, the reference's own results, which the step-by-step
+path matches: tests/test_gpu_solvers.py, tests/test_gpu_configs.py)."""
 import numpy as np
 import pytest
 
@@ -55,7 +55,7 @@ FIELDS = ("position", "velocity", "density", "pressure", "mass", "type", "tag")
 def pair(name):
     solver, search, settings, gen, prec, exact, build = CASES[name]
     col = build()
-    small = make_solver(solver, search, settings, gen, precision=prec, reference_order=exact)
+    small = make_solver(solver, search, settings, gen, precision=prec, reference_order=exact, one_kernel_steps=True)
     steps = make_solver(solver, search, settings, gen, precision=prec, reference_order=exact, sync_each_iteration=True)
     small.data.collection = col
     steps.data.collection = ParticleCollection(**{f: getattr(col, f).copy() for f in FIELDS if getattr(col, f) is not None})
@@ -103,7 +103,8 @@ def test_small_kernel_grows_the_lists():
     n = len(pos)
     col = ParticleCollection(position=pos, velocity=np.zeros_like(pos), mass=np.ones(n, np.float32),
                              density=np.ones(n, np.float32), type=np.zeros(n, np.uint8))
-    small = make_solver("sesph-2d", "hashed-2d", SES2, GEN2, precision="fp32", reference_order=True)
+    small = make_solver("sesph-2d", "hashed-2d", SES2, GEN2, precision="fp32", reference_order=True,
+                        one_kernel_steps=True)
     steps = make_solver("sesph-2d", "hashed-2d", SES2, GEN2, precision="fp32", reference_order=True,
                         sync_each_iteration=True)
     small.data.collection = col
