@@ -414,7 +414,7 @@ def run_batched(args, device, rank, world, max_over_ranks, barrier, tuning=None)
     configure_iisph(batch)
     if tuning and tuning["tuned"]:   # the shapes the 1M dam chose
         batch.set_tuning(tuning["first_loop_prefetch"], tuning["pressure_prefetch"], tuning["tile_cap"],
-                         tuning["block_size"])
+                         tuning["block_size"], tuning["pressure_threads_per_owner"])
     batch.run(args.warmup)
     stream = torch.cuda.ExternalStream(L.fs_stream(batch.ctx), device=torch.device("cuda", device))
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -441,7 +441,7 @@ def run_batched(args, device, rank, world, max_over_ranks, barrier, tuning=None)
             solver = make_solver(sc, device)
             if tuning and tuning["tuned"]:
                 solver.set_tuning(tuning["first_loop_prefetch"], tuning["pressure_prefetch"], tuning["tile_cap"],
-                                  tuning["block_size"])
+                                  tuning["block_size"], tuning["pressure_threads_per_owner"])
             solver.run(args.warmup)
             s2 = torch.cuda.ExternalStream(L.fs_stream(solver.ctx), device=torch.device("cuda", device))
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -119,14 +119,16 @@ class FsGlobalStats(ctypes.Structure):
 class FsTuning(ctypes.Structure):
     _fields_ = [
         ("tuned", c_int32), ("first_loop_prefetch", c_int32), ("pressure_prefetch", c_int32), ("tile_cap", c_int32),
-        ("block_size", c_int32), ("reserved", c_int32),
+        ("block_size", c_int32), ("pressure_threads_per_owner", c_int32),
         ("first_loop_ms", c_float * 4), ("pressure_iteration_ms", c_float * 4), ("step_ms_by_tile_cap", c_float * 4),
         ("step_ms_by_block_size", c_float * 3), ("fallback_tiles_by_tile_cap", c_float * 4),
+        ("pressure_iteration_ms_by_threads", c_float * 3),
     ]
 
 
 TILE_CAPS = (1024, 1536, 2048, 3072)   # include/fluidsolver_b200.h, fs_tuning
 BLOCK_SIZES = (128, 256, 512)
+THREADS_PER_OWNER = (1, 2, 4)
 
 
 class FsCamera(ctypes.Structure):

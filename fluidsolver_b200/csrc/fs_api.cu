@@ -934,6 +934,23 @@ fs_status enqueue_pressure_loop(fs_ctx* c, bool capture, bool two_d, bool fp64_t
     return FS_OK;
 }
 
+// One pressure iteration on tile lists: the acceleration pass, then the
+// update as its programmatic dependent (it reads what that pass does not
+// write before it waits); the convergence test follows (enqueue_pressure_loop).
+#define FSB_ACC_LAUNCH(...) __VA_ARGS__<<<tiles, threads, acc_smem, bs>>>(nf, s, T, L, k, c->scalars, c->status)
+#define FSB_UPDATE_LAUNCH(...) \
+    launch_pdl(true, __VA_ARGS__, tiles, threads, upd_smem, bs, nf, s, T, L, k, c->scalars, c->status)
+void enqueue_tile_pressure_iteration(fs_ctx* c, cudaStream_t bs, unsigned tiles, int64_t nf, const State<float>& s,
+                                     const TileLists& T, const Lists& L, const SolverConsts<float>& k) {
+    const int tpo = c->tuning.pressure_tpo;
+    const unsigned threads = (unsigned)(kTileOwners * tpo);
+    const size_t acc_smem = tile_pass_smem(20, T.K, false, T.cap), upd_smem = tile_pass_smem(32, T.K, false, T.cap);
+    FSB_PRESSURE_SWITCH(c->tuning.pressure_ahead, tpo, k_tile_iisph3d_pressure_acc, FSB_ACC_LAUNCH)
+    FSB_PRESSURE_SWITCH(c->tuning.pressure_ahead, tpo, k_tile_iisph3d_pressure_update, FSB_UPDATE_LAUNCH)
+}
+#undef FSB_ACC_LAUNCH
+#undef FSB_UPDATE_LAUNCH
+
 // the IISPH 3D step on tile lists (fs_tiles.cuh)
 fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
     cudaStream_t st = c->stream;
@@ -960,19 +977,7 @@ fs_status step_iisph3d_tiled(fs_ctx* c, bool capture) {
     // the second loop also ran the first pressure iteration (fs_tiles.cuh)
     FS_TRY(enqueue_pressure_loop(c, capture, false, true, [&](cudaStream_t bs) {
         c->launches += 2;
-        const bool slab = !kPressureGlobalEntries;
-        FSB_AHEAD_SWITCH(c->tuning.pressure_ahead, k_tile_iisph3d_pressure_acc,
-                         <<<tiles, kPassThreads, tile_pass_smem(20, T.K, slab, T.cap), bs>>>(nf, s, T, L, k, c->scalars,
-                                                                                       c->status))
-        // the update starts as a programmatic dependent of the acceleration pass (it
-        // reads what that pass does not write before it waits), and so does the test
-        const size_t usm = tile_pass_smem(32, T.K, slab, T.cap);
-        switch (c->tuning.pressure_ahead) {
-            case 1: launch_pdl(true, k_tile_iisph3d_pressure_update<1>, tiles, kPassThreads, usm, bs, nf, s, T, L, k, c->scalars, c->status); break;
-            case 2: launch_pdl(true, k_tile_iisph3d_pressure_update<2>, tiles, kPassThreads, usm, bs, nf, s, T, L, k, c->scalars, c->status); break;
-            case 3: launch_pdl(true, k_tile_iisph3d_pressure_update<3>, tiles, kPassThreads, usm, bs, nf, s, T, L, k, c->scalars, c->status); break;
-            default: launch_pdl(true, k_tile_iisph3d_pressure_update<kMaxAhead>, tiles, kPassThreads, usm, bs, nf, s, T, L, k, c->scalars, c->status); break;
-        }
+        enqueue_tile_pressure_iteration(c, bs, tiles, nf, s, T, L, k);
         return true;
     }, true));
     FS_TRY(mark(c, 4, st));
@@ -2182,6 +2187,7 @@ fs_status fs_autotune(fs_ctx* c, fs_tuning* out) {
     out->pressure_prefetch = c->tuning.pressure_ahead;
     out->tile_cap = c->tuning.cap;
     out->block_size = c->tuning.block;
+    out->pressure_threads_per_owner = c->tuning.pressure_tpo;
     // nothing tunable unless the IISPH passes are tiled
     if (!tiled_mode(c) || c->prm.solver != FS_SOLVER_IISPH_3D || c->n_fluid == 0) return FS_OK;
     FS_CUDA(cudaSetDevice(c->device));
@@ -2240,7 +2246,20 @@ fs_status fs_autotune(fs_ctx* c, fs_tuning* out) {
     }
     t->tuning.l1_ahead = best_l1;
     t->tuning.pressure_ahead = best_pi;
-    // 2. staging cap
+    // 2. threads per owner in the pressure passes, at the chosen depth
+    const int tpos[3] = {1, 2, 4};
+    double t_tpo = 1e30;
+    int best_tpo = t->tuning.pressure_tpo;
+    for (int q = 0; q < 3; q++) {
+        FS_TRY(fs_upload(t, &v));
+        t->tuning.pressure_tpo = tpos[q];
+        FS_TRY(time_steps(t, 2, 4, step_ms, l1_ms, iter_ms, samples));
+        if (!samples) continue;
+        out->pressure_iteration_ms_by_threads[q] = (float)iter_ms;
+        if (iter_ms < t_tpo) t_tpo = iter_ms, best_tpo = tpos[q];
+    }
+    t->tuning.pressure_tpo = best_tpo;
+    // 3. staging cap
     const int caps[4] = {1024, 1536, 2048, 3072};
     double best = 1e30;
     int best_cap = t->tuning.cap;
@@ -2253,7 +2272,7 @@ fs_status fs_autotune(fs_ctx* c, fs_tuning* out) {
         if (step_ms < best) best = step_ms, best_cap = caps[q];
     }
     t->tuning.cap = best_cap;
-    // 3. block size of the per-particle kernels
+    // 4. block size of the per-particle kernels
     const int blocks[3] = {128, 256, 512};
     best = 1e30;
     int best_block = t->tuning.block;
@@ -2269,6 +2288,7 @@ fs_status fs_autotune(fs_ctx* c, fs_tuning* out) {
     out->pressure_prefetch = best_pi;
     out->tile_cap = best_cap;
     out->block_size = best_block;
+    out->pressure_threads_per_owner = best_tpo;
     return fs_set_tuning(c, out);
 }
 
@@ -2359,13 +2379,17 @@ fs_status fs_set_tuning(fs_ctx* c, const fs_tuning* in) {
         return fail(FS_ERR_INVALID, "tile_cap must be 0 or a multiple of 4 in 256.." + std::to_string(kTileCapMax));
     if (in->block_size != 0 && (in->block_size < 32 || in->block_size > 1024 || in->block_size % 32 != 0))
         return fail(FS_ERR_INVALID, "block_size must be 0 or a multiple of 32 in 32..1024");
+    const int tpo = in->pressure_threads_per_owner;
+    if (tpo != 0 && tpo != 1 && tpo != 2 && tpo != 4)
+        return fail(FS_ERR_INVALID, "pressure_threads_per_owner must be 0, 1, 2 or 4");
     TileTuning next = c->tuning;
     next.l1_ahead = in->first_loop_prefetch;
     next.pressure_ahead = in->pressure_prefetch;
     if (in->tile_cap) next.cap = in->tile_cap;
     if (in->block_size) next.block = in->block_size;
+    if (tpo) next.pressure_tpo = tpo;
     if (next.l1_ahead != c->tuning.l1_ahead || next.pressure_ahead != c->tuning.pressure_ahead ||
-        next.cap != c->tuning.cap || next.block != c->tuning.block) {
+        next.cap != c->tuning.cap || next.block != c->tuning.block || next.pressure_tpo != c->tuning.pressure_tpo) {
         FS_CUDA(cudaSetDevice(c->device));
         if (c->stream) FS_CUDA(cudaStreamSynchronize(c->stream));
         clear_graphs(c);   // the captured steps launch the old instantiations and shapes

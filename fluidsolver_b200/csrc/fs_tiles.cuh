@@ -609,20 +609,95 @@ __device__ __forceinline__ void walk_tile_list(const TileLists& T, const TileSla
     }
 }
 
-// Walks owner k's 32-bit list in a fallback tile, the entries of this half
-// of the owner's thread pair (half, half + 2, ...): f(sorted index, boundary)
+// Walks owner k's 32-bit list in a fallback tile, the entries of this
+// thread of the owner's TPO (half, half + TPO, ...): f(sorted index, boundary)
 // for each (the fluid entries only with FLUID_ONLY), flush() after every 8
 // visits and at the end, as for_tile_entries does.
-template <bool FLUID_ONLY, typename F, typename Flush>
+template <bool FLUID_ONLY, int TPO = 2, typename F, typename Flush>
 __device__ __forceinline__ void walk_fallback_list(const Lists& L, int64_t k, int half, F&& f, Flush&& flush) {
     const uint32_t nn = L.size(k);
     uint32_t visited = 0;
-    for (uint32_t q = (uint32_t)half; q < nn; q += 2) {
+    for (uint32_t q = (uint32_t)half; q < nn; q += TPO) {
         const uint32_t e = L.at(k, q);
         const bool bnd = (e & kBoundaryBit) != 0u;
         if (FLUID_ONLY && bnd) continue;
         f(e & kIndexMask, bnd);
         if ((++visited & 7u) == 0u) flush();
+    }
+    flush();
+}
+
+// The pressure passes with TPO threads per owner (1, 2 or 4; fs_autotune
+// chooses): each thread takes a contiguous 8 / TPO of every octet of the
+// owner's fluid entries, 4 / TPO 32-bit words, read straight from the global
+// octet planes AHEAD octets ahead of use.
+template <int TPO> struct OctetShare {
+    uint32_t w[4 / TPO];
+};
+template <int TPO>
+__device__ __forceinline__ OctetShare<TPO> load_share(const uint4* __restrict__ e, int64_t stride, uint32_t o, int part) {
+    OctetShare<TPO> r;
+    const uint4* q = e + o * stride;
+    if constexpr (TPO == 1) {
+        const uint4 v = __ldg(q);
+        r.w[0] = v.x;
+        r.w[1] = v.y;
+        r.w[2] = v.z;
+        r.w[3] = v.w;
+    } else if constexpr (TPO == 2) {
+        const uint2 v = __ldg(reinterpret_cast<const uint2*>(q) + part);
+        r.w[0] = v.x;
+        r.w[1] = v.y;
+    } else {
+        r.w[0] = __ldg(reinterpret_cast<const uint32_t*>(q) + part);
+    }
+    return r;
+}
+// the first AHEAD octets' shares of owner k, issued before the tile's
+// staging has landed (h.octets: the tile's longest list in octets)
+template <int TPO, int AHEAD>
+__device__ __forceinline__ void prefetch_shares(const TileLists& T, const TileHead& h, int64_t k, int part,
+                                                OctetShare<TPO> (&ahead)[AHEAD]) {
+#pragma unroll
+    for (int d = 0; d < AHEAD; d++) {
+        if ((uint32_t)d < h.octets) {
+            ahead[d] = load_share<TPO>(T.ent + k, T.stride, d, part);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4 / TPO; i++) ahead[d].w[i] = 0u;
+        }
+    }
+}
+// Visits this thread's share of owner k's fluid entries: f(byte offset into
+// a staged float4 array) for each, flush() after every 8 visits and at the
+// end. With TPO 2 the visits and flushes are those of for_tile_entries.
+template <int TPO, int AHEAD, typename F, typename Flush>
+__device__ __forceinline__ void walk_fluid_shares(const TileLists& T, int64_t k, uint32_t cnt, int part,
+                                                  OctetShare<TPO> (&ahead)[AHEAD], F&& f, Flush&& flush) {
+    constexpr int W = 4 / TPO;
+    const uint32_t all = min(cnt & 0xffffu, (uint32_t)T.K);
+    const uint32_t n = min(cnt >> 16, all);
+    const uint32_t full = n / 8, octets = (n + 7) / 8;
+    for (uint32_t o = 0; o < full; o++) {
+        const OctetShare<TPO> cur = ahead[0];
+#pragma unroll
+        for (int d = 0; d + 1 < AHEAD; d++) ahead[d] = ahead[d + 1];
+        if (o + AHEAD < octets) ahead[AHEAD - 1] = load_share<TPO>(T.ent + k, T.stride, o + AHEAD, part);
+#pragma unroll
+        for (int i = 0; i < W; i++) {
+            f(cur.w[i] & 0xffffu);
+            f(cur.w[i] >> 16);
+        }
+        if ((o & (TPO - 1)) == TPO - 1) flush();
+    }
+    const int m = (int)(n - full * 8) - part * (8 / TPO);   // this thread's entries of the last, partial octet
+    if (m > 0) {
+        const OctetShare<TPO> cur = ahead[0];
+#pragma unroll
+        for (int i = 0; i < W; i++) {
+            if (2 * i < m) f(cur.w[i] & 0xffffu);
+            if (2 * i + 1 < m) f(cur.w[i] >> 16);
+        }
     }
     flush();
 }
@@ -638,6 +713,7 @@ struct TileTuning {
     int pressure_ahead = 3;
     int cap = kTileCap;   // staged candidates per tile
     int block = 128;      // threads per block of the step's per-particle kernels (keys, reorder, integration)
+    int pressure_tpo = 2; // threads per owner in the pressure passes (1, 2, 4)
 };
 
 // the slab after a pass's staged candidates (bytes_per_candidate each)
@@ -650,13 +726,15 @@ template <typename T> __device__ __forceinline__ const T& at_offset(const T* bas
     return *reinterpret_cast<const T*>(reinterpret_cast<const char*>(base) + off);
 }
 
-// value of a compensated accumulator, summed over the two threads of an owner
-__device__ __forceinline__ float pair_total(const Acc<float, true>& a) {
-    const float v = a.s - a.c;
-    return v + __shfl_xor_sync(0xffffffffu, v, 1);
+// value of a compensated accumulator, summed over the TPO threads of an owner
+template <int TPO = 2> __device__ __forceinline__ float pair_total(const Acc<float, true>& a) {
+    float v = a.s - a.c;
+#pragma unroll
+    for (int o = 1; o < TPO; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
 }
-__device__ __forceinline__ V3<float> pair_total(const Acc3<float, true>& a) {
-    return v3<float>(pair_total(a.x), pair_total(a.y), pair_total(a.z));
+template <int TPO = 2> __device__ __forceinline__ V3<float> pair_total(const Acc3<float, true>& a) {
+    return v3<float>(pair_total<TPO>(a.x), pair_total<TPO>(a.y), pair_total<TPO>(a.z));
 }
 
 __device__ __forceinline__ V3<float> sub3(float4 a, float4 b) { return v3<float>(a.x - b.x, a.y - b.y, a.z - b.z); }
@@ -884,17 +962,22 @@ __global__ void __launch_bounds__(kPassThreads, kL2GlobalEntries ? 4 : 3) k_tile
     reduce_err_parts(o, sc, scene);
 }
 
+// Blocks of the pressure passes with TPO threads per owner, and how many of
+// them an SM holds (the register budget each is compiled for)
+template <int TPO> constexpr int pressure_threads() { return kTileOwners * TPO; }
+template <int TPO> constexpr int acc_blocks_per_sm() { return TPO == 1 ? 6 : (TPO == 2 ? 5 : 2); }
+template <int TPO> constexpr int update_blocks_per_sm() { return TPO == 1 ? 4 : (TPO == 2 ? 4 : 2); }
+
 // iteration (a): pressure acceleration
-template <int AHEAD>
-__global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) k_tile_iisph3d_pressure_acc(int64_t n_fluid, State<float> s,
-                                                                            TileLists T, Lists L,
-                                                                            SolverConsts<float> c,
-                                                                            const StepScalars* __restrict__ sc,
-                                                                            int* __restrict__ status) {
+template <int AHEAD, int TPO>
+__global__ void __launch_bounds__(pressure_threads<TPO>(), acc_blocks_per_sm<TPO>()) k_tile_iisph3d_pressure_acc(
+    int64_t n_fluid, State<float> s, TileLists T, Lists L, SolverConsts<float> c, const StepScalars* __restrict__ sc,
+    int* __restrict__ status) {
+    static_assert(kPressureGlobalEntries, "the pressure passes read their entries from the global octet planes");
     extern __shared__ float4 tile_smem[];
     launch_dependents();   // the update pass may be scheduled while this grid runs
-    const int half = threadIdx.x & 1;
-    const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
+    const int half = threadIdx.x % TPO;   // this thread's share of the owner's entries
+    const int64_t k = blockIdx.x * (int64_t)kTileOwners + threadIdx.x / TPO;
     const TileDesc* d = T.desc + blockIdx.x;
     const int err = *status;
     const TileHead h = load_head(d);
@@ -922,9 +1005,9 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
     // boundary neighbors enter through sum_bnd m_j gradW (second loop), so
     // only the fluid candidates and entries are visited
     if (h.nranges == kTileFallback) {
-        // the owner's 32-bit list, split between its two threads
+        // the owner's 32-bit list, split between its threads
         if (valid)
-            walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.p[j]); }, flush);
+            walk_fallback_list<true, TPO>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.p[j]); }, flush);
     } else {
         float4* sp = tile_smem;
         float* sa = reinterpret_cast<float*>(tile_smem + T.cap);
@@ -932,17 +1015,17 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
         const float4* src4[1] = {s.pos};
         float4* dst4[1] = {sp};
         const TileSlab slab = slab_at(tile_smem, 20, T.K, T.cap);
-        stage_tile_async<1, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, s.p, sa, T, slab);
-        const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
-        uint2 ahead[AHEAD];
-        prefetch_tile_list<kPressureGlobalEntries>(T, h, k, half, ahead);
+        stage_tile_async<1, true, false>(stg, d, h, rg, src4, dst4, s.p, sa, T, slab);
+        const uint32_t cnt = T.count[kk];
+        OctetShare<TPO> ahead[AHEAD];
+        prefetch_shares<TPO, AHEAD>(T, h, k, half, ahead);
         if (!stage_tile_wait(stg, status)) return;
         if (valid)
-            walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool) {
+            walk_fluid_shares<TPO, AHEAD>(T, k, cnt, half, ahead, [&](uint32_t off) {
                 pair(at_offset(sp, off), at_offset(sa, off >> 2));
             }, flush);
     }
-    const V3<float> a = pair_total(pa);
+    const V3<float> a = pair_total<TPO>(pa);
     if (half || !valid) return;
     // boundary: - sum_bnd (lambda m_j p_i / rho0^2) gradW, lambda = 2 gamma (single layer) or 2
     const float wb = (c.single_layer ? c.two_gamma : 2.f) * prk;
@@ -952,16 +1035,14 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 5 : 4) 
 // iteration (b): A p, relaxed Jacobi update, density error, fused scan.
 // Launched as a programmatic dependent of the acceleration pass: it reads
 // what that pass does not write before waiting for it.
-template <int AHEAD>
-__global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) k_tile_iisph3d_pressure_update(int64_t n_fluid, State<float> s,
-                                                                               TileLists T, Lists L,
-                                                                               SolverConsts<float> c,
-                                                                               StepScalars* __restrict__ sc,
-                                                                               int* __restrict__ status) {
+template <int AHEAD, int TPO>
+__global__ void __launch_bounds__(pressure_threads<TPO>(), update_blocks_per_sm<TPO>()) k_tile_iisph3d_pressure_update(
+    int64_t n_fluid, State<float> s, TileLists T, Lists L, SolverConsts<float> c, StepScalars* __restrict__ sc,
+    int* __restrict__ status) {
     extern __shared__ float4 tile_smem[];
     launch_dependents();   // the convergence test may be scheduled while this grid runs
-    const int half = threadIdx.x & 1;
-    const int64_t k = blockIdx.x * (int64_t)kTileOwners + (threadIdx.x >> 1);
+    const int half = threadIdx.x % TPO;   // this thread's share of the owner's entries
+    const int64_t k = blockIdx.x * (int64_t)kTileOwners + threadIdx.x / TPO;
     const int64_t kk = k < n_fluid ? k : 0;
     const TileDesc* d = T.desc + blockIdx.x;
     const int err = *status;
@@ -977,7 +1058,7 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
     const bool valid = live;
     const float4 pk = s.pos[kk], vsk = s.vstar[kk], gbk = s.gbnd[kk];
     const float aii = gbk.w, prk = s.p[kk];   // gbnd.w: the diagonal (second loop)
-    const uint32_t cnt = kPressureGlobalEntries ? T.count[kk] : 0u;
+    const uint32_t cnt = T.count[kk];
     grid_dependency_wait();   // the accelerations of this iteration
     const float4 ak = s.acc[kk];
     const FastSpline S(c.kern);
@@ -994,8 +1075,9 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
     // boundary neighbors enter through sum_bnd m_j gradW (second loop)
     bool done = true;
     if (h.nranges == kTileFallback) {
-        // the owner's 32-bit list, split between its two threads
-        if (valid) walk_fallback_list<true>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.acc[j]); }, flush);
+        // the owner's 32-bit list, split between its threads
+        if (valid)
+            walk_fallback_list<true, TPO>(L, k, half, [&](uint32_t j, bool) { pair(s.pos[j], s.acc[j]); }, flush);
     } else {
         float4* sp = tile_smem;
         float4* sa = tile_smem + T.cap;
@@ -1003,18 +1085,18 @@ __global__ void __launch_bounds__(kPassThreads, kPressureGlobalEntries ? 4 : 3) 
         const float4* src4[2] = {s.pos, s.acc};
         float4* dst4[2] = {sp, sa};
         const TileSlab slab = slab_at(tile_smem, 32, T.K, T.cap);
-        stage_tile_async<2, true, !kPressureGlobalEntries>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
-        uint2 ahead[AHEAD];
-        prefetch_tile_list<kPressureGlobalEntries>(T, h, k, half, ahead);
+        stage_tile_async<2, true, false>(stg, d, h, rg, src4, dst4, nullptr, nullptr, T, slab);
+        OctetShare<TPO> ahead[AHEAD];
+        prefetch_shares<TPO, AHEAD>(T, h, k, half, ahead);
         done = stage_tile_wait(stg, status);
         if (done && valid)
-            walk_tile_list<kPressureGlobalEntries, true, AHEAD>(T, slab, k, cnt, half, ahead, [&](uint32_t off, bool) {
+            walk_fluid_shares<TPO, AHEAD>(T, k, cnt, half, ahead, [&](uint32_t off) {
                 pair(at_offset(sp, off), at_offset(sa, off));
             }, flush);
     }
     if (done) {
         // boundary: sum_bnd m_j dot(a_i, gradW) = dot(a_i, sum_bnd m_j gradW)
-        const float sum = pair_total(ap) + dot3(v3<float>(ak.x, ak.y, ak.z), v3<float>(gbk.x, gbk.y, gbk.z));
+        const float sum = pair_total<TPO>(ap) + dot3(v3<float>(ak.x, ak.y, ak.z), v3<float>(gbk.x, gbk.y, gbk.z));
         if (!half && valid)
             o = iisph3d_pressure_update_tail<float>(k, s, c, dt, v3<float>(ak.x, ak.y, ak.z), sum, vsk, aii, prk);
     }
@@ -1219,15 +1301,41 @@ __global__ void k_export_solver_lists(int64_t n_owners, bool tiled, TileLists T,
         default: KERNEL<kMaxAhead> __VA_ARGS__; break; \
     }
 
+// the pressure passes' instantiation for a prefetch depth and a number of
+// threads per owner (1, 2, 4)
+#define FSB_PRESSURE_SWITCH(ahead, tpo, KERNEL, CALL) \
+    switch ((ahead) * 8 + (tpo)) {                   \
+        case 1 * 8 + 1: CALL(KERNEL<1, 1>); break;    \
+        case 2 * 8 + 1: CALL(KERNEL<2, 1>); break;    \
+        case 3 * 8 + 1: CALL(KERNEL<3, 1>); break;    \
+        case 4 * 8 + 1: CALL(KERNEL<4, 1>); break;    \
+        case 1 * 8 + 4: CALL(KERNEL<1, 4>); break;    \
+        case 2 * 8 + 4: CALL(KERNEL<2, 4>); break;    \
+        case 3 * 8 + 4: CALL(KERNEL<3, 4>); break;    \
+        case 4 * 8 + 4: CALL(KERNEL<4, 4>); break;    \
+        case 1 * 8 + 2: CALL(KERNEL<1, 2>); break;    \
+        case 2 * 8 + 2: CALL(KERNEL<2, 2>); break;    \
+        case 3 * 8 + 2: CALL(KERNEL<3, 2>); break;    \
+        default: CALL(KERNEL<4, 2>); break;           \
+    }
+static_assert(kMaxAhead == 4, "FSB_PRESSURE_SWITCH lists depths 1..4");
+
+template <int AHEAD, int TPO> inline cudaError_t set_pressure_smem(int K) {
+    cudaError_t e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_acc<AHEAD, TPO>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)tile_pass_smem(20, K, false, kTileCapMax));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_update<AHEAD, TPO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_pass_smem(32, K, false, kTileCapMax));
+    return e;
+}
+
 template <int AHEAD> inline cudaError_t set_tuned_pass_smem(int K) {
     cudaError_t e = cudaFuncSetAttribute(k_tile_iisph3d_l1<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)tile_pass_smem(36, K, !kL1GlobalEntries, kTileCapMax));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_acc<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tile_pass_smem(20, K, !kPressureGlobalEntries, kTileCapMax));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_tile_iisph3d_pressure_update<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tile_pass_smem(32, K, !kPressureGlobalEntries, kTileCapMax));
+    if (e == cudaSuccess) e = set_pressure_smem<AHEAD, 1>(K);
+    if (e == cudaSuccess) e = set_pressure_smem<AHEAD, 2>(K);
+    if (e == cudaSuccess) e = set_pressure_smem<AHEAD, 4>(K);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_tile_sesph3d_density<AHEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)tile_pass_smem(16, K, false, kTileCapMax));

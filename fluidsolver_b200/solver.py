@@ -229,6 +229,9 @@ def _tuning_dict(t) -> dict:
     """fs_tuning as a dict: the values in use and every measured time, keyed by the value tried."""
     return {"tuned": bool(t.tuned), "first_loop_prefetch": t.first_loop_prefetch,
             "pressure_prefetch": t.pressure_prefetch, "tile_cap": t.tile_cap, "block_size": t.block_size,
+            "pressure_threads_per_owner": t.pressure_threads_per_owner,
+            "pressure_iteration_ms_by_threads": {q: v for q, v in zip(F.THREADS_PER_OWNER,
+                                                                    t.pressure_iteration_ms_by_threads) if v > 0},
             "first_loop_ms": {d + 1: v for d, v in enumerate(t.first_loop_ms) if v > 0},
             "pressure_iteration_ms": {d + 1: v for d, v in enumerate(t.pressure_iteration_ms) if v > 0},
             "step_ms_by_tile_cap": {c: v for c, v in zip(F.TILE_CAPS, t.step_ms_by_tile_cap) if v > 0},
@@ -463,10 +466,11 @@ class FluidSolverBase:
         return _tuning_dict(t)
 
     def set_tuning(self, first_loop_prefetch: int, pressure_prefetch: int, tile_cap: int = 0,
-                   block_size: int = 0) -> None:
-        """The fast mode's launch shapes (0 keeps the current cap / block size)."""
+                   block_size: int = 0, pressure_threads_per_owner: int = 0) -> None:
+        """The fast mode's launch shapes (0 keeps the current cap / block size / threads per owner)."""
         t = F.FsTuning(first_loop_prefetch=first_loop_prefetch, pressure_prefetch=pressure_prefetch,
-                       tile_cap=tile_cap, block_size=block_size)
+                       tile_cap=tile_cap, block_size=block_size,
+                       pressure_threads_per_owner=pressure_threads_per_owner)
         F.check(F.lib().fs_set_tuning(self.ctx, ctypes.byref(t)))
 
     # ---- the fluid path tracer (visualizer/raytracer/FluidRaytracer3D) ----
@@ -606,11 +610,12 @@ class BatchedIISPHFluidSolver3D:
         self.last_stats = None
 
     def set_tuning(self, first_loop_prefetch: int, pressure_prefetch: int, tile_cap: int = 0,
-                   block_size: int = 0) -> None:
+                   block_size: int = 0, pressure_threads_per_owner: int = 0) -> None:
         """The fast mode's launch shapes, e.g. as IISPHFluidSolver3D.autotune() chose them on a
-        representative scene (fs_set_tuning); 0 keeps the current cap / block size."""
+        representative scene (fs_set_tuning); 0 keeps the current cap / block size / threads per owner."""
         t = F.FsTuning(first_loop_prefetch=first_loop_prefetch, pressure_prefetch=pressure_prefetch,
-                       tile_cap=tile_cap, block_size=block_size)
+                       tile_cap=tile_cap, block_size=block_size,
+                       pressure_threads_per_owner=pressure_threads_per_owner)
         F.check(F.lib().fs_set_tuning(self.ctx, ctypes.byref(t)))
 
     @property

@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define FS_ABI_VERSION 3
+#define FS_ABI_VERSION 4
 
 typedef enum fs_status {
     FS_OK = 0,
@@ -304,12 +304,14 @@ typedef struct fs_tuning {
     int32_t pressure_prefetch;
     int32_t tile_cap;                /* fs_set_tuning: 0 keeps the current one */
     int32_t block_size;              /* fs_set_tuning: 0 keeps the current one */
-    int32_t reserved;
+    int32_t pressure_threads_per_owner; /* 1, 2 or 4 threads walk an owner's list in the pressure
+                                           passes (fs_set_tuning: 0 keeps the current one) */
     float first_loop_ms[4];          /* measured per depth 1..4 (0: not tried) */
     float pressure_iteration_ms[4];  /* per pressure iteration, per depth 1..4 */
     float step_ms_by_tile_cap[4];    /* whole step, caps 1024, 1536, 2048, 3072 */
     float step_ms_by_block_size[3];  /* whole step, block sizes 128, 256, 512 */
     float fallback_tiles_by_tile_cap[4]; /* fraction of tiles on 32-bit lists, per cap */
+    float pressure_iteration_ms_by_threads[3]; /* per pressure iteration, 1, 2, 4 threads per owner */
 } fs_tuning;
 fs_status fs_autotune(fs_ctx* ctx, fs_tuning* out);
 fs_status fs_set_tuning(fs_ctx* ctx, const fs_tuning* in);

@@ -40,7 +40,7 @@ def test_library_exports_every_declared_symbol(L):
 
 
 def test_abi_version(L):
-    assert L.fs_abi_version() == 3
+    assert L.fs_abi_version() == 4
 
 
 def test_structs_match_the_header(tmp_path):
