@@ -63,7 +63,7 @@ FS_TYPE_INACTIVE = 2
 EXPORTED_SYMBOLS = (
     "fs_abi_version", "fs_last_error", "fs_params_default", "fs_create", "fs_destroy", "fs_set_params",
     "fs_upload", "fs_download", "fs_find_neighbors", "fs_get_neighbors_csr", "fs_query_position", "fs_solve_step", "fs_step",
-    "fs_run", "fs_last_phase_times", "fs_stream", "fs_launch_count", "fs_batch_create", "fs_batch_run",
+    "fs_run", "fs_last_phase_times", "fs_stream", "fs_launch_count", "fs_small_blocks", "fs_batch_create", "fs_batch_run",
     "fs_query_position_noalloc", "fs_get_solver_lists_csr", "fs_boundary_preprocess", "fs_global_statistics",
     "fs_particles_file_info", "fs_particles_file_read", "fs_particles_file_write", "fs_dump",
     "fs_autotune", "fs_set_tuning", "fs_trace_rays", "fs_render_settings_default", "fs_render",
@@ -199,6 +199,8 @@ def lib() -> ctypes.CDLL:
     L.fs_stream.restype = c_void_p
     L.fs_launch_count.argtypes = [ctx_p]
     L.fs_launch_count.restype = c_int64
+    L.fs_small_blocks.argtypes = [ctx_p]
+    L.fs_small_blocks.restype = c_int32
     L.fs_batch_create.argtypes = [POINTER(FsParams), c_int32, c_void_p, POINTER(ctx_p)]
     L.fs_batch_run.argtypes = [ctx_p, c_int32, c_float, c_void_p]
     for name in ("fs_create", "fs_destroy", "fs_set_params", "fs_upload", "fs_download", "fs_find_neighbors",

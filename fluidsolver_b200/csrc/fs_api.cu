@@ -1385,9 +1385,9 @@ fs_status launch_small(fs_ctx* c, int32_t steps, float dt) {
     a.stamps = c->small_stamps;
     cudaError_t e;
     switch (c->prm.solver) {
-        case FS_SOLVER_IISPH_3D: e = launch_small_steps<R, KAHAN, kSmallIISPH3D>(a, c->stream); break;
-        case FS_SOLVER_IISPH_2D: e = launch_small_steps<R, KAHAN, kSmallIISPH2D>(a, c->stream); break;
-        default: e = launch_small_steps<R, KAHAN, kSmallSESPH>(a, c->stream); break;
+        case FS_SOLVER_IISPH_3D: e = launch_small_steps<R, KAHAN, kSmallIISPH3D>(a, c->stream, &c->small_blocks); break;
+        case FS_SOLVER_IISPH_2D: e = launch_small_steps<R, KAHAN, kSmallIISPH2D>(a, c->stream, &c->small_blocks); break;
+        default: e = launch_small_steps<R, KAHAN, kSmallSESPH>(a, c->stream, &c->small_blocks); break;
     }
     if (e != cudaSuccess) return fail(FS_ERR_CUDA, std::string("small-scene steps: ") + cudaGetErrorString(e));
     c->launches++;
@@ -2604,6 +2604,8 @@ fs_status fs_last_phase_times(fs_ctx* c, float* ms5) {
 void* fs_stream(fs_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 int64_t fs_launch_count(fs_ctx* c) { return c ? c->launches : 0; }
+
+int32_t fs_small_blocks(fs_ctx* c) { return c && c->small_last ? c->small_blocks : 0; }
 
 fs_status fs_batch_create(const fs_params* p, int32_t scenes, const int64_t* offsets, fs_ctx** out) {
     if (out) *out = nullptr;

@@ -122,6 +122,7 @@ struct fs_ctx {
     int* status = nullptr;                  // device status word
     unsigned long long* small_stamps = nullptr;  // phase boundaries of the small-scene kernel's last step (ns)
     bool small_last = false;                // the last steps ran in the small-scene kernel
+    int small_blocks = 0;                   // the blocks of its last launch
     fsb::StatsPart* stats_parts = nullptr;  // global statistics: per-block partials and the result
     fsb::StatsOut* stats_out = nullptr;
     fsb::StepScalars* scalars = nullptr;    // device

@@ -746,6 +746,15 @@ __device__ __forceinline__ V3<float> fma3(float s, V3<float> d, V3<float> acc) {
     return v3<float>(__fmaf_rn(s, d.x, acc.x), __fmaf_rn(s, d.y, acc.y), __fmaf_rn(s, d.z, acc.z));
 }
 
+// 1/sqrt(x) for normal x (the MUFU approximation; with x >= FastSpline::kTiny no input
+// is denormal, so the flush-to-zero form gives rsqrtf's result without its
+// denormal-input handling)
+__device__ __forceinline__ float rsqrt_normal(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // The cubic spline of the fast mode, evaluated from a listed pair's squared
 // distance r2 (r2 <= (2h)^2). The reference's piecewise cubic
 // (CubicSplineKernel3D.cpp:7-66) with its polynomials expanded, q = |d| / h:
@@ -764,13 +773,13 @@ struct FastSpline {
     __device__ explicit FastSpline(const SplineKernel<float>& k)
         : a(k.alpha), inv_h(1.f / k.h), a9(9.f * k.alpha), a12(12.f * k.alpha), a3h(3.f * k.alpha * k.h) {}
     __device__ __forceinline__ float grad(float r2) const {
-        const float inv = rsqrtf(fmaxf(r2, kTiny));
+        const float inv = rsqrt_normal(fmaxf(r2, kTiny));
         const float q = (r2 * inv) * inv_h;
         const float t = fmaxf(2.f - q, 0.f);
         return q < 1.f ? __fmaf_rn(a9, q, -a12) : -a3h * (t * t) * inv;
     }
     __device__ __forceinline__ void value_grad(float r2, float& w, float& f) const {
-        const float inv = rsqrtf(fmaxf(r2, kTiny));
+        const float inv = rsqrt_normal(fmaxf(r2, kTiny));
         const float q = (r2 * inv) * inv_h;
         const float t = fmaxf(2.f - q, 0.f);
         const bool inner = q < 1.f;

@@ -276,6 +276,10 @@ void* fs_stream(fs_ctx* ctx);
 /* Number of this library's own kernel launches since the context was created
  * (library kernels such as the radix sort's are not counted). */
 int64_t fs_launch_count(fs_ctx* ctx);
+/* Blocks (one thread-block cluster) of the last small-scene launch
+ * (FS_FLAG_ONE_KERNEL_STEPS), 0 when the last steps took the step-by-step
+ * path. */
+int32_t fs_small_blocks(fs_ctx* ctx);
 
 /* ---- tuning ------------------------------------------------------------------
  * The 3D fast mode's launch shapes (no reference counterpart: the reference's

@@ -1,11 +1,15 @@
 """The small-scene step kernel (csrc/fs_small.cu): with FS_FLAG_ONE_KERNEL_STEPS,
 fs_step / fs_run of a single scene of at most 4,096 particles run whole steps
-in one launch of one block. Its phases call the per-particle functions of the
-step-by-step kernels in the same order, so it must give the same state bit
-for bit as the host-driven step-by-step path (FS_FLAG_SYNC_EACH_ITERATION) in
-every precision mode, solver and contract it serves (and so, in the
-reference-order mode, the reference's own results, which the step-by-step
-path matches: tests/test_gpu_solvers.py, tests/test_gpu_configs.py)."""
+in one launch of one thread-block cluster (up to 16 blocks, about 256
+particles per block: the dams here take 4 to 16). Its phases call the
+per-particle functions of the step-by-step kernels in the same order, on
+shared-memory copies of the fields they gather, and its sort and cell table
+are its own (a cluster-wide stable sort, a binary-searched table), so it must
+give the same state bit for bit as the host-driven step-by-step path
+(FS_FLAG_SYNC_EACH_ITERATION) in every precision mode, solver and contract it
+serves (and so, in the reference-order mode, the reference's own results,
+which the step-by-step path matches: tests/test_gpu_solvers.py,
+tests/test_gpu_configs.py)."""
 import numpy as np
 import pytest
 
@@ -81,6 +85,10 @@ def test_small_kernel_equals_the_step_by_step_path(name):
 def test_small_kernel_runs_whole_steps_in_one_launch():
     small, steps = pair("iisph2d-hashed-exact")
     small.run(1)
+    # 1,218 particles: a cluster of 8 blocks of about 150 (16 and 4 blocks
+    # serve the other scenes here; a device that schedules no cluster that
+    # large runs fewer, larger blocks)
+    assert F.lib().fs_small_blocks(small.ctx) in (1, 2, 4, 8)
     before = F.lib().fs_launch_count(small.ctx)
     small.run(20)
     # fs_run: its first step settles the list capacity (one launch), the
@@ -120,3 +128,30 @@ def test_small_kernel_grows_the_lists():
         assert bits_equal(getattr(x, f), getattr(y, f)), f
     small.close()
     steps.close()
+
+
+@pytest.mark.parametrize("dims", [(6, 5, 14, 12), (12, 10, 24, 20)])
+def test_small_kernel_on_one_and_two_blocks(dims):
+    """Scenes of 162 and 330 particles: a cluster of one block and of two
+    (about 256 particles per block), in both 2D solvers and exact order."""
+    nx, ny, w, h = dims
+    for solver, settings in (("sesph-2d", SES2), ("iisph-2d", IIS2)):
+        col = scenes.breaking_dam_2d(nx, ny, width=w, height=h, seed=5).collection
+        small = make_solver(solver, "hashed-2d", settings, GEN2, precision="fp32", reference_order=True,
+                            one_kernel_steps=True)
+        steps = make_solver(solver, "hashed-2d", settings, GEN2, precision="fp32", reference_order=True,
+                            sync_each_iteration=True)
+        small.data.collection = col
+        steps.data.collection = ParticleCollection(**{f: getattr(col, f).copy() for f in FIELDS
+                                                      if getattr(col, f) is not None})
+        a = small.run(8)
+        assert F.lib().fs_small_blocks(small.ctx) == (1 if len(col) <= 256 else 2)
+        assert F.lib().fs_small_blocks(steps.ctx) == 0
+        for _ in range(8):
+            b = steps.step()
+        assert a.iterations == b.iterations
+        x, y = small.collection(), steps.collection()
+        for f in ("position", "velocity", "density", "pressure"):
+            assert bits_equal(getattr(x, f), getattr(y, f)), (solver, dims, f)
+        small.close()
+        steps.close()
