@@ -149,8 +149,11 @@ __device__ __forceinline__ unsigned long long cluster_load64(uint32_t addr) {
 // at most 40 bits), by the whole cluster, in two
 // phases. (1) Each CTA sorts its share of the pairs in shared memory as
 // unique 64-bit words (masked key << 12 | index: equal keys keep their index
-// order, which is what makes the result that of a stable sort), with a
-// bitonic network. (2) After a cluster barrier each CTA copies every CTA's
+// order, which is what makes the result that of a stable sort): each word
+// goes to the place given by the number of the share's words below it (a
+// bitonic network for shares above 2 kSmallThreads words, which only a
+// device that schedules no large cluster gives). (2) After a cluster
+// barrier each CTA copies every CTA's
 // sorted run out of that CTA's shared memory (distributed shared memory);
 // a word's place in the output is the sum over the runs of the number of
 // words below it, found by binary searches that step through all runs
@@ -162,69 +165,84 @@ __device__ __noinline__ void sort_small_cluster(const Team& T, int64_t n, int bi
     static_assert(kSmallMax <= 4096, "the index field of the sort words has 12 bits");
     unsigned long long* run = reinterpret_cast<unsigned long long*>(smem);
     unsigned long long* all = run + kSmallMax;
-    const int t = threadIdx.x;
-    const int64_t share = T.share(n), lo = min(n, (int64_t)T.rank * share), m = T.end(n) - lo;
-    int64_t P = 1;
-    while (P < m) P <<= 1;
+    const uint32_t t = threadIdx.x, N = (uint32_t)n;   // n <= kSmallMax: 32-bit indices throughout
+    const uint32_t share = (uint32_t)T.share(n), lo = min(N, T.rank * share), m = (uint32_t)T.end(n) - lo;
     // the radix passes' whole 8-bit digits: the key bits sort_small_block orders by
     const int rbits = (bits + 7) / 8 * 8;
     const K kmask = rbits >= (int)(8 * sizeof(K)) ? ~K(0) : (K(1) << rbits) - K(1);
-    for (int64_t i = t; i < P; i += kSmallThreads)
-        run[i] = i < m ? ((unsigned long long)(kin[lo + i] & kmask) << 12) | (unsigned long long)(lo + i) : ~0ull;
-    __syncthreads();
-    for (int64_t k = 2; k <= P; k <<= 1) {
-        for (int64_t j = k >> 1; j > 0; j >>= 1) {
-            for (int64_t i = t; i < P; i += kSmallThreads) {
-                const int64_t x = i ^ j;
-                if (x > i) {
-                    const unsigned long long u = run[i], w = run[x];
-                    if ((u > w) == ((i & k) == 0)) {
-                        run[i] = w;
-                        run[x] = u;
+    auto word = [&](uint32_t i) { return ((unsigned long long)(kin[lo + i] & kmask) << 12) | (unsigned long long)(lo + i); };
+    if (m <= 2 * kSmallThreads) {
+        // the share's words, each placed by the number of words below it
+        // (every thread reads the same word at a time: a broadcast)
+        for (uint32_t i = t; i < m; i += kSmallThreads) all[i] = word(i);
+        __syncthreads();
+        for (uint32_t i = t; i < m; i += kSmallThreads) {
+            const unsigned long long v = all[i];
+            uint32_t c = 0;
+#pragma unroll 8
+            for (uint32_t q = 0; q < m; q++) c += all[q] < v ? 1u : 0u;
+            run[c] = v;
+        }
+    } else {
+        // a larger share (a device that schedules only small clusters): bitonic network
+        uint32_t P = 1;
+        while (P < m) P <<= 1;
+        for (uint32_t i = t; i < P; i += kSmallThreads) run[i] = i < m ? word(i) : ~0ull;
+        __syncthreads();
+        for (uint32_t k = 2; k <= P; k <<= 1) {
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t i = t; i < P; i += kSmallThreads) {
+                    const uint32_t x = i ^ j;
+                    if (x > i) {
+                        const unsigned long long u = run[i], w = run[x];
+                        if ((u > w) == ((i & k) == 0)) {
+                            run[i] = w;
+                            run[x] = u;
+                        }
                     }
                 }
+                __syncthreads();
             }
-            __syncthreads();
         }
     }
     cluster_sync();
+    // run q: words [base[q], base[q] + len[q]) of `all`, in every CTA
+    uint32_t base[kSmallMaxCtas], len[kSmallMaxCtas];
+#pragma unroll
+    for (int q = 0; q < kSmallMaxCtas; q++) {
+        base[q] = min(N, (uint32_t)q * share);
+        len[q] = (q < (int)T.size ? min(N, (uint32_t)(q + 1) * share) : base[q]) - base[q];
+    }
     // every run's element j at once (their remote loads in flight together)
-    for (int64_t j0 = 0; j0 < share; j0 += kSmallThreads) {
-        const int64_t j = j0 + t;
+    for (uint32_t j0 = 0; j0 < share; j0 += kSmallThreads) {
+        const uint32_t j = j0 + t;
         unsigned long long v[kSmallMaxCtas];
 #pragma unroll
-        for (int q = 0; q < kSmallMaxCtas; q++) {
-            const int64_t b = min(n, (int64_t)q * share), len = min(n, (int64_t)(q + 1) * share) - b;
-            if (q < (int)T.size && j < len) v[q] = cluster_load64(cluster_addr(run + j, q));
-        }
+        for (int q = 0; q < kSmallMaxCtas; q++)
+            if (j < len[q]) v[q] = cluster_load64(cluster_addr(run + j, q));
 #pragma unroll
-        for (int q = 0; q < kSmallMaxCtas; q++) {
-            const int64_t b = min(n, (int64_t)q * share), len = min(n, (int64_t)(q + 1) * share) - b;
-            if (q < (int)T.size && j < len) all[b + j] = v[q];
-        }
+        for (int q = 0; q < kSmallMaxCtas; q++)
+            if (j < len[q]) all[base[q] + j] = v[q];
     }
     __syncthreads();
-    int64_t top = 1;   // the largest power of two <= share
+    uint32_t top = 1;   // the largest power of two <= share
     while (top * 2 <= share) top <<= 1;
-    for (int64_t i = t; i < m; i += kSmallThreads) {
+    for (uint32_t i = t; i < m; i += kSmallThreads) {
         const unsigned long long v = run[i];
         uint32_t pos[kSmallMaxCtas];
 #pragma unroll
         for (int q = 0; q < kSmallMaxCtas; q++) pos[q] = 0u;
-        for (int64_t step = top; step > 0; step >>= 1) {
+        for (uint32_t step = top; step > 0; step >>= 1) {
 #pragma unroll
             for (int q = 0; q < kSmallMaxCtas; q++) {
-                if (q < (int)T.size) {
-                    const int64_t b = min(n, (int64_t)q * share), len = min(n, (int64_t)(q + 1) * share) - b;
-                    const int64_t p = pos[q] + step;
-                    if (p <= len && all[b + p - 1] < v) pos[q] = (uint32_t)p;
-                }
+                const uint32_t p = pos[q] + step;
+                if (p <= len[q] && all[base[q] + p - 1] < v) pos[q] = p;
             }
         }
-        int64_t rank = 0;
+        uint32_t rank = 0;
 #pragma unroll
         for (int q = 0; q < kSmallMaxCtas; q++) rank += pos[q];
-        const int64_t k = (int64_t)(v & 0xfffu);
+        const uint32_t k = (uint32_t)(v & 0xfffu);
         kout[rank] = kin[k];
         vout[rank] = vin[k];
     }
@@ -393,7 +411,7 @@ __device__ __forceinline__ int small_search(const SmallStepArgs<R>& a, const Tea
         w.r = a.radius;
         w.r2 = a.radius2;
         w.dim = a.dim;
-        w.regions = a.regions;
+        w.regions = (int)min(a.regions, 2);   // solver lists never hold inactive particles (search_impl's walk)
         w.candidates_inactive = false;
         w.trunc = a.trunc;
         w.length_test = a.dim == 2;
