@@ -634,6 +634,27 @@ def run_configs(args, device):
                                       "k 1000, nu 0.01, dt 0.001", "gpu_ms_per_step": ms2,
                           "gpu_particle_steps_per_s": d2.n_fluid / (ms2 / 1e3),
                           "cpu": None}
+
+    def dam2d_ms(precision, reference_order, one_kernel_steps):
+        s = SESPHFluidSolver(search="hashed-2d", device=device, precision=precision,
+                             reference_order=reference_order, one_kernel_steps=one_kernel_steps)
+        s.parameters.rest_density, s.parameters.gravity, s.parameters.particle_size = 1.0, 9.81, 1.0
+        s.settings.StiffnessK, s.settings.Viscosity = 1000.0, 0.01
+        s.timestep_generator.settings.timestep = 0.001
+        s.data.collection = d2.collection
+        ms, _ = gpu_time(s, 200)
+        blocks = int(L.fs_small_blocks(s.ctx))
+        s.close()
+        return ms, blocks
+
+    # the same dam in the bit-exact reference-order mode, and both modes in
+    # the small-scene cluster kernel (FS_FLAG_ONE_KERNEL_STEPS: whole steps
+    # in one launch of one thread-block cluster)
+    ms2x, _ = dam2d_ms("fp32", True, False)
+    ms2c, blocks = dam2d_ms("fp32-kahan", False, True)
+    ms2cx, _ = dam2d_ms("fp32", True, True)
+    out["sesph2d_dam"].update({"gpu_ms_per_step_reference_order": ms2x, "cluster_kernel_ms_per_step": ms2c,
+                               "cluster_kernel_ms_per_step_reference_order": ms2cx, "cluster_blocks": blocks})
     if not args.no_cpu_baseline:
         from oracle import ref_oracle as R
         cpu = ref_time("sesph-2d", "hashed-2d", d2, (1.0, 9.81, 1.0), R.sesph2d_settings(1000.0, 0.01),

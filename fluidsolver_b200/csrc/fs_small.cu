@@ -229,24 +229,61 @@ __device__ __noinline__ void sort_small_cluster(const Team& T, int64_t n, int bi
     while (top * 2 <= share) top <<= 1;
     for (uint32_t i = t; i < m; i += kSmallThreads) {
         const unsigned long long v = run[i];
-        uint32_t pos[kSmallMaxCtas];
-#pragma unroll
-        for (int q = 0; q < kSmallMaxCtas; q++) pos[q] = 0u;
-        for (uint32_t step = top; step > 0; step >>= 1) {
-#pragma unroll
-            for (int q = 0; q < kSmallMaxCtas; q++) {
-                const uint32_t p = pos[q] + step;
-                if (p <= len[q] && all[base[q] + p - 1] < v) pos[q] = p;
-            }
-        }
+        // The input is the last step's sorted order, so a block's share
+        // mostly spans its own range of cells: against most runs a word lies
+        // below the first or above the last word, and only the runs it
+        // falls inside take a binary search.
         uint32_t rank = 0;
-#pragma unroll
-        for (int q = 0; q < kSmallMaxCtas; q++) rank += pos[q];
+#pragma unroll 1
+        for (int q = 0; q < (int)T.size; q++) {
+            const uint32_t b = min(N, (uint32_t)q * share), l = min(N, (uint32_t)(q + 1) * share) - b;
+            if (l == 0 || v < all[b]) continue;
+            if (v > all[b + l - 1]) {
+                rank += l;
+                continue;
+            }
+            uint32_t pos = 0;
+            for (uint32_t step = top; step > 0; step >>= 1) {
+                const uint32_t p = pos + step;
+                if (p <= l && all[b + p - 1] < v) pos = p;
+            }
+            rank += pos;
+        }
         const uint32_t k = (uint32_t)(v & 0xfffu);
         kout[rank] = kin[k];
         vout[rank] = vin[k];
     }
     cluster_sync();
+}
+
+// a float4 field and two scalar fields at once (the SESPH forces' gather)
+template <typename R>
+__device__ __noinline__ void stage_fields3(V4<R>* d4, const V4<R>* s4, R* d1, const R* s1, R* d2, const R* s2,
+                                           int64_t m) {
+    constexpr int U = 4;
+    for (int64_t b = threadIdx.x; b < m; b += U * kSmallThreads) {
+        V4<R> v[U];
+        R x[U], y[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t i = b + u * kSmallThreads;
+            if (i < m) {
+                v[u] = s4[i];
+                x[u] = s1[i];
+                y[u] = s2[i];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t i = b + u * kSmallThreads;
+            if (i < m) {
+                d4[i] = v[u];
+                d1[i] = x[u];
+                d2[i] = y[u];
+            }
+        }
+    }
+    __syncthreads();
 }
 
 // the search of one step (search_impl); returns the buffer set now current
@@ -362,7 +399,8 @@ __device__ __forceinline__ int small_search(const SmallStepArgs<R>& a, const Tea
                           (const V4<R>*)f.acc, (V4<R>*)g.acc, (const V4<R>*)f.ext, (V4<R>*)g.ext, rho[cur], rho[nx],
                           (const R*)f.p, (R*)g.p, f.type, g.type, f.hidx, g.hidx, nullptr, nullptr);
     }
-    cluster_sync();
+    // (no barrier: the cell table below needs only the sorted keys; the
+    // barrier after it publishes both)
     cur = nx;
     // Cell-start table (cell_start_table: zeroed run counts, scanned in
     // place): entry t, for region g and cell c at t = g (cells + 1) + c, is the
@@ -571,9 +609,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_small_steps(SmallStepArgs<
             stamp(T, a.stamps, 2);
             State<R> va = v;   // the acceleration gathers velocities, densities and pressures
             if (a.stage) {
-                stage_field(g.f4, s.vel, n);
-                stage_field(g.f1, s.rho, n);
-                stage_field(g.f2, s.p, n);
+                stage_fields3<R>(g.f4, s.vel, g.f1, s.rho, g.f2, s.p, n);
                 va.vel = g.f4;
                 va.rho = g.f1;
                 va.p = g.f2;
