@@ -34,6 +34,7 @@ import pytest
 
 from conftest import bits_equal
 from fluidsolver_b200 import NeighborhoodSearch, ParticleCollection, scenes
+from fluidsolver_b200 import _lib as F
 from tests.test_gpu_solvers import make_solver, simulator_step
 
 pytestmark = pytest.mark.gpu
@@ -102,23 +103,29 @@ def with_state(col0, st):
 # ---------------------------------------------------------------------------
 # 2D SESPH dam, all 1,000 steps
 # ---------------------------------------------------------------------------
+@pytest.mark.parametrize("path", ["graph", "cluster"])
 @pytest.mark.parametrize("search", ["hashed-2d", "quadratic-2d"])
-def test_sesph2d_dam_1000_steps_bit_exact(ref_oracle, search):
+def test_sesph2d_dam_1000_steps_bit_exact(ref_oracle, search, path):
     """The 2D SESPH breaking dam for its full 1,000 steps, every field of
     every checkpoint bit for bit. On hashed-2d this holds because the device
     keeps the reference's insertion order inside a cell
     (HashedNeighborhoodSearch.cpp:117-151), which decides the float
-    summation order once particles start changing cells."""
+    summation order once particles start changing cells. Both device paths:
+    the CUDA graph of per-phase kernels, and the small-scene kernel
+    (FS_FLAG_ONE_KERNEL_STEPS: up to 800 steps per launch of one
+    thread-block cluster)."""
     sc = scenes.breaking_dam_2d()
     col = sc.collection
     gen = (0.001, 0.4, 0.25)
     ref = ref_oracle.RefSolver("sesph-2d", search, col, (1.0, 9.81, 1.0), ref_oracle.sesph2d_settings(1000.0, 0.01),
                                gen, variant="omp")
-    s = make_solver("sesph-2d", search, [1000.0, 0.01], gen, precision="fp32", reference_order=True)
+    s = make_solver("sesph-2d", search, [1000.0, 0.01], gen, precision="fp32", reference_order=True,
+                    one_kernel_steps=path == "cluster")
     s.data.collection = col
-    done = 0
+    done, blocks = 0, []
     for chk in (1, 2, 10, 50, 100, 200, 400, 600, 800, 1000):
         s.run(chk - done)
+        blocks.append(int(F.lib().fs_small_blocks(s.ctx)))
         ref.run(chk - done)
         done = chk
         out, r = s.collection(), ref.state()
@@ -126,7 +133,9 @@ def test_sesph2d_dam_1000_steps_bit_exact(ref_oracle, search):
             assert bits_equal(getattr(out, f), r[f]), (search, chk, f)
     # the dam has moved: the order within cells has had to follow arrivals
     assert np.max(np.abs(out.position - col.position)) > 1.0
-    record(f"sesph2d_dam/{search}", {"steps": done, "bit_identical": True})
+    # the path the steps took
+    assert max(blocks) > 0 if path == "cluster" else max(blocks) == 0, blocks
+    record(f"sesph2d_dam/{search}/{path}", {"steps": done, "bit_identical": True})
     s.close()
     ref.close()
 
