@@ -1,7 +1,7 @@
 // The small-scene step kernel (fs_small.cuh): search and solver phases of
-// whole steps in one block, in the order of the step-by-step path
-// (fs_api.cu: search_impl, begin_solver_phases, step_sesph, step_iisph3d,
-// step_iisph2d), each phase a block-stride loop over the particles that
+// whole steps in one thread-block cluster, in the order of the step-by-step
+// path (fs_api.cu: search_impl, begin_solver_phases, step_sesph,
+// step_iisph3d, step_iisph2d), each phase a loop over the particles that
 // calls the same per-particle device function as the separate kernel does.
 #define FSB_COHERENT_LOADS 1
 
@@ -23,9 +23,10 @@ __device__ __forceinline__ unsigned long long global_ns() {
 __device__ __forceinline__ int status_now(const int* status) { return *(const volatile int*)status; }
 
 // The launch is one cluster of CTAs (1 to kSmallMaxCtas, one per SM). The
-// per-particle phases are block-stride loops over the whole cluster; the
-// one-block steps (the sort, the cell-table scan, the per-step scalars, the
-// convergence test) run in CTA 0. Phases are separated by the cluster
+// per-particle phases are loops over each CTA's share of the particles; the
+// per-step scalars and the convergence test are thread 0 of CTA 0's, the
+// sort and the cell table are the cluster's (sort_small_cluster, the
+// binary-searched table). Phases are separated by the cluster
 // barrier, whose arrive releases and whose wait acquires at cluster scope:
 // what one CTA wrote to global memory before the barrier is what every CTA
 // reads after it (this translation unit loads through coherent paths only).
