@@ -79,3 +79,25 @@ def test_the_largest_scene_fits_the_index_field():
     keys = rng.integers(0, 1 << 12, MAX_PARTICLES, dtype=np.uint64)
     order = cluster_sort_model(keys, 14, 16)
     assert order == np.argsort(keys, kind="stable").tolist()
+
+
+@pytest.mark.parametrize("regions", [1, 2, 3])
+def test_binary_searched_cell_table_equals_the_scanned_counts(regions):
+    """The small-scene kernel's cell-start table: entry t (region g, cell c
+    at t = g (cells + 1) + c) is the first sorted index whose key's entry is
+    >= t, found by binary search; the step-by-step path writes each run's
+    length at its first particle's entry and scans the table. Same table."""
+    rng = np.random.default_rng(regions)
+    cells, key_bits = 700, 10
+    for n in (0, 1, 50, 3000):
+        g = rng.integers(0, regions, n)
+        c = rng.integers(0, cells, n)
+        keys = np.sort((g << key_bits) | c)
+        te = (keys >> key_bits) * (cells + 1) + (keys & ((1 << key_bits) - 1))
+        table = regions * (cells + 1)
+        counts = np.zeros(table, np.int64)
+        for t in te:
+            counts[t] += 1
+        scanned = np.concatenate([[0], np.cumsum(counts)[:-1]])
+        searched = np.searchsorted(te, np.arange(table), side="left")
+        assert np.array_equal(scanned, searched)
